@@ -1,0 +1,22 @@
+"""bamrex_b200: the explicit finite-volume path of BAMReX on B200 (sm_100a).
+
+MUSCL-Hancock reconstruction with half-step evolution, HLLC / SLIC / FORCE /
+Lax-Friedrichs interface fluxes, the split conservative update, ghost fill
+and the CFL reduction, in hand-written CUDA kernels behind the C ABI of
+``libbamrex_cuda.so`` (include/bamrex_cuda.h).  This package holds the build
+recipe (``bamrex_b200.build``), the ctypes binding (``_abi``), the Python
+mirror of the reference's level surface (``level``) and seeded problem
+generators (``problems``).
+"""
+from . import problems
+from ._abi import (BC_PERIODIC, BC_REFLECTIVE, BC_TRANSMISSIVE, FORCE, HLLC, LAX_FRIEDRICHS, LIMITERS, METHODS,
+                   MINBEE, MUSCL_HANCOCK, SLIC, SUPERBEE, VAN_ALBADA, VAN_LEER, BamrexError, lib)
+from .level import (Level, Packing, Parm, compute_flux, compute_flux_LR, conservative_update, decompose,
+                    sweep_box, sweep_update)
+
+__all__ = [
+    "Level", "Packing", "Parm", "compute_flux", "compute_flux_LR", "conservative_update", "decompose", "sweep_box",
+    "sweep_update", "problems", "lib", "BamrexError", "MUSCL_HANCOCK", "HLLC", "SLIC", "FORCE", "LAX_FRIEDRICHS",
+    "METHODS", "LIMITERS", "MINBEE", "VAN_LEER", "VAN_ALBADA", "SUPERBEE", "BC_TRANSMISSIVE", "BC_PERIODIC",
+    "BC_REFLECTIVE",
+]

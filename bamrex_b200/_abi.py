@@ -1,0 +1,167 @@
+"""ctypes declarations of libbamrex_cuda.so (include/bamrex_cuda.h).
+
+The shared library is the product: there is no Python or CPU fallback.  If
+it is missing or fails to load, :func:`lib` raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libbamrex_cuda.so")
+
+MAX_NCOMP = 8
+
+# status codes
+OK, ERR_ARG, ERR_OOM, ERR_NAN, ERR_TIMEOUT, ERR_CUDA, ERR_UNSUPPORTED = range(7)
+# NumericalMethods::Method (Source/NumericalMethods.H:10-19)
+MUSCL_HANCOCK, HLLC, IMEX, RCM, SLIC, FORCE, LAX_FRIEDRICHS = range(7)
+METHODS = {"muscl_hancock": MUSCL_HANCOCK, "hllc": HLLC, "imex": IMEX, "rcm": RCM, "slic": SLIC,
+           "force": FORCE, "lax_friedrichs": LAX_FRIEDRICHS}
+# Limiter (Source/Fluxes/Limiters.H:13)
+MINBEE, VAN_LEER, VAN_ALBADA, SUPERBEE = range(4)
+LIMITERS = {"minbee": MINBEE, "van_leer": VAN_LEER, "van_albada": VAN_ALBADA, "superbee": SUPERBEE}
+# boundary kinds
+BC_TRANSMISSIVE, BC_PERIODIC, BC_REFLECTIVE = range(3)
+BCS = {"transmissive": BC_TRANSMISSIVE, "periodic": BC_PERIODIC, "reflective": BC_REFLECTIVE}
+
+
+class BamrexError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__("bamrex status %d: %s" % (status, message))
+        self.status = status
+
+
+class Box(ctypes.Structure):
+    _fields_ = [("lo", ctypes.c_int * 3), ("hi", ctypes.c_int * 3)]
+
+    @classmethod
+    def make(cls, lo, hi):
+        b = cls()
+        for d in range(3):
+            b.lo[d] = int(lo[d]) if d < len(lo) else 0
+            b.hi[d] = int(hi[d]) if d < len(hi) else 0
+        return b
+
+
+class Array4(ctypes.Structure):
+    _fields_ = [
+        ("p", ctypes.c_void_p),
+        ("jstride", ctypes.c_longlong),
+        ("kstride", ctypes.c_longlong),
+        ("nstride", ctypes.c_longlong),
+        ("begin", ctypes.c_int * 3),
+        ("end", ctypes.c_int * 3),
+        ("ncomp", ctypes.c_int),
+    ]
+
+
+class CParm(ctypes.Structure):
+    _fields_ = [
+        ("adiabatic", ctypes.c_double),
+        ("eos_mu", ctypes.c_double),
+        ("Pr", ctypes.c_double),
+        ("beta", ctypes.c_double),
+        ("eta_prime", ctypes.c_double),
+        ("T_prime", ctypes.c_double),
+        ("S_eta", ctypes.c_double),
+        ("epsilon", ctypes.c_double),
+        ("Re", ctypes.c_double),
+        ("R_spec", ctypes.c_double),
+        ("cv", ctypes.c_double),
+        ("cp", ctypes.c_double),
+        ("adia", ctypes.c_double * 9),
+        ("Reinv", ctypes.c_double),
+        ("limiter", ctypes.c_int),
+        ("limiter_indices", ctypes.c_uint * MAX_NCOMP),
+        ("limit_on_primv", ctypes.c_ubyte * MAX_NCOMP),
+        ("need_primitive_for_limiting", ctypes.c_ubyte),
+    ]
+
+
+class LevelDesc(ctypes.Structure):
+    _fields_ = [
+        ("spacedim", ctypes.c_int),
+        ("domain", Box),
+        ("prob_lo", ctypes.c_double * 3),
+        ("prob_hi", ctypes.c_double * 3),
+        ("bc_lo", ctypes.c_int * 3),
+        ("bc_hi", ctypes.c_int * 3),
+        ("boxes", ctypes.POINTER(Box)),
+        ("nboxes", ctypes.c_int),
+        ("ngrow", ctypes.c_int),
+        ("method", ctypes.c_int),
+        ("cfl", ctypes.c_double),
+        ("parm", CParm),
+        ("x_segment", ctypes.c_int),
+        ("s_segment", ctypes.c_int),
+    ]
+
+
+# Every symbol include/bamrex_cuda.h declares, with (restype, argtypes).
+_vp, _i, _d, _ll = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_longlong
+_dp = ctypes.POINTER(ctypes.c_double)
+SIGNATURES = {
+    "bamrex_abi_version": (_i, []),
+    "bamrex_last_error": (ctypes.c_char_p, []),
+    "bamrex_status_string": (ctypes.c_char_p, [_i]),
+    "bamrex_parm_set_defaults": (_i, [ctypes.POINTER(CParm), _i]),
+    "bamrex_parm_init": (_i, [ctypes.POINTER(CParm)]),
+    "bamrex_compute_flux": (_i, [_i, _i, _i, _d, ctypes.POINTER(Box), Array4, Array4, _dp, _d,
+                                 ctypes.POINTER(CParm), _vp]),
+    "bamrex_compute_flux_LR": (_i, [_i, _i, _i, _d, ctypes.POINTER(Box), Array4, Array4, Array4, _dp, _d,
+                                    ctypes.POINTER(CParm), _vp]),
+    "bamrex_sweep_update": (_i, [_i, _i, ctypes.POINTER(Box), Array4, Array4, Array4, _dp, _d, _vp]),
+    "bamrex_conservative_update": (_i, [_i, ctypes.POINTER(Box), Array4, Array4, ctypes.POINTER(Array4), _d,
+                                        _dp, _vp]),
+    "bamrex_sweep_box": (_i, [_i, _i, _i, ctypes.POINTER(Box), Array4, Array4, Array4, _dp, _d,
+                              ctypes.POINTER(CParm), _vp]),
+    "bamrex_level_create": (_i, [ctypes.POINTER(_vp), ctypes.POINTER(LevelDesc), _vp]),
+    "bamrex_level_destroy": (_i, [_vp]),
+    "bamrex_level_last_error": (ctypes.c_char_p, [_vp]),
+    "bamrex_level_num_cells": (_ll, [_vp]),
+    "bamrex_level_fab": (_i, [_vp, _i, ctypes.POINTER(Array4)]),
+    "bamrex_level_copy_in": (_i, [_vp, _vp]),
+    "bamrex_level_copy_out": (_i, [_vp, _vp]),
+    "bamrex_level_sync": (_i, [_vp]),
+    "bamrex_level_fill_boundary": (_i, [_vp]),
+    "bamrex_level_advance": (_i, [_vp, _d, _d, _i, _i, _dp]),
+    "bamrex_level_est_time_step": (_i, [_vp, _dp]),
+    "bamrex_level_run": (_i, [_vp, _i, _d, _i, _dp, ctypes.POINTER(_i)]),
+    "bamrex_level_run_async": (_i, [_vp, _i, _d, _i, _d]),
+    "bamrex_level_run_wait": (_i, [_vp, _dp, ctypes.POINTER(_i)]),
+    "bamrex_level_set_timing": (_i, [_vp, _i]),
+    "bamrex_level_counters": (_i, [_vp, ctypes.POINTER(_ll), _dp, ctypes.POINTER(_ll)]),
+    "bamrex_level_reset_counters": (_i, [_vp]),
+}
+
+_LIB = None
+
+
+def lib() -> ctypes.CDLL:
+    """Load libbamrex_cuda.so (raises if it is absent: there is no fallback)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError("libbamrex_cuda.so is not built (%s); run `python -m bamrex_b200.build`" % LIB_PATH)
+    L = ctypes.CDLL(LIB_PATH)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _LIB = L
+    return L
+
+
+def check(rc: int, level_handle=None) -> None:
+    if rc == OK:
+        return
+    L = lib()
+    msg = L.bamrex_last_error().decode()
+    if level_handle is not None:
+        lm = L.bamrex_level_last_error(level_handle)
+        if lm:
+            msg = lm.decode() or msg
+    raise BamrexError(rc, msg or L.bamrex_status_string(rc).decode())

@@ -1,0 +1,1181 @@
+// C ABI of libbamrex_cuda.so and the level driver (the host side of
+// AmrLevelAdv::advance / advance_explicit / estTimeStep / computeNewDt for
+// the explicit methods).  No C++ exception crosses the ABI: every entry point
+// returns a BAMREX_* status and records a message for bamrex_last_error().
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <new>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "bamrex_cuda.h"
+#include "launch.h"
+
+using namespace bamrex;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg)
+{
+    g_last_error = msg;
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char* what)
+{
+    g_last_error = std::string(what) + ": " + cudaGetErrorString(e);
+    return BAMREX_ERR_CUDA;
+}
+
+#define BX_CK(call)                                         \
+    do {                                                    \
+        cudaError_t e_ = (call);                            \
+        if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
+    } while (0)
+
+#define BX_TRY(call)                  \
+    do {                              \
+        int rc_ = (call);             \
+        if (rc_ != BAMREX_OK) return rc_; \
+    } while (0)
+
+bool method_supported(int m)
+{
+    return m == BAMREX_MUSCL_HANCOCK || m == BAMREX_HLLC || m == BAMREX_SLIC || m == BAMREX_FORCE ||
+           m == BAMREX_LAX_FRIEDRICHS;
+}
+
+int method_halo(int m) { return (m == BAMREX_MUSCL_HANCOCK || m == BAMREX_SLIC) ? 2 : 1; }
+
+// Physical constants in the reference's own expressions (HLLC.H:269-280).
+int make_consts(const bamrex_parm* p, int D, Consts& k)
+{
+    if (!p) return fail(BAMREX_ERR_ARG, "parm is NULL");
+    const double g = p->adiabatic, eps = p->epsilon;
+    if (!(g > 1.0) || !std::isfinite(g)) return fail(BAMREX_ERR_ARG, "adiabatic index must be > 1");
+    if (!(eps > 0.0) || !std::isfinite(eps)) return fail(BAMREX_ERR_ARG, "epsilon must be > 0");
+    if (p->limiter < BAMREX_MINBEE || p->limiter > BAMREX_SUPERBEE) return fail(BAMREX_ERR_ARG, "unknown limiter");
+    std::memset(&k, 0, sizeof(k));
+    k.gamma = g;
+    k.eps = eps;
+    k.inv_eps = 1.0 / eps;
+    k.gm1 = g - 1;
+    k.half_gm1 = (g - 1) / 2;
+    k.z = (g - 1) / (2 * g);
+    k.neg_z = -k.z;
+    k.inv_z = 1 / k.z;
+    k.gp1_2g = (g + 1) / (2 * g);
+    k.gamma_inv_eps = g / eps;
+    const double kr = std::nearbyint(k.inv_z);
+    if (kr >= 2 && kr <= 16 && std::fabs(k.inv_z - kr) <= 1e-12 * kr) {
+        k.root_k = (int)kr;
+        k.root_dpos = k.inv_z - kr;
+        k.root_dneg = (double)(1.0L / (long double)kr - (long double)k.z);
+    }
+    k.limiter = p->limiter;
+    const int NC = D + 2;
+    bool uniform = true, need_prim = false;
+    for (int n = 0; n < NC; ++n) {
+        const unsigned idx = p->limiter_indices[n];
+        if (idx >= (unsigned)NC)
+            return fail(BAMREX_ERR_UNSUPPORTED, "limiting variable index outside the state / primitive vector");
+        k.lim_var[n] = (int)idx;
+        k.lim_prim[n] = p->limit_on_primv[n] ? 1 : 0;
+        need_prim = need_prim || k.lim_prim[n];
+        if (idx != p->limiter_indices[0] || k.lim_prim[n]) uniform = false;
+    }
+    k.uniform_var = uniform ? (int)p->limiter_indices[0] : -1;
+    k.need_prim = need_prim ? 1 : 0;
+    return BAMREX_OK;
+}
+
+FabDev to_fab(const bamrex_array4& a)
+{
+    FabDev f;
+    f.p = a.p;
+    f.js = a.jstride;
+    f.ks = a.kstride;
+    f.ns = a.nstride;
+    f.b0 = a.begin[0];
+    f.b1 = a.begin[1];
+    f.b2 = a.begin[2];
+    return f;
+}
+
+bool valid_box(const bamrex_box* b, int D)
+{
+    if (!b) return false;
+    for (int d = 0; d < 3; ++d) {
+        if (d < D && b->hi[d] < b->lo[d]) return false;
+        if (d >= D && (b->lo[d] != 0 || b->hi[d] != 0)) return false;
+    }
+    return true;
+}
+
+// a covers [lo - grow_lo, hi + grow_hi] (per direction) with >= NC components
+bool covers(const bamrex_array4& a, const int* lo, const int* hi, const int* glo, const int* ghi, int NC)
+{
+    if (!a.p || a.ncomp < NC) return false;
+    for (int d = 0; d < 3; ++d)
+        if (a.begin[d] > lo[d] - glo[d] || a.end[d] <= hi[d] + ghi[d]) return false;
+    return true;
+}
+
+std::pair<uintptr_t, uintptr_t> byte_range(const bamrex_array4& a, int NC)
+{
+    const long long span = (long long)(a.end[0] - a.begin[0] - 1) + (long long)(a.end[1] - a.begin[1] - 1) * a.jstride +
+                           (long long)(a.end[2] - a.begin[2] - 1) * a.kstride + (long long)(NC - 1) * a.nstride;
+    const uintptr_t b = (uintptr_t)a.p;
+    return { b, b + (uintptr_t)(span + 1) * sizeof(double) };
+}
+
+bool overlaps(const bamrex_array4& a, const bamrex_array4& b, int NC)
+{
+    auto ra = byte_range(a, NC), rb = byte_range(b, NC);
+    return ra.first < rb.second && rb.first < ra.second;
+}
+
+// Work items of one box in one sweep direction.
+void box_items(int dir, const int* lo, const int* hi, int seglen, long long& items, int& nseg, int& ngroup)
+{
+    const int n[3] = { hi[0] - lo[0] + 1, hi[1] - lo[1] + 1, hi[2] - lo[2] + 1 };
+    nseg = (n[dir] + seglen - 1) / seglen;
+    if (dir == 0) {
+        ngroup = 1;
+        items = (long long)n[1] * n[2] * nseg;
+    } else {
+        ngroup = (n[0] + 31) / 32;
+        const int other = (dir == 1) ? n[2] : n[1];
+        items = (long long)ngroup * other * nseg;
+    }
+}
+
+// Segment length: the longest that still gives every resident warp several
+// items (few partial waves); x segments are multiples of 32.
+int choose_seglen(int dir, const std::vector<bamrex_box>& boxes, long long resident_warps)
+{
+    static const int xs[] = { 2048, 1024, 512, 256, 128, 64, 32 };
+    static const int ss[] = { 256, 128, 96, 64, 48, 32, 24, 16 };
+    const int* cand = dir == 0 ? xs : ss;
+    const int ncand = dir == 0 ? 7 : 8;
+    const long long want = std::max(1LL, resident_warps) * 6;
+    for (int c = 0; c < ncand; ++c) {
+        long long tot = 0;
+        int nseg, ngroup;
+        long long it;
+        for (const auto& b : boxes) {
+            box_items(dir, b.lo, b.hi, cand[c], it, nseg, ngroup);
+            tot += it;
+        }
+        if (tot >= want) return cand[c];
+    }
+    return cand[ncand - 1];
+}
+
+size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+}  // namespace
+
+// ======================================================================
+// library identity, errors, Parm
+// ======================================================================
+extern "C" int bamrex_abi_version(void) { return BAMREX_ABI_VERSION; }
+
+extern "C" const char* bamrex_last_error(void) { return g_last_error.c_str(); }
+
+extern "C" const char* bamrex_status_string(int status)
+{
+    switch (status) {
+    case BAMREX_OK: return "ok";
+    case BAMREX_ERR_ARG: return "invalid argument";
+    case BAMREX_ERR_OOM: return "out of memory";
+    case BAMREX_ERR_NAN: return "non-finite wave speed or time step";
+    case BAMREX_ERR_TIMEOUT: return "device wait timed out";
+    case BAMREX_ERR_CUDA: return "CUDA runtime error";
+    case BAMREX_ERR_UNSUPPORTED: return "unsupported method or option";
+    default: return "unknown status";
+    }
+}
+
+extern "C" int bamrex_parm_set_defaults(bamrex_parm* parm, int spacedim)
+{
+    if (!parm) return fail(BAMREX_ERR_ARG, "parm is NULL");
+    if (spacedim < 1 || spacedim > 3) return fail(BAMREX_ERR_ARG, "spacedim must be 1, 2 or 3");
+    std::memset(parm, 0, sizeof(*parm));
+    parm->adiabatic = -1;
+    parm->eos_mu = 28.96;
+    parm->Pr = 0.71;
+    parm->beta = 1.5;
+    parm->eta_prime = 1.716e-5;
+    parm->T_prime = 273;
+    parm->S_eta = 111;
+    parm->epsilon = 1;
+    parm->Re = 1;
+    parm->limiter = BAMREX_VAN_LEER;
+    for (int i = 0; i < BAMREX_MAX_NCOMP; ++i) {
+        parm->limiter_indices[i] = (unsigned)(1 + spacedim);  // UInd::E
+        parm->limit_on_primv[i] = 0;
+    }
+    parm->need_primitive_for_limiting = 0;
+    return BAMREX_OK;
+}
+
+extern "C" int bamrex_parm_init(bamrex_parm* parm)
+{
+    if (!parm) return fail(BAMREX_ERR_ARG, "parm is NULL");
+    const double a = parm->adiabatic;
+    parm->adia[0] = a;
+    parm->adia[1] = a + 1;
+    parm->adia[2] = a - 1;
+    parm->adia[3] = 1.0 / (a + 1);
+    parm->adia[4] = 1.0 / (a - 1);
+    parm->adia[5] = (a + 1) / (2 * a);
+    parm->adia[6] = (a - 1) / (2 * a);
+    parm->adia[7] = a / (a + 1);
+    parm->adia[8] = a / (a - 1);
+    const double Ru = 8.3145;
+    parm->R_spec = Ru / (parm->eos_mu * 1e-3);
+    parm->cv = parm->R_spec * parm->adia[4];
+    parm->cp = a * parm->cv;
+    parm->Reinv = 1.0 / parm->Re;
+    unsigned char need = 0;
+    for (int n = 0; n < BAMREX_MAX_NCOMP; ++n) need = need || parm->limit_on_primv[n];
+    parm->need_primitive_for_limiting = need;
+    return BAMREX_OK;
+}
+
+// ======================================================================
+// per-box entry points (Fluxes.H / Update.H surface)
+// ======================================================================
+static int per_box_sweep(int method, int dir, int D, const bamrex_box* bx, const bamrex_array4* Uout,
+                         const bamrex_array4& Uin, const bamrex_array4* flux, const double dx[3], double dt,
+                         const bamrex_parm* parm, void* stream)
+{
+    if (D < 1 || D > 3) return fail(BAMREX_ERR_ARG, "spacedim must be 1, 2 or 3");
+    if (dir < 0 || dir >= D) return fail(BAMREX_ERR_ARG, "dir out of range");
+    if (!method_supported(method)) return fail(BAMREX_ERR_UNSUPPORTED, "method not on the explicit path");
+    if (!valid_box(bx, D)) return fail(BAMREX_ERR_ARG, "invalid box");
+    if (!dx || !(dx[dir] > 0)) return fail(BAMREX_ERR_ARG, "dx must be positive");
+    if (!(dt > 0) || !std::isfinite(dt)) return fail(BAMREX_ERR_ARG, "dt must be positive and finite");
+    Consts k;
+    BX_TRY(make_consts(parm, D, k));
+    const int NC = D + 2;
+    const int H = method_halo(method);
+    int g[3] = { 0, 0, 0 }, z3[3] = { 0, 0, 0 }, f1[3] = { 0, 0, 0 };
+    g[dir] = H;
+    f1[dir] = 1;
+    if (!covers(Uin, bx->lo, bx->hi, g, g, NC))
+        return fail(BAMREX_ERR_ARG, "consv must cover the box grown by the stencil halo in dir");
+    if (Uout) {
+        if (!covers(*Uout, bx->lo, bx->hi, z3, z3, NC)) return fail(BAMREX_ERR_ARG, "Uout must cover the box");
+        if (overlaps(*Uout, Uin, NC)) return fail(BAMREX_ERR_ARG, "Uout and Uin must not overlap");
+    }
+    if (flux && flux->p) {
+        if (!covers(*flux, bx->lo, bx->hi, z3, f1, NC))
+            return fail(BAMREX_ERR_ARG, "flux must cover surroundingNodes(bx, dir)");
+        if (overlaps(*flux, Uin, NC)) return fail(BAMREX_ERR_ARG, "flux and consv must not overlap");
+    }
+    SweepArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.boxes = nullptr;
+    a.nboxes = 1;
+    SweepBox& B = a.one;
+    for (int d = 0; d < 3; ++d) {
+        B.lo[d] = bx->lo[d];
+        B.hi[d] = bx->hi[d];
+    }
+    B.in = to_fab(Uin);
+    if (Uout) B.out = to_fab(*Uout);
+    if (flux && flux->p) B.flux = to_fab(*flux);
+    a.seglen = dir == 0 ? 512 : 64;
+    long long items;
+    box_items(dir, B.lo, B.hi, a.seglen, items, B.nseg, B.ngroup);
+    B.item_begin = 0;
+    a.total_items = items;
+    a.halo = H;
+    a.dt_host = dt;
+    a.scal = nullptr;
+    a.dx = dx[dir];
+    a.k = k;
+    a.ws_max = nullptr;
+    a.do_update = Uout ? 1 : 0;
+    BX_CK(launch_sweep(D, dir, method, a, (cudaStream_t)stream));
+    return BAMREX_OK;
+}
+
+extern "C" int bamrex_compute_flux(int method, int dir, int spacedim, double time, const bamrex_box* bx,
+                                   bamrex_array4 flux, bamrex_array4 consv, const double dx[3], double dt,
+                                   const bamrex_parm* parm, void* stream)
+{
+    (void)time;
+    if (!flux.p) return fail(BAMREX_ERR_ARG, "flux.p is NULL");
+    return per_box_sweep(method, dir, spacedim, bx, nullptr, consv, &flux, dx, dt, parm, stream);
+}
+
+extern "C" int bamrex_sweep_box(int method, int dir, int spacedim, const bamrex_box* bx, bamrex_array4 Uout,
+                                bamrex_array4 Uin, bamrex_array4 flux, const double dx[3], double dt,
+                                const bamrex_parm* parm, void* stream)
+{
+    if (!Uout.p) return fail(BAMREX_ERR_ARG, "Uout.p is NULL");
+    return per_box_sweep(method, dir, spacedim, bx, &Uout, Uin, flux.p ? &flux : nullptr, dx, dt, parm, stream);
+}
+
+extern "C" int bamrex_compute_flux_LR(int kind, int dir, int spacedim, double time, const bamrex_box* bx,
+                                      bamrex_array4 flux, bamrex_array4 consv_L, bamrex_array4 consv_R,
+                                      const double dx[3], double dt, const bamrex_parm* parm, void* stream)
+{
+    (void)time;
+    const int D = spacedim;
+    if (D < 1 || D > 3) return fail(BAMREX_ERR_ARG, "spacedim must be 1, 2 or 3");
+    if (dir < 0 || dir >= D) return fail(BAMREX_ERR_ARG, "dir out of range");
+    if (kind != BAMREX_HLLC && kind != BAMREX_FORCE) return fail(BAMREX_ERR_UNSUPPORTED, "kind must be HLLC or FORCE");
+    if (!valid_box(bx, D)) return fail(BAMREX_ERR_ARG, "invalid box");
+    if (!dx || !(dx[dir] > 0)) return fail(BAMREX_ERR_ARG, "dx must be positive");
+    if (kind == BAMREX_FORCE && (!(dt > 0) || !std::isfinite(dt))) return fail(BAMREX_ERR_ARG, "dt must be positive");
+    Consts k;
+    BX_TRY(make_consts(parm, D, k));
+    const int NC = D + 2;
+    int z3[3] = { 0, 0, 0 }, f1[3] = { 0, 0, 0 };
+    f1[dir] = 1;
+    if (!flux.p || !covers(flux, bx->lo, bx->hi, z3, f1, NC))
+        return fail(BAMREX_ERR_ARG, "flux must cover surroundingNodes(bx, dir)");
+    if (!covers(consv_L, bx->lo, bx->hi, f1, z3, NC)) return fail(BAMREX_ERR_ARG, "consv_L must cover bx grown low by 1");
+    if (!covers(consv_R, bx->lo, bx->hi, z3, f1, NC)) return fail(BAMREX_ERR_ARG, "consv_R must cover bx grown high by 1");
+    BX_CK(launch_flux_LR(D, dir, kind, bx->lo, bx->hi, to_fab(flux), to_fab(consv_L),
+                         to_fab(consv_R), k, dx[dir], kind == BAMREX_FORCE ? dt : 1.0, (cudaStream_t)stream));
+    return BAMREX_OK;
+}
+
+extern "C" int bamrex_sweep_update(int dir, int spacedim, const bamrex_box* bx, bamrex_array4 Uout, bamrex_array4 Uin,
+                                   bamrex_array4 flux, const double dx[3], double dt, void* stream)
+{
+    const int D = spacedim;
+    if (D < 1 || D > 3) return fail(BAMREX_ERR_ARG, "spacedim must be 1, 2 or 3");
+    if (dir < 0 || dir >= D) return fail(BAMREX_ERR_ARG, "dir out of range");
+    if (!valid_box(bx, D)) return fail(BAMREX_ERR_ARG, "invalid box");
+    if (!dx || !(dx[dir] > 0)) return fail(BAMREX_ERR_ARG, "dx must be positive");
+    const int NC = D + 2;
+    int z3[3] = { 0, 0, 0 }, f1[3] = { 0, 0, 0 };
+    f1[dir] = 1;
+    if (!covers(Uout, bx->lo, bx->hi, z3, z3, NC) || !covers(Uin, bx->lo, bx->hi, z3, z3, NC))
+        return fail(BAMREX_ERR_ARG, "Uin/Uout must cover the box");
+    if (!covers(flux, bx->lo, bx->hi, z3, f1, NC)) return fail(BAMREX_ERR_ARG, "flux must cover surroundingNodes(bx, dir)");
+    UpdateArgs u;
+    std::memset(&u, 0, sizeof(u));
+    for (int d = 0; d < 3; ++d) {
+        u.lo[d] = bx->lo[d];
+        u.hi[d] = bx->hi[d];
+    }
+    u.out = to_fab(Uout);
+    u.in = to_fab(Uin);
+    u.flux[0] = to_fab(flux);
+    u.dtdx[0] = dt / dx[dir];
+    BX_CK(launch_sweep_update(D, dir, u, (cudaStream_t)stream));
+    return BAMREX_OK;
+}
+
+extern "C" int bamrex_conservative_update(int spacedim, const bamrex_box* bx, bamrex_array4 out, bamrex_array4 in,
+                                          const bamrex_array4* fluxes, double dt, const double idx[3], void* stream)
+{
+    const int D = spacedim;
+    if (D < 1 || D > 3) return fail(BAMREX_ERR_ARG, "spacedim must be 1, 2 or 3");
+    if (!valid_box(bx, D) || !fluxes || !idx) return fail(BAMREX_ERR_ARG, "invalid argument");
+    const int NC = D + 2;
+    int z3[3] = { 0, 0, 0 };
+    if (!covers(out, bx->lo, bx->hi, z3, z3, NC) || !covers(in, bx->lo, bx->hi, z3, z3, NC))
+        return fail(BAMREX_ERR_ARG, "in/out must cover the box");
+    UpdateArgs u;
+    std::memset(&u, 0, sizeof(u));
+    for (int d = 0; d < 3; ++d) {
+        u.lo[d] = bx->lo[d];
+        u.hi[d] = bx->hi[d];
+    }
+    u.out = to_fab(out);
+    u.in = to_fab(in);
+    for (int d = 0; d < D; ++d) {
+        int f1[3] = { 0, 0, 0 };
+        f1[d] = 1;
+        if (!covers(fluxes[d], bx->lo, bx->hi, z3, f1, NC)) return fail(BAMREX_ERR_ARG, "flux must cover surroundingNodes");
+        u.flux[d] = to_fab(fluxes[d]);
+        u.dtdx[d] = dt * idx[d];
+    }
+    BX_CK(launch_conservative_update(D, u, (cudaStream_t)stream));
+    return BAMREX_OK;
+}
+
+// ======================================================================
+// level
+// ======================================================================
+struct bamrex_level {
+    int D = 0, NC = 0, ngrow = 0, method = 0;
+    double cfl = 0.9;
+    bamrex_parm parm;
+    Consts k;
+    bamrex_box domain;
+    double dx[3] = { 1, 1, 1 };
+    int bc_lo[3] = { 0, 0, 0 }, bc_hi[3] = { 0, 0, 0 };
+    std::vector<bamrex_box> boxes;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int device = 0;
+
+    // device memory (one arena)
+    char* arena = nullptr;
+    double* state[2] = { nullptr, nullptr };
+    std::vector<FabDev> fab[2];
+    FabDev* d_fab[2] = { nullptr, nullptr };
+    SweepBox* d_sweep[3][2] = {};
+    long long items[3] = { 0, 0, 0 };
+    int seglen[3] = { 0, 0, 0 };
+    GhostOp* d_ghost[3] = { nullptr, nullptr, nullptr };
+    int nghost[3] = { 0, 0, 0 };
+    long long ghost_cells[3] = { 0, 0, 0 };
+    PackBox* d_pack = nullptr;
+    long long ncells = 0;
+    double* staging = nullptr;
+    StepScalars* d_scal = nullptr;
+    StepScalars* h_scal = nullptr;  // pinned
+    int cur = 0;
+    bool ws_valid = false;
+
+    // accounting
+    long long launches = 0;
+    bool timing = false;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> events;
+    size_t ev_used = 0;
+    double sweep_ms = 0.0;
+    long long sweep_launches = 0;
+
+    cudaGraphExec_t graph[2] = { nullptr, nullptr };
+    bool run_pending = false;
+    int run_start_parity = 0;
+    std::string err;
+
+    int set_err(int code) {
+        err = g_last_error;
+        return code;
+    }
+};
+
+namespace {
+
+// Uniform bucket grid over the domain for box-intersection queries.
+struct BoxIndex {
+    int D;
+    int lo[3], bs[3], nb[3];
+    std::vector<std::vector<int>> buckets;
+    const std::vector<bamrex_box>* boxes;
+
+    void build(const bamrex_box& dom, const std::vector<bamrex_box>& bxs, int D_)
+    {
+        D = D_;
+        boxes = &bxs;
+        for (int d = 0; d < 3; ++d) {
+            lo[d] = dom.lo[d];
+            int mx = 1;
+            for (const auto& b : bxs) mx = std::max(mx, b.hi[d] - b.lo[d] + 1);
+            bs[d] = mx;
+            nb[d] = (dom.hi[d] - dom.lo[d] + 1 + mx - 1) / mx;
+            if (nb[d] < 1) nb[d] = 1;
+        }
+        buckets.assign((size_t)nb[0] * nb[1] * nb[2], {});
+        for (int i = 0; i < (int)bxs.size(); ++i) {
+            int a[3], c[3];
+            for (int d = 0; d < 3; ++d) {
+                a[d] = std::max(0, (bxs[i].lo[d] - lo[d]) / bs[d]);
+                c[d] = std::min(nb[d] - 1, (bxs[i].hi[d] - lo[d]) / bs[d]);
+            }
+            for (int z = a[2]; z <= c[2]; ++z)
+                for (int y = a[1]; y <= c[1]; ++y)
+                    for (int x = a[0]; x <= c[0]; ++x) buckets[((size_t)z * nb[1] + y) * nb[0] + x].push_back(i);
+        }
+    }
+
+    // boxes intersecting region r
+    void query(const int* rlo, const int* rhi, std::vector<int>& out) const
+    {
+        out.clear();
+        int a[3], c[3];
+        for (int d = 0; d < 3; ++d) {
+            a[d] = std::max(0, (rlo[d] - lo[d]) / bs[d]);
+            c[d] = std::min(nb[d] - 1, (rhi[d] - lo[d]) / bs[d]);
+            if (rhi[d] < lo[d]) return;
+            if (a[d] > c[d]) return;
+        }
+        for (int z = a[2]; z <= c[2]; ++z)
+            for (int y = a[1]; y <= c[1]; ++y)
+                for (int x = a[0]; x <= c[0]; ++x)
+                    for (int i : buckets[((size_t)z * nb[1] + y) * nb[0] + x]) {
+                        const auto& b = (*boxes)[i];
+                        bool hit = true;
+                        for (int d = 0; d < 3; ++d) hit = hit && b.lo[d] <= rhi[d] && rlo[d] <= b.hi[d];
+                        if (hit && std::find(out.begin(), out.end(), i) == out.end()) out.push_back(i);
+                    }
+    }
+};
+
+// Ghost-fill ops of direction d for every box: the two ghost slabs of
+// width ngrow across the box's valid extent in the other directions.
+void build_ghost_ops(const bamrex_level* L, int d, const BoxIndex& idx, std::vector<GhostOp>& ops)
+{
+    const int g = L->ngrow;
+    const int dlo = L->domain.lo[d], dhi = L->domain.hi[d], len = dhi - dlo + 1;
+    std::vector<int> hits;
+    for (int b = 0; b < (int)L->boxes.size(); ++b) {
+        const bamrex_box& B = L->boxes[b];
+        for (int side = 0; side < 2; ++side) {
+            int rlo[3], rhi[3];
+            for (int q = 0; q < 3; ++q) {
+                rlo[q] = B.lo[q];
+                rhi[q] = B.hi[q];
+            }
+            if (side == 0) {
+                rlo[d] = B.lo[d] - g;
+                rhi[d] = B.lo[d] - 1;
+            } else {
+                rlo[d] = B.hi[d] + 1;
+                rhi[d] = B.hi[d] + g;
+            }
+            // split the slab into the part inside the domain and the part outside
+            int in_lo = std::max(rlo[d], dlo), in_hi = std::min(rhi[d], dhi);
+            if (in_lo <= in_hi) {
+                int qlo[3] = { rlo[0], rlo[1], rlo[2] }, qhi[3] = { rhi[0], rhi[1], rhi[2] };
+                qlo[d] = in_lo;
+                qhi[d] = in_hi;
+                idx.query(qlo, qhi, hits);
+                for (int s : hits) {
+                    if (s == b) continue;
+                    GhostOp op;
+                    std::memset(&op, 0, sizeof(op));
+                    op.dst = b;
+                    op.src = s;
+                    for (int q = 0; q < 3; ++q) {
+                        op.lo[q] = std::max(qlo[q], L->boxes[s].lo[q]);
+                        op.hi[q] = std::min(qhi[q], L->boxes[s].hi[q]);
+                        op.mul[q] = 1;
+                        op.off[q] = 0;
+                    }
+                    ops.push_back(op);
+                }
+            }
+            int out_lo = rlo[d], out_hi = rhi[d];
+            if (side == 0) out_hi = std::min(rhi[d], dlo - 1);
+            else out_lo = std::max(rlo[d], dhi + 1);
+            if (out_lo > out_hi) continue;
+            const int bc = side == 0 ? L->bc_lo[d] : L->bc_hi[d];
+            // ghost region outside the domain: dst cells [out_lo, out_hi] in d
+            int glo[3] = { rlo[0], rlo[1], rlo[2] }, ghi[3] = { rhi[0], rhi[1], rhi[2] };
+            glo[d] = out_lo;
+            ghi[d] = out_hi;
+            // the source region in d and the map src = off + mul * dst
+            int slo[3] = { glo[0], glo[1], glo[2] }, shi[3] = { ghi[0], ghi[1], ghi[2] };
+            int off = 0, mul = 1, neg = 0;
+            if (bc == BAMREX_BC_PERIODIC) {
+                off = side == 0 ? len : -len;
+                mul = 1;
+                slo[d] = glo[d] + off;
+                shi[d] = ghi[d] + off;
+            } else if (bc == BAMREX_BC_REFLECTIVE) {
+                off = side == 0 ? 2 * dlo - 1 : 2 * dhi + 1;
+                mul = -1;
+                slo[d] = off - ghi[d];
+                shi[d] = off - glo[d];
+                neg = 1 << (1 + d);
+            } else {  // transmissive: first-order extrapolation
+                off = side == 0 ? dlo : dhi;
+                mul = 0;
+                slo[d] = off;
+                shi[d] = off;
+            }
+            idx.query(slo, shi, hits);
+            for (int s : hits) {
+                const bamrex_box& S = L->boxes[s];
+                GhostOp op;
+                std::memset(&op, 0, sizeof(op));
+                op.dst = b;
+                op.src = s;
+                op.negmask = neg;
+                bool empty = false;
+                for (int q = 0; q < 3; ++q) {
+                    op.mul[q] = 1;
+                    op.off[q] = 0;
+                    if (q != d) {
+                        op.lo[q] = std::max(glo[q], S.lo[q]);
+                        op.hi[q] = std::min(ghi[q], S.hi[q]);
+                    }
+                    if (q != d && op.lo[q] > op.hi[q]) empty = true;
+                }
+                // dst range in d whose source lies in S
+                int ilo = std::max(slo[d], S.lo[d]), ihi = std::min(shi[d], S.hi[d]);
+                if (ilo > ihi) empty = true;
+                if (empty) continue;
+                op.mul[d] = mul;
+                op.off[d] = off;
+                if (mul == 1) {
+                    op.lo[d] = ilo - off;
+                    op.hi[d] = ihi - off;
+                } else if (mul == -1) {
+                    op.lo[d] = off - ihi;
+                    op.hi[d] = off - ilo;
+                } else {
+                    op.lo[d] = glo[d];
+                    op.hi[d] = ghi[d];
+                }
+                ops.push_back(op);
+            }
+        }
+    }
+    long long acc = 0;
+    for (auto& op : ops) {
+        op.cell_begin = acc;
+        acc += (long long)(op.hi[0] - op.lo[0] + 1) * (op.hi[1] - op.lo[1] + 1) * (op.hi[2] - op.lo[2] + 1);
+    }
+}
+
+long long ops_cells(const std::vector<GhostOp>& ops)
+{
+    if (ops.empty()) return 0;
+    const GhostOp& o = ops.back();
+    return o.cell_begin + (long long)(o.hi[0] - o.lo[0] + 1) * (o.hi[1] - o.lo[1] + 1) * (o.hi[2] - o.lo[2] + 1);
+}
+
+int level_launch(bamrex_level* L, cudaError_t e, const char* what)
+{
+    if (e != cudaSuccess) return L->set_err(cuda_fail(e, what));
+    L->launches++;
+    return BAMREX_OK;
+}
+
+int level_fill(bamrex_level* L, int d, int parity, const StepScalars* scal)
+{
+    if (L->nghost[d] == 0) return BAMREX_OK;
+    return level_launch(L, launch_ghost_fill(L->NC, L->d_ghost[d], L->nghost[d], L->ghost_cells[d], L->d_fab[parity], scal,
+                                             L->stream),
+                        "ghost fill");
+}
+
+int level_sweep(bamrex_level* L, int d, int parity, double dt_host, const StepScalars* scal, bool reduce_ws,
+                bool allow_timing)
+{
+    SweepArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.boxes = L->d_sweep[d][parity];
+    a.nboxes = (int)L->boxes.size();
+    a.total_items = L->items[d];
+    a.seglen = L->seglen[d];
+    a.halo = method_halo(L->method);
+    a.dt_host = dt_host;
+    a.scal = scal;
+    a.dx = L->dx[d];
+    a.k = L->k;
+    a.ws_max = reduce_ws ? &L->d_scal->ws_bits : nullptr;
+    a.do_update = 1;
+    const bool t = allow_timing && L->timing && L->ev_used < L->events.size();
+    if (t) cudaEventRecord(L->events[L->ev_used].first, L->stream);
+    const int rc = level_launch(L, launch_sweep(L->D, d, L->method, a, L->stream), "sweep");
+    if (rc != BAMREX_OK) return rc;
+    if (t) {
+        cudaEventRecord(L->events[L->ev_used].second, L->stream);
+        L->ev_used++;
+    }
+    return BAMREX_OK;
+}
+
+// One split step starting from buffer `parity`; the result lands in
+// parity ^ (D & 1).  dt from the host (scal == nullptr) or from the device.
+int level_step(bamrex_level* L, int parity, double dt_host, StepScalars* scal, bool allow_timing)
+{
+    BX_TRY(level_fill(L, 0, parity, scal));
+    int p = parity;
+    for (int d = 0; d < L->D; ++d) {
+        BX_TRY(level_sweep(L, d, p, dt_host, scal, d == L->D - 1, allow_timing));
+        p ^= 1;
+        if (d + 1 < L->D) BX_TRY(level_fill(L, d + 1, p, scal));
+    }
+    if (scal)
+        BX_TRY(level_launch(L, launch_step_dt(scal, L->D, L->dx[0], L->dx[1], L->dx[2], L->cfl, 1, L->stream), "step dt"));
+    return BAMREX_OK;
+}
+
+}  // namespace
+
+extern "C" int bamrex_level_create(bamrex_level** out, const bamrex_level_desc* desc, void* stream)
+{
+    if (!out || !desc) return fail(BAMREX_ERR_ARG, "NULL argument");
+    *out = nullptr;
+    const int D = desc->spacedim;
+    if (D < 1 || D > 3) return fail(BAMREX_ERR_ARG, "spacedim must be 1, 2 or 3");
+    if (!method_supported(desc->method)) return fail(BAMREX_ERR_UNSUPPORTED, "method not on the explicit path");
+    if (desc->ngrow < 2 || desc->ngrow > 16) return fail(BAMREX_ERR_ARG, "ngrow must be in [2, 16]");
+    if (desc->nboxes < 1 || !desc->boxes) return fail(BAMREX_ERR_ARG, "no boxes");
+    if (!valid_box(&desc->domain, D)) return fail(BAMREX_ERR_ARG, "invalid domain");
+    if (!(desc->cfl > 0)) return fail(BAMREX_ERR_ARG, "cfl must be positive");
+    for (int d = 0; d < D; ++d) {
+        if (!(desc->prob_hi[d] > desc->prob_lo[d])) return fail(BAMREX_ERR_ARG, "prob_hi must exceed prob_lo");
+        for (int s = 0; s < 2; ++s) {
+            const int bc = s ? desc->bc_hi[d] : desc->bc_lo[d];
+            if (bc < BAMREX_BC_TRANSMISSIVE || bc > BAMREX_BC_REFLECTIVE) return fail(BAMREX_ERR_ARG, "unknown boundary kind");
+        }
+        if ((desc->bc_lo[d] == BAMREX_BC_PERIODIC) != (desc->bc_hi[d] == BAMREX_BC_PERIODIC))
+            return fail(BAMREX_ERR_ARG, "periodic boundaries must be set on both sides");
+    }
+    long long covered = 0;
+    for (int b = 0; b < desc->nboxes; ++b) {
+        const bamrex_box& B = desc->boxes[b];
+        if (!valid_box(&B, D)) return fail(BAMREX_ERR_ARG, "invalid box in box array");
+        long long n = 1;
+        for (int d = 0; d < 3; ++d) {
+            if (B.lo[d] < desc->domain.lo[d] || B.hi[d] > desc->domain.hi[d]) return fail(BAMREX_ERR_ARG, "box outside the domain");
+            n *= (long long)(B.hi[d] - B.lo[d] + 1);
+        }
+        covered += n;
+    }
+
+    bamrex_level* L = new (std::nothrow) bamrex_level();
+    if (!L) return fail(BAMREX_ERR_OOM, "host allocation failed");
+    L->D = D;
+    L->NC = D + 2;
+    L->ngrow = desc->ngrow;
+    L->method = desc->method;
+    L->cfl = desc->cfl;
+    L->parm = desc->parm;
+    L->domain = desc->domain;
+    for (int d = 0; d < 3; ++d) {
+        L->bc_lo[d] = desc->bc_lo[d];
+        L->bc_hi[d] = desc->bc_hi[d];
+        L->dx[d] = d < D ? (desc->prob_hi[d] - desc->prob_lo[d]) / (double)(desc->domain.hi[d] - desc->domain.lo[d] + 1) : 1.0;
+    }
+    L->boxes.assign(desc->boxes, desc->boxes + desc->nboxes);
+    L->ncells = covered;
+    int rc = make_consts(&L->parm, D, L->k);
+    if (rc != BAMREX_OK) {
+        delete L;
+        return rc;
+    }
+    cudaGetDevice(&L->device);
+    if (stream) {
+        L->stream = (cudaStream_t)stream;
+    } else {
+        cudaError_t e = cudaStreamCreateWithFlags(&L->stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) {
+            delete L;
+            return cuda_fail(e, "cudaStreamCreateWithFlags");
+        }
+        L->own_stream = true;
+    }
+
+    // ---- layout of the state fabs: rows padded to 32 doubles, first valid
+    // cell of each row 256-byte aligned.
+    const int nb = desc->nboxes;
+    const int g = L->ngrow;
+    const int front = (32 - g % 32) % 32;
+    std::vector<long long> fab_off(nb);
+    long long per_buf = 0;
+    for (int b = 0; b < nb; ++b) {
+        const bamrex_box& B = L->boxes[b];
+        const int nxg = B.hi[0] - B.lo[0] + 1 + 2 * g;
+        const int nyg = D > 1 ? B.hi[1] - B.lo[1] + 1 + 2 * g : 1;
+        const int nzg = D > 2 ? B.hi[2] - B.lo[2] + 1 + 2 * g : 1;
+        FabDev f;
+        f.js = (long long)align_up((size_t)(front + nxg), 32);
+        f.ks = f.js * nyg;
+        f.ns = f.ks * nzg;
+        f.b0 = B.lo[0] - g;
+        f.b1 = D > 1 ? B.lo[1] - g : B.lo[1];
+        f.b2 = D > 2 ? B.lo[2] - g : B.lo[2];
+        f.p = nullptr;
+        fab_off[b] = per_buf + front;
+        per_buf += (long long)align_up((size_t)(f.ns * L->NC), 32);
+        L->fab[0].push_back(f);
+        L->fab[1].push_back(f);
+    }
+
+    // ---- items and segment lengths
+    std::vector<SweepBox> sweep_host[3];
+    for (int d = 0; d < D; ++d) {
+        L->seglen[d] = d == 0 ? desc->x_segment : desc->s_segment;
+        if (L->seglen[d] <= 0)
+            L->seglen[d] = choose_seglen(d, L->boxes, sweep_resident_warps(D, d, L->method));
+        if (d == 0) L->seglen[d] = (int)align_up((size_t)L->seglen[d], 32);
+        long long acc = 0;
+        for (int b = 0; b < nb; ++b) {
+            SweepBox sb;
+            std::memset(&sb, 0, sizeof(sb));
+            for (int q = 0; q < 3; ++q) {
+                sb.lo[q] = L->boxes[b].lo[q];
+                sb.hi[q] = L->boxes[b].hi[q];
+            }
+            long long it;
+            box_items(d, sb.lo, sb.hi, L->seglen[d], it, sb.nseg, sb.ngroup);
+            sb.item_begin = acc;
+            acc += it;
+            sweep_host[d].push_back(sb);
+        }
+        L->items[d] = acc;
+    }
+
+    // ---- ghost ops
+    BoxIndex bidx;
+    bidx.build(L->domain, L->boxes, D);
+    std::vector<GhostOp> ghost_host[3];
+    for (int d = 0; d < D; ++d) {
+        build_ghost_ops(L, d, bidx, ghost_host[d]);
+        L->nghost[d] = (int)ghost_host[d].size();
+        L->ghost_cells[d] = ops_cells(ghost_host[d]);
+    }
+
+    // ---- pack boxes
+    std::vector<PackBox> pack_host(nb);
+    {
+        long long acc = 0;
+        for (int b = 0; b < nb; ++b) {
+            for (int q = 0; q < 3; ++q) {
+                pack_host[b].lo[q] = L->boxes[b].lo[q];
+                pack_host[b].hi[q] = L->boxes[b].hi[q];
+            }
+            pack_host[b].cell_begin = acc;
+            acc += (long long)(L->boxes[b].hi[0] - L->boxes[b].lo[0] + 1) * (L->boxes[b].hi[1] - L->boxes[b].lo[1] + 1) *
+                   (L->boxes[b].hi[2] - L->boxes[b].lo[2] + 1);
+        }
+    }
+
+    // ---- one arena
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        const size_t o = off;
+        off = align_up(off + bytes, 256);
+        return o;
+    };
+    const size_t o_state0 = take((size_t)per_buf * 8);
+    const size_t o_state1 = take((size_t)per_buf * 8);
+    const size_t o_fab0 = take(sizeof(FabDev) * nb);
+    const size_t o_fab1 = take(sizeof(FabDev) * nb);
+    size_t o_sweep[3][2] = {};
+    for (int d = 0; d < D; ++d)
+        for (int p = 0; p < 2; ++p) o_sweep[d][p] = take(sizeof(SweepBox) * nb);
+    size_t o_ghost[3] = {};
+    for (int d = 0; d < D; ++d) o_ghost[d] = take(sizeof(GhostOp) * std::max<size_t>(1, ghost_host[d].size()));
+    const size_t o_pack = take(sizeof(PackBox) * nb);
+    const size_t o_stage = take((size_t)L->ncells * L->NC * 8);
+    const size_t o_scal = take(sizeof(StepScalars));
+    cudaError_t e = cudaMalloc((void**)&L->arena, off);
+    if (e != cudaSuccess) {
+        if (L->own_stream) cudaStreamDestroy(L->stream);
+        delete L;
+        return fail(BAMREX_ERR_OOM, std::string("cudaMalloc of the level arena failed: ") + cudaGetErrorString(e));
+    }
+    e = cudaMallocHost((void**)&L->h_scal, sizeof(StepScalars));
+    if (e != cudaSuccess) {
+        cudaFree(L->arena);
+        if (L->own_stream) cudaStreamDestroy(L->stream);
+        delete L;
+        return fail(BAMREX_ERR_OOM, "cudaMallocHost failed");
+    }
+    L->state[0] = (double*)(L->arena + o_state0);
+    L->state[1] = (double*)(L->arena + o_state1);
+    for (int p = 0; p < 2; ++p)
+        for (int b = 0; b < nb; ++b) L->fab[p][b].p = L->state[p] + fab_off[b];
+    L->d_fab[0] = (FabDev*)(L->arena + o_fab0);
+    L->d_fab[1] = (FabDev*)(L->arena + o_fab1);
+    for (int d = 0; d < D; ++d) {
+        for (int p = 0; p < 2; ++p) L->d_sweep[d][p] = (SweepBox*)(L->arena + o_sweep[d][p]);
+        L->d_ghost[d] = (GhostOp*)(L->arena + o_ghost[d]);
+    }
+    L->d_pack = (PackBox*)(L->arena + o_pack);
+    L->staging = (double*)(L->arena + o_stage);
+    L->d_scal = (StepScalars*)(L->arena + o_scal);
+
+    // upload tables (synchronous: setup only)
+    auto up = [&](void* dst, const void* src, size_t bytes) -> cudaError_t {
+        if (!bytes) return cudaSuccess;
+        return cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice);
+    };
+    cudaError_t ue = cudaSuccess;
+    for (int p = 0; p < 2 && ue == cudaSuccess; ++p) ue = up(L->d_fab[p], L->fab[p].data(), sizeof(FabDev) * nb);
+    for (int d = 0; d < D && ue == cudaSuccess; ++d) {
+        for (int p = 0; p < 2 && ue == cudaSuccess; ++p) {
+            std::vector<SweepBox> t = sweep_host[d];
+            for (int b = 0; b < nb; ++b) {
+                t[b].in = L->fab[p][b];
+                t[b].out = L->fab[p ^ 1][b];
+                t[b].flux.p = nullptr;
+            }
+            ue = up(L->d_sweep[d][p], t.data(), sizeof(SweepBox) * nb);
+        }
+        if (ue == cudaSuccess) ue = up(L->d_ghost[d], ghost_host[d].data(), sizeof(GhostOp) * ghost_host[d].size());
+    }
+    if (ue == cudaSuccess) ue = up(L->d_pack, pack_host.data(), sizeof(PackBox) * nb);
+    if (ue == cudaSuccess) ue = cudaMemset(L->arena + o_state0, 0, (size_t)per_buf * 8 * 2);
+    if (ue == cudaSuccess) ue = cudaMemset(L->d_scal, 0, sizeof(StepScalars));
+    if (ue != cudaSuccess) {
+        const int r = cuda_fail(ue, "level table upload");
+        bamrex_level_destroy(L);
+        return r;
+    }
+    *out = L;
+    return BAMREX_OK;
+}
+
+extern "C" int bamrex_level_destroy(bamrex_level* L)
+{
+    if (!L) return BAMREX_OK;
+    if (L->stream) cudaStreamSynchronize(L->stream);
+    for (int p = 0; p < 2; ++p)
+        if (L->graph[p]) cudaGraphExecDestroy(L->graph[p]);
+    for (auto& ev : L->events) {
+        cudaEventDestroy(ev.first);
+        cudaEventDestroy(ev.second);
+    }
+    if (L->arena) cudaFree(L->arena);
+    if (L->h_scal) cudaFreeHost(L->h_scal);
+    if (L->own_stream && L->stream) cudaStreamDestroy(L->stream);
+    delete L;
+    return BAMREX_OK;
+}
+
+extern "C" const char* bamrex_level_last_error(const bamrex_level* L) { return L ? L->err.c_str() : ""; }
+
+extern "C" long long bamrex_level_num_cells(const bamrex_level* L) { return L ? L->ncells : 0; }
+
+extern "C" int bamrex_level_fab(const bamrex_level* L, int box, bamrex_array4* out)
+{
+    if (!L || !out || box < 0 || box >= (int)L->boxes.size()) return fail(BAMREX_ERR_ARG, "bad level/box");
+    const FabDev& f = L->fab[L->cur][box];
+    const bamrex_box& B = L->boxes[box];
+    out->p = f.p;
+    out->jstride = f.js;
+    out->kstride = f.ks;
+    out->nstride = f.ns;
+    out->begin[0] = f.b0;
+    out->begin[1] = f.b1;
+    out->begin[2] = f.b2;
+    const int g = L->ngrow;
+    out->end[0] = B.hi[0] + g + 1;
+    out->end[1] = L->D > 1 ? B.hi[1] + g + 1 : B.hi[1] + 1;
+    out->end[2] = L->D > 2 ? B.hi[2] + g + 1 : B.hi[2] + 1;
+    out->ncomp = L->NC;
+    return BAMREX_OK;
+}
+
+extern "C" int bamrex_level_copy_in(bamrex_level* L, const double* src)
+{
+    if (!L || !src) return fail(BAMREX_ERR_ARG, "NULL argument");
+    cudaPointerAttributes at;
+    const double* from = src;
+    if (cudaPointerGetAttributes(&at, src) != cudaSuccess || at.type != cudaMemoryTypeDevice) {
+        cudaGetLastError();
+        const cudaError_t e = cudaMemcpyAsync(L->staging, src, (size_t)L->ncells * L->NC * 8, cudaMemcpyDefault, L->stream);
+        if (e != cudaSuccess) return L->set_err(cuda_fail(e, "copy_in memcpy"));
+        from = L->staging;
+    }
+    BX_TRY(level_launch(L, launch_pack(L->NC, L->d_fab[L->cur], L->d_pack, (int)L->boxes.size(), L->ncells,
+                                       const_cast<double*>(from), 0, L->stream),
+                        "unpack"));
+    L->ws_valid = false;
+    return BAMREX_OK;
+}
+
+extern "C" int bamrex_level_copy_out(bamrex_level* L, double* dst)
+{
+    if (!L || !dst) return fail(BAMREX_ERR_ARG, "NULL argument");
+    cudaPointerAttributes at;
+    const bool dev = cudaPointerGetAttributes(&at, dst) == cudaSuccess && at.type == cudaMemoryTypeDevice;
+    cudaGetLastError();
+    double* to = dev ? dst : L->staging;
+    BX_TRY(level_launch(L, launch_pack(L->NC, L->d_fab[L->cur], L->d_pack, (int)L->boxes.size(), L->ncells, to, 1, L->stream),
+                        "pack"));
+    if (!dev) {
+        const cudaError_t e = cudaMemcpyAsync(dst, L->staging, (size_t)L->ncells * L->NC * 8, cudaMemcpyDefault, L->stream);
+        if (e != cudaSuccess) return L->set_err(cuda_fail(e, "copy_out memcpy"));
+    }
+    return BAMREX_OK;
+}
+
+extern "C" int bamrex_level_sync(bamrex_level* L)
+{
+    if (!L) return fail(BAMREX_ERR_ARG, "NULL level");
+    const cudaError_t e = cudaStreamSynchronize(L->stream);
+    if (e != cudaSuccess) return L->set_err(cuda_fail(e, "cudaStreamSynchronize"));
+    return BAMREX_OK;
+}
+
+extern "C" int bamrex_level_fill_boundary(bamrex_level* L)
+{
+    if (!L) return fail(BAMREX_ERR_ARG, "NULL level");
+    for (int d = 0; d < L->D; ++d) BX_TRY(level_fill(L, d, L->cur, nullptr));
+    return BAMREX_OK;
+}
+
+extern "C" int bamrex_level_advance(bamrex_level* L, double time, double dt, int iteration, int ncycle, double* dt_out)
+{
+    (void)time;
+    (void)iteration;
+    (void)ncycle;
+    if (!L) return fail(BAMREX_ERR_ARG, "NULL level");
+    if (!(dt > 0) || !std::isfinite(dt)) return L->set_err(fail(BAMREX_ERR_ARG, "dt must be positive and finite"));
+    {
+        const cudaError_t e = cudaMemsetAsync(&L->d_scal->ws_bits, 0, sizeof(unsigned long long), L->stream);
+        if (e != cudaSuccess) return L->set_err(cuda_fail(e, "memset"));
+    }
+    BX_TRY(level_step(L, L->cur, dt, nullptr, true));
+    L->cur ^= (L->D & 1);
+    L->ws_valid = true;
+    if (dt_out) *dt_out = dt;
+    return BAMREX_OK;
+}
+
+extern "C" int bamrex_level_est_time_step(bamrex_level* L, double* dt_est)
+{
+    if (!L || !dt_est) return fail(BAMREX_ERR_ARG, "NULL argument");
+    if (!L->ws_valid) {
+        cudaError_t e = cudaMemsetAsync(&L->d_scal->ws_bits, 0, sizeof(unsigned long long), L->stream);
+        if (e != cudaSuccess) return L->set_err(cuda_fail(e, "memset"));
+        BX_TRY(level_launch(L, launch_max_wave_speed(L->D, L->d_fab[L->cur], L->d_pack, (int)L->boxes.size(), L->ncells, L->k,
+                                                     &L->d_scal->ws_bits, nullptr, L->stream),
+                            "max wave speed"));
+    }
+    cudaError_t e = cudaMemcpyAsync(L->h_scal, L->d_scal, sizeof(StepScalars), cudaMemcpyDeviceToHost, L->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(L->stream);
+    if (e != cudaSuccess) return L->set_err(cuda_fail(e, "est_time_step"));
+    L->ws_valid = true;
+    const double ms = [&] {
+        double v;
+        std::memcpy(&v, &L->h_scal->ws_bits, sizeof(double));
+        return v;
+    }();
+    double dt = 1.0e20;
+    for (int d = 0; d < L->D; ++d) dt = std::min(dt, L->dx[d] / ms);
+    dt *= L->cfl;
+    if (!std::isfinite(dt) || !(dt > 0)) return L->set_err(fail(BAMREX_ERR_NAN, "non-finite time step estimate"));
+    *dt_est = dt;
+    return BAMREX_OK;
+}
+
+extern "C" int bamrex_level_run_async(bamrex_level* L, int nsteps, double stop_time, int use_graph, double start_time)
+{
+    if (!L) return fail(BAMREX_ERR_ARG, "NULL level");
+    if (nsteps < 0) return L->set_err(fail(BAMREX_ERR_ARG, "nsteps must be >= 0"));
+    if (L->run_pending) return L->set_err(fail(BAMREX_ERR_ARG, "a run is pending: call bamrex_level_run_wait"));
+    StepScalars* h = L->h_scal;
+    std::memset(h, 0, sizeof(*h));
+    h->time = start_time;
+    h->stop_time = stop_time;
+    cudaError_t e = cudaMemcpyAsync(L->d_scal, h, sizeof(StepScalars), cudaMemcpyHostToDevice, L->stream);
+    if (e != cudaSuccess) return L->set_err(cuda_fail(e, "scalars upload"));
+    // computeInitialDt from the current state
+    BX_TRY(level_launch(L, launch_max_wave_speed(L->D, L->d_fab[L->cur], L->d_pack, (int)L->boxes.size(), L->ncells, L->k,
+                                                 &L->d_scal->ws_bits, L->d_scal, L->stream),
+                        "max wave speed"));
+    BX_TRY(level_launch(L, launch_step_dt(L->d_scal, L->D, L->dx[0], L->dx[1], L->dx[2], L->cfl, 0, L->stream), "step dt"));
+    const int start = L->cur;
+    int p = start;
+    for (int s = 0; s < nsteps; ++s) {
+        if (use_graph) {
+            if (!L->graph[p]) {
+                cudaGraph_t gr = nullptr;
+                e = cudaStreamBeginCapture(L->stream, cudaStreamCaptureModeThreadLocal);
+                if (e != cudaSuccess) return L->set_err(cuda_fail(e, "begin capture"));
+                const long long before = L->launches;
+                const int rc = level_step(L, p, 0.0, L->d_scal, false);
+                e = cudaStreamEndCapture(L->stream, &gr);
+                if (rc != BAMREX_OK) {
+                    if (gr) cudaGraphDestroy(gr);
+                    return rc;
+                }
+                if (e != cudaSuccess) return L->set_err(cuda_fail(e, "end capture"));
+                L->launches = before;  // counted per replay below
+                e = cudaGraphInstantiate(&L->graph[p], gr, 0);
+                cudaGraphDestroy(gr);
+                if (e != cudaSuccess) return L->set_err(cuda_fail(e, "graph instantiate"));
+            }
+            e = cudaGraphLaunch(L->graph[p], L->stream);
+            if (e != cudaSuccess) return L->set_err(cuda_fail(e, "graph launch"));
+            L->launches += 2 * L->D + 1;
+        } else {
+            BX_TRY(level_step(L, p, 0.0, L->d_scal, true));
+        }
+        p ^= (L->D & 1);
+    }
+    e = cudaMemcpyAsync(h, L->d_scal, sizeof(StepScalars), cudaMemcpyDeviceToHost, L->stream);
+    if (e != cudaSuccess) return L->set_err(cuda_fail(e, "scalars readback"));
+    L->run_pending = true;
+    L->run_start_parity = start;
+    return BAMREX_OK;
+}
+
+extern "C" int bamrex_level_run_wait(bamrex_level* L, double* time_out, int* steps_done)
+{
+    if (!L) return fail(BAMREX_ERR_ARG, "NULL level");
+    if (!L->run_pending) return L->set_err(fail(BAMREX_ERR_ARG, "no run pending"));
+    const cudaError_t e = cudaStreamSynchronize(L->stream);
+    L->run_pending = false;
+    if (e != cudaSuccess) return L->set_err(cuda_fail(e, "run"));
+    const StepScalars* h = L->h_scal;
+    L->cur = L->run_start_parity ^ ((h->steps * L->D) & 1);
+    L->ws_valid = false;
+    if (time_out) *time_out = h->time;
+    if (steps_done) *steps_done = h->steps;
+    if (h->status != 0) return L->set_err(fail(h->status, "non-finite time step during the run"));
+    return BAMREX_OK;
+}
+
+extern "C" int bamrex_level_run(bamrex_level* L, int nsteps, double stop_time, int use_graph, double* time_io,
+                                int* steps_done)
+{
+    if (!L || !time_io) return fail(BAMREX_ERR_ARG, "NULL argument");
+    BX_TRY(bamrex_level_run_async(L, nsteps, stop_time, use_graph, *time_io));
+    return bamrex_level_run_wait(L, time_io, steps_done);
+}
+
+extern "C" int bamrex_level_set_timing(bamrex_level* L, int enable)
+{
+    if (!L) return fail(BAMREX_ERR_ARG, "NULL level");
+    L->timing = enable != 0;
+    if (L->timing && L->events.empty()) {
+        L->events.resize(8192);
+        for (auto& ev : L->events) {
+            if (cudaEventCreate(&ev.first) != cudaSuccess || cudaEventCreate(&ev.second) != cudaSuccess)
+                return L->set_err(fail(BAMREX_ERR_CUDA, "cudaEventCreate failed"));
+        }
+    }
+    L->ev_used = 0;
+    return BAMREX_OK;
+}
+
+extern "C" int bamrex_level_counters(bamrex_level* L, long long* launches, double* sweep_ms, long long* sweep_launches)
+{
+    if (!L) return fail(BAMREX_ERR_ARG, "NULL level");
+    if (L->ev_used) {
+        const cudaError_t e = cudaStreamSynchronize(L->stream);
+        if (e != cudaSuccess) return L->set_err(cuda_fail(e, "sync"));
+        for (size_t i = 0; i < L->ev_used; ++i) {
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, L->events[i].first, L->events[i].second);
+            L->sweep_ms += ms;
+        }
+        L->sweep_launches += (long long)L->ev_used;
+        L->ev_used = 0;
+    }
+    if (launches) *launches = L->launches;
+    if (sweep_ms) *sweep_ms = L->sweep_ms;
+    if (sweep_launches) *sweep_launches = L->sweep_launches;
+    return BAMREX_OK;
+}
+
+extern "C" int bamrex_level_reset_counters(bamrex_level* L)
+{
+    if (!L) return fail(BAMREX_ERR_ARG, "NULL level");
+    if (L->ev_used) cudaStreamSynchronize(L->stream);
+    L->launches = 0;
+    L->ev_used = 0;
+    L->sweep_ms = 0.0;
+    L->sweep_launches = 0;
+    return BAMREX_OK;
+}

@@ -1,0 +1,365 @@
+// Light kernels of the explicit path: ghost fill (FillBoundary + physical
+// boundary conditions), pack/unpack of valid cells, the stand-alone max
+// wave speed reduction, device time-step bookkeeping, and the per-box
+// left/right flux and update kernels of the Fluxes.H / Update.H surface.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
+#include "common.cuh"
+#include "euler.cuh"
+#include "launch.h"
+
+namespace bamrex {
+
+namespace {
+
+constexpr int kThreads = 256;
+
+int grid_for(long long work, int per_thread = 1)
+{
+    const long long want = (work + (long long)kThreads * per_thread - 1) / ((long long)kThreads * per_thread);
+    const long long cap = (long long)device_sm_count() * 8;
+    return (int)std::max(1LL, std::min(want, cap));
+}
+
+__device__ __forceinline__ long long fab_index(const FabDev& f, int i, int j, int k)
+{
+    return (long long)(i - f.b0) + (long long)(j - f.b1) * f.js + (long long)(k - f.b2) * f.ks;
+}
+
+template <typename T>
+__device__ __forceinline__ int find_by_begin(const T* v, int n, long long idx)
+{
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (v[mid].cell_begin <= idx) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+// ---------------------------------------------------------------- ghosts
+// bamrexBCData::fill_consv_boundary (Source/BoundaryConditions/BCs.cpp:429-442)
+// expressed as a table of region copies built on the host.
+__global__ void ghost_fill_kernel(int NC, const GhostOp* __restrict__ ops, int nops, long long total,
+                                  const FabDev* __restrict__ fabs, const StepScalars* scal)
+{
+    if (scal && scal->done) return;
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const GhostOp& op = ops[find_by_begin(ops, nops, idx)];
+        const long long local = idx - op.cell_begin;
+        const int nx = op.hi[0] - op.lo[0] + 1, ny = op.hi[1] - op.lo[1] + 1;
+        const int ci = op.lo[0] + (int)(local % nx);
+        const int cj = op.lo[1] + (int)((local / nx) % ny);
+        const int ck = op.lo[2] + (int)(local / ((long long)nx * ny));
+        const int si = op.off[0] + op.mul[0] * ci;
+        const int sj = op.off[1] + op.mul[1] * cj;
+        const int sk = op.off[2] + op.mul[2] * ck;
+        const FabDev& d = fabs[op.dst];
+        const FabDev& s = fabs[op.src];
+        const double* ps = s.p + fab_index(s, si, sj, sk);
+        double* pd = d.p + fab_index(d, ci, cj, ck);
+        for (int n = 0; n < NC; ++n) {
+            const double v = ps[n * s.ns];
+            pd[n * d.ns] = ((op.negmask >> n) & 1) ? -v : v;
+        }
+    }
+}
+
+// ---------------------------------------------------------------- pack
+__global__ void pack_kernel(int NC, const FabDev* __restrict__ fabs, const PackBox* __restrict__ boxes, int nboxes,
+                            long long total, double* __restrict__ packed, int to_packed)
+{
+    // packed element e = cell_begin*NC + n*ncells_box + cell
+    const long long nel = total * NC;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < nel;
+         e += (long long)gridDim.x * blockDim.x) {
+        // find the box whose packed range contains e
+        int lo = 0, hi = nboxes - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (boxes[mid].cell_begin * NC <= e) lo = mid; else hi = mid - 1;
+        }
+        const PackBox& B = boxes[lo];
+        const int nx = B.hi[0] - B.lo[0] + 1, ny = B.hi[1] - B.lo[1] + 1, nz = B.hi[2] - B.lo[2] + 1;
+        const long long ncell = (long long)nx * ny * nz;
+        const long long local = e - B.cell_begin * NC;
+        const int n = (int)(local / ncell);
+        const long long c = local % ncell;
+        const int i = B.lo[0] + (int)(c % nx);
+        const int j = B.lo[1] + (int)((c / nx) % ny);
+        const int k = B.lo[2] + (int)(c / ((long long)nx * ny));
+        const FabDev& f = fabs[lo];
+        double* pf = f.p + fab_index(f, i, j, k) + n * f.ns;
+        if (to_packed) packed[e] = *pf;
+        else *pf = packed[e];
+    }
+}
+
+// ---------------------------------------------------------------- max speed
+// max_wave_speed (Source/System/Euler/Euler.cpp:46-74) over valid cells.
+template <int D>
+__global__ void max_ws_kernel(const FabDev* __restrict__ fabs, const PackBox* __restrict__ boxes, int nboxes,
+                              long long total, const Consts k, unsigned long long* ws_bits, const StepScalars* scal)
+{
+    if (scal && scal->done) return;
+    constexpr int NC = D + 2;
+    double wmax = 0.0;
+    bool nan_seen = false;
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < total;
+         c += (long long)gridDim.x * blockDim.x) {
+        const int b = find_by_begin(boxes, nboxes, c);
+        const PackBox& B = boxes[b];
+        const int nx = B.hi[0] - B.lo[0] + 1, ny = B.hi[1] - B.lo[1] + 1;
+        const long long local = c - B.cell_begin;
+        const int i = B.lo[0] + (int)(local % nx);
+        const int j = B.lo[1] + (int)((local / nx) % ny);
+        const int kk = B.lo[2] + (int)(local / ((long long)nx * ny));
+        const FabDev& f = fabs[b];
+        const double* p = f.p + fab_index(f, i, j, kk);
+        double U[NC];
+        for (int n = 0; n < NC; ++n) U[n] = p[n * f.ns];
+        const double w = wave_speed<D>(U, k);
+        wmax = fmax(wmax, w);
+        nan_seen = nan_seen || (w != w);
+    }
+    for (int off = 16; off > 0; off >>= 1) wmax = fmax(wmax, __shfl_xor_sync(0xffffffffu, wmax, off));
+    const bool any_nan = __any_sync(0xffffffffu, nan_seen);
+    if ((threadIdx.x & 31) == 0) {
+        if (any_nan) atomicMax(ws_bits, 0x7ff8000000000000ull);
+        else if (wmax > 0.0) atomicMax(ws_bits, (unsigned long long)__double_as_longlong(wmax));
+    }
+}
+
+// ---------------------------------------------------------------- dt
+// estTimeStep (Source/AmrLevelAdv.cpp:395-477 -> FluidSystem.cpp:194-206):
+// cfl * min_d dx_d / max_speed, then the stop-time clamp of
+// computeInitialDt / computeNewDt (Source/AmrLevelAdv.cpp:513-523, 600-611).
+__global__ void step_dt_kernel(StepScalars* s, int D, double dx0, double dx1, double dx2, double cfl, int mode)
+{
+    if (s->done) return;
+    if (mode == 1) {
+        s->time = s->time + s->dt;
+        s->steps += 1;
+    }
+    const double ms = __longlong_as_double((long long)s->ws_bits);
+    double dt_est = 1.0e20;
+    const double dxs[3] = { dx0, dx1, dx2 };
+    for (int d = 0; d < D; ++d) dt_est = fmin(dt_est, dxs[d] / ms);
+    dt_est *= cfl;
+    double dt_0 = dt_est;
+    if (s->stop_time >= 0.0) {
+        const double eps = 0.001 * dt_0;
+        if ((s->time + dt_0) > (s->stop_time - eps)) dt_0 = s->stop_time - s->time;
+        if (!(s->time < s->stop_time)) s->done = 1;
+    }
+    if (!(dt_est > 0.0) || dt_est != dt_est || isinf(dt_est)) {
+        s->status = 3; /* BAMREX_ERR_NAN */
+        s->done = 1;
+    }
+    s->dt = dt_0;
+    s->ws_bits = 0ull;
+}
+
+// ---------------------------------------------------------------- LR flux
+// compute_HLLC_flux_LR / compute_force_flux_LR on a box: one thread per face.
+template <int D, int DIR, int KIND>
+__global__ void flux_lr_kernel(int lo0, int lo1, int lo2, int hi0, int hi1, int hi2, const FabDev flux,
+                               const FabDev cL, const FabDev cR, const Consts k, double half_dx_dt, double dt_2dx)
+{
+    constexpr int NC = D + 2;
+    const int fhi[3] = { hi0 + (DIR == 0), hi1 + (DIR == 1), hi2 + (DIR == 2) };
+    const int nx = fhi[0] - lo0 + 1, ny = fhi[1] - lo1 + 1, nz = fhi[2] - lo2 + 1;
+    const long long total = (long long)nx * ny * nz;
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const int i = lo0 + (int)(idx % nx);
+        const int j = lo1 + (int)((idx / nx) % ny);
+        const int kk = lo2 + (int)(idx / ((long long)nx * ny));
+        double L[NC], R[NC], F[NC];
+        const double* pl = cL.p + fab_index(cL, i - (DIR == 0), j - (DIR == 1), kk - (DIR == 2));
+        const double* pr = cR.p + fab_index(cR, i, j, kk);
+        for (int n = 0; n < NC; ++n) {
+            L[n] = pl[n * cL.ns];
+            R[n] = pr[n * cR.ns];
+        }
+        if (KIND == M_HLLC) hllc_face<D, DIR>(L, R, k, F);
+        else force_face<D, DIR>(L, R, k, half_dx_dt, dt_2dx, F);
+        double* pf = flux.p + fab_index(flux, i, j, kk);
+        for (int n = 0; n < NC; ++n) pf[n * flux.ns] = F[n];
+    }
+}
+
+// ---------------------------------------------------------------- updates
+// AmrLevelAdv_advance.cpp:330-341 (sweep, dt/dx division form)
+template <int D, int DIR>
+__global__ void sweep_update_kernel(const UpdateArgs u)
+{
+    constexpr int NC = D + 2;
+    const int nx = u.hi[0] - u.lo[0] + 1, ny = u.hi[1] - u.lo[1] + 1, nz = u.hi[2] - u.lo[2] + 1;
+    const long long total = (long long)nx * ny * nz;
+    const FabDev& fl = u.flux[0];
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const int i = u.lo[0] + (int)(idx % nx);
+        const int j = u.lo[1] + (int)((idx / nx) % ny);
+        const int k = u.lo[2] + (int)(idx / ((long long)nx * ny));
+        const double* pin = u.in.p + fab_index(u.in, i, j, k);
+        const double* pf0 = fl.p + fab_index(fl, i, j, k);
+        const double* pf1 = fl.p + fab_index(fl, i + (DIR == 0), j + (DIR == 1), k + (DIR == 2));
+        double* po = u.out.p + fab_index(u.out, i, j, k);
+        for (int n = 0; n < NC; ++n)
+            po[n * u.out.ns] = pin[n * u.in.ns] - u.dtdx[0] * (pf1[n * fl.ns] - pf0[n * fl.ns]);
+    }
+}
+
+// conservative_update(bx, ...) (Source/Fluxes/Update.H:99-130, dt*idx form)
+template <int D>
+__global__ void cons_update_kernel(const UpdateArgs u)
+{
+    constexpr int NC = D + 2;
+    const int nx = u.hi[0] - u.lo[0] + 1, ny = u.hi[1] - u.lo[1] + 1, nz = u.hi[2] - u.lo[2] + 1;
+    const long long total = (long long)nx * ny * nz;
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const int i = u.lo[0] + (int)(idx % nx);
+        const int j = u.lo[1] + (int)((idx / nx) % ny);
+        const int k = u.lo[2] + (int)(idx / ((long long)nx * ny));
+        const double* pin = u.in.p + fab_index(u.in, i, j, k);
+        double* po = u.out.p + fab_index(u.out, i, j, k);
+        for (int n = 0; n < NC; ++n) {
+            double v = pin[n * u.in.ns];
+#pragma unroll
+            for (int d = 0; d < D; ++d) {
+                const FabDev& f = u.flux[d];
+                const double a = f.p[fab_index(f, i + (d == 0), j + (d == 1), k + (d == 2)) + n * f.ns];
+                const double b = f.p[fab_index(f, i, j, k) + n * f.ns];
+                v = v - u.dtdx[d] * (a - b);
+            }
+            po[n * u.out.ns] = v;
+        }
+    }
+}
+
+}  // namespace
+
+int device_sm_count()
+{
+    static int cache[64] = { 0 };
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) return 148;
+    if (!cache[dev]) {
+        int n = 0;
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        cache[dev] = n > 0 ? n : 148;
+    }
+    return cache[dev];
+}
+
+cudaError_t launch_ghost_fill(int NC, const GhostOp* ops, int nops, long long total_cells, const FabDev* fabs,
+                              const StepScalars* scal, cudaStream_t s)
+{
+    if (nops == 0 || total_cells == 0) return cudaSuccess;
+    ghost_fill_kernel<<<grid_for(total_cells), kThreads, 0, s>>>(NC, ops, nops, total_cells, fabs, scal);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pack(int NC, const FabDev* fabs, const PackBox* boxes, int nboxes, long long total_cells,
+                        double* packed, int to_packed, cudaStream_t s)
+{
+    if (total_cells == 0) return cudaSuccess;
+    pack_kernel<<<grid_for(total_cells * NC, 4), kThreads, 0, s>>>(NC, fabs, boxes, nboxes, total_cells, packed,
+                                                                  to_packed);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_max_wave_speed(int D, const FabDev* fabs, const PackBox* boxes, int nboxes,
+                                  long long total_cells, const Consts& k, unsigned long long* ws_bits,
+                                  const StepScalars* scal, cudaStream_t s)
+{
+    const int g = grid_for(total_cells, 4);
+    switch (D) {
+    case 1: max_ws_kernel<1><<<g, kThreads, 0, s>>>(fabs, boxes, nboxes, total_cells, k, ws_bits, scal); break;
+    case 2: max_ws_kernel<2><<<g, kThreads, 0, s>>>(fabs, boxes, nboxes, total_cells, k, ws_bits, scal); break;
+    case 3: max_ws_kernel<3><<<g, kThreads, 0, s>>>(fabs, boxes, nboxes, total_cells, k, ws_bits, scal); break;
+    default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_step_dt(StepScalars* scal, int D, double dx0, double dx1, double dx2, double cfl, int mode,
+                           cudaStream_t s)
+{
+    step_dt_kernel<<<1, 1, 0, s>>>(scal, D, dx0, dx1, dx2, cfl, mode);
+    return cudaGetLastError();
+}
+
+template <int D, int DIR>
+static cudaError_t flux_lr_dispatch(int kind, const int* lo, const int* hi, const FabDev& flux, const FabDev& cL,
+                                    const FabDev& cR, const Consts& k, double half_dx_dt, double dt_2dx,
+                                    cudaStream_t s)
+{
+    long long faces = 1;
+    for (int d = 0; d < 3; ++d) faces *= (long long)(hi[d] - lo[d] + 1 + (d == DIR));
+    const int g = grid_for(faces);
+    if (kind == M_HLLC)
+        flux_lr_kernel<D, DIR, M_HLLC><<<g, 128, 0, s>>>(lo[0], lo[1], lo[2], hi[0], hi[1], hi[2], flux, cL, cR, k,
+                                                         half_dx_dt, dt_2dx);
+    else
+        flux_lr_kernel<D, DIR, M_FORCE><<<g, 128, 0, s>>>(lo[0], lo[1], lo[2], hi[0], hi[1], hi[2], flux, cL, cR, k,
+                                                          half_dx_dt, dt_2dx);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_flux_LR(int D, int dir, int kind, const int* lo, const int* hi, const FabDev& flux,
+                           const FabDev& cL, const FabDev& cR, const Consts& k, double dx, double dt,
+                           cudaStream_t s)
+{
+    const double half_dx_dt = 0.5 * dx / dt, dt_2dx = dt / (2 * dx);
+#define BAMREX_LR(DD, DR) \
+    if (D == DD && dir == DR) return flux_lr_dispatch<DD, DR>(kind, lo, hi, flux, cL, cR, k, half_dx_dt, dt_2dx, s);
+    BAMREX_LR(1, 0)
+    BAMREX_LR(2, 0)
+    BAMREX_LR(2, 1)
+    BAMREX_LR(3, 0)
+    BAMREX_LR(3, 1)
+    BAMREX_LR(3, 2)
+#undef BAMREX_LR
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_sweep_update(int D, int dir, const UpdateArgs& u, cudaStream_t s)
+{
+    long long cells = 1;
+    for (int d = 0; d < 3; ++d) cells *= (long long)(u.hi[d] - u.lo[d] + 1);
+    const int g = grid_for(cells);
+#define BAMREX_UP(DD, DR) \
+    if (D == DD && dir == DR) { sweep_update_kernel<DD, DR><<<g, kThreads, 0, s>>>(u); return cudaGetLastError(); }
+    BAMREX_UP(1, 0)
+    BAMREX_UP(2, 0)
+    BAMREX_UP(2, 1)
+    BAMREX_UP(3, 0)
+    BAMREX_UP(3, 1)
+    BAMREX_UP(3, 2)
+#undef BAMREX_UP
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_conservative_update(int D, const UpdateArgs& u, cudaStream_t s)
+{
+    long long cells = 1;
+    for (int d = 0; d < 3; ++d) cells *= (long long)(u.hi[d] - u.lo[d] + 1);
+    const int g = grid_for(cells);
+    switch (D) {
+    case 1: cons_update_kernel<1><<<g, kThreads, 0, s>>>(u); break;
+    case 2: cons_update_kernel<2><<<g, kThreads, 0, s>>>(u); break;
+    case 3: cons_update_kernel<3><<<g, kThreads, 0, s>>>(u); break;
+    default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace bamrex

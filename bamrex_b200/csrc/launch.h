@@ -1,0 +1,67 @@
+// Host-side launch interface between the C ABI / level driver (abi.cu) and
+// the kernel translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+
+namespace bamrex {
+
+// Ghost-cell copy: dst box cell c takes src box cell s with
+// s_d = off[d] + mul[d] * c_d (mul 1: copy / periodic shift, -1: mirror,
+// 0: clamp to a boundary layer); components in negmask change sign.
+struct GhostOp {
+    int dst, src;
+    int lo[3], hi[3];
+    int off[3], mul[3];
+    int negmask;
+    int pad;
+    long long cell_begin;
+};
+
+// Valid region of a box in the packed (box-major, SoA) host layout.
+struct PackBox {
+    int lo[3], hi[3];
+    long long cell_begin;
+};
+
+struct UpdateArgs {
+    int lo[3], hi[3];
+    FabDev out, in, flux[3];
+    double dtdx[3];
+};
+
+int device_sm_count();
+
+cudaError_t launch_sweep(int D, int dir, int method, const SweepArgs& a, cudaStream_t s);
+
+// Warps of the sweep kernel that fit on the device at once (for choosing
+// segment lengths); 0 for an unsupported combination.
+long long sweep_resident_warps(int D, int dir, int method);
+
+cudaError_t launch_ghost_fill(int NC, const GhostOp* ops, int nops, long long total_cells, const FabDev* fabs,
+                              const StepScalars* scal, cudaStream_t s);
+
+cudaError_t launch_pack(int NC, const FabDev* fabs, const PackBox* boxes, int nboxes, long long total_cells,
+                        double* packed, int to_packed, cudaStream_t s);
+
+cudaError_t launch_max_wave_speed(int D, const FabDev* fabs, const PackBox* boxes, int nboxes,
+                                  long long total_cells, const Consts& k, unsigned long long* ws_bits,
+                                  const StepScalars* scal, cudaStream_t s);
+
+// Time-step bookkeeping on the device (computeInitialDt / computeNewDt).
+// mode 0: initial dt from ws_bits at the current time; mode 1: end of a
+// step (time += dt, steps++, then the next dt).
+cudaError_t launch_step_dt(StepScalars* scal, int D, double dx0, double dx1, double dx2, double cfl, int mode,
+                           cudaStream_t s);
+
+cudaError_t launch_flux_LR(int D, int dir, int kind, const int* lo, const int* hi, const FabDev& flux,
+                           const FabDev& cL, const FabDev& cR, const Consts& k, double dx, double dt,
+                           cudaStream_t s);
+
+cudaError_t launch_sweep_update(int D, int dir, const UpdateArgs& u, cudaStream_t s);
+
+cudaError_t launch_conservative_update(int D, const UpdateArgs& u, cudaStream_t s);
+
+}  // namespace bamrex

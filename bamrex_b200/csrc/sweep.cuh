@@ -1,0 +1,311 @@
+// Fused split-sweep kernels: per box, the interface flux of one direction
+// and the conservative update (compute_*_flux + the update lambda of
+// AmrLevelAdv::advance_explicit, Source/AmrLevelAdv_advance.cpp:290-341),
+// in one pass that reads U once and writes U once.
+//
+// Work decomposition: a launch covers every box of a sweep (the device box
+// table); each warp takes work items from a grid-stride loop.
+//  * x sweep (contiguous direction): an item is a segment of one row.  The
+//    warp marches along the row in 32-cell chunks, lane t holding cell
+//    x0+t; neighbour states come from warp shuffles, and the values of the
+//    previous chunk's top lanes carry the stencil across chunk boundaries.
+//  * y / z sweeps (strided directions): an item is a group of 32 adjacent
+//    columns x and a segment along the sweep; each thread marches its column
+//    keeping the stencil in registers.  Loads and stores are coalesced
+//    across the warp (32 consecutive doubles per component).
+// Pipeline per position o: load U(o+2); cell stage of cell o+1 (needs
+// U(o..o+2)); face o+1 from UR(o) and UL(o+1); update of cell o from faces o
+// and o+1.
+#pragma once
+
+#include "common.cuh"
+#include "euler.cuh"
+
+namespace bamrex {
+
+constexpr int kSweepThreads = 128;
+
+__device__ __forceinline__ int find_box(const SweepBox* boxes, int nboxes, long long item)
+{
+    int lo = 0, hi = nboxes - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (boxes[mid].item_begin <= item) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+struct StepFactors {
+    double dtdx, hdtdx, half_dx_dt, dt_2dx;
+};
+
+__device__ __forceinline__ bool step_factors(const SweepArgs& a, StepFactors& s)
+{
+    double dt = a.dt_host;
+    if (a.scal) {
+        if (a.scal->done) return false;
+        dt = a.scal->dt;
+    }
+    s.dtdx = dt / a.dx;               // (dt / dx[d]), AmrLevelAdv_advance.cpp:337
+    s.hdtdx = 0.5 * dt / a.dx;        // Flux_Helpers.cpp:138
+    s.half_dx_dt = 0.5 * a.dx / dt;   // Force.cpp:77, 144
+    s.dt_2dx = dt / (2 * a.dx);       // Force.cpp:91
+    return true;
+}
+
+// A benign state used for lanes that have nothing to load: keeps the
+// arithmetic of idle lanes finite.
+template <int NC>
+__device__ __forceinline__ void benign(double (&u)[NC])
+{
+    u[0] = 1.0;
+#pragma unroll
+    for (int n = 1; n < NC - 1; ++n) u[n] = 0.0;
+    u[NC - 1] = 1.0;
+}
+
+template <int NC>
+__device__ __forceinline__ void ld_state(const double* __restrict__ p, long long ns, double (&u)[NC])
+{
+#pragma unroll
+    for (int n = 0; n < NC; ++n) u[n] = __ldg(p + n * ns);
+}
+
+template <int NC>
+__device__ __forceinline__ void shfl_carry(const double (&cur)[NC], const double (&prev)[NC], int lane,
+                                           int shift, double (&out)[NC])
+{
+    // lane t receives cur[t-shift], or prev[32+t-shift] for t < shift
+    const bool from_prev = lane >= 32 - shift;
+#pragma unroll
+    for (int n = 0; n < NC; ++n)
+        out[n] = __shfl_sync(0xffffffffu, from_prev ? prev[n] : cur[n], (lane + 32 - shift) & 31);
+}
+
+// Warp max of the wave speed, then one atomicMax per warp on the ordered bit
+// pattern (non-negative doubles order like their bits).  A NaN anywhere is
+// reported as the NaN bit pattern, which is larger than every finite value,
+// so the time step becomes NaN and the host sees BAMREX_ERR_NAN.
+__device__ __forceinline__ void reduce_ws(double ws, bool nan_seen, unsigned long long* dst)
+{
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) ws = fmax(ws, __shfl_xor_sync(0xffffffffu, ws, off));
+    const bool any_nan = __any_sync(0xffffffffu, nan_seen);
+    if ((threadIdx.x & 31) == 0) {
+        if (any_nan) atomicMax(dst, 0x7ff8000000000000ull);
+        else if (ws > 0.0) atomicMax(dst, (unsigned long long)__double_as_longlong(ws));
+    }
+}
+
+__device__ __forceinline__ void track_ws(double w, double& wsmax, bool& nan_seen)
+{
+    wsmax = fmax(wsmax, w);
+    nan_seen = nan_seen || (w != w);
+}
+
+// ------------------------------------------------------------------ x sweep
+template <int D, int METHOD>
+__global__ void __launch_bounds__(kSweepThreads) sweep_x_kernel(const SweepArgs a)
+{
+    using S = Scheme<D, 0, METHOD>;
+    constexpr int NC = D + 2;
+    constexpr int H = S::kHalo;
+    StepFactors f;
+    if (!step_factors(a, f)) return;
+    const int lane = threadIdx.x & 31;
+    const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+    double wsmax = 0.0;
+    bool nan_seen = false;
+
+    for (long long it = gw; it < a.total_items; it += nw) {
+        const int b = a.boxes ? find_box(a.boxes, a.nboxes, it) : 0;
+        const SweepBox& B = a.boxes ? a.boxes[b] : a.one;
+        const long long local = it - B.item_begin;
+        const int seg = (int)(local % B.nseg);
+        const long long row = local / B.nseg;
+        const int ny = B.hi[1] - B.lo[1] + 1;
+        const int j = B.lo[1] + (int)(row % ny);
+        const int kk = B.lo[2] + (int)(row / ny);
+        const int s0 = B.lo[0] + seg * a.seglen;
+        const int s1 = min(s0 + a.seglen, B.hi[0] + 1);
+        const bool last_seg = (s1 == B.hi[0] + 1);
+
+        const double* __restrict__ in = B.in.p + (long long)(j - B.in.b1) * B.in.js + (long long)(kk - B.in.b2) * B.in.ks;
+        double* __restrict__ out = B.out.p + (long long)(j - B.out.b1) * B.out.js + (long long)(kk - B.out.b2) * B.out.ks;
+        double* __restrict__ fl = B.flux.p ? B.flux.p + (long long)(j - B.flux.b1) * B.flux.js + (long long)(kk - B.flux.b2) * B.flux.ks : nullptr;
+
+        double Ap[NC], URp[NC], Fp[NC];
+        benign(Ap);
+        benign(URp);
+#pragma unroll
+        for (int n = 0; n < NC; ++n) Fp[n] = 0.0;
+
+        // prefetch the first chunk
+        double An[NC];
+        {
+            const int xl = s0 - 32 + lane + 2;
+            if (xl >= s0 - H && xl <= s1 - 1 + H) ld_state(in + (xl - B.in.b0), B.in.ns, An);
+            else benign(An);
+        }
+        for (int x0 = s0 - 32; x0 < s1; x0 += 32) {
+            double A[NC];
+#pragma unroll
+            for (int n = 0; n < NC; ++n) A[n] = An[n];
+            {
+                const int xl = x0 + 32 + lane + 2;
+                if (x0 + 32 < s1 && xl >= s0 - H && xl <= s1 - 1 + H) ld_state(in + (xl - B.in.b0), B.in.ns, An);
+                else benign(An);
+            }
+            const int o = x0 + lane;
+            double Um1[NC], Um2[NC];
+            shfl_carry(A, Ap, lane, 1, Um1);  // U(o+1)
+            shfl_carry(A, Ap, lane, 2, Um2);  // U(o)
+            double UL[NC], UR[NC];
+            S::cell(Um2, Um1, A, a.k, f.hdtdx, UL, UR);  // cell o+1
+            double URm1[NC];
+            shfl_carry(UR, URp, lane, 1, URm1);  // UR(o)
+            double F[NC];
+            S::face(URm1, UL, a.k, f.half_dx_dt, f.dt_2dx, F);  // face o+1
+            double Fm1[NC];
+            shfl_carry(F, Fp, lane, 1, Fm1);  // face o
+            if (a.do_update && o >= s0 && o < s1) {
+                double Un[NC];
+#pragma unroll
+                for (int n = 0; n < NC; ++n) Un[n] = Um2[n] - f.dtdx * (F[n] - Fm1[n]);
+                double* po = out + (o - B.out.b0);
+#pragma unroll
+                for (int n = 0; n < NC; ++n) po[n * B.out.ns] = Un[n];
+                if (a.ws_max) track_ws(wave_speed<D>(Un, a.k), wsmax, nan_seen);
+            }
+            if (fl) {
+                const int fo = o + 1;
+                if (fo >= s0 && (fo < s1 || (fo == s1 && last_seg))) {
+                    double* pf = fl + (fo - B.flux.b0);
+#pragma unroll
+                    for (int n = 0; n < NC; ++n) pf[n * B.flux.ns] = F[n];
+                }
+            }
+#pragma unroll
+            for (int n = 0; n < NC; ++n) {
+                Ap[n] = A[n];
+                URp[n] = UR[n];
+                Fp[n] = F[n];
+            }
+        }
+    }
+    if (a.ws_max) reduce_ws(wsmax, nan_seen, a.ws_max);
+}
+
+// ------------------------------------------------------------ y / z sweeps
+template <int D, int DIR, int METHOD>
+__global__ void __launch_bounds__(kSweepThreads) sweep_s_kernel(const SweepArgs a)
+{
+    using S = Scheme<D, DIR, METHOD>;
+    constexpr int NC = D + 2;
+    constexpr int H = S::kHalo;
+    StepFactors f;
+    if (!step_factors(a, f)) return;
+    const int lane = threadIdx.x & 31;
+    const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+    double wsmax = 0.0;
+    bool nan_seen = false;
+
+    for (long long it = gw; it < a.total_items; it += nw) {
+        const int b = a.boxes ? find_box(a.boxes, a.nboxes, it) : 0;
+        const SweepBox& B = a.boxes ? a.boxes[b] : a.one;
+        const long long local = it - B.item_begin;
+        const int seg = (int)(local % B.nseg);
+        const long long rest = local / B.nseg;
+        const int grp = (int)(rest % B.ngroup);
+        const int t2 = (int)(rest / B.ngroup);  // the other transverse index
+        const int x = B.lo[0] + grp * 32 + lane;
+        const bool active = x <= B.hi[0];
+        const int s0 = B.lo[DIR] + seg * a.seglen;
+        const int s1 = min(s0 + a.seglen, B.hi[DIR] + 1);
+        const bool last_seg = (s1 == B.hi[DIR] + 1);
+
+        // column base pointers (position along DIR added per access)
+        long long inoff, outoff, floff = 0;
+        long long ins, outs, fls = 0;
+        if (DIR == 1) {
+            const int kk = (D == 3) ? B.lo[2] + t2 : 0;
+            inoff = (long long)(x - B.in.b0) + (long long)(kk - B.in.b2) * B.in.ks - (long long)B.in.b1 * B.in.js;
+            outoff = (long long)(x - B.out.b0) + (long long)(kk - B.out.b2) * B.out.ks - (long long)B.out.b1 * B.out.js;
+            ins = B.in.js;
+            outs = B.out.js;
+            if (B.flux.p) {
+                floff = (long long)(x - B.flux.b0) + (long long)(kk - B.flux.b2) * B.flux.ks - (long long)B.flux.b1 * B.flux.js;
+                fls = B.flux.js;
+            }
+        } else {
+            const int jj = B.lo[1] + t2;
+            inoff = (long long)(x - B.in.b0) + (long long)(jj - B.in.b1) * B.in.js - (long long)B.in.b2 * B.in.ks;
+            outoff = (long long)(x - B.out.b0) + (long long)(jj - B.out.b1) * B.out.js - (long long)B.out.b2 * B.out.ks;
+            ins = B.in.ks;
+            outs = B.out.ks;
+            if (B.flux.p) {
+                floff = (long long)(x - B.flux.b0) + (long long)(jj - B.flux.b1) * B.flux.js - (long long)B.flux.b2 * B.flux.ks;
+                fls = B.flux.ks;
+            }
+        }
+        const double* __restrict__ in = B.in.p + inoff;
+        double* __restrict__ out = B.out.p + outoff;
+
+        auto load = [&](int pos, double (&u)[NC]) {
+            if (active && pos >= s0 - H && pos <= s1 - 1 + H) ld_state(in + (long long)pos * ins, B.in.ns, u);
+            else benign(u);
+        };
+
+        double Uo[NC], Uo1[NC], Nx[NC];
+        load(s0 - 2, Uo);
+        load(s0 - 1, Uo1);
+        load(s0, Nx);
+        double URo[NC], Fo[NC];
+        benign(URo);
+#pragma unroll
+        for (int n = 0; n < NC; ++n) Fo[n] = 0.0;
+
+        for (int o = s0 - 2; o < s1; ++o) {
+            double U2[NC];
+#pragma unroll
+            for (int n = 0; n < NC; ++n) U2[n] = Nx[n];
+            load(o + 3, Nx);
+            double UL[NC], UR[NC];
+            S::cell(Uo, Uo1, U2, a.k, f.hdtdx, UL, UR);  // cell o+1
+            if (o >= s0 - 1) {
+                double F[NC];
+                S::face(URo, UL, a.k, f.half_dx_dt, f.dt_2dx, F);  // face o+1
+                if (o >= s0 && a.do_update && active) {
+                    double Un[NC];
+#pragma unroll
+                    for (int n = 0; n < NC; ++n) Un[n] = Uo[n] - f.dtdx * (F[n] - Fo[n]);
+                    double* po = out + (long long)o * outs;
+#pragma unroll
+                    for (int n = 0; n < NC; ++n) po[n * B.out.ns] = Un[n];
+                    if (a.ws_max) track_ws(wave_speed<D>(Un, a.k), wsmax, nan_seen);
+                }
+                if (B.flux.p && active) {
+                    const int fo = o + 1;
+                    if (fo >= s0 && (fo < s1 || (fo == s1 && last_seg))) {
+                        double* pf = B.flux.p + floff + (long long)fo * fls;
+#pragma unroll
+                        for (int n = 0; n < NC; ++n) pf[n * B.flux.ns] = F[n];
+                    }
+                }
+#pragma unroll
+                for (int n = 0; n < NC; ++n) Fo[n] = F[n];
+            }
+#pragma unroll
+            for (int n = 0; n < NC; ++n) {
+                URo[n] = UR[n];
+                Uo[n] = Uo1[n];
+                Uo1[n] = U2[n];
+            }
+        }
+    }
+    if (a.ws_max) reduce_ws(wsmax, nan_seen, a.ws_max);
+}
+
+}  // namespace bamrex

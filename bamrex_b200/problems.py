@@ -1,0 +1,94 @@
+"""Seeded initial data for the explicit-path workloads.
+
+Each generator returns the conserved state as a float64 array of shape
+(NC, nz, ny, nx), with cell centres x = prob_lo + (i + 0.5) dx as in the
+reference's problem setups.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+DEFAULT_SEED = 20261203
+
+
+def consv_from_primv(D, q, adiabatic, epsilon=1.0):
+    """Vectorised consv_from_primv (Source/System/Euler/Euler.H:138-165).
+    q: (NC, ...) primitive array (rho, u.., p)."""
+    u = np.empty_like(q)
+    u[0] = q[0]
+    for d in range(D):
+        u[1 + d] = q[0] * q[1 + d]
+    u_sq = q[1] * q[1]
+    for d in range(1, D):
+        u_sq = u_sq + q[1 + d] * q[1 + d]
+    u[1 + D] = q[1 + D] / (adiabatic - 1) + 0.5 * epsilon * q[0] * u_sq
+    return u
+
+
+def sod_1d(n=400, adiabatic=1.4):
+    """1D Sod shock tube on [0,1]: (rho,u,p) = (1,0,1) for x < 0.5, else
+    (0.125,0,0.1) (cell-centre test as Exec/RiemannProblem/Prob.cpp:104-109)."""
+    x = (np.arange(n) + 0.5) / n
+    q = np.zeros((3, 1, 1, n))
+    left = x < 0.5
+    q[0, 0, 0] = np.where(left, 1.0, 0.125)
+    q[2, 0, 0] = np.where(left, 1.0, 0.1)
+    return consv_from_primv(1, q, adiabatic)
+
+
+def quadrant_2d(n=4096, seed=DEFAULT_SEED, adiabatic=1.4, ny=None):
+    """2D four-quadrant Riemann problem on [0,1]^2.  Quadrant states from
+    numpy.random.default_rng(seed), drawn in the order TR, TL, BL, BR, each
+    (rho ~ U[0.1,1.5], u ~ U[-1,1], v ~ U[-1,1], p ~ U[0.03,1.5]); quadrant
+    rule as Exec/QuadrantProblem/Prob.cpp:85-94; then rho *= 1 + 1e-3 N(0,1)
+    per cell from the same stream."""
+    ny = n if ny is None else ny
+    rng = np.random.default_rng(seed)
+    states = {}
+    for name in ("TR", "TL", "BL", "BR"):
+        rho = rng.uniform(0.1, 1.5)
+        u = rng.uniform(-1.0, 1.0)
+        v = rng.uniform(-1.0, 1.0)
+        p = rng.uniform(0.03, 1.5)
+        states[name] = (rho, u, v, p)
+    x = (np.arange(n) + 0.5) / n
+    y = (np.arange(ny) + 0.5) / ny
+    X, Y = np.meshgrid(x, y)
+    q = np.empty((4, 1, ny, n))
+    sel = {
+        "TR": (X > 0.5) & (Y > 0.5),
+        "TL": (X < 0.5) & (Y > 0.5),
+        "BL": (X < 0.5) & (Y < 0.5),
+    }
+    sel["BR"] = ~(sel["TR"] | sel["TL"] | sel["BL"])
+    for name, m in sel.items():
+        for c in range(4):
+            q[c, 0][m] = states[name][c]
+    q[0, 0] *= 1.0 + 1e-3 * rng.standard_normal((ny, n))
+    return consv_from_primv(2, q, adiabatic)
+
+
+def blast_3d(n=256, adiabatic=1.4, radius=0.2, centre=(0.5, 0.5, 0.5)):
+    """3D spherical blast on [0,1]^3: rho = 1, u = 0, p = 10 for r < radius
+    around the centre, else 0.1 (radial rule as
+    Exec/CylindricalExplosion/Prob.cpp:79-91, centre moved)."""
+    c = (np.arange(n) + 0.5) / n
+    Z, Y, X = np.meshgrid(c, c, c, indexing="ij")
+    r2 = (X - centre[0]) ** 2 + (Y - centre[1]) ** 2 + (Z - centre[2]) ** 2
+    q = np.zeros((5, n, n, n))
+    q[0] = 1.0
+    q[4] = np.where(r2 < radius * radius, 10.0, 0.1)
+    return consv_from_primv(3, q, adiabatic)
+
+
+def random_states(D, shape, seed=DEFAULT_SEED, adiabatic=1.4):
+    """Random cells as Profiling/explicit_scaling.cpp:220-260: rho, p in
+    [1,2], velocities in [-1,1] (our own seeded stream)."""
+    rng = np.random.default_rng(seed)
+    nz, ny, nx = shape
+    q = np.empty((D + 2, nz, ny, nx))
+    q[0] = rng.uniform(1.0, 2.0, (nz, ny, nx))
+    for d in range(D):
+        q[1 + d] = rng.uniform(-1.0, 1.0, (nz, ny, nx))
+    q[1 + D] = rng.uniform(1.0, 2.0, (nz, ny, nx))
+    return consv_from_primv(D, q, adiabatic)

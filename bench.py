@@ -1,0 +1,397 @@
+#!/usr/bin/env python
+"""Throughput of the explicit finite-volume path on B200.
+
+Workload (one "step" = one full split time step, x sweep then y sweep, of
+the whole grid, with the device-side CFL reduction and dt update):
+2D four-quadrant Riemann problem, 4096 x 4096 cells on [0,1]^2, gamma 1.4,
+seeded quadrant states (rho ~ U[0.1,1.5], u,v ~ U[-1,1], p ~ U[0.03,1.5])
+with a 1e-3 relative white-noise density perturbation, MUSCL-Hancock with
+the minbee limiter + HLLC, CFL 0.8, transmissive boundaries, FP64.
+
+Prints one JSON line (rank 0).  ``--impl reference`` times the CPU
+restatement of the reference path (oracle/, the reference itself cannot be
+built without AMReX) on the host cores instead.
+"""
+from __future__ import annotations
+
+import argparse
+import datetime
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "cell-updates/s"
+NC2D = 4
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=4096, help="cells per side")
+    ap.add_argument("--max-grid-size", type=int, default=0, help="box size (0: one box per rank)")
+    ap.add_argument("--graph", type=int, default=0, help="1: time the CUDA-graph replay instead")
+    ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    return ap.parse_args()
+
+
+def workload_config(n, boxes, mgs, extra=None):
+    cfg = {
+        "workload": "2D four-quadrant Riemann problem %dx%d, MUSCL-Hancock/minbee + HLLC, CFL 0.8, transmissive, "
+                    "FP64, 1 step = x sweep + y sweep + CFL/dt" % (n, n),
+        "cells": n * n,
+        "boxes": boxes,
+        "max_grid_size": mgs,
+        "l2": "inputs larger than L2: %.0f MB state per buffer > 126 MB" % (NC2D * 8 * n * n / 1e6),
+        "seed": 20261203,
+    }
+    if extra:
+        cfg.update(extra)
+    return cfg
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons, sampled while running."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index, interval_ms=50):
+        self.index, self.interval_ms = index, interval_ms
+        self.proc, self.lines, self.marks = None, [], []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", str(self.interval_ms)],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append((time.time(), ln.strip()))
+
+    def mark(self, name):
+        self.marks.append((name, time.time()))
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self, t0, t1):
+        rows = []
+        for ts, ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                rows.append((ts, float(f[1]), float(f[2]), f))
+            except ValueError:
+                continue
+        inside = [r for r in rows if t0 <= r[0] <= t1]
+        window = "timed region"
+        if not inside:
+            inside = rows
+            window = "whole run (no sample fell inside the timed region)"
+        if not inside:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for _, _, _, f in inside:
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(r[1] for r in inside), "sm_max_mhz": max(r[2] for r in inside),
+                "reasons": sorted(reasons), "samples": len(inside), "window": window}
+
+
+# ------------------------------------------------------------------ helpers
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profiled_traffic(kind):
+    """DRAM bytes per cell per sweep launch from the committed ncu summary
+    (profiles/sweep_*.md, line 'dram_bytes_per_cell_<kind>: X'), or None."""
+    pdir = os.path.join(ROOT, "profiles")
+    if not os.path.isdir(pdir):
+        return None
+    for fn in sorted(os.listdir(pdir)):
+        if not fn.endswith(".md"):
+            continue
+        m = re.search(r"dram_bytes_per_cell_%s:\s*([0-9.]+)" % kind, open(os.path.join(pdir, fn)).read())
+        if m:
+            return float(m.group(1))
+    return None
+
+
+def cpu_baseline_run(n_full, seconds, warm_steps=0, fixed_steps=None):
+    """Time the CPU restatement (oracle/, optimised build, all host threads)
+    on the same workload with the reference's 64x64 boxes.  The sample is
+    the full grid when one step fits the time budget, else a smaller square
+    grid of the same problem.  Returns a dict (value in cell-updates/s)."""
+    import numpy as np
+
+    from bamrex_b200 import problems
+    from oracle import oracle as o
+
+    threads = o.num_threads(fast=True)
+
+    def setup(n):
+        hi = (n - 1, n - 1, 0)
+        boxes = o.decompose(2, (0, 0, 0), hi, 64)
+        lay = o.LevelLayout(2, (0, 0, 0), hi, boxes, 2, [1.0 / n, 1.0 / n])
+        S1, S2 = lay.alloc(), lay.alloc()
+        lay.scatter(S1, problems.quadrant_2d(n))
+        lay.fill_boundary(S1, fast=True)
+        return lay, S1, S2
+
+    parm = o.Parm(2, limiter=o.MINBEE)
+
+    def step(lay, S1, S2, t, dt):
+        S2[:] = S1
+        lay.advance_explicit(S1, S2, t, dt, o.MUSCL_HANCOCK, parm, fast=True)
+        lay.fill_boundary(S1, fast=True)
+        return lay.est_time_step(S1, 1.4, 1.0, 0.8, fast=True)
+
+    # calibrate on 512^2
+    lay, S1, S2 = setup(512)
+    dt = lay.est_time_step(S1, 1.4, 1.0, 0.8, fast=True)
+    t0 = time.perf_counter()
+    dt = step(lay, S1, S2, 0.0, dt)
+    rate = 512 * 512 / (time.perf_counter() - t0)
+    steps_wanted = fixed_steps if fixed_steps is not None else None
+    n = n_full
+    total = steps_wanted + warm_steps if steps_wanted else 1
+    while n > 512 and total * n * n / rate > seconds:
+        n //= 2
+    lay, S1, S2 = setup(n)
+    dt = lay.est_time_step(S1, 1.4, 1.0, 0.8, fast=True)
+    t = 0.0
+    for _ in range(warm_steps):
+        dt_new = step(lay, S1, S2, t, dt)
+        t += dt
+        dt = dt_new
+    steps = 0
+    t0 = time.perf_counter()
+    while True:
+        dt_new = step(lay, S1, S2, t, dt)
+        t += dt
+        dt = dt_new
+        steps += 1
+        el = time.perf_counter() - t0
+        if fixed_steps is not None:
+            if steps >= fixed_steps:
+                break
+        elif el >= seconds or steps >= 50:
+            break
+    el = time.perf_counter() - t0
+    value = n * n * steps / el
+    return {"value": value, "unit": METRIC, "cores": threads, "kind": "port", "elapsed_s": el, "steps": steps,
+            "n": n,
+            "sample": "%d step(s) of the same 2D quadrant problem at %dx%d (64x64 boxes, the reference's "
+                      "max_grid_size), CPU restatement of the reference path, -O3 -march=x86-64-v3, OpenMP over "
+                      "boxes, %d threads" % (steps, n, n, threads)}
+
+
+# ------------------------------------------------------------------ arms
+def run_reference(args, rank, world):
+    if rank != 0:
+        return 0
+    r = cpu_baseline_run(args.n, seconds=120.0, warm_steps=args.warmup, fixed_steps=args.steps)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": r["value"], "unit": METRIC, "n_gpus": args.gpus,
+        "steps": r["steps"], "warmup": args.warmup, "ms_per_step": 1e3 * r["elapsed_s"] / r["steps"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded four-quadrant initial state)",
+        "config": workload_config(args.n, None, 64, {"sample_n": r["n"], "threads": r["cores"]}),
+        "cpu_baseline": {"value": r["value"], "unit": METRIC, "cores": r["cores"], "kind": r["kind"],
+                         "sample": r["sample"]},
+        "e2e": {"value": r["value"], "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "the reference needs the AMReX library (not available offline), so its CPU path runs as the "
+                "line-by-line restatement in oracle/",
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args, rank, world, local_rank):
+    import numpy as np
+    import torch
+
+    import bamrex_b200 as bx
+    from bamrex_b200 import problems
+
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+    torch.cuda.set_device(local_rank)
+    dev_index = torch.cuda.current_device()
+    n = args.n
+    D = 2
+    hi = (n - 1, n - 1, 0)
+    mgs = args.max_grid_size if args.max_grid_size > 0 else n
+    boxes = bx.decompose(D, (0, 0, 0), hi, mgs)
+    u0 = problems.quadrant_2d(n)
+    stream = torch.cuda.Stream()
+    lev = bx.Level(D, (0, 0, 0), hi, [0.0, 0.0], [1.0, 1.0], boxes, bx.Parm(D, limiter=bx.MINBEE),
+                   method=bx.MUSCL_HANCOCK, cfl=0.8, stream=stream)
+    lev.set_state(u0)
+    use_graph = bool(args.graph)
+
+    # warm-up (also builds the CUDA graphs)
+    lev.run(args.warmup, use_graph=use_graph)
+    lev.run(1, use_graph=not use_graph)
+    lev.set_state(u0)
+
+    clocks = ClockSampler(dev_index)
+    clocks.start()
+    time.sleep(0.3)
+    lev.set_timing(not use_graph)
+    lev.reset_counters()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t_wall0 = time.time()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        ev0.record(stream)
+        lev.run_async(args.steps, use_graph=use_graph)
+        ev1.record(stream)
+    t_end, steps_done = lev.run_wait()
+    torch.cuda.synchronize()
+    t_wall1 = time.time()
+    if dist:
+        dist.barrier()
+    ms = ev0.elapsed_time(ev1)
+    launches, sweep_ms, sweep_launches = lev.counters()
+    lev.set_timing(False)
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    assert steps_done == args.steps, (steps_done, args.steps)
+
+    # e2e through the public API with host buffers: per step the state goes
+    # host -> device, one advance + estTimeStep, device -> host.
+    pk = lev.packing
+    host = torch.empty(pk.size, dtype=torch.float64, pin_memory=True)
+    host.numpy()[:] = pk.pack(u0)
+    hptr = host.data_ptr()
+    dt = lev.estTimeStep()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t_e0 = time.time()
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+        tsim = 0.0
+        for _ in range(args.e2e_steps):
+            lev.copy_in_ptr(hptr)
+            lev.advance(tsim, dt)
+            tsim += dt
+            dt = lev.estTimeStep()
+            lev.copy_out_ptr(hptr)
+        e1.record(stream)
+    lev.sync()
+    t_e1 = time.time()
+    e2e_ms = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    clocks.stop()
+    lev.close()
+
+    cells = n * n
+    value = world * cells * args.steps / (ms / 1e3)
+    e2e_value = world * cells * args.e2e_steps / (e2e_ms / 1e3)
+    state_bytes = NC2D * 8 * cells
+
+    roofline = None
+    if sweep_launches:
+        peak, peak_kind = measured_peaks()
+        per_launch_s = (sweep_ms / sweep_launches) / 1e3
+        alg_bytes = 2 * NC2D * 8 * cells  # read U once + write U once per sweep
+        achieved = alg_bytes / per_launch_s / 1e9
+        traffic = profiled_traffic("mhm2d")
+        roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                    "traffic": (traffic * cells) if traffic else None,
+                    "kernel": "sweep_x_kernel<2,MUSCL> + sweep_s_kernel<2,1,MUSCL> (both sweeps, averaged)",
+                    "algorithmic_bytes_per_launch": alg_bytes, "avg_launch_ms": per_launch_s * 1e3,
+                    "sweep_share_of_step": sweep_ms / ms if ms > 0 else None,
+                    "peak_source": "%s (MEASURED_PEAKS.json hbm_gbs)" % peak_kind if peak_kind == "measured"
+                    else "fallback 6650 GB/s"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        r = cpu_baseline_run(n, args.cpu_seconds)
+        cpu = {k: r[k] for k in ("value", "unit", "cores", "kind", "sample")}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (seeded four-quadrant initial state, generated on the host)",
+        "config": workload_config(n, len(boxes), mgs, {"graph_replay": use_graph,
+                                                        "parallelism": "replicas" if world > 1 else "single"}),
+        "roofline": roofline,
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": state_bytes,
+                "d2h_bytes_per_step": state_bytes + 8,
+                "path": "bamrex_level_copy_in (pinned host) + bamrex_level_advance + bamrex_level_est_time_step + "
+                        "bamrex_level_copy_out per step", "steps": args.e2e_steps},
+        "gpu_launches": launches,
+        "clocks": clocks.summary(t_wall0, t_wall1),
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        try:
+            return run_ours(args, rank, world, local_rank)
+        finally:
+            dist.destroy_process_group()
+    return run_ours(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,250 @@
+/*
+ * bamrex_cuda.h -- C ABI of libbamrex_cuda.so, the B200 (sm_100a) explicit
+ * finite-volume path of BAMReX: MUSCL-Hancock reconstruction with half-step
+ * evolution, HLLC / SLIC(FORCE) / FORCE / Lax-Friedrichs interface fluxes,
+ * the split conservative update, boundary/ghost fill and the CFL reduction.
+ *
+ * Plain C types only: device pointers are `double *`, streams are `void *`
+ * (a cudaStream_t; NULL = the legacy default stream).  Every entry point
+ * returns an int status (BAMREX_OK = 0) and never throws; a human-readable
+ * message for the last failure on the calling thread is available from
+ * bamrex_last_error().  Reference citations are paths inside the BAMReX tree.
+ */
+#ifndef BAMREX_CUDA_H_
+#define BAMREX_CUDA_H_
+
+#if defined(__GNUC__)
+#define BAMREX_API __attribute__((visibility("default")))
+#else
+#define BAMREX_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BAMREX_ABI_VERSION 1
+/* MAX_NCOMP = PUInd::size (Source/System/Parm.H:9) */
+#define BAMREX_MAX_NCOMP 8
+
+/* ---- status codes (the reference aborts instead: amrex::Abort / AMREX_ASSERT,
+ *      Source/AmrLevelAdv_advance.cpp:133-137, 182-185) ---- */
+enum {
+    BAMREX_OK = 0,
+    BAMREX_ERR_ARG = 1,         /* bad argument, box/fab geometry or layout */
+    BAMREX_ERR_OOM = 2,         /* device or host allocation failed */
+    BAMREX_ERR_NAN = 3,         /* non-finite wave speed / time step */
+    BAMREX_ERR_TIMEOUT = 4,     /* a bounded device wait gave up */
+    BAMREX_ERR_CUDA = 5,        /* a CUDA runtime call failed */
+    BAMREX_ERR_UNSUPPORTED = 6  /* method/option not provided by this build */
+};
+
+/* ---- numerical method, same values as NumericalMethods::Method
+ *      (Source/NumericalMethods.H:10-19) ---- */
+enum {
+    BAMREX_MUSCL_HANCOCK = 0,
+    BAMREX_HLLC = 1,
+    BAMREX_IMEX = 2, /* not on this path: BAMREX_ERR_UNSUPPORTED */
+    BAMREX_RCM = 3,  /* not on this path: BAMREX_ERR_UNSUPPORTED */
+    BAMREX_SLIC = 4,
+    BAMREX_FORCE = 5,
+    BAMREX_LAX_FRIEDRICHS = 6
+};
+
+/* ---- slope limiter, AMREX_ENUM(Limiter, ...) order (Source/Fluxes/Limiters.H:13) ---- */
+enum { BAMREX_MINBEE = 0, BAMREX_VAN_LEER = 1, BAMREX_VAN_ALBADA = 2, BAMREX_SUPERBEE = 3 };
+
+/* ---- domain boundary kind (BAMReXBCType; Source/BoundaryConditions/BCs.cpp:226-266):
+ *      transmissive = foextrap, periodic = int_dir, reflective = reflect_even
+ *      with reflect_odd on the normal momentum ---- */
+enum { BAMREX_BC_TRANSMISSIVE = 0, BAMREX_BC_PERIODIC = 1, BAMREX_BC_REFLECTIVE = 2 };
+
+/* amrex::Box: cell-centred, inclusive lo/hi; unused dimensions are 0..0. */
+typedef struct bamrex_box {
+    int lo[3];
+    int hi[3];
+} bamrex_box;
+
+/* amrex::Array4<Real>: element (i,j,k,n) lives at
+ * p[(i-begin[0]) + (j-begin[1])*jstride + (k-begin[2])*kstride + n*nstride];
+ * end[] is exclusive.  p is a device pointer. */
+typedef struct bamrex_array4 {
+    double *p;
+    long long jstride;
+    long long kstride;
+    long long nstride;
+    int begin[3];
+    int end[3];
+    int ncomp;
+} bamrex_array4;
+
+/* Parm POD (Source/System/Parm.H:14-61), field for field. */
+typedef struct bamrex_parm {
+    double adiabatic;
+    double eos_mu;
+    double Pr;
+    double beta;
+    double eta_prime;
+    double T_prime;
+    double S_eta;
+    double epsilon;
+    double Re;
+    double R_spec;
+    double cv;
+    double cp;
+    double adia[9];
+    double Reinv;
+    int limiter;
+    unsigned int limiter_indices[BAMREX_MAX_NCOMP];
+    unsigned char limit_on_primv[BAMREX_MAX_NCOMP];
+    unsigned char need_primitive_for_limiting;
+} bamrex_parm;
+
+/* Library identity and errors. */
+BAMREX_API int bamrex_abi_version(void);
+BAMREX_API const char *bamrex_last_error(void);
+BAMREX_API const char *bamrex_status_string(int status);
+
+/* FluidSystem::set_parm_defaults (Source/System/FluidSystem.cpp:52-71) for a
+ * spacedim-dimensional fluid (limiting variable = energy, UInd::E = 1+D). */
+BAMREX_API int bamrex_parm_set_defaults(bamrex_parm *parm, int spacedim);
+/* FluidSystem::init_parm (Source/System/FluidSystem.cpp:73-101): derived
+ * quantities adia[], R_spec, cv, cp, Reinv, need_primitive_for_limiting. */
+BAMREX_API int bamrex_parm_init(bamrex_parm *parm);
+
+/* ------------------------------------------------------------------ */
+/* Per-box flux and update (the Fluxes.H call surface)                 */
+/* ------------------------------------------------------------------ */
+
+/* compute_{MUSCL_hancock,HLLC,SLIC,force,LF}_flux(int dir, Real time,
+ * const Box& bx, const Array4<Real>& flux, const Array4<const Real>& consv,
+ * GpuArray<Real,D> const& dx, Real dt, const System*, const Parm* h_parm,
+ * const Parm* d_parm)  -- Source/Fluxes/Fluxes.H:35-56, 98-119, 131-152,
+ * 206-227, 237-257.  Selected by method (BAMREX_MUSCL_HANCOCK, BAMREX_HLLC,
+ * BAMREX_SLIC, BAMREX_FORCE, BAMREX_LAX_FRIEDRICHS).
+ * bx: the valid box; flux must cover surroundingNodes(bx, dir); consv must
+ * cover bx grown by 2 (MUSCL-Hancock, SLIC) or 1 (first-order methods) in dir.
+ * Asynchronous on `stream`. */
+BAMREX_API int bamrex_compute_flux(int method, int dir, int spacedim, double time, const bamrex_box *bx,
+                        bamrex_array4 flux, bamrex_array4 consv, const double dx[3], double dt,
+                        const bamrex_parm *parm, void *stream);
+
+/* compute_HLLC_flux_LR / compute_force_flux_LR with separate left/right
+ * arrays (Source/Fluxes/Fluxes.H:79-87, 179-187): the face between i-1 and
+ * i takes consv_L at i-1 and consv_R at i.  kind: BAMREX_HLLC or BAMREX_FORCE. */
+BAMREX_API int bamrex_compute_flux_LR(int kind, int dir, int spacedim, double time, const bamrex_box *bx,
+                           bamrex_array4 flux, bamrex_array4 consv_L, bamrex_array4 consv_R,
+                           const double dx[3], double dt, const bamrex_parm *parm, void *stream);
+
+/* The per-sweep conservative update of AmrLevelAdv::advance_explicit
+ * (Source/AmrLevelAdv_advance.cpp:330-341):
+ * Uout(i) = Uin(i) - (dt/dx[dir]) * (flux(i+1) - flux(i)) on bx. */
+BAMREX_API int bamrex_sweep_update(int dir, int spacedim, const bamrex_box *bx, bamrex_array4 Uout,
+                        bamrex_array4 Uin, bamrex_array4 flux, const double dx[3], double dt,
+                        void *stream);
+
+/* Unsplit conservative_update(bx, statein, fx, fy, fz, stateout, dt, idx)
+ * (Source/Fluxes/Update.H:99-130); fluxes[d] for d < spacedim. */
+BAMREX_API int bamrex_conservative_update(int spacedim, const bamrex_box *bx, bamrex_array4 out,
+                               bamrex_array4 in, const bamrex_array4 *fluxes, double dt,
+                               const double idx[3], void *stream);
+
+/* Fused per-box sweep: the flux of `method` in direction dir and the sweep
+ * update in one kernel (compute_*_flux + AmrLevelAdv_advance.cpp:330-341).
+ * If flux.p is non-NULL the face fluxes are also written (reflux input). */
+BAMREX_API int bamrex_sweep_box(int method, int dir, int spacedim, const bamrex_box *bx, bamrex_array4 Uout,
+                     bamrex_array4 Uin, bamrex_array4 flux, const double dx[3], double dt,
+                     const bamrex_parm *parm, void *stream);
+
+/* ------------------------------------------------------------------ */
+/* Level: every box of one AMR level in one device box table            */
+/* ------------------------------------------------------------------ */
+
+typedef struct bamrex_level bamrex_level;
+
+typedef struct bamrex_level_desc {
+    int spacedim;           /* 1, 2 or 3 */
+    bamrex_box domain;      /* the level's index domain (Geometry::Domain) */
+    double prob_lo[3];
+    double prob_hi[3];
+    int bc_lo[3];           /* BAMREX_BC_* per direction */
+    int bc_hi[3];
+    const bamrex_box *boxes; /* the level's BoxArray (disjoint, inside domain) */
+    int nboxes;
+    int ngrow;              /* ghost width of the state fabs, >= 2 (NUM_GROW) */
+    int method;             /* BAMREX_MUSCL_HANCOCK ... (adv.num_method) */
+    double cfl;             /* adv.cfl */
+    bamrex_parm parm;
+    int x_segment;          /* cells per warp item in x; 0 = automatic */
+    int s_segment;          /* cells per thread item in y/z; 0 = automatic */
+} bamrex_level_desc;
+
+/* Build the level: allocates the state fabs (two time-level buffers with
+ * ghost cells, 256-byte aligned rows), the device box table, ghost-fill
+ * tables and a small scalar block, all at creation (no allocation per step).
+ * Work is issued on `stream`. */
+BAMREX_API int bamrex_level_create(bamrex_level **out, const bamrex_level_desc *desc, void *stream);
+BAMREX_API int bamrex_level_destroy(bamrex_level *level);
+BAMREX_API const char *bamrex_level_last_error(const bamrex_level *level);
+
+/* Number of valid cells, and the Array4 of box b of the current state. */
+BAMREX_API long long bamrex_level_num_cells(const bamrex_level *level);
+BAMREX_API int bamrex_level_fab(const bamrex_level *level, int box, bamrex_array4 *out);
+
+/* Copy the valid cells of every box in from / out to a packed buffer
+ * (box-major; inside a box component-slowest, i-fastest; NCOMP*num_cells
+ * doubles).  `src`/`dst` may be host (pinned or pageable) or device memory. */
+BAMREX_API int bamrex_level_copy_in(bamrex_level *level, const double *src);
+BAMREX_API int bamrex_level_copy_out(bamrex_level *level, double *dst);
+
+/* Wait for all work the level issued on its stream. */
+BAMREX_API int bamrex_level_sync(bamrex_level *level);
+
+/* bamrexBCData::fill_consv_boundary on the current state
+ * (Source/BoundaryConditions/BCs.cpp:429-442): inter-box ghosts and
+ * transmissive / periodic / reflective domain ghosts (all directions). */
+BAMREX_API int bamrex_level_fill_boundary(bamrex_level *level);
+
+/* AmrLevelAdv::advance(time, dt, iteration, ncycle) for the explicit methods
+ * (Source/AmrLevelAdv.H:110-111, Source/AmrLevelAdv_advance.cpp:21-259,
+ * 261-439): ghost fill, one split sweep per direction in x, y, z order with a
+ * ghost fill after each, the result becoming the current state.  The
+ * max wave speed of the new state is reduced inside the last sweep.
+ * Asynchronous; returns the dt used in *dt_out (may be NULL). */
+BAMREX_API int bamrex_level_advance(bamrex_level *level, double time, double dt, int iteration, int ncycle,
+                         double *dt_out);
+
+/* AmrLevelAdv::estTimeStep (Source/AmrLevelAdv.cpp:395-477) on the current
+ * state: cfl * min_d dx_d / max(|u| + c).  Synchronises the stream. */
+BAMREX_API int bamrex_level_est_time_step(bamrex_level *level, double *dt_est);
+
+/* The coarse-step loop of a single-level run (Amr::coarseTimeStep with
+ * AmrLevelAdv::computeInitialDt / computeNewDt, Source/AmrLevelAdv.cpp:487-619):
+ * up to nsteps steps, dt computed on the device after every step with the
+ * stop-time clamp (stop_time < 0 disables it; steps stop once time reaches
+ * it).  With use_graph != 0 one step is captured as a CUDA graph and
+ * replayed.  On return (stream synchronised) *time_io holds the new time and
+ * *steps_done the number of steps taken.  *time_io is the start time on entry. */
+BAMREX_API int bamrex_level_run(bamrex_level *level, int nsteps, double stop_time, int use_graph, double *time_io,
+                     int *steps_done);
+
+/* The same loop split in two: bamrex_level_run_async issues the steps and
+ * returns at once (no host synchronisation); bamrex_level_run_wait
+ * synchronises the stream and reports the time and steps taken.  Between
+ * the two calls the caller may record its own events on the level's stream. */
+BAMREX_API int bamrex_level_run_async(bamrex_level *level, int nsteps, double stop_time, int use_graph,
+                                      double start_time);
+BAMREX_API int bamrex_level_run_wait(bamrex_level *level, double *time_out, int *steps_done);
+
+/* Kernel accounting for measurement: kernels launched by the level since
+ * creation / the last reset, and (when timing is enabled) the summed
+ * CUDA-event time of the sweep kernels and their count. */
+BAMREX_API int bamrex_level_set_timing(bamrex_level *level, int enable);
+BAMREX_API int bamrex_level_counters(bamrex_level *level, long long *launches, double *sweep_ms, long long *sweep_launches);
+BAMREX_API int bamrex_level_reset_counters(bamrex_level *level);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BAMREX_CUDA_H_ */

@@ -134,6 +134,7 @@ SIGNATURES = {
     "bamrex_level_set_timing": (_i, [_vp, _i]),
     "bamrex_level_counters": (_i, [_vp, ctypes.POINTER(_ll), _dp, ctypes.POINTER(_ll)]),
     "bamrex_level_reset_counters": (_i, [_vp]),
+    "bamrex_level_sweep_times": (_i, [_vp, _dp, ctypes.POINTER(_ll)]),
 }
 
 _LIB = None

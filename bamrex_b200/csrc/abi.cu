@@ -78,7 +78,10 @@ int make_consts(const bamrex_parm* p, int D, Consts& k)
         k.root_k = (int)kr;
         k.root_dpos = k.inv_z - kr;
         k.root_dneg = (double)(1.0L / (long double)kr - (long double)k.z);
+        k.root_dneg_l2 = (double)((1.0L / (long double)kr - (long double)k.z) * 0.69314718055994530942L);
+        k.root_dpos_l2 = (double)(((long double)k.inv_z - (long double)kr) * 0.69314718055994530942L);
     }
+    k.half_eps = 0.5 * eps;
     k.limiter = p->limiter;
     const int NC = D + 2;
     bool uniform = true, need_prim = false;
@@ -449,9 +452,12 @@ struct bamrex_level {
     long long launches = 0;
     bool timing = false;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> events;
+    std::vector<int> event_dir;
     size_t ev_used = 0;
     double sweep_ms = 0.0;
     long long sweep_launches = 0;
+    double dir_ms[3] = { 0, 0, 0 };
+    long long dir_launches[3] = { 0, 0, 0 };
 
     cudaGraphExec_t graph[2] = { nullptr, nullptr };
     bool run_pending = false;
@@ -683,6 +689,7 @@ int level_sweep(bamrex_level* L, int d, int parity, double dt_host, const StepSc
     if (rc != BAMREX_OK) return rc;
     if (t) {
         cudaEventRecord(L->events[L->ev_used].second, L->stream);
+        L->event_dir[L->ev_used] = d;
         L->ev_used++;
     }
     return BAMREX_OK;
@@ -802,7 +809,7 @@ extern "C" int bamrex_level_create(bamrex_level** out, const bamrex_level_desc* 
     for (int d = 0; d < D; ++d) {
         L->seglen[d] = d == 0 ? desc->x_segment : desc->s_segment;
         if (L->seglen[d] <= 0)
-            L->seglen[d] = choose_seglen(d, L->boxes, sweep_resident_warps(D, d, L->method));
+            L->seglen[d] = choose_seglen(d, L->boxes, sweep_resident_warps(D, d, L->method, L->k));
         if (d == 0) L->seglen[d] = (int)align_up((size_t)L->seglen[d], 32);
         long long acc = 0;
         for (int b = 0; b < nb; ++b) {
@@ -1140,6 +1147,7 @@ extern "C" int bamrex_level_set_timing(bamrex_level* L, int enable)
     L->timing = enable != 0;
     if (L->timing && L->events.empty()) {
         L->events.resize(8192);
+        L->event_dir.assign(8192, 0);
         for (auto& ev : L->events) {
             if (cudaEventCreate(&ev.first) != cudaSuccess || cudaEventCreate(&ev.second) != cudaSuccess)
                 return L->set_err(fail(BAMREX_ERR_CUDA, "cudaEventCreate failed"));
@@ -1149,23 +1157,41 @@ extern "C" int bamrex_level_set_timing(bamrex_level* L, int enable)
     return BAMREX_OK;
 }
 
+static int collect_events(bamrex_level* L)
+{
+    if (!L->ev_used) return BAMREX_OK;
+    const cudaError_t e = cudaStreamSynchronize(L->stream);
+    if (e != cudaSuccess) return L->set_err(cuda_fail(e, "sync"));
+    for (size_t i = 0; i < L->ev_used; ++i) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, L->events[i].first, L->events[i].second);
+        L->sweep_ms += ms;
+        L->dir_ms[L->event_dir[i]] += ms;
+        L->dir_launches[L->event_dir[i]] += 1;
+    }
+    L->sweep_launches += (long long)L->ev_used;
+    L->ev_used = 0;
+    return BAMREX_OK;
+}
+
 extern "C" int bamrex_level_counters(bamrex_level* L, long long* launches, double* sweep_ms, long long* sweep_launches)
 {
     if (!L) return fail(BAMREX_ERR_ARG, "NULL level");
-    if (L->ev_used) {
-        const cudaError_t e = cudaStreamSynchronize(L->stream);
-        if (e != cudaSuccess) return L->set_err(cuda_fail(e, "sync"));
-        for (size_t i = 0; i < L->ev_used; ++i) {
-            float ms = 0.f;
-            cudaEventElapsedTime(&ms, L->events[i].first, L->events[i].second);
-            L->sweep_ms += ms;
-        }
-        L->sweep_launches += (long long)L->ev_used;
-        L->ev_used = 0;
-    }
+    BX_TRY(collect_events(L));
     if (launches) *launches = L->launches;
     if (sweep_ms) *sweep_ms = L->sweep_ms;
     if (sweep_launches) *sweep_launches = L->sweep_launches;
+    return BAMREX_OK;
+}
+
+extern "C" int bamrex_level_sweep_times(bamrex_level* L, double* ms_by_dir, long long* launches_by_dir)
+{
+    if (!L || !ms_by_dir || !launches_by_dir) return fail(BAMREX_ERR_ARG, "NULL argument");
+    BX_TRY(collect_events(L));
+    for (int d = 0; d < 3; ++d) {
+        ms_by_dir[d] = L->dir_ms[d];
+        launches_by_dir[d] = L->dir_launches[d];
+    }
     return BAMREX_OK;
 }
 
@@ -1177,5 +1203,9 @@ extern "C" int bamrex_level_reset_counters(bamrex_level* L)
     L->ev_used = 0;
     L->sweep_ms = 0.0;
     L->sweep_launches = 0;
+    for (int d = 0; d < 3; ++d) {
+        L->dir_ms[d] = 0.0;
+        L->dir_launches[d] = 0;
+    }
     return BAMREX_OK;
 }

@@ -29,6 +29,9 @@ struct Consts {
     int root_k;
     double root_dneg;
     double root_dpos;
+    double root_dneg_l2;   // root_dneg * ln 2 (applied to log2 x)
+    double root_dpos_l2;   // root_dpos * ln 2
+    double half_eps;       // 0.5 * epsilon
     int limiter;        // BAMREX_MINBEE ..
     // Limiting variable per component (Parm::limiter_indices /
     // limit_on_primv, Source/Fluxes/CalcLimitingVal.H:9-22).  uniform_var >= 0

@@ -210,8 +210,10 @@ __global__ void sweep_update_kernel(const UpdateArgs u)
         const double* pf0 = fl.p + fab_index(fl, i, j, k);
         const double* pf1 = fl.p + fab_index(fl, i + (DIR == 0), j + (DIR == 1), k + (DIR == 2));
         double* po = u.out.p + fab_index(u.out, i, j, k);
+        // explicit rounding of the product: no FMA contraction, so the
+        // stand-alone update rounds exactly as the scalar reference does
         for (int n = 0; n < NC; ++n)
-            po[n * u.out.ns] = pin[n * u.in.ns] - u.dtdx[0] * (pf1[n * fl.ns] - pf0[n * fl.ns]);
+            po[n * u.out.ns] = pin[n * u.in.ns] - __dmul_rn(u.dtdx[0], pf1[n * fl.ns] - pf0[n * fl.ns]);
     }
 }
 
@@ -236,7 +238,7 @@ __global__ void cons_update_kernel(const UpdateArgs u)
                 const FabDev& f = u.flux[d];
                 const double a = f.p[fab_index(f, i + (d == 0), j + (d == 1), k + (d == 2)) + n * f.ns];
                 const double b = f.p[fab_index(f, i, j, k) + n * f.ns];
-                v = v - u.dtdx[d] * (a - b);
+                v = v - __dmul_rn(u.dtdx[d], a - b);
             }
             po[n * u.out.ns] = v;
         }

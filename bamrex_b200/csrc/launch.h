@@ -38,7 +38,11 @@ cudaError_t launch_sweep(int D, int dir, int method, const SweepArgs& a, cudaStr
 
 // Warps of the sweep kernel that fit on the device at once (for choosing
 // segment lengths); 0 for an unsupported combination.
-long long sweep_resident_warps(int D, int dir, int method);
+long long sweep_resident_warps(int D, int dir, int method, const Consts& k);
+
+// The fast-path limiter for this configuration (MUSCL-Hancock, energy
+// limiting, gamma with 1/z = 7), or -1 for the general kernels.
+int fast_limiter(int D, int method, const Consts& k);
 
 cudaError_t launch_ghost_fill(int NC, const GhostOp* ops, int nops, long long total_cells, const FabDev* fabs,
                               const StepScalars* scal, cudaStream_t s);

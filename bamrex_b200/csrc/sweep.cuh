@@ -7,15 +7,16 @@
 // table); each warp takes work items from a grid-stride loop.
 //  * x sweep (contiguous direction): an item is a segment of one row.  The
 //    warp marches along the row in 32-cell chunks, lane t holding cell
-//    x0+t; neighbour states come from warp shuffles, and the values of the
-//    previous chunk's top lanes carry the stencil across chunk boundaries.
+//    x0+t; neighbour states come from warp shuffles, and the values of
+//    earlier chunks carry the stencil across chunk boundaries.
 //  * y / z sweeps (strided directions): an item is a group of 32 adjacent
 //    columns x and a segment along the sweep; each thread marches its column
 //    keeping the stencil in registers.  Loads and stores are coalesced
 //    across the warp (32 consecutive doubles per component).
-// Pipeline per position o: load U(o+2); cell stage of cell o+1 (needs
-// U(o..o+2)); face o+1 from UR(o) and UL(o+1); update of cell o from faces o
-// and o+1.
+// Both are software-pipelined: the face stage of an iteration uses cell
+// stages finished in earlier iterations, so the cell stage (reconstruction
+// + half step) and the face stage (Riemann flux) of one iteration are
+// independent instruction streams the scheduler can interleave.
 #pragma once
 
 #include "common.cuh"
@@ -24,6 +25,12 @@
 namespace bamrex {
 
 constexpr int kSweepThreads = 128;
+// Resident 128-thread blocks per SM the sweep kernels are compiled for
+// (register budget 65536 / (128 * blocks)).
+#ifndef BAMREX_SWEEP_MIN_BLOCKS
+#define BAMREX_SWEEP_MIN_BLOCKS 3
+#endif
+constexpr int kSweepMinBlocks = BAMREX_SWEEP_MIN_BLOCKS;
 
 __device__ __forceinline__ int find_box(const SweepBox* boxes, int nboxes, long long item)
 {
@@ -72,6 +79,13 @@ __device__ __forceinline__ void ld_state(const double* __restrict__ p, long long
 }
 
 template <int NC>
+__device__ __forceinline__ void copy_state(const double (&s)[NC], double (&d)[NC])
+{
+#pragma unroll
+    for (int n = 0; n < NC; ++n) d[n] = s[n];
+}
+
+template <int NC>
 __device__ __forceinline__ void shfl_carry(const double (&cur)[NC], const double (&prev)[NC], int lane,
                                            int shift, double (&out)[NC])
 {
@@ -104,10 +118,12 @@ __device__ __forceinline__ void track_ws(double w, double& wsmax, bool& nan_seen
 }
 
 // ------------------------------------------------------------------ x sweep
-template <int D, int METHOD>
-__global__ void __launch_bounds__(kSweepThreads) sweep_x_kernel(const SweepArgs a)
+// Chunk x0, lane t: load A = U(x0+t+2); cell stage of cell x0+t+1; face
+// x0-31+t from the previous chunk's cell stages; update of cell x0-32+t.
+template <int D, int METHOD, int LIM>
+__global__ void __launch_bounds__(kSweepThreads, kSweepMinBlocks) sweep_x_kernel(const SweepArgs a)
 {
-    using S = Scheme<D, 0, METHOD>;
+    using S = Scheme<D, 0, METHOD, LIM>;
     constexpr int NC = D + 2;
     constexpr int H = S::kHalo;
     StepFactors f;
@@ -135,48 +151,55 @@ __global__ void __launch_bounds__(kSweepThreads) sweep_x_kernel(const SweepArgs 
         double* __restrict__ out = B.out.p + (long long)(j - B.out.b1) * B.out.js + (long long)(kk - B.out.b2) * B.out.ks;
         double* __restrict__ fl = B.flux.p ? B.flux.p + (long long)(j - B.flux.b1) * B.flux.js + (long long)(kk - B.flux.b2) * B.flux.ks : nullptr;
 
-        double Ap[NC], URp[NC], Fp[NC];
+        auto load = [&](int x0, double (&u)[NC]) {
+            const int xl = x0 + lane + 2;
+            if (xl >= s0 - H && xl <= s1 - 1 + H) ld_state(in + (xl - B.in.b0), B.in.ns, u);
+            else benign(u);
+        };
+
+        // carried across chunks
+        double Ap[NC];               // previous chunk's loads
+        double ULp[NC], URp[NC];     // previous chunk's cell stages
+        double URpp[NC];             // the chunk before that (its lane 31 is used)
+        double Fp[NC];               // previous chunk's faces (lane 31 used)
+        double Um2p[NC];             // previous chunk's U(x0-32+t)
         benign(Ap);
+        benign(ULp);
         benign(URp);
+        benign(URpp);
+        benign(Um2p);
 #pragma unroll
         for (int n = 0; n < NC; ++n) Fp[n] = 0.0;
 
-        // prefetch the first chunk
         double An[NC];
-        {
-            const int xl = s0 - 32 + lane + 2;
-            if (xl >= s0 - H && xl <= s1 - 1 + H) ld_state(in + (xl - B.in.b0), B.in.ns, An);
-            else benign(An);
-        }
-        for (int x0 = s0 - 32; x0 < s1; x0 += 32) {
+        load(s0 - 32, An);
+        for (int x0 = s0 - 32; x0 < s1 + 32; x0 += 32) {
             double A[NC];
-#pragma unroll
-            for (int n = 0; n < NC; ++n) A[n] = An[n];
-            {
-                const int xl = x0 + 32 + lane + 2;
-                if (x0 + 32 < s1 && xl >= s0 - H && xl <= s1 - 1 + H) ld_state(in + (xl - B.in.b0), B.in.ns, An);
-                else benign(An);
-            }
-            const int o = x0 + lane;
+            copy_state(An, A);
+            load(x0 + 32, An);
+            // cell stage of cell x0+t+1 (this chunk)
             double Um1[NC], Um2[NC];
-            shfl_carry(A, Ap, lane, 1, Um1);  // U(o+1)
-            shfl_carry(A, Ap, lane, 2, Um2);  // U(o)
+            shfl_carry(A, Ap, lane, 1, Um1);  // U(x0+t+1)
+            shfl_carry(A, Ap, lane, 2, Um2);  // U(x0+t)
             double UL[NC], UR[NC];
-            S::cell(Um2, Um1, A, a.k, f.hdtdx, UL, UR);  // cell o+1
-            double URm1[NC];
-            shfl_carry(UR, URp, lane, 1, URm1);  // UR(o)
+            S::cell(Um2, Um1, A, a.k, f.hdtdx, UL, UR);
+            // face x0-31+t from the previous chunk: UR(x0-32+t), UL(x0-31+t)
+            double URf[NC];
+            shfl_carry(URp, URpp, lane, 1, URf);
             double F[NC];
-            S::face(URm1, UL, a.k, f.half_dx_dt, f.dt_2dx, F);  // face o+1
-            double Fm1[NC];
-            shfl_carry(F, Fp, lane, 1, Fm1);  // face o
+            S::face(URf, ULp, a.k, f.half_dx_dt, f.dt_2dx, F);
+            // update of cell o = x0-32+t from faces o and o+1
+            double Fm[NC];
+            shfl_carry(F, Fp, lane, 1, Fm);
+            const int o = x0 - 32 + lane;
             if (a.do_update && o >= s0 && o < s1) {
                 double Un[NC];
 #pragma unroll
-                for (int n = 0; n < NC; ++n) Un[n] = Um2[n] - f.dtdx * (F[n] - Fm1[n]);
+                for (int n = 0; n < NC; ++n) Un[n] = Um2p[n] - f.dtdx * (F[n] - Fm[n]);
                 double* po = out + (o - B.out.b0);
 #pragma unroll
                 for (int n = 0; n < NC; ++n) po[n * B.out.ns] = Un[n];
-                if (a.ws_max) track_ws(wave_speed<D>(Un, a.k), wsmax, nan_seen);
+                if (a.ws_max) track_ws(S::speed(Un, a.k), wsmax, nan_seen);
             }
             if (fl) {
                 const int fo = o + 1;
@@ -186,22 +209,24 @@ __global__ void __launch_bounds__(kSweepThreads) sweep_x_kernel(const SweepArgs 
                     for (int n = 0; n < NC; ++n) pf[n * B.flux.ns] = F[n];
                 }
             }
-#pragma unroll
-            for (int n = 0; n < NC; ++n) {
-                Ap[n] = A[n];
-                URp[n] = UR[n];
-                Fp[n] = F[n];
-            }
+            copy_state(A, Ap);
+            copy_state(URp, URpp);
+            copy_state(UR, URp);
+            copy_state(UL, ULp);
+            copy_state(F, Fp);
+            copy_state(Um2, Um2p);
         }
     }
     if (a.ws_max) reduce_ws(wsmax, nan_seen, a.ws_max);
 }
 
 // ------------------------------------------------------------ y / z sweeps
-template <int D, int DIR, int METHOD>
-__global__ void __launch_bounds__(kSweepThreads) sweep_s_kernel(const SweepArgs a)
+// Iteration o: load U(o+4); cell stage of cell o+2; face o+1 from the cell
+// stages of cells o and o+1 (earlier iterations); update of cell o.
+template <int D, int DIR, int METHOD, int LIM>
+__global__ void __launch_bounds__(kSweepThreads, kSweepMinBlocks) sweep_s_kernel(const SweepArgs a)
 {
-    using S = Scheme<D, DIR, METHOD>;
+    using S = Scheme<D, DIR, METHOD, LIM>;
     constexpr int NC = D + 2;
     constexpr int H = S::kHalo;
     StepFactors f;
@@ -226,7 +251,7 @@ __global__ void __launch_bounds__(kSweepThreads) sweep_s_kernel(const SweepArgs 
         const int s1 = min(s0 + a.seglen, B.hi[DIR] + 1);
         const bool last_seg = (s1 == B.hi[DIR] + 1);
 
-        // column base pointers (position along DIR added per access)
+        // column base offsets (position along DIR added per access)
         long long inoff, outoff, floff = 0;
         long long ins, outs, fls = 0;
         if (DIR == 1) {
@@ -258,51 +283,53 @@ __global__ void __launch_bounds__(kSweepThreads) sweep_s_kernel(const SweepArgs 
             else benign(u);
         };
 
-        double Uo[NC], Uo1[NC], Nx[NC];
-        load(s0 - 2, Uo);
-        load(s0 - 1, Uo1);
-        load(s0, Nx);
-        double URo[NC], Fo[NC];
-        benign(URo);
+        // warm-up: cell stages of cells s0-1 and s0
+        double U0[NC], Ua[NC], Ub[NC], Nx[NC], Xm2[NC];
+        load(s0 - 2, Xm2);
+        load(s0 - 1, U0);
+        load(s0, Ua);
+        load(s0 + 1, Ub);
+        load(s0 + 2, Nx);
+        double URa[NC], URb[NC], ULb[NC], Fo[NC], tmp[NC];
+        S::cell(Xm2, U0, Ua, a.k, f.hdtdx, tmp, URa);   // cell s0-1 -> UR(s0-1)
+        S::cell(U0, Ua, Ub, a.k, f.hdtdx, ULb, URb);    // cell s0   -> UL(s0), UR(s0)
 #pragma unroll
         for (int n = 0; n < NC; ++n) Fo[n] = 0.0;
 
-        for (int o = s0 - 2; o < s1; ++o) {
-            double U2[NC];
+        // invariant at iteration o: U0 = U(o), Ua = U(o+1), Ub = U(o+2),
+        // Nx = U(o+3), URa = UR(o), URb = UR(o+1), ULb = UL(o+1), Fo = F(o)
+        for (int o = s0 - 1; o < s1; ++o) {
+            double U3[NC];
+            copy_state(Nx, U3);
+            load(o + 4, Nx);
+            double UL2[NC], UR2[NC];
+            S::cell(Ua, Ub, U3, a.k, f.hdtdx, UL2, UR2);   // cell o+2
+            double F1[NC];
+            S::face(URa, ULb, a.k, f.half_dx_dt, f.dt_2dx, F1);  // face o+1
+            if (o >= s0 && a.do_update && active) {
+                double Un[NC];
 #pragma unroll
-            for (int n = 0; n < NC; ++n) U2[n] = Nx[n];
-            load(o + 3, Nx);
-            double UL[NC], UR[NC];
-            S::cell(Uo, Uo1, U2, a.k, f.hdtdx, UL, UR);  // cell o+1
-            if (o >= s0 - 1) {
-                double F[NC];
-                S::face(URo, UL, a.k, f.half_dx_dt, f.dt_2dx, F);  // face o+1
-                if (o >= s0 && a.do_update && active) {
-                    double Un[NC];
+                for (int n = 0; n < NC; ++n) Un[n] = U0[n] - f.dtdx * (F1[n] - Fo[n]);
+                double* po = out + (long long)o * outs;
 #pragma unroll
-                    for (int n = 0; n < NC; ++n) Un[n] = Uo[n] - f.dtdx * (F[n] - Fo[n]);
-                    double* po = out + (long long)o * outs;
-#pragma unroll
-                    for (int n = 0; n < NC; ++n) po[n * B.out.ns] = Un[n];
-                    if (a.ws_max) track_ws(wave_speed<D>(Un, a.k), wsmax, nan_seen);
-                }
-                if (B.flux.p && active) {
-                    const int fo = o + 1;
-                    if (fo >= s0 && (fo < s1 || (fo == s1 && last_seg))) {
-                        double* pf = B.flux.p + floff + (long long)fo * fls;
-#pragma unroll
-                        for (int n = 0; n < NC; ++n) pf[n * B.flux.ns] = F[n];
-                    }
-                }
-#pragma unroll
-                for (int n = 0; n < NC; ++n) Fo[n] = F[n];
+                for (int n = 0; n < NC; ++n) po[n * B.out.ns] = Un[n];
+                if (a.ws_max) track_ws(S::speed(Un, a.k), wsmax, nan_seen);
             }
+            if (B.flux.p && active) {
+                const int fo = o + 1;
+                if (fo >= s0 && (fo < s1 || (fo == s1 && last_seg))) {
+                    double* pf = B.flux.p + floff + (long long)fo * fls;
 #pragma unroll
-            for (int n = 0; n < NC; ++n) {
-                URo[n] = UR[n];
-                Uo[n] = Uo1[n];
-                Uo1[n] = U2[n];
+                    for (int n = 0; n < NC; ++n) pf[n * B.flux.ns] = F1[n];
+                }
             }
+            copy_state(F1, Fo);
+            copy_state(Ua, U0);
+            copy_state(Ub, Ua);
+            copy_state(U3, Ub);
+            copy_state(URb, URa);
+            copy_state(UR2, URb);
+            copy_state(UL2, ULb);
         }
     }
     if (a.ws_max) reduce_ws(wsmax, nan_seen, a.ws_max);

@@ -303,3 +303,10 @@ class Level:
 
     def reset_counters(self):
         self._ck(lib().bamrex_level_reset_counters(self._h))
+
+    def sweep_times(self):
+        """Per-direction (ms, launches) of the timed sweep kernels."""
+        ms = (ctypes.c_double * 3)()
+        n = (ctypes.c_longlong * 3)()
+        self._ck(lib().bamrex_level_sweep_times(self._h, ms, n))
+        return [(ms[d], n[d]) for d in range(self.D)]

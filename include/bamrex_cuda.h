@@ -242,6 +242,9 @@ BAMREX_API int bamrex_level_run_wait(bamrex_level *level, double *time_out, int 
 BAMREX_API int bamrex_level_set_timing(bamrex_level *level, int enable);
 BAMREX_API int bamrex_level_counters(bamrex_level *level, long long *launches, double *sweep_ms, long long *sweep_launches);
 BAMREX_API int bamrex_level_reset_counters(bamrex_level *level);
+/* The timed sweep kernels split by direction: summed milliseconds and
+ * launches for x, y, z (arrays of 3). */
+BAMREX_API int bamrex_level_sweep_times(bamrex_level *level, double *ms_by_dir, long long *launches_by_dir);
 
 #ifdef __cplusplus
 }

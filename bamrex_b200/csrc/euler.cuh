@@ -404,12 +404,14 @@ __device__ __forceinline__ void muscl_cell_fast(const double (&Um)[D + 2], const
 {
     constexpr int NC = D + 2;
     constexpr int E = D + 1;
-    const double hphi = 0.5 * limiter_value_fast<LIM>(U0[E] - Um[E], Up[E] - U0[E]);
+    // 0.5 phi delta with delta = 0.5 (U0 - Um) + 0.5 (Up - U0) written as
+    // 0.25 phi (Up - Um) (within an ulp of the reference's rounding)
+    const double qphi = 0.25 * limiter_value_fast<LIM>(U0[E] - Um[E], Up[E] - U0[E]);
 #pragma unroll
     for (int n = 0; n < NC; ++n) {
-        const double delta = 0.5 * (U0[n] - Um[n]) + 0.5 * (Up[n] - U0[n]);
-        UL[n] = U0[n] - hphi * delta;
-        UR[n] = U0[n] + hphi * delta;
+        const double d2 = Up[n] - Um[n];
+        UL[n] = fma(-qphi, d2, U0[n]);
+        UR[n] = fma(qphi, d2, U0[n]);
     }
     double FL[NC], FR[NC];
     phys_flux_fast<D, DIR>(UL, k, FL);

@@ -31,6 +31,21 @@ constexpr int kSweepThreads = 128;
 #define BAMREX_SWEEP_MIN_BLOCKS 3
 #endif
 constexpr int kSweepMinBlocks = BAMREX_SWEEP_MIN_BLOCKS;
+// Unroll factor of the strided march loop.
+#ifndef BAMREX_MARCH_UNROLL
+#define BAMREX_MARCH_UNROLL 1
+#endif
+constexpr int kMarchUnroll = BAMREX_MARCH_UNROLL;
+// Out-of-range positions of the strided march: clamped into the box (1) or
+// replaced by a benign state (0).
+#ifndef BAMREX_CLAMP_LOADS
+#define BAMREX_CLAMP_LOADS 0
+#endif
+constexpr bool kClampLoads = BAMREX_CLAMP_LOADS != 0;
+// x sweep neighbour exchange: warp shuffles (0) or shared-memory rings (1).
+#ifndef BAMREX_X_SMEM
+#define BAMREX_X_SMEM 0
+#endif
 
 __device__ __forceinline__ int find_box(const SweepBox* boxes, int nboxes, long long item)
 {
@@ -119,9 +134,112 @@ __device__ __forceinline__ void track_ws(double w, double& wsmax, bool& nan_seen
 
 // ------------------------------------------------------------------ x sweep
 // Chunk x0, lane t: load A = U(x0+t+2); cell stage of cell x0+t+1; face
-// x0-31+t from the previous chunk's cell stages; update of cell x0-32+t.
+// x0-31+t from the previous chunks' cell stages; update of cell x0-32+t.
+// Neighbour values move between lanes through per-warp shared-memory rings
+// indexed by position (loads over 4 chunks, UR and faces over 2; the UR
+// ring is safe because a __syncwarp separates its reads from its writes),
+// so no lane needs a select on chunk boundaries.
+constexpr int kRingA = 128, kRingR = 64, kRingF = 64;  // powers of two
+
+// ring slot of a position (two's complement AND also wraps negative positions)
+__device__ __forceinline__ int ring(int pos, int n) { return pos & (n - 1); }
+
 template <int D, int METHOD, int LIM>
 __global__ void __launch_bounds__(kSweepThreads, kSweepMinBlocks) sweep_x_kernel(const SweepArgs a)
+{
+    using S = Scheme<D, 0, METHOD, LIM>;
+    constexpr int NC = D + 2;
+    constexpr int H = S::kHalo;
+    __shared__ double sA[kSweepThreads / 32][NC][kRingA];
+    __shared__ double sR[kSweepThreads / 32][NC][kRingR];
+    __shared__ double sF[kSweepThreads / 32][NC][kRingF];
+    StepFactors f;
+    if (!step_factors(a, f)) return;
+    const int lane = threadIdx.x & 31;
+    const int w = threadIdx.x >> 5;
+    const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+    double wsmax = 0.0;
+    bool nan_seen = false;
+
+    for (long long it = gw; it < a.total_items; it += nw) {
+        const int b = a.boxes ? find_box(a.boxes, a.nboxes, it) : 0;
+        const SweepBox& B = a.boxes ? a.boxes[b] : a.one;
+        const long long local = it - B.item_begin;
+        const int seg = (int)(local % B.nseg);
+        const long long row = local / B.nseg;
+        const int ny = B.hi[1] - B.lo[1] + 1;
+        const int j = B.lo[1] + (int)(row % ny);
+        const int kk = B.lo[2] + (int)(row / ny);
+        const int s0 = B.lo[0] + seg * a.seglen;
+        const int s1 = min(s0 + a.seglen, B.hi[0] + 1);
+        const bool last_seg = (s1 == B.hi[0] + 1);
+        const int plo = s0 - H, phi = s1 - 1 + H;  // loadable positions
+
+        const double* __restrict__ in = B.in.p + (long long)(j - B.in.b1) * B.in.js + (long long)(kk - B.in.b2) * B.in.ks - B.in.b0;
+        double* __restrict__ out = B.out.p + (long long)(j - B.out.b1) * B.out.js + (long long)(kk - B.out.b2) * B.out.ks - B.out.b0;
+        double* __restrict__ fl = B.flux.p ? B.flux.p + (long long)(j - B.flux.b1) * B.flux.js + (long long)(kk - B.flux.b2) * B.flux.ks - B.flux.b0 : nullptr;
+
+        double ULp[NC];  // this lane's UL from the previous chunk
+        benign(ULp);
+        double An[NC];
+        ld_state(in + min(max(s0 - 30 + lane, plo), phi), B.in.ns, An);
+        for (int x0 = s0 - 32; x0 < s1 + 32; x0 += 32) {
+            double A[NC];
+            copy_state(An, A);
+            ld_state(in + min(max(x0 + 34 + lane, plo), phi), B.in.ns, An);
+            const int p = x0 + lane;
+#pragma unroll
+            for (int n = 0; n < NC; ++n) sA[w][n][ring(p + 2, kRingA)] = A[n];
+            __syncwarp();
+            double Um1[NC], Um2[NC], URf[NC], Uo[NC];
+#pragma unroll
+            for (int n = 0; n < NC; ++n) {
+                Um1[n] = sA[w][n][ring(p + 1, kRingA)];
+                Um2[n] = sA[w][n][ring(p, kRingA)];
+                Uo[n] = sA[w][n][ring(p - 32, kRingA)];
+                URf[n] = sR[w][n][ring(p - 32, kRingR)];
+            }
+            double UL[NC], UR[NC];
+            S::cell(Um2, Um1, A, a.k, f.hdtdx, UL, UR);               // cell p+1
+            double F[NC];
+            S::face(URf, ULp, a.k, f.half_dx_dt, f.dt_2dx, F);       // face p-31
+#pragma unroll
+            for (int n = 0; n < NC; ++n) sF[w][n][ring(p - 31, kRingF)] = F[n];
+            __syncwarp();
+            double Fm[NC];
+#pragma unroll
+            for (int n = 0; n < NC; ++n) Fm[n] = sF[w][n][ring(p - 32, kRingF)];
+            const int o = p - 32;  // updated cell
+            if (a.do_update && o >= s0 && o < s1) {
+                double Un[NC];
+#pragma unroll
+                for (int n = 0; n < NC; ++n) Un[n] = Uo[n] - f.dtdx * (F[n] - Fm[n]);
+#pragma unroll
+                for (int n = 0; n < NC; ++n) out[o + n * B.out.ns] = Un[n];
+                if (a.ws_max) track_ws(S::speed(Un, a.k), wsmax, nan_seen);
+            }
+            if (fl) {
+                const int fo = o + 1;
+                if (fo >= s0 && (fo < s1 || (fo == s1 && last_seg))) {
+#pragma unroll
+                    for (int n = 0; n < NC; ++n) fl[fo + n * B.flux.ns] = F[n];
+                }
+            }
+#pragma unroll
+            for (int n = 0; n < NC; ++n) sR[w][n][ring(p + 1, kRingR)] = UR[n];
+            copy_state(UL, ULp);
+        }
+        __syncwarp();
+    }
+    if (a.ws_max) reduce_ws(wsmax, nan_seen, a.ws_max);
+}
+
+// ------------------------------------------------- x sweep, shuffle exchange
+// Chunk x0, lane t: load A = U(x0+t+2); cell stage of cell x0+t+1; face
+// x0-31+t from the previous chunk's cell stages; update of cell x0-32+t.
+template <int D, int METHOD, int LIM>
+__global__ void __launch_bounds__(kSweepThreads, kSweepMinBlocks) sweep_x_shfl_kernel(const SweepArgs a)
 {
     using S = Scheme<D, 0, METHOD, LIM>;
     constexpr int NC = D + 2;
@@ -247,6 +365,7 @@ __global__ void __launch_bounds__(kSweepThreads, kSweepMinBlocks) sweep_s_kernel
         const int t2 = (int)(rest / B.ngroup);  // the other transverse index
         const int x = B.lo[0] + grp * 32 + lane;
         const bool active = x <= B.hi[0];
+        const int xc = min(x, B.hi[0]);  // loads of idle lanes read a valid column
         const int s0 = B.lo[DIR] + seg * a.seglen;
         const int s1 = min(s0 + a.seglen, B.hi[DIR] + 1);
         const bool last_seg = (s1 == B.hi[DIR] + 1);
@@ -256,7 +375,7 @@ __global__ void __launch_bounds__(kSweepThreads, kSweepMinBlocks) sweep_s_kernel
         long long ins, outs, fls = 0;
         if (DIR == 1) {
             const int kk = (D == 3) ? B.lo[2] + t2 : 0;
-            inoff = (long long)(x - B.in.b0) + (long long)(kk - B.in.b2) * B.in.ks - (long long)B.in.b1 * B.in.js;
+            inoff = (long long)(xc - B.in.b0) + (long long)(kk - B.in.b2) * B.in.ks - (long long)B.in.b1 * B.in.js;
             outoff = (long long)(x - B.out.b0) + (long long)(kk - B.out.b2) * B.out.ks - (long long)B.out.b1 * B.out.js;
             ins = B.in.js;
             outs = B.out.js;
@@ -266,7 +385,7 @@ __global__ void __launch_bounds__(kSweepThreads, kSweepMinBlocks) sweep_s_kernel
             }
         } else {
             const int jj = B.lo[1] + t2;
-            inoff = (long long)(x - B.in.b0) + (long long)(jj - B.in.b1) * B.in.js - (long long)B.in.b2 * B.in.ks;
+            inoff = (long long)(xc - B.in.b0) + (long long)(jj - B.in.b1) * B.in.js - (long long)B.in.b2 * B.in.ks;
             outoff = (long long)(x - B.out.b0) + (long long)(jj - B.out.b1) * B.out.js - (long long)B.out.b2 * B.out.ks;
             ins = B.in.ks;
             outs = B.out.ks;
@@ -278,9 +397,14 @@ __global__ void __launch_bounds__(kSweepThreads, kSweepMinBlocks) sweep_s_kernel
         const double* __restrict__ in = B.in.p + inoff;
         double* __restrict__ out = B.out.p + outoff;
 
+        const int plo = s0 - H, phi = s1 - 1 + H;  // loadable positions
         auto load = [&](int pos, double (&u)[NC]) {
-            if (active && pos >= s0 - H && pos <= s1 - 1 + H) ld_state(in + (long long)pos * ins, B.in.ns, u);
-            else benign(u);
+            if constexpr (kClampLoads) {
+                ld_state(in + (long long)min(max(pos, plo), phi) * ins, B.in.ns, u);
+            } else {
+                if (pos >= plo && pos <= phi) ld_state(in + (long long)pos * ins, B.in.ns, u);
+                else benign(u);
+            }
         };
 
         // warm-up: cell stages of cells s0-1 and s0
@@ -298,6 +422,7 @@ __global__ void __launch_bounds__(kSweepThreads, kSweepMinBlocks) sweep_s_kernel
 
         // invariant at iteration o: U0 = U(o), Ua = U(o+1), Ub = U(o+2),
         // Nx = U(o+3), URa = UR(o), URb = UR(o+1), ULb = UL(o+1), Fo = F(o)
+#pragma unroll kMarchUnroll
         for (int o = s0 - 1; o < s1; ++o) {
             double U3[NC];
             copy_state(Nx, U3);

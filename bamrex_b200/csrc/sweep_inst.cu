@@ -16,7 +16,10 @@ namespace {
 template <int D, int DIR, int M, int LIM>
 const void* kernel_ptr()
 {
-    if constexpr (DIR == 0) return (const void*)sweep_x_kernel<D, M, LIM>;
+    if constexpr (DIR == 0) {
+        if constexpr (BAMREX_X_SMEM) return (const void*)sweep_x_kernel<D, M, LIM>;
+        else return (const void*)sweep_x_shfl_kernel<D, M, LIM>;
+    }
     else return (const void*)sweep_s_kernel<D, DIR, M, LIM>;
 }
 

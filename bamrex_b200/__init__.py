@@ -9,8 +9,8 @@ mirror of the reference's level surface (``level``) and seeded problem
 generators (``problems``).
 """
 from . import problems
-from ._abi import (BC_PERIODIC, BC_REFLECTIVE, BC_TRANSMISSIVE, FORCE, HLLC, LAX_FRIEDRICHS, LIMITERS, METHODS,
-                   MINBEE, MUSCL_HANCOCK, SLIC, SUPERBEE, VAN_ALBADA, VAN_LEER, BamrexError, lib)
+from ._abi import (BC_PERIODIC, BC_REFLECTIVE, BC_TRANSMISSIVE, FORCE, FP32_STORAGE, FP64, HLLC, LAX_FRIEDRICHS,
+                   LIMITERS, METHODS, MINBEE, MUSCL_HANCOCK, SLIC, SUPERBEE, VAN_ALBADA, VAN_LEER, BamrexError, lib)
 from .level import (Level, Packing, Parm, compute_flux, compute_flux_LR, conservative_update, decompose,
                     sweep_box, sweep_update)
 

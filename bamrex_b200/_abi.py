@@ -25,6 +25,8 @@ LIMITERS = {"minbee": MINBEE, "van_leer": VAN_LEER, "van_albada": VAN_ALBADA, "s
 # boundary kinds
 BC_TRANSMISSIVE, BC_PERIODIC, BC_REFLECTIVE = range(3)
 BCS = {"transmissive": BC_TRANSMISSIVE, "periodic": BC_PERIODIC, "reflective": BC_REFLECTIVE}
+# level state precision
+FP64, FP32_STORAGE = 0, 1
 
 
 class BamrexError(RuntimeError):
@@ -96,6 +98,7 @@ class LevelDesc(ctypes.Structure):
         ("parm", CParm),
         ("x_segment", ctypes.c_int),
         ("s_segment", ctypes.c_int),
+        ("precision", ctypes.c_int),
     ]
 
 
@@ -125,6 +128,7 @@ SIGNATURES = {
     "bamrex_level_copy_in": (_i, [_vp, _vp]),
     "bamrex_level_copy_out": (_i, [_vp, _vp]),
     "bamrex_level_sync": (_i, [_vp]),
+    "bamrex_level_conserved_sums": (_i, [_vp, _dp]),
     "bamrex_level_fill_boundary": (_i, [_vp]),
     "bamrex_level_advance": (_i, [_vp, _d, _d, _i, _i, _dp]),
     "bamrex_level_est_time_step": (_i, [_vp, _dp]),

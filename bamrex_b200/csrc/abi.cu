@@ -309,7 +309,7 @@ static int per_box_sweep(int method, int dir, int D, const bamrex_box* bx, const
     a.k = k;
     a.ws_max = nullptr;
     a.do_update = Uout ? 1 : 0;
-    BX_CK(launch_sweep(D, dir, method, a, (cudaStream_t)stream));
+    BX_CK(launch_sweep(D, dir, method, false, a, (cudaStream_t)stream));
     return BAMREX_OK;
 }
 
@@ -418,6 +418,8 @@ extern "C" int bamrex_conservative_update(int spacedim, const bamrex_box* bx, ba
 // ======================================================================
 struct bamrex_level {
     int D = 0, NC = 0, ngrow = 0, method = 0;
+    bool fp32 = false;   // FP32-storage variant
+    size_t esize = 8;    // bytes per stored value
     double cfl = 0.9;
     bamrex_parm parm;
     Consts k;
@@ -431,7 +433,8 @@ struct bamrex_level {
 
     // device memory (one arena)
     char* arena = nullptr;
-    double* state[2] = { nullptr, nullptr };
+    char* state[2] = { nullptr, nullptr };
+    double* d_box_sums = nullptr;  // nboxes x NC, conserved sums
     std::vector<FabDev> fab[2];
     FabDev* d_fab[2] = { nullptr, nullptr };
     SweepBox* d_sweep[3][2] = {};
@@ -662,7 +665,7 @@ int level_launch(bamrex_level* L, cudaError_t e, const char* what)
 int level_fill(bamrex_level* L, int d, int parity, const StepScalars* scal)
 {
     if (L->nghost[d] == 0) return BAMREX_OK;
-    return level_launch(L, launch_ghost_fill(L->NC, L->d_ghost[d], L->nghost[d], L->ghost_cells[d], L->d_fab[parity], scal,
+    return level_launch(L, launch_ghost_fill(L->NC, L->fp32, L->d_ghost[d], L->nghost[d], L->ghost_cells[d], L->d_fab[parity], scal,
                                              L->stream),
                         "ghost fill");
 }
@@ -685,7 +688,7 @@ int level_sweep(bamrex_level* L, int d, int parity, double dt_host, const StepSc
     a.do_update = 1;
     const bool t = allow_timing && L->timing && L->ev_used < L->events.size();
     if (t) cudaEventRecord(L->events[L->ev_used].first, L->stream);
-    const int rc = level_launch(L, launch_sweep(L->D, d, L->method, a, L->stream), "sweep");
+    const int rc = level_launch(L, launch_sweep(L->D, d, L->method, L->fp32, a, L->stream), "sweep");
     if (rc != BAMREX_OK) return rc;
     if (t) {
         cudaEventRecord(L->events[L->ev_used].second, L->stream);
@@ -761,6 +764,12 @@ extern "C" int bamrex_level_create(bamrex_level** out, const bamrex_level_desc* 
     }
     L->boxes.assign(desc->boxes, desc->boxes + desc->nboxes);
     L->ncells = covered;
+    if (desc->precision != BAMREX_FP64 && desc->precision != BAMREX_FP32_STORAGE) {
+        delete L;
+        return fail(BAMREX_ERR_ARG, "precision must be BAMREX_FP64 or BAMREX_FP32_STORAGE");
+    }
+    L->fp32 = desc->precision == BAMREX_FP32_STORAGE;
+    L->esize = L->fp32 ? 4 : 8;
     int rc = make_consts(&L->parm, D, L->k);
     if (rc != BAMREX_OK) {
         delete L;
@@ -778,11 +787,12 @@ extern "C" int bamrex_level_create(bamrex_level** out, const bamrex_level_desc* 
         L->own_stream = true;
     }
 
-    // ---- layout of the state fabs: rows padded to 32 doubles, first valid
+    // ---- layout of the state fabs: rows padded to 256 bytes, first valid
     // cell of each row 256-byte aligned.
     const int nb = desc->nboxes;
     const int g = L->ngrow;
-    const int front = (32 - g % 32) % 32;
+    const int al = (int)(256 / L->esize);  // elements per 256 bytes
+    const int front = (al - g % al) % al;
     std::vector<long long> fab_off(nb);
     long long per_buf = 0;
     for (int b = 0; b < nb; ++b) {
@@ -791,7 +801,7 @@ extern "C" int bamrex_level_create(bamrex_level** out, const bamrex_level_desc* 
         const int nyg = D > 1 ? B.hi[1] - B.lo[1] + 1 + 2 * g : 1;
         const int nzg = D > 2 ? B.hi[2] - B.lo[2] + 1 + 2 * g : 1;
         FabDev f;
-        f.js = (long long)align_up((size_t)(front + nxg), 32);
+        f.js = (long long)align_up((size_t)(front + nxg), al);
         f.ks = f.js * nyg;
         f.ns = f.ks * nzg;
         f.b0 = B.lo[0] - g;
@@ -799,7 +809,7 @@ extern "C" int bamrex_level_create(bamrex_level** out, const bamrex_level_desc* 
         f.b2 = D > 2 ? B.lo[2] - g : B.lo[2];
         f.p = nullptr;
         fab_off[b] = per_buf + front;
-        per_buf += (long long)align_up((size_t)(f.ns * L->NC), 32);
+        per_buf += (long long)align_up((size_t)(f.ns * L->NC), al);
         L->fab[0].push_back(f);
         L->fab[1].push_back(f);
     }
@@ -809,7 +819,7 @@ extern "C" int bamrex_level_create(bamrex_level** out, const bamrex_level_desc* 
     for (int d = 0; d < D; ++d) {
         L->seglen[d] = d == 0 ? desc->x_segment : desc->s_segment;
         if (L->seglen[d] <= 0)
-            L->seglen[d] = choose_seglen(d, L->boxes, sweep_resident_warps(D, d, L->method, L->k));
+            L->seglen[d] = choose_seglen(d, L->boxes, sweep_resident_warps(D, d, L->method, L->fp32, L->k));
         if (d == 0) L->seglen[d] = (int)align_up((size_t)L->seglen[d], 32);
         long long acc = 0;
         for (int b = 0; b < nb; ++b) {
@@ -860,8 +870,9 @@ extern "C" int bamrex_level_create(bamrex_level** out, const bamrex_level_desc* 
         off = align_up(off + bytes, 256);
         return o;
     };
-    const size_t o_state0 = take((size_t)per_buf * 8);
-    const size_t o_state1 = take((size_t)per_buf * 8);
+    const size_t o_state0 = take((size_t)per_buf * L->esize);
+    const size_t o_state1 = take((size_t)per_buf * L->esize);
+    const size_t o_sums = take(sizeof(double) * nb * L->NC);
     const size_t o_fab0 = take(sizeof(FabDev) * nb);
     const size_t o_fab1 = take(sizeof(FabDev) * nb);
     size_t o_sweep[3][2] = {};
@@ -885,10 +896,11 @@ extern "C" int bamrex_level_create(bamrex_level** out, const bamrex_level_desc* 
         delete L;
         return fail(BAMREX_ERR_OOM, "cudaMallocHost failed");
     }
-    L->state[0] = (double*)(L->arena + o_state0);
-    L->state[1] = (double*)(L->arena + o_state1);
+    L->state[0] = L->arena + o_state0;
+    L->state[1] = L->arena + o_state1;
+    L->d_box_sums = (double*)(L->arena + o_sums);
     for (int p = 0; p < 2; ++p)
-        for (int b = 0; b < nb; ++b) L->fab[p][b].p = L->state[p] + fab_off[b];
+        for (int b = 0; b < nb; ++b) L->fab[p][b].p = L->state[p] + (size_t)fab_off[b] * L->esize;
     L->d_fab[0] = (FabDev*)(L->arena + o_fab0);
     L->d_fab[1] = (FabDev*)(L->arena + o_fab1);
     for (int d = 0; d < D; ++d) {
@@ -919,7 +931,7 @@ extern "C" int bamrex_level_create(bamrex_level** out, const bamrex_level_desc* 
         if (ue == cudaSuccess) ue = up(L->d_ghost[d], ghost_host[d].data(), sizeof(GhostOp) * ghost_host[d].size());
     }
     if (ue == cudaSuccess) ue = up(L->d_pack, pack_host.data(), sizeof(PackBox) * nb);
-    if (ue == cudaSuccess) ue = cudaMemset(L->arena + o_state0, 0, (size_t)per_buf * 8 * 2);
+    if (ue == cudaSuccess) ue = cudaMemset(L->arena + o_state0, 0, (size_t)(o_state1 - o_state0) * 2);
     if (ue == cudaSuccess) ue = cudaMemset(L->d_scal, 0, sizeof(StepScalars));
     if (ue != cudaSuccess) {
         const int r = cuda_fail(ue, "level table upload");
@@ -956,7 +968,7 @@ extern "C" int bamrex_level_fab(const bamrex_level* L, int box, bamrex_array4* o
     if (!L || !out || box < 0 || box >= (int)L->boxes.size()) return fail(BAMREX_ERR_ARG, "bad level/box");
     const FabDev& f = L->fab[L->cur][box];
     const bamrex_box& B = L->boxes[box];
-    out->p = f.p;
+    out->p = static_cast<double*>(f.p);  // float elements for an FP32-storage level
     out->jstride = f.js;
     out->kstride = f.ks;
     out->nstride = f.ns;
@@ -982,7 +994,7 @@ extern "C" int bamrex_level_copy_in(bamrex_level* L, const double* src)
         if (e != cudaSuccess) return L->set_err(cuda_fail(e, "copy_in memcpy"));
         from = L->staging;
     }
-    BX_TRY(level_launch(L, launch_pack(L->NC, L->d_fab[L->cur], L->d_pack, (int)L->boxes.size(), L->ncells,
+    BX_TRY(level_launch(L, launch_pack(L->NC, L->fp32, L->d_fab[L->cur], L->d_pack, (int)L->boxes.size(), L->ncells,
                                        const_cast<double*>(from), 0, L->stream),
                         "unpack"));
     L->ws_valid = false;
@@ -996,7 +1008,7 @@ extern "C" int bamrex_level_copy_out(bamrex_level* L, double* dst)
     const bool dev = cudaPointerGetAttributes(&at, dst) == cudaSuccess && at.type == cudaMemoryTypeDevice;
     cudaGetLastError();
     double* to = dev ? dst : L->staging;
-    BX_TRY(level_launch(L, launch_pack(L->NC, L->d_fab[L->cur], L->d_pack, (int)L->boxes.size(), L->ncells, to, 1, L->stream),
+    BX_TRY(level_launch(L, launch_pack(L->NC, L->fp32, L->d_fab[L->cur], L->d_pack, (int)L->boxes.size(), L->ncells, to, 1, L->stream),
                         "pack"));
     if (!dev) {
         const cudaError_t e = cudaMemcpyAsync(dst, L->staging, (size_t)L->ncells * L->NC * 8, cudaMemcpyDefault, L->stream);
@@ -1010,6 +1022,26 @@ extern "C" int bamrex_level_sync(bamrex_level* L)
     if (!L) return fail(BAMREX_ERR_ARG, "NULL level");
     const cudaError_t e = cudaStreamSynchronize(L->stream);
     if (e != cudaSuccess) return L->set_err(cuda_fail(e, "cudaStreamSynchronize"));
+    return BAMREX_OK;
+}
+
+extern "C" int bamrex_level_conserved_sums(bamrex_level* L, double* totals)
+{
+    if (!L || !totals) return fail(BAMREX_ERR_ARG, "NULL argument");
+    const int nb = (int)L->boxes.size();
+    BX_TRY(level_launch(L, launch_box_sums(L->NC, L->fp32, L->d_fab[L->cur], L->d_pack, nb, L->d_box_sums, L->stream),
+                        "box sums"));
+    std::vector<double> h((size_t)nb * L->NC);
+    cudaError_t e = cudaMemcpyAsync(h.data(), L->d_box_sums, h.size() * sizeof(double), cudaMemcpyDeviceToHost, L->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(L->stream);
+    if (e != cudaSuccess) return L->set_err(cuda_fail(e, "conserved sums"));
+    double vol = 1.0;
+    for (int d = 0; d < L->D; ++d) vol *= L->dx[d];
+    for (int n = 0; n < L->NC; ++n) {
+        double s = 0.0;
+        for (int b = 0; b < nb; ++b) s += h[(size_t)b * L->NC + n];  // fixed box order
+        totals[n] = s * vol;
+    }
     return BAMREX_OK;
 }
 
@@ -1044,7 +1076,7 @@ extern "C" int bamrex_level_est_time_step(bamrex_level* L, double* dt_est)
     if (!L->ws_valid) {
         cudaError_t e = cudaMemsetAsync(&L->d_scal->ws_bits, 0, sizeof(unsigned long long), L->stream);
         if (e != cudaSuccess) return L->set_err(cuda_fail(e, "memset"));
-        BX_TRY(level_launch(L, launch_max_wave_speed(L->D, L->d_fab[L->cur], L->d_pack, (int)L->boxes.size(), L->ncells, L->k,
+        BX_TRY(level_launch(L, launch_max_wave_speed(L->D, L->fp32, L->d_fab[L->cur], L->d_pack, (int)L->boxes.size(), L->ncells, L->k,
                                                      &L->d_scal->ws_bits, nullptr, L->stream),
                             "max wave speed"));
     }
@@ -1077,7 +1109,7 @@ extern "C" int bamrex_level_run_async(bamrex_level* L, int nsteps, double stop_t
     cudaError_t e = cudaMemcpyAsync(L->d_scal, h, sizeof(StepScalars), cudaMemcpyHostToDevice, L->stream);
     if (e != cudaSuccess) return L->set_err(cuda_fail(e, "scalars upload"));
     // computeInitialDt from the current state
-    BX_TRY(level_launch(L, launch_max_wave_speed(L->D, L->d_fab[L->cur], L->d_pack, (int)L->boxes.size(), L->ncells, L->k,
+    BX_TRY(level_launch(L, launch_max_wave_speed(L->D, L->fp32, L->d_fab[L->cur], L->d_pack, (int)L->boxes.size(), L->ncells, L->k,
                                                  &L->d_scal->ws_bits, L->d_scal, L->stream),
                         "max wave speed"));
     BX_TRY(level_launch(L, launch_step_dt(L->d_scal, L->D, L->dx[0], L->dx[1], L->dx[2], L->cfl, 0, L->stream), "step dt"));

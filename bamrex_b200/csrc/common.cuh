@@ -43,8 +43,12 @@ struct Consts {
 };
 
 // A fab (amrex::Array4 geometry) on the device.
+// p points at elements of the storage type (double, or float for the
+// FP32-storage variant); strides count elements.
 struct FabDev {
-    double* p;
+    void* p;
+    template <typename T>
+    __host__ __device__ __forceinline__ T* ptr() const { return static_cast<T*>(p); }
     long long js, ks, ns;
     int b0, b1, b2;  // begin corner
 };

@@ -1,7 +1,9 @@
 // Light kernels of the explicit path: ghost fill (FillBoundary + physical
 // boundary conditions), pack/unpack of valid cells, the stand-alone max
-// wave speed reduction, device time-step bookkeeping, and the per-box
-// left/right flux and update kernels of the Fluxes.H / Update.H surface.
+// wave speed reduction, per-box conserved sums, device time-step
+// bookkeeping, and the per-box left/right flux and update kernels of the
+// Fluxes.H / Update.H surface.  Level kernels are templated on the storage
+// type (double, or float for the FP32-storage variant).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -28,8 +30,8 @@ __device__ __forceinline__ long long fab_index(const FabDev& f, int i, int j, in
     return (long long)(i - f.b0) + (long long)(j - f.b1) * f.js + (long long)(k - f.b2) * f.ks;
 }
 
-template <typename T>
-__device__ __forceinline__ int find_by_begin(const T* v, int n, long long idx)
+template <typename V>
+__device__ __forceinline__ int find_by_begin(const V* v, int n, long long idx)
 {
     int lo = 0, hi = n - 1;
     while (lo < hi) {
@@ -42,6 +44,7 @@ __device__ __forceinline__ int find_by_begin(const T* v, int n, long long idx)
 // ---------------------------------------------------------------- ghosts
 // bamrexBCData::fill_consv_boundary (Source/BoundaryConditions/BCs.cpp:429-442)
 // expressed as a table of region copies built on the host.
+template <typename T>
 __global__ void ghost_fill_kernel(int NC, const GhostOp* __restrict__ ops, int nops, long long total,
                                   const FabDev* __restrict__ fabs, const StepScalars* scal)
 {
@@ -59,24 +62,24 @@ __global__ void ghost_fill_kernel(int NC, const GhostOp* __restrict__ ops, int n
         const int sk = op.off[2] + op.mul[2] * ck;
         const FabDev& d = fabs[op.dst];
         const FabDev& s = fabs[op.src];
-        const double* ps = s.p + fab_index(s, si, sj, sk);
-        double* pd = d.p + fab_index(d, ci, cj, ck);
+        const T* ps = s.ptr<T>() + fab_index(s, si, sj, sk);
+        T* pd = d.ptr<T>() + fab_index(d, ci, cj, ck);
         for (int n = 0; n < NC; ++n) {
-            const double v = ps[n * s.ns];
+            const T v = ps[n * s.ns];
             pd[n * d.ns] = ((op.negmask >> n) & 1) ? -v : v;
         }
     }
 }
 
 // ---------------------------------------------------------------- pack
+// packed element e = cell_begin*NC + n*ncells_box + cell (always double)
+template <typename T>
 __global__ void pack_kernel(int NC, const FabDev* __restrict__ fabs, const PackBox* __restrict__ boxes, int nboxes,
                             long long total, double* __restrict__ packed, int to_packed)
 {
-    // packed element e = cell_begin*NC + n*ncells_box + cell
     const long long nel = total * NC;
     for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < nel;
          e += (long long)gridDim.x * blockDim.x) {
-        // find the box whose packed range contains e
         int lo = 0, hi = nboxes - 1;
         while (lo < hi) {
             const int mid = (lo + hi + 1) >> 1;
@@ -92,20 +95,21 @@ __global__ void pack_kernel(int NC, const FabDev* __restrict__ fabs, const PackB
         const int j = B.lo[1] + (int)((c / nx) % ny);
         const int k = B.lo[2] + (int)(c / ((long long)nx * ny));
         const FabDev& f = fabs[lo];
-        double* pf = f.p + fab_index(f, i, j, k) + n * f.ns;
-        if (to_packed) packed[e] = *pf;
-        else *pf = packed[e];
+        T* pf = f.ptr<T>() + fab_index(f, i, j, k) + n * f.ns;
+        if (to_packed) packed[e] = (double)*pf;
+        else *pf = (T)packed[e];
     }
 }
 
 // ---------------------------------------------------------------- max speed
 // max_wave_speed (Source/System/Euler/Euler.cpp:46-74) over valid cells.
-template <int D>
+template <typename T, int D>
 __global__ void max_ws_kernel(const FabDev* __restrict__ fabs, const PackBox* __restrict__ boxes, int nboxes,
-                              long long total, const Consts k, unsigned long long* ws_bits, const StepScalars* scal)
+                              long long total, const Consts kc, unsigned long long* ws_bits, const StepScalars* scal)
 {
     if (scal && scal->done) return;
     constexpr int NC = D + 2;
+    const K<T> k(kc);
     double wmax = 0.0;
     bool nan_seen = false;
     for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < total;
@@ -118,10 +122,10 @@ __global__ void max_ws_kernel(const FabDev* __restrict__ fabs, const PackBox* __
         const int j = B.lo[1] + (int)((local / nx) % ny);
         const int kk = B.lo[2] + (int)(local / ((long long)nx * ny));
         const FabDev& f = fabs[b];
-        const double* p = f.p + fab_index(f, i, j, kk);
-        double U[NC];
+        const T* p = f.ptr<T>() + fab_index(f, i, j, kk);
+        T U[NC];
         for (int n = 0; n < NC; ++n) U[n] = p[n * f.ns];
-        const double w = wave_speed<D>(U, k);
+        const double w = (double)wave_speed<T, D>(U, k);
         wmax = fmax(wmax, w);
         nan_seen = nan_seen || (w != w);
     }
@@ -130,6 +134,39 @@ __global__ void max_ws_kernel(const FabDev* __restrict__ fabs, const PackBox* __
     if ((threadIdx.x & 31) == 0) {
         if (any_nan) atomicMax(ws_bits, 0x7ff8000000000000ull);
         else if (wmax > 0.0) atomicMax(ws_bits, (unsigned long long)__double_as_longlong(wmax));
+    }
+}
+
+// ---------------------------------------------------------------- box sums
+// One block per box; each thread sums a fixed strided subset of cells in
+// double, then a fixed-shape tree reduction: the result does not depend on
+// scheduling, so repeated runs give identical totals.
+template <typename T>
+__global__ void box_sums_kernel(int NC, const FabDev* __restrict__ fabs, const PackBox* __restrict__ boxes,
+                                double* __restrict__ sums)
+{
+    __shared__ double red[256];
+    const int b = blockIdx.x;
+    const PackBox& B = boxes[b];
+    const FabDev& f = fabs[b];
+    const int nx = B.hi[0] - B.lo[0] + 1, ny = B.hi[1] - B.lo[1] + 1, nz = B.hi[2] - B.lo[2] + 1;
+    const long long ncell = (long long)nx * ny * nz;
+    for (int n = 0; n < NC; ++n) {
+        double acc = 0.0;
+        for (long long c = threadIdx.x; c < ncell; c += blockDim.x) {
+            const int i = B.lo[0] + (int)(c % nx);
+            const int j = B.lo[1] + (int)((c / nx) % ny);
+            const int k = B.lo[2] + (int)(c / ((long long)nx * ny));
+            acc += (double)f.ptr<T>()[fab_index(f, i, j, k) + n * f.ns];
+        }
+        red[threadIdx.x] = acc;
+        __syncthreads();
+        for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+            if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) sums[(long long)b * NC + n] = red[0];
+        __syncthreads();
     }
 }
 
@@ -167,9 +204,10 @@ __global__ void step_dt_kernel(StepScalars* s, int D, double dx0, double dx1, do
 // compute_HLLC_flux_LR / compute_force_flux_LR on a box: one thread per face.
 template <int D, int DIR, int KIND>
 __global__ void flux_lr_kernel(int lo0, int lo1, int lo2, int hi0, int hi1, int hi2, const FabDev flux,
-                               const FabDev cL, const FabDev cR, const Consts k, double half_dx_dt, double dt_2dx)
+                               const FabDev cL, const FabDev cR, const Consts kc, double half_dx_dt, double dt_2dx)
 {
     constexpr int NC = D + 2;
+    const K<double> k(kc);
     const int fhi[3] = { hi0 + (DIR == 0), hi1 + (DIR == 1), hi2 + (DIR == 2) };
     const int nx = fhi[0] - lo0 + 1, ny = fhi[1] - lo1 + 1, nz = fhi[2] - lo2 + 1;
     const long long total = (long long)nx * ny * nz;
@@ -179,15 +217,15 @@ __global__ void flux_lr_kernel(int lo0, int lo1, int lo2, int hi0, int hi1, int 
         const int j = lo1 + (int)((idx / nx) % ny);
         const int kk = lo2 + (int)(idx / ((long long)nx * ny));
         double L[NC], R[NC], F[NC];
-        const double* pl = cL.p + fab_index(cL, i - (DIR == 0), j - (DIR == 1), kk - (DIR == 2));
-        const double* pr = cR.p + fab_index(cR, i, j, kk);
+        const double* pl = cL.ptr<double>() + fab_index(cL, i - (DIR == 0), j - (DIR == 1), kk - (DIR == 2));
+        const double* pr = cR.ptr<double>() + fab_index(cR, i, j, kk);
         for (int n = 0; n < NC; ++n) {
             L[n] = pl[n * cL.ns];
             R[n] = pr[n * cR.ns];
         }
-        if (KIND == M_HLLC) hllc_face<D, DIR>(L, R, k, F);
-        else force_face<D, DIR>(L, R, k, half_dx_dt, dt_2dx, F);
-        double* pf = flux.p + fab_index(flux, i, j, kk);
+        if (KIND == M_HLLC) hllc_face<double, D, DIR>(L, R, k, F);
+        else force_face<double, D, DIR>(L, R, k, half_dx_dt, dt_2dx, F);
+        double* pf = flux.ptr<double>() + fab_index(flux, i, j, kk);
         for (int n = 0; n < NC; ++n) pf[n * flux.ns] = F[n];
     }
 }
@@ -206,10 +244,10 @@ __global__ void sweep_update_kernel(const UpdateArgs u)
         const int i = u.lo[0] + (int)(idx % nx);
         const int j = u.lo[1] + (int)((idx / nx) % ny);
         const int k = u.lo[2] + (int)(idx / ((long long)nx * ny));
-        const double* pin = u.in.p + fab_index(u.in, i, j, k);
-        const double* pf0 = fl.p + fab_index(fl, i, j, k);
-        const double* pf1 = fl.p + fab_index(fl, i + (DIR == 0), j + (DIR == 1), k + (DIR == 2));
-        double* po = u.out.p + fab_index(u.out, i, j, k);
+        const double* pin = u.in.ptr<double>() + fab_index(u.in, i, j, k);
+        const double* pf0 = fl.ptr<double>() + fab_index(fl, i, j, k);
+        const double* pf1 = fl.ptr<double>() + fab_index(fl, i + (DIR == 0), j + (DIR == 1), k + (DIR == 2));
+        double* po = u.out.ptr<double>() + fab_index(u.out, i, j, k);
         // explicit rounding of the product: no FMA contraction, so the
         // stand-alone update rounds exactly as the scalar reference does
         for (int n = 0; n < NC; ++n)
@@ -229,15 +267,15 @@ __global__ void cons_update_kernel(const UpdateArgs u)
         const int i = u.lo[0] + (int)(idx % nx);
         const int j = u.lo[1] + (int)((idx / nx) % ny);
         const int k = u.lo[2] + (int)(idx / ((long long)nx * ny));
-        const double* pin = u.in.p + fab_index(u.in, i, j, k);
-        double* po = u.out.p + fab_index(u.out, i, j, k);
+        const double* pin = u.in.ptr<double>() + fab_index(u.in, i, j, k);
+        double* po = u.out.ptr<double>() + fab_index(u.out, i, j, k);
         for (int n = 0; n < NC; ++n) {
             double v = pin[n * u.in.ns];
 #pragma unroll
             for (int d = 0; d < D; ++d) {
                 const FabDev& f = u.flux[d];
-                const double a = f.p[fab_index(f, i + (d == 0), j + (d == 1), k + (d == 2)) + n * f.ns];
-                const double b = f.p[fab_index(f, i, j, k) + n * f.ns];
+                const double a = f.ptr<double>()[fab_index(f, i + (d == 0), j + (d == 1), k + (d == 2)) + n * f.ns];
+                const double b = f.ptr<double>()[fab_index(f, i, j, k) + n * f.ns];
                 v = v - __dmul_rn(u.dtdx[d], a - b);
             }
             po[n * u.out.ns] = v;
@@ -261,34 +299,54 @@ int device_sm_count()
     return cache[dev];
 }
 
-cudaError_t launch_ghost_fill(int NC, const GhostOp* ops, int nops, long long total_cells, const FabDev* fabs,
-                              const StepScalars* scal, cudaStream_t s)
+cudaError_t launch_ghost_fill(int NC, bool fp32, const GhostOp* ops, int nops, long long total_cells,
+                              const FabDev* fabs, const StepScalars* scal, cudaStream_t s)
 {
     if (nops == 0 || total_cells == 0) return cudaSuccess;
-    ghost_fill_kernel<<<grid_for(total_cells), kThreads, 0, s>>>(NC, ops, nops, total_cells, fabs, scal);
+    if (fp32) ghost_fill_kernel<float><<<grid_for(total_cells), kThreads, 0, s>>>(NC, ops, nops, total_cells, fabs, scal);
+    else ghost_fill_kernel<double><<<grid_for(total_cells), kThreads, 0, s>>>(NC, ops, nops, total_cells, fabs, scal);
     return cudaGetLastError();
 }
 
-cudaError_t launch_pack(int NC, const FabDev* fabs, const PackBox* boxes, int nboxes, long long total_cells,
-                        double* packed, int to_packed, cudaStream_t s)
+cudaError_t launch_pack(int NC, bool fp32, const FabDev* fabs, const PackBox* boxes, int nboxes,
+                        long long total_cells, double* packed, int to_packed, cudaStream_t s)
 {
     if (total_cells == 0) return cudaSuccess;
-    pack_kernel<<<grid_for(total_cells * NC, 4), kThreads, 0, s>>>(NC, fabs, boxes, nboxes, total_cells, packed,
-                                                                  to_packed);
+    const int g = grid_for(total_cells * NC, 4);
+    if (fp32) pack_kernel<float><<<g, kThreads, 0, s>>>(NC, fabs, boxes, nboxes, total_cells, packed, to_packed);
+    else pack_kernel<double><<<g, kThreads, 0, s>>>(NC, fabs, boxes, nboxes, total_cells, packed, to_packed);
     return cudaGetLastError();
 }
 
-cudaError_t launch_max_wave_speed(int D, const FabDev* fabs, const PackBox* boxes, int nboxes,
-                                  long long total_cells, const Consts& k, unsigned long long* ws_bits,
-                                  const StepScalars* scal, cudaStream_t s)
+template <typename T>
+static cudaError_t max_ws_dispatch(int D, const FabDev* fabs, const PackBox* boxes, int nboxes, long long total_cells,
+                                   const Consts& k, unsigned long long* ws_bits, const StepScalars* scal,
+                                   cudaStream_t s)
 {
     const int g = grid_for(total_cells, 4);
     switch (D) {
-    case 1: max_ws_kernel<1><<<g, kThreads, 0, s>>>(fabs, boxes, nboxes, total_cells, k, ws_bits, scal); break;
-    case 2: max_ws_kernel<2><<<g, kThreads, 0, s>>>(fabs, boxes, nboxes, total_cells, k, ws_bits, scal); break;
-    case 3: max_ws_kernel<3><<<g, kThreads, 0, s>>>(fabs, boxes, nboxes, total_cells, k, ws_bits, scal); break;
+    case 1: max_ws_kernel<T, 1><<<g, kThreads, 0, s>>>(fabs, boxes, nboxes, total_cells, k, ws_bits, scal); break;
+    case 2: max_ws_kernel<T, 2><<<g, kThreads, 0, s>>>(fabs, boxes, nboxes, total_cells, k, ws_bits, scal); break;
+    case 3: max_ws_kernel<T, 3><<<g, kThreads, 0, s>>>(fabs, boxes, nboxes, total_cells, k, ws_bits, scal); break;
     default: return cudaErrorInvalidValue;
     }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_max_wave_speed(int D, bool fp32, const FabDev* fabs, const PackBox* boxes, int nboxes,
+                                  long long total_cells, const Consts& k, unsigned long long* ws_bits,
+                                  const StepScalars* scal, cudaStream_t s)
+{
+    if (fp32) return max_ws_dispatch<float>(D, fabs, boxes, nboxes, total_cells, k, ws_bits, scal, s);
+    return max_ws_dispatch<double>(D, fabs, boxes, nboxes, total_cells, k, ws_bits, scal, s);
+}
+
+cudaError_t launch_box_sums(int NC, bool fp32, const FabDev* fabs, const PackBox* boxes, int nboxes, double* sums,
+                            cudaStream_t s)
+{
+    if (nboxes == 0) return cudaSuccess;
+    if (fp32) box_sums_kernel<float><<<nboxes, 256, 0, s>>>(NC, fabs, boxes, sums);
+    else box_sums_kernel<double><<<nboxes, 256, 0, s>>>(NC, fabs, boxes, sums);
     return cudaGetLastError();
 }
 

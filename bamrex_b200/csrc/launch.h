@@ -1,5 +1,6 @@
 // Host-side launch interface between the C ABI / level driver (abi.cu) and
-// the kernel translation units.
+// the kernel translation units.  `fp32` selects the FP32-storage kernels
+// (state in float); the per-box reference surface is FP64 only.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -34,25 +35,31 @@ struct UpdateArgs {
 
 int device_sm_count();
 
-cudaError_t launch_sweep(int D, int dir, int method, const SweepArgs& a, cudaStream_t s);
+cudaError_t launch_sweep(int D, int dir, int method, bool fp32, const SweepArgs& a, cudaStream_t s);
 
 // Warps of the sweep kernel that fit on the device at once (for choosing
 // segment lengths); 0 for an unsupported combination.
-long long sweep_resident_warps(int D, int dir, int method, const Consts& k);
+long long sweep_resident_warps(int D, int dir, int method, bool fp32, const Consts& k);
 
 // The fast-path limiter for this configuration (MUSCL-Hancock, energy
 // limiting, gamma with 1/z = 7), or -1 for the general kernels.
 int fast_limiter(int D, int method, const Consts& k);
 
-cudaError_t launch_ghost_fill(int NC, const GhostOp* ops, int nops, long long total_cells, const FabDev* fabs,
-                              const StepScalars* scal, cudaStream_t s);
+cudaError_t launch_ghost_fill(int NC, bool fp32, const GhostOp* ops, int nops, long long total_cells,
+                              const FabDev* fabs, const StepScalars* scal, cudaStream_t s);
 
-cudaError_t launch_pack(int NC, const FabDev* fabs, const PackBox* boxes, int nboxes, long long total_cells,
-                        double* packed, int to_packed, cudaStream_t s);
+// Packed buffer is always double; fabs are double or float.
+cudaError_t launch_pack(int NC, bool fp32, const FabDev* fabs, const PackBox* boxes, int nboxes,
+                        long long total_cells, double* packed, int to_packed, cudaStream_t s);
 
-cudaError_t launch_max_wave_speed(int D, const FabDev* fabs, const PackBox* boxes, int nboxes,
+cudaError_t launch_max_wave_speed(int D, bool fp32, const FabDev* fabs, const PackBox* boxes, int nboxes,
                                   long long total_cells, const Consts& k, unsigned long long* ws_bits,
                                   const StepScalars* scal, cudaStream_t s);
+
+// Per-box sums of each component over valid cells, accumulated in double in
+// a fixed order (one block per box); sums[b * NC + n].
+cudaError_t launch_box_sums(int NC, bool fp32, const FabDev* fabs, const PackBox* boxes, int nboxes, double* sums,
+                            cudaStream_t s);
 
 // Time-step bookkeeping on the device (computeInitialDt / computeNewDt).
 // mode 0: initial dt from ws_bits at the current time; mode 1: end of a

@@ -1,7 +1,9 @@
 // Fused split-sweep kernels: per box, the interface flux of one direction
 // and the conservative update (compute_*_flux + the update lambda of
 // AmrLevelAdv::advance_explicit, Source/AmrLevelAdv_advance.cpp:290-341),
-// in one pass that reads U once and writes U once.
+// in one pass that reads U once and writes U once.  T is the storage and
+// arithmetic type (double: the drop-in path; float: the FP32-storage
+// variant); the wave-speed reduction is carried out in double either way.
 //
 // Work decomposition: a launch covers every box of a sweep (the device box
 // table); each warp takes work items from a grid-stride loop.
@@ -12,7 +14,7 @@
 //  * y / z sweeps (strided directions): an item is a group of 32 adjacent
 //    columns x and a segment along the sweep; each thread marches its column
 //    keeping the stencil in registers.  Loads and stores are coalesced
-//    across the warp (32 consecutive doubles per component).
+//    across the warp (32 consecutive values per component).
 // Both are software-pipelined: the face stage of an iteration uses cell
 // stages finished in earlier iterations, so the cell stage (reconstruction
 // + half step) and the face stage (Riemann flux) of one iteration are
@@ -26,26 +28,23 @@ namespace bamrex {
 
 constexpr int kSweepThreads = 128;
 // Resident 128-thread blocks per SM the sweep kernels are compiled for
-// (register budget 65536 / (128 * blocks)).
+// (register budget 65536 / (128 * blocks)).  3 measured best for FP64
+// (2 and 4 were slower on the 4096^2 MUSCL-Hancock step).
 #ifndef BAMREX_SWEEP_MIN_BLOCKS
 #define BAMREX_SWEEP_MIN_BLOCKS 3
 #endif
 constexpr int kSweepMinBlocks = BAMREX_SWEEP_MIN_BLOCKS;
+// The FP32-storage kernels hold half the registers per state value.
+#ifndef BAMREX_SWEEP_MIN_BLOCKS_F32
+#define BAMREX_SWEEP_MIN_BLOCKS_F32 4
+#endif
+template <typename T>
+constexpr int min_blocks() { return sizeof(T) == 4 ? BAMREX_SWEEP_MIN_BLOCKS_F32 : kSweepMinBlocks; }
 // Unroll factor of the strided march loop.
 #ifndef BAMREX_MARCH_UNROLL
 #define BAMREX_MARCH_UNROLL 1
 #endif
 constexpr int kMarchUnroll = BAMREX_MARCH_UNROLL;
-// Out-of-range positions of the strided march: clamped into the box (1) or
-// replaced by a benign state (0).
-#ifndef BAMREX_CLAMP_LOADS
-#define BAMREX_CLAMP_LOADS 0
-#endif
-constexpr bool kClampLoads = BAMREX_CLAMP_LOADS != 0;
-// x sweep neighbour exchange: warp shuffles (0) or shared-memory rings (1).
-#ifndef BAMREX_X_SMEM
-#define BAMREX_X_SMEM 0
-#endif
 
 __device__ __forceinline__ int find_box(const SweepBox* boxes, int nboxes, long long item)
 {
@@ -57,52 +56,54 @@ __device__ __forceinline__ int find_box(const SweepBox* boxes, int nboxes, long 
     return lo;
 }
 
+template <typename T>
 struct StepFactors {
-    double dtdx, hdtdx, half_dx_dt, dt_2dx;
+    T dtdx, hdtdx, half_dx_dt, dt_2dx;
 };
 
-__device__ __forceinline__ bool step_factors(const SweepArgs& a, StepFactors& s)
+template <typename T>
+__device__ __forceinline__ bool step_factors(const SweepArgs& a, StepFactors<T>& s)
 {
     double dt = a.dt_host;
     if (a.scal) {
         if (a.scal->done) return false;
         dt = a.scal->dt;
     }
-    s.dtdx = dt / a.dx;               // (dt / dx[d]), AmrLevelAdv_advance.cpp:337
-    s.hdtdx = 0.5 * dt / a.dx;        // Flux_Helpers.cpp:138
-    s.half_dx_dt = 0.5 * a.dx / dt;   // Force.cpp:77, 144
-    s.dt_2dx = dt / (2 * a.dx);       // Force.cpp:91
+    s.dtdx = (T)(dt / a.dx);               // (dt / dx[d]), AmrLevelAdv_advance.cpp:337
+    s.hdtdx = (T)(0.5 * dt / a.dx);        // Flux_Helpers.cpp:138
+    s.half_dx_dt = (T)(0.5 * a.dx / dt);   // Force.cpp:77, 144
+    s.dt_2dx = (T)(dt / (2 * a.dx));       // Force.cpp:91
     return true;
 }
 
 // A benign state used for lanes that have nothing to load: keeps the
 // arithmetic of idle lanes finite.
-template <int NC>
-__device__ __forceinline__ void benign(double (&u)[NC])
+template <typename T, int NC>
+__device__ __forceinline__ void benign(T (&u)[NC])
 {
-    u[0] = 1.0;
+    u[0] = T(1);
 #pragma unroll
-    for (int n = 1; n < NC - 1; ++n) u[n] = 0.0;
-    u[NC - 1] = 1.0;
+    for (int n = 1; n < NC - 1; ++n) u[n] = T(0);
+    u[NC - 1] = T(1);
 }
 
-template <int NC>
-__device__ __forceinline__ void ld_state(const double* __restrict__ p, long long ns, double (&u)[NC])
+template <typename T, int NC>
+__device__ __forceinline__ void ld_state(const T* __restrict__ p, long long ns, T (&u)[NC])
 {
 #pragma unroll
     for (int n = 0; n < NC; ++n) u[n] = __ldg(p + n * ns);
 }
 
-template <int NC>
-__device__ __forceinline__ void copy_state(const double (&s)[NC], double (&d)[NC])
+template <typename T, int NC>
+__device__ __forceinline__ void copy_state(const T (&s)[NC], T (&d)[NC])
 {
 #pragma unroll
     for (int n = 0; n < NC; ++n) d[n] = s[n];
 }
 
-template <int NC>
-__device__ __forceinline__ void shfl_carry(const double (&cur)[NC], const double (&prev)[NC], int lane,
-                                           int shift, double (&out)[NC])
+template <typename T, int NC>
+__device__ __forceinline__ void shfl_carry(const T (&cur)[NC], const T (&prev)[NC], int lane, int shift,
+                                           T (&out)[NC])
 {
     // lane t receives cur[t-shift], or prev[32+t-shift] for t < shift
     const bool from_prev = lane >= 32 - shift;
@@ -134,118 +135,16 @@ __device__ __forceinline__ void track_ws(double w, double& wsmax, bool& nan_seen
 
 // ------------------------------------------------------------------ x sweep
 // Chunk x0, lane t: load A = U(x0+t+2); cell stage of cell x0+t+1; face
-// x0-31+t from the previous chunks' cell stages; update of cell x0-32+t.
-// Neighbour values move between lanes through per-warp shared-memory rings
-// indexed by position (loads over 4 chunks, UR and faces over 2; the UR
-// ring is safe because a __syncwarp separates its reads from its writes),
-// so no lane needs a select on chunk boundaries.
-constexpr int kRingA = 128, kRingR = 64, kRingF = 64;  // powers of two
-
-// ring slot of a position (two's complement AND also wraps negative positions)
-__device__ __forceinline__ int ring(int pos, int n) { return pos & (n - 1); }
-
-template <int D, int METHOD, int LIM>
-__global__ void __launch_bounds__(kSweepThreads, kSweepMinBlocks) sweep_x_kernel(const SweepArgs a)
-{
-    using S = Scheme<D, 0, METHOD, LIM>;
-    constexpr int NC = D + 2;
-    constexpr int H = S::kHalo;
-    __shared__ double sA[kSweepThreads / 32][NC][kRingA];
-    __shared__ double sR[kSweepThreads / 32][NC][kRingR];
-    __shared__ double sF[kSweepThreads / 32][NC][kRingF];
-    StepFactors f;
-    if (!step_factors(a, f)) return;
-    const int lane = threadIdx.x & 31;
-    const int w = threadIdx.x >> 5;
-    const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
-    double wsmax = 0.0;
-    bool nan_seen = false;
-
-    for (long long it = gw; it < a.total_items; it += nw) {
-        const int b = a.boxes ? find_box(a.boxes, a.nboxes, it) : 0;
-        const SweepBox& B = a.boxes ? a.boxes[b] : a.one;
-        const long long local = it - B.item_begin;
-        const int seg = (int)(local % B.nseg);
-        const long long row = local / B.nseg;
-        const int ny = B.hi[1] - B.lo[1] + 1;
-        const int j = B.lo[1] + (int)(row % ny);
-        const int kk = B.lo[2] + (int)(row / ny);
-        const int s0 = B.lo[0] + seg * a.seglen;
-        const int s1 = min(s0 + a.seglen, B.hi[0] + 1);
-        const bool last_seg = (s1 == B.hi[0] + 1);
-        const int plo = s0 - H, phi = s1 - 1 + H;  // loadable positions
-
-        const double* __restrict__ in = B.in.p + (long long)(j - B.in.b1) * B.in.js + (long long)(kk - B.in.b2) * B.in.ks - B.in.b0;
-        double* __restrict__ out = B.out.p + (long long)(j - B.out.b1) * B.out.js + (long long)(kk - B.out.b2) * B.out.ks - B.out.b0;
-        double* __restrict__ fl = B.flux.p ? B.flux.p + (long long)(j - B.flux.b1) * B.flux.js + (long long)(kk - B.flux.b2) * B.flux.ks - B.flux.b0 : nullptr;
-
-        double ULp[NC];  // this lane's UL from the previous chunk
-        benign(ULp);
-        double An[NC];
-        ld_state(in + min(max(s0 - 30 + lane, plo), phi), B.in.ns, An);
-        for (int x0 = s0 - 32; x0 < s1 + 32; x0 += 32) {
-            double A[NC];
-            copy_state(An, A);
-            ld_state(in + min(max(x0 + 34 + lane, plo), phi), B.in.ns, An);
-            const int p = x0 + lane;
-#pragma unroll
-            for (int n = 0; n < NC; ++n) sA[w][n][ring(p + 2, kRingA)] = A[n];
-            __syncwarp();
-            double Um1[NC], Um2[NC], URf[NC], Uo[NC];
-#pragma unroll
-            for (int n = 0; n < NC; ++n) {
-                Um1[n] = sA[w][n][ring(p + 1, kRingA)];
-                Um2[n] = sA[w][n][ring(p, kRingA)];
-                Uo[n] = sA[w][n][ring(p - 32, kRingA)];
-                URf[n] = sR[w][n][ring(p - 32, kRingR)];
-            }
-            double UL[NC], UR[NC];
-            S::cell(Um2, Um1, A, a.k, f.hdtdx, UL, UR);               // cell p+1
-            double F[NC];
-            S::face(URf, ULp, a.k, f.half_dx_dt, f.dt_2dx, F);       // face p-31
-#pragma unroll
-            for (int n = 0; n < NC; ++n) sF[w][n][ring(p - 31, kRingF)] = F[n];
-            __syncwarp();
-            double Fm[NC];
-#pragma unroll
-            for (int n = 0; n < NC; ++n) Fm[n] = sF[w][n][ring(p - 32, kRingF)];
-            const int o = p - 32;  // updated cell
-            if (a.do_update && o >= s0 && o < s1) {
-                double Un[NC];
-#pragma unroll
-                for (int n = 0; n < NC; ++n) Un[n] = Uo[n] - f.dtdx * (F[n] - Fm[n]);
-#pragma unroll
-                for (int n = 0; n < NC; ++n) out[o + n * B.out.ns] = Un[n];
-                if (a.ws_max) track_ws(S::speed(Un, a.k), wsmax, nan_seen);
-            }
-            if (fl) {
-                const int fo = o + 1;
-                if (fo >= s0 && (fo < s1 || (fo == s1 && last_seg))) {
-#pragma unroll
-                    for (int n = 0; n < NC; ++n) fl[fo + n * B.flux.ns] = F[n];
-                }
-            }
-#pragma unroll
-            for (int n = 0; n < NC; ++n) sR[w][n][ring(p + 1, kRingR)] = UR[n];
-            copy_state(UL, ULp);
-        }
-        __syncwarp();
-    }
-    if (a.ws_max) reduce_ws(wsmax, nan_seen, a.ws_max);
-}
-
-// ------------------------------------------------- x sweep, shuffle exchange
-// Chunk x0, lane t: load A = U(x0+t+2); cell stage of cell x0+t+1; face
 // x0-31+t from the previous chunk's cell stages; update of cell x0-32+t.
-template <int D, int METHOD, int LIM>
-__global__ void __launch_bounds__(kSweepThreads, kSweepMinBlocks) sweep_x_shfl_kernel(const SweepArgs a)
+template <typename T, int D, int METHOD, int LIM>
+__global__ void __launch_bounds__(kSweepThreads, min_blocks<T>()) sweep_x_kernel(const SweepArgs a)
 {
-    using S = Scheme<D, 0, METHOD, LIM>;
+    using S = Scheme<T, D, 0, METHOD, LIM>;
     constexpr int NC = D + 2;
     constexpr int H = S::kHalo;
-    StepFactors f;
+    StepFactors<T> f;
     if (!step_factors(a, f)) return;
+    const K<T> k(a.k);
     const int lane = threadIdx.x & 31;
     const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
@@ -265,64 +164,64 @@ __global__ void __launch_bounds__(kSweepThreads, kSweepMinBlocks) sweep_x_shfl_k
         const int s1 = min(s0 + a.seglen, B.hi[0] + 1);
         const bool last_seg = (s1 == B.hi[0] + 1);
 
-        const double* __restrict__ in = B.in.p + (long long)(j - B.in.b1) * B.in.js + (long long)(kk - B.in.b2) * B.in.ks;
-        double* __restrict__ out = B.out.p + (long long)(j - B.out.b1) * B.out.js + (long long)(kk - B.out.b2) * B.out.ks;
-        double* __restrict__ fl = B.flux.p ? B.flux.p + (long long)(j - B.flux.b1) * B.flux.js + (long long)(kk - B.flux.b2) * B.flux.ks : nullptr;
+        const T* __restrict__ in = B.in.ptr<T>() + (long long)(j - B.in.b1) * B.in.js + (long long)(kk - B.in.b2) * B.in.ks;
+        T* __restrict__ out = B.out.ptr<T>() + (long long)(j - B.out.b1) * B.out.js + (long long)(kk - B.out.b2) * B.out.ks;
+        T* __restrict__ fl = B.flux.p ? B.flux.ptr<T>() + (long long)(j - B.flux.b1) * B.flux.js + (long long)(kk - B.flux.b2) * B.flux.ks : nullptr;
 
-        auto load = [&](int x0, double (&u)[NC]) {
+        auto load = [&](int x0, T (&u)[NC]) {
             const int xl = x0 + lane + 2;
             if (xl >= s0 - H && xl <= s1 - 1 + H) ld_state(in + (xl - B.in.b0), B.in.ns, u);
             else benign(u);
         };
 
         // carried across chunks
-        double Ap[NC];               // previous chunk's loads
-        double ULp[NC], URp[NC];     // previous chunk's cell stages
-        double URpp[NC];             // the chunk before that (its lane 31 is used)
-        double Fp[NC];               // previous chunk's faces (lane 31 used)
-        double Um2p[NC];             // previous chunk's U(x0-32+t)
+        T Ap[NC];               // previous chunk's loads
+        T ULp[NC], URp[NC];     // previous chunk's cell stages
+        T URpp[NC];             // the chunk before that (its lane 31 is used)
+        T Fp[NC];               // previous chunk's faces (lane 31 used)
+        T Um2p[NC];             // previous chunk's U(x0-32+t)
         benign(Ap);
         benign(ULp);
         benign(URp);
         benign(URpp);
         benign(Um2p);
 #pragma unroll
-        for (int n = 0; n < NC; ++n) Fp[n] = 0.0;
+        for (int n = 0; n < NC; ++n) Fp[n] = T(0);
 
-        double An[NC];
+        T An[NC];
         load(s0 - 32, An);
         for (int x0 = s0 - 32; x0 < s1 + 32; x0 += 32) {
-            double A[NC];
+            T A[NC];
             copy_state(An, A);
             load(x0 + 32, An);
             // cell stage of cell x0+t+1 (this chunk)
-            double Um1[NC], Um2[NC];
+            T Um1[NC], Um2[NC];
             shfl_carry(A, Ap, lane, 1, Um1);  // U(x0+t+1)
             shfl_carry(A, Ap, lane, 2, Um2);  // U(x0+t)
-            double UL[NC], UR[NC];
-            S::cell(Um2, Um1, A, a.k, f.hdtdx, UL, UR);
+            T UL[NC], UR[NC];
+            S::cell(Um2, Um1, A, k, f.hdtdx, UL, UR);
             // face x0-31+t from the previous chunk: UR(x0-32+t), UL(x0-31+t)
-            double URf[NC];
+            T URf[NC];
             shfl_carry(URp, URpp, lane, 1, URf);
-            double F[NC];
-            S::face(URf, ULp, a.k, f.half_dx_dt, f.dt_2dx, F);
+            T F[NC];
+            S::face(URf, ULp, k, f.half_dx_dt, f.dt_2dx, F);
             // update of cell o = x0-32+t from faces o and o+1
-            double Fm[NC];
+            T Fm[NC];
             shfl_carry(F, Fp, lane, 1, Fm);
             const int o = x0 - 32 + lane;
             if (a.do_update && o >= s0 && o < s1) {
-                double Un[NC];
+                T Un[NC];
 #pragma unroll
                 for (int n = 0; n < NC; ++n) Un[n] = Um2p[n] - f.dtdx * (F[n] - Fm[n]);
-                double* po = out + (o - B.out.b0);
+                T* po = out + (o - B.out.b0);
 #pragma unroll
                 for (int n = 0; n < NC; ++n) po[n * B.out.ns] = Un[n];
-                if (a.ws_max) track_ws(S::speed(Un, a.k), wsmax, nan_seen);
+                if (a.ws_max) track_ws((double)S::speed(Un, k), wsmax, nan_seen);
             }
             if (fl) {
                 const int fo = o + 1;
                 if (fo >= s0 && (fo < s1 || (fo == s1 && last_seg))) {
-                    double* pf = fl + (fo - B.flux.b0);
+                    T* pf = fl + (fo - B.flux.b0);
 #pragma unroll
                     for (int n = 0; n < NC; ++n) pf[n * B.flux.ns] = F[n];
                 }
@@ -341,14 +240,15 @@ __global__ void __launch_bounds__(kSweepThreads, kSweepMinBlocks) sweep_x_shfl_k
 // ------------------------------------------------------------ y / z sweeps
 // Iteration o: load U(o+4); cell stage of cell o+2; face o+1 from the cell
 // stages of cells o and o+1 (earlier iterations); update of cell o.
-template <int D, int DIR, int METHOD, int LIM>
-__global__ void __launch_bounds__(kSweepThreads, kSweepMinBlocks) sweep_s_kernel(const SweepArgs a)
+template <typename T, int D, int DIR, int METHOD, int LIM>
+__global__ void __launch_bounds__(kSweepThreads, min_blocks<T>()) sweep_s_kernel(const SweepArgs a)
 {
-    using S = Scheme<D, DIR, METHOD, LIM>;
+    using S = Scheme<T, D, DIR, METHOD, LIM>;
     constexpr int NC = D + 2;
     constexpr int H = S::kHalo;
-    StepFactors f;
+    StepFactors<T> f;
     if (!step_factors(a, f)) return;
+    const K<T> k(a.k);
     const int lane = threadIdx.x & 31;
     const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
@@ -365,7 +265,6 @@ __global__ void __launch_bounds__(kSweepThreads, kSweepMinBlocks) sweep_s_kernel
         const int t2 = (int)(rest / B.ngroup);  // the other transverse index
         const int x = B.lo[0] + grp * 32 + lane;
         const bool active = x <= B.hi[0];
-        const int xc = min(x, B.hi[0]);  // loads of idle lanes read a valid column
         const int s0 = B.lo[DIR] + seg * a.seglen;
         const int s1 = min(s0 + a.seglen, B.hi[DIR] + 1);
         const bool last_seg = (s1 == B.hi[DIR] + 1);
@@ -375,7 +274,7 @@ __global__ void __launch_bounds__(kSweepThreads, kSweepMinBlocks) sweep_s_kernel
         long long ins, outs, fls = 0;
         if (DIR == 1) {
             const int kk = (D == 3) ? B.lo[2] + t2 : 0;
-            inoff = (long long)(xc - B.in.b0) + (long long)(kk - B.in.b2) * B.in.ks - (long long)B.in.b1 * B.in.js;
+            inoff = (long long)(x - B.in.b0) + (long long)(kk - B.in.b2) * B.in.ks - (long long)B.in.b1 * B.in.js;
             outoff = (long long)(x - B.out.b0) + (long long)(kk - B.out.b2) * B.out.ks - (long long)B.out.b1 * B.out.js;
             ins = B.in.js;
             outs = B.out.js;
@@ -385,7 +284,7 @@ __global__ void __launch_bounds__(kSweepThreads, kSweepMinBlocks) sweep_s_kernel
             }
         } else {
             const int jj = B.lo[1] + t2;
-            inoff = (long long)(xc - B.in.b0) + (long long)(jj - B.in.b1) * B.in.js - (long long)B.in.b2 * B.in.ks;
+            inoff = (long long)(x - B.in.b0) + (long long)(jj - B.in.b1) * B.in.js - (long long)B.in.b2 * B.in.ks;
             outoff = (long long)(x - B.out.b0) + (long long)(jj - B.out.b1) * B.out.js - (long long)B.out.b2 * B.out.ks;
             ins = B.in.ks;
             outs = B.out.ks;
@@ -394,56 +293,52 @@ __global__ void __launch_bounds__(kSweepThreads, kSweepMinBlocks) sweep_s_kernel
                 fls = B.flux.ks;
             }
         }
-        const double* __restrict__ in = B.in.p + inoff;
-        double* __restrict__ out = B.out.p + outoff;
+        const T* __restrict__ in = B.in.ptr<T>() + inoff;
+        T* __restrict__ out = B.out.ptr<T>() + outoff;
 
         const int plo = s0 - H, phi = s1 - 1 + H;  // loadable positions
-        auto load = [&](int pos, double (&u)[NC]) {
-            if constexpr (kClampLoads) {
-                ld_state(in + (long long)min(max(pos, plo), phi) * ins, B.in.ns, u);
-            } else {
-                if (pos >= plo && pos <= phi) ld_state(in + (long long)pos * ins, B.in.ns, u);
-                else benign(u);
-            }
+        auto load = [&](int pos, T (&u)[NC]) {
+            if (active && pos >= plo && pos <= phi) ld_state(in + (long long)pos * ins, B.in.ns, u);
+            else benign(u);
         };
 
         // warm-up: cell stages of cells s0-1 and s0
-        double U0[NC], Ua[NC], Ub[NC], Nx[NC], Xm2[NC];
+        T U0[NC], Ua[NC], Ub[NC], Nx[NC], Xm2[NC];
         load(s0 - 2, Xm2);
         load(s0 - 1, U0);
         load(s0, Ua);
         load(s0 + 1, Ub);
         load(s0 + 2, Nx);
-        double URa[NC], URb[NC], ULb[NC], Fo[NC], tmp[NC];
-        S::cell(Xm2, U0, Ua, a.k, f.hdtdx, tmp, URa);   // cell s0-1 -> UR(s0-1)
-        S::cell(U0, Ua, Ub, a.k, f.hdtdx, ULb, URb);    // cell s0   -> UL(s0), UR(s0)
+        T URa[NC], URb[NC], ULb[NC], Fo[NC], tmp[NC];
+        S::cell(Xm2, U0, Ua, k, f.hdtdx, tmp, URa);   // cell s0-1 -> UR(s0-1)
+        S::cell(U0, Ua, Ub, k, f.hdtdx, ULb, URb);    // cell s0   -> UL(s0), UR(s0)
 #pragma unroll
-        for (int n = 0; n < NC; ++n) Fo[n] = 0.0;
+        for (int n = 0; n < NC; ++n) Fo[n] = T(0);
 
         // invariant at iteration o: U0 = U(o), Ua = U(o+1), Ub = U(o+2),
         // Nx = U(o+3), URa = UR(o), URb = UR(o+1), ULb = UL(o+1), Fo = F(o)
 #pragma unroll kMarchUnroll
         for (int o = s0 - 1; o < s1; ++o) {
-            double U3[NC];
+            T U3[NC];
             copy_state(Nx, U3);
             load(o + 4, Nx);
-            double UL2[NC], UR2[NC];
-            S::cell(Ua, Ub, U3, a.k, f.hdtdx, UL2, UR2);   // cell o+2
-            double F1[NC];
-            S::face(URa, ULb, a.k, f.half_dx_dt, f.dt_2dx, F1);  // face o+1
+            T UL2[NC], UR2[NC];
+            S::cell(Ua, Ub, U3, k, f.hdtdx, UL2, UR2);   // cell o+2
+            T F1[NC];
+            S::face(URa, ULb, k, f.half_dx_dt, f.dt_2dx, F1);  // face o+1
             if (o >= s0 && a.do_update && active) {
-                double Un[NC];
+                T Un[NC];
 #pragma unroll
                 for (int n = 0; n < NC; ++n) Un[n] = U0[n] - f.dtdx * (F1[n] - Fo[n]);
-                double* po = out + (long long)o * outs;
+                T* po = out + (long long)o * outs;
 #pragma unroll
                 for (int n = 0; n < NC; ++n) po[n * B.out.ns] = Un[n];
-                if (a.ws_max) track_ws(S::speed(Un, a.k), wsmax, nan_seen);
+                if (a.ws_max) track_ws((double)S::speed(Un, k), wsmax, nan_seen);
             }
             if (B.flux.p && active) {
                 const int fo = o + 1;
                 if (fo >= s0 && (fo < s1 || (fo == s1 && last_seg))) {
-                    double* pf = B.flux.p + floff + (long long)fo * fls;
+                    T* pf = B.flux.ptr<T>() + floff + (long long)fo * fls;
 #pragma unroll
                     for (int n = 0; n < NC; ++n) pf[n * B.flux.ns] = F1[n];
                 }

@@ -1,0 +1,77 @@
+// Launch of the fused sweep kernels: kernel choice (storage type, fast or
+// general path), persistent grid size from the occupancy of the chosen
+// kernel.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <mutex>
+#include <unordered_map>
+
+#include "common.cuh"
+#include "euler.cuh"
+#include "launch.h"
+
+namespace bamrex {
+
+template <typename T>
+const void* pick_sweep_kernel(int D, int dir, int method, int fast_lim);
+extern template const void* pick_sweep_kernel<double>(int, int, int, int);
+extern template const void* pick_sweep_kernel<float>(int, int, int, int);
+
+constexpr int kLaunchThreads = 128;  // kSweepThreads of sweep.cuh
+
+namespace {
+
+const void* pick(int D, int dir, int method, bool fp32, int fast_lim)
+{
+    return fp32 ? pick_sweep_kernel<float>(D, dir, method, fast_lim)
+                : pick_sweep_kernel<double>(D, dir, method, fast_lim);
+}
+
+// Resident blocks per SM of each kernel on the current device.
+int blocks_per_sm(const void* fn)
+{
+    static std::mutex mu;
+    static std::unordered_map<const void*, int> cache[64];
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lock(mu);
+    auto& c = cache[dev & 63];
+    auto it = c.find(fn);
+    if (it != c.end()) return it->second;
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, kLaunchThreads, 0) != cudaSuccess || n < 1) n = 1;
+    c[fn] = n;
+    return n;
+}
+
+}  // namespace
+
+int fast_limiter(int D, int method, const Consts& k)
+{
+    if (method != M_MUSCL || k.root_k != 7 || k.uniform_var != D + 1) return -1;
+    return k.limiter;
+}
+
+cudaError_t launch_sweep(int D, int dir, int method, bool fp32, const SweepArgs& a, cudaStream_t s)
+{
+    const void* fn = pick(D, dir, method, fp32, fast_limiter(D, method, a.k));
+    if (!fn) return cudaErrorInvalidValue;
+    if (a.total_items <= 0) return cudaSuccess;
+    // Persistent grid: every resident warp loops over the items.
+    const long long warps_per_block = kLaunchThreads / 32;
+    const long long need = (a.total_items + warps_per_block - 1) / warps_per_block;
+    const long long cap = (long long)device_sm_count() * blocks_per_sm(fn);
+    const int grid = (int)std::max(1LL, std::min(need, cap));
+    void* args[] = { (void*)&a };
+    return cudaLaunchKernel(fn, dim3(grid), dim3(kLaunchThreads), args, 0, s);
+}
+
+long long sweep_resident_warps(int D, int dir, int method, bool fp32, const Consts& k)
+{
+    const void* fn = pick(D, dir, method, fp32, fast_limiter(D, method, k));
+    if (!fn) return 0;
+    return (long long)device_sm_count() * blocks_per_sm(fn) * (kLaunchThreads / 32);
+}
+
+}  // namespace bamrex

@@ -190,7 +190,8 @@ class Level:
     """One AMR level on the device (all boxes in one box table)."""
 
     def __init__(self, spacedim, dom_lo, dom_hi, prob_lo, prob_hi, boxes, parm: Parm, method=_abi.MUSCL_HANCOCK,
-                 cfl=0.9, ngrow=2, bc_lo=None, bc_hi=None, stream=None, x_segment=0, s_segment=0):
+                 cfl=0.9, ngrow=2, bc_lo=None, bc_hi=None, stream=None, x_segment=0, s_segment=0,
+                 precision=_abi.FP64):
         self.D, self.NC = spacedim, spacedim + 2
         self.boxes = [(tuple(lo) + (0,) * (3 - len(lo)), tuple(hi) + (0,) * (3 - len(hi))) for lo, hi in boxes]
         self.dom_lo = tuple(dom_lo) + (0,) * (3 - len(dom_lo))
@@ -213,6 +214,8 @@ class Level:
         d.parm = parm.to_c()
         d.x_segment = x_segment
         d.s_segment = s_segment
+        d.precision = precision
+        self.precision = precision
         self._h = ctypes.c_void_p()
         check(lib().bamrex_level_create(ctypes.byref(self._h), ctypes.byref(d), _stream_ptr(stream)))
         self.packing = Packing(spacedim, self.dom_lo, self.boxes)
@@ -265,6 +268,12 @@ class Level:
     # the reference's level surface
     def fill_boundary(self):
         self._ck(lib().bamrex_level_fill_boundary(self._h))
+
+    def conserved_sums(self):
+        """sum(U) * cell volume per component (FP64, fixed order)."""
+        out = (ctypes.c_double * self.NC)()
+        self._ck(lib().bamrex_level_conserved_sums(self._h, out))
+        return np.array(list(out))
 
     def advance(self, time, dt, iteration=1, ncycle=1) -> float:
         out = ctypes.c_double()

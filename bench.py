@@ -43,6 +43,7 @@ def parse_args():
     ap.add_argument("--graph", type=int, default=0, help="1: time the CUDA-graph replay instead")
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp32", action="store_true", help="skip the FP32-storage variant")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     return ap.parse_args()
 
@@ -291,6 +292,7 @@ def run_ours(args, rank, world, local_rank):
     ms = ev0.elapsed_time(ev1)
     launches, sweep_ms, sweep_launches = lev.counters()
     lev.set_timing(False)
+    u_fp64 = lev.get_state() if (rank == 0 and not args.no_fp32) else None
     if dist:
         t = torch.tensor([ms], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -328,6 +330,39 @@ def run_ours(args, rank, world, local_rank):
         e2e_ms = float(t.item())
     clocks.stop()
     lev.close()
+
+    # FP32-storage variant on the same workload: throughput, roofline, and
+    # density / energy L1 error against the FP64 path after the same number
+    # of steps (the FP64 path matches the FP64 oracle to 1e-12 per step).
+    fp32 = None
+    if u_fp64 is not None:
+        lev32 = bx.Level(D, (0, 0, 0), hi, [0.0, 0.0], [1.0, 1.0], boxes, bx.Parm(D, limiter=bx.MINBEE),
+                         method=bx.MUSCL_HANCOCK, cfl=0.8, stream=stream, precision=bx.FP32_STORAGE)
+        lev32.set_state(u0)
+        lev32.run(args.warmup, use_graph=use_graph)
+        lev32.set_state(u0)
+        lev32.set_timing(not use_graph)
+        lev32.reset_counters()
+        torch.cuda.synchronize()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            f0.record(stream)
+            lev32.run_async(args.steps, use_graph=use_graph)
+            f1.record(stream)
+        lev32.run_wait()
+        torch.cuda.synchronize()
+        ms32 = f0.elapsed_time(f1)
+        _, sweep_ms32, sweep_n32 = lev32.counters()
+        u32 = lev32.get_state()
+        lev32.close()
+        l1 = lambda a, b: float(np.abs(a - b).sum() / np.abs(b).sum())  # noqa: E731
+        peak, _ = measured_peaks()
+        ach32 = (2 * NC2D * 4 * n * n) / ((sweep_ms32 / sweep_n32) / 1e3) / 1e9 if sweep_n32 else None
+        fp32 = {"value": n * n * args.steps / (ms32 / 1e3), "unit": METRIC, "ms_per_step": ms32 / args.steps,
+                "roofline": {"bound": "hbm", "achieved": ach32, "peak": peak, "unit": "GB/s",
+                             "frac": ach32 / peak if ach32 else None, "algorithmic_bytes_per_cell_sweep": 32},
+                "rel_l1_rho": l1(u32[0], u_fp64[0]), "rel_l1_E": l1(u32[3], u_fp64[3]),
+                "l1_reference": "FP64 path after the same %d steps" % args.steps}
 
     cells = n * n
     value = world * cells * args.steps / (ms / 1e3)
@@ -368,6 +403,7 @@ def run_ours(args, rank, world, local_rank):
                         "bamrex_level_copy_out per step", "steps": args.e2e_steps},
         "gpu_launches": launches,
         "clocks": clocks.summary(t_wall0, t_wall1),
+        "fp32_storage": fp32,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)

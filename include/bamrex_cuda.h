@@ -59,6 +59,10 @@ enum { BAMREX_MINBEE = 0, BAMREX_VAN_LEER = 1, BAMREX_VAN_ALBADA = 2, BAMREX_SUP
  *      with reflect_odd on the normal momentum ---- */
 enum { BAMREX_BC_TRANSMISSIVE = 0, BAMREX_BC_PERIODIC = 1, BAMREX_BC_REFLECTIVE = 2 };
 
+/* ---- level state precision: FP64 (the drop-in), or FP32 storage with FP32
+ *      fluxes (the CFL/dt reduction and the conserved sums stay FP64) ---- */
+enum { BAMREX_FP64 = 0, BAMREX_FP32_STORAGE = 1 };
+
 /* amrex::Box: cell-centred, inclusive lo/hi; unused dimensions are 0..0. */
 typedef struct bamrex_box {
     int lo[3];
@@ -177,6 +181,7 @@ typedef struct bamrex_level_desc {
     bamrex_parm parm;
     int x_segment;          /* cells per warp item in x; 0 = automatic */
     int s_segment;          /* cells per thread item in y/z; 0 = automatic */
+    int precision;          /* BAMREX_FP64 (0) or BAMREX_FP32_STORAGE */
 } bamrex_level_desc;
 
 /* Build the level: allocates the state fabs (two time-level buffers with
@@ -196,6 +201,12 @@ BAMREX_API int bamrex_level_fab(const bamrex_level *level, int box, bamrex_array
  * doubles).  `src`/`dst` may be host (pinned or pageable) or device memory. */
 BAMREX_API int bamrex_level_copy_in(bamrex_level *level, const double *src);
 BAMREX_API int bamrex_level_copy_out(bamrex_level *level, double *dst);
+
+/* Conserved totals sum(U) * cell volume per component over the valid cells
+ * of the current state, accumulated in FP64 in a fixed order (per box, then
+ * boxes in order), so repeated calls agree bit for bit.  totals: NCOMP
+ * doubles.  Synchronises the stream. */
+BAMREX_API int bamrex_level_conserved_sums(bamrex_level *level, double *totals);
 
 /* Wait for all work the level issued on its stream. */
 BAMREX_API int bamrex_level_sync(bamrex_level *level);

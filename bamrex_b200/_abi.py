@@ -102,6 +102,32 @@ class LevelDesc(ctypes.Structure):
     ]
 
 
+MAX_LEVELS = 8
+
+
+class AmrDesc(ctypes.Structure):
+    _fields_ = [
+        ("base", LevelDesc),
+        ("max_level", ctypes.c_int),
+        ("ref_ratio", ctypes.c_int),
+        ("blocking_factor", ctypes.c_int),
+        ("max_grid_size", ctypes.c_int),
+        ("n_error_buf", ctypes.c_int),
+        ("n_proper", ctypes.c_int),
+        ("grid_eff", ctypes.c_double),
+        ("regrid_int", ctypes.c_int),
+        ("do_reflux", ctypes.c_int),
+        ("phigrad_var", ctypes.c_int),
+        ("phigrad_var_is_primv", ctypes.c_int),
+        ("phigrad", ctypes.c_double * MAX_LEVELS),
+        ("max_phigrad_lev", ctypes.c_int),
+        ("phierr_var", ctypes.c_int),
+        ("phierr_var_is_primv", ctypes.c_int),
+        ("phierr", ctypes.c_double * MAX_LEVELS),
+        ("max_phierr_lev", ctypes.c_int),
+    ]
+
+
 # Every symbol include/bamrex_cuda.h declares, with (restype, argtypes).
 _vp, _i, _d, _ll = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_longlong
 _dp = ctypes.POINTER(ctypes.c_double)
@@ -139,6 +165,30 @@ SIGNATURES = {
     "bamrex_level_counters": (_i, [_vp, ctypes.POINTER(_ll), _dp, ctypes.POINTER(_ll)]),
     "bamrex_level_reset_counters": (_i, [_vp]),
     "bamrex_level_sweep_times": (_i, [_vp, _dp, ctypes.POINTER(_ll)]),
+    "bamrex_level_tag": (_i, [_vp, _i, _i, _d, _i, _i, _i, _d, ctypes.c_char_p]),
+    "bamrex_coupling_create": (_i, [ctypes.POINTER(_vp), _vp, _vp, _i]),
+    "bamrex_coupling_destroy": (_i, [_vp]),
+    "bamrex_coupling_save_coarse_old": (_i, [_vp, _d, _d]),
+    "bamrex_coupling_fill_patch": (_i, [_vp, _d]),
+    "bamrex_coupling_fill_coarse_patch": (_i, [_vp]),
+    "bamrex_coupling_reflux": (_i, [_vp]),
+    "bamrex_coupling_avg_down": (_i, [_vp]),
+    "bamrex_coupling_covered_sums": (_i, [_vp, _dp]),
+    "bamrex_coupling_register": (_i, [_vp, _i, _dp, ctypes.POINTER(_i)]),
+    "bamrex_cluster_tags": (_i, [_i, ctypes.POINTER(Box), ctypes.POINTER(_i), ctypes.POINTER(Box), _i, ctypes.c_char_p,
+                                 _i, _i, _i, _i, _i, _d, ctypes.POINTER(Box), _i, ctypes.POINTER(_i)]),
+    "bamrex_amr_create": (_i, [ctypes.POINTER(_vp), ctypes.POINTER(AmrDesc), _vp]),
+    "bamrex_amr_destroy": (_i, [_vp]),
+    "bamrex_amr_last_error": (ctypes.c_char_p, [_vp]),
+    "bamrex_amr_finest_level": (_i, [_vp]),
+    "bamrex_amr_level": (_vp, [_vp, _i]),
+    "bamrex_amr_boxes": (_i, [_vp, _i, ctypes.POINTER(Box), _i, ctypes.POINTER(_i)]),
+    "bamrex_amr_set_level_boxes": (_i, [_vp, _i, ctypes.POINTER(Box), _i]),
+    "bamrex_amr_regrid": (_i, [_vp, _i, _d]),
+    "bamrex_amr_avg_down_all": (_i, [_vp]),
+    "bamrex_amr_coarse_step": (_i, [_vp, _d, _dp, _dp]),
+    "bamrex_amr_dt_level": (_i, [_vp, _dp]),
+    "bamrex_amr_conserved_sums": (_i, [_vp, _dp]),
 }
 
 _LIB = None
@@ -160,7 +210,7 @@ def lib() -> ctypes.CDLL:
     return L
 
 
-def check(rc: int, level_handle=None) -> None:
+def check(rc: int, level_handle=None, amr_handle=None) -> None:
     if rc == OK:
         return
     L = lib()
@@ -169,4 +219,8 @@ def check(rc: int, level_handle=None) -> None:
         lm = L.bamrex_level_last_error(level_handle)
         if lm:
             msg = lm.decode() or msg
+    if amr_handle is not None:
+        am = L.bamrex_amr_last_error(amr_handle)
+        if am:
+            msg = am.decode() or msg
     raise BamrexError(rc, msg or L.bamrex_status_string(rc).decode())

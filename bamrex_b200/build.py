@@ -25,6 +25,9 @@ INCLUDE = os.path.join(ROOT, "include")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
          "--expt-relaxed-constexpr", "-I", INCLUDE, "-I", CSRC]
+# Per-file extra flags: the AMR coupling kernels round every product and sum
+# separately so a CPU restatement reproduces them exactly.
+FILE_FLAGS = {"amr_kernels.cu": ["-fmad=false"]}
 
 
 def nvcc() -> str:
@@ -60,7 +63,7 @@ def build(force: bool = False, jobs: int = 0, verbose: bool = False) -> str:
     def compile_one(src):
         obj = os.path.join(BUILD, os.path.basename(src)[:-3] + ".o")
         if force or _stale(obj, [src] + deps):
-            cmd = [cc] + ARCH + FLAGS + ["-c", src, "-o", obj]
+            cmd = [cc] + ARCH + FLAGS + FILE_FLAGS.get(os.path.basename(src), []) + ["-c", src, "-o", obj]
             r = subprocess.run(cmd, capture_output=True, text=True)
             if r.returncode != 0:
                 raise RuntimeError("nvcc failed for %s:\n%s\n%s" % (src, r.stdout, r.stderr))

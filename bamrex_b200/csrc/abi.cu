@@ -15,12 +15,15 @@
 
 #include "bamrex_cuda.h"
 #include "launch.h"
+#include "level_impl.h"
 
 using namespace bamrex;
 
 namespace {
-
 thread_local std::string g_last_error;
+}  // namespace
+
+namespace bamrex {
 
 int fail(int code, const std::string& msg)
 {
@@ -34,17 +37,19 @@ int cuda_fail(cudaError_t e, const char* what)
     return BAMREX_ERR_CUDA;
 }
 
-#define BX_CK(call)                                         \
-    do {                                                    \
-        cudaError_t e_ = (call);                            \
-        if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
-    } while (0)
+const char* last_error_text() { return g_last_error.c_str(); }
 
-#define BX_TRY(call)                  \
-    do {                              \
-        int rc_ = (call);             \
-        if (rc_ != BAMREX_OK) return rc_; \
-    } while (0)
+size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+}  // namespace bamrex
+
+int bamrex_level::set_err(int code)
+{
+    err = g_last_error;
+    return code;
+}
+
+namespace {
 
 bool method_supported(int m)
 {
@@ -181,8 +186,6 @@ int choose_seglen(int dir, const std::vector<bamrex_box>& boxes, long long resid
     }
     return cand[ncand - 1];
 }
-
-size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
 }  // namespace
 
@@ -416,119 +419,57 @@ extern "C" int bamrex_conservative_update(int spacedim, const bamrex_box* bx, ba
 // ======================================================================
 // level
 // ======================================================================
-struct bamrex_level {
-    int D = 0, NC = 0, ngrow = 0, method = 0;
-    bool fp32 = false;   // FP32-storage variant
-    size_t esize = 8;    // bytes per stored value
-    double cfl = 0.9;
-    bamrex_parm parm;
-    Consts k;
-    bamrex_box domain;
-    double dx[3] = { 1, 1, 1 };
-    int bc_lo[3] = { 0, 0, 0 }, bc_hi[3] = { 0, 0, 0 };
-    std::vector<bamrex_box> boxes;
-    cudaStream_t stream = nullptr;
-    bool own_stream = false;
-    int device = 0;
+namespace bamrex {
 
-    // device memory (one arena)
-    char* arena = nullptr;
-    char* state[2] = { nullptr, nullptr };
-    double* d_box_sums = nullptr;  // nboxes x NC, conserved sums
-    std::vector<FabDev> fab[2];
-    FabDev* d_fab[2] = { nullptr, nullptr };
-    SweepBox* d_sweep[3][2] = {};
-    long long items[3] = { 0, 0, 0 };
-    int seglen[3] = { 0, 0, 0 };
-    GhostOp* d_ghost[3] = { nullptr, nullptr, nullptr };
-    int nghost[3] = { 0, 0, 0 };
-    long long ghost_cells[3] = { 0, 0, 0 };
-    PackBox* d_pack = nullptr;
-    long long ncells = 0;
-    double* staging = nullptr;
-    StepScalars* d_scal = nullptr;
-    StepScalars* h_scal = nullptr;  // pinned
-    int cur = 0;
-    bool ws_valid = false;
-
-    // accounting
-    long long launches = 0;
-    bool timing = false;
-    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> events;
-    std::vector<int> event_dir;
-    size_t ev_used = 0;
-    double sweep_ms = 0.0;
-    long long sweep_launches = 0;
-    double dir_ms[3] = { 0, 0, 0 };
-    long long dir_launches[3] = { 0, 0, 0 };
-
-    cudaGraphExec_t graph[2] = { nullptr, nullptr };
-    bool run_pending = false;
-    int run_start_parity = 0;
-    std::string err;
-
-    int set_err(int code) {
-        err = g_last_error;
-        return code;
+void BoxIndex::build(const bamrex_box& dom, const std::vector<bamrex_box>& bxs, int D_)
+{
+    D = D_;
+    boxes = &bxs;
+    for (int d = 0; d < 3; ++d) {
+        lo[d] = dom.lo[d];
+        int mx = 1;
+        for (const auto& b : bxs) mx = std::max(mx, b.hi[d] - b.lo[d] + 1);
+        bs[d] = mx;
+        nb[d] = (dom.hi[d] - dom.lo[d] + 1 + mx - 1) / mx;
+        if (nb[d] < 1) nb[d] = 1;
     }
-};
-
-namespace {
-
-// Uniform bucket grid over the domain for box-intersection queries.
-struct BoxIndex {
-    int D;
-    int lo[3], bs[3], nb[3];
-    std::vector<std::vector<int>> buckets;
-    const std::vector<bamrex_box>* boxes;
-
-    void build(const bamrex_box& dom, const std::vector<bamrex_box>& bxs, int D_)
-    {
-        D = D_;
-        boxes = &bxs;
-        for (int d = 0; d < 3; ++d) {
-            lo[d] = dom.lo[d];
-            int mx = 1;
-            for (const auto& b : bxs) mx = std::max(mx, b.hi[d] - b.lo[d] + 1);
-            bs[d] = mx;
-            nb[d] = (dom.hi[d] - dom.lo[d] + 1 + mx - 1) / mx;
-            if (nb[d] < 1) nb[d] = 1;
-        }
-        buckets.assign((size_t)nb[0] * nb[1] * nb[2], {});
-        for (int i = 0; i < (int)bxs.size(); ++i) {
-            int a[3], c[3];
-            for (int d = 0; d < 3; ++d) {
-                a[d] = std::max(0, (bxs[i].lo[d] - lo[d]) / bs[d]);
-                c[d] = std::min(nb[d] - 1, (bxs[i].hi[d] - lo[d]) / bs[d]);
-            }
-            for (int z = a[2]; z <= c[2]; ++z)
-                for (int y = a[1]; y <= c[1]; ++y)
-                    for (int x = a[0]; x <= c[0]; ++x) buckets[((size_t)z * nb[1] + y) * nb[0] + x].push_back(i);
-        }
-    }
-
-    // boxes intersecting region r
-    void query(const int* rlo, const int* rhi, std::vector<int>& out) const
-    {
-        out.clear();
+    buckets.assign((size_t)nb[0] * nb[1] * nb[2], {});
+    for (int i = 0; i < (int)bxs.size(); ++i) {
         int a[3], c[3];
         for (int d = 0; d < 3; ++d) {
-            a[d] = std::max(0, (rlo[d] - lo[d]) / bs[d]);
-            c[d] = std::min(nb[d] - 1, (rhi[d] - lo[d]) / bs[d]);
-            if (rhi[d] < lo[d]) return;
-            if (a[d] > c[d]) return;
+            a[d] = std::max(0, (bxs[i].lo[d] - lo[d]) / bs[d]);
+            c[d] = std::min(nb[d] - 1, (bxs[i].hi[d] - lo[d]) / bs[d]);
         }
         for (int z = a[2]; z <= c[2]; ++z)
             for (int y = a[1]; y <= c[1]; ++y)
-                for (int x = a[0]; x <= c[0]; ++x)
-                    for (int i : buckets[((size_t)z * nb[1] + y) * nb[0] + x]) {
-                        const auto& b = (*boxes)[i];
-                        bool hit = true;
-                        for (int d = 0; d < 3; ++d) hit = hit && b.lo[d] <= rhi[d] && rlo[d] <= b.hi[d];
-                        if (hit && std::find(out.begin(), out.end(), i) == out.end()) out.push_back(i);
-                    }
+                for (int x = a[0]; x <= c[0]; ++x) buckets[((size_t)z * nb[1] + y) * nb[0] + x].push_back(i);
     }
-};
+}
+
+void BoxIndex::query(const int* rlo, const int* rhi, std::vector<int>& out) const
+{
+    out.clear();
+    int a[3], c[3];
+    for (int d = 0; d < 3; ++d) {
+        if (rhi[d] < lo[d] || rhi[d] < rlo[d]) return;
+        a[d] = std::max(0, (rlo[d] - lo[d]) / bs[d]);
+        c[d] = std::min(nb[d] - 1, (rhi[d] - lo[d]) / bs[d]);
+        if (a[d] > c[d]) return;
+    }
+    for (int z = a[2]; z <= c[2]; ++z)
+        for (int y = a[1]; y <= c[1]; ++y)
+            for (int x = a[0]; x <= c[0]; ++x)
+                for (int i : buckets[((size_t)z * nb[1] + y) * nb[0] + x]) {
+                    const auto& b = (*boxes)[i];
+                    bool hit = true;
+                    for (int d = 0; d < 3; ++d) hit = hit && b.lo[d] <= rhi[d] && rlo[d] <= b.hi[d];
+                    if (hit && std::find(out.begin(), out.end(), i) == out.end()) out.push_back(i);
+                }
+}
+
+}  // namespace bamrex
+
+namespace {
 
 // Ghost-fill ops of direction d for every box: the two ghost slabs of
 // width ngrow across the box's valid extent in the other directions.
@@ -655,6 +596,10 @@ long long ops_cells(const std::vector<GhostOp>& ops)
     return o.cell_begin + (long long)(o.hi[0] - o.lo[0] + 1) * (o.hi[1] - o.lo[1] + 1) * (o.hi[2] - o.lo[2] + 1);
 }
 
+}  // namespace
+
+namespace bamrex {
+
 int level_launch(bamrex_level* L, cudaError_t e, const char* what)
 {
     if (e != cudaSuccess) return L->set_err(cuda_fail(e, what));
@@ -669,6 +614,10 @@ int level_fill(bamrex_level* L, int d, int parity, const StepScalars* scal)
                                              L->stream),
                         "ghost fill");
 }
+
+}  // namespace bamrex
+
+namespace {
 
 int level_sweep(bamrex_level* L, int d, int parity, double dt_host, const StepScalars* scal, bool reduce_ws,
                 bool allow_timing)
@@ -698,14 +647,30 @@ int level_sweep(bamrex_level* L, int d, int parity, double dt_host, const StepSc
     return BAMREX_OK;
 }
 
-// One split step starting from buffer `parity`; the result lands in
-// parity ^ (D & 1).  dt from the host (scal == nullptr) or from the device.
+}  // namespace
+
+namespace bamrex {
+
 int level_step(bamrex_level* L, int parity, double dt_host, StepScalars* scal, bool allow_timing)
 {
     BX_TRY(level_fill(L, 0, parity, scal));
     int p = parity;
     for (int d = 0; d < L->D; ++d) {
         BX_TRY(level_sweep(L, d, p, dt_host, scal, d == L->D - 1, allow_timing));
+        if (!L->reg_tasks[d].empty()) {
+            // Flux-register faces of this sweep, from its input (buffer p,
+            // which the next sweep overwrites).  The flux is scaled by dt and
+            // the face area as AmrLevelAdv::advance does before
+            // FineAdd/CrseInit (Source/AmrLevelAdv_advance.cpp:192-210).
+            if (scal) return L->set_err(fail(BAMREX_ERR_UNSUPPORTED, "flux registers need a host time step"));
+            double scale = dt_host;
+            for (int e = 0; e < L->D; ++e)
+                if (e != d) scale *= L->dx[e];
+            for (const RegisterTask& t : L->reg_tasks[d])
+                BX_TRY(level_launch(L, launch_register_faces(L->D, d, L->method, L->fp32, L->k, L->d_fab[p], t, L->NC,
+                                                             dt_host, L->dx[d], scale, L->stream),
+                                    "flux register faces"));
+        }
         p ^= 1;
         if (d + 1 < L->D) BX_TRY(level_fill(L, d + 1, p, scal));
     }
@@ -714,7 +679,7 @@ int level_step(bamrex_level* L, int parity, double dt_host, StepScalars* scal, b
     return BAMREX_OK;
 }
 
-}  // namespace
+}  // namespace bamrex
 
 extern "C" int bamrex_level_create(bamrex_level** out, const bamrex_level_desc* desc, void* stream)
 {
@@ -761,6 +726,7 @@ extern "C" int bamrex_level_create(bamrex_level** out, const bamrex_level_desc* 
         L->bc_lo[d] = desc->bc_lo[d];
         L->bc_hi[d] = desc->bc_hi[d];
         L->dx[d] = d < D ? (desc->prob_hi[d] - desc->prob_lo[d]) / (double)(desc->domain.hi[d] - desc->domain.lo[d] + 1) : 1.0;
+        L->prob_lo[d] = d < D ? desc->prob_lo[d] : 0.0;
     }
     L->boxes.assign(desc->boxes, desc->boxes + desc->nboxes);
     L->ncells = covered;
@@ -870,6 +836,7 @@ extern "C" int bamrex_level_create(bamrex_level** out, const bamrex_level_desc* 
         off = align_up(off + bytes, 256);
         return o;
     };
+    L->state_bytes = (size_t)per_buf * L->esize;
     const size_t o_state0 = take((size_t)per_buf * L->esize);
     const size_t o_state1 = take((size_t)per_buf * L->esize);
     const size_t o_sums = take(sizeof(double) * nb * L->NC);

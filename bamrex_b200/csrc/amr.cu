@@ -1,0 +1,1395 @@
+// Host side of the AMR glue: the coarse/fine coupling of two levels (flux
+// register faces, coarse patches for fine ghost interpolation, average_down
+// and reflux tables), error-estimation tagging, Berger-Rigoutsos grid
+// generation and the subcycled hierarchy time step.  Tables are built once
+// per grid configuration; every step then runs a fixed set of kernels on the
+// levels' stream.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <new>
+#include <set>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "amr.h"
+#include "bamrex_cuda.h"
+#include "level_impl.h"
+
+using namespace bamrex;
+
+namespace {
+
+int floor_div(int a, int b) { return a >= 0 ? a / b : -((-a + b - 1) / b); }
+
+long long box_volume(const bamrex_box& b)
+{
+    return (long long)(b.hi[0] - b.lo[0] + 1) * (b.hi[1] - b.lo[1] + 1) * (b.hi[2] - b.lo[2] + 1);
+}
+
+bool box_empty(const bamrex_box& b) { return b.hi[0] < b.lo[0] || b.hi[1] < b.lo[1] || b.hi[2] < b.lo[2]; }
+
+bamrex_box intersect(const bamrex_box& a, const bamrex_box& b)
+{
+    bamrex_box r;
+    for (int d = 0; d < 3; ++d) {
+        r.lo[d] = std::max(a.lo[d], b.lo[d]);
+        r.hi[d] = std::min(a.hi[d], b.hi[d]);
+    }
+    return r;
+}
+
+bamrex_box coarsen(const bamrex_box& b, int r, int D)
+{
+    bamrex_box c = b;
+    for (int d = 0; d < D; ++d) {
+        c.lo[d] = floor_div(b.lo[d], r);
+        c.hi[d] = floor_div(b.hi[d], r);
+    }
+    return c;
+}
+
+bamrex_box refine(const bamrex_box& b, int r, int D)
+{
+    bamrex_box c = b;
+    for (int d = 0; d < D; ++d) {
+        c.lo[d] = b.lo[d] * r;
+        c.hi[d] = (b.hi[d] + 1) * r - 1;
+    }
+    return c;
+}
+
+// a minus b as disjoint boxes
+void subtract(const bamrex_box& a, const bamrex_box& b, std::vector<bamrex_box>& out)
+{
+    const bamrex_box x = intersect(a, b);
+    if (box_empty(x)) {
+        out.push_back(a);
+        return;
+    }
+    bamrex_box rest = a;
+    for (int d = 0; d < 3; ++d) {
+        if (rest.lo[d] < x.lo[d]) {
+            bamrex_box p = rest;
+            p.hi[d] = x.lo[d] - 1;
+            out.push_back(p);
+            rest.lo[d] = x.lo[d];
+        }
+        if (rest.hi[d] > x.hi[d]) {
+            bamrex_box p = rest;
+            p.lo[d] = x.hi[d] + 1;
+            out.push_back(p);
+            rest.hi[d] = x.hi[d];
+        }
+    }
+}
+
+// region minus every box of the index
+void subtract_boxes(const bamrex_box& region, const BoxIndex& idx, const std::vector<bamrex_box>& boxes,
+                    std::vector<bamrex_box>& out)
+{
+    std::vector<int> hits;
+    idx.query(region.lo, region.hi, hits);
+    std::sort(hits.begin(), hits.end());
+    std::vector<bamrex_box> cur{ region }, next;
+    for (int h : hits) {
+        next.clear();
+        for (const auto& p : cur) subtract(p, boxes[h], next);
+        cur.swap(next);
+        if (cur.empty()) break;
+    }
+    out.insert(out.end(), cur.begin(), cur.end());
+}
+
+int find_containing(const BoxIndex& idx, const std::vector<bamrex_box>& boxes, const int* c)
+{
+    std::vector<int> hits;
+    idx.query(c, c, hits);
+    int best = -1;
+    for (int h : hits) {
+        const bamrex_box& b = boxes[h];
+        if (c[0] >= b.lo[0] && c[0] <= b.hi[0] && c[1] >= b.lo[1] && c[1] <= b.hi[1] && c[2] >= b.lo[2] &&
+            c[2] <= b.hi[2])
+            best = (best < 0) ? h : std::min(best, h);
+    }
+    return best;
+}
+
+}  // namespace
+
+struct bamrex_coupling {
+    bamrex_level* crse = nullptr;
+    bamrex_level* fine = nullptr;
+    int r = 2, D = 0, NC = 0;
+    char* arena = nullptr;
+    // coarse old time level
+    char* old_state = nullptr;
+    FabDev* d_old_fab = nullptr;
+    bool old_valid = false;
+    double t_old = 0, t_new = 0;
+    // interpolation: [0] coarse/fine ghosts, [1] whole fine boxes (FillCoarsePatch)
+    CfRegion* d_reg_set[2] = { nullptr, nullptr };
+    int nreg_set[2] = { 0, 0 };
+    long long ncell_set[2] = { 0, 0 };
+    CfPatchCell* d_pcell_set[2] = { nullptr, nullptr };
+    long long npatch_set[2] = { 0, 0 };
+    double* d_patch_set[2] = { nullptr, nullptr };
+    // flux registers
+    int nslots[3] = { 0, 0, 0 };
+    FaceRec* d_cfaces[3] = { nullptr, nullptr, nullptr };
+    FaceRec* d_ffaces[3] = { nullptr, nullptr, nullptr };
+    RefluxRec* d_rr[3] = { nullptr, nullptr, nullptr };
+    double* d_reg[3] = { nullptr, nullptr, nullptr };
+    // average_down and covered sums
+    AvgOp* d_avg = nullptr;
+    int navg = 0;
+    long long navg_cells = 0;
+    PackBox* d_cov_box = nullptr;
+    FabDev* d_cov_fab[2] = { nullptr, nullptr };
+    double* d_cov_sums = nullptr;
+};
+
+namespace {
+
+// Map a coarse cell into the domain by the boundary rules (periodic shift,
+// reflection with the normal momentum negated, or extrapolation).
+void map_into_domain(const bamrex_level* L, int* c, int& negmask)
+{
+    for (int d = 0; d < L->D; ++d) {
+        const int lo = L->domain.lo[d], hi = L->domain.hi[d], len = hi - lo + 1;
+        if (c[d] >= lo && c[d] <= hi) continue;
+        const int bc = c[d] < lo ? L->bc_lo[d] : L->bc_hi[d];
+        if (bc == BAMREX_BC_PERIODIC) {
+            c[d] = lo + (((c[d] - lo) % len) + len) % len;
+        } else if (bc == BAMREX_BC_REFLECTIVE) {
+            c[d] = c[d] < lo ? 2 * lo - 1 - c[d] : 2 * hi + 1 - c[d];
+            negmask ^= 1 << (1 + d);
+        } else {
+            c[d] = c[d] < lo ? lo : hi;
+        }
+    }
+}
+
+// Coarse patches (coarsened region grown by one coarse cell) of a set of
+// fine regions.
+int build_patches(const bamrex_coupling* C, std::vector<CfRegion>& regs, std::vector<CfPatchCell>& cells,
+                  const BoxIndex& cidx)
+{
+    const bamrex_level* Lc = C->crse;
+    long long pacc = 0, cacc = 0;
+    for (auto& R : regs) {
+        bamrex_box w;
+        for (int d = 0; d < 3; ++d) {
+            w.lo[d] = R.lo[d] + R.shift[d];
+            w.hi[d] = R.hi[d] + R.shift[d];
+        }
+        bamrex_box p = coarsen(w, C->r, C->D);
+        for (int d = 0; d < C->D; ++d) {
+            p.lo[d] -= 1;
+            p.hi[d] += 1;
+        }
+        for (int d = 0; d < 3; ++d) {
+            R.plo[d] = p.lo[d];
+            R.pn[d] = p.hi[d] - p.lo[d] + 1;
+        }
+        R.patch_begin = pacc;
+        R.cell_begin = cacc;
+        pacc += box_volume(p);
+        cacc += (long long)(R.hi[0] - R.lo[0] + 1) * (R.hi[1] - R.lo[1] + 1) * (R.hi[2] - R.lo[2] + 1);
+        for (int k = p.lo[2]; k <= p.hi[2]; ++k)
+            for (int j = p.lo[1]; j <= p.hi[1]; ++j)
+                for (int i = p.lo[0]; i <= p.hi[0]; ++i) {
+                    int c[3] = { i, j, k };
+                    int neg = 0;
+                    map_into_domain(Lc, c, neg);
+                    const int b = find_containing(cidx, Lc->boxes, c);
+                    if (b < 0)
+                        return fail(BAMREX_ERR_ARG,
+                                    "fine level not properly nested: coarse cell (" + std::to_string(c[0]) + "," +
+                                        std::to_string(c[1]) + "," + std::to_string(c[2]) + ") is not a valid coarse cell");
+                    CfPatchCell pc;
+                    pc.box = b;
+                    pc.i = c[0];
+                    pc.j = c[1];
+                    pc.k = c[2];
+                    pc.negmask = neg;
+                    cells.push_back(pc);
+                }
+    }
+    return BAMREX_OK;
+}
+
+CfRegion make_region(int dst, const bamrex_box& b, const int* shift)
+{
+    CfRegion R;
+    std::memset(&R, 0, sizeof(R));
+    R.dst = dst;
+    for (int d = 0; d < 3; ++d) {
+        R.lo[d] = b.lo[d] - shift[d];
+        R.hi[d] = b.hi[d] - shift[d];
+        R.shift[d] = shift[d];
+    }
+    return R;
+}
+
+// The fine ghost regions to interpolate: face slabs of depth ngrow of every
+// fine box, inside the domain (or the periodic image outside it), minus the
+// fine boxes.
+void build_ghost_regions(const bamrex_level* Lf, const BoxIndex& fidx, std::vector<CfRegion>& regs)
+{
+    const int g = Lf->ngrow;
+    for (int b = 0; b < (int)Lf->boxes.size(); ++b) {
+        const bamrex_box& B = Lf->boxes[b];
+        for (int d = 0; d < Lf->D; ++d) {
+            const int dlo = Lf->domain.lo[d], dhi = Lf->domain.hi[d], len = dhi - dlo + 1;
+            for (int side = 0; side < 2; ++side) {
+                bamrex_box slab = B;
+                if (side == 0) {
+                    slab.lo[d] = B.lo[d] - g;
+                    slab.hi[d] = B.lo[d] - 1;
+                } else {
+                    slab.lo[d] = B.hi[d] + 1;
+                    slab.hi[d] = B.hi[d] + g;
+                }
+                bamrex_box in = slab;
+                in.lo[d] = std::max(slab.lo[d], dlo);
+                in.hi[d] = std::min(slab.hi[d], dhi);
+                const int zero[3] = { 0, 0, 0 };
+                if (in.lo[d] <= in.hi[d]) {
+                    std::vector<bamrex_box> pieces;
+                    subtract_boxes(in, fidx, Lf->boxes, pieces);
+                    for (const auto& p : pieces) regs.push_back(make_region(b, p, zero));
+                }
+                const int bc = side == 0 ? Lf->bc_lo[d] : Lf->bc_hi[d];
+                if (bc != BAMREX_BC_PERIODIC) continue;  // physical ghosts: the level's own boundary fill
+                bamrex_box out = slab;
+                if (side == 0) out.hi[d] = std::min(slab.hi[d], dlo - 1);
+                else out.lo[d] = std::max(slab.lo[d], dhi + 1);
+                if (out.lo[d] > out.hi[d]) continue;
+                int shift[3] = { 0, 0, 0 };
+                shift[d] = side == 0 ? len : -len;
+                bamrex_box img = out;
+                img.lo[d] += shift[d];
+                img.hi[d] += shift[d];
+                std::vector<bamrex_box> pieces;
+                subtract_boxes(img, fidx, Lf->boxes, pieces);
+                for (const auto& p : pieces) regs.push_back(make_region(b, p, shift));
+            }
+        }
+    }
+}
+
+// Flux-register slots of direction d.
+int build_register(const bamrex_coupling* C, int d, const BoxIndex& fidx, const BoxIndex& cidx,
+                   std::vector<FaceRec>& cf, std::vector<FaceRec>& ff, std::vector<RefluxRec>& rr)
+{
+    const bamrex_level* Lf = C->fine;
+    const bamrex_level* Lc = C->crse;
+    const int r = C->r, D = C->D;
+    const int dlo = Lf->domain.lo[d], dhi = Lf->domain.hi[d], len = dhi - dlo + 1;
+    std::set<std::tuple<int, int, int>> seen;
+    for (int b = 0; b < (int)Lf->boxes.size(); ++b) {
+        const bamrex_box& B = Lf->boxes[b];
+        for (int side = 0; side < 2; ++side) {
+            bamrex_box layer = B;
+            layer.lo[d] = layer.hi[d] = side == 0 ? B.lo[d] - 1 : B.hi[d] + 1;
+            int shift = 0;
+            if (layer.lo[d] < dlo || layer.lo[d] > dhi) {
+                const int bc = side == 0 ? Lf->bc_lo[d] : Lf->bc_hi[d];
+                if (bc != BAMREX_BC_PERIODIC) continue;  // domain face: no coarse neighbour
+                shift = side == 0 ? len : -len;
+                layer.lo[d] += shift;
+                layer.hi[d] += shift;
+            }
+            std::vector<bamrex_box> pieces;
+            subtract_boxes(layer, fidx, Lf->boxes, pieces);
+            const int fface = side == 0 ? B.lo[d] : B.hi[d] + 1;
+            for (const auto& p : pieces) {
+                const bamrex_box cp = coarsen(p, r, D);
+                for (int k = cp.lo[2]; k <= cp.hi[2]; ++k)
+                    for (int j = cp.lo[1]; j <= cp.hi[1]; ++j)
+                        for (int i = cp.lo[0]; i <= cp.hi[0]; ++i) {
+                            int c[3] = { i, j, k };
+                            const int cb = find_containing(cidx, Lc->boxes, c);
+                            if (cb < 0) return fail(BAMREX_ERR_ARG, "fine level not properly nested (flux register)");
+                            if (!seen.insert(std::make_tuple(i, j, k)).second)
+                                return fail(BAMREX_ERR_ARG,
+                                            "fine boxes closer than two coarse cells: a coarse cell borders the fine "
+                                            "region on both sides");
+                            RefluxRec q;
+                            q.box = cb;
+                            q.i = i;
+                            q.j = j;
+                            q.k = k;
+                            q.sign = side == 0 ? -1 : 1;
+                            rr.push_back(q);
+                            FaceRec f;
+                            f.box = cb;
+                            f.i = i;
+                            f.j = j;
+                            f.k = k;
+                            const int cface = c[d] + (side == 0 ? 1 : 0);
+                            if (d == 0) f.i = cface;
+                            else if (d == 1) f.j = cface;
+                            else f.k = cface;
+                            cf.push_back(f);
+                            // the r^(D-1) fine faces under this coarse face,
+                            // transverse index fastest in x, then y, then z
+                            const int tz = (D > 2 && d != 2) ? r : 1;
+                            const int ty = (D > 1 && d != 1) ? r : 1;
+                            const int tx = (d != 0) ? r : 1;
+                            for (int a2 = 0; a2 < tz; ++a2)
+                                for (int a1 = 0; a1 < ty; ++a1)
+                                    for (int a0 = 0; a0 < tx; ++a0) {
+                                        FaceRec g;
+                                        g.box = b;
+                                        g.i = d == 0 ? fface : c[0] * r + a0;
+                                        g.j = d == 1 ? fface : (D > 1 ? c[1] * r + a1 : 0);
+                                        g.k = d == 2 ? fface : (D > 2 ? c[2] * r + a2 : 0);
+                                        ff.push_back(g);
+                                    }
+                        }
+            }
+        }
+    }
+    return BAMREX_OK;
+}
+
+void drop_tasks(bamrex_level* L, const double* reg)
+{
+    if (!L) return;
+    for (int d = 0; d < 3; ++d) {
+        auto& v = L->reg_tasks[d];
+        v.erase(std::remove_if(v.begin(), v.end(), [&](const RegisterTask& t) { return t.reg == reg; }), v.end());
+    }
+}
+
+int cpl_launch(bamrex_coupling* C, cudaError_t e, const char* what)
+{
+    if (e != cudaSuccess) return cuda_fail(e, what);
+    C->fine->launches++;
+    return BAMREX_OK;
+}
+
+}  // namespace
+
+extern "C" int bamrex_coupling_create(bamrex_coupling** out, bamrex_level* crse, bamrex_level* fine, int ref_ratio)
+{
+    if (!out || !crse || !fine) return fail(BAMREX_ERR_ARG, "NULL argument");
+    *out = nullptr;
+    const int D = crse->D, r = ref_ratio;
+    if (r != 2 && r != 4) return fail(BAMREX_ERR_ARG, "ref_ratio must be 2 or 4");
+    if (fine->D != D || fine->fp32 != crse->fp32 || fine->method != crse->method)
+        return fail(BAMREX_ERR_ARG, "coarse and fine levels differ in dimension, precision or method");
+    if (fine->stream != crse->stream) return fail(BAMREX_ERR_ARG, "coarse and fine levels must share a stream");
+    if (fine->ngrow < 2) return fail(BAMREX_ERR_ARG, "fine ngrow must be >= 2");
+    for (int d = 0; d < D; ++d) {
+        if (fine->domain.lo[d] != crse->domain.lo[d] * r || fine->domain.hi[d] != (crse->domain.hi[d] + 1) * r - 1)
+            return fail(BAMREX_ERR_ARG, "fine domain is not the refined coarse domain");
+        if (fine->bc_lo[d] != crse->bc_lo[d] || fine->bc_hi[d] != crse->bc_hi[d])
+            return fail(BAMREX_ERR_ARG, "coarse and fine boundary conditions differ");
+    }
+    for (const auto& B : fine->boxes)
+        for (int d = 0; d < D; ++d)
+            if (B.lo[d] % r != 0 || (B.hi[d] + 1) % r != 0)
+                return fail(BAMREX_ERR_ARG, "fine boxes must be aligned to the refinement ratio");
+
+    std::unique_ptr<bamrex_coupling> C(new (std::nothrow) bamrex_coupling());
+    if (!C) return fail(BAMREX_ERR_OOM, "host allocation failed");
+    C->crse = crse;
+    C->fine = fine;
+    C->r = r;
+    C->D = D;
+    C->NC = crse->NC;
+
+    BoxIndex fidx, cidx;
+    fidx.build(fine->domain, fine->boxes, D);
+    cidx.build(crse->domain, crse->boxes, D);
+
+    // interpolation regions and their coarse patches
+    std::vector<CfRegion> regs[2];
+    std::vector<CfPatchCell> pcells[2];
+    build_ghost_regions(fine, fidx, regs[0]);
+    const int zero[3] = { 0, 0, 0 };
+    for (int b = 0; b < (int)fine->boxes.size(); ++b) regs[1].push_back(make_region(b, fine->boxes[b], zero));
+    for (int s = 0; s < 2; ++s) BX_TRY(build_patches(C.get(), regs[s], pcells[s], cidx));
+
+    // flux registers
+    std::vector<FaceRec> cf[3], ff[3];
+    std::vector<RefluxRec> rr[3];
+    for (int d = 0; d < D; ++d) BX_TRY(build_register(C.get(), d, fidx, cidx, cf[d], ff[d], rr[d]));
+
+    // average_down
+    std::vector<AvgOp> avg;
+    {
+        long long acc = 0;
+        std::vector<int> hits;
+        for (int b = 0; b < (int)fine->boxes.size(); ++b) {
+            const bamrex_box cb = coarsen(fine->boxes[b], r, D);
+            cidx.query(cb.lo, cb.hi, hits);
+            std::sort(hits.begin(), hits.end());
+            long long covered = 0;
+            for (int h : hits) {
+                const bamrex_box x = intersect(cb, crse->boxes[h]);
+                if (box_empty(x)) continue;
+                AvgOp op;
+                std::memset(&op, 0, sizeof(op));
+                op.crse = h;
+                op.fine = b;
+                for (int d = 0; d < 3; ++d) {
+                    op.lo[d] = x.lo[d];
+                    op.hi[d] = x.hi[d];
+                }
+                op.cell_begin = acc;
+                acc += box_volume(x);
+                covered += box_volume(x);
+                avg.push_back(op);
+            }
+            if (covered != box_volume(cb)) return fail(BAMREX_ERR_ARG, "fine level not covered by the coarse level");
+        }
+        C->navg = (int)avg.size();
+        C->navg_cells = acc;
+    }
+    std::vector<PackBox> cov(avg.size());
+    std::vector<FabDev> covfab[2];
+    for (size_t i = 0; i < avg.size(); ++i) {
+        for (int d = 0; d < 3; ++d) {
+            cov[i].lo[d] = avg[i].lo[d];
+            cov[i].hi[d] = avg[i].hi[d];
+        }
+        cov[i].cell_begin = avg[i].cell_begin;
+        for (int p = 0; p < 2; ++p) covfab[p].push_back(crse->fab[p][avg[i].crse]);
+    }
+
+    // one arena
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        const size_t o = off;
+        off = align_up(off + std::max<size_t>(bytes, 1), 256);
+        return o;
+    };
+    const int nbc = (int)crse->boxes.size();
+    const size_t o_old = take(crse->state_bytes);
+    const size_t o_oldfab = take(sizeof(FabDev) * nbc);
+    size_t o_reg[2], o_pc[2], o_patch[2];
+    for (int s = 0; s < 2; ++s) {
+        o_reg[s] = take(sizeof(CfRegion) * regs[s].size());
+        o_pc[s] = take(sizeof(CfPatchCell) * pcells[s].size());
+        o_patch[s] = take(sizeof(double) * C->NC * pcells[s].size());
+    }
+    size_t o_cf[3] = {}, o_ff[3] = {}, o_rr[3] = {}, o_rg[3] = {};
+    for (int d = 0; d < D; ++d) {
+        o_cf[d] = take(sizeof(FaceRec) * cf[d].size());
+        o_ff[d] = take(sizeof(FaceRec) * ff[d].size());
+        o_rr[d] = take(sizeof(RefluxRec) * rr[d].size());
+        o_rg[d] = take(sizeof(double) * C->NC * rr[d].size());
+    }
+    const size_t o_avg = take(sizeof(AvgOp) * avg.size());
+    const size_t o_cov = take(sizeof(PackBox) * cov.size());
+    const size_t o_covf0 = take(sizeof(FabDev) * cov.size());
+    const size_t o_covf1 = take(sizeof(FabDev) * cov.size());
+    const size_t o_covs = take(sizeof(double) * C->NC * std::max<size_t>(1, cov.size()));
+    cudaError_t e = cudaMalloc((void**)&C->arena, off);
+    if (e != cudaSuccess) return fail(BAMREX_ERR_OOM, std::string("cudaMalloc of the coupling failed: ") + cudaGetErrorString(e));
+    char* A = C->arena;
+    C->old_state = A + o_old;
+    C->d_old_fab = (FabDev*)(A + o_oldfab);
+    for (int s = 0; s < 2; ++s) {
+        C->d_reg_set[s] = (CfRegion*)(A + o_reg[s]);
+        C->nreg_set[s] = (int)regs[s].size();
+        C->ncell_set[s] = regs[s].empty() ? 0
+                                          : regs[s].back().cell_begin + (long long)(regs[s].back().hi[0] - regs[s].back().lo[0] + 1) *
+                                                                          (regs[s].back().hi[1] - regs[s].back().lo[1] + 1) *
+                                                                          (regs[s].back().hi[2] - regs[s].back().lo[2] + 1);
+        C->d_pcell_set[s] = (CfPatchCell*)(A + o_pc[s]);
+        C->npatch_set[s] = (long long)pcells[s].size();
+        C->d_patch_set[s] = (double*)(A + o_patch[s]);
+    }
+    for (int d = 0; d < D; ++d) {
+        C->nslots[d] = (int)rr[d].size();
+        C->d_cfaces[d] = (FaceRec*)(A + o_cf[d]);
+        C->d_ffaces[d] = (FaceRec*)(A + o_ff[d]);
+        C->d_rr[d] = (RefluxRec*)(A + o_rr[d]);
+        C->d_reg[d] = (double*)(A + o_rg[d]);
+    }
+    C->d_avg = (AvgOp*)(A + o_avg);
+    C->d_cov_box = (PackBox*)(A + o_cov);
+    C->d_cov_fab[0] = (FabDev*)(A + o_covf0);
+    C->d_cov_fab[1] = (FabDev*)(A + o_covf1);
+    C->d_cov_sums = (double*)(A + o_covs);
+
+    std::vector<FabDev> oldfab = crse->fab[0];
+    for (int b = 0; b < nbc; ++b)
+        oldfab[b].p = C->old_state + ((char*)crse->fab[0][b].p - crse->state[0]);
+    auto up = [&](void* dst, const void* src, size_t bytes) -> cudaError_t {
+        return bytes ? cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice) : cudaSuccess;
+    };
+    e = up(C->d_old_fab, oldfab.data(), sizeof(FabDev) * nbc);
+    for (int s = 0; s < 2 && e == cudaSuccess; ++s) {
+        e = up(C->d_reg_set[s], regs[s].data(), sizeof(CfRegion) * regs[s].size());
+        if (e == cudaSuccess) e = up(C->d_pcell_set[s], pcells[s].data(), sizeof(CfPatchCell) * pcells[s].size());
+    }
+    for (int d = 0; d < D && e == cudaSuccess; ++d) {
+        e = up(C->d_cfaces[d], cf[d].data(), sizeof(FaceRec) * cf[d].size());
+        if (e == cudaSuccess) e = up(C->d_ffaces[d], ff[d].data(), sizeof(FaceRec) * ff[d].size());
+        if (e == cudaSuccess) e = up(C->d_rr[d], rr[d].data(), sizeof(RefluxRec) * rr[d].size());
+        if (e == cudaSuccess) e = cudaMemset(C->d_reg[d], 0, sizeof(double) * C->NC * rr[d].size());
+    }
+    if (e == cudaSuccess) e = up(C->d_avg, avg.data(), sizeof(AvgOp) * avg.size());
+    if (e == cudaSuccess) e = up(C->d_cov_box, cov.data(), sizeof(PackBox) * cov.size());
+    for (int p = 0; p < 2 && e == cudaSuccess; ++p) e = up(C->d_cov_fab[p], covfab[p].data(), sizeof(FabDev) * cov.size());
+    if (e != cudaSuccess) {
+        cudaFree(C->arena);
+        return cuda_fail(e, "coupling table upload");
+    }
+    const int per_slot = D == 1 ? 1 : (D == 2 ? r : r * r);
+    for (int d = 0; d < D; ++d) {
+        if (!C->nslots[d]) continue;
+        RegisterTask tc;
+        tc.faces = C->d_cfaces[d];
+        tc.nslots = C->nslots[d];
+        tc.per_slot = 1;
+        tc.reg = C->d_reg[d];
+        tc.mode = 0;
+        crse->reg_tasks[d].push_back(tc);
+        RegisterTask tf = tc;
+        tf.faces = C->d_ffaces[d];
+        tf.per_slot = per_slot;
+        tf.mode = 1;
+        fine->reg_tasks[d].push_back(tf);
+    }
+    *out = C.release();
+    return BAMREX_OK;
+}
+
+extern "C" int bamrex_coupling_destroy(bamrex_coupling* C)
+{
+    if (!C) return BAMREX_OK;
+    if (C->crse && C->crse->stream) cudaStreamSynchronize(C->crse->stream);
+    for (int d = 0; d < 3; ++d) {
+        if (!C->d_reg[d]) continue;
+        drop_tasks(C->crse, C->d_reg[d]);
+        drop_tasks(C->fine, C->d_reg[d]);
+    }
+    if (C->arena) cudaFree(C->arena);
+    delete C;
+    return BAMREX_OK;
+}
+
+extern "C" int bamrex_coupling_save_coarse_old(bamrex_coupling* C, double t_old, double t_new)
+{
+    if (!C) return fail(BAMREX_ERR_ARG, "NULL coupling");
+    if (!(t_new > t_old)) return fail(BAMREX_ERR_ARG, "t_new must exceed t_old");
+    bamrex_level* Lc = C->crse;
+    BX_CK(cudaMemcpyAsync(C->old_state, Lc->state[Lc->cur], Lc->state_bytes, cudaMemcpyDeviceToDevice, Lc->stream));
+    C->old_valid = true;
+    C->t_old = t_old;
+    C->t_new = t_new;
+    return BAMREX_OK;
+}
+
+static int run_interp(bamrex_coupling* C, int set, int mode, double a_old, double a_new)
+{
+    bamrex_level* Lc = C->crse;
+    bamrex_level* Lf = C->fine;
+    if (!C->ncell_set[set]) return BAMREX_OK;
+    BX_TRY(cpl_launch(C, launch_cf_gather(C->NC, Lc->fp32, C->d_pcell_set[set], C->npatch_set[set], C->d_old_fab,
+                                          Lc->d_fab[Lc->cur], mode, a_old, a_new, C->d_patch_set[set], Lc->stream),
+                      "coarse patch gather"));
+    CfInterpArgs a;
+    a.regions = C->d_reg_set[set];
+    a.nregions = C->nreg_set[set];
+    a.ncells = C->ncell_set[set];
+    a.patch = C->d_patch_set[set];
+    a.npatch = C->npatch_set[set];
+    a.fine0 = Lf->d_fab[0];
+    a.fine1 = Lf->d_fab[1];
+    a.D = C->D;
+    a.NC = C->NC;
+    a.ratio = C->r;
+    BX_TRY(cpl_launch(C, launch_cf_interp(Lc->fp32, a, Lc->stream), "coarse/fine interpolation"));
+    Lf->ws_valid = false;
+    return BAMREX_OK;
+}
+
+extern "C" int bamrex_coupling_fill_patch(bamrex_coupling* C, double time)
+{
+    if (!C) return fail(BAMREX_ERR_ARG, "NULL coupling");
+    int mode = 1;
+    double a_old = 0.0, a_new = 1.0;
+    if (C->old_valid) {
+        const double span = C->t_new - C->t_old;
+        const double teps = 1e-3 * span;
+        if (time < C->t_old - teps || time > C->t_new + teps)
+            return fail(BAMREX_ERR_ARG, "fill_patch time outside the coarse old/new interval");
+        if (std::fabs(time - C->t_old) < teps) {
+            mode = 0;
+        } else if (std::fabs(time - C->t_new) < teps) {
+            mode = 1;
+        } else {
+            mode = 2;
+            a_old = (C->t_new - time) / span;
+            a_new = (time - C->t_old) / span;
+        }
+    }
+    return run_interp(C, 0, mode, a_old, a_new);
+}
+
+extern "C" int bamrex_coupling_fill_coarse_patch(bamrex_coupling* C)
+{
+    if (!C) return fail(BAMREX_ERR_ARG, "NULL coupling");
+    return run_interp(C, 1, 1, 0.0, 1.0);
+}
+
+extern "C" int bamrex_coupling_reflux(bamrex_coupling* C)
+{
+    if (!C) return fail(BAMREX_ERR_ARG, "NULL coupling");
+    bamrex_level* Lc = C->crse;
+    double vol = 1.0;
+    for (int d = 0; d < C->D; ++d) vol *= Lc->dx[d];
+    for (int d = 0; d < C->D; ++d)
+        BX_TRY(cpl_launch(C, launch_reflux(C->NC, Lc->fp32, C->d_rr[d], C->nslots[d], C->d_reg[d], vol, Lc->d_fab[Lc->cur],
+                                           Lc->stream),
+                          "reflux"));
+    Lc->ws_valid = false;
+    return BAMREX_OK;
+}
+
+extern "C" int bamrex_coupling_avg_down(bamrex_coupling* C)
+{
+    if (!C) return fail(BAMREX_ERR_ARG, "NULL coupling");
+    bamrex_level* Lc = C->crse;
+    bamrex_level* Lf = C->fine;
+    BX_TRY(cpl_launch(C, launch_avg_down(C->D, C->NC, C->r, Lc->fp32, C->d_avg, C->navg, C->navg_cells, Lc->d_fab[Lc->cur],
+                                         Lf->d_fab[Lf->cur], Lc->stream),
+                      "average_down"));
+    Lc->ws_valid = false;
+    return BAMREX_OK;
+}
+
+extern "C" int bamrex_coupling_covered_sums(bamrex_coupling* C, double* sums)
+{
+    if (!C || !sums) return fail(BAMREX_ERR_ARG, "NULL argument");
+    bamrex_level* Lc = C->crse;
+    const int n = C->navg;
+    for (int m = 0; m < C->NC; ++m) sums[m] = 0.0;
+    if (!n) return BAMREX_OK;
+    BX_TRY(cpl_launch(C, launch_box_sums(C->NC, Lc->fp32, C->d_cov_fab[Lc->cur], C->d_cov_box, n, C->d_cov_sums, Lc->stream),
+                      "covered sums"));
+    std::vector<double> h((size_t)n * C->NC);
+    BX_CK(cudaMemcpyAsync(h.data(), C->d_cov_sums, h.size() * sizeof(double), cudaMemcpyDeviceToHost, Lc->stream));
+    BX_CK(cudaStreamSynchronize(Lc->stream));
+    double vol = 1.0;
+    for (int d = 0; d < C->D; ++d) vol *= Lc->dx[d];
+    for (int m = 0; m < C->NC; ++m) {
+        double s = 0.0;
+        for (int b = 0; b < n; ++b) s += h[(size_t)b * C->NC + m];
+        sums[m] = s * vol;
+    }
+    return BAMREX_OK;
+}
+
+extern "C" int bamrex_coupling_register(bamrex_coupling* C, int dir, double* reg, int* nslots)
+{
+    if (!C || !nslots || dir < 0 || dir >= C->D) return fail(BAMREX_ERR_ARG, "bad argument");
+    *nslots = C->nslots[dir];
+    if (!reg || !C->nslots[dir]) return BAMREX_OK;
+    BX_CK(cudaMemcpyAsync(reg, C->d_reg[dir], sizeof(double) * C->NC * C->nslots[dir], cudaMemcpyDeviceToHost,
+                          C->crse->stream));
+    BX_CK(cudaStreamSynchronize(C->crse->stream));
+    return BAMREX_OK;
+}
+
+extern "C" int bamrex_level_tag(bamrex_level* L, int grad_var, int grad_var_is_primv, double grad_threshold,
+                                int do_err, int err_var, int err_var_is_primv, double phierr, char* tags)
+{
+    if (!L || !tags) return fail(BAMREX_ERR_ARG, "NULL argument");
+    const bool do_grad = grad_threshold > 0;
+    if ((do_grad && (grad_var < 0 || grad_var >= L->NC)) || (do_err && (err_var < 0 || err_var >= L->NC)))
+        return L->set_err(fail(BAMREX_ERR_ARG, "tagging variable index outside the state vector"));
+    for (int d = 0; d < L->D; ++d) BX_TRY(level_fill(L, d, L->cur, nullptr));
+    TagSpec spec;
+    spec.do_err = do_err ? 1 : 0;
+    spec.err_var = err_var;
+    spec.err_primv = err_var_is_primv ? 1 : 0;
+    spec.err_thr = phierr;
+    spec.do_grad = do_grad ? 1 : 0;
+    spec.grad_var = grad_var;
+    spec.grad_primv = grad_var_is_primv ? 1 : 0;
+    spec.grad_thr = grad_threshold;
+    char* dtags = reinterpret_cast<char*>(L->staging);  // ncells bytes <= staging size
+    BX_TRY(level_launch(L, launch_tag(L->D, L->fp32, L->d_fab[L->cur], L->d_pack, (int)L->boxes.size(), L->ncells, L->k,
+                                      spec, dtags, L->stream),
+                        "tagging"));
+    cudaError_t e = cudaMemcpyAsync(tags, dtags, (size_t)L->ncells, cudaMemcpyDeviceToHost, L->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(L->stream);
+    if (e != cudaSuccess) return L->set_err(cuda_fail(e, "tag readback"));
+    return BAMREX_OK;
+}
+
+// ======================================================================
+// grid generation
+// ======================================================================
+namespace {
+
+struct Mask3 {
+    int n[3] = { 1, 1, 1 };
+    std::vector<unsigned char> v;
+    void init(const int* nn, unsigned char x)
+    {
+        for (int d = 0; d < 3; ++d) n[d] = nn[d];
+        v.assign((size_t)n[0] * n[1] * n[2], x);
+    }
+    unsigned char& at(int i, int j, int k) { return v[((size_t)k * n[1] + j) * n[0] + i]; }
+    unsigned char at(int i, int j, int k) const { return v[((size_t)k * n[1] + j) * n[0] + i]; }
+};
+
+// out(x) = OR / AND of in over x-rad..x+rad along dim d; positions outside
+// the domain wrap (periodic) or take `outside`.
+void sweep_max(Mask3& m, int d, int rad, bool periodic, bool use_and, unsigned char outside)
+{
+    if (rad <= 0) return;
+    Mask3 o = m;
+    const int n = m.n[d];
+    for (int k = 0; k < m.n[2]; ++k)
+        for (int j = 0; j < m.n[1]; ++j)
+            for (int i = 0; i < m.n[0]; ++i) {
+                int c[3] = { i, j, k };
+                const int x0 = c[d];
+                unsigned char acc = use_and ? 1 : 0;
+                for (int s = -rad; s <= rad; ++s) {
+                    int x = x0 + s;
+                    unsigned char v;
+                    if (x < 0 || x >= n) {
+                        if (periodic) {
+                            x = ((x % n) + n) % n;
+                            c[d] = x;
+                            v = m.at(c[0], c[1], c[2]);
+                        } else {
+                            v = outside;
+                        }
+                    } else {
+                        c[d] = x;
+                        v = m.at(c[0], c[1], c[2]);
+                    }
+                    if (use_and) acc = acc && v;
+                    else acc = acc || v;
+                }
+                o.at(i, j, k) = acc;
+            }
+    m.v.swap(o.v);
+}
+
+struct Cluster {
+    const Mask3* tags;
+    double eff;
+    int D;
+    std::vector<bamrex_box> out;
+
+    long long count(const bamrex_box& b) const
+    {
+        long long c = 0;
+        for (int k = b.lo[2]; k <= b.hi[2]; ++k)
+            for (int j = b.lo[1]; j <= b.hi[1]; ++j)
+                for (int i = b.lo[0]; i <= b.hi[0]; ++i) c += tags->at(i, j, k) ? 1 : 0;
+        return c;
+    }
+
+    bool shrink(bamrex_box& b) const
+    {
+        int lo[3] = { b.hi[0] + 1, b.hi[1] + 1, b.hi[2] + 1 }, hi[3] = { b.lo[0] - 1, b.lo[1] - 1, b.lo[2] - 1 };
+        bool any = false;
+        for (int k = b.lo[2]; k <= b.hi[2]; ++k)
+            for (int j = b.lo[1]; j <= b.hi[1]; ++j)
+                for (int i = b.lo[0]; i <= b.hi[0]; ++i)
+                    if (tags->at(i, j, k)) {
+                        any = true;
+                        const int c[3] = { i, j, k };
+                        for (int d = 0; d < 3; ++d) {
+                            lo[d] = std::min(lo[d], c[d]);
+                            hi[d] = std::max(hi[d], c[d]);
+                        }
+                    }
+        if (!any) return false;
+        for (int d = 0; d < 3; ++d) {
+            b.lo[d] = lo[d];
+            b.hi[d] = hi[d];
+        }
+        return true;
+    }
+
+    void run(bamrex_box b, int depth)
+    {
+        if (!shrink(b)) return;
+        const long long vol = box_volume(b), nt = count(b);
+        bool all_unit = true;
+        for (int d = 0; d < D; ++d) all_unit = all_unit && b.hi[d] == b.lo[d];
+        if ((double)nt >= eff * (double)vol || all_unit || depth > 64) {
+            out.push_back(b);
+            return;
+        }
+        // signatures along each direction
+        std::vector<long long> sig[3];
+        for (int d = 0; d < D; ++d) sig[d].assign(b.hi[d] - b.lo[d] + 1, 0);
+        for (int k = b.lo[2]; k <= b.hi[2]; ++k)
+            for (int j = b.lo[1]; j <= b.hi[1]; ++j)
+                for (int i = b.lo[0]; i <= b.hi[0]; ++i)
+                    if (tags->at(i, j, k)) {
+                        const int c[3] = { i, j, k };
+                        for (int d = 0; d < D; ++d) sig[d][c[d] - b.lo[d]]++;
+                    }
+        int best_d = -1, best_cut = 0;
+        // 1) a hole (zero signature) closest to the middle
+        long long best_score = -1;
+        for (int d = 0; d < D; ++d) {
+            const int n = (int)sig[d].size();
+            for (int x = 1; x < n - 1; ++x)
+                if (sig[d][x] == 0) {
+                    const long long score = (long long)n * 4 - std::abs(2 * x - n);
+                    if (score > best_score) {
+                        best_score = score;
+                        best_d = d;
+                        best_cut = x;
+                    }
+                }
+        }
+        if (best_d < 0) {
+            // 2) the strongest inflection of the signature (sign change of
+            // its second difference)
+            long long best_jump = 0;
+            for (int d = 0; d < D; ++d) {
+                const int n = (int)sig[d].size();
+                if (n < 4) continue;
+                std::vector<long long> lap(n, 0);
+                for (int x = 1; x < n - 1; ++x) lap[x] = sig[d][x - 1] - 2 * sig[d][x] + sig[d][x + 1];
+                for (int x = 1; x < n - 2; ++x) {
+                    if ((lap[x] > 0 && lap[x + 1] < 0) || (lap[x] < 0 && lap[x + 1] > 0)) {
+                        const long long jump = std::llabs(lap[x] - lap[x + 1]);
+                        if (jump > best_jump) {
+                            best_jump = jump;
+                            best_d = d;
+                            best_cut = x + 1;
+                        }
+                    }
+                }
+            }
+        }
+        if (best_d < 0) {
+            // 3) halve the longest side
+            int len = 0;
+            for (int d = 0; d < D; ++d)
+                if (b.hi[d] - b.lo[d] + 1 > len) {
+                    len = b.hi[d] - b.lo[d] + 1;
+                    best_d = d;
+                }
+            best_cut = len / 2;
+        }
+        bamrex_box a = b, c = b;
+        a.hi[best_d] = b.lo[best_d] + best_cut - 1;
+        c.lo[best_d] = b.lo[best_d] + best_cut;
+        run(a, depth + 1);
+        run(c, depth + 1);
+    }
+};
+
+// Split b until every piece lies inside `allowed` (pieces with no allowed
+// cell are dropped).
+void clip_to_allowed(const Mask3& allowed, const bamrex_box& b, int D, std::vector<bamrex_box>& out)
+{
+    long long nin = 0;
+    for (int k = b.lo[2]; k <= b.hi[2]; ++k)
+        for (int j = b.lo[1]; j <= b.hi[1]; ++j)
+            for (int i = b.lo[0]; i <= b.hi[0]; ++i) nin += allowed.at(i, j, k) ? 1 : 0;
+    if (nin == 0) return;
+    if (nin == box_volume(b)) {
+        out.push_back(b);
+        return;
+    }
+    int best_d = 0, len = 0;
+    for (int d = 0; d < D; ++d)
+        if (b.hi[d] - b.lo[d] + 1 > len) {
+            len = b.hi[d] - b.lo[d] + 1;
+            best_d = d;
+        }
+    bamrex_box a = b, c = b;
+    a.hi[best_d] = b.lo[best_d] + len / 2 - 1;
+    c.lo[best_d] = b.lo[best_d] + len / 2;
+    clip_to_allowed(allowed, a, D, out);
+    clip_to_allowed(allowed, c, D, out);
+}
+
+void chop(const bamrex_box& b, int D, int mgs, std::vector<bamrex_box>& out)
+{
+    for (int d = 0; d < D; ++d) {
+        const int len = b.hi[d] - b.lo[d] + 1;
+        if (len > mgs) {
+            const int pieces = (len + mgs - 1) / mgs;
+            const int base = len / pieces, extra = len % pieces;
+            int lo = b.lo[d];
+            for (int p = 0; p < pieces; ++p) {
+                bamrex_box q = b;
+                q.lo[d] = lo;
+                q.hi[d] = lo + base + (p < extra ? 1 : 0) - 1;
+                lo = q.hi[d] + 1;
+                chop(q, D, mgs, out);
+            }
+            return;
+        }
+    }
+    out.push_back(b);
+}
+
+}  // namespace
+
+extern "C" int bamrex_cluster_tags(int D, const bamrex_box* domain, const int* periodic, const bamrex_box* boxes,
+                                   int nboxes, const char* tags, int ref_ratio, int blocking_factor,
+                                   int max_grid_size, int n_error_buf, int n_proper, double grid_eff,
+                                   bamrex_box* out, int max_out, int* nout)
+{
+    if (!domain || !boxes || !tags || !nout || D < 1 || D > 3 || nboxes < 1) return fail(BAMREX_ERR_ARG, "bad argument");
+    if (ref_ratio != 2 && ref_ratio != 4) return fail(BAMREX_ERR_ARG, "ref_ratio must be 2 or 4");
+    if (blocking_factor < 2 * ref_ratio || blocking_factor % (2 * ref_ratio) != 0)
+        return fail(BAMREX_ERR_ARG, "blocking_factor must be a multiple of 2 * ref_ratio");
+    if (max_grid_size < blocking_factor || max_grid_size % blocking_factor != 0)
+        return fail(BAMREX_ERR_ARG, "max_grid_size must be a multiple of blocking_factor");
+    if (n_error_buf < 0 || n_proper < 0 || !(grid_eff > 0 && grid_eff <= 1))
+        return fail(BAMREX_ERR_ARG, "bad n_error_buf / n_proper / grid_eff");
+    const int c = blocking_factor / ref_ratio;  // level-l cells per blocked cell
+    int n[3] = { 1, 1, 1 }, nt[3] = { 1, 1, 1 };
+    for (int d = 0; d < D; ++d) {
+        n[d] = domain->hi[d] - domain->lo[d] + 1;
+        if (n[d] % c != 0) return fail(BAMREX_ERR_ARG, "domain not divisible by blocking_factor / ref_ratio");
+        nt[d] = n[d] / c;
+    }
+    const int dl[3] = { domain->lo[0], domain->lo[1], domain->lo[2] };
+    Mask3 tag, cov;
+    tag.init(n, 0);
+    cov.init(n, 0);
+    long long off = 0;
+    for (int b = 0; b < nboxes; ++b) {
+        const bamrex_box& B = boxes[b];
+        for (int k = B.lo[2]; k <= B.hi[2]; ++k)
+            for (int j = B.lo[1]; j <= B.hi[1]; ++j)
+                for (int i = B.lo[0]; i <= B.hi[0]; ++i) {
+                    const int x = i - dl[0], y = j - dl[1], z = k - dl[2];
+                    if (x < 0 || y < 0 || z < 0 || x >= n[0] || y >= n[1] || z >= n[2])
+                        return fail(BAMREX_ERR_ARG, "box outside the domain");
+                    cov.at(x, y, z) = 1;
+                    if (tags[off]) tag.at(x, y, z) = 1;
+                    ++off;
+                }
+    }
+    // buffer the tags, restrict them to the proper nesting region
+    for (int d = 0; d < D; ++d) sweep_max(tag, d, n_error_buf, periodic && periodic[d], false, 0);
+    Mask3 allowed = cov;
+    for (int d = 0; d < D; ++d) sweep_max(allowed, d, n_proper, periodic && periodic[d], true, 1);
+    for (size_t q = 0; q < tag.v.size(); ++q) tag.v[q] = tag.v[q] && allowed.v[q];
+    // blocked space: a blocked cell is allowed if its whole footprint is,
+    // tagged if any footprint cell is
+    Mask3 btag, ball;
+    btag.init(nt, 0);
+    ball.init(nt, 1);
+    for (int k = 0; k < n[2]; ++k)
+        for (int j = 0; j < n[1]; ++j)
+            for (int i = 0; i < n[0]; ++i) {
+                const int I = i / (D > 0 ? c : 1), J = D > 1 ? j / c : j, K = D > 2 ? k / c : k;
+                if (tag.at(i, j, k)) btag.at(I, J, K) = 1;
+                if (!allowed.at(i, j, k)) ball.at(I, J, K) = 0;
+            }
+    for (size_t q = 0; q < btag.v.size(); ++q) btag.v[q] = btag.v[q] && ball.v[q];
+    Cluster cl;
+    cl.tags = &btag;
+    cl.eff = grid_eff;
+    cl.D = D;
+    bamrex_box all;
+    for (int d = 0; d < 3; ++d) {
+        all.lo[d] = 0;
+        all.hi[d] = nt[d] - 1;
+    }
+    cl.run(all, 0);
+    std::vector<bamrex_box> clipped, chopped;
+    for (const auto& b : cl.out) clip_to_allowed(ball, b, D, clipped);
+    const int mgs_t = max_grid_size / blocking_factor;
+    for (const auto& b : clipped) chop(b, D, mgs_t, chopped);
+    std::sort(chopped.begin(), chopped.end(), [](const bamrex_box& a, const bamrex_box& b) {
+        return std::make_tuple(a.lo[2], a.lo[1], a.lo[0]) < std::make_tuple(b.lo[2], b.lo[1], b.lo[0]);
+    });
+    *nout = (int)chopped.size();
+    if ((int)chopped.size() > max_out) return fail(BAMREX_ERR_ARG, "output box array too small");
+    for (size_t q = 0; q < chopped.size(); ++q) {
+        bamrex_box f;
+        for (int d = 0; d < 3; ++d) {
+            if (d < D) {
+                f.lo[d] = (chopped[q].lo[d] * c + dl[d]) * ref_ratio;
+                f.hi[d] = ((chopped[q].hi[d] + 1) * c + dl[d]) * ref_ratio - 1;
+            } else {
+                f.lo[d] = f.hi[d] = 0;
+            }
+        }
+        out[q] = f;
+    }
+    return BAMREX_OK;
+}
+
+// ======================================================================
+// hierarchy
+// ======================================================================
+struct bamrex_amr {
+    bamrex_amr_desc desc;
+    int D = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    std::vector<bamrex_level*> levels;
+    std::vector<bamrex_coupling*> cpl;  // cpl[l] couples l-1 and l
+    std::vector<double> dt_level;
+    int steps = 0;
+    bool have_dt = false;
+    std::string err;
+    int set_err(int code)
+    {
+        err = last_error_text();
+        return code;
+    }
+};
+
+namespace {
+
+int amr_fail(bamrex_amr* A, int code, const std::string& msg) { return A->set_err(fail(code, msg)); }
+
+#define AMR_TRY(A, call)                           \
+    do {                                           \
+        int rc_ = (call);                          \
+        if (rc_ != BAMREX_OK) return (A)->set_err(rc_); \
+    } while (0)
+
+int make_level(bamrex_amr* A, int lev, const std::vector<bamrex_box>& boxes, bamrex_level** out)
+{
+    bamrex_level_desc d = A->desc.base;
+    int f = 1;
+    for (int l = 0; l < lev; ++l) f *= A->desc.ref_ratio;
+    for (int q = 0; q < A->D; ++q) {
+        d.domain.lo[q] = A->desc.base.domain.lo[q] * f;
+        d.domain.hi[q] = (A->desc.base.domain.hi[q] + 1) * f - 1;
+    }
+    d.boxes = boxes.data();
+    d.nboxes = (int)boxes.size();
+    return bamrex_level_create(out, &d, A->stream);
+}
+
+void drop_levels_above(bamrex_amr* A, int lev)
+{
+    while ((int)A->levels.size() > lev + 1) {
+        const int l = (int)A->levels.size() - 1;
+        bamrex_coupling_destroy(A->cpl[l]);
+        bamrex_level_destroy(A->levels[l]);
+        A->cpl.pop_back();
+        A->levels.pop_back();
+    }
+    A->dt_level.resize(A->levels.size(), A->dt_level.empty() ? 0.0 : A->dt_level.back());
+}
+
+bool same_boxes(const std::vector<bamrex_box>& a, const std::vector<bamrex_box>& b)
+{
+    if (a.size() != b.size()) return false;
+    for (size_t i = 0; i < a.size(); ++i)
+        for (int d = 0; d < 3; ++d)
+            if (a[i].lo[d] != b[i].lo[d] || a[i].hi[d] != b[i].hi[d]) return false;
+    return true;
+}
+
+int set_level(bamrex_amr* A, int lev, const std::vector<bamrex_box>& boxes)
+{
+    const int finest = (int)A->levels.size() - 1;
+    if (lev < 1 || lev > finest + 1 || lev > A->desc.max_level) return amr_fail(A, BAMREX_ERR_ARG, "level out of range");
+    const int bf = A->desc.blocking_factor;
+    for (const auto& b : boxes)
+        for (int d = 0; d < A->D; ++d)
+            if (b.lo[d] % bf != 0 || (b.hi[d] + 1) % bf != 0)
+                return amr_fail(A, BAMREX_ERR_ARG, "fine boxes must be aligned to blocking_factor");
+    if (lev <= finest && same_boxes(boxes, A->levels[lev]->boxes)) {
+        drop_levels_above(A, lev);
+        return BAMREX_OK;
+    }
+    bamrex_level* L = nullptr;
+    AMR_TRY(A, make_level(A, lev, boxes, &L));
+    bamrex_coupling* C = nullptr;
+    int rc = bamrex_coupling_create(&C, A->levels[lev - 1], L, A->desc.ref_ratio);
+    if (rc != BAMREX_OK) {
+        bamrex_level_destroy(L);
+        return A->set_err(rc);
+    }
+    rc = bamrex_coupling_fill_coarse_patch(C);
+    if (rc == BAMREX_OK && lev <= finest) {
+        // old data of this level where the new boxes overlap it
+        bamrex_level* O = A->levels[lev];
+        std::vector<GhostOp> ops;
+        const int nnew = (int)L->boxes.size();
+        for (int b = 0; b < nnew; ++b)
+            for (int s = 0; s < (int)O->boxes.size(); ++s) {
+                const bamrex_box x = intersect(L->boxes[b], O->boxes[s]);
+                if (box_empty(x)) continue;
+                GhostOp op;
+                std::memset(&op, 0, sizeof(op));
+                op.dst = b;
+                op.src = nnew + s;
+                for (int d = 0; d < 3; ++d) {
+                    op.lo[d] = x.lo[d];
+                    op.hi[d] = x.hi[d];
+                    op.mul[d] = 1;
+                }
+                ops.push_back(op);
+            }
+        long long acc = 0;
+        for (auto& op : ops) {
+            op.cell_begin = acc;
+            acc += (long long)(op.hi[0] - op.lo[0] + 1) * (op.hi[1] - op.lo[1] + 1) * (op.hi[2] - op.lo[2] + 1);
+        }
+        if (!ops.empty()) {
+            std::vector<FabDev> tab = L->fab[L->cur];
+            tab.insert(tab.end(), O->fab[O->cur].begin(), O->fab[O->cur].end());
+            void* dmem = nullptr;
+            const size_t tb = sizeof(FabDev) * tab.size(), ob = sizeof(GhostOp) * ops.size();
+            cudaError_t e = cudaMalloc(&dmem, align_up(tb, 256) + ob);
+            if (e == cudaSuccess) e = cudaMemcpy(dmem, tab.data(), tb, cudaMemcpyHostToDevice);
+            GhostOp* dops = (GhostOp*)((char*)dmem + align_up(tb, 256));
+            if (e == cudaSuccess) e = cudaMemcpy(dops, ops.data(), ob, cudaMemcpyHostToDevice);
+            if (e == cudaSuccess)
+                e = launch_ghost_fill(L->NC, L->fp32, dops, (int)ops.size(), acc, (const FabDev*)dmem, nullptr, A->stream);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(A->stream);
+            if (dmem) cudaFree(dmem);
+            if (e != cudaSuccess) rc = cuda_fail(e, "regrid copy");
+        }
+    }
+    if (rc == BAMREX_OK) rc = bamrex_level_sync(L);
+    if (rc != BAMREX_OK) {
+        bamrex_coupling_destroy(C);
+        bamrex_level_destroy(L);
+        return A->set_err(rc);
+    }
+    drop_levels_above(A, lev - 1);
+    A->levels.push_back(L);
+    A->cpl.push_back(C);
+    A->dt_level.resize(A->levels.size(), A->dt_level.empty() ? 0.0 : A->dt_level.back() / A->desc.ref_ratio);
+    return BAMREX_OK;
+}
+
+int level_tags(bamrex_amr* A, int l, double time, std::vector<char>& tags)
+{
+    bamrex_level* L = A->levels[l];
+    if (l > 0) AMR_TRY(A, bamrex_coupling_fill_patch(A->cpl[l], time));
+    const bamrex_amr_desc& d = A->desc;
+    const double gthr = l < d.max_phigrad_lev ? d.phigrad[l] : 0.0;
+    const int do_err = l < d.max_phierr_lev ? 1 : 0;
+    tags.assign((size_t)L->ncells, 0);
+    AMR_TRY(A, bamrex_level_tag(L, d.phigrad_var, d.phigrad_var_is_primv, gthr, do_err, d.phierr_var, d.phierr_var_is_primv,
+                                do_err ? d.phierr[l] : 0.0, tags.data()));
+    return BAMREX_OK;
+}
+
+int regrid(bamrex_amr* A, int lbase, double time)
+{
+    const bamrex_amr_desc& d = A->desc;
+    for (int l = lbase; l < d.max_level && l < (int)A->levels.size(); ++l) {
+        std::vector<char> tags;
+        BX_TRY(level_tags(A, l, time, tags));
+        bamrex_level* L = A->levels[l];
+        int periodic[3] = { 0, 0, 0 };
+        for (int q = 0; q < A->D; ++q) periodic[q] = L->bc_lo[q] == BAMREX_BC_PERIODIC;
+        long long dom = 1;
+        for (int q = 0; q < A->D; ++q) dom *= (L->domain.hi[q] - L->domain.lo[q] + 1);
+        std::vector<bamrex_box> nb((size_t)std::max<long long>(1, dom));
+        int n = 0;
+        AMR_TRY(A, bamrex_cluster_tags(A->D, &L->domain, periodic, L->boxes.data(), (int)L->boxes.size(), tags.data(),
+                                       d.ref_ratio, d.blocking_factor, d.max_grid_size, d.n_error_buf, d.n_proper,
+                                       d.grid_eff, nb.data(), (int)nb.size(), &n));
+        nb.resize(n);
+        if (n == 0) {
+            drop_levels_above(A, l);
+            break;
+        }
+        BX_TRY(set_level(A, l + 1, nb));
+    }
+    return BAMREX_OK;
+}
+
+int compute_dt(bamrex_amr* A, double time, double stop_time, bool initial, bool post_regrid)
+{
+    const int nl = (int)A->levels.size();
+    std::vector<double> dt_min(nl);
+    for (int l = 0; l < nl; ++l) {
+        double e = 0;
+        AMR_TRY(A, bamrex_level_est_time_step(A->levels[l], &e));
+        dt_min[l] = e;
+        if (!initial && post_regrid && l < (int)A->dt_level.size() && A->dt_level[l] > 0)
+            dt_min[l] = std::min(dt_min[l], A->dt_level[l]);
+    }
+    double dt0 = 1.0e100;
+    long long nf = 1;
+    for (int l = 0; l < nl; ++l) {
+        if (l > 0) nf *= A->desc.ref_ratio;
+        dt0 = std::min(dt0, (double)nf * dt_min[l]);
+    }
+    const double eps = 0.001 * dt0;
+    if (stop_time >= 0.0 && (time + dt0) > (stop_time - eps)) dt0 = stop_time - time;
+    A->dt_level.assign(nl, 0.0);
+    nf = 1;
+    for (int l = 0; l < nl; ++l) {
+        if (l > 0) nf *= A->desc.ref_ratio;
+        A->dt_level[l] = dt0 / (double)nf;
+    }
+    A->have_dt = true;
+    return BAMREX_OK;
+}
+
+int time_step(bamrex_amr* A, int l, double time)
+{
+    const int finest = (int)A->levels.size() - 1;
+    const double dt = A->dt_level[l];
+    bamrex_level* L = A->levels[l];
+    if (l < finest) AMR_TRY(A, bamrex_coupling_save_coarse_old(A->cpl[l + 1], time, time + dt));
+    if (l > 0) AMR_TRY(A, bamrex_coupling_fill_patch(A->cpl[l], time));
+    double used = 0;
+    AMR_TRY(A, bamrex_level_advance(L, time, dt, 1, 1, &used));
+    if (l < finest) {
+        const double dtf = A->dt_level[l + 1];
+        for (int i = 0; i < A->desc.ref_ratio; ++i) BX_TRY(time_step(A, l + 1, time + i * dtf));
+        if (A->desc.do_reflux) AMR_TRY(A, bamrex_coupling_reflux(A->cpl[l + 1]));
+        AMR_TRY(A, bamrex_coupling_avg_down(A->cpl[l + 1]));
+    }
+    return BAMREX_OK;
+}
+
+}  // namespace
+
+extern "C" int bamrex_amr_create(bamrex_amr** out, const bamrex_amr_desc* desc, void* stream)
+{
+    if (!out || !desc) return fail(BAMREX_ERR_ARG, "NULL argument");
+    *out = nullptr;
+    const int D = desc->base.spacedim;
+    if (desc->max_level < 0 || desc->max_level >= BAMREX_MAX_LEVELS) return fail(BAMREX_ERR_ARG, "max_level out of range");
+    if (desc->ref_ratio != 2 && desc->ref_ratio != 4) return fail(BAMREX_ERR_ARG, "ref_ratio must be 2 or 4");
+    if (desc->max_level > 0) {
+        if (desc->blocking_factor < 2 * desc->ref_ratio || desc->blocking_factor % (2 * desc->ref_ratio) != 0)
+            return fail(BAMREX_ERR_ARG, "blocking_factor must be a multiple of 2 * ref_ratio");
+        if (desc->max_grid_size < desc->blocking_factor || desc->max_grid_size % desc->blocking_factor != 0)
+            return fail(BAMREX_ERR_ARG, "max_grid_size must be a multiple of blocking_factor");
+    }
+    std::unique_ptr<bamrex_amr> A(new (std::nothrow) bamrex_amr());
+    if (!A) return fail(BAMREX_ERR_OOM, "host allocation failed");
+    A->desc = *desc;
+    A->D = D;
+    if (stream) {
+        A->stream = (cudaStream_t)stream;
+    } else {
+        BX_CK(cudaStreamCreateWithFlags(&A->stream, cudaStreamNonBlocking));
+        A->own_stream = true;
+    }
+    bamrex_level* L0 = nullptr;
+    const int rc = bamrex_level_create(&L0, &desc->base, A->stream);
+    if (rc != BAMREX_OK) {
+        if (A->own_stream) cudaStreamDestroy(A->stream);
+        return rc;
+    }
+    A->levels.push_back(L0);
+    A->cpl.push_back(nullptr);
+    A->dt_level.push_back(0.0);
+    *out = A.release();
+    return BAMREX_OK;
+}
+
+extern "C" int bamrex_amr_destroy(bamrex_amr* A)
+{
+    if (!A) return BAMREX_OK;
+    drop_levels_above(A, 0);
+    if (!A->levels.empty()) bamrex_level_destroy(A->levels[0]);
+    if (A->own_stream) cudaStreamDestroy(A->stream);
+    delete A;
+    return BAMREX_OK;
+}
+
+extern "C" const char* bamrex_amr_last_error(const bamrex_amr* A) { return A ? A->err.c_str() : ""; }
+
+extern "C" int bamrex_amr_finest_level(const bamrex_amr* A) { return A ? (int)A->levels.size() - 1 : -1; }
+
+extern "C" bamrex_level* bamrex_amr_level(bamrex_amr* A, int lev)
+{
+    if (!A || lev < 0 || lev >= (int)A->levels.size()) return nullptr;
+    return A->levels[lev];
+}
+
+extern "C" int bamrex_amr_boxes(const bamrex_amr* A, int lev, bamrex_box* out, int max_out, int* nout)
+{
+    if (!A || !nout || lev < 0 || lev >= (int)A->levels.size()) return fail(BAMREX_ERR_ARG, "bad argument");
+    const auto& b = A->levels[lev]->boxes;
+    *nout = (int)b.size();
+    if (!out) return BAMREX_OK;
+    if ((int)b.size() > max_out) return fail(BAMREX_ERR_ARG, "output array too small");
+    std::copy(b.begin(), b.end(), out);
+    return BAMREX_OK;
+}
+
+extern "C" int bamrex_amr_set_level_boxes(bamrex_amr* A, int lev, const bamrex_box* boxes, int nboxes)
+{
+    if (!A || !boxes || nboxes < 1) return fail(BAMREX_ERR_ARG, "bad argument");
+    std::vector<bamrex_box> b(boxes, boxes + nboxes);
+    return set_level(A, lev, b);
+}
+
+extern "C" int bamrex_amr_regrid(bamrex_amr* A, int lbase, double time)
+{
+    if (!A || lbase < 0 || lbase >= (int)A->levels.size()) return fail(BAMREX_ERR_ARG, "bad argument");
+    return regrid(A, lbase, time);
+}
+
+extern "C" int bamrex_amr_avg_down_all(bamrex_amr* A)
+{
+    if (!A) return fail(BAMREX_ERR_ARG, "NULL hierarchy");
+    for (int l = (int)A->levels.size() - 1; l >= 1; --l) AMR_TRY(A, bamrex_coupling_avg_down(A->cpl[l]));
+    return BAMREX_OK;
+}
+
+extern "C" int bamrex_amr_coarse_step(bamrex_amr* A, double stop_time, double* time_io, double* dt_out)
+{
+    if (!A || !time_io) return fail(BAMREX_ERR_ARG, "NULL argument");
+    const double time = *time_io;
+    bool regridded = false;
+    if (A->steps > 0 && A->desc.regrid_int > 0 && A->desc.max_level > 0 && A->steps % A->desc.regrid_int == 0) {
+        BX_TRY(regrid(A, 0, time));
+        regridded = true;
+    }
+    BX_TRY(compute_dt(A, time, stop_time, A->steps == 0, regridded));
+    if (!(A->dt_level[0] > 0) || !std::isfinite(A->dt_level[0]))
+        return amr_fail(A, BAMREX_ERR_NAN, "non-positive or non-finite coarse time step");
+    BX_TRY(time_step(A, 0, time));
+    AMR_TRY(A, bamrex_level_sync(A->levels[0]));
+    A->steps++;
+    *time_io = time + A->dt_level[0];
+    if (dt_out) *dt_out = A->dt_level[0];
+    return BAMREX_OK;
+}
+
+extern "C" int bamrex_amr_dt_level(const bamrex_amr* A, double* dt_level)
+{
+    if (!A || !dt_level) return fail(BAMREX_ERR_ARG, "NULL argument");
+    for (size_t l = 0; l < A->dt_level.size(); ++l) dt_level[l] = A->dt_level[l];
+    return BAMREX_OK;
+}
+
+extern "C" int bamrex_amr_conserved_sums(bamrex_amr* A, double* totals)
+{
+    if (!A || !totals) return fail(BAMREX_ERR_ARG, "NULL argument");
+    const int NC = A->D + 2;
+    for (int m = 0; m < NC; ++m) totals[m] = 0.0;
+    double s[BAMREX_MAX_NCOMP], c[BAMREX_MAX_NCOMP];
+    for (int l = 0; l < (int)A->levels.size(); ++l) {
+        AMR_TRY(A, bamrex_level_conserved_sums(A->levels[l], s));
+        for (int m = 0; m < NC; ++m) c[m] = 0.0;
+        if (l + 1 < (int)A->levels.size()) AMR_TRY(A, bamrex_coupling_covered_sums(A->cpl[l + 1], c));
+        for (int m = 0; m < NC; ++m) totals[m] += s[m] - c[m];
+    }
+    return BAMREX_OK;
+}

@@ -1,0 +1,97 @@
+// Coarse/fine coupling of two AMR levels: tables shared by the host builder
+// (amr.cu) and the kernels (amr_kernels.cu).
+//
+// The arithmetic AMReX performs for the reference at these call sites
+// (FillPatch with cell_cons_interp and time interpolation, FluxRegister
+// Reflux, average_down) lives in AMReX, which is not part of the reference;
+// the kernels here implement the published methods:
+//  * time interpolation: alpha * S_old + beta * S_new with
+//    alpha = (t_new - t) / (t_new - t_old), beta = (t - t_old) / (t_new - t_old),
+//    and the old or new state itself when t is within 1e-3 (t_new - t_old) of
+//    either end;
+//  * spatial interpolation: conservative piecewise-linear reconstruction from
+//    the coarse cell with monotonized-central slopes (van Leer 1977) and a
+//    Barth-Jespersen (1989) scale that keeps every fine value inside the
+//    range of the coarse cell and its face neighbours;
+//  * average_down: the mean of the r^D fine cells over each covered coarse
+//    cell;
+//  * reflux: each coarse cell next to the fine region is corrected by
+//    -/+ (sum of dt-and-area-scaled fine fluxes - scaled coarse flux) / V.
+#pragma once
+
+#include "common.cuh"
+#include "launch.h"
+
+namespace bamrex {
+
+// One cell of a coarse patch: the coarse state at (i,j,k) of box `box`
+// (after periodic / reflective / extrapolating boundary mapping), with the
+// components in negmask (bit n) sign-flipped by a reflecting wall.
+struct CfPatchCell {
+    int box;
+    int i, j, k;
+    int negmask;
+};
+
+// A fine ghost region filled by interpolation: fine cells [lo, hi] of box
+// dst (unshifted index space), whose periodic image is cell + shift; the
+// coarse patch [plo, plo + pn) of the image starts at patch_begin.
+struct CfRegion {
+    int dst;
+    int lo[3], hi[3];
+    int shift[3];
+    int plo[3], pn[3];
+    int pad;
+    long long patch_begin;
+    long long cell_begin;
+};
+
+// Coarse cells [lo, hi] of coarse box `crse` covered by fine box `fine`.
+struct AvgOp {
+    int crse, fine;
+    int lo[3], hi[3];
+    long long cell_begin;
+};
+
+// Coarse cell corrected by one flux-register slot, and the side it sits on
+// (sign -1: the face is its high face, +1: its low face).
+struct RefluxRec {
+    int box;
+    int i, j, k;
+    int sign;
+};
+
+struct CfInterpArgs {
+    const CfRegion* regions;
+    int nregions;
+    long long ncells;
+    const double* patch;  // NC * npatch, component-major
+    long long npatch;
+    const FabDev* fine0;  // both state buffers of the fine level
+    const FabDev* fine1;
+    int D, NC, ratio;
+};
+
+cudaError_t launch_cf_gather(int NC, bool fp32, const CfPatchCell* cells, long long ncells, const FabDev* crse_old,
+                             const FabDev* crse_new, int mode, double a_old, double a_new, double* patch,
+                             cudaStream_t s);
+cudaError_t launch_cf_interp(bool fp32, const CfInterpArgs& a, cudaStream_t s);
+cudaError_t launch_avg_down(int D, int NC, int ratio, bool fp32, const AvgOp* ops, int nops, long long ncells,
+                            const FabDev* crse, const FabDev* fine, cudaStream_t s);
+cudaError_t launch_reflux(int NC, bool fp32, const RefluxRec* recs, int nslots, const double* reg, double vol,
+                          const FabDev* crse, cudaStream_t s);
+// Tagging criteria of AmrLevelAdv::errorEst (Source/AmrLevelAdv.cpp:711-832):
+// state_error on err_var >= err_thr, grad_error on grad_var with relative
+// threshold grad_thr; *_primv selects the primitive vector.
+struct TagSpec {
+    int do_err, err_var, err_primv;
+    int do_grad, grad_var, grad_primv;
+    double err_thr, grad_thr;
+};
+
+// grad_error / state_error tagging (Source/Src_K/tagging_K.H:9-60) over the
+// valid cells of a level, tags (0/1) in the packed cell order.
+cudaError_t launch_tag(int D, bool fp32, const FabDev* fabs, const PackBox* boxes, int nboxes, long long ncells,
+                       const Consts& k, const TagSpec& spec, char* tags, cudaStream_t s);
+
+}  // namespace bamrex

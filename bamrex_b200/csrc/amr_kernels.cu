@@ -1,0 +1,287 @@
+// Kernels of the coarse/fine coupling (time and space interpolation of fine
+// ghost cells, average_down, reflux) and of grad_error / state_error
+// tagging.  This file is compiled with -fmad=false: every product and sum
+// is rounded separately, so the results are reproducible operation by
+// operation by a CPU restatement.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
+#include "amr.h"
+#include "common.cuh"
+#include "euler.cuh"
+
+namespace bamrex {
+
+namespace {
+
+constexpr int kThreads = 256;
+
+int grid_for(long long work)
+{
+    const long long want = (work + kThreads - 1) / kThreads;
+    const long long cap = (long long)device_sm_count() * 8;
+    return (int)std::max(1LL, std::min(want, cap));
+}
+
+__device__ __forceinline__ long long fidx(const FabDev& f, int i, int j, int k)
+{
+    return (long long)(i - f.b0) + (long long)(j - f.b1) * f.js + (long long)(k - f.b2) * f.ks;
+}
+
+template <typename V>
+__device__ __forceinline__ int find_begin(const V* v, int n, long long idx)
+{
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (v[mid].cell_begin <= idx) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ int floor_div(int a, int b) { return a >= 0 ? a / b : -((-a + b - 1) / b); }
+
+// ------------------------------------------------------------ coarse patch
+// mode 0: old state, 1: new state, 2: a_old * old + a_new * new
+template <typename T>
+__global__ void cf_gather_kernel(int NC, const CfPatchCell* __restrict__ cells, long long n,
+                                 const FabDev* __restrict__ old_fabs, const FabDev* __restrict__ new_fabs, int mode,
+                                 double a_old, double a_new, double* __restrict__ patch)
+{
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n;
+         e += (long long)gridDim.x * blockDim.x) {
+        const CfPatchCell c = cells[e];
+        const FabDev& fo = old_fabs[c.box];
+        const FabDev& fn = new_fabs[c.box];
+        const long long io = fidx(fo, c.i, c.j, c.k), in = fidx(fn, c.i, c.j, c.k);
+        for (int m = 0; m < NC; ++m) {
+            double v;
+            if (mode == 0) v = (double)fo.ptr<T>()[io + m * fo.ns];
+            else if (mode == 1) v = (double)fn.ptr<T>()[in + m * fn.ns];
+            else v = a_old * (double)fo.ptr<T>()[io + m * fo.ns] + a_new * (double)fn.ptr<T>()[in + m * fn.ns];
+            if ((c.negmask >> m) & 1) v = -v;
+            patch[(long long)m * n + e] = v;
+        }
+    }
+}
+
+// ------------------------------------------------------------ interpolation
+template <typename T>
+__global__ void cf_interp_kernel(const CfInterpArgs a)
+{
+    const int r = a.ratio;
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < a.ncells;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const CfRegion& R = a.regions[find_begin(a.regions, a.nregions, idx)];
+        const long long local = idx - R.cell_begin;
+        const int nx = R.hi[0] - R.lo[0] + 1, ny = R.hi[1] - R.lo[1] + 1;
+        const int f[3] = { R.lo[0] + (int)(local % nx), R.lo[1] + (int)((local / nx) % ny),
+                           R.lo[2] + (int)(local / ((long long)nx * ny)) };
+        int c[3];
+        double xi[3];
+        for (int d = 0; d < 3; ++d) {
+            const int w = f[d] + R.shift[d];
+            c[d] = d < a.D ? floor_div(w, r) : w;
+            // fine-cell centre relative to the coarse centre, in coarse cells
+            xi[d] = d < a.D ? (double)(2 * (w - c[d] * r) + 1 - r) / (double)(2 * r) : 0.0;
+        }
+        const long long pc = R.patch_begin + ((long long)(c[2] - R.plo[2]) * R.pn[1] + (c[1] - R.plo[1])) * R.pn[0] +
+                             (c[0] - R.plo[0]);
+        const long long pstride[3] = { 1, R.pn[0], (long long)R.pn[0] * R.pn[1] };
+        // the largest |xi| of any fine cell in a coarse cell
+        const double xmax = (double)(r - 1) / (double)(2 * r);
+        const FabDev& d0 = a.fine0[R.dst];
+        const FabDev& d1 = a.fine1[R.dst];
+        const long long i0 = fidx(d0, f[0], f[1], f[2]), i1 = fidx(d1, f[0], f[1], f[2]);
+        for (int m = 0; m < a.NC; ++m) {
+            const double* P = a.patch + (long long)m * a.npatch;
+            const double uc = P[pc];
+            double umin = uc, umax = uc, ext = 0.0, s = 0.0;
+            double slope[3] = { 0.0, 0.0, 0.0 };
+            for (int d = 0; d < a.D; ++d) {
+                const double ul = P[pc - pstride[d]], ur = P[pc + pstride[d]];
+                const double dc = 0.5 * (ur - ul);
+                const double dl = 2.0 * (uc - ul);
+                const double dr = 2.0 * (ur - uc);
+                double sl = 0.0;
+                if (dl * dr > 0.0) sl = copysign(fmin(fabs(dc), fmin(fabs(dl), fabs(dr))), dc);
+                slope[d] = sl;
+                umin = fmin(umin, fmin(ul, ur));
+                umax = fmax(umax, fmax(ul, ur));
+                ext = ext + fabs(sl) * xmax;
+            }
+            double alpha = 1.0;
+            if (ext > 0.0) {
+                alpha = fmin(alpha, (umax - uc) / ext);
+                alpha = fmin(alpha, (uc - umin) / ext);
+            }
+            for (int d = 0; d < a.D; ++d) s = s + slope[d] * xi[d];
+            const T v = (T)(uc + alpha * s);
+            d0.ptr<T>()[i0 + m * d0.ns] = v;
+            d1.ptr<T>()[i1 + m * d1.ns] = v;
+        }
+    }
+}
+
+// ------------------------------------------------------------ average_down
+template <typename T>
+__global__ void avg_down_kernel(int D, int NC, int r, const AvgOp* __restrict__ ops, int nops, long long n,
+                                const FabDev* __restrict__ crse, const FabDev* __restrict__ fine)
+{
+    const int rz = D > 2 ? r : 1, ry = D > 1 ? r : 1;
+    const double w = 1.0 / (double)(r * ry * rz);  // exact: r^D is a power of two
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < n;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const AvgOp& op = ops[find_begin(ops, nops, idx)];
+        const long long local = idx - op.cell_begin;
+        const int nx = op.hi[0] - op.lo[0] + 1, ny = op.hi[1] - op.lo[1] + 1;
+        const int i = op.lo[0] + (int)(local % nx);
+        const int j = op.lo[1] + (int)((local / nx) % ny);
+        const int k = op.lo[2] + (int)(local / ((long long)nx * ny));
+        const FabDev& fc = crse[op.crse];
+        const FabDev& ff = fine[op.fine];
+        const long long ic = fidx(fc, i, j, k);
+        const long long if0 = fidx(ff, i * r, D > 1 ? j * r : j, D > 2 ? k * r : k);
+        for (int m = 0; m < NC; ++m) {
+            const T* p = ff.ptr<T>() + if0 + m * ff.ns;
+            double sum = 0.0;
+            for (int kk = 0; kk < rz; ++kk)
+                for (int jj = 0; jj < ry; ++jj)
+                    for (int ii = 0; ii < r; ++ii) sum = sum + (double)p[ii + jj * ff.js + kk * ff.ks];
+            fc.ptr<T>()[ic + m * fc.ns] = (T)(sum * w);
+        }
+    }
+}
+
+// ------------------------------------------------------------ reflux
+template <typename T>
+__global__ void reflux_kernel(int NC, const RefluxRec* __restrict__ recs, int nslots, const double* __restrict__ reg,
+                              double vol, const FabDev* __restrict__ crse)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nslots) return;
+    const RefluxRec rc = recs[s];
+    const FabDev& f = crse[rc.box];
+    T* p = f.ptr<T>() + fidx(f, rc.i, rc.j, rc.k);
+    for (int m = 0; m < NC; ++m) {
+        const double corr = ((double)rc.sign * reg[(long long)m * nslots + s]) / vol;
+        p[m * f.ns] = (T)((double)p[m * f.ns] + corr);
+    }
+}
+
+// ------------------------------------------------------------ tagging
+template <typename T, int D>
+__device__ __forceinline__ double tag_value(const FabDev& f, int i, int j, int k, const K<T>& kk, int var, int primv)
+{
+    constexpr int NC = D + 2;
+    const T* p = f.ptr<T>() + fidx(f, i, j, k);
+    if (!primv) return (double)p[var * f.ns];
+    T U[NC], q[NC], ir;
+#pragma unroll
+    for (int n = 0; n < NC; ++n) U[n] = p[n * f.ns];
+    to_prim<T, D>(U, kk, q, ir);
+    return (double)sel(q, var);
+}
+
+template <typename T, int D>
+__global__ void tag_kernel(const FabDev* __restrict__ fab_tab, const PackBox* __restrict__ boxes, int nboxes,
+                           long long total, const Consts kc, const TagSpec spec, char* __restrict__ tags)
+{
+    const K<T> kk(kc);
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < total;
+         c += (long long)gridDim.x * blockDim.x) {
+        const int b = find_begin(boxes, nboxes, c);
+        const PackBox& B = boxes[b];
+        const int nx = B.hi[0] - B.lo[0] + 1, ny = B.hi[1] - B.lo[1] + 1;
+        const long long local = c - B.cell_begin;
+        const int i = B.lo[0] + (int)(local % nx);
+        const int j = B.lo[1] + (int)((local / nx) % ny);
+        const int k = B.lo[2] + (int)(local / ((long long)nx * ny));
+        const FabDev& f = fab_tab[b];
+        char t = 0;
+        // state_error (tagging_K.H:9-19)
+        if (spec.do_err && tag_value<T, D>(f, i, j, k, kk, spec.err_var, spec.err_primv) >= spec.err_thr) t = 1;
+        // grad_error (tagging_K.H:21-60)
+        if (spec.do_grad) {
+            const int var = spec.grad_var, pv = spec.grad_primv;
+            const double v = tag_value<T, D>(f, i, j, k, kk, var, pv);
+            double ax = fabs(tag_value<T, D>(f, i - 1, j, k, kk, var, pv) - v);
+            ax = fmax(ax, fabs(v - tag_value<T, D>(f, i + 1, j, k, kk, var, pv)));
+            double ay = 0.0, az = 0.0;
+            if (D > 1) {
+                ay = fabs(tag_value<T, D>(f, i, j - 1, k, kk, var, pv) - v);
+                ay = fmax(ay, fabs(v - tag_value<T, D>(f, i, j + 1, k, kk, var, pv)));
+            }
+            if (D > 2) {
+                az = fabs(tag_value<T, D>(f, i, j, k - 1, kk, var, pv) - v);
+                az = fmax(az, fabs(v - tag_value<T, D>(f, i, j, k + 1, kk, var, pv)));
+            }
+            if (fmax(ax, fmax(ay, az)) >= spec.grad_thr * fmax(fabs(v), 1e-14)) t = 1;
+        }
+        tags[c] = t;
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_cf_gather(int NC, bool fp32, const CfPatchCell* cells, long long ncells, const FabDev* crse_old,
+                             const FabDev* crse_new, int mode, double a_old, double a_new, double* patch,
+                             cudaStream_t s)
+{
+    if (ncells <= 0) return cudaSuccess;
+    const int g = grid_for(ncells);
+    if (fp32) cf_gather_kernel<float><<<g, kThreads, 0, s>>>(NC, cells, ncells, crse_old, crse_new, mode, a_old, a_new, patch);
+    else cf_gather_kernel<double><<<g, kThreads, 0, s>>>(NC, cells, ncells, crse_old, crse_new, mode, a_old, a_new, patch);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_cf_interp(bool fp32, const CfInterpArgs& a, cudaStream_t s)
+{
+    if (a.ncells <= 0) return cudaSuccess;
+    const int g = grid_for(a.ncells);
+    if (fp32) cf_interp_kernel<float><<<g, kThreads, 0, s>>>(a);
+    else cf_interp_kernel<double><<<g, kThreads, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_avg_down(int D, int NC, int ratio, bool fp32, const AvgOp* ops, int nops, long long ncells,
+                            const FabDev* crse, const FabDev* fine, cudaStream_t s)
+{
+    if (ncells <= 0) return cudaSuccess;
+    const int g = grid_for(ncells);
+    if (fp32) avg_down_kernel<float><<<g, kThreads, 0, s>>>(D, NC, ratio, ops, nops, ncells, crse, fine);
+    else avg_down_kernel<double><<<g, kThreads, 0, s>>>(D, NC, ratio, ops, nops, ncells, crse, fine);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_reflux(int NC, bool fp32, const RefluxRec* recs, int nslots, const double* reg, double vol,
+                          const FabDev* crse, cudaStream_t s)
+{
+    if (nslots <= 0) return cudaSuccess;
+    const int g = (nslots + kThreads - 1) / kThreads;
+    if (fp32) reflux_kernel<float><<<g, kThreads, 0, s>>>(NC, recs, nslots, reg, vol, crse);
+    else reflux_kernel<double><<<g, kThreads, 0, s>>>(NC, recs, nslots, reg, vol, crse);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_tag(int D, bool fp32, const FabDev* fabs, const PackBox* boxes, int nboxes, long long ncells,
+                       const Consts& k, const TagSpec& spec, char* tags, cudaStream_t s)
+{
+    if (ncells <= 0) return cudaSuccess;
+    const int g = grid_for(ncells);
+#define BX_TAG(TT, DD) tag_kernel<TT, DD><<<g, kThreads, 0, s>>>(fabs, boxes, nboxes, ncells, k, spec, tags)
+    if (fp32) {
+        if (D == 1) BX_TAG(float, 1);
+        else if (D == 2) BX_TAG(float, 2);
+        else BX_TAG(float, 3);
+    } else {
+        if (D == 1) BX_TAG(double, 1);
+        else if (D == 2) BX_TAG(double, 2);
+        else BX_TAG(double, 3);
+    }
+#undef BX_TAG
+    return cudaGetLastError();
+}
+
+}  // namespace bamrex

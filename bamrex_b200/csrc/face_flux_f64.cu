@@ -1,0 +1,6 @@
+// FP64 flux-register face kernels (see face_flux.cuh).
+#include "face_flux.cuh"
+
+namespace bamrex {
+template const void* pick_register_kernel<double>(int, int, int, int);
+}

@@ -1,0 +1,139 @@
+// Private host-side definition of bamrex_level and the level-step helpers,
+// shared by the C ABI (abi.cu) and the coarse/fine coupling (amr.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "bamrex_cuda.h"
+#include "launch.h"
+
+namespace bamrex {
+
+// Error reporting shared by every entry point (thread-local message).
+int fail(int code, const std::string& msg);
+int cuda_fail(cudaError_t e, const char* what);
+const char* last_error_text();
+
+#define BX_CK(call)                                                  \
+    do {                                                             \
+        cudaError_t e_ = (call);                                     \
+        if (e_ != cudaSuccess) return ::bamrex::cuda_fail(e_, #call); \
+    } while (0)
+
+#define BX_TRY(call)                      \
+    do {                                  \
+        int rc_ = (call);                 \
+        if (rc_ != BAMREX_OK) return rc_; \
+    } while (0)
+
+size_t align_up(size_t v, size_t a);
+
+// Faces whose flux a level step records into a flux register (the FluxRegister
+// CrseInit / FineAdd calls of AmrLevelAdv::advance,
+// Source/AmrLevelAdv_advance.cpp:236-254).  One slot per coarse face; a slot
+// takes `per_slot` consecutive face records.
+struct FaceRec {
+    int box;
+    int i, j, k;  // face index: the face between cells (i,j,k) - e_dir and (i,j,k)
+};
+
+struct RegisterTask {
+    const FaceRec* faces = nullptr;  // device, nslots * per_slot records
+    int nslots = 0;
+    int per_slot = 1;
+    double* reg = nullptr;  // device, NC * nslots (component-major)
+    int mode = 0;           // 0: reg = -(F * scale) (CrseInit); 1: reg += F * scale per face (FineAdd)
+};
+
+}  // namespace bamrex
+
+struct bamrex_level {
+    int D = 0, NC = 0, ngrow = 0, method = 0;
+    bool fp32 = false;   // FP32-storage variant
+    size_t esize = 8;    // bytes per stored value
+    double cfl = 0.9;
+    bamrex_parm parm;
+    bamrex::Consts k;
+    bamrex_box domain;
+    double dx[3] = { 1, 1, 1 };
+    double prob_lo[3] = { 0, 0, 0 };
+    int bc_lo[3] = { 0, 0, 0 }, bc_hi[3] = { 0, 0, 0 };
+    std::vector<bamrex_box> boxes;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int device = 0;
+
+    // device memory (one arena)
+    char* arena = nullptr;
+    char* state[2] = { nullptr, nullptr };
+    double* d_box_sums = nullptr;  // nboxes x NC, conserved sums
+    std::vector<bamrex::FabDev> fab[2];
+    bamrex::FabDev* d_fab[2] = { nullptr, nullptr };
+    bamrex::SweepBox* d_sweep[3][2] = {};
+    long long items[3] = { 0, 0, 0 };
+    int seglen[3] = { 0, 0, 0 };
+    bamrex::GhostOp* d_ghost[3] = { nullptr, nullptr, nullptr };
+    int nghost[3] = { 0, 0, 0 };
+    long long ghost_cells[3] = { 0, 0, 0 };
+    bamrex::PackBox* d_pack = nullptr;
+    long long ncells = 0;
+    size_t state_bytes = 0;  // bytes of one state buffer
+    double* staging = nullptr;
+    bamrex::StepScalars* d_scal = nullptr;
+    bamrex::StepScalars* h_scal = nullptr;  // pinned
+    int cur = 0;
+    bool ws_valid = false;
+
+    // flux-register recording by direction (set by the coarse/fine coupling)
+    std::vector<bamrex::RegisterTask> reg_tasks[3];
+
+    // accounting
+    long long launches = 0;
+    bool timing = false;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> events;
+    std::vector<int> event_dir;
+    size_t ev_used = 0;
+    double sweep_ms = 0.0;
+    long long sweep_launches = 0;
+    double dir_ms[3] = { 0, 0, 0 };
+    long long dir_launches[3] = { 0, 0, 0 };
+
+    cudaGraphExec_t graph[2] = { nullptr, nullptr };
+    bool run_pending = false;
+    int run_start_parity = 0;
+    std::string err;
+
+    int set_err(int code);
+};
+
+namespace bamrex {
+
+// Uniform bucket grid over the domain for box-intersection queries.
+struct BoxIndex {
+    int D = 0;
+    int lo[3] = { 0, 0, 0 }, bs[3] = { 1, 1, 1 }, nb[3] = { 1, 1, 1 };
+    std::vector<std::vector<int>> buckets;
+    const std::vector<bamrex_box>* boxes = nullptr;
+
+    void build(const bamrex_box& dom, const std::vector<bamrex_box>& bxs, int D_);
+    // indices of the boxes intersecting [rlo, rhi]
+    void query(const int* rlo, const int* rhi, std::vector<int>& out) const;
+};
+
+int level_launch(bamrex_level* L, cudaError_t e, const char* what);
+int level_fill(bamrex_level* L, int d, int parity, const StepScalars* scal);
+// One split step starting from buffer `parity`; the result lands in
+// parity ^ (D & 1).  dt from the host (scal == nullptr) or from the device.
+int level_step(bamrex_level* L, int parity, double dt_host, StepScalars* scal, bool allow_timing);
+
+// Face fluxes of direction `dir` recomputed from the sweep input `in` at the
+// faces of a register task (face_flux.cu).
+cudaError_t launch_register_faces(int D, int dir, int method, bool fp32, const Consts& k, const FabDev* in,
+                                  const RegisterTask& t, int NC, double dt, double dx_dir, double scale,
+                                  cudaStream_t s);
+
+}  // namespace bamrex

@@ -222,12 +222,30 @@ class Level:
         self.ncells = lib().bamrex_level_num_cells(self._h)
         self.dx = [(float(prob_hi[q]) - float(prob_lo[q])) / (self.dom_hi[q] - self.dom_lo[q] + 1)
                    for q in range(spacedim)]
+        self._owned = True
+
+    @classmethod
+    def wrap(cls, handle, spacedim, dom_lo, dom_hi, prob_lo, prob_hi, boxes, parm, method, cfl, precision):
+        """A non-owning view of a level created elsewhere (an AMR hierarchy)."""
+        self = cls.__new__(cls)
+        self.D, self.NC = spacedim, spacedim + 2
+        self.boxes = [(tuple(lo) + (0,) * (3 - len(lo)), tuple(hi) + (0,) * (3 - len(hi))) for lo, hi in boxes]
+        self.dom_lo = tuple(dom_lo) + (0,) * (3 - len(dom_lo))
+        self.dom_hi = tuple(dom_hi) + (0,) * (3 - len(dom_hi))
+        self.parm, self.method, self.cfl, self.precision = parm, method, cfl, precision
+        self._h = ctypes.c_void_p(handle)
+        self.packing = Packing(spacedim, self.dom_lo, self.boxes)
+        self.ncells = lib().bamrex_level_num_cells(self._h)
+        self.dx = [(float(prob_hi[q]) - float(prob_lo[q])) / (self.dom_hi[q] - self.dom_lo[q] + 1)
+                   for q in range(spacedim)]
+        self._owned = False
+        return self
 
     # lifetime
     def close(self):
-        if self._h:
+        if self._h and getattr(self, "_owned", True):
             lib().bamrex_level_destroy(self._h)
-            self._h = ctypes.c_void_p()
+        self._h = ctypes.c_void_p()
 
     def __del__(self):
         try:
@@ -268,6 +286,15 @@ class Level:
     # the reference's level surface
     def fill_boundary(self):
         self._ck(lib().bamrex_level_fill_boundary(self._h))
+
+    def tag(self, grad_var=0, grad_threshold=0.0, grad_var_is_primv=False, err_var=None, phierr=0.0,
+            err_var_is_primv=False) -> np.ndarray:
+        """errorEst tags (1 = refine) of the valid cells in packed order."""
+        buf = ctypes.create_string_buffer(int(self.ncells))
+        self._ck(lib().bamrex_level_tag(self._h, int(grad_var), 1 if grad_var_is_primv else 0, float(grad_threshold),
+                                        0 if err_var is None else 1, int(err_var or 0), 1 if err_var_is_primv else 0,
+                                        float(phierr), buf))
+        return np.frombuffer(buf.raw, dtype=np.uint8).copy()
 
     def conserved_sums(self):
         """sum(U) * cell volume per component (FP64, fixed order)."""

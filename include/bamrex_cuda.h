@@ -257,6 +257,138 @@ BAMREX_API int bamrex_level_reset_counters(bamrex_level *level);
  * launches for x, y, z (arrays of 3). */
 BAMREX_API int bamrex_level_sweep_times(bamrex_level *level, double *ms_by_dir, long long *launches_by_dir);
 
+/* ------------------------------------------------------------------ */
+/* AMR: coarse/fine coupling of two levels                              */
+/* ------------------------------------------------------------------ */
+
+/* Error estimation of AmrLevelAdv::errorEst (Source/AmrLevelAdv.cpp:711-832)
+ * on the current state: grad_error (Source/Src_K/tagging_K.H:21-60) on
+ * component grad_var (of the primitive vector if grad_var_is_primv) with the
+ * relative threshold grad_threshold (skipped if <= 0), and state_error
+ * (tagging_K.H:9-19) on err_var >= phierr (skipped if do_err == 0).  Ghost
+ * cells one deep must be valid: the call fills the level's own inter-box and
+ * physical ghosts; coarse/fine ghosts come from bamrex_coupling_fill_patch.
+ * tags: num_cells chars (1 = refine) in the packed order of
+ * bamrex_level_copy_out.  Synchronises the stream. */
+BAMREX_API int bamrex_level_tag(bamrex_level *level, int grad_var, int grad_var_is_primv, double grad_threshold,
+                                int do_err, int err_var, int err_var_is_primv, double phierr, char *tags);
+
+/* The coupling of a coarse level and the next finer level (refinement ratio
+ * 2 or 4).  It stands for the AMReX pieces the reference calls between two
+ * AmrLevelAdv levels: the FluxRegister (FineAdd / CrseInit in
+ * AmrLevelAdv::advance, Source/AmrLevelAdv_advance.cpp:236-254, Reflux in
+ * AmrLevelAdv::reflux, Source/AmrLevelAdv.cpp:918-945), FillPatch /
+ * FillPatcherFill with cell_cons_interp for the fine level's coarse/fine ghost
+ * cells (AmrLevelAdv_advance.cpp:108), FillCoarsePatch for new fine data
+ * (AmrLevelAdv.cpp:371), and average_down (AmrLevelAdv.cpp:947-987).
+ *
+ * Creation checks proper nesting (every coarse cell the fine level needs is a
+ * valid coarse cell) and builds all tables.  From then on, every
+ * bamrex_level_advance of the coarse level stores -dt*area*F at the
+ * coarse/fine faces (CrseInit) and every advance of the fine level adds
+ * dt*area*F of its faces (FineAdd), in the same kernels' stream order.  Both
+ * levels must use the same stream.  Destroy the coupling before either
+ * level. */
+typedef struct bamrex_coupling bamrex_coupling;
+BAMREX_API int bamrex_coupling_create(bamrex_coupling **out, bamrex_level *crse, bamrex_level *fine, int ref_ratio);
+BAMREX_API int bamrex_coupling_destroy(bamrex_coupling *c);
+
+/* Keep a copy of the coarse level's current state as its old time level
+ * (StateData::swapTimeLevels at the start of AmrLevelAdv::advance) with the
+ * times it spans, for time interpolation of fine ghost cells. */
+BAMREX_API int bamrex_coupling_save_coarse_old(bamrex_coupling *c, double t_old, double t_new);
+
+/* Fill the fine level's coarse/fine ghost cells (both state buffers) at
+ * `time`: coarse data interpolated in time between the saved old state and
+ * the current coarse state, then conservatively interpolated in space. */
+BAMREX_API int bamrex_coupling_fill_patch(bamrex_coupling *c, double time);
+
+/* Every valid fine cell from the current coarse state (FillCoarsePatch, for
+ * a newly created fine level). */
+BAMREX_API int bamrex_coupling_fill_coarse_patch(bamrex_coupling *c);
+
+/* Reflux (AmrLevelAdv::reflux) and average_down (AmrLevelAdv::avgDown) on
+ * the current coarse state. */
+BAMREX_API int bamrex_coupling_reflux(bamrex_coupling *c);
+BAMREX_API int bamrex_coupling_avg_down(bamrex_coupling *c);
+
+/* Sums of the current coarse state over the coarse cells covered by the
+ * fine level, times the coarse cell volume (NCOMP doubles; synchronises).
+ * A composite total is sum over levels of (level totals - covered sums). */
+BAMREX_API int bamrex_coupling_covered_sums(bamrex_coupling *c, double *sums);
+
+/* Number of flux-register slots (coarse faces) in direction dir, and a copy
+ * of the register (NCOMP * nslots doubles, component-major; reg may be NULL
+ * to query the count).  Synchronises the stream. */
+BAMREX_API int bamrex_coupling_register(bamrex_coupling *c, int dir, double *reg, int *nslots);
+
+/* Grid generation for a new level l+1 from tags on level l (the role of
+ * AMReX Amr::grid_places): tags buffered by n_error_buf cells, restricted to
+ * cells n_proper cells inside level l's boxes (domain faces excepted),
+ * coarsened by blocking_factor / ref_ratio, clustered by Berger-Rigoutsos
+ * with efficiency grid_eff, chopped to max_grid_size and refined.  domain and
+ * boxes are level l's; tags in the packed order of bamrex_level_tag;
+ * periodic[d] != 0 for periodic directions.  Output: level l+1 boxes.  Host
+ * only (no device work). */
+BAMREX_API int bamrex_cluster_tags(int spacedim, const bamrex_box *domain, const int *periodic,
+                                   const bamrex_box *boxes, int nboxes, const char *tags, int ref_ratio,
+                                   int blocking_factor, int max_grid_size, int n_error_buf, int n_proper,
+                                   double grid_eff, bamrex_box *out, int max_out, int *nout);
+
+/* ------------------------------------------------------------------ */
+/* AMR hierarchy with subcycling (the Amr time loop around AmrLevelAdv)  */
+/* ------------------------------------------------------------------ */
+
+#define BAMREX_MAX_LEVELS 8
+
+typedef struct bamrex_amr bamrex_amr;
+
+typedef struct bamrex_amr_desc {
+    bamrex_level_desc base;   /* level 0; finer levels share its parameters */
+    int max_level;            /* amr.max_level */
+    int ref_ratio;            /* amr.ref_ratio (2 or 4, every level) */
+    int blocking_factor;      /* amr.blocking_factor (fine cells; multiple of 2*ref_ratio) */
+    int max_grid_size;        /* amr.max_grid_size (fine cells; multiple of blocking_factor) */
+    int n_error_buf;          /* amr.n_error_buf */
+    int n_proper;             /* amr.n_proper (coarse cells) */
+    double grid_eff;          /* amr.grid_eff */
+    int regrid_int;           /* amr.regrid_int (coarse steps; 0 = never) */
+    int do_reflux;            /* adv.do_reflux */
+    int phigrad_var, phigrad_var_is_primv;
+    double phigrad[BAMREX_MAX_LEVELS];   /* tagging.phigrad per level */
+    int max_phigrad_lev;                 /* tagging.max_phigrad_lev */
+    int phierr_var, phierr_var_is_primv;
+    double phierr[BAMREX_MAX_LEVELS];    /* tagging.phierr per level */
+    int max_phierr_lev;                  /* tagging.max_phierr_lev */
+} bamrex_amr_desc;
+
+BAMREX_API int bamrex_amr_create(bamrex_amr **out, const bamrex_amr_desc *desc, void *stream);
+BAMREX_API int bamrex_amr_destroy(bamrex_amr *amr);
+BAMREX_API const char *bamrex_amr_last_error(const bamrex_amr *amr);
+BAMREX_API int bamrex_amr_finest_level(const bamrex_amr *amr);
+/* The level object (owned by the hierarchy: valid until the next regrid). */
+BAMREX_API bamrex_level *bamrex_amr_level(bamrex_amr *amr, int lev);
+BAMREX_API int bamrex_amr_boxes(const bamrex_amr *amr, int lev, bamrex_box *out, int max_out, int *nout);
+/* Replace level lev (1 <= lev <= finest + 1, lev <= max_level) by the given
+ * boxes: new data from the old level where it overlaps, from coarse
+ * interpolation elsewhere.  Levels above lev are removed. */
+BAMREX_API int bamrex_amr_set_level_boxes(bamrex_amr *amr, int lev, const bamrex_box *boxes, int nboxes);
+/* Regrid levels lbase+1 .. from tags (errorEst) on levels lbase .. at `time`. */
+BAMREX_API int bamrex_amr_regrid(bamrex_amr *amr, int lbase, double time);
+/* average_down from the finest level to level 0 (AmrLevelAdv::post_init). */
+BAMREX_API int bamrex_amr_avg_down_all(bamrex_amr *amr);
+/* One coarse step of the subcycled hierarchy (Amr::coarseTimeStep with
+ * AmrLevelAdv's computeInitialDt / computeNewDt, Source/AmrLevelAdv.cpp:487-619,
+ * timeStep recursion, and post_timestep reflux + avgDown, :624-652).  Regrids
+ * first when regrid_int divides the coarse steps taken.  *time_io is the time
+ * on entry and the new time on return; *dt_out the coarse dt taken. */
+BAMREX_API int bamrex_amr_coarse_step(bamrex_amr *amr, double stop_time, double *time_io, double *dt_out);
+/* dt of every level after the last computeInitialDt / computeNewDt. */
+BAMREX_API int bamrex_amr_dt_level(const bamrex_amr *amr, double *dt_level);
+/* Composite conserved totals: every level's sums minus those of its cells
+ * covered by the next finer level (NCOMP doubles; synchronises). */
+BAMREX_API int bamrex_amr_conserved_sums(bamrex_amr *amr, double *totals);
+
 #ifdef __cplusplus
 }
 #endif

@@ -370,6 +370,48 @@ class LevelLayout:
         if rc != 0:
             raise ValueError("oracle advance failed")
 
+    def advance_explicit_fluxes(self, S1, S2, time, dt, method, parm: Parm, nthreads=0, fast=False):
+        """advance_explicit that also returns the fluxes of every sweep:
+        out[d][b] is a (NC, nz, ny, nx) array on surroundingNodes(box b, d)
+        (the reference's fluxes[d] MultiFab, unscaled)."""
+        cp = parm.to_c()
+        bufs, offs, strs, shapes = [], [], [], []
+        for d in range(3):
+            if d >= self.D:
+                bufs.append(np.zeros(1))
+                offs.append(np.zeros(max(1, len(self.boxes)), dtype=np.int64))
+                strs.append(np.zeros(3 * max(1, len(self.boxes)), dtype=np.int64))
+                shapes.append([])
+                continue
+            o, st, sh, acc = [], [], [], 0
+            for lo, hi in self.boxes:
+                n = [hi[q] - lo[q] + 1 + (1 if q == d else 0) for q in range(3)]
+                o.append(acc)
+                st += [n[0], n[0] * n[1], n[0] * n[1] * n[2]]
+                sh.append((self.NC, n[2], n[1], n[0]))
+                acc += self.NC * n[0] * n[1] * n[2]
+            bufs.append(np.full(acc, np.nan))
+            offs.append(np.array(o, dtype=np.int64))
+            strs.append(np.array(st, dtype=np.int64))
+            shapes.append(sh)
+        dp = ctypes.POINTER(ctypes.c_double)
+        llp = ctypes.POINTER(ctypes.c_longlong)
+        fo = (dp * 3)(*[_dp(b) for b in bufs])
+        oo = (llp * 3)(*[o.ctypes.data_as(llp) for o in offs])
+        so = (llp * 3)(*[s.ctypes.data_as(llp) for s in strs])
+        rc = lib(fast).oracle_advance_explicit(ctypes.byref(self._c), _dp(S1), _dp(S2), time, dt, method,
+                                               ctypes.byref(cp), fo, oo, so, nthreads)
+        if rc != 0:
+            raise ValueError("oracle advance failed")
+        out = []
+        for d in range(self.D):
+            per = []
+            for b, sh in enumerate(shapes[d]):
+                o = int(offs[d][b])
+                per.append(bufs[d][o:o + int(np.prod(sh))].reshape(sh))
+            out.append(per)
+        return out
+
 
 def num_threads(fast=False) -> int:
     return lib(fast).oracle_num_threads()

@@ -1,0 +1,161 @@
+"""AMR pieces that run without a GPU: the library's host-side grid
+generation (bamrex_cluster_tags) and the CPU restatement of the coupling
+(oracle/amr_oracle.py) checked against conservation and consistency
+properties."""
+import numpy as np
+import pytest
+
+from bamrex_b200 import problems
+
+
+def _blob_tags(D, n, centres, radius):
+    x = np.arange(n) + 0.5
+    g = np.meshgrid(*([x] * D), indexing="ij")
+    t = np.zeros([n] * D, dtype=bool)
+    for c in centres:
+        t |= sum((gi - ci) ** 2 for gi, ci in zip(g, c)) < radius ** 2
+    return t
+
+
+def _packed(D, t, boxes):
+    # packed order: box-major, x fastest; t is indexed [x, y, z]
+    out = []
+    for lo, hi in boxes:
+        sl = tuple(slice(lo[d], hi[d] + 1) for d in range(D))
+        out.append(np.transpose(t[sl]).ravel())
+    return np.concatenate(out).astype(np.uint8)
+
+
+@pytest.mark.parametrize("D,n,mgs,bf", [(2, 64, 32, 8), (2, 64, 16, 4), (3, 32, 16, 8)])
+def test_cluster_tags_properties(D, n, mgs, bf):
+    from bamrex_b200.amr import cluster_tags
+    from oracle import oracle as O
+    boxes = O.decompose(D, (0, 0, 0), tuple(n - 1 if d < D else 0 for d in range(3)), 16)
+    t = _blob_tags(D, n, [(0.3 * n,) * D, (0.7 * n, 0.6 * n, 0.5 * n)[:D]], 0.12 * n)
+    nb = 1
+    fine = cluster_tags(D, (0, 0, 0), tuple(n - 1 if d < D else 0 for d in range(3)), boxes, _packed(D, t, boxes),
+                        ref_ratio=2, blocking_factor=bf, max_grid_size=mgs, n_error_buf=nb, n_proper=1, grid_eff=0.7)
+    assert fine
+    cover = np.zeros([2 * n] * D, dtype=int)
+    for lo, hi in fine:
+        for d in range(D):
+            assert lo[d] % bf == 0 and (hi[d] + 1) % bf == 0, "blocking factor alignment"
+            assert hi[d] - lo[d] + 1 <= mgs, "max_grid_size"
+            assert 0 <= lo[d] and hi[d] < 2 * n
+        cover[tuple(slice(lo[d], hi[d] + 1) for d in range(D))] += 1
+    assert cover.max() == 1, "boxes overlap"
+    # every tagged cell (buffered) is refined: level-0 cell c is covered if
+    # its fine children are
+    tb = t.copy()
+    for d in range(D):
+        tb = np.maximum.reduce([np.roll(tb, s, axis=d) for s in range(-nb, nb + 1)]) if nb else tb
+    child = cover[tuple(slice(0, None, 2) for _ in range(D))] > 0
+    assert np.all(child[t]), "a tagged cell is not refined"
+
+
+def test_cluster_tags_validation():
+    from bamrex_b200 import BamrexError
+    from bamrex_b200.amr import cluster_tags
+    boxes = [((0, 0, 0), (31, 31, 0))]
+    tags = np.zeros(32 * 32, dtype=np.uint8)
+    with pytest.raises(BamrexError):
+        cluster_tags(2, (0, 0, 0), (31, 31, 0), boxes, tags, ref_ratio=2, blocking_factor=6)
+    with pytest.raises(BamrexError):
+        cluster_tags(2, (0, 0, 0), (31, 31, 0), boxes, tags, ref_ratio=2, blocking_factor=8, max_grid_size=12)
+    assert cluster_tags(2, (0, 0, 0), (31, 31, 0), boxes, tags) == []
+
+
+def _smooth_blob(D, n):
+    x = (np.arange(n) + 0.5) / n
+    g = np.meshgrid(*([x] * D), indexing="ij")
+    shp = (1,) * (3 - D) + (n,) * D
+    q = np.zeros((D + 2,) + shp)
+    rho = 1 + 0.3 * np.sin(2 * np.pi * g[0])
+    r2 = sum((gi - 0.5) ** 2 for gi in g)
+    p = 1 + 0.2 * np.cos(2 * np.pi * g[-1]) + 2.0 * (r2 < 0.04)
+    q[0] = np.transpose(rho).reshape(shp)
+    q[D + 1] = np.transpose(p).reshape(shp)
+    for d in range(D):
+        q[1 + d] = 0.2 - 0.1 * d
+    return problems.consv_from_primv(D, q, 1.4)
+
+
+@pytest.mark.parametrize("D", [2, 3])
+def test_oracle_amr_conserves_with_reflux(oracle, D):
+    from oracle.amr_oracle import OAmr
+    n = 32 if D == 2 else 16
+    q = n // 2
+    hi0 = tuple(n - 1 if d < D else 0 for d in range(3))
+    fine = [(tuple(q if d < D else 0 for d in range(3)), tuple(3 * q - 1 if d < D else 0 for d in range(3)))]
+    bc = (oracle.PERIODIC,) * 3
+    u0 = _smooth_blob(D, n)
+    drift = {}
+    for reflux in (True, False):
+        A = OAmr(D, (0, 0, 0), hi0, [0.0] * D, [1.0] * D, [[((0, 0, 0), hi0)], fine], oracle.Parm(D, limiter=1),
+                 oracle.MUSCL_HANCOCK, 0.8, bc_lo=bc, bc_hi=bc, do_reflux=reflux)
+        A.levels[0].set_dense(u0)
+        A.cpl[1].fill_coarse_patch()
+        A.avg_down_all()
+        s0 = A.conserved_sums()
+        for _ in range(3):
+            A.coarse_step()
+        drift[reflux] = np.abs(A.conserved_sums() - s0) / np.abs(s0).max()
+    assert drift[True].max() <= 1e-13, drift[True]
+    assert drift[False].max() > 1e-8, drift[False]
+
+
+def test_oracle_interp_reproduces_linear_and_averages(oracle):
+    from oracle.amr_oracle import _interp, _padded
+    D, n, r = 2, 8, 2
+    x = np.arange(n)
+    Y, X = np.meshgrid(x, x, indexing="ij")
+    dense = np.zeros((4, 1, n, n))
+    dense[0, 0] = 1.0 + 0.25 * X + 0.125 * Y  # linear: reproduced exactly
+    dense[1, 0] = np.where((X + Y) % 3 == 0, 2.0, 1.0)  # rough: bounded, conservative
+    dense[2, 0] = 0.5
+    dense[3, 0] = 2.0
+    P = _padded(dense, D, (0, 0, 0), (0, 0, 0), 2)
+    fi = np.arange(2, 2 * n - 2)
+    FY, FX = np.meshgrid(fi, fi, indexing="ij")
+    w = [FX.ravel(), FY.ravel(), np.zeros(FX.size, dtype=np.int64)]
+    v = _interp(P, D, r, 2, w)
+    exact = 1.0 + 0.25 * ((w[0] + 0.5) / 2 - 0.5) + 0.125 * ((w[1] + 0.5) / 2 - 0.5)
+    np.testing.assert_allclose(v[0], exact, rtol=0, atol=1e-14)
+    c = (w[1] // 2, w[0] // 2)
+    nb_min = np.minimum.reduce([dense[1, 0][np.clip(c[0] + a, 0, n - 1), np.clip(c[1] + b, 0, n - 1)]
+                                for a, b in ((0, 0), (1, 0), (-1, 0), (0, 1), (0, -1))])
+    nb_max = np.maximum.reduce([dense[1, 0][np.clip(c[0] + a, 0, n - 1), np.clip(c[1] + b, 0, n - 1)]
+                                for a, b in ((0, 0), (1, 0), (-1, 0), (0, 1), (0, -1))])
+    assert np.all(v[1] >= nb_min - 1e-15) and np.all(v[1] <= nb_max + 1e-15)
+    # children average to the parent
+    m = v[1].reshape(FY.shape)
+    avg = 0.25 * (m[0::2, 0::2] + m[1::2, 0::2] + m[0::2, 1::2] + m[1::2, 1::2])
+    np.testing.assert_allclose(avg, dense[1, 0][1:n - 1, 1:n - 1], rtol=0, atol=1e-14)
+
+
+def test_oracle_fine_everywhere_equals_single_fine_level(oracle):
+    """A fine level covering the whole domain advances exactly like a single
+    level at the fine resolution with the same time steps."""
+    from oracle.amr_oracle import OAmr
+    D, n = 2, 16
+    u0 = _smooth_blob(D, 2 * n)
+    A = OAmr(D, (0, 0, 0), (n - 1, n - 1, 0), [0.0, 0.0], [1.0, 1.0],
+             [[((0, 0, 0), (n - 1, n - 1, 0))], [((0, 0, 0), (2 * n - 1, 2 * n - 1, 0))]], oracle.Parm(D),
+             oracle.MUSCL_HANCOCK, 0.8)
+    A.levels[1].set_dense(u0)
+    A.avg_down_all()
+    dts = []
+    for _ in range(2):
+        A.coarse_step()
+        dts += [A.dt_level[1]] * 2
+    lay = oracle.LevelLayout(D, (0, 0, 0), (2 * n - 1, 2 * n - 1, 0), [((0, 0, 0), (2 * n - 1, 2 * n - 1, 0))], 2,
+                             [1.0 / (2 * n)] * 2)
+    S = lay.alloc()
+    lay.scatter(S, u0)
+    t = 0.0
+    for dt in dts:
+        lay.fill_boundary(S)
+        S2 = S.copy()
+        lay.advance_explicit(S, S2, t, dt, oracle.MUSCL_HANCOCK, oracle.Parm(D))
+        t += dt
+    np.testing.assert_array_equal(A.levels[1].dense(), lay.gather(S))

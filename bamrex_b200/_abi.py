@@ -165,6 +165,7 @@ SIGNATURES = {
     "bamrex_level_counters": (_i, [_vp, ctypes.POINTER(_ll), _dp, ctypes.POINTER(_ll)]),
     "bamrex_level_reset_counters": (_i, [_vp]),
     "bamrex_level_sweep_times": (_i, [_vp, _dp, ctypes.POINTER(_ll)]),
+    "bamrex_conserved_sums_noalloc": (_i, [_i, ctypes.POINTER(Box), ctypes.POINTER(Array4), _i, _dp, _dp, _vp]),
     "bamrex_level_tag": (_i, [_vp, _i, _i, _d, _i, _i, _i, _d, ctypes.c_char_p]),
     "bamrex_coupling_create": (_i, [ctypes.POINTER(_vp), _vp, _vp, _i]),
     "bamrex_coupling_destroy": (_i, [_vp]),

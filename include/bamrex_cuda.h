@@ -208,6 +208,21 @@ BAMREX_API int bamrex_level_copy_out(bamrex_level *level, double *dst);
  * doubles.  Synchronises the stream. */
 BAMREX_API int bamrex_level_conserved_sums(bamrex_level *level, double *totals);
 
+/* The same totals for caller-owned fabs (box b's valid cells in fabs[b],
+ * FP64), computed without any device allocation: this entry point has no
+ * counterpart in the reference.  It serves callers that must not have a
+ * library allocate device memory for them (a host code whose own arena owns
+ * the GPU's memory, or an error path that no longer trusts the allocator).
+ * All scratch lives in one fixed file-scope device array: at most 4096
+ * boxes per call (larger counts are rejected with BAMREX_ERR_ARG).  The
+ * first call on each device looks up that array's address
+ * (cudaGetSymbolAddress) and must come before any stream capture.  Calls
+ * that overlap in time share the array and race: serialise them.  Issues
+ * its work on `stream` and synchronises it.  totals: NCOMP doubles, equal
+ * bit for bit to bamrex_level_conserved_sums on a level's own fabs. */
+BAMREX_API int bamrex_conserved_sums_noalloc(int spacedim, const bamrex_box *boxes, const bamrex_array4 *fabs,
+                                             int nboxes, const double dx[3], double *totals, void *stream);
+
 /* Wait for all work the level issued on its stream. */
 BAMREX_API int bamrex_level_sync(bamrex_level *level);
 

@@ -103,6 +103,23 @@ class LevelDesc(ctypes.Structure):
 
 
 MAX_LEVELS = 8
+# linear-operator boundary types (amrex::LinOpBCType subset)
+LINOP_PERIODIC, LINOP_NEUMANN, LINOP_DIRICHLET = range(3)
+
+
+class HelmholtzDesc(ctypes.Structure):
+    _fields_ = [
+        ("spacedim", ctypes.c_int),
+        ("n", ctypes.c_int * 3),
+        ("prob_lo", ctypes.c_double * 3),
+        ("prob_hi", ctypes.c_double * 3),
+        ("bc_lo", ctypes.c_int * 3),
+        ("bc_hi", ctypes.c_int * 3),
+        ("max_levels", ctypes.c_int),
+        ("nu1", ctypes.c_int),
+        ("nu2", ctypes.c_int),
+        ("bottom_sweeps", ctypes.c_int),
+    ]
 
 
 class AmrDesc(ctypes.Structure):
@@ -190,6 +207,20 @@ SIGNATURES = {
     "bamrex_amr_coarse_step": (_i, [_vp, _d, _dp, _dp]),
     "bamrex_amr_dt_level": (_i, [_vp, _dp]),
     "bamrex_amr_conserved_sums": (_i, [_vp, _dp]),
+    "bamrex_helmholtz_create": (_i, [ctypes.POINTER(_vp), ctypes.POINTER(HelmholtzDesc), _vp]),
+    "bamrex_helmholtz_destroy": (_i, [_vp]),
+    "bamrex_helmholtz_last_error": (ctypes.c_char_p, [_vp]),
+    "bamrex_helmholtz_num_levels": (_i, [_vp]),
+    "bamrex_helmholtz_set_scalars": (_i, [_vp, _d, _d, _d]),
+    "bamrex_helmholtz_set_acoeffs": (_i, [_vp, _vp, _d]),
+    "bamrex_helmholtz_set_bcoeffs": (_i, [_vp, _vp, _vp, _vp]),
+    "bamrex_helmholtz_set_bcoeffs_from_cell": (_i, [_vp, _vp]),
+    "bamrex_helmholtz_set_ccoeffs": (_i, [_vp, _vp]),
+    "bamrex_helmholtz_apply": (_i, [_vp, _vp, _vp]),
+    "bamrex_helmholtz_smooth": (_i, [_vp, _vp, _vp, _i]),
+    "bamrex_helmholtz_vcycle": (_i, [_vp, _vp, _vp]),
+    "bamrex_helmholtz_solve": (_i, [_vp, _vp, _vp, _d, _d, _i, _i, ctypes.POINTER(_i), _dp]),
+    "bamrex_helmholtz_launches": (_ll, [_vp]),
 }
 
 _LIB = None

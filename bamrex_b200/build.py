@@ -27,7 +27,7 @@ FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", 
          "--expt-relaxed-constexpr", "-I", INCLUDE, "-I", CSRC]
 # Per-file extra flags: the AMR coupling kernels round every product and sum
 # separately so a CPU restatement reproduces them exactly.
-FILE_FLAGS = {"amr_kernels.cu": ["-fmad=false"]}
+FILE_FLAGS = {"amr_kernels.cu": ["-fmad=false"], "helmholtz.cu": ["-fmad=false"]}
 
 
 def nvcc() -> str:

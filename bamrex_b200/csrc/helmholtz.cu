@@ -1,0 +1,898 @@
+// The pressure Helmholtz operator of the IMEX path on the device:
+//   y = A a x - B div(b grad x) + C c . grad x
+// (MLABecLaplacianGrad: mlalapgrad_adotx, Source/LinearSolver/
+// MLALapGrad_2D_K.H:9-33 and MLALapGrad_3D_K.H:9-38), its red-black
+// Gauss-Seidel smoother (alapgrad_gsrb, MLALapGrad_2D_K.H:180-230: plain
+// Gauss-Seidel in 2D; MLALapGrad_3D_K.H:258-324: over-relaxed, omega 1.15,
+// in 3D), a geometric multigrid V-cycle over a hierarchy of coarsened copies
+// of the operator (coefficients averaged down as averageDownCoeffs,
+// MLALaplacianGrad.H:950-986), and a BiCGStab solve preconditioned by one
+// V-cycle (the solve of setup_pressure_op / solve_pressure,
+// Source/IMEX/IMEX_O1.cpp:570-640, to a relative residual).
+//
+// One box per level: the whole domain, i fastest, no ghost cells.  Domain
+// boundaries are applied where a stencil leaves the box: periodic wrap, or
+// the boundary value cf * x(cell) with cf = +1 (homogeneous Neumann) or -1
+// (homogeneous Dirichlet on the face); the smoother moves the cf part to the
+// left-hand side as the reference's cf/delta terms do.  Every kernel is
+// HBM-bound; this file is compiled with -fmad=false so each operation rounds
+// exactly as written and a CPU restatement reproduces apply and smooth bit
+// for bit.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "bamrex_cuda.h"
+#include "level_impl.h"
+
+using namespace bamrex;
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kDotBlocks = 1184;  // 148 SMs x 8
+
+struct HLev {
+    int n[3];
+    long long ncell;
+    double dx[3];
+    double* a;     // ncell
+    double* b[3];  // faces: (n0+1)*n1*n2, n0*(n1+1)*n2, n0*n1*(n2+1)
+    double* c;     // D * ncell (component-major) or nullptr
+    double* phi;   // ncell
+    double* rhs;   // ncell
+    double* res;   // ncell
+};
+
+struct HOp {
+    double ascal, bscal, cscal;
+    int bc_lo[3], bc_hi[3];
+};
+
+__device__ __forceinline__ long long cidx(const HLev& L, int i, int j, int k)
+{
+    return (long long)i + (long long)L.n[0] * ((long long)j + (long long)L.n[1] * k);
+}
+
+__device__ __forceinline__ long long fidx(const HLev& L, int d, int i, int j, int k)
+{
+    const int nx = L.n[0] + (d == 0), ny = L.n[1] + (d == 1);
+    return (long long)i + (long long)nx * ((long long)j + (long long)ny * k);
+}
+
+// Neighbour value of x at cell (i,j,k) + s e_d (s = -1 or +1).  cf
+// receives the boundary factor (0 inside the domain or across a periodic
+// face).
+__device__ __forceinline__ double nbr(const double* __restrict__ x, const HLev& L, const HOp& op, int i, int j, int k,
+                                      int d, int s, double xc, double& cf)
+{
+    int q[3] = { i, j, k };
+    q[d] += s;
+    cf = 0.0;
+    if (q[d] < 0 || q[d] >= L.n[d]) {
+        const int bc = s < 0 ? op.bc_lo[d] : op.bc_hi[d];
+        if (bc == BAMREX_LINOP_PERIODIC) {
+            q[d] = q[d] < 0 ? q[d] + L.n[d] : q[d] - L.n[d];
+        } else {
+            cf = bc == BAMREX_LINOP_NEUMANN ? 1.0 : -1.0;
+            return cf * xc;
+        }
+    }
+    return x[cidx(L, q[0], q[1], q[2])];
+}
+
+// y = A x (mode 0) or y = rhs - A x (mode 1), the operator of
+// mlalapgrad_adotx with dhx = B dxinv^2, chdx = C c 0.5 dxinv.
+template <int D>
+__global__ void apply_kernel(const HLev L, const HOp op, const double* __restrict__ x, double* __restrict__ y,
+                             const double* __restrict__ rhs, int mode)
+{
+    double dxinv[3], dh[3];
+    for (int d = 0; d < 3; ++d) {
+        dxinv[d] = 1.0 / L.dx[d];
+        dh[d] = op.bscal * dxinv[d] * dxinv[d];
+    }
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < L.ncell;
+         c += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(c % L.n[0]);
+        const int j = (int)((c / L.n[0]) % L.n[1]);
+        const int k = (int)(c / ((long long)L.n[0] * L.n[1]));
+        const double xc = x[c];
+        double xm[3], xp[3], cf;
+        for (int d = 0; d < D; ++d) {
+            xm[d] = nbr(x, L, op, i, j, k, d, -1, xc, cf);
+            xp[d] = nbr(x, L, op, i, j, k, d, +1, xc, cf);
+        }
+        double v = op.ascal * L.a[c] * xc;
+        for (int d = 0; d < D; ++d) {
+            const int ih = i + (d == 0), jh = j + (d == 1), kh = k + (d == 2);
+            const double bl = L.b[d][fidx(L, d, i, j, k)], bh = L.b[d][fidx(L, d, ih, jh, kh)];
+            v = v - dh[d] * (bh * (xp[d] - xc) - bl * (xc - xm[d]));
+        }
+        if (L.c) {
+            for (int d = 0; d < D; ++d) {
+                const double chd = op.cscal * L.c[(long long)d * L.ncell + c] * 0.5 * dxinv[d];
+                v = v + chd * (xp[d] - xm[d]);
+            }
+        }
+        y[c] = mode ? rhs[c] - v : v;
+    }
+}
+
+// One colour of the red-black smoother: cells with (i+j+k+color) even.
+template <int D>
+__global__ void gsrb_kernel(const HLev L, const HOp op, double* __restrict__ phi, const double* __restrict__ rhs,
+                            int color)
+{
+    double dh[3], cdh[3];
+    for (int d = 0; d < 3; ++d) {
+        dh[d] = op.bscal / (L.dx[d] * L.dx[d]);
+        cdh[d] = op.cscal / (2 * L.dx[d]);
+    }
+    const long long half = (L.ncell + 1) / 2;
+    const int nxh = (L.n[0] + 1) / 2;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < half;
+         t += (long long)gridDim.x * blockDim.x) {
+        const long long row = t / nxh;
+        const int j = (int)(row % L.n[1]);
+        const int k = (int)(row / L.n[1]);
+        const int i = 2 * (int)(t % nxh) + ((j + k + color) & 1);
+        if (i >= L.n[0] || j >= L.n[1] || k >= L.n[2]) continue;
+        const long long c = cidx(L, i, j, k);
+        const double pc = phi[c];
+        double pm[3], pp[3], cfm[3], cfp[3], bl[3], bh[3], cc[3];
+        for (int d = 0; d < D; ++d) {
+            pm[d] = nbr(phi, L, op, i, j, k, d, -1, pc, cfm[d]);
+            pp[d] = nbr(phi, L, op, i, j, k, d, +1, pc, cfp[d]);
+            const int ih = i + (d == 0), jh = j + (d == 1), kh = k + (d == 2);
+            bl[d] = L.b[d][fidx(L, d, i, j, k)];
+            bh[d] = L.b[d][fidx(L, d, ih, jh, kh)];
+            cc[d] = L.c ? L.c[(long long)d * L.ncell + c] : 0.0;
+        }
+        double gamma = op.ascal * L.a[c];
+        for (int d = 0; d < D; ++d) gamma = gamma + dh[d] * (bl[d] + bh[d]);
+        double delta = dh[0] * (bl[0] * cfm[0] + bh[0] * cfp[0]);
+        for (int d = 1; d < D; ++d) delta = delta + dh[d] * (bl[d] * cfm[d] + bh[d] * cfp[d]);
+        for (int d = 0; d < D; ++d) delta = delta + cdh[d] * cc[d] * (cfm[d] - cfp[d]);
+        double rho = dh[0] * (bl[0] * pm[0] + bh[0] * pp[0]);
+        for (int d = 1; d < D; ++d) rho = rho + dh[d] * (bl[d] * pm[d] + bh[d] * pp[d]);
+        for (int d = 0; d < D; ++d) rho = rho - cdh[d] * cc[d] * (pp[d] - pm[d]);
+        if (D == 3) {
+            // MLALapGrad_3D_K.H:293-323
+            const double omega = 1.15;
+            const double g_m_d = gamma - delta;
+            const double res = rhs[c] - (gamma * pc - rho);
+            phi[c] = pc + omega / g_m_d * res;
+        } else {
+            // MLALapGrad_2D_K.H:205-228
+            phi[c] = (rhs[c] + rho - pc * delta) / (gamma - delta);
+        }
+    }
+}
+
+// rhs_c = mean of the 2^D children of the fine residual
+template <int D>
+__global__ void restrict_kernel(const HLev F, const HLev C)
+{
+    const double w = D == 3 ? 0.125 : (D == 2 ? 0.25 : 0.5);
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < C.ncell;
+         c += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(c % C.n[0]);
+        const int j = (int)((c / C.n[0]) % C.n[1]);
+        const int k = (int)(c / ((long long)C.n[0] * C.n[1]));
+        double s = 0.0;
+        for (int kk = 0; kk < (D > 2 ? 2 : 1); ++kk)
+            for (int jj = 0; jj < (D > 1 ? 2 : 1); ++jj)
+                for (int ii = 0; ii < 2; ++ii)
+                    s = s + F.res[cidx(F, 2 * i + ii, D > 1 ? 2 * j + jj : j, D > 2 ? 2 * k + kk : k)];
+        C.rhs[c] = s * w;
+        C.phi[c] = 0.0;
+    }
+}
+
+// phi_f += phi_c(parent)
+template <int D>
+__global__ void prolong_kernel(const HLev F, const HLev C)
+{
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < F.ncell;
+         c += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(c % F.n[0]);
+        const int j = (int)((c / F.n[0]) % F.n[1]);
+        const int k = (int)(c / ((long long)F.n[0] * F.n[1]));
+        F.phi[c] = F.phi[c] + C.phi[cidx(C, i / 2, D > 1 ? j / 2 : j, D > 2 ? k / 2 : k)];
+    }
+}
+
+// averageDownCoeffs: cell coefficients by the mean of the children, face
+// coefficients by the mean of the fine faces on each coarse face.
+template <int D>
+__global__ void coarsen_coeffs_kernel(const HLev F, const HLev C, int has_c)
+{
+    const double w = D == 3 ? 0.125 : (D == 2 ? 0.25 : 0.5);
+    const double wf = D == 3 ? 0.25 : (D == 2 ? 0.5 : 1.0);
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < C.ncell;
+         c += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(c % C.n[0]);
+        const int j = (int)((c / C.n[0]) % C.n[1]);
+        const int k = (int)(c / ((long long)C.n[0] * C.n[1]));
+        for (int m = -1; m < (has_c ? D : 0); ++m) {
+            const double* src = m < 0 ? F.a : F.c + (long long)m * F.ncell;
+            double s = 0.0;
+            for (int kk = 0; kk < (D > 2 ? 2 : 1); ++kk)
+                for (int jj = 0; jj < (D > 1 ? 2 : 1); ++jj)
+                    for (int ii = 0; ii < 2; ++ii)
+                        s = s + src[cidx(F, 2 * i + ii, D > 1 ? 2 * j + jj : j, D > 2 ? 2 * k + kk : k)];
+            if (m < 0) C.a[c] = s * w;
+            else C.c[(long long)m * C.ncell + c] = s * w;
+        }
+        // faces: the low face of this coarse cell in each direction, plus the
+        // high face for the last cell of a row
+        for (int d = 0; d < D; ++d) {
+            for (int hiface = 0; hiface < 2; ++hiface) {
+                const int q[3] = { i, j, k };
+                if (hiface && q[d] != C.n[d] - 1) continue;
+                int cf[3] = { i, j, k };
+                cf[d] += hiface;
+                double s = 0.0;
+                const int e1 = d == 0 ? 1 : 0, e2 = d == 2 ? 1 : 2;
+                for (int t2 = 0; t2 < (D > 2 ? 2 : 1); ++t2)
+                    for (int t1 = 0; t1 < (D > 1 ? 2 : 1); ++t1) {
+                        int f[3];
+                        f[d] = 2 * cf[d];
+                        f[e1] = (e1 < D) ? 2 * cf[e1] + t1 : cf[e1];
+                        f[e2] = (e2 < D && e2 != d) ? 2 * cf[e2] + t2 : cf[e2];
+                        s = s + F.b[d][fidx(F, d, f[0], f[1], f[2])];
+                    }
+                C.b[d][fidx(C, d, cf[0], cf[1], cf[2])] = s * wf;
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------- vectors
+// Deterministic dot product: fixed-grid partials, then one block in a
+// fixed tree order.
+__global__ void dot_partial_kernel(const double* __restrict__ x, const double* __restrict__ y, long long n,
+                                   double* __restrict__ part)
+{
+    __shared__ double red[kThreads];
+    double acc = 0.0;
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x)
+        acc = acc + x[c] * y[c];
+    red[threadIdx.x] = acc;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) red[threadIdx.x] = red[threadIdx.x] + red[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[blockIdx.x] = red[0];
+}
+
+__global__ void dot_final_kernel(const double* __restrict__ part, int nparts, double* __restrict__ out)
+{
+    __shared__ double red[kThreads];
+    double acc = 0.0;
+    for (int q = threadIdx.x; q < nparts; q += blockDim.x) acc = acc + part[q];
+    red[threadIdx.x] = acc;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) red[threadIdx.x] = red[threadIdx.x] + red[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *out = red[0];
+}
+
+// BiCGStab scalars (device resident)
+struct KScal {
+    double rho, rho_old, alpha, omega, beta;
+    double rv, ts, tt, rr, ss, bb;
+    int breakdown;
+    int pad;
+};
+
+__global__ void bicg_p_kernel(double* __restrict__ p, const double* __restrict__ r, const double* __restrict__ v,
+                              const KScal* __restrict__ S, long long n)
+{
+    // p = r + beta (p - omega v), beta = (rho / rho_old) (alpha / omega)
+    const double beta = (S->rho / S->rho_old) * (S->alpha / S->omega);
+    const double om = S->omega;
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x)
+        p[c] = r[c] + beta * (p[c] - om * v[c]);
+}
+
+__global__ void bicg_s_kernel(double* __restrict__ s, const double* __restrict__ r, const double* __restrict__ v,
+                              const KScal* __restrict__ S, long long n)
+{
+    const double alpha = S->rho / S->rv;
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x)
+        s[c] = r[c] - alpha * v[c];
+}
+
+// x += alpha phat + omega shat; r = s - omega t
+__global__ void bicg_xr_kernel(double* __restrict__ x, double* __restrict__ r, const double* __restrict__ ph,
+                               const double* __restrict__ sh, const double* __restrict__ s,
+                               const double* __restrict__ t, const KScal* __restrict__ S, long long n)
+{
+    const double alpha = S->rho / S->rv;
+    const double omega = S->ts / S->tt;
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n;
+         c += (long long)gridDim.x * blockDim.x) {
+        x[c] = x[c] + alpha * ph[c] + omega * sh[c];
+        r[c] = s[c] - omega * t[c];
+    }
+}
+
+__global__ void bicg_scalars_kernel(KScal* S, int stage)
+{
+    if (stage == 0) {  // start of an iteration after the first
+        S->rho_old = S->rho;
+    } else if (stage == 1) {  // after (t,s) and (t,t): omega for the next iteration
+        S->alpha = S->rho / S->rv;
+        S->omega = S->ts / S->tt;
+    }
+}
+
+__global__ void copy_kernel(double* __restrict__ d, const double* __restrict__ s, long long n)
+{
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x)
+        d[c] = s[c];
+}
+
+__global__ void face_avg_kernel(const double* __restrict__ cc, double* __restrict__ f, int d, int n0, int n1, int n2,
+                                int periodic)
+{
+    const int m[3] = { n0 + (d == 0), n1 + (d == 1), n2 + (d == 2) };
+    const long long nf = (long long)m[0] * m[1] * m[2];
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < nf;
+         q += (long long)gridDim.x * blockDim.x) {
+        int p[3] = { (int)(q % m[0]), (int)((q / m[0]) % m[1]), (int)(q / ((long long)m[0] * m[1])) };
+        int lo[3] = { p[0], p[1], p[2] }, hi[3] = { p[0], p[1], p[2] };
+        const int nd = d == 0 ? n0 : (d == 1 ? n1 : n2);
+        lo[d] = p[d] - 1;
+        hi[d] = p[d];
+        if (lo[d] < 0) lo[d] = periodic ? nd - 1 : 0;
+        if (hi[d] >= nd) hi[d] = periodic ? 0 : nd - 1;
+        const double vl = cc[(long long)lo[0] + (long long)n0 * ((long long)lo[1] + (long long)n1 * lo[2])];
+        const double vh = cc[(long long)hi[0] + (long long)n0 * ((long long)hi[1] + (long long)n1 * hi[2])];
+        f[q] = 0.5 * (vl + vh);
+    }
+}
+
+int grid_for(long long n)
+{
+    const long long want = (n + kThreads - 1) / kThreads;
+    return (int)std::max(1LL, std::min(want, (long long)device_sm_count() * 8));
+}
+
+}  // namespace
+
+struct bamrex_helmholtz {
+    int D = 2;
+    HOp op;
+    int nu1 = 2, nu2 = 2, bottom = 16;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    std::vector<HLev> lev;
+    char* arena = nullptr;
+    bool has_c = false;
+    bool coeffs_dirty = true;
+    // Krylov vectors on the finest level
+    double *x = nullptr, *r = nullptr, *rh = nullptr, *p = nullptr, *v = nullptr, *ph = nullptr, *s = nullptr,
+           *sh = nullptr, *t = nullptr, *bvec = nullptr;
+    double* part = nullptr;
+    KScal* d_scal = nullptr;
+    KScal* h_scal = nullptr;  // pinned
+    std::vector<double*> cbufs;  // per level, D * ncell: the C coefficients
+    cudaGraphExec_t iter_graph = nullptr;
+    long long launches = 0;
+    std::string err;
+};
+
+namespace {
+
+int hfail(bamrex_helmholtz* H, int code, const std::string& msg)
+{
+    const int rc = fail(code, msg);
+    if (H) H->err = last_error_text();
+    return rc;
+}
+
+int hck(bamrex_helmholtz* H, cudaError_t e, const char* what)
+{
+    if (e != cudaSuccess) {
+        const int rc = cuda_fail(e, what);
+        H->err = last_error_text();
+        return rc;
+    }
+    H->launches++;
+    return BAMREX_OK;
+}
+
+#define H_TRY(call)                       \
+    do {                                  \
+        int rc_ = (call);                 \
+        if (rc_ != BAMREX_OK) return rc_; \
+    } while (0)
+
+int launch_apply(bamrex_helmholtz* H, int l, const double* x, double* y, const double* rhs, int mode)
+{
+    const HLev& L = H->lev[l];
+    const int g = grid_for(L.ncell);
+    if (H->D == 3) apply_kernel<3><<<g, kThreads, 0, H->stream>>>(L, H->op, x, y, rhs, mode);
+    else apply_kernel<2><<<g, kThreads, 0, H->stream>>>(L, H->op, x, y, rhs, mode);
+    return hck(H, cudaGetLastError(), "helmholtz apply");
+}
+
+int launch_gsrb(bamrex_helmholtz* H, int l, int color)
+{
+    const HLev& L = H->lev[l];
+    const int g = grid_for((L.ncell + 1) / 2);
+    if (H->D == 3) gsrb_kernel<3><<<g, kThreads, 0, H->stream>>>(L, H->op, L.phi, L.rhs, color);
+    else gsrb_kernel<2><<<g, kThreads, 0, H->stream>>>(L, H->op, L.phi, L.rhs, color);
+    return hck(H, cudaGetLastError(), "helmholtz gsrb");
+}
+
+int smooth(bamrex_helmholtz* H, int l, int sweeps)
+{
+    for (int s = 0; s < sweeps; ++s) {
+        H_TRY(launch_gsrb(H, l, 0));
+        H_TRY(launch_gsrb(H, l, 1));
+    }
+    return BAMREX_OK;
+}
+
+int vcycle(bamrex_helmholtz* H, int l)
+{
+    const int nl = (int)H->lev.size();
+    if (l == nl - 1) return smooth(H, l, H->bottom);
+    H_TRY(smooth(H, l, H->nu1));
+    const HLev& F = H->lev[l];
+    const HLev& C = H->lev[l + 1];
+    H_TRY(launch_apply(H, l, F.phi, F.res, F.rhs, 1));
+    const int g = grid_for(C.ncell);
+    if (H->D == 3) restrict_kernel<3><<<g, kThreads, 0, H->stream>>>(F, C);
+    else restrict_kernel<2><<<g, kThreads, 0, H->stream>>>(F, C);
+    H_TRY(hck(H, cudaGetLastError(), "restrict"));
+    H_TRY(vcycle(H, l + 1));
+    const int gf = grid_for(F.ncell);
+    if (H->D == 3) prolong_kernel<3><<<gf, kThreads, 0, H->stream>>>(F, C);
+    else prolong_kernel<2><<<gf, kThreads, 0, H->stream>>>(F, C);
+    H_TRY(hck(H, cudaGetLastError(), "prolong"));
+    return smooth(H, l, H->nu2);
+}
+
+int coarsen_coeffs(bamrex_helmholtz* H)
+{
+    for (size_t l = 1; l < H->lev.size(); ++l) {
+        const int g = grid_for(H->lev[l].ncell);
+        if (H->D == 3) coarsen_coeffs_kernel<3><<<g, kThreads, 0, H->stream>>>(H->lev[l - 1], H->lev[l], H->has_c);
+        else coarsen_coeffs_kernel<2><<<g, kThreads, 0, H->stream>>>(H->lev[l - 1], H->lev[l], H->has_c);
+        H_TRY(hck(H, cudaGetLastError(), "coarsen coefficients"));
+    }
+    H->coeffs_dirty = false;
+    return BAMREX_OK;
+}
+
+int dot(bamrex_helmholtz* H, const double* x, const double* y, double* out)
+{
+    const long long n = H->lev[0].ncell;
+    dot_partial_kernel<<<kDotBlocks, kThreads, 0, H->stream>>>(x, y, n, H->part);
+    H_TRY(hck(H, cudaGetLastError(), "dot partial"));
+    dot_final_kernel<<<1, kThreads, 0, H->stream>>>(H->part, kDotBlocks, out);
+    return hck(H, cudaGetLastError(), "dot final");
+}
+
+int copy_vec(bamrex_helmholtz* H, double* d, const double* s)
+{
+    const long long n = H->lev[0].ncell;
+    copy_kernel<<<grid_for(n), kThreads, 0, H->stream>>>(d, s, n);
+    return hck(H, cudaGetLastError(), "copy");
+}
+
+// z = M y: one V-cycle from a zero guess
+int precondition(bamrex_helmholtz* H, double* z, const double* y)
+{
+    const HLev& F = H->lev[0];
+    H_TRY(copy_vec(H, F.rhs, y));
+    H_TRY(hck(H, cudaMemsetAsync(F.phi, 0, sizeof(double) * F.ncell, H->stream), "memset"));
+    H_TRY(vcycle(H, 0));
+    return copy_vec(H, z, F.phi);
+}
+
+// One BiCGStab iteration (right preconditioning), all scalars on the device.
+int bicg_iteration(bamrex_helmholtz* H)
+{
+    const long long n = H->lev[0].ncell;
+    const int g = grid_for(n);
+    KScal* S = H->d_scal;
+    bicg_scalars_kernel<<<1, 1, 0, H->stream>>>(S, 0);
+    H_TRY(hck(H, cudaGetLastError(), "scalars"));
+    H_TRY(dot(H, H->rh, H->r, &S->rho));
+    bicg_p_kernel<<<g, kThreads, 0, H->stream>>>(H->p, H->r, H->v, S, n);
+    H_TRY(hck(H, cudaGetLastError(), "bicg p"));
+    H_TRY(precondition(H, H->ph, H->p));
+    H_TRY(launch_apply(H, 0, H->ph, H->v, nullptr, 0));
+    H_TRY(dot(H, H->rh, H->v, &S->rv));
+    bicg_s_kernel<<<g, kThreads, 0, H->stream>>>(H->s, H->r, H->v, S, n);
+    H_TRY(hck(H, cudaGetLastError(), "bicg s"));
+    H_TRY(precondition(H, H->sh, H->s));
+    H_TRY(launch_apply(H, 0, H->sh, H->t, nullptr, 0));
+    H_TRY(dot(H, H->t, H->s, &S->ts));
+    H_TRY(dot(H, H->t, H->t, &S->tt));
+    bicg_xr_kernel<<<g, kThreads, 0, H->stream>>>(H->x, H->r, H->ph, H->sh, H->s, H->t, S, n);
+    H_TRY(hck(H, cudaGetLastError(), "bicg xr"));
+    bicg_scalars_kernel<<<1, 1, 0, H->stream>>>(S, 1);
+    H_TRY(hck(H, cudaGetLastError(), "scalars"));
+    return dot(H, H->r, H->r, &S->rr);
+}
+
+bool is_device_ptr(const void* p)
+{
+    cudaPointerAttributes at;
+    const bool dev = cudaPointerGetAttributes(&at, p) == cudaSuccess &&
+                     (at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged);
+    cudaGetLastError();
+    return dev;
+}
+
+int upload(bamrex_helmholtz* H, double* dst, const double* src, size_t n)
+{
+    return hck(H, cudaMemcpyAsync(dst, src, n * sizeof(double), cudaMemcpyDefault, H->stream), "coefficient copy");
+}
+
+}  // namespace
+
+extern "C" int bamrex_helmholtz_create(bamrex_helmholtz** out, const bamrex_helmholtz_desc* d, void* stream)
+{
+    if (!out || !d) return fail(BAMREX_ERR_ARG, "NULL argument");
+    *out = nullptr;
+    const int D = d->spacedim;
+    if (D != 2 && D != 3) return fail(BAMREX_ERR_ARG, "spacedim must be 2 or 3");
+    for (int q = 0; q < D; ++q) {
+        if (d->n[q] < 2) return fail(BAMREX_ERR_ARG, "at least two cells per direction");
+        if (!(d->prob_hi[q] > d->prob_lo[q])) return fail(BAMREX_ERR_ARG, "prob_hi must exceed prob_lo");
+        for (int s = 0; s < 2; ++s) {
+            const int bc = s ? d->bc_hi[q] : d->bc_lo[q];
+            if (bc < BAMREX_LINOP_PERIODIC || bc > BAMREX_LINOP_DIRICHLET) return fail(BAMREX_ERR_ARG, "unknown boundary type");
+        }
+        if ((d->bc_lo[q] == BAMREX_LINOP_PERIODIC) != (d->bc_hi[q] == BAMREX_LINOP_PERIODIC))
+            return fail(BAMREX_ERR_ARG, "periodic boundaries must be set on both sides");
+    }
+    std::unique_ptr<bamrex_helmholtz> H(new (std::nothrow) bamrex_helmholtz());
+    if (!H) return fail(BAMREX_ERR_OOM, "host allocation failed");
+    H->D = D;
+    H->op.ascal = 1.0;
+    H->op.bscal = 1.0;
+    H->op.cscal = 0.0;
+    for (int q = 0; q < 3; ++q) {
+        H->op.bc_lo[q] = q < D ? d->bc_lo[q] : BAMREX_LINOP_PERIODIC;
+        H->op.bc_hi[q] = q < D ? d->bc_hi[q] : BAMREX_LINOP_PERIODIC;
+    }
+    H->nu1 = d->nu1 > 0 ? d->nu1 : 2;
+    H->nu2 = d->nu2 > 0 ? d->nu2 : 2;
+    H->bottom = d->bottom_sweeps > 0 ? d->bottom_sweeps : 16;
+    // levels: halve every direction while all are even and >= 4
+    int n[3] = { d->n[0], d->n[1], D > 2 ? d->n[2] : 1 };
+    double dx[3];
+    for (int q = 0; q < 3; ++q) dx[q] = q < D ? (d->prob_hi[q] - d->prob_lo[q]) / n[q] : 1.0;
+    const int maxl = d->max_levels > 0 ? d->max_levels : 64;
+    for (int l = 0; l < maxl; ++l) {
+        HLev L;
+        std::memset(&L, 0, sizeof(L));
+        for (int q = 0; q < 3; ++q) {
+            L.n[q] = n[q];
+            L.dx[q] = dx[q];
+        }
+        L.ncell = (long long)n[0] * n[1] * n[2];
+        H->lev.push_back(L);
+        bool can = true;
+        for (int q = 0; q < D; ++q) can = can && n[q] % 2 == 0 && n[q] >= 4;
+        if (!can) break;
+        for (int q = 0; q < D; ++q) {
+            n[q] /= 2;
+            dx[q] *= 2;
+        }
+    }
+    // one arena: per level a, b[D], c[D], phi, rhs, res; Krylov vectors; partials
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        const size_t o = off;
+        off = align_up(off + std::max<size_t>(bytes, 8), 256);
+        return o;
+    };
+    struct Offs {
+        size_t a, b[3], c, phi, rhs, res;
+    };
+    std::vector<Offs> lo(H->lev.size());
+    for (size_t l = 0; l < H->lev.size(); ++l) {
+        const HLev& L = H->lev[l];
+        lo[l].a = take(sizeof(double) * L.ncell);
+        for (int q = 0; q < 3; ++q) {
+            const long long nf = (long long)(L.n[0] + (q == 0)) * (L.n[1] + (q == 1)) * (L.n[2] + (q == 2));
+            lo[l].b[q] = q < D ? take(sizeof(double) * nf) : 0;
+        }
+        lo[l].c = take(sizeof(double) * D * L.ncell);
+        lo[l].phi = take(sizeof(double) * L.ncell);
+        lo[l].rhs = take(sizeof(double) * L.ncell);
+        lo[l].res = take(sizeof(double) * L.ncell);
+    }
+    const long long n0 = H->lev[0].ncell;
+    size_t ov[10];
+    for (int q = 0; q < 10; ++q) ov[q] = take(sizeof(double) * n0);
+    const size_t opart = take(sizeof(double) * kDotBlocks);
+    const size_t oscal = take(sizeof(KScal));
+    cudaError_t e = cudaMalloc((void**)&H->arena, off);
+    if (e != cudaSuccess) return fail(BAMREX_ERR_OOM, std::string("cudaMalloc of the Helmholtz arena failed: ") + cudaGetErrorString(e));
+    e = cudaMallocHost((void**)&H->h_scal, sizeof(KScal));
+    if (e != cudaSuccess) {
+        cudaFree(H->arena);
+        return fail(BAMREX_ERR_OOM, "cudaMallocHost failed");
+    }
+    char* A = H->arena;
+    for (size_t l = 0; l < H->lev.size(); ++l) {
+        HLev& L = H->lev[l];
+        L.a = (double*)(A + lo[l].a);
+        for (int q = 0; q < 3; ++q) L.b[q] = q < D ? (double*)(A + lo[l].b[q]) : nullptr;
+        L.c = nullptr;  // set when C coefficients are given
+        L.phi = (double*)(A + lo[l].phi);
+        L.rhs = (double*)(A + lo[l].rhs);
+        L.res = (double*)(A + lo[l].res);
+    }
+    std::vector<double*> cbuf(H->lev.size());
+    for (size_t l = 0; l < H->lev.size(); ++l) cbuf[l] = (double*)(A + lo[l].c);
+    double** vv[10] = { &H->x, &H->r, &H->rh, &H->p, &H->v, &H->ph, &H->s, &H->sh, &H->t, &H->bvec };
+    for (int q = 0; q < 10; ++q) *vv[q] = (double*)(A + ov[q]);
+    H->part = (double*)(A + opart);
+    H->d_scal = (KScal*)(A + oscal);
+    e = cudaMemset(H->arena, 0, off);
+    if (e != cudaSuccess) {
+        cudaFree(H->arena);
+        cudaFreeHost(H->h_scal);
+        return cuda_fail(e, "memset");
+    }
+    H->cbufs = cbuf;
+    if (stream) {
+        H->stream = (cudaStream_t)stream;
+    } else {
+        e = cudaStreamCreateWithFlags(&H->stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) {
+            cudaFree(H->arena);
+            cudaFreeHost(H->h_scal);
+            return cuda_fail(e, "cudaStreamCreateWithFlags");
+        }
+        H->own_stream = true;
+    }
+    // default coefficients: a = 1, b = 1
+    for (size_t l = 0; l < H->lev.size(); ++l) {
+        HLev& L = H->lev[l];
+        std::vector<double> ones((size_t)L.ncell, 1.0);
+        cudaMemcpy(L.a, ones.data(), sizeof(double) * L.ncell, cudaMemcpyHostToDevice);
+        for (int q = 0; q < D; ++q) {
+            const long long nf = (long long)(L.n[0] + (q == 0)) * (L.n[1] + (q == 1)) * (L.n[2] + (q == 2));
+            std::vector<double> fo((size_t)nf, 1.0);
+            cudaMemcpy(L.b[q], fo.data(), sizeof(double) * nf, cudaMemcpyHostToDevice);
+        }
+    }
+    *out = H.release();
+    return BAMREX_OK;
+}
+
+extern "C" int bamrex_helmholtz_destroy(bamrex_helmholtz* H)
+{
+    if (!H) return BAMREX_OK;
+    if (H->stream) cudaStreamSynchronize(H->stream);
+    if (H->iter_graph) cudaGraphExecDestroy(H->iter_graph);
+    if (H->arena) cudaFree(H->arena);
+    if (H->h_scal) cudaFreeHost(H->h_scal);
+    if (H->own_stream) cudaStreamDestroy(H->stream);
+    delete H;
+    return BAMREX_OK;
+}
+
+extern "C" const char* bamrex_helmholtz_last_error(const bamrex_helmholtz* H) { return H ? H->err.c_str() : ""; }
+
+extern "C" int bamrex_helmholtz_num_levels(const bamrex_helmholtz* H) { return H ? (int)H->lev.size() : 0; }
+
+extern "C" int bamrex_helmholtz_set_scalars(bamrex_helmholtz* H, double a, double b, double c)
+{
+    if (!H) return fail(BAMREX_ERR_ARG, "NULL operator");
+    H->op.ascal = a;
+    H->op.bscal = b;
+    H->op.cscal = c;
+    if (H->iter_graph) {
+        cudaGraphExecDestroy(H->iter_graph);
+        H->iter_graph = nullptr;
+    }
+    return BAMREX_OK;
+}
+
+extern "C" int bamrex_helmholtz_set_acoeffs(bamrex_helmholtz* H, const double* alpha, double alpha_const)
+{
+    if (!H) return fail(BAMREX_ERR_ARG, "NULL operator");
+    HLev& L = H->lev[0];
+    if (alpha) {
+        H_TRY(upload(H, L.a, alpha, (size_t)L.ncell));
+    } else {
+        std::vector<double> v((size_t)L.ncell, alpha_const);
+        H_TRY(upload(H, L.a, v.data(), v.size()));
+        H_TRY(hck(H, cudaStreamSynchronize(H->stream), "sync"));
+    }
+    H->coeffs_dirty = true;
+    return BAMREX_OK;
+}
+
+extern "C" int bamrex_helmholtz_set_bcoeffs(bamrex_helmholtz* H, const double* bx, const double* by, const double* bz)
+{
+    if (!H) return fail(BAMREX_ERR_ARG, "NULL operator");
+    const double* src[3] = { bx, by, bz };
+    HLev& L = H->lev[0];
+    for (int q = 0; q < H->D; ++q) {
+        if (!src[q]) return hfail(H, BAMREX_ERR_ARG, "missing face coefficients");
+        const long long nf = (long long)(L.n[0] + (q == 0)) * (L.n[1] + (q == 1)) * (L.n[2] + (q == 2));
+        H_TRY(upload(H, L.b[q], src[q], (size_t)nf));
+    }
+    H->coeffs_dirty = true;
+    return BAMREX_OK;
+}
+
+extern "C" int bamrex_helmholtz_set_bcoeffs_from_cell(bamrex_helmholtz* H, const double* beta_cc)
+{
+    if (!H || !beta_cc) return fail(BAMREX_ERR_ARG, "NULL argument");
+    HLev& L = H->lev[0];
+    const double* src = beta_cc;
+    if (!is_device_ptr(beta_cc)) {
+        H_TRY(upload(H, H->bvec, beta_cc, (size_t)L.ncell));
+        src = H->bvec;
+    }
+    for (int q = 0; q < H->D; ++q) {
+        const long long nf = (long long)(L.n[0] + (q == 0)) * (L.n[1] + (q == 1)) * (L.n[2] + (q == 2));
+        face_avg_kernel<<<grid_for(nf), kThreads, 0, H->stream>>>(src, L.b[q], q, L.n[0], L.n[1], L.n[2],
+                                                                 H->op.bc_lo[q] == BAMREX_LINOP_PERIODIC);
+        H_TRY(hck(H, cudaGetLastError(), "face average"));
+    }
+    H->coeffs_dirty = true;
+    return BAMREX_OK;
+}
+
+extern "C" int bamrex_helmholtz_set_ccoeffs(bamrex_helmholtz* H, const double* c)
+{
+    if (!H) return fail(BAMREX_ERR_ARG, "NULL operator");
+    if (!c) {
+        for (auto& L : H->lev) L.c = nullptr;
+        H->has_c = false;
+    } else {
+        for (size_t l = 0; l < H->lev.size(); ++l) H->lev[l].c = H->cbufs[l];
+        H_TRY(upload(H, H->lev[0].c, c, (size_t)H->D * H->lev[0].ncell));
+        H->has_c = true;
+    }
+    if (H->iter_graph) {
+        cudaGraphExecDestroy(H->iter_graph);
+        H->iter_graph = nullptr;
+    }
+    H->coeffs_dirty = true;
+    return BAMREX_OK;
+}
+
+static int prepare(bamrex_helmholtz* H)
+{
+    if (H->coeffs_dirty) {
+        H_TRY(coarsen_coeffs(H));
+        if (H->iter_graph) {
+            cudaGraphExecDestroy(H->iter_graph);
+            H->iter_graph = nullptr;
+        }
+    }
+    return BAMREX_OK;
+}
+
+// In/out vectors may be host or device memory: host data go through the
+// finest level's work vectors.
+extern "C" int bamrex_helmholtz_apply(bamrex_helmholtz* H, const double* x, double* y)
+{
+    if (!H || !x || !y) return fail(BAMREX_ERR_ARG, "NULL argument");
+    const long long n = H->lev[0].ncell;
+    const bool dx = is_device_ptr(x), dy = is_device_ptr(y);
+    const double* xi = x;
+    if (!dx) {
+        H_TRY(upload(H, H->p, x, (size_t)n));
+        xi = H->p;
+    }
+    double* yo = dy ? y : H->v;
+    H_TRY(launch_apply(H, 0, xi, yo, nullptr, 0));
+    if (!dy) H_TRY(hck(H, cudaMemcpyAsync(y, yo, sizeof(double) * n, cudaMemcpyDeviceToHost, H->stream), "copy out"));
+    return hck(H, cudaStreamSynchronize(H->stream), "sync");
+}
+
+extern "C" int bamrex_helmholtz_smooth(bamrex_helmholtz* H, double* phi, const double* rhs, int redblack)
+{
+    if (!H || !phi || !rhs) return fail(BAMREX_ERR_ARG, "NULL argument");
+    HLev& L = H->lev[0];
+    const long long n = L.ncell;
+    H_TRY(upload(H, L.phi, phi, (size_t)n));
+    H_TRY(upload(H, L.rhs, rhs, (size_t)n));
+    H_TRY(launch_gsrb(H, 0, redblack & 1));
+    H_TRY(hck(H, cudaMemcpyAsync(phi, L.phi, sizeof(double) * n, cudaMemcpyDefault, H->stream), "copy out"));
+    return hck(H, cudaStreamSynchronize(H->stream), "sync");
+}
+
+extern "C" int bamrex_helmholtz_vcycle(bamrex_helmholtz* H, double* z, const double* r)
+{
+    if (!H || !z || !r) return fail(BAMREX_ERR_ARG, "NULL argument");
+    H_TRY(prepare(H));
+    const long long n = H->lev[0].ncell;
+    H_TRY(upload(H, H->s, r, (size_t)n));
+    H_TRY(precondition(H, H->sh, H->s));
+    H_TRY(hck(H, cudaMemcpyAsync(z, H->sh, sizeof(double) * n, cudaMemcpyDefault, H->stream), "copy out"));
+    return hck(H, cudaStreamSynchronize(H->stream), "sync");
+}
+
+extern "C" int bamrex_helmholtz_solve(bamrex_helmholtz* H, double* x, const double* rhs, double tol_rel, double tol_abs,
+                                      int max_iter, int use_graph, int* iters, double* rel_res)
+{
+    if (!H || !x || !rhs) return fail(BAMREX_ERR_ARG, "NULL argument");
+    if (max_iter < 1) return hfail(H, BAMREX_ERR_ARG, "max_iter must be >= 1");
+    H_TRY(prepare(H));
+    const long long n = H->lev[0].ncell;
+    KScal* S = H->d_scal;
+    H_TRY(upload(H, H->x, x, (size_t)n));
+    H_TRY(upload(H, H->bvec, rhs, (size_t)n));
+    // r = b - A x, rhat = r; rho = alpha = omega = 1, p = v = 0
+    H_TRY(launch_apply(H, 0, H->x, H->r, H->bvec, 1));
+    H_TRY(copy_vec(H, H->rh, H->r));
+    H_TRY(hck(H, cudaMemsetAsync(H->p, 0, sizeof(double) * n, H->stream), "memset"));
+    H_TRY(hck(H, cudaMemsetAsync(H->v, 0, sizeof(double) * n, H->stream), "memset"));
+    KScal init;
+    std::memset(&init, 0, sizeof(init));
+    init.rho = init.alpha = init.omega = init.rv = init.ts = init.tt = 1.0;
+    *H->h_scal = init;
+    H_TRY(hck(H, cudaMemcpyAsync(S, H->h_scal, sizeof(KScal), cudaMemcpyHostToDevice, H->stream), "scalars"));
+    H_TRY(dot(H, H->bvec, H->bvec, &S->bb));
+    H_TRY(dot(H, H->r, H->r, &S->rr));
+    H_TRY(hck(H, cudaMemcpyAsync(H->h_scal, S, sizeof(KScal), cudaMemcpyDeviceToHost, H->stream), "scalars"));
+    H_TRY(hck(H, cudaStreamSynchronize(H->stream), "sync"));
+    const double bnorm = std::sqrt(H->h_scal->bb);
+    double rnorm = std::sqrt(H->h_scal->rr);
+    const double target = std::max(tol_rel * bnorm, tol_abs);
+    int it = 0;
+    while (rnorm > target && it < max_iter) {
+        if (use_graph) {
+            if (!H->iter_graph) {
+                cudaGraph_t g = nullptr;
+                H_TRY(hck(H, cudaStreamBeginCapture(H->stream, cudaStreamCaptureModeThreadLocal), "begin capture"));
+                const long long before = H->launches;
+                const int rc = bicg_iteration(H);
+                cudaError_t e = cudaStreamEndCapture(H->stream, &g);
+                if (rc != BAMREX_OK) {
+                    if (g) cudaGraphDestroy(g);
+                    return rc;
+                }
+                H_TRY(hck(H, e, "end capture"));
+                H->launches = before;
+                e = cudaGraphInstantiate(&H->iter_graph, g, 0);
+                cudaGraphDestroy(g);
+                H_TRY(hck(H, e, "graph instantiate"));
+            }
+            H_TRY(hck(H, cudaGraphLaunch(H->iter_graph, H->stream), "graph launch"));
+        } else {
+            H_TRY(bicg_iteration(H));
+        }
+        H_TRY(hck(H, cudaMemcpyAsync(H->h_scal, S, sizeof(KScal), cudaMemcpyDeviceToHost, H->stream), "scalars"));
+        H_TRY(hck(H, cudaStreamSynchronize(H->stream), "sync"));
+        ++it;
+        rnorm = std::sqrt(H->h_scal->rr);
+        if (!std::isfinite(rnorm)) return hfail(H, BAMREX_ERR_NAN, "BiCGStab breakdown (non-finite residual)");
+    }
+    H_TRY(hck(H, cudaMemcpyAsync(x, H->x, sizeof(double) * n, cudaMemcpyDefault, H->stream), "copy out"));
+    H_TRY(hck(H, cudaStreamSynchronize(H->stream), "sync"));
+    if (iters) *iters = it;
+    if (rel_res) *rel_res = bnorm > 0 ? rnorm / bnorm : rnorm;
+    return BAMREX_OK;
+}
+
+extern "C" long long bamrex_helmholtz_launches(const bamrex_helmholtz* H) { return H ? H->launches : 0; }

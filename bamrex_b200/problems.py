@@ -92,3 +92,34 @@ def random_states(D, shape, seed=DEFAULT_SEED, adiabatic=1.4):
         q[1 + d] = rng.uniform(-1.0, 1.0, (nz, ny, nx))
     q[1 + D] = rng.uniform(1.0, 2.0, (nz, ny, nx))
     return consv_from_primv(D, q, adiabatic)
+
+
+def gaussian_random_field(shape, corr_cells, seed, rng=None):
+    """Unit-variance periodic Gaussian random field on a grid of `shape`
+    (nz, ny, nx): white noise filtered in Fourier space by a Gaussian of
+    correlation length corr_cells cells."""
+    rng = np.random.default_rng(seed) if rng is None else rng
+    w = rng.standard_normal(shape)
+    k = np.meshgrid(*[np.fft.fftfreq(n) for n in shape], indexing="ij")
+    k2 = sum(ki ** 2 for ki in k)
+    filt = np.exp(-0.5 * (2 * np.pi * corr_cells) ** 2 * k2)
+    g = np.real(np.fft.ifftn(np.fft.fftn(w) * filt))
+    return (g - g.mean()) / g.std()
+
+
+def low_mach_pressure_problem(n=2048, seed=DEFAULT_SEED, log_sigma=1.0, corr_cells=32, mach=0.01, adiabatic=1.4,
+                              cfl=0.8):
+    """The 2D IMEX pressure solve workload: density a lognormal field
+    (log-sigma 1.0, correlation length 32 cells), beta = 1/rho on cells,
+    the Helmholtz scalars of setup_pressure_op (Source/IMEX/IMEX_O1.cpp:
+    592-596): A = 1, a = epsilon / (gamma - 1) with epsilon = Mach^2, B = dt^2
+    with dt from the flow CFL at speed `mach`, and a seeded smooth right-hand
+    side.  Returns dict(rho, beta_cc, a, B, rhs, dx) with (1, n, n) arrays."""
+    rng = np.random.default_rng(seed)
+    g = gaussian_random_field((n, n), corr_cells, seed, rng)
+    rho = np.exp(log_sigma * g)
+    eps = mach * mach
+    dx = 1.0 / n
+    dt = cfl * dx / mach
+    rhs = gaussian_random_field((n, n), 2 * corr_cells, seed + 1, rng)
+    return dict(rho=rho[None], beta_cc=(1.0 / rho)[None], a=eps / (adiabatic - 1), B=dt * dt, rhs=rhs[None], dx=dx)

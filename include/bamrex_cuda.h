@@ -404,6 +404,68 @@ BAMREX_API int bamrex_amr_dt_level(const bamrex_amr *amr, double *dt_level);
  * covered by the next finer level (NCOMP doubles; synchronises). */
 BAMREX_API int bamrex_amr_conserved_sums(bamrex_amr *amr, double *totals);
 
+/* ------------------------------------------------------------------ */
+/* Pressure Helmholtz operator and solver (IMEX path)                    */
+/* ------------------------------------------------------------------ */
+
+/* Domain boundary types of the linear operator (amrex::LinOpBCType as set
+ * by set_pressure_domain_BC, Source/IMEX/IMEX_O1.cpp:663-690): periodic,
+ * homogeneous Neumann, homogeneous Dirichlet on the domain face. */
+enum { BAMREX_LINOP_PERIODIC = 0, BAMREX_LINOP_NEUMANN = 1, BAMREX_LINOP_DIRICHLET = 2 };
+
+typedef struct bamrex_helmholtz bamrex_helmholtz;
+
+typedef struct bamrex_helmholtz_desc {
+    int spacedim;          /* 2 or 3 */
+    int n[3];              /* cells per direction: one box covering the domain */
+    double prob_lo[3];
+    double prob_hi[3];
+    int bc_lo[3];          /* BAMREX_LINOP_* */
+    int bc_hi[3];
+    int max_levels;        /* multigrid levels including the finest; 0 = coarsen while every n is even and >= 4 */
+    int nu1, nu2;          /* red+black sweeps before / after the coarse correction (0 = 2) */
+    int bottom_sweeps;     /* sweeps on the coarsest level (0 = 16) */
+} bamrex_helmholtz_desc;
+
+/* The operator of MLABecLaplacianGrad (Source/LinearSolver/MLALaplacianGrad.H):
+ *   y = A a x - B div(b grad x) + C c . grad x
+ * with Fapply = mlalapgrad_adotx (MLALapGrad_2D_K.H:9-33, MLALapGrad_3D_K.H:9-38)
+ * and Fsmooth = alapgrad_gsrb (MLALapGrad_2D_K.H:180-230, MLALapGrad_3D_K.H:258-324).
+ * Vectors are dense arrays of n[0]*n[1]*n[2] doubles, i fastest; face
+ * coefficients b[d] have one more entry along d.  Every pointer argument may
+ * be host or device memory.  Coefficients default to a = 1, b = 1, no c,
+ * scalars (A, B, C) = (1, 1, 0). */
+BAMREX_API int bamrex_helmholtz_create(bamrex_helmholtz **out, const bamrex_helmholtz_desc *desc, void *stream);
+BAMREX_API int bamrex_helmholtz_destroy(bamrex_helmholtz *h);
+BAMREX_API const char *bamrex_helmholtz_last_error(const bamrex_helmholtz *h);
+BAMREX_API int bamrex_helmholtz_num_levels(const bamrex_helmholtz *h);
+/* setScalars(A, B, C) (MLALaplacianGrad.H:380) */
+BAMREX_API int bamrex_helmholtz_set_scalars(bamrex_helmholtz *h, double a, double b, double c);
+/* setACoeffs: a cell field, or the constant alpha_const when alpha is NULL */
+BAMREX_API int bamrex_helmholtz_set_acoeffs(bamrex_helmholtz *h, const double *alpha, double alpha_const);
+/* setBCoeffs: face fields per direction */
+BAMREX_API int bamrex_helmholtz_set_bcoeffs(bamrex_helmholtz *h, const double *bx, const double *by, const double *bz);
+/* setBCoeffs from a cell field by average_cellcenter_to_face
+ * (IMEX_O1.cpp:599-609): b = (cell left + cell right) / 2, the boundary
+ * cell itself outside a non-periodic face. */
+BAMREX_API int bamrex_helmholtz_set_bcoeffs_from_cell(bamrex_helmholtz *h, const double *beta_cc);
+/* setCCoeffs: spacedim cell fields (component-major), or NULL for none */
+BAMREX_API int bamrex_helmholtz_set_ccoeffs(bamrex_helmholtz *h, const double *c);
+/* y = A x on the finest level (Fapply) */
+BAMREX_API int bamrex_helmholtz_apply(bamrex_helmholtz *h, const double *x, double *y);
+/* One colour (redblack 0 or 1) of the Gauss-Seidel smoother (Fsmooth) */
+BAMREX_API int bamrex_helmholtz_smooth(bamrex_helmholtz *h, double *phi, const double *rhs, int redblack);
+/* z = one multigrid V-cycle applied to r from a zero initial guess */
+BAMREX_API int bamrex_helmholtz_vcycle(bamrex_helmholtz *h, double *z, const double *r);
+/* Solve A x = rhs by BiCGStab preconditioned with one V-cycle, from the
+ * initial x, until ||rhs - A x||_2 <= max(tol_rel ||rhs||_2, tol_abs) or
+ * max_iter iterations (solve_pressure, IMEX_O1.cpp:616-640).  use_graph != 0
+ * replays each iteration as one CUDA graph. */
+BAMREX_API int bamrex_helmholtz_solve(bamrex_helmholtz *h, double *x, const double *rhs, double tol_rel,
+                                      double tol_abs, int max_iter, int use_graph, int *iters, double *rel_res);
+/* Kernels launched by the operator so far (graph replays excluded). */
+BAMREX_API long long bamrex_helmholtz_launches(const bamrex_helmholtz *h);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,108 @@
+"""The device Helmholtz operator (apply, red-black smoother, V-cycle) bit for
+bit against the restatement, and the BiCGStab/multigrid solve against the
+reference's solver test and on the low-Mach pressure problem."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def torch_cuda():
+    import torch
+    assert torch.cuda.is_available()
+    return torch
+
+
+def _random_op(D, n, bc, with_c, seed=0):
+    from oracle import helmholtz_oracle as H
+    rng = np.random.default_rng(seed)
+    shape = (n if D > 2 else 1, n, n)
+    a = rng.uniform(0.5, 1.5, shape)
+    faces = []
+    for d in range(D):
+        fs = list(shape)
+        fs[2 - d] += 1
+        f = rng.uniform(0.5, 2.0, fs)
+        if bc == H.PERIODIC:  # the same face on both sides of the periodic boundary
+            sl0 = [slice(None)] * 3
+            sln = [slice(None)] * 3
+            sl0[2 - d] = 0
+            sln[2 - d] = n
+            f[tuple(sln)] = f[tuple(sl0)]
+        faces.append(f)
+    c = [rng.uniform(-1, 1, shape) for _ in range(D)] if with_c else None
+    op = H.Op(D, (n,) * D, [1.0 / n] * D, (bc,) * 3, (bc,) * 3, 0.7, 3e-3, -0.4 if with_c else 0.0, a, faces, c)
+    return op
+
+
+def _device(op, **kw):
+    from bamrex_b200.helmholtz import Helmholtz
+    h = Helmholtz(op.D, op.n[:op.D], [0.0] * op.D, [1.0] * op.D, op.bc_lo[:op.D], op.bc_hi[:op.D], **kw)
+    h.setScalars(op.ascal, op.bscal, op.cscal)
+    h.setACoeffs(op.a)
+    h.setBCoeffs(op.b)
+    h.setCCoeffs(None if op.c is None else np.concatenate([cd.ravel() for cd in op.c]))
+    return h
+
+
+@pytest.mark.parametrize("D,bc,with_c", [(2, 0, False), (2, 1, True), (2, 2, False), (3, 0, True), (3, 1, False)])
+def test_apply_smooth_vcycle_bitwise(torch_cuda, D, bc, with_c):
+    from oracle import helmholtz_oracle as H
+    n = 32 if D == 2 else 16
+    op = _random_op(D, n, bc, with_c, seed=D + 3 * bc)
+    h = _device(op)
+    rng = np.random.default_rng(9)
+    x = rng.standard_normal(op.shape)
+    rhs = rng.standard_normal(op.shape)
+    np.testing.assert_array_equal(h.apply(x), op.apply(x))
+    for color in (0, 1):
+        np.testing.assert_array_equal(h.smooth(x, rhs, color), op.gsrb(x, rhs, color))
+    ops = H.hierarchy(op)
+    assert h.num_levels == len(ops)
+    np.testing.assert_array_equal(h.vcycle(rhs), H.vcycle(ops, rhs))
+    h.close()
+
+
+@pytest.mark.parametrize("D", [2, 3])
+@pytest.mark.parametrize("abc", [(1, 2, 0), (1, 2, -4)])
+def test_solve_reference_unit_domain(torch_cuda, D, abc):
+    """Tests/MLABecLapGrad01.cpp: interior residual <= 1e-12 ||rhs||_2."""
+    from oracle import helmholtz_oracle as H
+    a, b, c = abc
+    alpha, faces, gam, src, dx = H.unit_domain_problem(D, 8)
+    op = H.Op(D, (8,) * D, [dx] * D, (H.NEUMANN,) * 3, (H.NEUMANN,) * 3, a, b, c, alpha, faces, gam if c else None)
+    h = _device(op)
+    for graph in (False, True):
+        x, it, rr = h.solve(src, tol_rel=1e-12, use_graph=graph)
+        res = H.reference_residual(a, b, c, alpha, faces, gam, src, x, dx, D)
+        assert np.abs(res).max() <= 1e-12 * np.sqrt((src * src).sum())
+        assert rr <= 1e-12 and it <= 20
+    h.close()
+
+
+def test_solve_low_mach_pressure(torch_cuda):
+    """The IMEX pressure problem (lognormal density, beta = 1/rho) at 256^2:
+    relative residual 1e-8, checked with the restated operator."""
+    from bamrex_b200 import problems
+    from bamrex_b200.helmholtz import Helmholtz
+    from oracle import helmholtz_oracle as H
+    n = 256
+    p = problems.low_mach_pressure_problem(n=n, corr_cells=4)
+    h = Helmholtz(2, (n, n))
+    h.setScalars(1.0, p["B"], 0.0)
+    h.setACoeffs(p["a"])
+    h.setBCoeffsFromCell(p["beta_cc"])
+    x, it, rr = h.solve(p["rhs"], tol_rel=1e-8)
+    assert rr <= 1e-8 and it <= 30
+    bcc = p["beta_cc"]
+    faces = []
+    for d in range(2):
+        ax = 2 - d
+        f = 0.5 * (np.roll(bcc, 1, axis=ax) + bcc)
+        f = np.concatenate([f, f.take([0], axis=ax)], axis=ax)
+        faces.append(f)
+    op = H.Op(2, (n, n), [1.0 / n] * 2, (0, 0, 0), (0, 0, 0), 1.0, p["B"], 0.0, np.full((1, n, n), p["a"]), faces)
+    r = p["rhs"] - op.apply(x)
+    assert np.sqrt((r * r).sum()) <= 1.01e-8 * np.sqrt((p["rhs"] ** 2).sum())
+    h.close()

@@ -105,6 +105,8 @@ class LevelDesc(ctypes.Structure):
 MAX_LEVELS = 8
 # linear-operator boundary types (amrex::LinOpBCType subset)
 LINOP_PERIODIC, LINOP_NEUMANN, LINOP_DIRICHLET = range(3)
+# preconditioners of the flexible solve
+PRECOND_NETWORK, PRECOND_NETWORK_VCYCLE, PRECOND_VCYCLE, PRECOND_VCYCLE_NETWORK = range(4)
 
 
 class HelmholtzDesc(ctypes.Structure):
@@ -221,6 +223,18 @@ SIGNATURES = {
     "bamrex_helmholtz_vcycle": (_i, [_vp, _vp, _vp]),
     "bamrex_helmholtz_solve": (_i, [_vp, _vp, _vp, _d, _d, _i, _i, ctypes.POINTER(_i), _dp]),
     "bamrex_helmholtz_launches": (_ll, [_vp]),
+    "bamrex_precnet_create": (_i, [ctypes.POINTER(_vp), _i, _i, _i, ctypes.c_ulonglong, _vp]),
+    "bamrex_precnet_destroy": (_i, [_vp]),
+    "bamrex_precnet_last_error": (ctypes.c_char_p, [_vp]),
+    "bamrex_precnet_num_params": (_i, [_vp]),
+    "bamrex_precnet_resize": (_i, [_vp, _i, _i, _i]),
+    "bamrex_precnet_get_weights": (_i, [_vp, _vp]),
+    "bamrex_precnet_set_weights": (_i, [_vp, _vp]),
+    "bamrex_precnet_forward": (_i, [_vp, _vp, _vp]),
+    "bamrex_precnet_backward": (_i, [_vp, _vp, _vp]),
+    "bamrex_precnet_train_step": (_i, [_vp, _vp, _vp, ctypes.c_float, _dp]),
+    "bamrex_helmholtz_solve_learned": (_i, [_vp, _vp, _i, _vp, _vp, _d, _d, _i, _i, ctypes.POINTER(_i),
+                                            ctypes.POINTER(_i), _dp, ctypes.POINTER(_i)]),
 }
 
 _LIB = None

@@ -364,6 +364,107 @@ __global__ void face_avg_kernel(const double* __restrict__ cc, double* __restric
     }
 }
 
+// ---------------------------------------------------------------- FGMRES
+constexpr int kMaxVec = 64;
+
+__global__ void logbeta_cell_kernel(const double* __restrict__ beta, float* __restrict__ lb, long long n)
+{
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x)
+        lb[c] = (float)log(beta[c]);
+}
+
+// cell beta as the mean of the cell's 2D faces (for face coefficients given
+// directly)
+template <int D>
+__global__ void logbeta_faces_kernel(const HLev L, float* __restrict__ lb)
+{
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < L.ncell;
+         c += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(c % L.n[0]);
+        const int j = (int)((c / L.n[0]) % L.n[1]);
+        const int k = (int)(c / ((long long)L.n[0] * L.n[1]));
+        double s = 0.0;
+        for (int d = 0; d < D; ++d) {
+            const int ih = i + (d == 0), jh = j + (d == 1), kh = k + (d == 2);
+            s = s + L.b[d][fidx(L, d, i, j, k)] + L.b[d][fidx(L, d, ih, jh, kh)];
+        }
+        lb[c] = (float)log(s / (2 * D));
+    }
+}
+
+__global__ void net_input_kernel(const double* __restrict__ v, double scale, const float* __restrict__ lb,
+                                 float* __restrict__ in, long long n)
+{
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+        in[c] = (float)(v[c] * scale);
+        in[n + c] = lb[c];
+    }
+}
+
+__global__ void net_output_kernel(const float* __restrict__ out, double scale, double* __restrict__ z, long long n)
+{
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x)
+        z[c] = (double)out[c] * scale;
+}
+
+__global__ void mdot_partial_kernel(const double* __restrict__ V, long long ldv, int nvec, const double* __restrict__ w,
+                                    long long n, double* __restrict__ part)
+{
+    __shared__ double red[kThreads];
+    for (int i = 0; i < nvec; ++i) {
+        const double* vi = V + (long long)i * ldv;
+        double acc = 0.0;
+        for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x)
+            acc = acc + vi[c] * w[c];
+        red[threadIdx.x] = acc;
+        __syncthreads();
+        for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+            if (threadIdx.x < s) red[threadIdx.x] = red[threadIdx.x] + red[threadIdx.x + s];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) part[(long long)blockIdx.x * kMaxVec + i] = red[0];
+        __syncthreads();
+    }
+}
+
+__global__ void mdot_final_kernel(const double* __restrict__ part, int nblocks, double* __restrict__ out, int accumulate)
+{
+    __shared__ double red[kThreads];
+    const int i = blockIdx.x;
+    double acc = 0.0;
+    for (int q = threadIdx.x; q < nblocks; q += blockDim.x) acc = acc + part[(long long)q * kMaxVec + i];
+    red[threadIdx.x] = acc;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) red[threadIdx.x] = red[threadIdx.x] + red[threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[i] = accumulate ? out[i] + red[0] : red[0];
+}
+
+// w += sign * sum_i h[i] V_i
+__global__ void mupdate_kernel(double* __restrict__ w, const double* __restrict__ V, long long ldv, int nvec,
+                               const double* __restrict__ h, double sign, long long n)
+{
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+        double s = 0.0;
+        for (int i = 0; i < nvec; ++i) s = s + h[i] * V[(long long)i * ldv + c];
+        w[c] = w[c] + sign * s;
+    }
+}
+
+__global__ void scale_add_kernel(double* __restrict__ d, const double* __restrict__ src, long long n)
+{
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x)
+        d[c] = d[c] + src[c];
+}
+
+__global__ void scale_kernel(double* __restrict__ d, const double* __restrict__ src, double a, long long n)
+{
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x)
+        d[c] = a * src[c];
+}
+
 int grid_for(long long n)
 {
     const long long want = (n + kThreads - 1) / kThreads;
@@ -389,6 +490,12 @@ struct bamrex_helmholtz {
     KScal* d_scal = nullptr;
     KScal* h_scal = nullptr;  // pinned
     std::vector<double*> cbufs;  // per level, D * ncell: the C coefficients
+    // learned-preconditioner solve
+    float* logbeta = nullptr;    // log of the cell beta (network input)
+    double* krylov = nullptr;    // FGMRES: V (m + 1 vectors) then Z (m vectors)
+    int krylov_m = 0;
+    double* mpart = nullptr;     // multi-dot partials (kDotBlocks x kMaxVec)
+    double* hdev = nullptr;      // multi-dot results (kMaxVec + 1)
     cudaGraphExec_t iter_graph = nullptr;
     long long launches = 0;
     std::string err;
@@ -668,6 +775,17 @@ extern "C" int bamrex_helmholtz_create(bamrex_helmholtz** out, const bamrex_helm
         }
         H->own_stream = true;
     }
+    e = cudaMalloc((void**)&H->logbeta, sizeof(float) * n0);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&H->mpart, sizeof(double) * ((size_t)kDotBlocks * kMaxVec + kMaxVec + 1));
+    if (e != cudaSuccess) {
+        cudaFree(H->arena);
+        cudaFreeHost(H->h_scal);
+        if (H->logbeta) cudaFree(H->logbeta);
+        if (H->own_stream) cudaStreamDestroy(H->stream);
+        return fail(BAMREX_ERR_OOM, "cudaMalloc of the Krylov workspace failed");
+    }
+    H->hdev = H->mpart + (size_t)kDotBlocks * kMaxVec;
+    cudaMemset(H->logbeta, 0, sizeof(float) * n0);  // log(1): the default b = 1
     // default coefficients: a = 1, b = 1
     for (size_t l = 0; l < H->lev.size(); ++l) {
         HLev& L = H->lev[l];
@@ -688,6 +806,9 @@ extern "C" int bamrex_helmholtz_destroy(bamrex_helmholtz* H)
     if (!H) return BAMREX_OK;
     if (H->stream) cudaStreamSynchronize(H->stream);
     if (H->iter_graph) cudaGraphExecDestroy(H->iter_graph);
+    if (H->krylov) cudaFree(H->krylov);
+    if (H->logbeta) cudaFree(H->logbeta);
+    if (H->mpart) cudaFree(H->mpart);
     if (H->arena) cudaFree(H->arena);
     if (H->h_scal) cudaFreeHost(H->h_scal);
     if (H->own_stream) cudaStreamDestroy(H->stream);
@@ -737,6 +858,11 @@ extern "C" int bamrex_helmholtz_set_bcoeffs(bamrex_helmholtz* H, const double* b
         const long long nf = (long long)(L.n[0] + (q == 0)) * (L.n[1] + (q == 1)) * (L.n[2] + (q == 2));
         H_TRY(upload(H, L.b[q], src[q], (size_t)nf));
     }
+    if (H->logbeta) {
+        if (H->D == 3) logbeta_faces_kernel<3><<<grid_for(L.ncell), kThreads, 0, H->stream>>>(L, H->logbeta);
+        else logbeta_faces_kernel<2><<<grid_for(L.ncell), kThreads, 0, H->stream>>>(L, H->logbeta);
+        H_TRY(hck(H, cudaGetLastError(), "log beta"));
+    }
     H->coeffs_dirty = true;
     return BAMREX_OK;
 }
@@ -755,6 +881,10 @@ extern "C" int bamrex_helmholtz_set_bcoeffs_from_cell(bamrex_helmholtz* H, const
         face_avg_kernel<<<grid_for(nf), kThreads, 0, H->stream>>>(src, L.b[q], q, L.n[0], L.n[1], L.n[2],
                                                                  H->op.bc_lo[q] == BAMREX_LINOP_PERIODIC);
         H_TRY(hck(H, cudaGetLastError(), "face average"));
+    }
+    if (H->logbeta) {
+        logbeta_cell_kernel<<<grid_for(L.ncell), kThreads, 0, H->stream>>>(src, H->logbeta, L.ncell);
+        H_TRY(hck(H, cudaGetLastError(), "log beta"));
     }
     H->coeffs_dirty = true;
     return BAMREX_OK;
@@ -896,3 +1026,191 @@ extern "C" int bamrex_helmholtz_solve(bamrex_helmholtz* H, double* x, const doub
 }
 
 extern "C" long long bamrex_helmholtz_launches(const bamrex_helmholtz* H) { return H ? H->launches : 0; }
+
+// ---------------------------------------------------------------- learned
+namespace {
+
+int mdot(bamrex_helmholtz* H, const double* V, long long ldv, int nvec, const double* w, double* out, int accumulate)
+{
+    const long long n = H->lev[0].ncell;
+    mdot_partial_kernel<<<kDotBlocks, kThreads, 0, H->stream>>>(V, ldv, nvec, w, n, H->mpart);
+    H_TRY(hck(H, cudaGetLastError(), "multi-dot partial"));
+    mdot_final_kernel<<<nvec, kThreads, 0, H->stream>>>(H->mpart, kDotBlocks, out, accumulate);
+    return hck(H, cudaGetLastError(), "multi-dot final");
+}
+
+// z = M v with the network: input (v / rms(v), log beta), output scaled by
+// rms(v) dx0 dx1 / B.  rms_v is known on the host.
+int net_precondition(bamrex_helmholtz* H, bamrex_precnet* N, const double* v, double rms_v, double* z)
+{
+    const HLev& L = H->lev[0];
+    const long long n = L.ncell;
+    float* in = precnet_input(N);
+    net_input_kernel<<<grid_for(n), kThreads, 0, H->stream>>>(v, 1.0 / rms_v, H->logbeta, in, n);
+    H_TRY(hck(H, cudaGetLastError(), "network input"));
+    const int rc = precnet_run(N, H->stream);
+    if (rc != BAMREX_OK) {
+        H->err = last_error_text();
+        return rc;
+    }
+    H->launches += 20;
+    const double scale = rms_v * L.dx[0] * L.dx[1] / H->op.bscal;
+    net_output_kernel<<<grid_for(n), kThreads, 0, H->stream>>>(precnet_output(N), scale, z, n);
+    return hck(H, cudaGetLastError(), "network output");
+}
+
+}  // namespace
+
+extern "C" int bamrex_helmholtz_solve_learned(bamrex_helmholtz* H, bamrex_precnet* N, int mode, double* x,
+                                              const double* rhs, double tol_rel, double tol_abs, int max_iter, int restart,
+                                              int* iters, int* plain_iters, double* rel_res, int* fell_back)
+{
+    if (!H || !x || !rhs) return fail(BAMREX_ERR_ARG, "NULL argument");
+    if (mode < BAMREX_PRECOND_NETWORK || mode > BAMREX_PRECOND_VCYCLE_NETWORK) return hfail(H, BAMREX_ERR_ARG, "unknown mode");
+    if (!N && mode != BAMREX_PRECOND_VCYCLE) return hfail(H, BAMREX_ERR_ARG, "the mode needs a network");
+    if (H->D != 2) return hfail(H, BAMREX_ERR_UNSUPPORTED, "the learned preconditioner is two-dimensional");
+    if (restart < 1 || restart + 1 > kMaxVec) return hfail(H, BAMREX_ERR_ARG, "restart must be in [1, 63]");
+    if (max_iter < 0) return hfail(H, BAMREX_ERR_ARG, "max_iter must be >= 0");
+    const HLev& L = H->lev[0];
+    if (N) {
+        int nnx, nny, nb;
+        precnet_size(N, &nnx, &nny, &nb);
+        if (nnx != L.n[0] || nny != L.n[1] || nb != 1)
+            return hfail(H, BAMREX_ERR_ARG, "the network workspace must match the operator grid with batch 1");
+    }
+    for (int q = 0; q < 2 && N; ++q)
+        if (H->op.bc_lo[q] != BAMREX_LINOP_PERIODIC)
+            return hfail(H, BAMREX_ERR_UNSUPPORTED, "the network pads periodically: periodic domains only");
+    H_TRY(prepare(H));
+    const long long n = L.ncell;
+    const int m = restart;
+    if (H->krylov_m < m) {
+        if (H->krylov) cudaFree(H->krylov);
+        H->krylov = nullptr;
+        H->krylov_m = 0;
+        const cudaError_t e = cudaMalloc((void**)&H->krylov, sizeof(double) * (size_t)n * (2 * m + 1));
+        if (e != cudaSuccess) return hfail(H, BAMREX_ERR_OOM, "cudaMalloc of the FGMRES basis failed");
+        H->krylov_m = m;
+    }
+    double* V = H->krylov;
+    double* Z = H->krylov + (size_t)n * (m + 1);
+    double* hd = H->hdev;
+    H_TRY(upload(H, H->x, x, (size_t)n));
+    H_TRY(upload(H, H->bvec, rhs, (size_t)n));
+    H_TRY(dot(H, H->bvec, H->bvec, &hd[0]));
+    double hb = 0;
+    H_TRY(hck(H, cudaMemcpyAsync(&hb, hd, sizeof(double), cudaMemcpyDeviceToHost, H->stream), "copy"));
+    H_TRY(hck(H, cudaStreamSynchronize(H->stream), "sync"));
+    const double bnorm = std::sqrt(hb);
+    const double target = std::max(tol_rel * bnorm, tol_abs);
+    const double rms_unit = 1.0 / std::sqrt((double)n);  // rms of a unit vector
+    std::vector<double> Hm((size_t)(m + 1) * m), cs(m), sn(m), g(m + 1), y(m), hv(kMaxVec + 1);
+    int total = 0;
+    double rnorm = 0.0;
+    for (;;) {
+        // r = b - A x into V_0, beta = ||r||
+        H_TRY(launch_apply(H, 0, H->x, V, H->bvec, 1));
+        H_TRY(dot(H, V, V, &hd[0]));
+        H_TRY(hck(H, cudaMemcpyAsync(&hb, hd, sizeof(double), cudaMemcpyDeviceToHost, H->stream), "copy"));
+        H_TRY(hck(H, cudaStreamSynchronize(H->stream), "sync"));
+        rnorm = std::sqrt(hb);
+        if (rnorm <= target || total >= max_iter || !std::isfinite(rnorm)) break;
+        scale_kernel<<<grid_for(n), kThreads, 0, H->stream>>>(V, V, 1.0 / rnorm, n);
+        H_TRY(hck(H, cudaGetLastError(), "scale"));
+        std::fill(g.begin(), g.end(), 0.0);
+        g[0] = rnorm;
+        int k = 0;
+        for (int j = 0; j < m && total < max_iter; ++j) {
+            double* vj = V + (size_t)j * n;
+            double* zj = Z + (size_t)j * n;
+            double* w = V + (size_t)(j + 1) * n;
+            if (mode == BAMREX_PRECOND_VCYCLE) {
+                H_TRY(precondition(H, zj, vj));
+            } else if (mode == BAMREX_PRECOND_VCYCLE_NETWORK) {
+                // z = V(v); z += N(v - A z): the network on what the V-cycle left
+                H_TRY(precondition(H, zj, vj));
+                H_TRY(launch_apply(H, 0, zj, H->t, vj, 1));
+                H_TRY(dot(H, H->t, H->t, &hd[kMaxVec]));
+                double tt = 0;
+                H_TRY(hck(H, cudaMemcpyAsync(&tt, &hd[kMaxVec], sizeof(double), cudaMemcpyDeviceToHost, H->stream), "copy"));
+                H_TRY(hck(H, cudaStreamSynchronize(H->stream), "sync"));
+                if (tt > 0) {
+                    H_TRY(net_precondition(H, N, H->t, std::sqrt(tt / (double)n), H->sh));
+                    scale_add_kernel<<<grid_for(n), kThreads, 0, H->stream>>>(zj, H->sh, n);
+                    H_TRY(hck(H, cudaGetLastError(), "combine"));
+                }
+            } else {
+                H_TRY(net_precondition(H, N, vj, rms_unit, zj));
+                if (mode == BAMREX_PRECOND_NETWORK_VCYCLE) {
+                    // z += V(v - A z): one V-cycle on what the network left
+                    H_TRY(launch_apply(H, 0, zj, H->t, vj, 1));
+                    H_TRY(precondition(H, H->sh, H->t));
+                    scale_add_kernel<<<grid_for(n), kThreads, 0, H->stream>>>(zj, H->sh, n);
+                    H_TRY(hck(H, cudaGetLastError(), "combine"));
+                }
+            }
+            H_TRY(launch_apply(H, 0, zj, w, nullptr, 0));
+            // classical Gram-Schmidt, twice
+            H_TRY(mdot(H, V, n, j + 1, w, hd, 0));
+            mupdate_kernel<<<grid_for(n), kThreads, 0, H->stream>>>(w, V, n, j + 1, hd, -1.0, n);
+            H_TRY(hck(H, cudaGetLastError(), "orthogonalise"));
+            H_TRY(mdot(H, V, n, j + 1, w, hd + kMaxVec / 2, 0));
+            mupdate_kernel<<<grid_for(n), kThreads, 0, H->stream>>>(w, V, n, j + 1, hd + kMaxVec / 2, -1.0, n);
+            H_TRY(hck(H, cudaGetLastError(), "orthogonalise"));
+            H_TRY(dot(H, w, w, hd + kMaxVec));
+            H_TRY(hck(H, cudaMemcpyAsync(hv.data(), hd, sizeof(double) * (kMaxVec + 1), cudaMemcpyDeviceToHost, H->stream),
+                      "copy"));
+            H_TRY(hck(H, cudaStreamSynchronize(H->stream), "sync"));
+            for (int i = 0; i <= j; ++i) Hm[(size_t)i * m + j] = hv[i] + hv[kMaxVec / 2 + i];
+            const double hn = std::sqrt(hv[kMaxVec]);
+            Hm[(size_t)(j + 1) * m + j] = hn;
+            if (hn > 0) {
+                scale_kernel<<<grid_for(n), kThreads, 0, H->stream>>>(w, w, 1.0 / hn, n);
+                H_TRY(hck(H, cudaGetLastError(), "scale"));
+            }
+            // Givens rotations on the new column
+            for (int i = 0; i < j; ++i) {
+                const double a = Hm[(size_t)i * m + j], b = Hm[(size_t)(i + 1) * m + j];
+                Hm[(size_t)i * m + j] = cs[i] * a + sn[i] * b;
+                Hm[(size_t)(i + 1) * m + j] = -sn[i] * a + cs[i] * b;
+            }
+            const double a = Hm[(size_t)j * m + j], b = Hm[(size_t)(j + 1) * m + j];
+            const double den = std::hypot(a, b);
+            cs[j] = den > 0 ? a / den : 1.0;
+            sn[j] = den > 0 ? b / den : 0.0;
+            Hm[(size_t)j * m + j] = den;
+            Hm[(size_t)(j + 1) * m + j] = 0.0;
+            g[j + 1] = -sn[j] * g[j];
+            g[j] = cs[j] * g[j];
+            ++total;
+            k = j + 1;
+            if (std::fabs(g[j + 1]) <= target || hn == 0.0) break;
+        }
+        // y = R^{-1} g; x += Z y
+        for (int i = k - 1; i >= 0; --i) {
+            double sres = g[i];
+            for (int q = i + 1; q < k; ++q) sres -= Hm[(size_t)i * m + q] * y[q];
+            y[i] = sres / Hm[(size_t)i * m + i];
+        }
+        H_TRY(hck(H, cudaMemcpyAsync(hd, y.data(), sizeof(double) * k, cudaMemcpyHostToDevice, H->stream), "copy"));
+        mupdate_kernel<<<grid_for(n), kThreads, 0, H->stream>>>(H->x, Z, n, k, hd, 1.0, n);
+        H_TRY(hck(H, cudaGetLastError(), "update x"));
+    }
+    int fb = 0, pit = 0;
+    double rr = bnorm > 0 ? rnorm / bnorm : rnorm;
+    if (!(rnorm <= target)) {
+        // fallback: the plain solve from the current iterate
+        fb = 1;
+        H_TRY(hck(H, cudaMemcpyAsync(x, H->x, sizeof(double) * n, cudaMemcpyDefault, H->stream), "copy out"));
+        H_TRY(hck(H, cudaStreamSynchronize(H->stream), "sync"));
+        H_TRY(bamrex_helmholtz_solve(H, x, rhs, tol_rel, tol_abs, 1000, 1, &pit, &rr));
+    } else {
+        H_TRY(hck(H, cudaMemcpyAsync(x, H->x, sizeof(double) * n, cudaMemcpyDefault, H->stream), "copy out"));
+        H_TRY(hck(H, cudaStreamSynchronize(H->stream), "sync"));
+    }
+    if (iters) *iters = total;
+    if (plain_iters) *plain_iters = pit;
+    if (rel_res) *rel_res = rr;
+    if (fell_back) *fell_back = fb;
+    return BAMREX_OK;
+}

@@ -136,4 +136,12 @@ cudaError_t launch_register_faces(int D, int dir, int method, bool fp32, const C
                                   const RegisterTask& t, int NC, double dt, double dx_dir, double scale,
                                   cudaStream_t s);
 
+// The preconditioner network (precnet.cu) on device buffers: its input
+// buffer (batch x 2 x ny x nx floats), output buffer (batch x ny x nx),
+// size, and a forward pass on stream s.
+float* precnet_input(bamrex_precnet* N);
+const float* precnet_output(bamrex_precnet* N);
+void precnet_size(const bamrex_precnet* N, int* nx, int* ny, int* batch);
+int precnet_run(bamrex_precnet* N, cudaStream_t s);
+
 }  // namespace bamrex

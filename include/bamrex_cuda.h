@@ -466,6 +466,58 @@ BAMREX_API int bamrex_helmholtz_solve(bamrex_helmholtz *h, double *x, const doub
 /* Kernels launched by the operator so far (graph replays excluded). */
 BAMREX_API long long bamrex_helmholtz_launches(const bamrex_helmholtz *h);
 
+/* ------------------------------------------------------------------ */
+/* Learned preconditioner (no counterpart in the reference)             */
+/* ------------------------------------------------------------------ */
+
+/* A 2D convolutional network M(r) ~ A^{-1} r for the pressure solve: four
+ * resolution levels, 16 channels, 3x3 kernels, periodic padding, BF16
+ * weights with FP32 accumulation; inputs (r / rms(r), log beta) per cell,
+ * output the correction scaled by dx^2 / B.  Trained on the device with the
+ * library's own forward, backward and Adam kernels. */
+typedef struct bamrex_precnet bamrex_precnet;
+BAMREX_API int bamrex_precnet_create(bamrex_precnet **out, int nx, int ny, int batch, unsigned long long seed,
+                                     void *stream);
+BAMREX_API int bamrex_precnet_destroy(bamrex_precnet *net);
+BAMREX_API const char *bamrex_precnet_last_error(const bamrex_precnet *net);
+BAMREX_API int bamrex_precnet_num_params(const bamrex_precnet *net);
+/* Change the grid (sides multiples of 8) and batch of the workspace. */
+BAMREX_API int bamrex_precnet_resize(bamrex_precnet *net, int nx, int ny, int batch);
+/* FP32 master weights (num_params floats). */
+BAMREX_API int bamrex_precnet_get_weights(bamrex_precnet *net, float *w);
+BAMREX_API int bamrex_precnet_set_weights(bamrex_precnet *net, const float *w);
+/* in: batch x 2 x ny x nx floats; out: batch x ny x nx floats. */
+BAMREX_API int bamrex_precnet_forward(bamrex_precnet *net, const float *in, float *out);
+/* Parameter gradient of sum(out * dout) after a forward on the same input. */
+BAMREX_API int bamrex_precnet_backward(bamrex_precnet *net, const float *dout, float *grad);
+/* One Adam step on the relative squared error ||out - target||^2 / ||target||^2
+ * averaged over the batch; *loss is the value before the step. */
+BAMREX_API int bamrex_precnet_train_step(bamrex_precnet *net, const float *in, const float *target, float lr,
+                                         double *loss);
+
+/* Preconditioners of the flexible solve: the network alone; the network
+ * followed by one V-cycle on the residual it leaves (z = N(v) + V(v - A N(v)));
+ * the V-cycle alone (the same solve without the network); or the V-cycle
+ * followed by the network on what it left (z = V(v) + N(v - A V(v))). */
+enum {
+    BAMREX_PRECOND_NETWORK = 0,
+    BAMREX_PRECOND_NETWORK_VCYCLE = 1,
+    BAMREX_PRECOND_VCYCLE = 2,
+    BAMREX_PRECOND_VCYCLE_NETWORK = 3
+};
+
+/* Solve A x = rhs by restarted flexible GMRES(restart) with the chosen
+ * preconditioner (the network sized to the operator's grid, batch 1; NULL
+ * for BAMREX_PRECOND_VCYCLE; periodic domains); if it has not reached the
+ * tolerance after max_iter iterations, the plain BiCGStab/multigrid solve
+ * continues from its iterate (*fell_back = 1).  Same stopping rule as
+ * bamrex_helmholtz_solve; *iters counts the GMRES iterations and
+ * *plain_iters the fallback's. */
+BAMREX_API int bamrex_helmholtz_solve_learned(bamrex_helmholtz *h, bamrex_precnet *net, int mode, double *x,
+                                              const double *rhs, double tol_rel, double tol_abs, int max_iter,
+                                              int restart, int *iters, int *plain_iters, double *rel_res,
+                                              int *fell_back);
+
 #ifdef __cplusplus
 }
 #endif

@@ -82,6 +82,10 @@ class CParm(ctypes.Structure):
     ]
 
 
+class Region(ctypes.Structure):
+    _fields_ = [("box", ctypes.c_int), ("lo", ctypes.c_int * 3), ("hi", ctypes.c_int * 3), ("offset", ctypes.c_longlong)]
+
+
 class LevelDesc(ctypes.Structure):
     _fields_ = [
         ("spacedim", ctypes.c_int),
@@ -185,6 +189,12 @@ SIGNATURES = {
     "bamrex_level_reset_counters": (_i, [_vp]),
     "bamrex_level_sweep_times": (_i, [_vp, _dp, ctypes.POINTER(_ll)]),
     "bamrex_conserved_sums_noalloc": (_i, [_i, ctypes.POINTER(Box), ctypes.POINTER(Array4), _i, _dp, _dp, _vp]),
+    "bamrex_level_set_halo": (_i, [_vp, _i, ctypes.POINTER(Region), _i, ctypes.POINTER(Region), _i]),
+    "bamrex_level_halo_pack": (_i, [_vp, _i, _vp]),
+    "bamrex_level_halo_unpack": (_i, [_vp, _i, _vp]),
+    "bamrex_level_fill_dir": (_i, [_vp, _i]),
+    "bamrex_level_sweep_dir": (_i, [_vp, _i, _d, _i]),
+    "bamrex_level_wave_speed": (_i, [_vp, _dp]),
     "bamrex_level_tag": (_i, [_vp, _i, _i, _d, _i, _i, _i, _d, ctypes.c_char_p]),
     "bamrex_coupling_create": (_i, [ctypes.POINTER(_vp), _vp, _vp, _i]),
     "bamrex_coupling_destroy": (_i, [_vp]),

@@ -615,10 +615,6 @@ int level_fill(bamrex_level* L, int d, int parity, const StepScalars* scal)
                         "ghost fill");
 }
 
-}  // namespace bamrex
-
-namespace {
-
 int level_sweep(bamrex_level* L, int d, int parity, double dt_host, const StepScalars* scal, bool reduce_ws,
                 bool allow_timing)
 {
@@ -646,10 +642,6 @@ int level_sweep(bamrex_level* L, int d, int parity, double dt_host, const StepSc
     }
     return BAMREX_OK;
 }
-
-}  // namespace
-
-namespace bamrex {
 
 int level_step(bamrex_level* L, int parity, double dt_host, StepScalars* scal, bool allow_timing)
 {
@@ -920,6 +912,8 @@ extern "C" int bamrex_level_destroy(bamrex_level* L)
         cudaEventDestroy(ev.second);
     }
     if (L->arena) cudaFree(L->arena);
+    for (int d = 0; d < 3; ++d)
+        if (L->halo_mem[d]) cudaFree(L->halo_mem[d]);
     if (L->h_scal) cudaFreeHost(L->h_scal);
     if (L->own_stream && L->stream) cudaStreamDestroy(L->stream);
     delete L;

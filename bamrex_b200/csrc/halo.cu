@@ -1,0 +1,146 @@
+// A level split over several processes: halo exchange tables and the step
+// taken one sweep at a time, so a host driver can exchange the ghost slabs
+// of boxes owned by other ranks between sweeps (the FillBoundary of
+// bamrexBCData::fill_consv_boundary across ranks, called after every sweep
+// at Source/AmrLevelAdv_advance.cpp:356).  The level holds only this rank's
+// boxes; its own ghost fill covers copies between them and the physical
+// boundaries, and the host driver supplies the rest through these buffers.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "bamrex_cuda.h"
+#include "level_impl.h"
+
+using namespace bamrex;
+
+extern "C" int bamrex_level_set_halo(bamrex_level* L, int dir, const bamrex_region* send, int nsend,
+                                     const bamrex_region* recv, int nrecv)
+{
+    if (!L || dir < 0 || dir >= L->D || nsend < 0 || nrecv < 0 || (nsend && !send) || (nrecv && !recv))
+        return fail(BAMREX_ERR_ARG, "bad argument");
+    const int nb = (int)L->boxes.size();
+    std::vector<PackBox> pb[2];
+    std::vector<FabDev> fb[2][2];
+    const bamrex_region* src[2] = { send, recv };
+    const int cnt[2] = { nsend, nrecv };
+    long long cells[2] = { 0, 0 };
+    for (int s = 0; s < 2; ++s) {
+        for (int q = 0; q < cnt[s]; ++q) {
+            const bamrex_region& r = src[s][q];
+            if (r.box < 0 || r.box >= nb) return L->set_err(fail(BAMREX_ERR_ARG, "halo region names an unknown box"));
+            const bamrex_box& B = L->boxes[r.box];
+            for (int d = 0; d < 3; ++d) {
+                const int g = d < L->D ? L->ngrow : 0;
+                if (r.hi[d] < r.lo[d] || r.lo[d] < B.lo[d] - g || r.hi[d] > B.hi[d] + g)
+                    return L->set_err(fail(BAMREX_ERR_ARG, "halo region outside its box's fab"));
+            }
+            if (r.offset != cells[s]) return L->set_err(fail(BAMREX_ERR_ARG, "halo regions must be packed in order"));
+            PackBox p;
+            for (int d = 0; d < 3; ++d) {
+                p.lo[d] = r.lo[d];
+                p.hi[d] = r.hi[d];
+            }
+            p.cell_begin = r.offset;
+            cells[s] += (long long)(r.hi[0] - r.lo[0] + 1) * (r.hi[1] - r.lo[1] + 1) * (r.hi[2] - r.lo[2] + 1);
+            pb[s].push_back(p);
+            for (int par = 0; par < 2; ++par) fb[s][par].push_back(L->fab[par][r.box]);
+        }
+    }
+    if (L->halo_mem[dir]) {
+        cudaStreamSynchronize(L->stream);
+        cudaFree(L->halo_mem[dir]);
+        L->halo_mem[dir] = nullptr;
+    }
+    size_t off = 0;
+    size_t o_pb[2], o_fb[2][2];
+    for (int s = 0; s < 2; ++s) {
+        o_pb[s] = off;
+        off = align_up(off + sizeof(PackBox) * std::max<size_t>(1, pb[s].size()), 256);
+        for (int par = 0; par < 2; ++par) {
+            o_fb[s][par] = off;
+            off = align_up(off + sizeof(FabDev) * std::max<size_t>(1, fb[s][par].size()), 256);
+        }
+    }
+    cudaError_t e = cudaMalloc((void**)&L->halo_mem[dir], off);
+    if (e != cudaSuccess) return L->set_err(fail(BAMREX_ERR_OOM, "cudaMalloc of the halo tables failed"));
+    char* m = L->halo_mem[dir];
+    bamrex_level::Halo* H[2] = { &L->halo_send[dir], &L->halo_recv[dir] };
+    for (int s = 0; s < 2; ++s) {
+        H[s]->boxes = (PackBox*)(m + o_pb[s]);
+        H[s]->nops = (int)pb[s].size();
+        H[s]->cells = cells[s];
+        if (!pb[s].empty()) e = cudaMemcpy(H[s]->boxes, pb[s].data(), sizeof(PackBox) * pb[s].size(), cudaMemcpyHostToDevice);
+        for (int par = 0; par < 2 && e == cudaSuccess; ++par) {
+            H[s]->fabs[par] = (FabDev*)(m + o_fb[s][par]);
+            if (!fb[s][par].empty())
+                e = cudaMemcpy(H[s]->fabs[par], fb[s][par].data(), sizeof(FabDev) * fb[s][par].size(), cudaMemcpyHostToDevice);
+        }
+        if (e != cudaSuccess) return L->set_err(cuda_fail(e, "halo table upload"));
+    }
+    return BAMREX_OK;
+}
+
+extern "C" int bamrex_level_halo_pack(bamrex_level* L, int dir, double* sendbuf)
+{
+    if (!L || dir < 0 || dir >= L->D) return fail(BAMREX_ERR_ARG, "bad argument");
+    const auto& h = L->halo_send[dir];
+    if (!h.cells) return BAMREX_OK;
+    if (!sendbuf) return L->set_err(fail(BAMREX_ERR_ARG, "NULL buffer"));
+    return level_launch(L, launch_pack(L->NC, L->fp32, h.fabs[L->cur], h.boxes, h.nops, h.cells, sendbuf, 1, L->stream),
+                        "halo pack");
+}
+
+extern "C" int bamrex_level_halo_unpack(bamrex_level* L, int dir, const double* recvbuf)
+{
+    if (!L || dir < 0 || dir >= L->D) return fail(BAMREX_ERR_ARG, "bad argument");
+    const auto& h = L->halo_recv[dir];
+    if (!h.cells) return BAMREX_OK;
+    if (!recvbuf) return L->set_err(fail(BAMREX_ERR_ARG, "NULL buffer"));
+    return level_launch(L, launch_pack(L->NC, L->fp32, h.fabs[L->cur], h.boxes, h.nops, h.cells, const_cast<double*>(recvbuf),
+                                       0, L->stream),
+                        "halo unpack");
+}
+
+extern "C" int bamrex_level_fill_dir(bamrex_level* L, int dir)
+{
+    if (!L || dir < 0 || dir >= L->D) return fail(BAMREX_ERR_ARG, "bad argument");
+    return level_fill(L, dir, L->cur, nullptr);
+}
+
+extern "C" int bamrex_level_sweep_dir(bamrex_level* L, int dir, double dt, int reduce_ws)
+{
+    if (!L || dir < 0 || dir >= L->D) return fail(BAMREX_ERR_ARG, "bad argument");
+    if (!(dt > 0)) return L->set_err(fail(BAMREX_ERR_ARG, "dt must be positive"));
+    if (!L->reg_tasks[dir].empty())
+        return L->set_err(fail(BAMREX_ERR_UNSUPPORTED, "flux registers are recorded by bamrex_level_advance only"));
+    if (reduce_ws) {
+        const cudaError_t e = cudaMemsetAsync(&L->d_scal->ws_bits, 0, sizeof(unsigned long long), L->stream);
+        if (e != cudaSuccess) return L->set_err(cuda_fail(e, "memset"));
+    }
+    BX_TRY(level_sweep(L, dir, L->cur, dt, nullptr, reduce_ws != 0, true));
+    L->cur ^= 1;
+    L->ws_valid = reduce_ws != 0;
+    return BAMREX_OK;
+}
+
+extern "C" int bamrex_level_wave_speed(bamrex_level* L, double* ws)
+{
+    if (!L || !ws) return fail(BAMREX_ERR_ARG, "NULL argument");
+    if (!L->ws_valid) {
+        cudaError_t e = cudaMemsetAsync(&L->d_scal->ws_bits, 0, sizeof(unsigned long long), L->stream);
+        if (e != cudaSuccess) return L->set_err(cuda_fail(e, "memset"));
+        BX_TRY(level_launch(L, launch_max_wave_speed(L->D, L->fp32, L->d_fab[L->cur], L->d_pack, (int)L->boxes.size(),
+                                                     L->ncells, L->k, &L->d_scal->ws_bits, nullptr, L->stream),
+                            "max wave speed"));
+    }
+    unsigned long long bits = 0;
+    cudaError_t e = cudaMemcpyAsync(&bits, &L->d_scal->ws_bits, sizeof(bits), cudaMemcpyDeviceToHost, L->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(L->stream);
+    if (e != cudaSuccess) return L->set_err(cuda_fail(e, "wave speed"));
+    L->ws_valid = true;
+    std::memcpy(ws, &bits, sizeof(double));
+    return BAMREX_OK;
+}

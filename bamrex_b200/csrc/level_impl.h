@@ -91,6 +91,17 @@ struct bamrex_level {
     // flux-register recording by direction (set by the coarse/fine coupling)
     std::vector<bamrex::RegisterTask> reg_tasks[3];
 
+    // halo exchange with other ranks, per direction: ops of the send and
+    // receive buffers (device tables, one fab table per parity)
+    struct Halo {
+        bamrex::PackBox* boxes = nullptr;  // region + buffer cell offset
+        bamrex::FabDev* fabs[2] = { nullptr, nullptr };
+        int nops = 0;
+        long long cells = 0;
+    };
+    Halo halo_send[3], halo_recv[3];
+    char* halo_mem[3] = { nullptr, nullptr, nullptr };
+
     // accounting
     long long launches = 0;
     bool timing = false;
@@ -126,6 +137,10 @@ struct BoxIndex {
 
 int level_launch(bamrex_level* L, cudaError_t e, const char* what);
 int level_fill(bamrex_level* L, int d, int parity, const StepScalars* scal);
+// One sweep of direction d from buffer `parity` into parity ^ 1; reduce_ws:
+// also reduce the max wave speed of the output into d_scal->ws_bits.
+int level_sweep(bamrex_level* L, int d, int parity, double dt_host, const StepScalars* scal, bool reduce_ws,
+                bool allow_timing);
 // One split step starting from buffer `parity`; the result lands in
 // parity ^ (D & 1).  dt from the host (scal == nullptr) or from the device.
 int level_step(bamrex_level* L, int parity, double dt_host, StepScalars* scal, bool allow_timing);

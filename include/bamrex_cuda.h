@@ -273,6 +273,40 @@ BAMREX_API int bamrex_level_reset_counters(bamrex_level *level);
 BAMREX_API int bamrex_level_sweep_times(bamrex_level *level, double *ms_by_dir, long long *launches_by_dir);
 
 /* ------------------------------------------------------------------ */
+/* A level split over processes (one GPU per rank)                      */
+/* ------------------------------------------------------------------ */
+
+/* A level created with only this rank's boxes fills the ghosts those boxes
+ * can fill themselves (copies between local boxes, physical boundaries);
+ * the cells that come from other ranks' boxes travel through these buffers.
+ * This is the FillBoundary step of bamrexBCData::fill_consv_boundary, run
+ * after every sweep (Source/AmrLevelAdv_advance.cpp:356), across ranks. */
+typedef struct bamrex_region {
+    int box;            /* index into the level's boxes */
+    int lo[3], hi[3];   /* cells of that box's fab (valid or ghost) */
+    long long offset;   /* first cell in the buffer; regions are packed in order */
+} bamrex_region;
+
+/* Direction dir's send regions (valid cells read into the send buffer) and
+ * receive regions (ghost cells written from the receive buffer).  A buffer
+ * holds, region after region, NCOMP x (region cells) doubles, component
+ * slowest: value (cell c, component n) of a region at offset o is at
+ * buf[o*NCOMP + n*cells + c]. */
+BAMREX_API int bamrex_level_set_halo(bamrex_level *level, int dir, const bamrex_region *send, int nsend,
+                                     const bamrex_region *recv, int nrecv);
+/* Device buffers, asynchronous on the level's stream. */
+BAMREX_API int bamrex_level_halo_pack(bamrex_level *level, int dir, double *sendbuf);
+BAMREX_API int bamrex_level_halo_unpack(bamrex_level *level, int dir, const double *recvbuf);
+/* The step one piece at a time: ghost fill of direction dir, then its sweep
+ * (reduce_ws != 0 also reduces the max wave speed of the result); after the
+ * last direction the level's current state is the new time level. */
+BAMREX_API int bamrex_level_fill_dir(bamrex_level *level, int dir);
+BAMREX_API int bamrex_level_sweep_dir(bamrex_level *level, int dir, double dt, int reduce_ws);
+/* Max wave speed |u| + c over this rank's valid cells (from the last sweep
+ * that reduced it, else computed); synchronises the stream. */
+BAMREX_API int bamrex_level_wave_speed(bamrex_level *level, double *ws);
+
+/* ------------------------------------------------------------------ */
 /* AMR: coarse/fine coupling of two levels                              */
 /* ------------------------------------------------------------------ */
 

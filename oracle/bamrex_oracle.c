@@ -694,6 +694,27 @@ int oracle_advance_explicit(const o_level *L, double *S1, double *S2, double tim
     return err;
 }
 
+/* One sweep of advance_explicit (Source/AmrLevelAdv_advance.cpp:290-341) in
+ * direction d over every box: Sout's valid cells from Sin (ghost-filled).
+ * Ghost cells of Sout are not touched. */
+int oracle_sweep_dir(const o_level *L, const double *Sin, double *Sout, int d, double dt, int method,
+                     const oracle_parm *parm)
+{
+    const int D = L->D, NC = D + 2;
+    int err = 0;
+#pragma omp parallel for schedule(dynamic) reduction(| : err)
+    for (int b = 0; b < L->nboxes; ++b) {
+        o_box bx = level_box(L, b);
+        o_a4 Uin = level_fab(L, (double *)Sin, b), Uout = level_fab(L, Sout, b);
+        o_box fb = surrounding_nodes(bx, d);
+        o_a4 flux = alloc_fab(fb, NC);
+        if (oracle_compute_flux(D, method, d, bx.lo, bx.hi, flux, Uin, L->dx, dt, parm) != 0) err |= 1;
+        oracle_sweep_update(D, d, bx.lo, bx.hi, Uout, Uin, flux, L->dx, dt);
+        free(flux.p);
+    }
+    return err;
+}
+
 int oracle_num_threads(void)
 {
 #ifdef _OPENMP

@@ -120,6 +120,9 @@ def lib(fast: bool = False) -> ctypes.CDLL:
     L.oracle_advance_explicit.argtypes = [ctypes.POINTER(_OLevel), dp, dp, ctypes.c_double, ctypes.c_double,
                                           ctypes.c_int, ctypes.POINTER(_OParm), ppd, ppll, ppll, ctypes.c_int]
     L.oracle_advance_explicit.restype = ctypes.c_int
+    L.oracle_sweep_dir.argtypes = [ctypes.POINTER(_OLevel), dp, dp, ctypes.c_int, ctypes.c_double, ctypes.c_int,
+                                   ctypes.POINTER(_OParm)]
+    L.oracle_sweep_dir.restype = ctypes.c_int
     L.oracle_num_threads.restype = ctypes.c_int
     _LIBS[fast] = L
     return L
@@ -369,6 +372,12 @@ class LevelLayout:
                                                ctypes.byref(cp), None, None, None, nthreads)
         if rc != 0:
             raise ValueError("oracle advance failed")
+
+    def sweep_dir(self, Sin, Sout, d, dt, method, parm: Parm, fast=False):
+        """One sweep in direction d: Sout's valid cells from ghost-filled Sin."""
+        cp = parm.to_c()
+        if lib(fast).oracle_sweep_dir(ctypes.byref(self._c), _dp(Sin), _dp(Sout), d, dt, method, ctypes.byref(cp)) != 0:
+            raise ValueError("oracle sweep failed")
 
     def advance_explicit_fluxes(self, S1, S2, time, dt, method, parm: Parm, nthreads=0, fast=False):
         """advance_explicit that also returns the fluxes of every sweep:

@@ -1,0 +1,78 @@
+"""The device side of the multi-rank level on one GPU: two Levels hold the
+two halves of the boxes (as two ranks would), their halo buffers are packed
+and unpacked by the library and handed across in this process (no
+collective), and after the split steps the union equals one Level over all
+boxes bit for bit."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("D,n,mgs,bc", [(2, 128, 32, 0), (2, 96, 32, 1), (3, 32, 16, 2)])
+def test_two_levels_with_device_halos_equal_one(oracle, D, n, mgs, bc):
+    import torch
+    assert torch.cuda.is_available()
+    import bamrex_b200 as bx
+    from bamrex_b200 import problems
+    from bamrex_b200.distributed import DeviceEngine, HaloPlan, partition
+    hi = tuple(n - 1 if d < D else 0 for d in range(3))
+    boxes = oracle.decompose(D, (0, 0, 0), hi, mgs)
+    owners = partition(boxes, 2)
+    u0 = problems.random_states(D, tuple(reversed([n if d < D else 1 for d in range(3)])), seed=8) if D == 2 \
+        else problems.blast_3d(n, radius=0.3)
+    kw = dict(cfl=0.8, bc_lo=(bc,) * 3, bc_hi=(bc,) * 3)
+    stream = torch.cuda.current_stream()
+    parm = bx.Parm(D, limiter=bx.VAN_LEER)
+    ranks = []
+    for r in range(2):
+        mine = [boxes[b] for b in range(len(boxes)) if owners[b] == r]
+        lev = bx.Level(D, (0, 0, 0), hi, [0.0] * D, [1.0] * D, mine, parm, stream=stream, **kw)
+        full = np.zeros_like(u0)
+        lev.set_state(u0)
+        eng = DeviceEngine(lev)
+        plan = HaloPlan(D, (0, 0, 0), hi, boxes, owners, 2, (bc,) * 3, (bc,) * 3, r)
+        bufs = []
+        for d in range(D):
+            send, recv = plan.dirs[d]
+            eng.set_halo(d, send, recv)
+            bufs.append((eng.buffer(send["cells"]), eng.buffer(recv["cells"])))
+        ranks.append((lev, eng, plan, bufs))
+        del full
+    ref = bx.Level(D, (0, 0, 0), hi, [0.0] * D, [1.0] * D, boxes, parm, stream=stream, **kw)
+    ref.set_state(u0)
+    NC = D + 2
+    for step in range(3):
+        ws = max(e.wave_speed() for _, e, _, _ in ranks)
+        dt = 0.8 * min(1.0 / n / ws for _ in range(D))
+        for d in range(D):
+            for lev, e, plan, bufs in ranks:
+                e.pack(d, bufs[d][0])
+            for r, (lev, e, plan, bufs) in enumerate(ranks):
+                peer = ranks[1 - r]
+                recv = plan.dirs[d][1]
+                psend = peer[2].dirs[d][0]
+                for p, start, cnt in recv["peers"]:
+                    ps = [q for q in psend["peers"] if q[0] == r][0]
+                    bufs[d][1][start * NC:(start + cnt) * NC] = peer[3][d][0][ps[1] * NC:(ps[1] + cnt) * NC]
+            for lev, e, plan, bufs in ranks:
+                e.unpack(d, bufs[d][1])
+                e.fill_dir(d)
+                e.sweep_dir(d, dt, d == D - 1)
+        ref.advance(0.0, dt)
+    torch.cuda.synchronize()
+    got = np.full_like(u0, np.nan)
+    for lev, e, plan, bufs in ranks:
+        part = np.full_like(u0, np.nan)
+        packed = np.empty(lev.packing.size)
+        lev.copy_out_ptr(packed.ctypes.data)
+        lev.sync()
+        lev.packing.unpack(packed, part)
+        m = ~np.isnan(part)
+        got[m] = part[m]
+    want = ref.get_state()
+    assert not np.isnan(got).any()
+    np.testing.assert_array_equal(got, want)
+    for lev, *_ in ranks:
+        lev.close()
+    ref.close()

@@ -173,6 +173,7 @@ SIGNATURES = {
     "bamrex_level_destroy": (_i, [_vp]),
     "bamrex_level_last_error": (ctypes.c_char_p, [_vp]),
     "bamrex_level_num_cells": (_ll, [_vp]),
+    "bamrex_level_stream": (_vp, [_vp]),
     "bamrex_level_fab": (_i, [_vp, _i, ctypes.POINTER(Array4)]),
     "bamrex_level_copy_in": (_i, [_vp, _vp]),
     "bamrex_level_copy_out": (_i, [_vp, _vp]),

@@ -924,6 +924,8 @@ extern "C" const char* bamrex_level_last_error(const bamrex_level* L) { return L
 
 extern "C" long long bamrex_level_num_cells(const bamrex_level* L) { return L ? L->ncells : 0; }
 
+extern "C" void* bamrex_level_stream(const bamrex_level* L) { return L ? (void*)L->stream : nullptr; }
+
 extern "C" int bamrex_level_fab(const bamrex_level* L, int box, bamrex_array4* out)
 {
     if (!L || !out || box < 0 || box >= (int)L->boxes.size()) return fail(BAMREX_ERR_ARG, "bad level/box");

@@ -150,6 +150,11 @@ class DeviceEngine:
         self.device = "cuda"
         self.level = level
         self.NC = level.NC
+        # the level's stream, so buffer traffic and NCCL order with its kernels
+        self.stream = torch.cuda.ExternalStream(level.stream_handle())
+
+    def stream_context(self):
+        return self.torch.cuda.stream(self.stream)
 
     def set_halo(self, d, send, recv):
         from ._abi import Region, check, lib
@@ -169,7 +174,8 @@ class DeviceEngine:
               self.level._h)
 
     def buffer(self, cells):
-        return self.torch.empty(max(1, cells * self.NC), dtype=self.torch.float64, device="cuda")
+        with self.stream_context():
+            return self.torch.zeros(max(1, cells * self.NC), dtype=self.torch.float64, device="cuda")
 
     def pack(self, d, buf):
         import ctypes
@@ -216,21 +222,23 @@ class DistLevel:
         sbuf, rbuf = self.bufs[d]
         self.e.pack(d, sbuf)
         NC = self.e.NC
-        reqs = []
-        for peer, start, n in recv["peers"]:
-            reqs.append(self.dist.irecv(rbuf[start * NC:(start + n) * NC], src=peer))
-        for peer, start, n in send["peers"]:
-            reqs.append(self.dist.isend(sbuf[start * NC:(start + n) * NC], dst=peer))
-        for r in reqs:
-            r.wait()
+        with self.e.stream_context():
+            reqs = []
+            for peer, start, n in recv["peers"]:
+                reqs.append(self.dist.irecv(rbuf[start * NC:(start + n) * NC], src=peer))
+            for peer, start, n in send["peers"]:
+                reqs.append(self.dist.isend(sbuf[start * NC:(start + n) * NC], dst=peer))
+            for r in reqs:
+                r.wait()
         self.e.unpack(d, rbuf)
 
     def global_wave_speed(self):
         ws = self.e.wave_speed()
         if self.world > 1:
-            t = self.e.torch.tensor([ws], dtype=self.e.torch.float64, device=self.e.device)
-            self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
-            ws = float(t.item())
+            with self.e.stream_context():
+                t = self.e.torch.tensor([ws], dtype=self.e.torch.float64, device=self.e.device)
+                self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+                ws = float(t.item())
         return ws
 
     def est_time_step(self):

@@ -278,6 +278,10 @@ class Level:
     def sync(self):
         self._ck(lib().bamrex_level_sync(self._h))
 
+    def stream_handle(self) -> int:
+        """The cudaStream_t the level works on (as an integer)."""
+        return lib().bamrex_level_stream(self._h) or 0
+
     def fab(self, b) -> Array4:
         a = Array4()
         self._ck(lib().bamrex_level_fab(self._h, b, ctypes.byref(a)))

@@ -511,9 +511,9 @@ def run_ours_dist(args, rank, world, local_rank):
     for b, (lo, bhi) in enumerate(boxes):
         if owners[b] == rank:
             glob[:, :, lo[1]:bhi[1] + 1, :] = block
-    stream = torch.cuda.current_stream()
     lev = bx.Level(D, (0, 0, 0), hi, [0.0, 0.0], [1.0, float(world)], mine, bx.Parm(D, limiter=bx.MINBEE),
-                   method=bx.MUSCL_HANCOCK, cfl=0.8, stream=stream)
+                   method=bx.MUSCL_HANCOCK, cfl=0.8)
+    stream = torch.cuda.ExternalStream(lev.stream_handle())  # the level's own stream
     lev.set_state(glob)
     del glob
     dl = DistLevel(DeviceEngine(lev), D, (0, 0, 0), hi, boxes, owners, 2, (0, 0, 0), (0, 0, 0), lev.dx, 0.8, rank,

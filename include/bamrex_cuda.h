@@ -187,10 +187,15 @@ typedef struct bamrex_level_desc {
 /* Build the level: allocates the state fabs (two time-level buffers with
  * ghost cells, 256-byte aligned rows), the device box table, ghost-fill
  * tables and a small scalar block, all at creation (no allocation per step).
- * Work is issued on `stream`. */
+ * Work is issued on `stream`; with stream NULL the level creates and owns a
+ * non-blocking stream of its own (bamrex_level_stream returns it). */
 BAMREX_API int bamrex_level_create(bamrex_level **out, const bamrex_level_desc *desc, void *stream);
 BAMREX_API int bamrex_level_destroy(bamrex_level *level);
 BAMREX_API const char *bamrex_level_last_error(const bamrex_level *level);
+
+/* The stream the level issues its work on (the one given at creation, or
+ * the level's own non-blocking stream when that was NULL). */
+BAMREX_API void *bamrex_level_stream(const bamrex_level *level);
 
 /* Number of valid cells, and the Array4 of box b of the current state. */
 BAMREX_API long long bamrex_level_num_cells(const bamrex_level *level);

@@ -25,6 +25,10 @@ class OracleEngine:
     def set_halo(self, d, send, recv):
         self.halo[d] = (send, recv)
 
+    def stream_context(self):
+        import contextlib
+        return contextlib.nullcontext()
+
     def buffer(self, cells):
         return self.torch.zeros(max(1, cells * self.NC), dtype=self.torch.float64)
 

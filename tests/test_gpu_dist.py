@@ -22,12 +22,11 @@ def test_two_levels_with_device_halos_equal_one(oracle, D, n, mgs, bc):
     u0 = problems.random_states(D, tuple(reversed([n if d < D else 1 for d in range(3)])), seed=8) if D == 2 \
         else problems.blast_3d(n, radius=0.3)
     kw = dict(cfl=0.8, bc_lo=(bc,) * 3, bc_hi=(bc,) * 3)
-    stream = torch.cuda.current_stream()
     parm = bx.Parm(D, limiter=bx.VAN_LEER)
     ranks = []
     for r in range(2):
         mine = [boxes[b] for b in range(len(boxes)) if owners[b] == r]
-        lev = bx.Level(D, (0, 0, 0), hi, [0.0] * D, [1.0] * D, mine, parm, stream=stream, **kw)
+        lev = bx.Level(D, (0, 0, 0), hi, [0.0] * D, [1.0] * D, mine, parm, **kw)
         full = np.zeros_like(u0)
         lev.set_state(u0)
         eng = DeviceEngine(lev)
@@ -39,7 +38,7 @@ def test_two_levels_with_device_halos_equal_one(oracle, D, n, mgs, bc):
             bufs.append((eng.buffer(send["cells"]), eng.buffer(recv["cells"])))
         ranks.append((lev, eng, plan, bufs))
         del full
-    ref = bx.Level(D, (0, 0, 0), hi, [0.0] * D, [1.0] * D, boxes, parm, stream=stream, **kw)
+    ref = bx.Level(D, (0, 0, 0), hi, [0.0] * D, [1.0] * D, boxes, parm, **kw)
     ref.set_state(u0)
     NC = D + 2
     for step in range(3):
@@ -52,9 +51,15 @@ def test_two_levels_with_device_halos_equal_one(oracle, D, n, mgs, bc):
                 peer = ranks[1 - r]
                 recv = plan.dirs[d][1]
                 psend = peer[2].dirs[d][0]
-                for p, start, cnt in recv["peers"]:
-                    ps = [q for q in psend["peers"] if q[0] == r][0]
-                    bufs[d][1][start * NC:(start + cnt) * NC] = peer[3][d][0][ps[1] * NC:(ps[1] + cnt) * NC]
+                # the receiving level's stream waits for the sender's pack
+                e.stream.wait_stream(peer[1].stream)
+                with e.stream_context():
+                    for p, start, cnt in recv["peers"]:
+                        ps = [q for q in psend["peers"] if q[0] == r][0]
+                        bufs[d][1][start * NC:(start + cnt) * NC] = peer[3][d][0][ps[1] * NC:(ps[1] + cnt) * NC]
+            for r, (lev, e, plan, bufs) in enumerate(ranks):
+                # a rank packs its next buffer only after the peer copied this one
+                e.stream.wait_stream(ranks[1 - r][1].stream)
             for lev, e, plan, bufs in ranks:
                 e.unpack(d, bufs[d][1])
                 e.fill_dir(d)

@@ -45,6 +45,11 @@ constexpr int min_blocks() { return sizeof(T) == 4 ? BAMREX_SWEEP_MIN_BLOCKS_F32
 #define BAMREX_MARCH_UNROLL 1
 #endif
 constexpr int kMarchUnroll = BAMREX_MARCH_UNROLL;
+// Unroll factor of the x-sweep chunk loop.
+#ifndef BAMREX_XCHUNK_UNROLL
+#define BAMREX_XCHUNK_UNROLL 1
+#endif
+constexpr int kXChunkUnroll = BAMREX_XCHUNK_UNROLL;
 
 __device__ __forceinline__ int find_box(const SweepBox* boxes, int nboxes, long long item)
 {
@@ -190,6 +195,7 @@ __global__ void __launch_bounds__(kSweepThreads, min_blocks<T>()) sweep_x_kernel
 
         T An[NC];
         load(s0 - 32, An);
+#pragma unroll kXChunkUnroll
         for (int x0 = s0 - 32; x0 < s1 + 32; x0 += 32) {
             T A[NC];
             copy_state(An, A);

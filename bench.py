@@ -48,6 +48,7 @@ def parse_args():
     ap.add_argument("--no-fp32", action="store_true", help="skip the FP32-storage variant")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-imex", action="store_true", help="skip the IMEX pressure-solve comparison")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the library's default sweep segments")
     ap.add_argument("--imex-n", type=int, default=2048, help="cells per side of the IMEX pressure problem")
     return ap.parse_args()
 
@@ -332,8 +333,15 @@ def run_ours(args, rank, world, local_rank):
     boxes = bx.decompose(D, (0, 0, 0), hi, mgs)
     u0 = problems.quadrant_2d(n)
     stream = torch.cuda.Stream()
-    lev = bx.Level(D, (0, 0, 0), hi, [0.0, 0.0], [1.0, 1.0], boxes, bx.Parm(D, limiter=bx.MINBEE),
-                   method=bx.MUSCL_HANCOCK, cfl=0.8, stream=stream)
+    parm = bx.Parm(D, limiter=bx.MINBEE)
+    xseg, sseg, tuned = 0, 0, None
+    if not args.no_autotune:
+        from bamrex_b200.autotune import segment_table_summary, tune_segments
+        xseg, sseg, table = tune_segments(D, (0, 0, 0), hi, [0.0, 0.0], [1.0, 1.0], boxes, parm, u0, steps=3)
+        tuned = {"x_segment": xseg or "library default", "s_segment": sseg or "library default",
+                 "candidates_ms_per_step": segment_table_summary(table)}
+    lev = bx.Level(D, (0, 0, 0), hi, [0.0, 0.0], [1.0, 1.0], boxes, parm, method=bx.MUSCL_HANCOCK, cfl=0.8,
+                   stream=stream, x_segment=xseg, s_segment=sseg)
     lev.set_state(u0)
     use_graph = bool(args.graph)
 
@@ -469,8 +477,8 @@ def run_ours(args, rank, world, local_rank):
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic (seeded four-quadrant initial state, generated on the host)",
-        "config": workload_config(n, len(boxes), mgs, {"graph_replay": use_graph,
-                                                        "parallelism": "replicas" if world > 1 else "single"}),
+        "config": workload_config(n, len(boxes), mgs, {"graph_replay": use_graph, "parallelism": "single",
+                                                        "autotune": tuned}),
         "roofline": roofline,
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": state_bytes,

@@ -137,3 +137,38 @@ class Helmholtz:
 
     def launches(self):
         return lib().bamrex_helmholtz_launches(self._h)
+
+
+def _main(argv=None):
+    """python -m bamrex_b200.helmholtz [--n N] [--solves K]: the low-Mach
+    pressure solve (lognormal density, beta = 1/rho) on the device, timed."""
+    import argparse
+    import time
+
+    import torch
+
+    from . import problems
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--n", type=int, default=1024)
+    ap.add_argument("--solves", type=int, default=3)
+    ap.add_argument("--tol", type=float, default=1e-8)
+    a = ap.parse_args(argv)
+    p = problems.low_mach_pressure_problem(n=a.n)
+    h = Helmholtz(2, (a.n, a.n))
+    h.setScalars(1.0, p["B"], 0.0)
+    h.setACoeffs(p["a"])
+    h.setBCoeffsFromCell(p["beta_cc"])
+    rhs = torch.from_numpy(p["rhs"].copy()).cuda()
+    x = torch.zeros_like(rhs)
+    for k in range(a.solves):
+        x.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        it, rr = h.solve_device(x, rhs, tol_rel=a.tol)
+        torch.cuda.synchronize()
+        print("solve %d: %d iterations, relative residual %.2e, %.2f ms" % (k, it, rr, 1e3 * (time.perf_counter() - t0)))
+    h.close()
+
+
+if __name__ == "__main__":
+    _main()

@@ -162,3 +162,28 @@ def solve_learned_device(h: Helmholtz, net, x, rhs, tol_rel=1e-8, tol_abs=0.0, m
                                                tol_abs, max_iter, restart, ctypes.byref(it), ctypes.byref(pit),
                                                ctypes.byref(rr), ctypes.byref(fb)))
     return it.value, pit.value, rr.value, bool(fb.value)
+
+
+def _main(argv=None):
+    """python -m bamrex_b200.learned [--n N] [--forwards K]: forward passes
+    of the preconditioner network (untrained weights) on an N x N grid."""
+    import argparse
+
+    import torch
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--n", type=int, default=1024)
+    ap.add_argument("--forwards", type=int, default=3)
+    a = ap.parse_args(argv)
+    net = PrecNet(a.n, a.n, batch=1, seed=1)
+    inp = np.random.default_rng(0).standard_normal((1, 2, a.n, a.n)).astype(np.float32)
+    for k in range(a.forwards):
+        t0 = time.perf_counter()
+        out = net.forward(inp)
+        torch.cuda.synchronize()
+        print("forward %d: %.2f ms (host copies included), |out| %.3e" % (k, 1e3 * (time.perf_counter() - t0),
+                                                                         float(np.abs(out).mean())))
+    net.close()
+
+
+if __name__ == "__main__":
+    _main()

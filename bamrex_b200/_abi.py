@@ -244,6 +244,7 @@ SIGNATURES = {
     "bamrex_precnet_forward": (_i, [_vp, _vp, _vp]),
     "bamrex_precnet_backward": (_i, [_vp, _vp, _vp]),
     "bamrex_precnet_train_step": (_i, [_vp, _vp, _vp, ctypes.c_float, _dp]),
+    "bamrex_precnet_set_tensor_cores": (_i, [_vp, _i]),
     "bamrex_helmholtz_solve_learned": (_i, [_vp, _vp, _i, _vp, _vp, _d, _d, _i, _i, ctypes.POINTER(_i),
                                             ctypes.POINTER(_i), _dp, ctypes.POINTER(_i)]),
 }

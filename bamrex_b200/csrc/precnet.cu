@@ -150,6 +150,113 @@ __global__ void __launch_bounds__(kT) conv_bwd_data_kernel(const float* __restri
     }
 }
 
+// The 16 -> 16 channel convolution on the tensor cores (inference):
+// implicit GEMM with M = pixels, N = 16 output channels, K = 9 taps x 16
+// input channels, mma.sync m16n8k16 with BF16 operands and FP32
+// accumulators.  A block of 4 warps takes a tile of 4 rows x 32 pixels; the
+// input rows the taps read (6 rows x 34 pixels x 16 channels) are staged in
+// shared memory as BF16, pixel-major with a 24-element pixel stride so the
+// fragment loads of a warp hit 32 distinct banks.  Each warp keeps the
+// weight fragments of all 9 taps in registers and computes its row as two
+// m16 tiles x two n8 tiles.  Requires W % 32 == 0 and H % 4 == 0.
+constexpr int kMmaTW = 32, kMmaTH = 4, kMmaPS = 24;
+
+__device__ __forceinline__ unsigned pack_bf16(float lo, float hi)
+{
+    const unsigned l = __bfloat16_as_ushort(__float2bfloat16_rn(lo));
+    const unsigned h = __bfloat16_as_ushort(__float2bfloat16_rn(hi));
+    return l | (h << 16);
+}
+
+__device__ __forceinline__ void mma_bf16_16816(float (&d)[4], const unsigned (&a)[4], unsigned b0, unsigned b1)
+{
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};\n"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+__global__ void __launch_bounds__(128) conv16_mma_kernel(const float* __restrict__ x, float* __restrict__ y,
+                                                         const float* __restrict__ w, const float* __restrict__ bias,
+                                                         int H, int W, int batch, int relu)
+{
+    __shared__ __align__(16) __nv_bfloat16 xs[(kMmaTH + 2) * (kMmaTW + 2) * kMmaPS];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int g = lane >> 2, t = lane & 3;
+    // weight fragments: B[k = ci][n = co] for every tap and both n8 tiles
+    unsigned bw[9][2][2];
+#pragma unroll
+    for (int tap = 0; tap < 9; ++tap)
+#pragma unroll
+        for (int nt = 0; nt < 2; ++nt) {
+            const int co = nt * 8 + g;
+            bw[tap][nt][0] = pack_bf16(w[(co * C + 2 * t) * 9 + tap], w[(co * C + 2 * t + 1) * 9 + tap]);
+            bw[tap][nt][1] = pack_bf16(w[(co * C + 2 * t + 8) * 9 + tap], w[(co * C + 2 * t + 9) * 9 + tap]);
+        }
+    float bv[2][2];
+#pragma unroll
+    for (int nt = 0; nt < 2; ++nt) {
+        bv[nt][0] = bias[nt * 8 + 2 * t];
+        bv[nt][1] = bias[nt * 8 + 2 * t + 1];
+    }
+    const long long HW = (long long)H * W;
+    const int tx = W / kMmaTW, ty = H / kMmaTH;
+    const long long ntiles = (long long)batch * tx * ty;
+    constexpr int SR = kMmaTH + 2, SC = kMmaTW + 2;
+    for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const int b = (int)(tile / ((long long)tx * ty));
+        const int rem = (int)(tile % ((long long)tx * ty));
+        const int j0 = (rem / tx) * kMmaTH, i0 = (rem % tx) * kMmaTW;
+        const float* xb = x + (long long)b * C * HW;
+        __syncthreads();  // the previous tile's fragments are consumed
+        for (int q = threadIdx.x; q < C * SR * SC; q += blockDim.x) {
+            const int ci = q / (SR * SC), r = (q / SC) % SR, c = q % SC;
+            const int jj = wrap(j0 + r - 1, H), ii = wrap(i0 + c - 1, W);
+            xs[(r * SC + c) * kMmaPS + ci] = __float2bfloat16_rn(xb[(long long)ci * HW + (long long)jj * W + ii]);
+        }
+        __syncthreads();
+        float acc[2][2][4];
+#pragma unroll
+        for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+            for (int nt = 0; nt < 2; ++nt) {
+                acc[mt][nt][0] = acc[mt][nt][2] = bv[nt][0];
+                acc[mt][nt][1] = acc[mt][nt][3] = bv[nt][1];
+            }
+#pragma unroll
+        for (int tap = 0; tap < 9; ++tap) {
+            const int dy = tap / 3, dx = tap % 3;  // smem row warp + dy, column pixel + dx
+#pragma unroll
+            for (int mt = 0; mt < 2; ++mt) {
+                const __nv_bfloat16* base = xs + ((warp + dy) * SC + mt * 16 + dx) * kMmaPS;
+                unsigned a[4];
+                a[0] = *reinterpret_cast<const unsigned*>(base + g * kMmaPS + 2 * t);
+                a[1] = *reinterpret_cast<const unsigned*>(base + (g + 8) * kMmaPS + 2 * t);
+                a[2] = *reinterpret_cast<const unsigned*>(base + g * kMmaPS + 2 * t + 8);
+                a[3] = *reinterpret_cast<const unsigned*>(base + (g + 8) * kMmaPS + 2 * t + 8);
+#pragma unroll
+                for (int nt = 0; nt < 2; ++nt) mma_bf16_16816(acc[mt][nt], a, bw[tap][nt][0], bw[tap][nt][1]);
+            }
+        }
+        float* yb = y + (long long)b * C * HW + (long long)(j0 + warp) * W + i0;
+#pragma unroll
+        for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+            for (int nt = 0; nt < 2; ++nt) {
+                const int p0 = mt * 16 + g, co = nt * 8 + 2 * t;
+                float v[4] = { acc[mt][nt][0], acc[mt][nt][1], acc[mt][nt][2], acc[mt][nt][3] };
+                if (relu)
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) v[e] = fmaxf(v[e], 0.0f);
+                yb[(long long)co * HW + p0] = v[0];
+                yb[(long long)(co + 1) * HW + p0] = v[1];
+                yb[(long long)co * HW + p0 + 8] = v[2];
+                yb[(long long)(co + 1) * HW + p0 + 8] = v[3];
+            }
+    }
+}
+
 // Partial weight gradients.  Work is split into tiles of one row segment
 // (TW pixels) of one sample; each block loops over tiles, stages the masked
 // output gradient g = dy * relu'(y) and the three input rows the 3x3 taps
@@ -372,6 +479,7 @@ struct bamrex_precnet {
     size_t act_floats = 0;
     int adam_t = 0;
     bool wb_dirty = true;
+    bool tensor_cores = true;  // inference forward of 16 -> 16 convolutions on the tensor cores
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     std::string err;
@@ -479,7 +587,11 @@ int launch_conv_fwd(bamrex_precnet* N, const Layer& L)
     const float* b = N->d_wb + L.b_off;
     if (L.cin == 2 && L.cout == C)
         conv_fwd_kernel<2, C><<<gridn(n), kT, 0, N->stream>>>(A(N, L.in), A(N, L.out), w, b, H, W, N->batch, L.relu);
-    else if (L.cin == C && L.cout == C)
+    else if (L.cin == C && L.cout == C && N->tensor_cores && W % kMmaTW == 0 && H % kMmaTH == 0) {
+        const long long tiles = (long long)N->batch * (W / kMmaTW) * (H / kMmaTH);
+        const int grid = (int)std::max(1LL, std::min(tiles, (long long)device_sm_count() * 8));
+        conv16_mma_kernel<<<grid, 128, 0, N->stream>>>(A(N, L.in), A(N, L.out), w, b, H, W, N->batch, L.relu);
+    } else if (L.cin == C && L.cout == C)
         conv_fwd_kernel<C, C><<<gridn(n), kT, 0, N->stream>>>(A(N, L.in), A(N, L.out), w, b, H, W, N->batch, L.relu);
     else
         conv_fwd_kernel<C, 1><<<gridn(n), kT, 0, N->stream>>>(A(N, L.in), A(N, L.out), w, b, H, W, N->batch, L.relu);
@@ -688,7 +800,11 @@ extern "C" int bamrex_precnet_train_step(bamrex_precnet* N, const float* in, con
     const size_t nin = (size_t)N->batch * 2 * HW, nout = (size_t)N->batch * HW;
     P_TRY(pck(N, cudaMemcpyAsync(A(N, 0), in, sizeof(float) * nin, cudaMemcpyDefault, N->stream), "input"));
     P_TRY(pck(N, cudaMemcpyAsync(N->d_tgt, target, sizeof(float) * nout, cudaMemcpyDefault, N->stream), "target"));
-    P_TRY(forward(N));
+    const bool tc = N->tensor_cores;
+    N->tensor_cores = false;  // the backward differentiates the FP32 forward
+    const int frc = forward(N);
+    N->tensor_cores = tc;
+    P_TRY(frc);
     const int last = (int)N->acts.size() - 1;
     const int nb = 512;
     float* qbuf = N->d_q;  // q = A_beta (out - target)
@@ -735,3 +851,10 @@ int precnet_run(bamrex_precnet* N, cudaStream_t s)
 }
 
 }  // namespace bamrex
+
+extern "C" int bamrex_precnet_set_tensor_cores(bamrex_precnet* N, int on)
+{
+    if (!N) return fail(BAMREX_ERR_ARG, "NULL network");
+    N->tensor_cores = on != 0;
+    return BAMREX_OK;
+}

@@ -46,6 +46,9 @@ class PrecNet:
         self._ck(lib().bamrex_precnet_resize(self._h, nx, ny, batch))
         self.nx, self.ny, self.batch = nx, ny, batch
 
+    def set_tensor_cores(self, on=True):
+        self._ck(lib().bamrex_precnet_set_tensor_cores(self._h, 1 if on else 0))
+
     def get_weights(self):
         w = np.empty(self.num_params, dtype=np.float32)
         self._ck(lib().bamrex_precnet_get_weights(self._h, ctypes.c_void_p(w.ctypes.data)))

@@ -529,6 +529,11 @@ BAMREX_API int bamrex_precnet_set_weights(bamrex_precnet *net, const float *w);
 BAMREX_API int bamrex_precnet_forward(bamrex_precnet *net, const float *in, float *out);
 /* Parameter gradient of sum(out * dout) after a forward on the same input. */
 BAMREX_API int bamrex_precnet_backward(bamrex_precnet *net, const float *dout, float *grad);
+/* Inference forwards (bamrex_precnet_forward and the learned solve) run the
+ * 16-channel convolutions on the tensor cores (BF16 operands, FP32
+ * accumulators) when on != 0 (the default) and the level's width is a
+ * multiple of 32 and its height of 4; training always uses the FP32 path. */
+BAMREX_API int bamrex_precnet_set_tensor_cores(bamrex_precnet *net, int on);
 /* One Adam step on the relative squared error ||out - target||^2 / ||target||^2
  * averaged over the batch; *loss is the value before the step. */
 BAMREX_API int bamrex_precnet_train_step(bamrex_precnet *net, const float *in, const float *target, float lr,

@@ -20,6 +20,7 @@ def test_forward_and_gradient_match_oracle(torch_cuda):
     from oracle import precnet_oracle as P
     rng = np.random.default_rng(5)
     net = PrecNet(32, 24, batch=2, seed=11)
+    net.set_tensor_cores(False)  # the FP32 forward, the one training differentiates
     w = net.get_weights().astype(np.float64)
     _, n = P.param_slices()
     assert net.num_params == n
@@ -39,6 +40,23 @@ def test_forward_and_gradient_match_oracle(torch_cuda):
             continue
         a, b = g[s[0]:s[2]], gref[s[0]:s[2]]
         assert np.linalg.norm(a - b) <= 1e-3 * np.linalg.norm(b) + 1e-6
+    net.close()
+
+
+def test_tensor_core_forward_matches_fp32(torch_cuda):
+    """The BF16 tensor-core convolutions agree with the FP32 ones to BF16
+    rounding of the activations."""
+    from bamrex_b200.learned import PrecNet
+    rng = np.random.default_rng(6)
+    net = PrecNet(128, 64, batch=2, seed=4)
+    x = rng.standard_normal((2, 2, 64, 128)).astype(np.float32)
+    net.set_tensor_cores(False)
+    ref = net.forward(x)
+    net.set_tensor_cores(True)
+    got = net.forward(x)
+    err = np.linalg.norm(got - ref) / np.linalg.norm(ref)
+    assert err <= 2e-2, err
+    assert not np.array_equal(got, ref)  # the tensor-core path did run
     net.close()
 
 

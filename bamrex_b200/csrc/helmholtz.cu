@@ -48,6 +48,7 @@ struct HLev {
     double* phi;   // ncell
     double* rhs;   // ncell
     double* res;   // ncell
+    double* tmp;   // ncell: the second buffer of the fused smoother
 };
 
 struct HOp {
@@ -125,16 +126,61 @@ __global__ void apply_kernel(const HLev L, const HOp op, const double* __restric
     }
 }
 
+// The Gauss-Seidel update of one cell from its neighbours pm/pp (boundary
+// factors cfm/cfp), in the operation order of alapgrad_gsrb.
+struct GsCoef {
+    double dh[3], cdh[3];  // B / h^2 and C / (2 h) as Fsmooth computes them
+};
+
+__device__ __forceinline__ GsCoef gs_coef(const HLev& L, const HOp& op)
+{
+    GsCoef g;
+    for (int d = 0; d < 3; ++d) {
+        g.dh[d] = op.bscal / (L.dx[d] * L.dx[d]);
+        g.cdh[d] = op.cscal / (2 * L.dx[d]);
+    }
+    return g;
+}
+
+template <int D>
+__device__ __forceinline__ double gsrb_value(const HLev& L, const HOp& op, const GsCoef& gc, long long c, int i, int j,
+                                             int k, double pc, const double (&pm)[3], const double (&pp)[3],
+                                             const double (&cfm)[3], const double (&cfp)[3], double rhs)
+{
+    const double* dh = gc.dh;
+    const double* cdh = gc.cdh;
+    double bl[3], bh[3], cc[3];
+    for (int d = 0; d < D; ++d) {
+        const int ih = i + (d == 0), jh = j + (d == 1), kh = k + (d == 2);
+        bl[d] = L.b[d][fidx(L, d, i, j, k)];
+        bh[d] = L.b[d][fidx(L, d, ih, jh, kh)];
+        cc[d] = L.c ? L.c[(long long)d * L.ncell + c] : 0.0;
+    }
+    double gamma = op.ascal * L.a[c];
+    for (int d = 0; d < D; ++d) gamma = gamma + dh[d] * (bl[d] + bh[d]);
+    double delta = dh[0] * (bl[0] * cfm[0] + bh[0] * cfp[0]);
+    for (int d = 1; d < D; ++d) delta = delta + dh[d] * (bl[d] * cfm[d] + bh[d] * cfp[d]);
+    for (int d = 0; d < D; ++d) delta = delta + cdh[d] * cc[d] * (cfm[d] - cfp[d]);
+    double rho = dh[0] * (bl[0] * pm[0] + bh[0] * pp[0]);
+    for (int d = 1; d < D; ++d) rho = rho + dh[d] * (bl[d] * pm[d] + bh[d] * pp[d]);
+    for (int d = 0; d < D; ++d) rho = rho - cdh[d] * cc[d] * (pp[d] - pm[d]);
+    if (D == 3) {
+        // MLALapGrad_3D_K.H:293-323
+        const double omega = 1.15;
+        const double g_m_d = gamma - delta;
+        const double res = rhs - (gamma * pc - rho);
+        return pc + omega / g_m_d * res;
+    }
+    // MLALapGrad_2D_K.H:205-228
+    return (rhs + rho - pc * delta) / (gamma - delta);
+}
+
 // One colour of the red-black smoother: cells with (i+j+k+color) even.
 template <int D>
 __global__ void gsrb_kernel(const HLev L, const HOp op, double* __restrict__ phi, const double* __restrict__ rhs,
                             int color)
 {
-    double dh[3], cdh[3];
-    for (int d = 0; d < 3; ++d) {
-        dh[d] = op.bscal / (L.dx[d] * L.dx[d]);
-        cdh[d] = op.cscal / (2 * L.dx[d]);
-    }
+    const GsCoef gc = gs_coef(L, op);
     const long long half = (L.ncell + 1) / 2;
     const int nxh = (L.n[0] + 1) / 2;
     for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < half;
@@ -146,32 +192,93 @@ __global__ void gsrb_kernel(const HLev L, const HOp op, double* __restrict__ phi
         if (i >= L.n[0] || j >= L.n[1] || k >= L.n[2]) continue;
         const long long c = cidx(L, i, j, k);
         const double pc = phi[c];
-        double pm[3], pp[3], cfm[3], cfp[3], bl[3], bh[3], cc[3];
+        double pm[3], pp[3], cfm[3], cfp[3];
         for (int d = 0; d < D; ++d) {
             pm[d] = nbr(phi, L, op, i, j, k, d, -1, pc, cfm[d]);
             pp[d] = nbr(phi, L, op, i, j, k, d, +1, pc, cfp[d]);
-            const int ih = i + (d == 0), jh = j + (d == 1), kh = k + (d == 2);
-            bl[d] = L.b[d][fidx(L, d, i, j, k)];
-            bh[d] = L.b[d][fidx(L, d, ih, jh, kh)];
-            cc[d] = L.c ? L.c[(long long)d * L.ncell + c] : 0.0;
         }
-        double gamma = op.ascal * L.a[c];
-        for (int d = 0; d < D; ++d) gamma = gamma + dh[d] * (bl[d] + bh[d]);
-        double delta = dh[0] * (bl[0] * cfm[0] + bh[0] * cfp[0]);
-        for (int d = 1; d < D; ++d) delta = delta + dh[d] * (bl[d] * cfm[d] + bh[d] * cfp[d]);
-        for (int d = 0; d < D; ++d) delta = delta + cdh[d] * cc[d] * (cfm[d] - cfp[d]);
-        double rho = dh[0] * (bl[0] * pm[0] + bh[0] * pp[0]);
-        for (int d = 1; d < D; ++d) rho = rho + dh[d] * (bl[d] * pm[d] + bh[d] * pp[d]);
-        for (int d = 0; d < D; ++d) rho = rho - cdh[d] * cc[d] * (pp[d] - pm[d]);
-        if (D == 3) {
-            // MLALapGrad_3D_K.H:293-323
-            const double omega = 1.15;
-            const double g_m_d = gamma - delta;
-            const double res = rhs[c] - (gamma * pc - rho);
-            phi[c] = pc + omega / g_m_d * res;
-        } else {
-            // MLALapGrad_2D_K.H:205-228
-            phi[c] = (rhs[c] + rho - pc * delta) / (gamma - delta);
+        phi[c] = gsrb_value<D>(L, op, gc, c, i, j, k, pc, pm, pp, cfm, cfp, rhs[c]);
+    }
+}
+
+// A full 2D sweep (red, then black) in one launch over tiles of 32 x 16
+// cells: the tile and a 2-cell halo of phi are staged in shared memory,
+// red is updated on the tile grown by one cell (the halo's red cells are
+// recomputed from the same inputs their own tile uses, so every value is
+// the one the two half-sweeps give), then black on the tile, which is
+// written to the other buffer (tiles read their halos from the old one).
+// One read and one write of phi per sweep instead of two each.  Requires
+// n0 % 32 == 0 and n1 % 16 == 0.
+constexpr int kGsTX = 32, kGsTY = 16;
+
+__global__ void __launch_bounds__(256) gsrb2_fused_kernel(const HLev L, const HOp op, const double* __restrict__ phi,
+                                                          double* __restrict__ phi_out, const double* __restrict__ rhs)
+{
+    constexpr int SX = kGsTX + 4, SY = kGsTY + 4;
+    __shared__ double sp[SY][SX];
+    const GsCoef gc = gs_coef(L, op);
+    const int tx = L.n[0] / kGsTX, ty = L.n[1] / kGsTY;
+    for (int tile = blockIdx.x; tile < tx * ty; tile += gridDim.x) {
+        const int i0 = (tile % tx) * kGsTX, j0 = (tile / tx) * kGsTY;
+        __syncthreads();
+        for (int q = threadIdx.x; q < SX * SY; q += blockDim.x) {
+            const int li = q % SX - 2, lj = q / SX - 2;
+            int gi = i0 + li, gj = j0 + lj;
+            // periodic images; outside a non-periodic face the value is never read
+            if (gi < 0) gi = op.bc_lo[0] == BAMREX_LINOP_PERIODIC ? gi + L.n[0] : 0;
+            if (gi >= L.n[0]) gi = op.bc_hi[0] == BAMREX_LINOP_PERIODIC ? gi - L.n[0] : L.n[0] - 1;
+            if (gj < 0) gj = op.bc_lo[1] == BAMREX_LINOP_PERIODIC ? gj + L.n[1] : 0;
+            if (gj >= L.n[1]) gj = op.bc_hi[1] == BAMREX_LINOP_PERIODIC ? gj - L.n[1] : L.n[1] - 1;
+            sp[lj + 2][li + 2] = phi[(long long)gj * L.n[0] + gi];
+        }
+        __syncthreads();
+        for (int pass = 0; pass < 2; ++pass) {
+            // pass 0: red on [-1, TX] x [-1, TY]; pass 1: black on the tile.
+            // Threads take the cells of the pass's colour only: row lj holds
+            // w / 2 of them, at columns of parity (lj + pass + i0 + j0) & 1.
+            const int lo = pass == 0 ? -1 : 0;
+            const int w = kGsTX + (pass == 0 ? 2 : 0), h = kGsTY + (pass == 0 ? 2 : 0);
+            const int wh = w / 2;
+            for (int q = threadIdx.x; q < wh * h; q += blockDim.x) {
+                const int lj = lo + q / wh;
+                const int par = ((i0 + j0 + lj + lo + pass) & 1);  // first column of the colour in this row
+                const int li = lo + 2 * (q % wh) + par;
+                const int gi0 = i0 + li, gj0 = j0 + lj;
+                // the cell itself in global indices (a periodic image for halo cells)
+                int gi = gi0, gj = gj0;
+                if (gi < 0 || gi >= L.n[0]) {
+                    if (op.bc_lo[0] != BAMREX_LINOP_PERIODIC) continue;
+                    gi = gi < 0 ? gi + L.n[0] : gi - L.n[0];
+                }
+                if (gj < 0 || gj >= L.n[1]) {
+                    if (op.bc_lo[1] != BAMREX_LINOP_PERIODIC) continue;
+                    gj = gj < 0 ? gj + L.n[1] : gj - L.n[1];
+                }
+                const double pc = sp[lj + 2][li + 2];
+                double pm[3], pp[3], cfm[3] = { 0, 0, 0 }, cfp[3] = { 0, 0, 0 };
+                const int nn[2] = { L.n[0], L.n[1] };
+                const int g[2] = { gi, gj };
+                for (int d = 0; d < 2; ++d) {
+                    const int si = d == 0 ? 1 : 0, sj = d == 1 ? 1 : 0;
+                    pm[d] = sp[lj + 2 - sj][li + 2 - si];
+                    pp[d] = sp[lj + 2 + sj][li + 2 + si];
+                    if (g[d] == 0 && op.bc_lo[d] != BAMREX_LINOP_PERIODIC) {
+                        cfm[d] = op.bc_lo[d] == BAMREX_LINOP_NEUMANN ? 1.0 : -1.0;
+                        pm[d] = cfm[d] * pc;
+                    }
+                    if (g[d] == nn[d] - 1 && op.bc_hi[d] != BAMREX_LINOP_PERIODIC) {
+                        cfp[d] = op.bc_hi[d] == BAMREX_LINOP_NEUMANN ? 1.0 : -1.0;
+                        pp[d] = cfp[d] * pc;
+                    }
+                }
+                const long long c = (long long)gj * L.n[0] + gi;
+                sp[lj + 2][li + 2] = gsrb_value<2>(L, op, gc, c, gi, gj, 0, pc, pm, pp, cfm, cfp, rhs[c]);
+            }
+            __syncthreads();
+        }
+        for (int q = threadIdx.x; q < kGsTX * kGsTY; q += blockDim.x) {
+            const int li = q % kGsTX, lj = q / kGsTX;
+            phi_out[(long long)(j0 + lj) * L.n[0] + i0 + li] = sp[lj + 2][li + 2];
         }
     }
 }
@@ -547,6 +654,23 @@ int launch_gsrb(bamrex_helmholtz* H, int l, int color)
 
 int smooth(bamrex_helmholtz* H, int l, int sweeps)
 {
+    const HLev& L = H->lev[l];
+    const bool fused = H->D == 2 && L.n[0] % kGsTX == 0 && L.n[1] % kGsTY == 0;
+    if (fused) {
+        // ping-pong between phi and tmp; an odd count ends with a copy back
+        const int tiles = (L.n[0] / kGsTX) * (L.n[1] / kGsTY);
+        const int g = std::max(1, std::min(tiles, device_sm_count() * 8));
+        for (int s = 0; s < sweeps; ++s) {
+            const double* in = (s & 1) ? L.tmp : L.phi;
+            double* out = (s & 1) ? L.phi : L.tmp;
+            gsrb2_fused_kernel<<<g, 256, 0, H->stream>>>(L, H->op, in, out, L.rhs);
+            H_TRY(hck(H, cudaGetLastError(), "helmholtz gsrb (fused)"));
+        }
+        if (sweeps & 1)
+            H_TRY(hck(H, cudaMemcpyAsync(L.phi, L.tmp, sizeof(double) * L.ncell, cudaMemcpyDeviceToDevice, H->stream),
+                      "smoother copy"));
+        return BAMREX_OK;
+    }
     for (int s = 0; s < sweeps; ++s) {
         H_TRY(launch_gsrb(H, l, 0));
         H_TRY(launch_gsrb(H, l, 1));
@@ -714,7 +838,7 @@ extern "C" int bamrex_helmholtz_create(bamrex_helmholtz** out, const bamrex_helm
         return o;
     };
     struct Offs {
-        size_t a, b[3], c, phi, rhs, res;
+        size_t a, b[3], c, phi, rhs, res, tmp;
     };
     std::vector<Offs> lo(H->lev.size());
     for (size_t l = 0; l < H->lev.size(); ++l) {
@@ -728,6 +852,7 @@ extern "C" int bamrex_helmholtz_create(bamrex_helmholtz** out, const bamrex_helm
         lo[l].phi = take(sizeof(double) * L.ncell);
         lo[l].rhs = take(sizeof(double) * L.ncell);
         lo[l].res = take(sizeof(double) * L.ncell);
+        lo[l].tmp = take(sizeof(double) * L.ncell);
     }
     const long long n0 = H->lev[0].ncell;
     size_t ov[10];
@@ -750,6 +875,7 @@ extern "C" int bamrex_helmholtz_create(bamrex_helmholtz** out, const bamrex_helm
         L.phi = (double*)(A + lo[l].phi);
         L.rhs = (double*)(A + lo[l].rhs);
         L.res = (double*)(A + lo[l].res);
+        L.tmp = (double*)(A + lo[l].tmp);
     }
     std::vector<double*> cbuf(H->lev.size());
     for (size_t l = 0; l < H->lev.size(); ++l) cbuf[l] = (double*)(A + lo[l].c);

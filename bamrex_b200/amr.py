@@ -262,6 +262,9 @@ class Amr:
             dts.append(self.coarse_step(stop_time))
         return dts
 
+    def set_regrid_int(self, n):
+        self._ck(lib().bamrex_amr_set_regrid_int(self._h, n))
+
     def dt_level(self):
         out = (ctypes.c_double * _abi.MAX_LEVELS)()
         self._ck(lib().bamrex_amr_dt_level(self._h, out))

@@ -1110,10 +1110,7 @@ int set_level(bamrex_amr* A, int lev, const std::vector<bamrex_box>& boxes)
         for (int d = 0; d < A->D; ++d)
             if (b.lo[d] % bf != 0 || (b.hi[d] + 1) % bf != 0)
                 return amr_fail(A, BAMREX_ERR_ARG, "fine boxes must be aligned to blocking_factor");
-    if (lev <= finest && same_boxes(boxes, A->levels[lev]->boxes)) {
-        drop_levels_above(A, lev);
-        return BAMREX_OK;
-    }
+    if (lev <= finest && same_boxes(boxes, A->levels[lev]->boxes)) return BAMREX_OK;
     bamrex_level* L = nullptr;
     AMR_TRY(A, make_level(A, lev, boxes, &L));
     bamrex_coupling* C = nullptr;
@@ -1170,10 +1167,29 @@ int set_level(bamrex_amr* A, int lev, const std::vector<bamrex_box>& boxes)
         bamrex_level_destroy(L);
         return A->set_err(rc);
     }
-    drop_levels_above(A, lev - 1);
-    A->levels.push_back(L);
-    A->cpl.push_back(C);
-    A->dt_level.resize(A->levels.size(), A->dt_level.empty() ? 0.0 : A->dt_level.back() / A->desc.ref_ratio);
+    // the next finer level stays if it is still properly nested in the new
+    // boxes (coupled afresh), else it and everything above it go
+    bamrex_coupling* C2 = nullptr;
+    bool keep_finer = false;
+    if (lev + 1 <= finest) {
+        bamrex_coupling_destroy(A->cpl[lev + 1]);
+        A->cpl[lev + 1] = nullptr;
+        keep_finer = bamrex_coupling_create(&C2, L, A->levels[lev + 1], A->desc.ref_ratio) == BAMREX_OK;
+    }
+    if (lev <= finest) {
+        bamrex_coupling_destroy(A->cpl[lev]);
+        bamrex_level_destroy(A->levels[lev]);
+        A->levels[lev] = L;
+        A->cpl[lev] = C;
+    } else {
+        A->levels.push_back(L);
+        A->cpl.push_back(C);
+        A->dt_level.resize(A->levels.size(), A->dt_level.empty() ? 0.0 : A->dt_level.back() / A->desc.ref_ratio);
+    }
+    if (lev + 1 <= finest) {
+        if (keep_finer) A->cpl[lev + 1] = C2;
+        else drop_levels_above(A, lev);
+    }
     return BAMREX_OK;
 }
 
@@ -1369,6 +1385,13 @@ extern "C" int bamrex_amr_coarse_step(bamrex_amr* A, double stop_time, double* t
     A->steps++;
     *time_io = time + A->dt_level[0];
     if (dt_out) *dt_out = A->dt_level[0];
+    return BAMREX_OK;
+}
+
+extern "C" int bamrex_amr_set_regrid_int(bamrex_amr* A, int regrid_int)
+{
+    if (!A || regrid_int < 0) return fail(BAMREX_ERR_ARG, "bad argument");
+    A->desc.regrid_int = regrid_int;
     return BAMREX_OK;
 }
 

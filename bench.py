@@ -49,6 +49,9 @@ def parse_args():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-imex", action="store_true", help="skip the IMEX pressure-solve comparison")
     ap.add_argument("--no-autotune", action="store_true", help="keep the library's default sweep segments")
+    ap.add_argument("--no-amr", action="store_true", help="skip the 3D AMR blast sample")
+    ap.add_argument("--amr-n", type=int, default=128, help="base cells per side of the AMR blast sample")
+    ap.add_argument("--amr-steps", type=int, default=6, help="timed coarse steps of the AMR blast sample")
     ap.add_argument("--imex-n", type=int, default=2048, help="cells per side of the IMEX pressure problem")
     return ap.parse_args()
 
@@ -294,6 +297,84 @@ def imex_pressure_run(n):
     }
 
 
+def _chop_drawn(boxes, choices, rng, D=3):
+    """Boxes cut so each piece's sides are at most a max_grid_size drawn per
+    box from `choices` (all multiples of the blocking factor)."""
+    out = []
+    for lo, hi in boxes:
+        m = int(rng.choice(choices))
+        pieces = [(list(lo), list(hi))]
+        for d in range(D):
+            nxt = []
+            for plo, phi in pieces:
+                a = plo[d]
+                while a <= phi[d]:
+                    b = min(phi[d], a + m - 1)
+                    qlo, qhi = list(plo), list(phi)
+                    qlo[d], qhi[d] = a, b
+                    nxt.append((qlo, qhi))
+                    a = b + 1
+            pieces = nxt
+        out += [(tuple(a), tuple(b)) for a, b in pieces]
+    return out
+
+
+def amr_blast_run(n0, coarse_steps, precision):
+    """The 3D spherical blast on a 3-level hierarchy (ratio 2, blocking
+    factor 8, max_grid_size drawn per box from {16,32,48,64}, grad_error on
+    rho >= 0.1, regrid every 2 coarse steps, subcycling): cell-updates/s
+    over `coarse_steps` coarse steps after the levels have formed."""
+    import torch
+
+    import bamrex_b200 as bx
+    from bamrex_b200 import problems
+    from bamrex_b200.amr import Amr
+
+    hi = (n0 - 1,) * 3
+    rng = np.random.default_rng(20261203)
+    base = _chop_drawn([((0, 0, 0), hi)], (16, 32, 48, 64), rng)
+    A = Amr(3, (0, 0, 0), hi, [0.0] * 3, [1.0] * 3, base, bx.Parm(3, limiter=bx.MINBEE), cfl=0.8, max_level=2,
+            ref_ratio=2, blocking_factor=8, max_grid_size=64, n_error_buf=2, grid_eff=0.7, regrid_int=2,
+            phigrad=[0.1, 0.1], phigrad_var=0, precision=precision)
+    A.set_state(0, problems.blast_3d(n0, radius=0.2))
+    # the density is uniform at t = 0: levels form from the first regrids
+    for _ in range(4):
+        A.coarse_step()
+
+    def redraw():
+        old = [A.boxes(lev) for lev in range(A.finest_level + 1)]
+        for lev in range(1, len(old)):
+            A.set_level_boxes(lev, _chop_drawn(old[lev], (16, 32, 48, 64), rng))
+
+    redraw()
+    cells = [sum(int(np.prod([h[d] - l[d] + 1 for d in range(3)])) for l, h in A.boxes(lev))
+             for lev in range(A.finest_level + 1)]
+    nboxes = [len(A.boxes(lev)) for lev in range(A.finest_level + 1)]
+    updates_per_step = sum(c * 2 ** lev for lev, c in enumerate(cells))
+    s0 = A.conserved_sums()
+    # stepping alone (fixed grids), then with a regrid every 2 coarse steps
+    A.set_regrid_int(0)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(coarse_steps):
+        A.coarse_step()
+    torch.cuda.synchronize()
+    dt_fixed = time.perf_counter() - t0
+    s1 = A.conserved_sums()
+    A.set_regrid_int(2)
+    t0 = time.perf_counter()
+    for _ in range(coarse_steps):
+        A.coarse_step()
+    torch.cuda.synchronize()
+    dt_regrid = time.perf_counter() - t0
+    A.close()
+    return {"cells_per_level": cells, "boxes_per_level": nboxes, "coarse_steps": coarse_steps,
+            "ms_per_coarse_step": dt_fixed / coarse_steps * 1e3,
+            "cell_updates_per_s": updates_per_step * coarse_steps / dt_fixed,
+            "ms_per_coarse_step_with_regrid_every_2": dt_regrid / coarse_steps * 1e3,
+            "mass_drift_rel": float(abs(s1[0] - s0[0]) / abs(s0[0]))}
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return 0
@@ -472,6 +553,13 @@ def run_ours(args, rank, world, local_rank):
     imex = None
     if rank == 0 and world == 1 and not args.no_imex:
         imex = imex_pressure_run(args.imex_n)
+    amr = None
+    if rank == 0 and world == 1 and not args.no_amr:
+        amr = {"workload": "3D spherical blast (p 10 inside r < 0.2, 0.1 outside, rho 1), base %d^3, 3 levels, "
+                           "ratio 2, blocking factor 8, max_grid_size drawn per box from {16,32,48,64}, grad_error "
+                           "on rho >= 0.1, MUSCL-Hancock/minbee, CFL 0.8, subcycling" % args.amr_n,
+               "fp64": amr_blast_run(args.amr_n, args.amr_steps, bx.FP64),
+               "fp32_storage": amr_blast_run(args.amr_n, args.amr_steps, bx.FP32_STORAGE)}
 
     line = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -489,6 +577,7 @@ def run_ours(args, rank, world, local_rank):
         "clocks": clocks.summary(t_wall0, t_wall1),
         "fp32_storage": fp32,
         "imex_pressure_solve": imex,
+        "amr_blast3d": amr,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)

@@ -425,7 +425,9 @@ BAMREX_API bamrex_level *bamrex_amr_level(bamrex_amr *amr, int lev);
 BAMREX_API int bamrex_amr_boxes(const bamrex_amr *amr, int lev, bamrex_box *out, int max_out, int *nout);
 /* Replace level lev (1 <= lev <= finest + 1, lev <= max_level) by the given
  * boxes: new data from the old level where it overlaps, from coarse
- * interpolation elsewhere.  Levels above lev are removed. */
+ * interpolation elsewhere.  The next finer level stays (with its data) when
+ * it is still properly nested in the new boxes; otherwise it and the levels
+ * above it are removed. */
 BAMREX_API int bamrex_amr_set_level_boxes(bamrex_amr *amr, int lev, const bamrex_box *boxes, int nboxes);
 /* Regrid levels lbase+1 .. from tags (errorEst) on levels lbase .. at `time`. */
 BAMREX_API int bamrex_amr_regrid(bamrex_amr *amr, int lbase, double time);
@@ -437,6 +439,8 @@ BAMREX_API int bamrex_amr_avg_down_all(bamrex_amr *amr);
  * first when regrid_int divides the coarse steps taken.  *time_io is the time
  * on entry and the new time on return; *dt_out the coarse dt taken. */
 BAMREX_API int bamrex_amr_coarse_step(bamrex_amr *amr, double stop_time, double *time_io, double *dt_out);
+/* Change amr.regrid_int (0: no more regrids). */
+BAMREX_API int bamrex_amr_set_regrid_int(bamrex_amr *amr, int regrid_int);
 /* dt of every level after the last computeInitialDt / computeNewDt. */
 BAMREX_API int bamrex_amr_dt_level(const bamrex_amr *amr, double *dt_level);
 /* Composite conserved totals: every level's sums minus those of its cells

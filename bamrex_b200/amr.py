@@ -79,10 +79,10 @@ def cluster_tags(spacedim, dom_lo, dom_hi, boxes, tags, ref_ratio=2, blocking_fa
     dom = Box.make(dom_lo, dom_hi)
     cb = (Box * len(boxes))(*[Box.make(lo, hi) for lo, hi in boxes])
     per = (ctypes.c_int * 3)(*[int(p) for p in periodic])
-    n_dom = 1
+    n_blk = 1  # at most one new box per blocked cell
     for d in range(spacedim):
-        n_dom *= dom_hi[d] - dom_lo[d] + 1
-    out = (Box * max(1, n_dom))()
+        n_blk *= (dom_hi[d] - dom_lo[d] + 1) // max(1, blocking_factor // ref_ratio)
+    out = (Box * max(1, n_blk))()
     nout = ctypes.c_int()
     t = np.ascontiguousarray(tags, dtype=np.uint8).tobytes()
     check(lib().bamrex_cluster_tags(spacedim, ctypes.byref(dom), per, cb, len(boxes), t, ref_ratio, blocking_factor,

@@ -704,6 +704,18 @@ extern "C" int bamrex_level_create(bamrex_level** out, const bamrex_level_desc* 
         }
         covered += n;
     }
+    {
+        // a level's boxes are disjoint
+        const std::vector<bamrex_box> bv(desc->boxes, desc->boxes + desc->nboxes);
+        BoxIndex oidx;
+        oidx.build(desc->domain, bv, D);
+        std::vector<int> hits;
+        for (int b = 0; b < desc->nboxes; ++b) {
+            oidx.query(bv[b].lo, bv[b].hi, hits);
+            for (int h : hits)
+                if (h != b) return fail(BAMREX_ERR_ARG, "boxes of a level overlap");
+        }
+    }
 
     bamrex_level* L = new (std::nothrow) bamrex_level();
     if (!L) return fail(BAMREX_ERR_OOM, "host allocation failed");

@@ -11,7 +11,6 @@
 #include <cstring>
 #include <memory>
 #include <new>
-#include <set>
 #include <string>
 #include <tuple>
 #include <vector>
@@ -105,9 +104,8 @@ void subtract_boxes(const bamrex_box& region, const BoxIndex& idx, const std::ve
     out.insert(out.end(), cur.begin(), cur.end());
 }
 
-int find_containing(const BoxIndex& idx, const std::vector<bamrex_box>& boxes, const int* c)
+int find_containing(const BoxIndex& idx, const std::vector<bamrex_box>& boxes, const int* c, std::vector<int>& hits)
 {
-    std::vector<int> hits;
     idx.query(c, c, hits);
     int best = -1;
     for (int h : hits) {
@@ -117,6 +115,25 @@ int find_containing(const BoxIndex& idx, const std::vector<bamrex_box>& boxes, c
             best = (best < 0) ? h : std::min(best, h);
     }
     return best;
+}
+
+// The box containing each cell of q (x fastest), -1 where none; a level's
+// boxes are disjoint, so the owner is unique.
+void cell_owners(const BoxIndex& idx, const std::vector<bamrex_box>& boxes, const bamrex_box& q, std::vector<int>& own,
+                 std::vector<int>& hits)
+{
+    const int nx = q.hi[0] - q.lo[0] + 1, ny = q.hi[1] - q.lo[1] + 1;
+    own.assign((size_t)box_volume(q), -1);
+    idx.query(q.lo, q.hi, hits);
+    for (int h : hits) {
+        const bamrex_box x = intersect(q, boxes[h]);
+        if (box_empty(x)) continue;
+        for (int k = x.lo[2]; k <= x.hi[2]; ++k)
+            for (int j = x.lo[1]; j <= x.hi[1]; ++j) {
+                int* row = own.data() + ((size_t)(k - q.lo[2]) * ny + (j - q.lo[1])) * nx - q.lo[0];
+                for (int i = x.lo[0]; i <= x.hi[0]; ++i) row[i] = h;
+            }
+    }
 }
 
 }  // namespace
@@ -181,6 +198,7 @@ int build_patches(const bamrex_coupling* C, std::vector<CfRegion>& regs, std::ve
 {
     const bamrex_level* Lc = C->crse;
     long long pacc = 0, cacc = 0;
+    std::vector<int> own, hits;
     for (auto& R : regs) {
         bamrex_box w;
         for (int d = 0; d < 3; ++d) {
@@ -200,13 +218,16 @@ int build_patches(const bamrex_coupling* C, std::vector<CfRegion>& regs, std::ve
         R.cell_begin = cacc;
         pacc += box_volume(p);
         cacc += (long long)(R.hi[0] - R.lo[0] + 1) * (R.hi[1] - R.lo[1] + 1) * (R.hi[2] - R.lo[2] + 1);
+        cell_owners(cidx, Lc->boxes, p, own, hits);
+        size_t q = 0;
         for (int k = p.lo[2]; k <= p.hi[2]; ++k)
             for (int j = p.lo[1]; j <= p.hi[1]; ++j)
-                for (int i = p.lo[0]; i <= p.hi[0]; ++i) {
+                for (int i = p.lo[0]; i <= p.hi[0]; ++i, ++q) {
                     int c[3] = { i, j, k };
                     int neg = 0;
                     map_into_domain(Lc, c, neg);
-                    const int b = find_containing(cidx, Lc->boxes, c);
+                    const bool moved = c[0] != i || c[1] != j || c[2] != k;
+                    const int b = moved ? find_containing(cidx, Lc->boxes, c, hits) : own[q];
                     if (b < 0)
                         return fail(BAMREX_ERR_ARG,
                                     "fine level not properly nested: coarse cell (" + std::to_string(c[0]) + "," +
@@ -291,7 +312,7 @@ int build_register(const bamrex_coupling* C, int d, const BoxIndex& fidx, const 
     const bamrex_level* Lc = C->crse;
     const int r = C->r, D = C->D;
     const int dlo = Lf->domain.lo[d], dhi = Lf->domain.hi[d], len = dhi - dlo + 1;
-    std::set<std::tuple<int, int, int>> seen;
+    std::vector<int> own, hits;
     for (int b = 0; b < (int)Lf->boxes.size(); ++b) {
         const bamrex_box& B = Lf->boxes[b];
         for (int side = 0; side < 2; ++side) {
@@ -310,16 +331,14 @@ int build_register(const bamrex_coupling* C, int d, const BoxIndex& fidx, const 
             const int fface = side == 0 ? B.lo[d] : B.hi[d] + 1;
             for (const auto& p : pieces) {
                 const bamrex_box cp = coarsen(p, r, D);
+                cell_owners(cidx, Lc->boxes, cp, own, hits);
+                size_t oq = 0;
                 for (int k = cp.lo[2]; k <= cp.hi[2]; ++k)
                     for (int j = cp.lo[1]; j <= cp.hi[1]; ++j)
-                        for (int i = cp.lo[0]; i <= cp.hi[0]; ++i) {
+                        for (int i = cp.lo[0]; i <= cp.hi[0]; ++i, ++oq) {
                             int c[3] = { i, j, k };
-                            const int cb = find_containing(cidx, Lc->boxes, c);
+                            const int cb = own[oq];
                             if (cb < 0) return fail(BAMREX_ERR_ARG, "fine level not properly nested (flux register)");
-                            if (!seen.insert(std::make_tuple(i, j, k)).second)
-                                return fail(BAMREX_ERR_ARG,
-                                            "fine boxes closer than two coarse cells: a coarse cell borders the fine "
-                                            "region on both sides");
                             RefluxRec q;
                             q.box = cb;
                             q.i = i;
@@ -356,6 +375,16 @@ int build_register(const bamrex_coupling* C, int d, const BoxIndex& fidx, const 
             }
         }
     }
+    // a coarse cell may border the fine region on one side only
+    std::vector<unsigned long long> keys(rr.size());
+    const int* cl = Lc->domain.lo;
+    for (size_t q = 0; q < rr.size(); ++q)
+        keys[q] = ((unsigned long long)(rr[q].k - cl[2]) << 42) | ((unsigned long long)(rr[q].j - cl[1]) << 21) |
+                  (unsigned long long)(rr[q].i - cl[0]);
+    std::sort(keys.begin(), keys.end());
+    if (std::adjacent_find(keys.begin(), keys.end()) != keys.end())
+        return fail(BAMREX_ERR_ARG,
+                    "fine boxes closer than two coarse cells: a coarse cell borders the fine region on both sides");
     return BAMREX_OK;
 }
 
@@ -397,6 +426,9 @@ extern "C" int bamrex_coupling_create(bamrex_coupling** out, bamrex_level* crse,
         for (int d = 0; d < D; ++d)
             if (B.lo[d] % r != 0 || (B.hi[d] + 1) % r != 0)
                 return fail(BAMREX_ERR_ARG, "fine boxes must be aligned to the refinement ratio");
+    for (int d = 0; d < 3; ++d)
+        if (crse->domain.hi[d] - crse->domain.lo[d] >= (1 << 21))
+            return fail(BAMREX_ERR_ARG, "coarse domain wider than 2^21 cells");
 
     std::unique_ptr<bamrex_coupling> C(new (std::nothrow) bamrex_coupling());
     if (!C) return fail(BAMREX_ERR_OOM, "host allocation failed");
@@ -748,41 +780,100 @@ struct Mask3 {
     unsigned char at(int i, int j, int k) const { return v[((size_t)k * n[1] + j) * n[0] + i]; }
 };
 
-// out(x) = OR / AND of in over x-rad..x+rad along dim d; positions outside
-// the domain wrap (periodic) or take `outside`.
-void sweep_max(Mask3& m, int d, int rad, bool periodic, bool use_and, unsigned char outside)
-{
-    if (rad <= 0) return;
-    Mask3 o = m;
-    const int n = m.n[d];
-    for (int k = 0; k < m.n[2]; ++k)
-        for (int j = 0; j < m.n[1]; ++j)
-            for (int i = 0; i < m.n[0]; ++i) {
-                int c[3] = { i, j, k };
-                const int x0 = c[d];
-                unsigned char acc = use_and ? 1 : 0;
-                for (int s = -rad; s <= rad; ++s) {
-                    int x = x0 + s;
-                    unsigned char v;
-                    if (x < 0 || x >= n) {
-                        if (periodic) {
-                            x = ((x % n) + n) % n;
-                            c[d] = x;
-                            v = m.at(c[0], c[1], c[2]);
-                        } else {
-                            v = outside;
-                        }
-                    } else {
-                        c[d] = x;
-                        v = m.at(c[0], c[1], c[2]);
-                    }
-                    if (use_and) acc = acc && v;
-                    else acc = acc || v;
-                }
-                o.at(i, j, k) = acc;
+// Blocked-space tags and the proper-nesting test of grid generation, built
+// from the level's boxes without a cell mask over the whole domain.  A
+// blocked cell (c level-l cells per side) is tagged when a tagged cell lies
+// within n_error_buf cells of its footprint, and allowed when every cell
+// within n_proper cells of its footprint is covered by the level's boxes
+// (across a non-periodic domain side every cell counts as covered, a
+// periodic side wraps).  A blocked cell refines when it is both.  This is
+// the same as buffering the tags cell by cell, dropping buffered tags
+// outside the n_proper-eroded coverage and then blocking, because every
+// footprint cell of an allowed blocked cell lies in the eroded coverage.
+struct BlockedSpace {
+    int D = 0, c = 1, nbuf = 0, nprop = 0;
+    int n[3] = { 1, 1, 1 }, nt[3] = { 1, 1, 1 }, dl[3] = { 0, 0, 0 }, per[3] = { 0, 0, 0 };
+    const std::vector<bamrex_box>* boxes = nullptr;
+    BoxIndex idx;
+    Mask3 near_tag;   // a tag within n_error_buf of the footprint
+    Mask3 allowed;    // 0 / 1, 2 = not evaluated yet
+    std::vector<int> hits;
+
+    int cell(int d) const { return d < D ? c : 1; }
+
+    // the blocked indices [a, b] of dimension d wrapped (periodic) or
+    // clipped into range; returns the number of pieces written to lo/hi
+    int pieces(int d, int a, int b, int* lo, int* hi, int N) const
+    {
+        if (per[d]) {
+            if (b - a + 1 >= N) {
+                lo[0] = 0;
+                hi[0] = N - 1;
+                return 1;
             }
-    m.v.swap(o.v);
-}
+            const int a2 = ((a % N) + N) % N, b2 = a2 + (b - a);
+            if (b2 < N) {
+                lo[0] = a2;
+                hi[0] = b2;
+                return 1;
+            }
+            lo[0] = a2;
+            hi[0] = N - 1;
+            lo[1] = 0;
+            hi[1] = b2 - N;
+            return 2;
+        }
+        lo[0] = std::max(a, 0);
+        hi[0] = std::min(b, N - 1);
+        return lo[0] <= hi[0] ? 1 : 0;
+    }
+
+    void mark_run(int x0, int x1, int y, int z)
+    {
+        const int cl[3] = { x0, y, z }, ch[3] = { x1, y, z };
+        int lo[3][2], hi[3][2], np[3];
+        for (int d = 0; d < 3; ++d) {
+            const int nb = d < D ? nbuf : 0, cc = cell(d);
+            np[d] = pieces(d, floor_div(cl[d] - nb, cc), floor_div(ch[d] + nb, cc), lo[d], hi[d], nt[d]);
+        }
+        for (int pz = 0; pz < np[2]; ++pz)
+            for (int K = lo[2][pz]; K <= hi[2][pz]; ++K)
+                for (int py = 0; py < np[1]; ++py)
+                    for (int J = lo[1][py]; J <= hi[1][py]; ++J)
+                        for (int px = 0; px < np[0]; ++px)
+                            for (int I = lo[0][px]; I <= hi[0][px]; ++I) near_tag.at(I, J, K) = 1;
+    }
+
+    bool is_allowed(int I, int J, int K)
+    {
+        unsigned char& v = allowed.at(I, J, K);
+        if (v != 2) return v != 0;
+        const int B[3] = { I, J, K };
+        int lo[3][2], hi[3][2], np[3];
+        for (int d = 0; d < 3; ++d) {
+            const int pr = d < D ? nprop : 0, cc = cell(d);
+            np[d] = pieces(d, B[d] * cc - pr, B[d] * cc + cc - 1 + pr, lo[d], hi[d], n[d]);
+        }
+        bool ok = true;
+        for (int pz = 0; pz < np[2] && ok; ++pz)
+            for (int py = 0; py < np[1] && ok; ++py)
+                for (int px = 0; px < np[0] && ok; ++px) {
+                    bamrex_box q;
+                    q.lo[0] = lo[0][px] + dl[0];
+                    q.hi[0] = hi[0][px] + dl[0];
+                    q.lo[1] = lo[1][py] + dl[1];
+                    q.hi[1] = hi[1][py] + dl[1];
+                    q.lo[2] = lo[2][pz] + dl[2];
+                    q.hi[2] = hi[2][pz] + dl[2];
+                    idx.query(q.lo, q.hi, hits);
+                    long long got = 0;
+                    for (int h : hits) got += box_volume(intersect(q, (*boxes)[h]));
+                    ok = got == box_volume(q);  // the level's boxes are disjoint
+                }
+        v = ok ? 1 : 0;
+        return ok;
+    }
+};
 
 struct Cluster {
     const Mask3* tags;
@@ -896,14 +987,14 @@ struct Cluster {
     }
 };
 
-// Split b until every piece lies inside `allowed` (pieces with no allowed
-// cell are dropped).
-void clip_to_allowed(const Mask3& allowed, const bamrex_box& b, int D, std::vector<bamrex_box>& out)
+// Split b until every piece lies inside the allowed blocked cells (pieces
+// with no allowed cell are dropped).
+void clip_to_allowed(BlockedSpace& bs, const bamrex_box& b, int D, std::vector<bamrex_box>& out)
 {
     long long nin = 0;
     for (int k = b.lo[2]; k <= b.hi[2]; ++k)
         for (int j = b.lo[1]; j <= b.hi[1]; ++j)
-            for (int i = b.lo[0]; i <= b.hi[0]; ++i) nin += allowed.at(i, j, k) ? 1 : 0;
+            for (int i = b.lo[0]; i <= b.hi[0]; ++i) nin += bs.is_allowed(i, j, k) ? 1 : 0;
     if (nin == 0) return;
     if (nin == box_volume(b)) {
         out.push_back(b);
@@ -918,8 +1009,8 @@ void clip_to_allowed(const Mask3& allowed, const bamrex_box& b, int D, std::vect
     bamrex_box a = b, c = b;
     a.hi[best_d] = b.lo[best_d] + len / 2 - 1;
     c.lo[best_d] = b.lo[best_d] + len / 2;
-    clip_to_allowed(allowed, a, D, out);
-    clip_to_allowed(allowed, c, D, out);
+    clip_to_allowed(bs, a, D, out);
+    clip_to_allowed(bs, c, D, out);
 }
 
 void chop(const bamrex_box& b, int D, int mgs, std::vector<bamrex_box>& out)
@@ -966,41 +1057,52 @@ extern "C" int bamrex_cluster_tags(int D, const bamrex_box* domain, const int* p
         nt[d] = n[d] / c;
     }
     const int dl[3] = { domain->lo[0], domain->lo[1], domain->lo[2] };
-    Mask3 tag, cov;
-    tag.init(n, 0);
-    cov.init(n, 0);
-    long long off = 0;
-    for (int b = 0; b < nboxes; ++b) {
-        const bamrex_box& B = boxes[b];
-        for (int k = B.lo[2]; k <= B.hi[2]; ++k)
-            for (int j = B.lo[1]; j <= B.hi[1]; ++j)
-                for (int i = B.lo[0]; i <= B.hi[0]; ++i) {
-                    const int x = i - dl[0], y = j - dl[1], z = k - dl[2];
-                    if (x < 0 || y < 0 || z < 0 || x >= n[0] || y >= n[1] || z >= n[2])
-                        return fail(BAMREX_ERR_ARG, "box outside the domain");
-                    cov.at(x, y, z) = 1;
-                    if (tags[off]) tag.at(x, y, z) = 1;
-                    ++off;
-                }
+    std::vector<bamrex_box> bxs(boxes, boxes + nboxes);
+    for (const auto& B : bxs)
+        for (int d = 0; d < 3; ++d)
+            if (B.lo[d] < dl[d] || B.hi[d] >= dl[d] + n[d] || B.hi[d] < B.lo[d])
+                return fail(BAMREX_ERR_ARG, "box outside the domain");
+    BlockedSpace bs;
+    bs.D = D;
+    bs.c = c;
+    bs.nbuf = n_error_buf;
+    bs.nprop = n_proper;
+    for (int d = 0; d < 3; ++d) {
+        bs.n[d] = n[d];
+        bs.nt[d] = nt[d];
+        bs.dl[d] = dl[d];
+        bs.per[d] = (periodic && d < D) ? (periodic[d] != 0) : 0;
     }
-    // buffer the tags, restrict them to the proper nesting region
-    for (int d = 0; d < D; ++d) sweep_max(tag, d, n_error_buf, periodic && periodic[d], false, 0);
-    Mask3 allowed = cov;
-    for (int d = 0; d < D; ++d) sweep_max(allowed, d, n_proper, periodic && periodic[d], true, 1);
-    for (size_t q = 0; q < tag.v.size(); ++q) tag.v[q] = tag.v[q] && allowed.v[q];
-    // blocked space: a blocked cell is allowed if its whole footprint is,
-    // tagged if any footprint cell is
-    Mask3 btag, ball;
-    btag.init(nt, 0);
-    ball.init(nt, 1);
-    for (int k = 0; k < n[2]; ++k)
-        for (int j = 0; j < n[1]; ++j)
-            for (int i = 0; i < n[0]; ++i) {
-                const int I = i / (D > 0 ? c : 1), J = D > 1 ? j / c : j, K = D > 2 ? k / c : k;
-                if (tag.at(i, j, k)) btag.at(I, J, K) = 1;
-                if (!allowed.at(i, j, k)) ball.at(I, J, K) = 0;
+    bs.boxes = &bxs;
+    bs.idx.build(*domain, bxs, D);
+    bs.near_tag.init(nt, 0);
+    bs.allowed.init(nt, 2);
+    // runs of tagged cells along x, box by box in packed order
+    long long off = 0;
+    for (const auto& B : bxs) {
+        const int len = B.hi[0] - B.lo[0] + 1;
+        for (int k = B.lo[2]; k <= B.hi[2]; ++k)
+            for (int j = B.lo[1]; j <= B.hi[1]; ++j) {
+                const char* row = tags + off;
+                off += len;
+                for (int i = 0; i < len;) {
+                    if (!row[i]) {
+                        ++i;
+                        continue;
+                    }
+                    int e = i;
+                    while (e + 1 < len && row[e + 1]) ++e;
+                    bs.mark_run(B.lo[0] + i - dl[0], B.lo[0] + e - dl[0], j - dl[1], k - dl[2]);
+                    i = e + 1;
+                }
             }
-    for (size_t q = 0; q < btag.v.size(); ++q) btag.v[q] = btag.v[q] && ball.v[q];
+    }
+    Mask3 btag;
+    btag.init(nt, 0);
+    for (int K = 0; K < nt[2]; ++K)
+        for (int J = 0; J < nt[1]; ++J)
+            for (int I = 0; I < nt[0]; ++I)
+                if (bs.near_tag.at(I, J, K) && bs.is_allowed(I, J, K)) btag.at(I, J, K) = 1;
     Cluster cl;
     cl.tags = &btag;
     cl.eff = grid_eff;
@@ -1012,7 +1114,7 @@ extern "C" int bamrex_cluster_tags(int D, const bamrex_box* domain, const int* p
     }
     cl.run(all, 0);
     std::vector<bamrex_box> clipped, chopped;
-    for (const auto& b : cl.out) clip_to_allowed(ball, b, D, clipped);
+    for (const auto& b : cl.out) clip_to_allowed(bs, b, D, clipped);
     const int mgs_t = max_grid_size / blocking_factor;
     for (const auto& b : clipped) chop(b, D, mgs_t, chopped);
     std::sort(chopped.begin(), chopped.end(), [](const bamrex_box& a, const bamrex_box& b) {
@@ -1125,8 +1227,13 @@ int set_level(bamrex_amr* A, int lev, const std::vector<bamrex_box>& boxes)
         bamrex_level* O = A->levels[lev];
         std::vector<GhostOp> ops;
         const int nnew = (int)L->boxes.size();
-        for (int b = 0; b < nnew; ++b)
-            for (int s = 0; s < (int)O->boxes.size(); ++s) {
+        BoxIndex oidx;
+        oidx.build(O->domain, O->boxes, A->D);
+        std::vector<int> hits;
+        for (int b = 0; b < nnew; ++b) {
+            oidx.query(L->boxes[b].lo, L->boxes[b].hi, hits);
+            std::sort(hits.begin(), hits.end());
+            for (int s : hits) {
                 const bamrex_box x = intersect(L->boxes[b], O->boxes[s]);
                 if (box_empty(x)) continue;
                 GhostOp op;
@@ -1140,6 +1247,7 @@ int set_level(bamrex_amr* A, int lev, const std::vector<bamrex_box>& boxes)
                 }
                 ops.push_back(op);
             }
+        }
         long long acc = 0;
         for (auto& op : ops) {
             op.cell_begin = acc;
@@ -1215,9 +1323,11 @@ int regrid(bamrex_amr* A, int lbase, double time)
         bamrex_level* L = A->levels[l];
         int periodic[3] = { 0, 0, 0 };
         for (int q = 0; q < A->D; ++q) periodic[q] = L->bc_lo[q] == BAMREX_BC_PERIODIC;
-        long long dom = 1;
-        for (int q = 0; q < A->D; ++q) dom *= (L->domain.hi[q] - L->domain.lo[q] + 1);
-        std::vector<bamrex_box> nb((size_t)std::max<long long>(1, dom));
+        // at most one new box per blocked cell
+        const int cb = d.blocking_factor / d.ref_ratio;
+        long long nblk = 1;
+        for (int q = 0; q < A->D; ++q) nblk *= (L->domain.hi[q] - L->domain.lo[q] + 1) / cb;
+        std::vector<bamrex_box> nb((size_t)std::max<long long>(1, nblk));
         int n = 0;
         AMR_TRY(A, bamrex_cluster_tags(A->D, &L->domain, periodic, L->boxes.data(), (int)L->boxes.size(), tags.data(),
                                        d.ref_ratio, d.blocking_factor, d.max_grid_size, d.n_error_buf, d.n_proper,

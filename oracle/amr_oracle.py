@@ -491,3 +491,178 @@ class OAmr:
             m = ~np.isnan(d[0]) & ~cov
             tot += np.array([d[n][m].sum() for n in range(NC)]) * v
         return tot
+
+
+# ----------------------------------------------------------------------
+# grid generation (bamrex_cluster_tags), dense restatement
+# ----------------------------------------------------------------------
+
+def _shift_mask(m, d, s, periodic, outside):
+    """out[x] = m[x + s] along axis d (wrapped, or `outside` past the ends)."""
+    n = m.shape[d]
+    if periodic:
+        return np.roll(m, -s, axis=d)
+    out = np.full_like(m, outside)
+    if abs(s) < n:
+        src = [slice(None)] * 3
+        dst = [slice(None)] * 3
+        src[d] = slice(s, n) if s >= 0 else slice(0, n + s)
+        dst[d] = slice(0, n - s) if s >= 0 else slice(-s, n)
+        out[tuple(dst)] = m[tuple(src)]
+    return out
+
+
+def _sweep(m, d, rad, periodic, use_and, outside):
+    if rad <= 0:
+        return m
+    acc = None
+    for s in range(-rad, rad + 1):
+        sh = _shift_mask(m, d, s, periodic, outside)
+        acc = sh if acc is None else ((acc & sh) if use_and else (acc | sh))
+    return acc
+
+
+def _cluster(btag, D, eff, lo, hi, depth, out):
+    sub = btag[lo[0]:hi[0] + 1, lo[1]:hi[1] + 1, lo[2]:hi[2] + 1]
+    if not sub.any():
+        return
+    idx = np.nonzero(sub)
+    base = list(lo)
+    lo = [base[d] + int(idx[d].min()) for d in range(3)]
+    hi = [base[d] + int(idx[d].max()) for d in range(3)]
+    sub = btag[lo[0]:hi[0] + 1, lo[1]:hi[1] + 1, lo[2]:hi[2] + 1]
+    vol = sub.size
+    nt = int(sub.sum())
+    all_unit = all(hi[d] == lo[d] for d in range(D))
+    if nt >= eff * vol or all_unit or depth > 64:
+        out.append((tuple(lo), tuple(hi)))
+        return
+    sig = [sub.sum(axis=tuple(a for a in range(3) if a != d)).astype(np.int64) for d in range(D)]
+    best_d, best_cut = -1, 0
+    best_score = -1
+    for d in range(D):
+        n = len(sig[d])
+        for x in range(1, n - 1):
+            if sig[d][x] == 0:
+                score = n * 4 - abs(2 * x - n)
+                if score > best_score:
+                    best_score, best_d, best_cut = score, d, x
+    if best_d < 0:
+        best_jump = 0
+        for d in range(D):
+            n = len(sig[d])
+            if n < 4:
+                continue
+            lap = np.zeros(n, dtype=np.int64)
+            lap[1:n - 1] = sig[d][:n - 2] - 2 * sig[d][1:n - 1] + sig[d][2:]
+            for x in range(1, n - 2):
+                if (lap[x] > 0 and lap[x + 1] < 0) or (lap[x] < 0 and lap[x + 1] > 0):
+                    jump = abs(int(lap[x]) - int(lap[x + 1]))
+                    if jump > best_jump:
+                        best_jump, best_d, best_cut = jump, d, x + 1
+    if best_d < 0:
+        ln = 0
+        for d in range(D):
+            if hi[d] - lo[d] + 1 > ln:
+                ln, best_d = hi[d] - lo[d] + 1, d
+        best_cut = ln // 2
+    ahi = list(hi)
+    ahi[best_d] = lo[best_d] + best_cut - 1
+    clo = list(lo)
+    clo[best_d] = lo[best_d] + best_cut
+    _cluster(btag, D, eff, lo, ahi, depth + 1, out)
+    _cluster(btag, D, eff, clo, hi, depth + 1, out)
+
+
+def _clip(allowed, D, lo, hi, out):
+    sub = allowed[lo[0]:hi[0] + 1, lo[1]:hi[1] + 1, lo[2]:hi[2] + 1]
+    nin = int(sub.sum())
+    if nin == 0:
+        return
+    if nin == sub.size:
+        out.append((tuple(lo), tuple(hi)))
+        return
+    best_d, ln = 0, 0
+    for d in range(D):
+        if hi[d] - lo[d] + 1 > ln:
+            ln, best_d = hi[d] - lo[d] + 1, d
+    ahi = list(hi)
+    ahi[best_d] = lo[best_d] + ln // 2 - 1
+    clo = list(lo)
+    clo[best_d] = lo[best_d] + ln // 2
+    _clip(allowed, D, lo, ahi, out)
+    _clip(allowed, D, clo, hi, out)
+
+
+def _chop(lo, hi, D, mgs, out):
+    for d in range(D):
+        ln = hi[d] - lo[d] + 1
+        if ln > mgs:
+            pieces = (ln + mgs - 1) // mgs
+            base, extra = ln // pieces, ln % pieces
+            a = lo[d]
+            for p in range(pieces):
+                qlo, qhi = list(lo), list(hi)
+                qlo[d] = a
+                qhi[d] = a + base + (1 if p < extra else 0) - 1
+                a = qhi[d] + 1
+                _chop(qlo, qhi, D, mgs, out)
+            return
+    out.append((tuple(lo), tuple(hi)))
+
+
+def cluster_tags_dense(D, dom_lo, dom_hi, boxes, tags_packed, ref_ratio=2, blocking_factor=8, max_grid_size=32,
+                       n_error_buf=2, n_proper=1, grid_eff=0.7, periodic=(0, 0, 0)):
+    """Level l+1 boxes from level-l tags, on cell masks over the whole
+    domain: buffer the tags by n_error_buf (per direction), erode the box
+    coverage by n_proper (cells across a non-periodic side count as covered,
+    periodic sides wrap), drop buffered tags outside the eroded coverage,
+    block by blocking_factor / ref_ratio (tagged if any footprint cell is,
+    allowed if every one is), cluster the blocked tags by signatures (a zero
+    of the signature nearest the middle, else the strongest inflection,
+    else halve the longest side) until a box is grid_eff full, split the
+    clusters into allowed pieces, chop at max_grid_size, order by
+    (z, y, x) of the lower corner and refine."""
+    dl = [dom_lo[d] if d < D else 0 for d in range(3)]
+    n = [dom_hi[d] - dom_lo[d] + 1 if d < D else 1 for d in range(3)]
+    c = blocking_factor // ref_ratio
+    cc = [c if d < D else 1 for d in range(3)]
+    nt = [n[d] // cc[d] for d in range(3)]
+    tag = np.zeros(n, dtype=bool)
+    cov = np.zeros(n, dtype=bool)
+    off = 0
+    for lo, hi in boxes:
+        lo = tuple(lo) + (0,) * (3 - len(lo))
+        hi = tuple(hi) + (0,) * (3 - len(hi))
+        ext = [hi[d] - lo[d] + 1 for d in range(3)]
+        vol = ext[0] * ext[1] * ext[2]
+        blk = np.asarray(tags_packed[off:off + vol]).reshape(ext[2], ext[1], ext[0]).transpose(2, 1, 0) != 0
+        off += vol
+        sl = tuple(slice(lo[d] - dl[d], hi[d] - dl[d] + 1) for d in range(3))
+        cov[sl] = True
+        tag[sl] = blk
+    for d in range(D):
+        tag = _sweep(tag, d, n_error_buf, bool(periodic[d]), False, False)
+    allowed = cov
+    for d in range(D):
+        allowed = _sweep(allowed, d, n_proper, bool(periodic[d]), True, True)
+    tag = tag & allowed
+    btag = tag.reshape(nt[0], cc[0], nt[1], cc[1], nt[2], cc[2]).any(axis=(1, 3, 5))
+    ball = allowed.reshape(nt[0], cc[0], nt[1], cc[1], nt[2], cc[2]).all(axis=(1, 3, 5))
+    btag = btag & ball
+    clusters = []
+    _cluster(btag, D, grid_eff, [0, 0, 0], [nt[0] - 1, nt[1] - 1, nt[2] - 1], 0, clusters)
+    clipped = []
+    for lo, hi in clusters:
+        _clip(ball, D, list(lo), list(hi), clipped)
+    mgs_t = max_grid_size // blocking_factor
+    chopped = []
+    for lo, hi in clipped:
+        _chop(list(lo), list(hi), D, mgs_t, chopped)
+    chopped.sort(key=lambda b: (b[0][2], b[0][1], b[0][0]))
+    out = []
+    for lo, hi in chopped:
+        flo = tuple((lo[d] * c + dl[d]) * ref_ratio if d < D else 0 for d in range(3))
+        fhi = tuple(((hi[d] + 1) * c + dl[d]) * ref_ratio - 1 if d < D else 0 for d in range(3))
+        out.append((flo, fhi))
+    return out

@@ -159,3 +159,47 @@ def test_oracle_fine_everywhere_equals_single_fine_level(oracle):
         lay.advance_explicit(S, S2, t, dt, oracle.MUSCL_HANCOCK, oracle.Parm(D))
         t += dt
     np.testing.assert_array_equal(A.levels[1].dense(), lay.gather(S))
+
+
+def _random_level_boxes(rng, D, n, align):
+    cuts = []
+    for d in range(3):
+        if d < D:
+            c = [0]
+            while c[-1] < n:
+                c.append(min(n, c[-1] + align * int(rng.integers(1, 5))))
+            cuts.append(list(zip(c[:-1], [x - 1 for x in c[1:]])))
+        else:
+            cuts.append([(0, 0)])
+    keep = rng.uniform(0.4, 1.0)
+    boxes = [((x0, y0, z0), (x1, y1, z1)) for (z0, z1) in cuts[2] for (y0, y1) in cuts[1] for (x0, x1) in cuts[0]
+             if rng.random() < keep]
+    return boxes or [((0, 0, 0), (cuts[0][0][1], cuts[1][0][1], cuts[2][0][1]))]
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_cluster_tags_matches_dense_restatement(seed):
+    """The library's grid generation works box by box in blocked space; the
+    oracle buffers, erodes and blocks cell masks over the whole domain.  The
+    box lists agree exactly over ragged, partly covered levels, periodic and
+    non-periodic sides, both refinement ratios and several buffers."""
+    from bamrex_b200.amr import cluster_tags
+    from oracle import amr_oracle as AO
+    rng = np.random.default_rng(1000 + seed)
+    for _ in range(12):
+        D = int(rng.integers(1, 4))
+        ratio = int(rng.choice([2, 4]))
+        bf = 2 * ratio * int(rng.integers(1, 3))
+        c = bf // ratio
+        n = c * int(rng.integers(2, {1: 40, 2: 14, 3: 7}[D]))
+        boxes = _random_level_boxes(rng, D, n, int(rng.choice([1, 2, c])))
+        t = rng.random([n] * D) < rng.choice([0.002, 0.02, 0.2])
+        per = tuple(int(rng.random() < 0.4) if d < D else 0 for d in range(3))
+        kw = dict(ref_ratio=ratio, blocking_factor=bf, max_grid_size=bf * int(rng.integers(1, 5)),
+                  n_error_buf=int(rng.integers(0, 4)), n_proper=int(rng.integers(0, 3)),
+                  grid_eff=float(rng.choice([0.5, 0.7, 0.9])), periodic=per)
+        hi = tuple(n - 1 if d < D else 0 for d in range(3))
+        tags = _packed(D, t, boxes)
+        got = cluster_tags(D, (0, 0, 0), hi, boxes, tags, **kw)
+        want = AO.cluster_tags_dense(D, (0, 0, 0), hi, boxes, tags, **kw)
+        assert got == want, (D, n, kw)

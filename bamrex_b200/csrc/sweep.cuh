@@ -215,14 +215,21 @@ __global__ void __launch_bounds__(kSweepThreads, min_blocks<T>()) sweep_x_kernel
             T Fm[NC];
             shfl_carry(F, Fp, lane, 1, Fm);
             const int o = x0 - 32 + lane;
-            if (a.do_update && o >= s0 && o < s1) {
-                T Un[NC];
+            // the update is computed by every lane (idle lanes hold benign
+            // states) and stored by the lanes that own a cell, so the chunk
+            // stays one basic block
+            const bool upd = a.do_update && o >= s0 && o < s1;
+            T Un[NC];
 #pragma unroll
-                for (int n = 0; n < NC; ++n) Un[n] = Um2p[n] - f.dtdx * (F[n] - Fm[n]);
+            for (int n = 0; n < NC; ++n) Un[n] = Um2p[n] - f.dtdx * (F[n] - Fm[n]);
+            if (upd) {
                 T* po = out + (o - B.out.b0);
 #pragma unroll
                 for (int n = 0; n < NC; ++n) po[n * B.out.ns] = Un[n];
-                if (a.ws_max) track_ws((double)S::speed(Un, k), wsmax, nan_seen);
+            }
+            if (a.ws_max) {
+                const double w = (double)S::speed(Un, k);
+                track_ws(upd ? w : 0.0, wsmax, nan_seen);
             }
             if (fl) {
                 const int fo = o + 1;
@@ -332,14 +339,18 @@ __global__ void __launch_bounds__(kSweepThreads, min_blocks<T>()) sweep_s_kernel
             S::cell(Ua, Ub, U3, k, f.hdtdx, UL2, UR2);   // cell o+2
             T F1[NC];
             S::face(URa, ULb, k, f.half_dx_dt, f.dt_2dx, F1);  // face o+1
-            if (o >= s0 && a.do_update && active) {
-                T Un[NC];
+            const bool upd = o >= s0 && a.do_update && active;
+            T Un[NC];
 #pragma unroll
-                for (int n = 0; n < NC; ++n) Un[n] = U0[n] - f.dtdx * (F1[n] - Fo[n]);
+            for (int n = 0; n < NC; ++n) Un[n] = U0[n] - f.dtdx * (F1[n] - Fo[n]);
+            if (upd) {
                 T* po = out + (long long)o * outs;
 #pragma unroll
                 for (int n = 0; n < NC; ++n) po[n * B.out.ns] = Un[n];
-                if (a.ws_max) track_ws((double)S::speed(Un, k), wsmax, nan_seen);
+            }
+            if (a.ws_max) {
+                const double w = (double)S::speed(Un, k);
+                track_ws(upd ? w : 0.0, wsmax, nan_seen);
             }
             if (B.flux.p && active) {
                 const int fo = o + 1;

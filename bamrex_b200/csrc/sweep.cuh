@@ -169,13 +169,18 @@ __global__ void __launch_bounds__(kSweepThreads, min_blocks<T>()) sweep_x_kernel
         const int s1 = min(s0 + a.seglen, B.hi[0] + 1);
         const bool last_seg = (s1 == B.hi[0] + 1);
 
-        const T* __restrict__ in = B.in.ptr<T>() + (long long)(j - B.in.b1) * B.in.js + (long long)(kk - B.in.b2) * B.in.ks;
-        T* __restrict__ out = B.out.ptr<T>() + (long long)(j - B.out.b1) * B.out.js + (long long)(kk - B.out.b2) * B.out.ks;
-        T* __restrict__ fl = B.flux.p ? B.flux.ptr<T>() + (long long)(j - B.flux.b1) * B.flux.js + (long long)(kk - B.flux.b2) * B.flux.ks : nullptr;
+        // row pointers indexed by the absolute x, and the component strides,
+        // held in registers for the whole item
+        const T* __restrict__ in = B.in.ptr<T>() + (long long)(j - B.in.b1) * B.in.js + (long long)(kk - B.in.b2) * B.in.ks - B.in.b0;
+        T* __restrict__ out = B.out.ptr<T>() + (long long)(j - B.out.b1) * B.out.js + (long long)(kk - B.out.b2) * B.out.ks - B.out.b0;
+        T* __restrict__ fl = B.flux.p ? B.flux.ptr<T>() + (long long)(j - B.flux.b1) * B.flux.js + (long long)(kk - B.flux.b2) * B.flux.ks - B.flux.b0 : nullptr;
+        const long long ins = B.in.ns, ons = B.out.ns, fns = B.flux.ns;
+        const bool do_update = a.do_update != 0;
+        const bool ws_on = a.ws_max != nullptr;
 
         auto load = [&](int x0, T (&u)[NC]) {
             const int xl = x0 + lane + 2;
-            if (xl >= s0 - H && xl <= s1 - 1 + H) ld_state(in + (xl - B.in.b0), B.in.ns, u);
+            if (xl >= s0 - H && xl <= s1 - 1 + H) ld_state(in + xl, ins, u);
             else benign(u);
         };
 
@@ -218,25 +223,23 @@ __global__ void __launch_bounds__(kSweepThreads, min_blocks<T>()) sweep_x_kernel
             // the update is computed by every lane (idle lanes hold benign
             // states) and stored by the lanes that own a cell, so the chunk
             // stays one basic block
-            const bool upd = a.do_update && o >= s0 && o < s1;
+            const bool upd = do_update && o >= s0 && o < s1;
             T Un[NC];
 #pragma unroll
             for (int n = 0; n < NC; ++n) Un[n] = Um2p[n] - f.dtdx * (F[n] - Fm[n]);
             if (upd) {
-                T* po = out + (o - B.out.b0);
 #pragma unroll
-                for (int n = 0; n < NC; ++n) po[n * B.out.ns] = Un[n];
+                for (int n = 0; n < NC; ++n) out[o + n * ons] = Un[n];
             }
-            if (a.ws_max) {
+            if (ws_on) {
                 const double w = (double)S::speed(Un, k);
                 track_ws(upd ? w : 0.0, wsmax, nan_seen);
             }
             if (fl) {
                 const int fo = o + 1;
                 if (fo >= s0 && (fo < s1 || (fo == s1 && last_seg))) {
-                    T* pf = fl + (fo - B.flux.b0);
 #pragma unroll
-                    for (int n = 0; n < NC; ++n) pf[n * B.flux.ns] = F[n];
+                    for (int n = 0; n < NC; ++n) fl[fo + n * fns] = F[n];
                 }
             }
             copy_state(A, Ap);
@@ -308,10 +311,14 @@ __global__ void __launch_bounds__(kSweepThreads, min_blocks<T>()) sweep_s_kernel
         }
         const T* __restrict__ in = B.in.ptr<T>() + inoff;
         T* __restrict__ out = B.out.ptr<T>() + outoff;
+        T* __restrict__ fl = B.flux.p ? B.flux.ptr<T>() + floff : nullptr;
+        const long long inns = B.in.ns, ons = B.out.ns, fns = B.flux.ns;
+        const bool do_update = a.do_update != 0;
+        const bool ws_on = a.ws_max != nullptr;
 
         const int plo = s0 - H, phi = s1 - 1 + H;  // loadable positions
         auto load = [&](int pos, T (&u)[NC]) {
-            if (active && pos >= plo && pos <= phi) ld_state(in + (long long)pos * ins, B.in.ns, u);
+            if (active && pos >= plo && pos <= phi) ld_state(in + (long long)pos * ins, inns, u);
             else benign(u);
         };
 
@@ -339,25 +346,25 @@ __global__ void __launch_bounds__(kSweepThreads, min_blocks<T>()) sweep_s_kernel
             S::cell(Ua, Ub, U3, k, f.hdtdx, UL2, UR2);   // cell o+2
             T F1[NC];
             S::face(URa, ULb, k, f.half_dx_dt, f.dt_2dx, F1);  // face o+1
-            const bool upd = o >= s0 && a.do_update && active;
+            const bool upd = o >= s0 && do_update && active;
             T Un[NC];
 #pragma unroll
             for (int n = 0; n < NC; ++n) Un[n] = U0[n] - f.dtdx * (F1[n] - Fo[n]);
             if (upd) {
                 T* po = out + (long long)o * outs;
 #pragma unroll
-                for (int n = 0; n < NC; ++n) po[n * B.out.ns] = Un[n];
+                for (int n = 0; n < NC; ++n) po[n * ons] = Un[n];
             }
-            if (a.ws_max) {
+            if (ws_on) {
                 const double w = (double)S::speed(Un, k);
                 track_ws(upd ? w : 0.0, wsmax, nan_seen);
             }
-            if (B.flux.p && active) {
+            if (fl && active) {
                 const int fo = o + 1;
                 if (fo >= s0 && (fo < s1 || (fo == s1 && last_seg))) {
-                    T* pf = B.flux.ptr<T>() + floff + (long long)fo * fls;
+                    T* pf = fl + (long long)fo * fls;
 #pragma unroll
-                    for (int n = 0; n < NC; ++n) pf[n * B.flux.ns] = F1[n];
+                    for (int n = 0; n < NC; ++n) pf[n * fns] = F1[n];
                 }
             }
             copy_state(F1, Fo);

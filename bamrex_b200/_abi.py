@@ -103,8 +103,12 @@ class LevelDesc(ctypes.Structure):
         ("x_segment", ctypes.c_int),
         ("s_segment", ctypes.c_int),
         ("precision", ctypes.c_int),
+        ("x_mode", ctypes.c_int),
     ]
 
+
+# x-sweep kernels (BAMREX_XSWEEP_*)
+XSWEEP_AUTO, XSWEEP_ROWS, XSWEEP_MARCH = 0, 1, 2
 
 MAX_LEVELS = 8
 # linear-operator boundary types (amrex::LinOpBCType subset)
@@ -174,6 +178,7 @@ SIGNATURES = {
     "bamrex_level_last_error": (ctypes.c_char_p, [_vp]),
     "bamrex_level_num_cells": (_ll, [_vp]),
     "bamrex_level_stream": (_vp, [_vp]),
+    "bamrex_level_x_mode": (_i, [_vp]),
     "bamrex_level_fab": (_i, [_vp, _i, ctypes.POINTER(Array4)]),
     "bamrex_level_copy_in": (_i, [_vp, _vp]),
     "bamrex_level_copy_out": (_i, [_vp, _vp]),

@@ -151,40 +151,79 @@ bool overlaps(const bamrex_array4& a, const bamrex_array4& b, int NC)
 }
 
 // Work items of one box in one sweep direction.
-void box_items(int dir, const int* lo, const int* hi, int seglen, long long& items, int& nseg, int& ngroup)
+// Work items of one box for the sweep of direction dir: warp-per-row-segment
+// items for the x sweep (march = false), else segments of 32 adjacent
+// columns (rows for the marching x sweep).
+// The box's segments have equal lengths (at most seglen; multiples of 32
+// for the row kernel), returned in box_seglen.
+void box_items(int dir, const int* lo, const int* hi, int seglen, long long& items, int& nseg, int& ngroup,
+               bool march = false, int* box_seglen = nullptr)
 {
     const int n[3] = { hi[0] - lo[0] + 1, hi[1] - lo[1] + 1, hi[2] - lo[2] + 1 };
     nseg = (n[dir] + seglen - 1) / seglen;
-    if (dir == 0) {
+    int bl = (n[dir] + nseg - 1) / nseg;
+    if (dir == 0 && !march) bl = std::min(seglen, (bl + 31) / 32 * 32);
+    if (box_seglen) *box_seglen = bl;
+    if (dir == 0 && !march) {
         ngroup = 1;
         items = (long long)n[1] * n[2] * nseg;
     } else {
-        ngroup = (n[0] + 31) / 32;
-        const int other = (dir == 1) ? n[2] : n[1];
+        const int across = dir == 0 ? n[1] : n[0];
+        ngroup = (across + 31) / 32;
+        const int other = (dir == 2) ? n[1] : n[2];
         items = (long long)ngroup * other * nseg;
     }
 }
 
 // Segment length: the longest that still gives every resident warp several
-// items (few partial waves); x segments are multiples of 32.
-int choose_seglen(int dir, const std::vector<bamrex_box>& boxes, long long resident_warps)
+// items (few partial waves); x segments of the row kernel are multiples of 32.
+int choose_seglen(int dir, const std::vector<bamrex_box>& boxes, long long resident_warps, bool march = false)
 {
     static const int xs[] = { 2048, 1024, 512, 256, 128, 64, 32 };
     static const int ss[] = { 256, 128, 96, 64, 48, 32, 24, 16 };
-    const int* cand = dir == 0 ? xs : ss;
-    const int ncand = dir == 0 ? 7 : 8;
+    const bool rows = dir == 0 && !march;
+    const int* cand = rows ? xs : ss;
+    const int ncand = rows ? 7 : 8;
     const long long want = std::max(1LL, resident_warps) * 6;
     for (int c = 0; c < ncand; ++c) {
         long long tot = 0;
         int nseg, ngroup;
         long long it;
         for (const auto& b : boxes) {
-            box_items(dir, b.lo, b.hi, cand[c], it, nseg, ngroup);
+            box_items(dir, b.lo, b.hi, cand[c], it, nseg, ngroup, march);
             tot += it;
         }
         if (tot >= want) return cand[c];
     }
     return cand[ncand - 1];
+}
+
+// Lane-cell slots of the two x-sweep kernels over a set of boxes: the row
+// kernel spends two extra 32-cell chunks on every row segment (its
+// software pipeline), the marching kernel four extra cells per segment and
+// idle lanes when a box is not a multiple of 32 rows high; its per-cell cost
+// carries a 30% allowance for staging rows through shared memory (measured
+// on 4096^2 in boxes of 32 to 4096 cells).
+bool prefer_x_march(int D, const std::vector<bamrex_box>& boxes, int seg_rows, int seg_march)
+{
+    if (D < 2) return false;
+    double rows = 0, march = 0;
+    for (const auto& b : boxes) {
+        const long long n0 = b.hi[0] - b.lo[0] + 1, n1 = b.hi[1] - b.lo[1] + 1, n2 = b.hi[2] - b.lo[2] + 1;
+        long long items;
+        int nseg, ngroup, bl;
+        box_items(0, b.lo, b.hi, seg_rows, items, nseg, ngroup, false, &bl);
+        for (long long x = 0; x < n0; x += bl) {
+            const long long len = std::min<long long>(bl, n0 - x);
+            rows += (double)(n1 * n2) * 32.0 * (double)((len + 64 + 31) / 32);
+        }
+        box_items(0, b.lo, b.hi, seg_march, items, nseg, ngroup, true, &bl);
+        for (long long x = 0; x < n0; x += bl) {
+            const long long len = std::min<long long>(bl, n0 - x);
+            march += 1.3 * (double)(((n1 + 31) / 32) * 32 * n2) * (double)(len + 4);
+        }
+    }
+    return march < rows;
 }
 
 }  // namespace
@@ -300,9 +339,11 @@ static int per_box_sweep(int method, int dir, int D, const bamrex_box* bx, const
     B.in = to_fab(Uin);
     if (Uout) B.out = to_fab(*Uout);
     if (flux && flux->p) B.flux = to_fab(*flux);
-    a.seglen = dir == 0 ? 512 : 64;
+    const std::vector<bamrex_box> one(1, *bx);
+    const bool march = dir == 0 && prefer_x_march(D, one, 512, 64);
+    a.seglen = (dir == 0 && !march) ? 512 : 64;
     long long items;
-    box_items(dir, B.lo, B.hi, a.seglen, items, B.nseg, B.ngroup);
+    box_items(dir, B.lo, B.hi, a.seglen, items, B.nseg, B.ngroup, march, &B.seglen);
     B.item_begin = 0;
     a.total_items = items;
     a.halo = H;
@@ -312,7 +353,7 @@ static int per_box_sweep(int method, int dir, int D, const bamrex_box* bx, const
     a.k = k;
     a.ws_max = nullptr;
     a.do_update = Uout ? 1 : 0;
-    BX_CK(launch_sweep(D, dir, method, false, a, (cudaStream_t)stream));
+    BX_CK(launch_sweep(D, dir, method, false, a, (cudaStream_t)stream, march));
     return BAMREX_OK;
 }
 
@@ -633,7 +674,8 @@ int level_sweep(bamrex_level* L, int d, int parity, double dt_host, const StepSc
     a.do_update = 1;
     const bool t = allow_timing && L->timing && L->ev_used < L->events.size();
     if (t) cudaEventRecord(L->events[L->ev_used].first, L->stream);
-    const int rc = level_launch(L, launch_sweep(L->D, d, L->method, L->fp32, a, L->stream), "sweep");
+    const int rc = level_launch(L, launch_sweep(L->D, d, L->method, L->fp32, a, L->stream, d == 0 && L->x_march),
+                                "sweep");
     if (rc != BAMREX_OK) return rc;
     if (t) {
         cudaEventRecord(L->events[L->ev_used].second, L->stream);
@@ -734,6 +776,10 @@ extern "C" int bamrex_level_create(bamrex_level** out, const bamrex_level_desc* 
     }
     L->boxes.assign(desc->boxes, desc->boxes + desc->nboxes);
     L->ncells = covered;
+    if (desc->x_mode < BAMREX_XSWEEP_AUTO || desc->x_mode > BAMREX_XSWEEP_MARCH) {
+        delete L;
+        return fail(BAMREX_ERR_ARG, "x_mode must be BAMREX_XSWEEP_AUTO, _ROWS or _MARCH");
+    }
     if (desc->precision != BAMREX_FP64 && desc->precision != BAMREX_FP32_STORAGE) {
         delete L;
         return fail(BAMREX_ERR_ARG, "precision must be BAMREX_FP64 or BAMREX_FP32_STORAGE");
@@ -786,11 +832,23 @@ extern "C" int bamrex_level_create(bamrex_level** out, const bamrex_level_desc* 
 
     // ---- items and segment lengths
     std::vector<SweepBox> sweep_host[3];
+    // x-sweep kernel: one warp per row segment, or one thread per row
+    // (levels of narrow boxes); automatic by the lane-slot estimate
+    if (desc->x_mode == BAMREX_XSWEEP_MARCH) L->x_march = D >= 2;
+    else if (desc->x_mode == BAMREX_XSWEEP_ROWS) L->x_march = false;
+    else {
+        const int sr = desc->x_segment > 0 ? (int)align_up((size_t)desc->x_segment, 32)
+                                           : choose_seglen(0, L->boxes, sweep_resident_warps(D, 0, L->method, L->fp32, L->k));
+        const int sm = desc->x_segment > 0 ? desc->x_segment
+                                           : choose_seglen(0, L->boxes, sweep_resident_warps(D, 0, L->method, L->fp32, L->k, true), true);
+        L->x_march = prefer_x_march(D, L->boxes, sr, sm);
+    }
     for (int d = 0; d < D; ++d) {
+        const bool march = d == 0 && L->x_march;
         L->seglen[d] = d == 0 ? desc->x_segment : desc->s_segment;
         if (L->seglen[d] <= 0)
-            L->seglen[d] = choose_seglen(d, L->boxes, sweep_resident_warps(D, d, L->method, L->fp32, L->k));
-        if (d == 0) L->seglen[d] = (int)align_up((size_t)L->seglen[d], 32);
+            L->seglen[d] = choose_seglen(d, L->boxes, sweep_resident_warps(D, d, L->method, L->fp32, L->k, march), march);
+        if (d == 0 && !march) L->seglen[d] = (int)align_up((size_t)L->seglen[d], 32);
         long long acc = 0;
         for (int b = 0; b < nb; ++b) {
             SweepBox sb;
@@ -800,7 +858,7 @@ extern "C" int bamrex_level_create(bamrex_level** out, const bamrex_level_desc* 
                 sb.hi[q] = L->boxes[b].hi[q];
             }
             long long it;
-            box_items(d, sb.lo, sb.hi, L->seglen[d], it, sb.nseg, sb.ngroup);
+            box_items(d, sb.lo, sb.hi, L->seglen[d], it, sb.nseg, sb.ngroup, march, &sb.seglen);
             sb.item_begin = acc;
             acc += it;
             sweep_host[d].push_back(sb);
@@ -956,6 +1014,12 @@ extern "C" int bamrex_level_fab(const bamrex_level* L, int box, bamrex_array4* o
     out->end[2] = L->D > 2 ? B.hi[2] + g + 1 : B.hi[2] + 1;
     out->ncomp = L->NC;
     return BAMREX_OK;
+}
+
+extern "C" int bamrex_level_x_mode(const bamrex_level* L)
+{
+    if (!L) return fail(BAMREX_ERR_ARG, "NULL level");
+    return L->x_march ? BAMREX_XSWEEP_MARCH : BAMREX_XSWEEP_ROWS;
 }
 
 extern "C" int bamrex_level_copy_in(bamrex_level* L, const double* src)

@@ -59,7 +59,8 @@ struct SweepBox {
     FabDev in, out, flux;      // flux.p == nullptr: no flux output
     long long item_begin;      // first work item of this box
     int nseg;                  // segments along the sweep direction
-    int ngroup;                // lane groups across x (strided sweeps)
+    int ngroup;                // lane groups of 32 columns (marching sweeps)
+    int seglen;                // cells per segment (the last one may be shorter)
 };
 
 // Device-resident step scalars (graph-friendly time stepping).
@@ -79,7 +80,7 @@ struct SweepArgs {
     SweepBox one;              // single box passed by value (per-box calls)
     int nboxes;
     long long total_items;
-    int seglen;
+    int seglen;                // the level's segment length (boxes hold their own)
     int halo;                  // 2 for reconstructing methods, 1 for first order
     double dt_host;
     const StepScalars* scal;   // non-null: dt from scal->dt, skip if done

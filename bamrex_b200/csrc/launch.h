@@ -35,11 +35,15 @@ struct UpdateArgs {
 
 int device_sm_count();
 
-cudaError_t launch_sweep(int D, int dir, int method, bool fp32, const SweepArgs& a, cudaStream_t s);
+// march: run the x sweep (dir 0, D >= 2) as one thread per row instead of
+// one warp per row segment; the box table's items must be laid out to match
+// (sweep_items).
+cudaError_t launch_sweep(int D, int dir, int method, bool fp32, const SweepArgs& a, cudaStream_t s,
+                         bool march = false);
 
 // Warps of the sweep kernel that fit on the device at once (for choosing
 // segment lengths); 0 for an unsupported combination.
-long long sweep_resident_warps(int D, int dir, int method, bool fp32, const Consts& k);
+long long sweep_resident_warps(int D, int dir, int method, bool fp32, const Consts& k, bool march = false);
 
 // The fast-path limiter for this configuration (MUSCL-Hancock, energy
 // limiting, gamma with 1/z = 7), or -1 for the general kernels.

@@ -76,6 +76,7 @@ struct bamrex_level {
     bamrex::SweepBox* d_sweep[3][2] = {};
     long long items[3] = { 0, 0, 0 };
     int seglen[3] = { 0, 0, 0 };
+    bool x_march = false;  // x sweep by the marching (thread-per-row) kernel
     bamrex::GhostOp* d_ghost[3] = { nullptr, nullptr, nullptr };
     int nghost[3] = { 0, 0, 0 };
     long long ghost_cells[3] = { 0, 0, 0 };

@@ -23,6 +23,7 @@
 
 #include "common.cuh"
 #include "euler.cuh"
+#include "sweep_stage.h"
 
 namespace bamrex {
 
@@ -45,6 +46,7 @@ constexpr int min_blocks() { return sizeof(T) == 4 ? BAMREX_SWEEP_MIN_BLOCKS_F32
 #define BAMREX_MARCH_UNROLL 1
 #endif
 constexpr int kMarchUnroll = BAMREX_MARCH_UNROLL;
+static_assert(kSweepThreads == kStageBlockThreads, "staging sized for the sweep block");
 // Unroll factor of the x-sweep chunk loop.
 #ifndef BAMREX_XCHUNK_UNROLL
 #define BAMREX_XCHUNK_UNROLL 1
@@ -165,8 +167,8 @@ __global__ void __launch_bounds__(kSweepThreads, min_blocks<T>()) sweep_x_kernel
         const int ny = B.hi[1] - B.lo[1] + 1;
         const int j = B.lo[1] + (int)(row % ny);
         const int kk = B.lo[2] + (int)(row / ny);
-        const int s0 = B.lo[0] + seg * a.seglen;
-        const int s1 = min(s0 + a.seglen, B.hi[0] + 1);
+        const int s0 = B.lo[0] + seg * B.seglen;
+        const int s1 = min(s0 + B.seglen, B.hi[0] + 1);
         const bool last_seg = (s1 == B.hi[0] + 1);
 
         // row pointers indexed by the absolute x, and the component strides,
@@ -253,7 +255,12 @@ __global__ void __launch_bounds__(kSweepThreads, min_blocks<T>()) sweep_x_kernel
     if (a.ws_max) reduce_ws(wsmax, nan_seen, a.ws_max);
 }
 
-// ------------------------------------------------------------ y / z sweeps
+// ----------------------------------------------------- marching sweeps
+// y / z sweeps, and the x sweep of levels made of narrow boxes: each thread
+// marches one column (one row for DIR = 0) keeping the stencil in
+// registers; the 32 lanes of a warp take 32 adjacent columns across x (for
+// DIR = 0: 32 adjacent rows across y, staged through shared memory so that
+// global loads and stores stay coalesced; see sweep_stage.h).
 // Iteration o: load U(o+4); cell stage of cell o+2; face o+1 from the cell
 // stages of cells o and o+1 (earlier iterations); update of cell o.
 template <typename T, int D, int DIR, int METHOD, int LIM>
@@ -279,36 +286,33 @@ __global__ void __launch_bounds__(kSweepThreads, min_blocks<T>()) sweep_s_kernel
         const long long rest = local / B.nseg;
         const int grp = (int)(rest % B.ngroup);
         const int t2 = (int)(rest / B.ngroup);  // the other transverse index
-        const int x = B.lo[0] + grp * 32 + lane;
-        const bool active = x <= B.hi[0];
-        const int s0 = B.lo[DIR] + seg * a.seglen;
-        const int s1 = min(s0 + a.seglen, B.hi[DIR] + 1);
+        constexpr int LD = (DIR == 0) ? 1 : 0;  // the direction across the lanes
+        const int lp = B.lo[LD] + grp * 32 + lane;
+        const bool active = lp <= B.hi[LD];
+        const int s0 = B.lo[DIR] + seg * B.seglen;
+        const int s1 = min(s0 + B.seglen, B.hi[DIR] + 1);
         const bool last_seg = (s1 == B.hi[DIR] + 1);
 
-        // column base offsets (position along DIR added per access)
+        // column base offsets (position along DIR added per access): cell
+        // (i, j, k) sits at (i - b0) + (j - b1) js + (k - b2) ks
+        const int tr = (DIR == 2) ? B.lo[1] + t2 : ((D == 3) ? B.lo[2] + t2 : B.lo[2]);  // the other index
+        auto column = [&](const FabDev& G, long long& off, long long& step) {
+            if (DIR == 0) {
+                off = (long long)(lp - G.b1) * G.js + (long long)(tr - G.b2) * G.ks - (long long)G.b0;
+                step = 1;
+            } else if (DIR == 1) {
+                off = (long long)(lp - G.b0) + (long long)(tr - G.b2) * G.ks - (long long)G.b1 * G.js;
+                step = G.js;
+            } else {
+                off = (long long)(lp - G.b0) + (long long)(tr - G.b1) * G.js - (long long)G.b2 * G.ks;
+                step = G.ks;
+            }
+        };
         long long inoff, outoff, floff = 0;
         long long ins, outs, fls = 0;
-        if (DIR == 1) {
-            const int kk = (D == 3) ? B.lo[2] + t2 : 0;
-            inoff = (long long)(x - B.in.b0) + (long long)(kk - B.in.b2) * B.in.ks - (long long)B.in.b1 * B.in.js;
-            outoff = (long long)(x - B.out.b0) + (long long)(kk - B.out.b2) * B.out.ks - (long long)B.out.b1 * B.out.js;
-            ins = B.in.js;
-            outs = B.out.js;
-            if (B.flux.p) {
-                floff = (long long)(x - B.flux.b0) + (long long)(kk - B.flux.b2) * B.flux.ks - (long long)B.flux.b1 * B.flux.js;
-                fls = B.flux.js;
-            }
-        } else {
-            const int jj = B.lo[1] + t2;
-            inoff = (long long)(x - B.in.b0) + (long long)(jj - B.in.b1) * B.in.js - (long long)B.in.b2 * B.in.ks;
-            outoff = (long long)(x - B.out.b0) + (long long)(jj - B.out.b1) * B.out.js - (long long)B.out.b2 * B.out.ks;
-            ins = B.in.ks;
-            outs = B.out.ks;
-            if (B.flux.p) {
-                floff = (long long)(x - B.flux.b0) + (long long)(jj - B.flux.b1) * B.flux.js - (long long)B.flux.b2 * B.flux.ks;
-                fls = B.flux.ks;
-            }
-        }
+        column(B.in, inoff, ins);
+        column(B.out, outoff, outs);
+        if (B.flux.p) column(B.flux, floff, fls);
         const T* __restrict__ in = B.in.ptr<T>() + inoff;
         T* __restrict__ out = B.out.ptr<T>() + outoff;
         T* __restrict__ fl = B.flux.p ? B.flux.ptr<T>() + floff : nullptr;
@@ -317,9 +321,73 @@ __global__ void __launch_bounds__(kSweepThreads, min_blocks<T>()) sweep_s_kernel
         const bool ws_on = a.ws_max != nullptr;
 
         const int plo = s0 - H, phi = s1 - 1 + H;  // loadable positions
+        // x sweep: the staged rows; positions are read in order, so a
+        // warp-uniform test refills the buffer every kStageW reads, and the
+        // updates leave through the output buffer every kStageW cells
+        T* sin = nullptr;
+        T* sout = nullptr;
+        int pbase = 0, pnext = 0, obase = s0;
+        const int rows_left = B.hi[LD] - (B.lo[LD] + grp * 32) + 1;
+        const T* gin = nullptr;
+        T* gout = nullptr;
+        long long step8 = 0, ostep8 = 0;
+        auto refill = [&](int p0) {
+            __syncwarp();
+            const int c = lane & 3;
+            const bool pin = p0 + c >= plo && p0 + c <= phi;
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const int r = (lane >> 2) + 8 * i;
+                T u[NC];
+                if (pin && r < rows_left) ld_state(gin + i * step8 + p0, inns, u);
+                else benign(u);
+#pragma unroll
+                for (int n = 0; n < NC; ++n) sin[(n * 32 + r) * kStagePitch + c] = u[n];
+            }
+            __syncwarp();
+        };
+        auto flush = [&](int count) {
+            __syncwarp();
+            const int c = lane & 3;
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const int r = (lane >> 2) + 8 * i;
+                if (c < count && r < rows_left) {
+#pragma unroll
+                    for (int n = 0; n < NC; ++n) gout[i * ostep8 + obase + n * ons] = sout[(n * 32 + r) * kStagePitch + c];
+                }
+            }
+            __syncwarp();
+        };
+        if constexpr (DIR == 0) {
+            extern __shared__ __align__(16) unsigned char bamrex_stage_smem[];
+            sin = reinterpret_cast<T*>(bamrex_stage_smem) + (threadIdx.x >> 5) * stage_elems_per_warp<T, NC>();
+            sout = sin + NC * 32 * kStagePitch;
+            // lane (r0 = lane / 4, c = lane % 4) moves rows r0 + 8 i, cell c
+            const long long rb = (long long)(lane >> 2) + (B.lo[LD] + grp * 32) - lp;
+            gin = in + rb * B.in.js + (lane & 3);
+            gout = out + rb * B.out.js + (lane & 3);
+            step8 = 8 * B.in.js;
+            ostep8 = 8 * B.out.js;
+            pbase = s0 - 2;
+            pnext = s0 - 2;
+            refill(pbase);
+        }
         auto load = [&](int pos, T (&u)[NC]) {
-            if (active && pos >= plo && pos <= phi) ld_state(in + (long long)pos * ins, inns, u);
-            else benign(u);
+            if constexpr (DIR == 0) {
+                if (pnext == pbase + kStageW) {
+                    pbase += kStageW;
+                    refill(pbase);
+                }
+                const int c = pnext - pbase;
+#pragma unroll
+                for (int n = 0; n < NC; ++n) u[n] = sin[(n * 32 + lane) * kStagePitch + c];
+                ++pnext;
+                (void)pos;
+            } else {
+                if (active && pos >= plo && pos <= phi) ld_state(in + (long long)pos * ins, inns, u);
+                else benign(u);
+            }
         };
 
         // warm-up: cell stages of cells s0-1 and s0
@@ -350,7 +418,16 @@ __global__ void __launch_bounds__(kSweepThreads, min_blocks<T>()) sweep_s_kernel
             T Un[NC];
 #pragma unroll
             for (int n = 0; n < NC; ++n) Un[n] = U0[n] - f.dtdx * (F1[n] - Fo[n]);
-            if (upd) {
+            if constexpr (DIR == 0) {
+                if (o >= s0 && do_update) {
+#pragma unroll
+                    for (int n = 0; n < NC; ++n) sout[(n * 32 + lane) * kStagePitch + (o - obase)] = Un[n];
+                    if (o - obase == kStageW - 1 || o == s1 - 1) {
+                        flush(o - obase + 1);
+                        obase += kStageW;
+                    }
+                }
+            } else if (upd) {
                 T* po = out + (long long)o * outs;
 #pragma unroll
                 for (int n = 0; n < NC; ++n) po[n * ons] = Un[n];

@@ -2,5 +2,5 @@
 #include "sweep_pick.cuh"
 
 namespace bamrex {
-template const void* pick_sweep_kernel<float>(int, int, int, int);
+template const void* pick_sweep_kernel<float>(int, int, int, int, bool);
 }  // namespace bamrex

@@ -191,7 +191,7 @@ class Level:
 
     def __init__(self, spacedim, dom_lo, dom_hi, prob_lo, prob_hi, boxes, parm: Parm, method=_abi.MUSCL_HANCOCK,
                  cfl=0.9, ngrow=2, bc_lo=None, bc_hi=None, stream=None, x_segment=0, s_segment=0,
-                 precision=_abi.FP64):
+                 precision=_abi.FP64, x_mode=_abi.XSWEEP_AUTO):
         self.D, self.NC = spacedim, spacedim + 2
         self.boxes = [(tuple(lo) + (0,) * (3 - len(lo)), tuple(hi) + (0,) * (3 - len(hi))) for lo, hi in boxes]
         self.dom_lo = tuple(dom_lo) + (0,) * (3 - len(dom_lo))
@@ -215,6 +215,7 @@ class Level:
         d.x_segment = x_segment
         d.s_segment = s_segment
         d.precision = precision
+        d.x_mode = x_mode
         self.precision = precision
         self._h = ctypes.c_void_p()
         check(lib().bamrex_level_create(ctypes.byref(self._h), ctypes.byref(d), _stream_ptr(stream)))
@@ -277,6 +278,11 @@ class Level:
 
     def sync(self):
         self._ck(lib().bamrex_level_sync(self._h))
+
+    @property
+    def x_mode(self) -> int:
+        """The x-sweep kernel in use: XSWEEP_ROWS or XSWEEP_MARCH."""
+        return lib().bamrex_level_x_mode(self._h)
 
     def stream_handle(self) -> int:
         """The cudaStream_t the level works on (as an integer)."""

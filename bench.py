@@ -49,6 +49,7 @@ def parse_args():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-imex", action="store_true", help="skip the IMEX pressure-solve comparison")
     ap.add_argument("--no-autotune", action="store_true", help="keep the library's default sweep segments")
+    ap.add_argument("--x-mode", type=int, default=0, help="x-sweep kernel: 0 automatic, 1 warp per row, 2 thread per row")
     ap.add_argument("--no-amr", action="store_true", help="skip the 3D AMR blast sample")
     ap.add_argument("--amr-n", type=int, default=128, help="base cells per side of the AMR blast sample")
     ap.add_argument("--amr-steps", type=int, default=6, help="timed coarse steps of the AMR blast sample")
@@ -422,7 +423,8 @@ def run_ours(args, rank, world, local_rank):
         tuned = {"x_segment": xseg or "library default", "s_segment": sseg or "library default",
                  "candidates_ms_per_step": segment_table_summary(table)}
     lev = bx.Level(D, (0, 0, 0), hi, [0.0, 0.0], [1.0, 1.0], boxes, parm, method=bx.MUSCL_HANCOCK, cfl=0.8,
-                   stream=stream, x_segment=xseg, s_segment=sseg)
+                   stream=stream, x_segment=xseg, s_segment=sseg, x_mode=args.x_mode)
+    x_rows = lev.x_mode == bx.XSWEEP_ROWS
     lev.set_state(u0)
     use_graph = bool(args.graph)
 
@@ -498,7 +500,8 @@ def run_ours(args, rank, world, local_rank):
     fp32 = None
     if u_fp64 is not None:
         lev32 = bx.Level(D, (0, 0, 0), hi, [0.0, 0.0], [1.0, 1.0], boxes, bx.Parm(D, limiter=bx.MINBEE),
-                         method=bx.MUSCL_HANCOCK, cfl=0.8, stream=stream, precision=bx.FP32_STORAGE)
+                         method=bx.MUSCL_HANCOCK, cfl=0.8, stream=stream, precision=bx.FP32_STORAGE,
+                         x_mode=args.x_mode)
         lev32.set_state(u0)
         lev32.run(args.warmup, use_graph=use_graph)
         lev32.set_state(u0)
@@ -539,7 +542,8 @@ def run_ours(args, rank, world, local_rank):
         traffic = profiled_traffic("mhm2d")
         roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                     "traffic": (traffic * cells) if traffic else None,
-                    "kernel": "sweep_x_kernel<2,MUSCL> + sweep_s_kernel<2,1,MUSCL> (both sweeps, averaged)",
+                    "kernel": ("sweep_x_kernel<2,MUSCL>" if x_rows else "sweep_s_kernel<2,0,MUSCL>")
+                    + " + sweep_s_kernel<2,1,MUSCL> (both sweeps, averaged)",
                     "algorithmic_bytes_per_launch": alg_bytes, "avg_launch_ms": per_launch_s * 1e3,
                     "sweep_share_of_step": sweep_ms / ms if ms > 0 else None,
                     "peak_source": "%s (MEASURED_PEAKS.json hbm_gbs)" % peak_kind if peak_kind == "measured"
@@ -566,7 +570,7 @@ def run_ours(args, rank, world, local_rank):
         "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic (seeded four-quadrant initial state, generated on the host)",
         "config": workload_config(n, len(boxes), mgs, {"graph_replay": use_graph, "parallelism": "single",
-                                                        "autotune": tuned}),
+                                                        "x_sweep": "warp per row segment" if x_rows else "thread per row", "autotune": tuned}),
         "roofline": roofline,
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": state_bytes,

@@ -23,7 +23,7 @@
 extern "C" {
 #endif
 
-#define BAMREX_ABI_VERSION 1
+#define BAMREX_ABI_VERSION 2
 /* MAX_NCOMP = PUInd::size (Source/System/Parm.H:9) */
 #define BAMREX_MAX_NCOMP 8
 
@@ -182,7 +182,21 @@ typedef struct bamrex_level_desc {
     int x_segment;          /* cells per warp item in x; 0 = automatic */
     int s_segment;          /* cells per thread item in y/z; 0 = automatic */
     int precision;          /* BAMREX_FP64 (0) or BAMREX_FP32_STORAGE */
+    int x_mode;             /* BAMREX_XSWEEP_*: kernel of the x sweep; 0 = automatic */
 } bamrex_level_desc;
+
+/* Kernel of a level's x sweep.  ROWS: a warp marches along a row segment,
+ * lanes on consecutive cells (best for wide boxes: it spends two extra
+ * 32-cell chunks per row segment).  MARCH: each thread marches one row,
+ * lanes on 32 adjacent rows (best for levels of narrow boxes, such as
+ * max_grid_size 32-128).  AUTO picks by an estimate of the lane slots each
+ * spends on the level's boxes.  Both evaluate the same scheme per cell
+ * (results agree to rounding: multiply-add contraction may differ). */
+enum {
+    BAMREX_XSWEEP_AUTO = 0,
+    BAMREX_XSWEEP_ROWS = 1,
+    BAMREX_XSWEEP_MARCH = 2
+};
 
 /* Build the level: allocates the state fabs (two time-level buffers with
  * ghost cells, 256-byte aligned rows), the device box table, ghost-fill
@@ -196,6 +210,9 @@ BAMREX_API const char *bamrex_level_last_error(const bamrex_level *level);
 /* The stream the level issues its work on (the one given at creation, or
  * the level's own non-blocking stream when that was NULL). */
 BAMREX_API void *bamrex_level_stream(const bamrex_level *level);
+
+/* The x-sweep kernel the level runs: BAMREX_XSWEEP_ROWS or _MARCH. */
+BAMREX_API int bamrex_level_x_mode(const bamrex_level *level);
 
 /* Number of valid cells, and the Array4 of box b of the current state. */
 BAMREX_API long long bamrex_level_num_cells(const bamrex_level *level);

@@ -193,13 +193,13 @@ def test_unsplit_conservative_update(torch_cuda, oracle, D):
 
 
 # ------------------------------------------------------------------ levels
-def _make_levels(oracle, D, n, mgs, bc, method, limiter, cfl):
+def _make_levels(oracle, D, n, mgs, bc, method, limiter, cfl, x_mode=0):
     import bamrex_b200 as bx
     hi = tuple(n - 1 if d < D else 0 for d in range(3))
     boxes = oracle.decompose(D, (0, 0, 0), hi, mgs)
     lay = oracle.LevelLayout(D, (0, 0, 0), hi, boxes, 2, [1.0 / n] * D, bc_lo=(bc,) * 3, bc_hi=(bc,) * 3)
     lev = bx.Level(D, (0, 0, 0), hi, [0.0] * D, [1.0] * D, boxes, bx.Parm(D, limiter=limiter), method=method,
-                   cfl=cfl, bc_lo=(bc,) * 3, bc_hi=(bc,) * 3)
+                   cfl=cfl, bc_lo=(bc,) * 3, bc_hi=(bc,) * 3, x_mode=x_mode)
     return lay, lev
 
 
@@ -231,12 +231,15 @@ def _initial(kind, D, n):
     return problems.random_states(D, tuple(n if d < D else 1 for d in (2, 1, 0)), seed=21)
 
 
+@pytest.mark.parametrize("x_mode", [1, 2], ids=["xrows", "xmarch"])
 @pytest.mark.parametrize("case", LEVEL_CASES, ids=[str(c) for c in LEVEL_CASES])
-def test_level_step_parity(torch_cuda, oracle, case):
+def test_level_step_parity(torch_cuda, oracle, case, x_mode):
     """AmrLevelAdv::advance (one split step) on a whole level: same dt from
-    estTimeStep, then the state after the step, vs the oracle."""
+    estTimeStep, then the state after the step, vs the oracle; with either
+    x-sweep kernel (warp per row segment, thread per row)."""
     D, n, mgs, bc, method, lim, cfl, init = case
-    lay, lev = _make_levels(oracle, D, n, mgs, bc, method, lim, cfl)
+    lay, lev = _make_levels(oracle, D, n, mgs, bc, method, lim, cfl, x_mode)
+    assert lev.x_mode == (x_mode if D > 1 else 1)
     u0 = _initial(init, D, n)
     # oracle
     S1, S2 = lay.alloc(), lay.alloc()
@@ -333,3 +336,37 @@ def test_graph_replay_and_decomposition_are_exact(torch_cuda, oracle):
         lev.close()
     for o in outs[1:]:
         np.testing.assert_array_equal(o, outs[0])
+
+
+@pytest.mark.parametrize("D", [2, 3])
+@pytest.mark.parametrize("method,limiter", [(0, 0), (0, 2), (4, 1), (1, 1), (6, 1)])
+def test_x_sweep_kernels_agree(torch_cuda, oracle, D, method, limiter):
+    """The two x-sweep kernels evaluate the same scheme functions per cell;
+    the compiler may contract multiply-adds differently in each, so a level
+    run three steps with either agrees to the per-step bar times the steps
+    (both are also held to the oracle by test_level_step_parity), on ragged
+    boxes (widths and heights that are not multiples of 32); the automatic
+    choice takes the thread-per-row kernel for narrow boxes."""
+    import bamrex_b200 as bx
+    from bamrex_b200 import problems
+    n = 100 if D == 2 else 36
+    hi = tuple(n - 1 if d < D else 0 for d in range(3))
+    boxes = oracle.decompose(D, (0, 0, 0), hi, 24 if D == 2 else 12)
+    u0 = problems.random_states(D, tuple(n if d < D else 1 for d in (2, 1, 0)), seed=5)
+    outs = []
+    for mode in (bx.XSWEEP_ROWS, bx.XSWEEP_MARCH, bx.XSWEEP_AUTO):
+        lev = bx.Level(D, (0, 0, 0), hi, [0.0] * D, [1.0] * D, boxes, bx.Parm(D, limiter=limiter), method=method,
+                       cfl=0.6, bc_lo=(1,) * 3, bc_hi=(1,) * 3, x_mode=mode)
+        if mode == bx.XSWEEP_AUTO:
+            assert lev.x_mode == bx.XSWEEP_MARCH
+        lev.set_state(u0)
+        lev.run(3, use_graph=False)
+        outs.append(lev.get_state())
+        lev.close()
+    for o in outs[1:]:
+        assert rel_linf(o, outs[0]) <= 3 * RTOL_STEP
+    # a single wide box keeps the row kernel
+    lev = bx.Level(2, (0, 0, 0), (4095, 4095, 0), [0.0, 0.0], [1.0, 1.0], [((0, 0, 0), (4095, 4095, 0))],
+                   bx.Parm(2), cfl=0.6)
+    assert lev.x_mode == bx.XSWEEP_ROWS
+    lev.close()

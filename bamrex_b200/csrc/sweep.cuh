@@ -322,28 +322,40 @@ __global__ void __launch_bounds__(kSweepThreads, min_blocks<T>()) sweep_s_kernel
 
         const int plo = s0 - H, phi = s1 - 1 + H;  // loadable positions
         // x sweep: the staged rows; positions are read in order, so a
-        // warp-uniform test refills the buffer every kStageW reads, and the
-        // updates leave through the output buffer every kStageW cells
-        T* sin = nullptr;
+        // warp-uniform test switches input buffers every kStageW reads, and
+        // the updates leave through the output buffer every kStageW cells
+        T* sin = nullptr;   // two input buffers: the chunk being read, the next one in flight
         T* sout = nullptr;
-        int pbase = 0, pnext = 0, obase = s0;
+        int pbase = 0, pnext = 0, obase = s0, cur = 0;
         const int rows_left = B.hi[LD] - (B.lo[LD] + grp * 32) + 1;
         const T* gin = nullptr;
         T* gout = nullptr;
         long long step8 = 0, ostep8 = 0;
-        auto refill = [&](int p0) {
-            __syncwarp();
+        // start the asynchronous copy of the chunk at p0 into input buffer b
+        // (positions outside the loadable range, or rows outside the box, get
+        // the benign state); completes at the next wait_stage
+        auto issue = [&](int p0, int b) {
+            T* buf = sin + b * (NC * 32 * kStageW);
             const int c = lane & 3;
             const bool pin = p0 + c >= plo && p0 + c <= phi;
 #pragma unroll
             for (int i = 0; i < 4; ++i) {
                 const int r = (lane >> 2) + 8 * i;
-                T u[NC];
-                if (pin && r < rows_left) ld_state(gin + i * step8 + p0, inns, u);
-                else benign(u);
+                if (pin && r < rows_left) {
 #pragma unroll
-                for (int n = 0; n < NC; ++n) sin[(n * 32 + r) * kStagePitch + c] = u[n];
+                    for (int n = 0; n < NC; ++n)
+                        cp_async_elem(&buf[stage_slot(n * 32 + r, c)], gin + i * step8 + p0 + n * inns);
+                } else {
+                    T u[NC];
+                    benign(u);
+#pragma unroll
+                    for (int n = 0; n < NC; ++n) buf[stage_slot(n * 32 + r, c)] = u[n];
+                }
             }
+            cp_async_commit();
+        };
+        auto wait_stage = [&]() {
+            cp_async_wait_all();
             __syncwarp();
         };
         auto flush = [&](int count) {
@@ -354,7 +366,7 @@ __global__ void __launch_bounds__(kSweepThreads, min_blocks<T>()) sweep_s_kernel
                 const int r = (lane >> 2) + 8 * i;
                 if (c < count && r < rows_left) {
 #pragma unroll
-                    for (int n = 0; n < NC; ++n) gout[i * ostep8 + obase + n * ons] = sout[(n * 32 + r) * kStagePitch + c];
+                    for (int n = 0; n < NC; ++n) gout[i * ostep8 + obase + n * ons] = sout[stage_slot(n * 32 + r, c)];
                 }
             }
             __syncwarp();
@@ -362,7 +374,7 @@ __global__ void __launch_bounds__(kSweepThreads, min_blocks<T>()) sweep_s_kernel
         if constexpr (DIR == 0) {
             extern __shared__ __align__(16) unsigned char bamrex_stage_smem[];
             sin = reinterpret_cast<T*>(bamrex_stage_smem) + (threadIdx.x >> 5) * stage_elems_per_warp<T, NC>();
-            sout = sin + NC * 32 * kStagePitch;
+            sout = sin + 2 * NC * 32 * kStageW;
             // lane (r0 = lane / 4, c = lane % 4) moves rows r0 + 8 i, cell c
             const long long rb = (long long)(lane >> 2) + (B.lo[LD] + grp * 32) - lp;
             gin = in + rb * B.in.js + (lane & 3);
@@ -371,17 +383,25 @@ __global__ void __launch_bounds__(kSweepThreads, min_blocks<T>()) sweep_s_kernel
             ostep8 = 8 * B.out.js;
             pbase = s0 - 2;
             pnext = s0 - 2;
-            refill(pbase);
+            wait_stage();  // the previous item's copies have landed and its reads are done
+            issue(pbase, 0);
+            wait_stage();
+            issue(pbase + kStageW, 1);
         }
         auto load = [&](int pos, T (&u)[NC]) {
             if constexpr (DIR == 0) {
                 if (pnext == pbase + kStageW) {
+                    // the next chunk has landed; the one just read takes the
+                    // chunk after it
                     pbase += kStageW;
-                    refill(pbase);
+                    cur ^= 1;
+                    wait_stage();
+                    issue(pbase + kStageW, cur ^ 1);
                 }
                 const int c = pnext - pbase;
+                const T* buf = sin + cur * (NC * 32 * kStageW);
 #pragma unroll
-                for (int n = 0; n < NC; ++n) u[n] = sin[(n * 32 + lane) * kStagePitch + c];
+                for (int n = 0; n < NC; ++n) u[n] = buf[stage_slot(n * 32 + lane, c)];
                 ++pnext;
                 (void)pos;
             } else {
@@ -421,7 +441,7 @@ __global__ void __launch_bounds__(kSweepThreads, min_blocks<T>()) sweep_s_kernel
             if constexpr (DIR == 0) {
                 if (o >= s0 && do_update) {
 #pragma unroll
-                    for (int n = 0; n < NC; ++n) sout[(n * 32 + lane) * kStagePitch + (o - obase)] = Un[n];
+                    for (int n = 0; n < NC; ++n) sout[stage_slot(n * 32 + lane, o - obase)] = Un[n];
                     if (o - obase == kStageW - 1 || o == s1 - 1) {
                         flush(o - obase + 1);
                         obase += kStageW;
@@ -453,6 +473,7 @@ __global__ void __launch_bounds__(kSweepThreads, min_blocks<T>()) sweep_s_kernel
             copy_state(UL2, ULb);
         }
     }
+    if constexpr (DIR == 0) cp_async_wait_all();  // no copy outlives the kernel
     if (a.ws_max) reduce_ws(wsmax, nan_seen, a.ws_max);
 }
 

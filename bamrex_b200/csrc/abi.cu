@@ -623,19 +623,8 @@ void build_ghost_ops(const bamrex_level* L, int d, const BoxIndex& idx, std::vec
             }
         }
     }
-    long long acc = 0;
-    for (auto& op : ops) {
-        op.cell_begin = acc;
-        acc += (long long)(op.hi[0] - op.lo[0] + 1) * (op.hi[1] - op.lo[1] + 1) * (op.hi[2] - op.lo[2] + 1);
-    }
 }
 
-long long ops_cells(const std::vector<GhostOp>& ops)
-{
-    if (ops.empty()) return 0;
-    const GhostOp& o = ops.back();
-    return o.cell_begin + (long long)(o.hi[0] - o.lo[0] + 1) * (o.hi[1] - o.lo[1] + 1) * (o.hi[2] - o.lo[2] + 1);
-}
 
 }  // namespace
 
@@ -651,7 +640,7 @@ int level_launch(bamrex_level* L, cudaError_t e, const char* what)
 int level_fill(bamrex_level* L, int d, int parity, const StepScalars* scal)
 {
     if (L->nghost[d] == 0) return BAMREX_OK;
-    return level_launch(L, launch_ghost_fill(L->NC, L->fp32, L->d_ghost[d], L->nghost[d], L->ghost_cells[d], L->d_fab[parity], scal,
+    return level_launch(L, launch_ghost_fill(L->NC, L->fp32, L->d_ghost[d], L->nghost[d], L->ghost_chunks[d], L->d_fab[parity], scal,
                                              L->stream),
                         "ghost fill");
 }
@@ -873,7 +862,7 @@ extern "C" int bamrex_level_create(bamrex_level** out, const bamrex_level_desc* 
     for (int d = 0; d < D; ++d) {
         build_ghost_ops(L, d, bidx, ghost_host[d]);
         L->nghost[d] = (int)ghost_host[d].size();
-        L->ghost_cells[d] = ops_cells(ghost_host[d]);
+        L->ghost_chunks[d] = number_ghost_ops(ghost_host[d]);
     }
 
     // ---- pack boxes

@@ -1248,11 +1248,7 @@ int set_level(bamrex_amr* A, int lev, const std::vector<bamrex_box>& boxes)
                 ops.push_back(op);
             }
         }
-        long long acc = 0;
-        for (auto& op : ops) {
-            op.cell_begin = acc;
-            acc += (long long)(op.hi[0] - op.lo[0] + 1) * (op.hi[1] - op.lo[1] + 1) * (op.hi[2] - op.lo[2] + 1);
-        }
+        const int nchunks = number_ghost_ops(ops);
         if (!ops.empty()) {
             std::vector<FabDev> tab = L->fab[L->cur];
             tab.insert(tab.end(), O->fab[O->cur].begin(), O->fab[O->cur].end());
@@ -1263,7 +1259,7 @@ int set_level(bamrex_amr* A, int lev, const std::vector<bamrex_box>& boxes)
             GhostOp* dops = (GhostOp*)((char*)dmem + align_up(tb, 256));
             if (e == cudaSuccess) e = cudaMemcpy(dops, ops.data(), ob, cudaMemcpyHostToDevice);
             if (e == cudaSuccess)
-                e = launch_ghost_fill(L->NC, L->fp32, dops, (int)ops.size(), acc, (const FabDev*)dmem, nullptr, A->stream);
+                e = launch_ghost_fill(L->NC, L->fp32, dops, (int)ops.size(), nchunks, (const FabDev*)dmem, nullptr, A->stream);
             if (e == cudaSuccess) e = cudaStreamSynchronize(A->stream);
             if (dmem) cudaFree(dmem);
             if (e != cudaSuccess) rc = cuda_fail(e, "regrid copy");

@@ -45,28 +45,44 @@ __device__ __forceinline__ int find_by_begin(const V* v, int n, long long idx)
 // bamrexBCData::fill_consv_boundary (Source/BoundaryConditions/BCs.cpp:429-442)
 // expressed as a table of region copies built on the host.
 template <typename T>
-__global__ void ghost_fill_kernel(int NC, const GhostOp* __restrict__ ops, int nops, long long total,
+__global__ void ghost_fill_kernel(int NC, const GhostOp* __restrict__ ops, int nops, int nchunks,
                                   const FabDev* __restrict__ fabs, const StepScalars* scal)
 {
+    static_assert(kGhostChunk == 32, "one ghost chunk per warp");
     if (scal && scal->done) return;
-    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
-         idx += (long long)gridDim.x * blockDim.x) {
-        const GhostOp& op = ops[find_by_begin(ops, nops, idx)];
-        const long long local = idx - op.cell_begin;
+    const int lane = threadIdx.x & 31;
+    const int w = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int nw = (int)((gridDim.x * blockDim.x) >> 5);
+    for (int q = w; q < nchunks; q += nw) {
+        // lane 0 finds the op of chunk q, the warp shares it
+        int opi = 0;
+        if (lane == 0) {
+            int lo = 0, hi = nops - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (ops[mid].chunk_begin <= q) lo = mid; else hi = mid - 1;
+            }
+            opi = lo;
+        }
+        opi = __shfl_sync(0xffffffffu, opi, 0);
+        const GhostOp& op = ops[opi];
+        const long long local = (long long)(q - op.chunk_begin) * kGhostChunk + lane;
         const int nx = op.hi[0] - op.lo[0] + 1, ny = op.hi[1] - op.lo[1] + 1;
-        const int ci = op.lo[0] + (int)(local % nx);
-        const int cj = op.lo[1] + (int)((local / nx) % ny);
-        const int ck = op.lo[2] + (int)(local / ((long long)nx * ny));
-        const int si = op.off[0] + op.mul[0] * ci;
-        const int sj = op.off[1] + op.mul[1] * cj;
-        const int sk = op.off[2] + op.mul[2] * ck;
-        const FabDev& d = fabs[op.dst];
-        const FabDev& s = fabs[op.src];
-        const T* ps = s.ptr<T>() + fab_index(s, si, sj, sk);
-        T* pd = d.ptr<T>() + fab_index(d, ci, cj, ck);
-        for (int n = 0; n < NC; ++n) {
-            const T v = ps[n * s.ns];
-            pd[n * d.ns] = ((op.negmask >> n) & 1) ? -v : v;
+        if (local < ghost_op_cells(op)) {
+            const int ci = op.lo[0] + (int)(local % nx);
+            const int cj = op.lo[1] + (int)((local / nx) % ny);
+            const int ck = op.lo[2] + (int)(local / ((long long)nx * ny));
+            const int si = op.off[0] + op.mul[0] * ci;
+            const int sj = op.off[1] + op.mul[1] * cj;
+            const int sk = op.off[2] + op.mul[2] * ck;
+            const FabDev& d = fabs[op.dst];
+            const FabDev& s = fabs[op.src];
+            const T* ps = s.ptr<T>() + fab_index(s, si, sj, sk);
+            T* pd = d.ptr<T>() + fab_index(d, ci, cj, ck);
+            for (int n = 0; n < NC; ++n) {
+                const T v = ps[n * s.ns];
+                pd[n * d.ns] = ((op.negmask >> n) & 1) ? -v : v;
+            }
         }
     }
 }
@@ -299,12 +315,14 @@ int device_sm_count()
     return cache[dev];
 }
 
-cudaError_t launch_ghost_fill(int NC, bool fp32, const GhostOp* ops, int nops, long long total_cells,
-                              const FabDev* fabs, const StepScalars* scal, cudaStream_t s)
+cudaError_t launch_ghost_fill(int NC, bool fp32, const GhostOp* ops, int nops, int nchunks, const FabDev* fabs,
+                              const StepScalars* scal, cudaStream_t s)
 {
-    if (nops == 0 || total_cells == 0) return cudaSuccess;
-    if (fp32) ghost_fill_kernel<float><<<grid_for(total_cells), kThreads, 0, s>>>(NC, ops, nops, total_cells, fabs, scal);
-    else ghost_fill_kernel<double><<<grid_for(total_cells), kThreads, 0, s>>>(NC, ops, nops, total_cells, fabs, scal);
+    if (nops == 0 || nchunks == 0) return cudaSuccess;
+    const long long warps = kThreads / 32;
+    const int g = (int)std::min<long long>((nchunks + warps - 1) / warps, (long long)device_sm_count() * 8);
+    if (fp32) ghost_fill_kernel<float><<<g, kThreads, 0, s>>>(NC, ops, nops, nchunks, fabs, scal);
+    else ghost_fill_kernel<double><<<g, kThreads, 0, s>>>(NC, ops, nops, nchunks, fabs, scal);
     return cudaGetLastError();
 }
 

@@ -5,6 +5,8 @@
 
 #include <cuda_runtime.h>
 
+#include <vector>
+
 #include "common.cuh"
 
 namespace bamrex {
@@ -17,9 +19,33 @@ struct GhostOp {
     int lo[3], hi[3];
     int off[3], mul[3];
     int negmask;
-    int pad;
+    int chunk_begin;  // first block-sized chunk of this op (number_ghost_ops)
     long long cell_begin;
 };
+
+// Cells per warp of the ghost-fill kernel; every op starts a new chunk, so a
+// warp finds its op once instead of every thread searching per cell, and
+// small ops (the ghost slabs of narrow boxes) still fill whole warps.
+constexpr int kGhostChunk = 32;
+
+__host__ __device__ inline long long ghost_op_cells(const GhostOp& o)
+{
+    return (long long)(o.hi[0] - o.lo[0] + 1) * (o.hi[1] - o.lo[1] + 1) * (o.hi[2] - o.lo[2] + 1);
+}
+
+// Sets cell_begin and chunk_begin of every op; returns the number of chunks.
+inline int number_ghost_ops(std::vector<GhostOp>& ops)
+{
+    long long cells = 0, chunks = 0;
+    for (auto& op : ops) {
+        op.cell_begin = cells;
+        op.chunk_begin = (int)chunks;
+        const long long n = ghost_op_cells(op);
+        cells += n;
+        chunks += (n + kGhostChunk - 1) / kGhostChunk;
+    }
+    return (int)chunks;
+}
 
 // Valid region of a box in the packed (box-major, SoA) host layout.
 struct PackBox {
@@ -49,8 +75,8 @@ long long sweep_resident_warps(int D, int dir, int method, bool fp32, const Cons
 // limiting, gamma with 1/z = 7), or -1 for the general kernels.
 int fast_limiter(int D, int method, const Consts& k);
 
-cudaError_t launch_ghost_fill(int NC, bool fp32, const GhostOp* ops, int nops, long long total_cells,
-                              const FabDev* fabs, const StepScalars* scal, cudaStream_t s);
+cudaError_t launch_ghost_fill(int NC, bool fp32, const GhostOp* ops, int nops, int nchunks, const FabDev* fabs,
+                              const StepScalars* scal, cudaStream_t s);
 
 // Packed buffer is always double; fabs are double or float.
 cudaError_t launch_pack(int NC, bool fp32, const FabDev* fabs, const PackBox* boxes, int nboxes,

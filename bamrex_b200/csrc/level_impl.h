@@ -79,7 +79,7 @@ struct bamrex_level {
     bool x_march = false;  // x sweep by the marching (thread-per-row) kernel
     bamrex::GhostOp* d_ghost[3] = { nullptr, nullptr, nullptr };
     int nghost[3] = { 0, 0, 0 };
-    long long ghost_cells[3] = { 0, 0, 0 };
+    int ghost_chunks[3] = { 0, 0, 0 };
     bamrex::PackBox* d_pack = nullptr;
     long long ncells = 0;
     size_t state_bytes = 0;  // bytes of one state buffer

@@ -168,10 +168,11 @@ void box_items(int dir, const int* lo, const int* hi, int seglen, long long& ite
         ngroup = 1;
         items = (long long)n[1] * n[2] * nseg;
     } else {
-        const int across = dir == 0 ? n[1] : n[0];
-        ngroup = (across + 31) / 32;
-        const int other = (dir == 2) ? n[1] : n[2];
-        items = (long long)ngroup * other * nseg;
+        // 32 columns of the plane across dir per group (boxes narrower than
+        // 32 cells fill the lanes from the next plane)
+        const long long cols = (long long)(dir == 0 ? n[1] : n[0]) * (dir == 2 ? n[1] : n[2]);
+        ngroup = (int)((cols + 31) / 32);
+        items = (long long)ngroup * nseg;
     }
 }
 
@@ -201,7 +202,7 @@ int choose_seglen(int dir, const std::vector<bamrex_box>& boxes, long long resid
 // Lane-cell slots of the two x-sweep kernels over a set of boxes: the row
 // kernel spends two extra 32-cell chunks on every row segment (its
 // software pipeline), the marching kernel four extra cells per segment and
-// idle lanes when a box is not a multiple of 32 rows high; its per-cell cost
+// idle lanes in its last group of 32 rows; its per-cell cost
 // carries a 30% allowance for staging rows through shared memory (measured
 // on 4096^2 in boxes of 32 to 4096 cells).
 bool prefer_x_march(int D, const std::vector<bamrex_box>& boxes, int seg_rows, int seg_march)
@@ -220,7 +221,7 @@ bool prefer_x_march(int D, const std::vector<bamrex_box>& boxes, int seg_rows, i
         box_items(0, b.lo, b.hi, seg_march, items, nseg, ngroup, true, &bl);
         for (long long x = 0; x < n0; x += bl) {
             const long long len = std::min<long long>(bl, n0 - x);
-            march += 1.3 * (double)(((n1 + 31) / 32) * 32 * n2) * (double)(len + 4);
+            march += 1.3 * (double)((n1 * n2 + 31) / 32 * 32) * (double)(len + 4);
         }
     }
     return march < rows;

@@ -284,18 +284,25 @@ __global__ void __launch_bounds__(kSweepThreads, min_blocks<T>()) sweep_s_kernel
         const long long local = it - B.item_begin;
         const int seg = (int)(local % B.nseg);
         const long long rest = local / B.nseg;
-        const int grp = (int)(rest % B.ngroup);
-        const int t2 = (int)(rest / B.ngroup);  // the other transverse index
-        constexpr int LD = (DIR == 0) ? 1 : 0;  // the direction across the lanes
-        const int lp = B.lo[LD] + grp * 32 + lane;
-        const bool active = lp <= B.hi[LD];
+        const int grp = (int)rest;
+        // The lanes take 32 consecutive columns of the plane across DIR,
+        // numbered with LD fastest then OT, so boxes narrower than 32 cells
+        // still fill the warp (a group may span several OT planes).
+        constexpr int LD = (DIR == 0) ? 1 : 0;  // the faster direction across the lanes
+        constexpr int OT = (DIR == 2) ? 1 : 2;  // the slower one
+        const int nld = B.hi[LD] - B.lo[LD] + 1;
+        const int ncol = nld * (B.hi[OT] - B.lo[OT] + 1);
+        const int fi = grp * 32 + lane;
+        const bool active = fi < ncol;
+        const int fa = active ? fi : 0;
+        const int lp = B.lo[LD] + fa % nld;
+        const int tr = B.lo[OT] + fa / nld;
         const int s0 = B.lo[DIR] + seg * B.seglen;
         const int s1 = min(s0 + B.seglen, B.hi[DIR] + 1);
         const bool last_seg = (s1 == B.hi[DIR] + 1);
 
         // column base offsets (position along DIR added per access): cell
         // (i, j, k) sits at (i - b0) + (j - b1) js + (k - b2) ks
-        const int tr = (DIR == 2) ? B.lo[1] + t2 : ((D == 3) ? B.lo[2] + t2 : B.lo[2]);  // the other index
         auto column = [&](const FabDev& G, long long& off, long long& step) {
             if (DIR == 0) {
                 off = (long long)(lp - G.b1) * G.js + (long long)(tr - G.b2) * G.ks - (long long)G.b0;
@@ -327,10 +334,10 @@ __global__ void __launch_bounds__(kSweepThreads, min_blocks<T>()) sweep_s_kernel
         T* sin = nullptr;   // two input buffers: the chunk being read, the next one in flight
         T* sout = nullptr;
         int pbase = 0, pnext = 0, obase = s0, cur = 0;
-        const int rows_left = B.hi[LD] - (B.lo[LD] + grp * 32) + 1;
-        const T* gin = nullptr;
+        const int rows_left = ncol - grp * 32;
+        const T* gin = nullptr;   // row 0 of the input / output fab, cell (lane % 4) of a chunk
         T* gout = nullptr;
-        long long step8 = 0, ostep8 = 0;
+        long long* srow = nullptr;  // per warp: the 32 rows' offsets in the input and output fabs
         // start the asynchronous copy of the chunk at p0 into input buffer b
         // (positions outside the loadable range, or rows outside the box, get
         // the benign state); completes at the next wait_stage
@@ -342,9 +349,9 @@ __global__ void __launch_bounds__(kSweepThreads, min_blocks<T>()) sweep_s_kernel
             for (int i = 0; i < 4; ++i) {
                 const int r = (lane >> 2) + 8 * i;
                 if (pin && r < rows_left) {
+                    const T* src = gin + srow[r] + p0;
 #pragma unroll
-                    for (int n = 0; n < NC; ++n)
-                        cp_async_elem(&buf[stage_slot(n * 32 + r, c)], gin + i * step8 + p0 + n * inns);
+                    for (int n = 0; n < NC; ++n) cp_async_elem(&buf[stage_slot(n * 32 + r, c)], src + n * inns);
                 } else {
                     T u[NC];
                     benign(u);
@@ -365,25 +372,30 @@ __global__ void __launch_bounds__(kSweepThreads, min_blocks<T>()) sweep_s_kernel
             for (int i = 0; i < 4; ++i) {
                 const int r = (lane >> 2) + 8 * i;
                 if (c < count && r < rows_left) {
+                    T* dst = gout + srow[32 + r] + obase;
 #pragma unroll
-                    for (int n = 0; n < NC; ++n) gout[i * ostep8 + obase + n * ons] = sout[stage_slot(n * 32 + r, c)];
+                    for (int n = 0; n < NC; ++n) dst[n * ons] = sout[stage_slot(n * 32 + r, c)];
                 }
             }
             __syncwarp();
         };
         if constexpr (DIR == 0) {
             extern __shared__ __align__(16) unsigned char bamrex_stage_smem[];
-            sin = reinterpret_cast<T*>(bamrex_stage_smem) + (threadIdx.x >> 5) * stage_elems_per_warp<T, NC>();
+            const int wib = threadIdx.x >> 5;
+            sin = reinterpret_cast<T*>(bamrex_stage_smem) + wib * stage_elems_per_warp<T, NC>();
             sout = sin + 2 * NC * 32 * kStageW;
+            srow = reinterpret_cast<long long*>(bamrex_stage_smem + (size_t)(kSweepThreads / 32) *
+                                                                          stage_elems_per_warp<T, NC>() * sizeof(T)) +
+                   wib * 64;
             // lane (r0 = lane / 4, c = lane % 4) moves rows r0 + 8 i, cell c
-            const long long rb = (long long)(lane >> 2) + (B.lo[LD] + grp * 32) - lp;
-            gin = in + rb * B.in.js + (lane & 3);
-            gout = out + rb * B.out.js + (lane & 3);
-            step8 = 8 * B.in.js;
-            ostep8 = 8 * B.out.js;
+            gin = B.in.ptr<T>() + (lane & 3);
+            gout = B.out.ptr<T>() + (lane & 3);
             pbase = s0 - 2;
             pnext = s0 - 2;
             wait_stage();  // the previous item's copies have landed and its reads are done
+            srow[lane] = inoff;        // this lane's row: cell (i, lp, tr) at inoff + i
+            srow[32 + lane] = outoff;
+            __syncwarp();
             issue(pbase, 0);
             wait_stage();
             issue(pbase + kStageW, 1);

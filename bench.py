@@ -356,11 +356,15 @@ def amr_blast_run(n0, coarse_steps, precision):
     # stepping alone (fixed grids), then with a regrid every 2 coarse steps
     A.set_regrid_int(0)
     torch.cuda.synchronize()
+    # an NVTX range lets a profiler capture exactly these steps
+    # (ncu --nvtx --nvtx-include "amr_fixed_steps_fp64/")
+    torch.cuda.nvtx.range_push("amr_fixed_steps_" + ("fp64" if precision == bx.FP64 else "fp32"))
     t0 = time.perf_counter()
     for _ in range(coarse_steps):
         A.coarse_step()
     torch.cuda.synchronize()
     dt_fixed = time.perf_counter() - t0
+    torch.cuda.nvtx.range_pop()
     s1 = A.conserved_sums()
     A.set_regrid_int(2)
     t0 = time.perf_counter()

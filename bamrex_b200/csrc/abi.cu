@@ -898,7 +898,7 @@ extern "C" int bamrex_level_create(bamrex_level** out, const bamrex_level_desc* 
     for (int d = 0; d < D; ++d)
         for (int p = 0; p < 2; ++p) o_sweep[d][p] = take(sizeof(SweepBox) * nb);
     size_t o_ghost[3] = {};
-    for (int d = 0; d < D; ++d) o_ghost[d] = take(sizeof(GhostOp) * std::max<size_t>(1, ghost_host[d].size()));
+    for (int d = 0; d < D; ++d) o_ghost[d] = take(std::max<size_t>(1, ghost_table_bytes(ghost_host[d].size(), L->ghost_chunks[d])));
     const size_t o_pack = take(sizeof(PackBox) * nb);
     const size_t o_stage = take((size_t)L->ncells * L->NC * 8);
     const size_t o_scal = take(sizeof(StepScalars));
@@ -948,6 +948,10 @@ extern "C" int bamrex_level_create(bamrex_level** out, const bamrex_level_desc* 
             ue = up(L->d_sweep[d][p], t.data(), sizeof(SweepBox) * nb);
         }
         if (ue == cudaSuccess) ue = up(L->d_ghost[d], ghost_host[d].data(), sizeof(GhostOp) * ghost_host[d].size());
+        if (ue == cudaSuccess) {
+            const std::vector<int> ct = ghost_chunk_table(ghost_host[d], L->ghost_chunks[d]);
+            ue = up(L->d_ghost[d] + ghost_host[d].size(), ct.data(), sizeof(int) * ct.size());
+        }
     }
     if (ue == cudaSuccess) ue = up(L->d_pack, pack_host.data(), sizeof(PackBox) * nb);
     if (ue == cudaSuccess) ue = cudaMemset(L->arena + o_state0, 0, (size_t)(o_state1 - o_state0) * 2);

@@ -1254,10 +1254,12 @@ int set_level(bamrex_amr* A, int lev, const std::vector<bamrex_box>& boxes)
             tab.insert(tab.end(), O->fab[O->cur].begin(), O->fab[O->cur].end());
             void* dmem = nullptr;
             const size_t tb = sizeof(FabDev) * tab.size(), ob = sizeof(GhostOp) * ops.size();
-            cudaError_t e = cudaMalloc(&dmem, align_up(tb, 256) + ob);
+            const std::vector<int> ct = ghost_chunk_table(ops, nchunks);
+            cudaError_t e = cudaMalloc(&dmem, align_up(tb, 256) + ghost_table_bytes(ops.size(), nchunks));
             if (e == cudaSuccess) e = cudaMemcpy(dmem, tab.data(), tb, cudaMemcpyHostToDevice);
             GhostOp* dops = (GhostOp*)((char*)dmem + align_up(tb, 256));
             if (e == cudaSuccess) e = cudaMemcpy(dops, ops.data(), ob, cudaMemcpyHostToDevice);
+            if (e == cudaSuccess) e = cudaMemcpy(dops + ops.size(), ct.data(), sizeof(int) * ct.size(), cudaMemcpyHostToDevice);
             if (e == cudaSuccess)
                 e = launch_ghost_fill(L->NC, L->fp32, dops, (int)ops.size(), nchunks, (const FabDev*)dmem, nullptr, A->stream);
             if (e == cudaSuccess) e = cudaStreamSynchronize(A->stream);

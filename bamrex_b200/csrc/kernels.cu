@@ -50,28 +50,21 @@ __global__ void ghost_fill_kernel(int NC, const GhostOp* __restrict__ ops, int n
 {
     static_assert(kGhostChunk == 32, "one ghost chunk per warp");
     if (scal && scal->done) return;
+    const int* __restrict__ chunk_op = reinterpret_cast<const int*>(ops + nops);
     const int lane = threadIdx.x & 31;
     const int w = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     const int nw = (int)((gridDim.x * blockDim.x) >> 5);
     for (int q = w; q < nchunks; q += nw) {
-        // lane 0 finds the op of chunk q, the warp shares it
-        int opi = 0;
-        if (lane == 0) {
-            int lo = 0, hi = nops - 1;
-            while (lo < hi) {
-                const int mid = (lo + hi + 1) >> 1;
-                if (ops[mid].chunk_begin <= q) lo = mid; else hi = mid - 1;
-            }
-            opi = lo;
-        }
-        opi = __shfl_sync(0xffffffffu, opi, 0);
-        const GhostOp& op = ops[opi];
-        const long long local = (long long)(q - op.chunk_begin) * kGhostChunk + lane;
+        const GhostOp& op = ops[chunk_op[q]];
+        // 32-bit index arithmetic: a copy op is a ghost slab, far below 2^31 cells
+        const int local = (q - op.chunk_begin) * kGhostChunk + lane;
         const int nx = op.hi[0] - op.lo[0] + 1, ny = op.hi[1] - op.lo[1] + 1;
-        if (local < ghost_op_cells(op)) {
-            const int ci = op.lo[0] + (int)(local % nx);
-            const int cj = op.lo[1] + (int)((local / nx) % ny);
-            const int ck = op.lo[2] + (int)(local / ((long long)nx * ny));
+        if (local < (int)ghost_op_cells(op)) {
+            const int row = local / nx;
+            const int ci = op.lo[0] + (local - row * nx);
+            const int kk = row / ny;
+            const int cj = op.lo[1] + (row - kk * ny);
+            const int ck = op.lo[2] + kk;
             const int si = op.off[0] + op.mul[0] * ci;
             const int sj = op.off[1] + op.mul[1] * cj;
             const int sk = op.off[2] + op.mul[2] * ck;
@@ -79,10 +72,15 @@ __global__ void ghost_fill_kernel(int NC, const GhostOp* __restrict__ ops, int n
             const FabDev& s = fabs[op.src];
             const T* ps = s.ptr<T>() + fab_index(s, si, sj, sk);
             T* pd = d.ptr<T>() + fab_index(d, ci, cj, ck);
-            for (int n = 0; n < NC; ++n) {
-                const T v = ps[n * s.ns];
-                pd[n * d.ns] = ((op.negmask >> n) & 1) ? -v : v;
-            }
+            // every load issued before the first store (the compiler cannot
+            // tell that source and destination do not alias)
+            T v[kMaxComp];
+#pragma unroll
+            for (int n = 0; n < kMaxComp; ++n)
+                if (n < NC) v[n] = ps[n * s.ns];
+#pragma unroll
+            for (int n = 0; n < kMaxComp; ++n)
+                if (n < NC) pd[n * d.ns] = ((op.negmask >> n) & 1) ? -v[n] : v[n];
         }
     }
 }

@@ -34,6 +34,8 @@ __host__ __device__ inline long long ghost_op_cells(const GhostOp& o)
 }
 
 // Sets cell_begin and chunk_begin of every op; returns the number of chunks.
+// On the device the ops are followed by the op index of every chunk
+// (ghost_chunk_table), which launch_ghost_fill expects.
 inline int number_ghost_ops(std::vector<GhostOp>& ops)
 {
     long long cells = 0, chunks = 0;
@@ -46,6 +48,19 @@ inline int number_ghost_ops(std::vector<GhostOp>& ops)
     }
     return (int)chunks;
 }
+
+inline std::vector<int> ghost_chunk_table(const std::vector<GhostOp>& ops, int nchunks)
+{
+    std::vector<int> t((size_t)nchunks);
+    for (size_t i = 0; i < ops.size(); ++i) {
+        const int end = i + 1 < ops.size() ? ops[i + 1].chunk_begin : nchunks;
+        for (int q = ops[i].chunk_begin; q < end; ++q) t[(size_t)q] = (int)i;
+    }
+    return t;
+}
+
+// Bytes of the device copy of ops + chunk table.
+inline size_t ghost_table_bytes(size_t nops, int nchunks) { return sizeof(GhostOp) * nops + sizeof(int) * (size_t)nchunks; }
 
 // Valid region of a box in the packed (box-major, SoA) host layout.
 struct PackBox {

@@ -74,10 +74,11 @@ __global__ void cf_interp_kernel(const CfInterpArgs a)
     for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < a.ncells;
          idx += (long long)gridDim.x * blockDim.x) {
         const CfRegion& R = a.regions[find_begin(a.regions, a.nregions, idx)];
-        const long long local = idx - R.cell_begin;
+        // 32-bit index arithmetic: a region is a ghost slab or one fine box
+        const int local = (int)(idx - R.cell_begin);
         const int nx = R.hi[0] - R.lo[0] + 1, ny = R.hi[1] - R.lo[1] + 1;
-        const int f[3] = { R.lo[0] + (int)(local % nx), R.lo[1] + (int)((local / nx) % ny),
-                           R.lo[2] + (int)(local / ((long long)nx * ny)) };
+        const int row = local / nx, kk = row / ny;
+        const int f[3] = { R.lo[0] + (local - row * nx), R.lo[1] + (row - kk * ny), R.lo[2] + kk };
         int c[3];
         double xi[3];
         for (int d = 0; d < 3; ++d) {
@@ -134,11 +135,12 @@ __global__ void avg_down_kernel(int D, int NC, int r, const AvgOp* __restrict__ 
     for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < n;
          idx += (long long)gridDim.x * blockDim.x) {
         const AvgOp& op = ops[find_begin(ops, nops, idx)];
-        const long long local = idx - op.cell_begin;
+        const int local = (int)(idx - op.cell_begin);  // one coarse/fine box intersection
         const int nx = op.hi[0] - op.lo[0] + 1, ny = op.hi[1] - op.lo[1] + 1;
-        const int i = op.lo[0] + (int)(local % nx);
-        const int j = op.lo[1] + (int)((local / nx) % ny);
-        const int k = op.lo[2] + (int)(local / ((long long)nx * ny));
+        const int row = local / nx, kk0 = row / ny;
+        const int i = op.lo[0] + (local - row * nx);
+        const int j = op.lo[1] + (row - kk0 * ny);
+        const int k = op.lo[2] + kk0;
         const FabDev& fc = crse[op.crse];
         const FabDev& ff = fine[op.fine];
         const long long ic = fidx(fc, i, j, k);

@@ -14,7 +14,7 @@ LIB_PATH = os.path.join(HERE, "libbamrex_cuda.so")
 MAX_NCOMP = 8
 
 # status codes
-OK, ERR_ARG, ERR_OOM, ERR_NAN, ERR_TIMEOUT, ERR_CUDA, ERR_UNSUPPORTED = range(7)
+OK, ERR_ARG, ERR_OOM, ERR_NAN, ERR_TIMEOUT, ERR_CUDA, ERR_UNSUPPORTED, ERR_NOT_CONVERGED = range(8)
 # NumericalMethods::Method (Source/NumericalMethods.H:10-19)
 MUSCL_HANCOCK, HLLC, IMEX, RCM, SLIC, FORCE, LAX_FRIEDRICHS = range(7)
 METHODS = {"muscl_hancock": MUSCL_HANCOCK, "hllc": HLLC, "imex": IMEX, "rcm": RCM, "slic": SLIC,
@@ -129,6 +129,33 @@ class HelmholtzDesc(ctypes.Structure):
         ("nu1", ctypes.c_int),
         ("nu2", ctypes.c_int),
         ("bottom_sweeps", ctypes.c_int),
+    ]
+
+
+# IMEX settings (BAMREX_IMEX_*) and fields of the last step
+IMEX_RUSANOV, IMEX_MUSCL_RUSANOV = 0, 1
+ENTH_REUSE_PRESSURE, ENTH_CONSERVATIVE, ENTH_CONSERVATIVE_EX = 0, 1, 2
+KE_CONSERVATIVE, KE_EX, KE_SPLIT = 0, 1, 2
+(FIELD_UEX, FIELD_ENTHALPY, FIELD_KE, FIELD_RHS, FIELD_PRESSURE, FIELD_FLUX_X, FIELD_FLUX_Y,
+ FIELD_FLUX_Z) = range(8)
+
+
+class ImexDesc(ctypes.Structure):
+    _fields_ = [
+        ("spacedim", ctypes.c_int),
+        ("n", ctypes.c_int * 3),
+        ("prob_lo", ctypes.c_double * 3),
+        ("prob_hi", ctypes.c_double * 3),
+        ("bc_lo", ctypes.c_int * 3),
+        ("bc_hi", ctypes.c_int * 3),
+        ("parm", CParm),
+        ("advection_flux", ctypes.c_int),
+        ("enthalpy_method", ctypes.c_int),
+        ("ke_method", ctypes.c_int),
+        ("cfl", ctypes.c_double),
+        ("tol_rel", ctypes.c_double),
+        ("tol_abs", ctypes.c_double),
+        ("max_iter", ctypes.c_int),
     ]
 
 
@@ -253,6 +280,17 @@ SIGNATURES = {
     "bamrex_precnet_set_tensor_cores": (_i, [_vp, _i]),
     "bamrex_helmholtz_solve_learned": (_i, [_vp, _vp, _i, _vp, _vp, _d, _d, _i, _i, ctypes.POINTER(_i),
                                             ctypes.POINTER(_i), _dp, ctypes.POINTER(_i)]),
+    "bamrex_imex_create": (_i, [ctypes.POINTER(_vp), ctypes.POINTER(ImexDesc), _vp]),
+    "bamrex_imex_destroy": (_i, [_vp]),
+    "bamrex_imex_last_error": (ctypes.c_char_p, [_vp]),
+    "bamrex_imex_set_state": (_i, [_vp, _vp, _vp]),
+    "bamrex_imex_get_state": (_i, [_vp, _vp, _vp]),
+    "bamrex_imex_est_time_step": (_i, [_vp, _dp]),
+    "bamrex_imex_step": (_i, [_vp, _d, ctypes.POINTER(_i), _dp]),
+    "bamrex_imex_set_precnet": (_i, [_vp, _vp, _i]),
+    "bamrex_imex_operator": (_vp, [_vp]),
+    "bamrex_imex_field": (_i, [_vp, _i, _vp, ctypes.POINTER(_ll)]),
+    "bamrex_imex_launches": (_ll, [_vp]),
 }
 
 _LIB = None

@@ -246,6 +246,7 @@ extern "C" const char* bamrex_status_string(int status)
     case BAMREX_ERR_TIMEOUT: return "device wait timed out";
     case BAMREX_ERR_CUDA: return "CUDA runtime error";
     case BAMREX_ERR_UNSUPPORTED: return "unsupported method or option";
+    case BAMREX_ERR_NOT_CONVERGED: return "iterative solve did not converge";
     default: return "unknown status";
     }
 }

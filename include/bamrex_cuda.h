@@ -36,7 +36,8 @@ enum {
     BAMREX_ERR_NAN = 3,         /* non-finite wave speed / time step */
     BAMREX_ERR_TIMEOUT = 4,     /* a bounded device wait gave up */
     BAMREX_ERR_CUDA = 5,        /* a CUDA runtime call failed */
-    BAMREX_ERR_UNSUPPORTED = 6  /* method/option not provided by this build */
+    BAMREX_ERR_UNSUPPORTED = 6, /* method/option not provided by this build */
+    BAMREX_ERR_NOT_CONVERGED = 7 /* an iterative solve did not reach its tolerance */
 };
 
 /* ---- numerical method, same values as NumericalMethods::Method
@@ -44,7 +45,7 @@ enum {
 enum {
     BAMREX_MUSCL_HANCOCK = 0,
     BAMREX_HLLC = 1,
-    BAMREX_IMEX = 2, /* not on this path: BAMREX_ERR_UNSUPPORTED */
+    BAMREX_IMEX = 2, /* not a level method: the IMEX step is bamrex_imex (below) */
     BAMREX_RCM = 3,  /* not on this path: BAMREX_ERR_UNSUPPORTED */
     BAMREX_SLIC = 4,
     BAMREX_FORCE = 5,
@@ -582,6 +583,84 @@ BAMREX_API int bamrex_helmholtz_solve_learned(bamrex_helmholtz *h, bamrex_precne
                                               const double *rhs, double tol_rel, double tol_abs, int max_iter,
                                               int restart, int *iters, int *plain_iters, double *rel_res,
                                               int *fell_back);
+
+/* ------------------------------------------------------------------ */
+/* The first-order IMEX step (advance_imex_rk with the SP111 tableau and   */
+/* the linearised pressure equation, Source/IMEX/IMEX_RK.cpp:23-86,        */
+/* Source/IMEX/IMEX_O1.cpp:19-176) on one box covering the domain          */
+/* ------------------------------------------------------------------ */
+
+typedef struct bamrex_imex bamrex_imex;
+
+/* IMEXSettings (Source/IMEX/IMEXSettings.H:6-79) */
+enum { BAMREX_IMEX_RUSANOV = 0, BAMREX_IMEX_MUSCL_RUSANOV = 1 };
+enum {
+    BAMREX_IMEX_ENTH_REUSE_PRESSURE = 0,
+    BAMREX_IMEX_ENTH_CONSERVATIVE = 1,
+    BAMREX_IMEX_ENTH_CONSERVATIVE_EX = 2
+};
+enum { BAMREX_IMEX_KE_CONSERVATIVE = 0, BAMREX_IMEX_KE_EX = 1, BAMREX_IMEX_KE_SPLIT = 2 };
+
+typedef struct bamrex_imex_desc {
+    int spacedim;            /* 2 or 3 */
+    int n[3];                /* cells per direction (one box: the domain) */
+    double prob_lo[3];
+    double prob_hi[3];
+    int bc_lo[3];            /* BAMREX_BC_TRANSMISSIVE / PERIODIC / REFLECTIVE; the */
+    int bc_hi[3];            /* pressure operator takes Neumann for the last two    */
+    bamrex_parm parm;        /* adiabatic (gamma) and epsilon are used */
+    int advection_flux;      /* imex.advection_flux */
+    int enthalpy_method;     /* imex.enthalpy_method */
+    int ke_method;           /* imex.ke_method */
+    double cfl;              /* adv.cfl (0 = 0.5) */
+    double tol_rel, tol_abs; /* pressure solve; 0 = 1e-12 / 1e-15 as solve_pressure */
+    int max_iter;            /* 0 = 1000 as solve_pressure */
+} bamrex_imex_desc;
+
+/* Allocates the state (with ghost cells), the intermediate fields and the
+ * pressure operator at creation; a step allocates nothing.  Work is issued on
+ * `stream` (NULL: the object's own non-blocking stream). */
+BAMREX_API int bamrex_imex_create(bamrex_imex **out, const bamrex_imex_desc *desc, void *stream);
+BAMREX_API int bamrex_imex_destroy(bamrex_imex *h);
+BAMREX_API const char *bamrex_imex_last_error(const bamrex_imex *h);
+/* The state: (D+2) components of n[0]*n[1]*n[2] doubles each, component-
+ * major, i fastest (host or device memory).  p: the pressure (same cell
+ * order), or NULL to take (gamma-1)(E - eps |m|^2 / (2 rho)) (copy_pressure). */
+BAMREX_API int bamrex_imex_set_state(bamrex_imex *h, const double *U, const double *p);
+BAMREX_API int bamrex_imex_get_state(bamrex_imex *h, double *U, double *p);
+/* cfl / max (|m_x|/dx + |m_y|/dy [+ |m_z|/dz]) / rho: estTimeStep for IMEX
+ * after the acoustic start-up (Source/AmrLevelAdv.cpp:417-468,
+ * Source/System/Euler/Euler.cpp:107-129). */
+BAMREX_API int bamrex_imex_est_time_step(bamrex_imex *h, double *dt);
+/* One step of size dt; *iters and *rel_res report the pressure solve.  A
+ * solve that does not reach its tolerance returns BAMREX_ERR_NOT_CONVERGED
+ * and leaves the state unchanged. */
+BAMREX_API int bamrex_imex_step(bamrex_imex *h, double dt, int *iters, double *rel_res);
+/* Solve the pressure equation with FGMRES and the learned preconditioner
+ * (bamrex_helmholtz_solve_learned, falling back to the plain solve) instead
+ * of BiCGStab + multigrid; net NULL restores the plain solve. */
+BAMREX_API int bamrex_imex_set_precnet(bamrex_imex *h, bamrex_precnet *net, int mode);
+/* The pressure operator of the step (its coefficients are those of the last
+ * step). */
+BAMREX_API bamrex_helmholtz *bamrex_imex_operator(bamrex_imex *h);
+/* Intermediate fields of the last step, for checking: *count receives the
+ * number of doubles (out NULL: size query).  UEX and ENTHALPY cover the
+ * valid box grown by one cell in every direction; KE, RHS and PRESSURE the
+ * valid box; FLUX_d the faces of direction d of the valid box ((D+2)
+ * components, one more entry along d). */
+enum {
+    BAMREX_IMEX_FIELD_UEX = 0,
+    BAMREX_IMEX_FIELD_ENTHALPY = 1,
+    BAMREX_IMEX_FIELD_KE = 2,
+    BAMREX_IMEX_FIELD_RHS = 3,
+    BAMREX_IMEX_FIELD_PRESSURE = 4,
+    BAMREX_IMEX_FIELD_FLUX_X = 5,
+    BAMREX_IMEX_FIELD_FLUX_Y = 6,
+    BAMREX_IMEX_FIELD_FLUX_Z = 7
+};
+BAMREX_API int bamrex_imex_field(bamrex_imex *h, int which, double *out, long long *count);
+/* Kernels launched by the step object (the pressure operator's excluded). */
+BAMREX_API long long bamrex_imex_launches(const bamrex_imex *h);
 
 #ifdef __cplusplus
 }

@@ -451,6 +451,12 @@ __global__ void copy_kernel(double* __restrict__ d, const double* __restrict__ s
         d[c] = s[c];
 }
 
+__global__ void fill_value_kernel(double* __restrict__ d, double v, long long n)
+{
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x)
+        d[c] = v;
+}
+
 __global__ void face_avg_kernel(const double* __restrict__ cc, double* __restrict__ f, int d, int n0, int n1, int n2,
                                 int periodic)
 {
@@ -966,9 +972,8 @@ extern "C" int bamrex_helmholtz_set_acoeffs(bamrex_helmholtz* H, const double* a
     if (alpha) {
         H_TRY(upload(H, L.a, alpha, (size_t)L.ncell));
     } else {
-        std::vector<double> v((size_t)L.ncell, alpha_const);
-        H_TRY(upload(H, L.a, v.data(), v.size()));
-        H_TRY(hck(H, cudaStreamSynchronize(H->stream), "sync"));
+        fill_value_kernel<<<grid_for(L.ncell), kThreads, 0, H->stream>>>(L.a, alpha_const, L.ncell);
+        H_TRY(hck(H, cudaGetLastError(), "a coefficients"));
     }
     H->coeffs_dirty = true;
     return BAMREX_OK;

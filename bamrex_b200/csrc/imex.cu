@@ -659,11 +659,16 @@ int step_impl(bamrex_imex* h, double dt, int* iters, double* rel_res)
     double rr = 0.0;
     if (h->net) {
         int plain = 0, fb = 0;
+        // one FGMRES(30) cycle with the network; the plain solve continues
+        // from its iterate if that does not reach the tolerance
         I_TRY(h, hck(bamrex_helmholtz_solve_learned(h->H, h->net, h->net_mode, h->p, h->rhs, h->tol_rel, h->tol_abs,
-                                                    h->max_iter, 30, &it, &plain, &rr, &fb)));
+                                                    30, 30, &it, &plain, &rr, &fb)));
         it += plain;
     } else {
-        I_TRY(h, hck(bamrex_helmholtz_solve(h->H, h->p, h->rhs, h->tol_rel, h->tol_abs, h->max_iter, 1, &it, &rr)));
+        // no CUDA graph: the scalars change every step (dt), so each step
+        // would capture a new one, and the solve needs few iterations from
+        // the previous pressure
+        I_TRY(h, hck(bamrex_helmholtz_solve(h->H, h->p, h->rhs, h->tol_rel, h->tol_abs, h->max_iter, 0, &it, &rr)));
     }
     if (iters) *iters = it;
     if (rel_res) *rel_res = rr;

@@ -123,3 +123,27 @@ def low_mach_pressure_problem(n=2048, seed=DEFAULT_SEED, log_sigma=1.0, corr_cel
     dt = cfl * dx / mach
     rhs = gaussian_random_field((n, n), 2 * corr_cells, seed + 1, rng)
     return dict(rho=rho[None], beta_cc=(1.0 / rho)[None], a=eps / (adiabatic - 1), B=dt * dt, rhs=rhs[None], dx=dx)
+
+
+def low_mach_state(n=2048, seed=DEFAULT_SEED, log_sigma=1.0, corr_cells=32, amplitude=0.01, adiabatic=1.4,
+                   epsilon=1.0):
+    """The 2D low-Mach IMEX state: density lognormal (log-sigma 1.0,
+    correlation length 32 cells), velocity the curl of a seeded stream
+    function (a Gaussian random field, central differences on the periodic
+    grid) scaled to peak speed `amplitude`, pressure 1/gamma, so the sound
+    speed is O(1) and the Mach number about `amplitude`.  Returns
+    (U (4, 1, n, n), p (1, n, n))."""
+    rng = np.random.default_rng(seed)
+    rho = np.exp(log_sigma * gaussian_random_field((n, n), corr_cells, seed, rng))
+    psi = gaussian_random_field((n, n), corr_cells, seed + 2, rng)
+    u = 0.5 * (np.roll(psi, -1, axis=0) - np.roll(psi, 1, axis=0))   # d psi / dy (rows are y)
+    v = -0.5 * (np.roll(psi, -1, axis=1) - np.roll(psi, 1, axis=1))  # -d psi / dx
+    scale = amplitude / np.max(np.sqrt(u * u + v * v))
+    u, v = u * scale, v * scale
+    p = np.full((n, n), 1.0 / adiabatic)
+    U = np.empty((4, 1, n, n))
+    U[0, 0] = rho
+    U[1, 0] = rho * u
+    U[2, 0] = rho * v
+    U[3, 0] = p / (adiabatic - 1) + 0.5 * epsilon * rho * (u * u + v * v)
+    return U, p[None]

@@ -283,6 +283,8 @@ def imex_pressure_run(n):
                          "fell_back": fb}
     best = min(("network+vcycle", "vcycle+network"), key=lambda k: learned[k]["ms"])
     h.close()
+    step = imex_step_run(n, net, {"network+vcycle": PRECOND_NETWORK_VCYCLE,
+                                  "vcycle+network": PRECOND_VCYCLE_NETWORK}[best])
     net.close()
     return {
         "workload": "2D IMEX pressure solve %dx%d, lognormal density (log-sigma 1, correlation 32 cells), beta = 1/rho, "
@@ -295,7 +297,47 @@ def imex_pressure_run(n):
                                                                         float(np.mean(losses[-10:]))]},
         "learned_over_plain_time": learned[best]["ms"] / plain_ms,
         "target_ratio": 0.5,
+        "imex_step": step,
     }
+
+
+def imex_step_run(n, net, mode, steps=5):
+    """Full first-order IMEX steps (bamrex_imex: Rusanov advection, enthalpy
+    from the previous pressure, explicit kinetic energy, pressure solve to
+    1e-8, fluxes, update) on the 2D low-Mach state at n^2, periodic, CFL 0.8
+    on the advective speed: ms per step with the plain and with the learned
+    pressure solve."""
+    import torch
+
+    import bamrex_b200 as bx
+    from bamrex_b200 import problems
+    from bamrex_b200.imex import Imex
+
+    U, p = problems.low_mach_state(n)
+    out = {"workload": "2D low-Mach IMEX step %dx%d: lognormal density (log-sigma 1, correlation 32 cells), "
+                       "velocity the curl of a random stream function at peak 0.01, p = 1/gamma, epsilon 1, periodic, "
+                       "Rusanov advection, enthalpy from the previous pressure, explicit kinetic energy, pressure solve "
+                       "to 1e-8, advective CFL 0.8" % (n, n), "steps": steps}
+    for name in ("plain", "learned"):
+        im = Imex(2, (n, n), [0.0, 0.0], [1.0, 1.0], bx.Parm(2, adiabatic=1.4, epsilon=1.0), bc_lo=[1, 1],
+                  bc_hi=[1, 1], cfl=0.8, tol_rel=1e-8)
+        if name == "learned":
+            im.set_precnet(net, mode)
+        im.set_state(U, p)
+        im.step(im.est_time_step())  # builds the solver's graphs
+        im.set_state(U, p)
+        its = []
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            it, rr = im.step(im.est_time_step())
+            its.append(it)
+        torch.cuda.synchronize()
+        ms = (time.perf_counter() - t0) * 1e3 / steps
+        out[name] = {"ms_per_step": ms, "solve_iterations": its, "last_rel_residual": rr}
+        im.close()
+    out["learned_over_plain_step_time"] = out["learned"]["ms_per_step"] / out["plain"]["ms_per_step"]
+    return out
 
 
 def _chop_drawn(boxes, choices, rng, D=3):

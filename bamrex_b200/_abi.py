@@ -136,6 +136,7 @@ class HelmholtzDesc(ctypes.Structure):
 IMEX_RUSANOV, IMEX_MUSCL_RUSANOV = 0, 1
 ENTH_REUSE_PRESSURE, ENTH_CONSERVATIVE, ENTH_CONSERVATIVE_EX = 0, 1, 2
 KE_CONSERVATIVE, KE_EX, KE_SPLIT = 0, 1, 2
+SP111, SSP222, SASSP322, SASSP332, SSP433 = range(5)
 (FIELD_UEX, FIELD_ENTHALPY, FIELD_KE, FIELD_RHS, FIELD_PRESSURE, FIELD_FLUX_X, FIELD_FLUX_Y,
  FIELD_FLUX_Z) = range(8)
 
@@ -156,6 +157,7 @@ class ImexDesc(ctypes.Structure):
         ("tol_rel", ctypes.c_double),
         ("tol_abs", ctypes.c_double),
         ("max_iter", ctypes.c_int),
+        ("tableau", ctypes.c_int),
     ]
 
 

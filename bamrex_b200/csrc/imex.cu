@@ -212,11 +212,12 @@ __device__ __forceinline__ double minmod(double a, double b)
     return (a > 0 && b > 0) ? fmin(a, b) : ((a < 0 && b < 0) ? fmax(a, b) : 0.0);
 }
 
-// MUSCL-Rusanov reconstruction on the valid box grown by two with the local
-// half step: SL[d] = U - h - hadv (F(U+h) - F(U-h)), SR[d] likewise
+// MUSCL-Rusanov reconstruction on the valid box grown by two, with the local
+// half step when local_step (SP111): SL[d] = U - h - hadv (F(U+h) - F(U-h)),
+// SR[d] likewise
 template <int D>
 __global__ void muscl_states_kernel(const double* __restrict__ U, Grid3 gU, double* __restrict__ SL,
-                                    double* __restrict__ SR, Grid3 g2, IK c)
+                                    double* __restrict__ SR, Grid3 g2, IK c, int local_step)
 {
     const long long n2 = g2.size();
     GRID_LOOP(t, n2)
@@ -239,15 +240,23 @@ __global__ void muscl_states_kernel(const double* __restrict__ U, Grid3 gU, doub
                 sl[n] = C[n] - hdelta;
                 sr[n] = C[n] + hdelta;
             }
-            double fl[D + 2], fr[D + 2];
-            adv_flux<D>(sl, d, c.eps, fl);
-            adv_flux<D>(sr, d, c.eps, fr);
             const long long base = (long long)d * (D + 2) * n2 + t;
+            if (local_step) {
+                double fl[D + 2], fr[D + 2];
+                adv_flux<D>(sl, d, c.eps, fl);
+                adv_flux<D>(sr, d, c.eps, fr);
 #pragma unroll
-            for (int n = 0; n < D + 2; ++n) {
-                const double upd = c.hadv[d] * (fr[n] - fl[n]);
-                SL[base + n * n2] = sl[n] - upd;
-                SR[base + n * n2] = sr[n] - upd;
+                for (int n = 0; n < D + 2; ++n) {
+                    const double upd = c.hadv[d] * (fr[n] - fl[n]);
+                    SL[base + n * n2] = sl[n] - upd;
+                    SR[base + n * n2] = sr[n] - upd;
+                }
+            } else {
+#pragma unroll
+                for (int n = 0; n < D + 2; ++n) {
+                    SL[base + n * n2] = sl[n];
+                    SR[base + n * n2] = sr[n];
+                }
             }
         }
     }
@@ -281,6 +290,7 @@ __global__ void muscl_faces_kernel(const double* __restrict__ SL, const double* 
 }
 
 // explicit update on the grown box: Uex = U - (sum_d dt/dx_d (F(f+1) - F(f)))
+// with U the state to update (the implicit-stage state)
 template <int D>
 __global__ void explicit_update_kernel(const double* __restrict__ U, Grid3 gU, const double* __restrict__ AF0,
                                        const double* __restrict__ AF1, const double* __restrict__ AF2, Grid3 gF0,
@@ -470,6 +480,118 @@ __global__ void update_kernel(double* __restrict__ U, Grid3 gU, const double* __
     }
 }
 
+// The two stage states (conservative_update with two outputs,
+// Source/Fluxes/Update.H:216-300): out = in - sum over the earlier stages i
+// of (c_i,x dFx_i + c_i,y dFy_i [+ c_i,z dFz_i]), with c = a_i dt idx for the
+// implicit (1) and explicit (2) rows of the tableau.
+struct StageArgs {
+    const double* F[3][3];  // [stage][direction]
+    Grid3 gF[3];
+    double c1[3][3], c2[3][3];  // [stage][direction]
+    int nprev;
+};
+
+template <int D>
+__global__ void stage_state_kernel(const double* __restrict__ U, Grid3 gU, double* __restrict__ O1,
+                                   double* __restrict__ O2, Grid3 gV, StageArgs a)
+{
+    GRID_LOOP(t, gV.size())
+    {
+        int i, j, k;
+        gV.cell(t, i, j, k);
+        const long long iu = gU.at(i, j, k);
+        for (int n = 0; n < D + 2; ++n) {
+            const double u = U[iu + n * gU.size()];
+            double o1 = u, o2 = u;
+            for (int s = 0; s < a.nprev; ++s) {
+                double acc1 = 0.0, acc2 = 0.0;
+#pragma unroll
+                for (int d = 0; d < D; ++d) {
+                    int p[3] = { i, j, k };
+                    p[d] += 1;
+                    const long long fs = a.gF[d].size();
+                    const double df = a.F[s][d][a.gF[d].at(p[0], p[1], p[2]) + n * fs] - a.F[s][d][a.gF[d].at(i, j, k) + n * fs];
+                    const double t1 = a.c1[s][d] * df, t2 = a.c2[s][d] * df;
+                    acc1 = d == 0 ? t1 : acc1 + t1;
+                    acc2 = d == 0 ? t2 : acc2 + t2;
+                }
+                o1 = o1 - acc1;
+                o2 = o2 - acc2;
+            }
+            O1[iu + n * gU.size()] = o1;
+            O2[iu + n * gU.size()] = o2;
+        }
+    }
+}
+
+// compute_pressure (Source/IMEX/IMEX_O1.cpp:292-378) for a later stage of the
+// linearised scheme, valid cells: split kinetic energy
+// (gamma-1)(E_new - eps/2 m_old . m_new / rho_old); explicit kinetic energy
+// (gamma-1)(E_new - eps/2 |m_ex|^2 / rho_new) with m_ex the old stage state
+// advanced by adt with its own advection fluxes AF; otherwise pressure(new).
+template <int D>
+__global__ void stage_pressure_kernel(const double* __restrict__ Unew, const double* __restrict__ Uold, Grid3 gU,
+                                      const double* __restrict__ AF0, const double* __restrict__ AF1,
+                                      const double* __restrict__ AF2, Grid3 gA0, Grid3 gA1, Grid3 gA2,
+                                      double* __restrict__ p, Grid3 gV, int ke_method, IK c)
+{
+    const double* AF[3] = { AF0, AF1, AF2 };
+    const Grid3 gA[3] = { gA0, gA1, gA2 };
+    GRID_LOOP(t, gV.size())
+    {
+        int i, j, k;
+        gV.cell(t, i, j, k);
+        const long long iu = gU.at(i, j, k);
+        double un[D + 2], uo[D + 2];
+        load<D>(Unew, iu, gU.size(), un);
+        load<D>(Uold, iu, gU.size(), uo);
+        double v;
+        if (ke_method == BAMREX_IMEX_KE_SPLIT) {
+            double dot = uo[1] * un[1];
+#pragma unroll
+            for (int d = 1; d < D; ++d) dot = dot + uo[1 + d] * un[1 + d];
+            v = (c.adia - 1) * (un[1 + D] - 0.5 * c.eps * dot / uo[0]);
+        } else if (ke_method == BAMREX_IMEX_KE_EX) {
+            double ex[D + 2];
+#pragma unroll
+            for (int n = 0; n < D + 2; ++n) {
+                double acc = 0.0;
+#pragma unroll
+                for (int d = 0; d < D; ++d) {
+                    int q[3] = { i, j, k };
+                    q[d] += 1;
+                    const long long fs = gA[d].size();
+                    const double term = c.dtdx[d] * (AF[d][gA[d].at(q[0], q[1], q[2]) + n * fs] - AF[d][gA[d].at(i, j, k) + n * fs]);
+                    acc = d == 0 ? term : acc + term;
+                }
+                ex[n] = uo[n] - acc;
+            }
+            double m2 = ex[1] * ex[1];
+#pragma unroll
+            for (int d = 1; d < D; ++d) m2 = m2 + ex[1 + d] * ex[1 + d];
+            v = (c.adia - 1) * (un[1 + D] - 0.5 * c.eps * m2 / un[0]);
+        } else {
+            v = (c.adia - 1) * (un[1 + D] - kinetic_energy<D>(un, c.eps));
+        }
+        p[t] = v;
+    }
+}
+
+// sum_fluxes (Source/IMEX/IMEX_RK.cpp:196-235): dst = F_0 b_0 + F_1 b_1 + ...
+__global__ void flux_sum_kernel(double* __restrict__ dst, const double* __restrict__ F0, const double* __restrict__ F1,
+                                const double* __restrict__ F2, const double* __restrict__ F3, double b0, double b1,
+                                double b2, double b3, int nstage, long long n)
+{
+    GRID_LOOP(t, n)
+    {
+        double v = F0[t] * b0;
+        if (nstage > 1) v += F1[t] * b1;
+        if (nstage > 2) v += F2[t] * b2;
+        if (nstage > 3) v += F3[t] * b3;
+        dst[t] = v;
+    }
+}
+
 // pressure(U) = (gamma - 1)(E - KE) on the valid cells (copy_pressure)
 template <int D>
 __global__ void pressure_kernel(const double* __restrict__ U, Grid3 gU, double* __restrict__ p, Grid3 gV, IK c)
@@ -536,6 +658,11 @@ struct bamrex_imex {
     double *af[3] = { nullptr, nullptr, nullptr }, *fl[3] = { nullptr, nullptr, nullptr };
     double *SL = nullptr, *SR = nullptr;
     double* stage = nullptr;  // the valid state, dense, on its way to or from the caller
+    // the tableau and the stage buffers
+    int tab = BAMREX_IMEX_SP111, S = 1;
+    double Ai[4][4] = {}, Ae[4][4] = {}, b[4] = {};
+    double *Uimp = nullptr, *Uexb[2] = { nullptr, nullptr };
+    double* sf[4][3] = {};  // stage fluxes [stage][direction]; stage 0 of SP111 is fl
     unsigned long long* speed = nullptr;
     long long launches = 0;
     std::string err;
@@ -600,21 +727,25 @@ int fill_ghosts(bamrex_imex* h, double* a, const Grid3& g, int ncomp, int G, boo
     return BAMREX_OK;
 }
 
+// compute_flux_imex_o1 (IMEX_O1.cpp:19-176): the fluxes of one implicit
+// stage of size adt into out[d], from the explicit-stage state Ue (whose
+// ghost cells are filled) applied to the implicit-stage state Ui; the
+// pressure (valid cells, h->p) is the solve's initial guess and result
 template <int D>
-int step_impl(bamrex_imex* h, double dt, int* iters, double* rel_res)
+int stage_flux(bamrex_imex* h, const double* Ui, const double* Ue, double adt, bool local_step, double* const* out,
+               int* iters, double* rel_res)
 {
-    const IK c = make_consts(h, dt);
+    const IK c = make_consts(h, adt);
     cudaStream_t s = h->stream;
     const int gV = grid_for(h->gV.size());
-    // state and pressure ghosts (the stage input after fill_consv_boundary;
-    // P_new after fill_pressure_boundary)
-    I_TRY(h, fill_ghosts(h, h->U, h->gU, h->NC, h->G, true));
+    // pressure ghosts (fill_pressure_boundary)
     to_grown_kernel<<<gV, kThreads, 0, s>>>(h->p, h->gV, h->pg, h->g1, 1);
     I_TRY(h, ilaunch(h, "IMEX pressure copy"));
     I_TRY(h, fill_ghosts(h, h->pg, h->g1, 1, 1, false));
     // 1. explicit advection on the grown box
     if (h->method == BAMREX_IMEX_MUSCL_RUSANOV) {
-        muscl_states_kernel<D><<<grid_for(h->g2.size()), kThreads, 0, s>>>(h->U, h->gU, h->SL, h->SR, h->g2, c);
+        muscl_states_kernel<D><<<grid_for(h->g2.size()), kThreads, 0, s>>>(Ue, h->gU, h->SL, h->SR, h->g2, c,
+                                                                           local_step ? 1 : 0);
         I_TRY(h, ilaunch(h, "IMEX MUSCL states"));
         for (int d = 0; d < D; ++d) {
             muscl_faces_kernel<D><<<grid_for(h->gA[d].size()), kThreads, 0, s>>>(h->SL, h->SR, h->g2, h->af[d], h->gA[d], d,
@@ -623,21 +754,20 @@ int step_impl(bamrex_imex* h, double dt, int* iters, double* rel_res)
         }
     } else {
         for (int d = 0; d < D; ++d) {
-            rusanov_faces_kernel<D><<<grid_for(h->gA[d].size()), kThreads, 0, s>>>(h->U, h->gU, h->af[d], h->gA[d], d,
-                                                                                    h->eps);
+            rusanov_faces_kernel<D><<<grid_for(h->gA[d].size()), kThreads, 0, s>>>(Ue, h->gU, h->af[d], h->gA[d], d, h->eps);
             I_TRY(h, ilaunch(h, "IMEX Rusanov faces"));
         }
     }
-    explicit_update_kernel<D><<<grid_for(h->g1.size()), kThreads, 0, s>>>(h->U, h->gU, h->af[0], h->af[1], h->af[2],
+    explicit_update_kernel<D><<<grid_for(h->g1.size()), kThreads, 0, s>>>(Ui, h->gU, h->af[0], h->af[1], h->af[2],
                                                                           h->gA[0], h->gA[1], h->gA[2], h->Uex, h->g1, c);
     I_TRY(h, ilaunch(h, "IMEX explicit update"));
     // 2. enthalpy, kinetic energy, velocity, pressure source
-    enthalpy_kernel<D><<<grid_for(h->g1.size()), kThreads, 0, s>>>(h->U, h->gU, h->Uex, h->g1, h->pg, h->enth, h->p,
-                                                                   h->gV, h->enth_method, c);
+    enthalpy_kernel<D><<<grid_for(h->g1.size()), kThreads, 0, s>>>(Ue, h->gU, h->Uex, h->g1, h->pg, h->enth, h->p, h->gV,
+                                                                   h->enth_method, c);
     I_TRY(h, ilaunch(h, "IMEX enthalpy"));
     const bool split = h->ke_method == BAMREX_IMEX_KE_SPLIT;
-    source_kernel<D><<<gV, kThreads, 0, s>>>(h->U, h->gU, h->Uex, h->g1, h->enth, h->ke, split ? h->vel : nullptr,
-                                             h->rhs, h->gV, h->ke_method, c);
+    source_kernel<D><<<gV, kThreads, 0, s>>>(Ue, h->gU, h->Uex, h->g1, h->enth, h->ke, split ? h->vel : nullptr, h->rhs,
+                                             h->gV, h->ke_method, c);
     I_TRY(h, ilaunch(h, "IMEX pressure source"));
     for (int d = 0; d < D; ++d) {
         bface_kernel<<<grid_for(h->gF[d].size()), kThreads, 0, s>>>(h->enth, h->g1, h->bf[d], h->gF[d], d);
@@ -651,7 +781,7 @@ int step_impl(bamrex_imex* h, double dt, int* iters, double* rel_res)
         }
         return (int)BAMREX_OK;
     };
-    I_TRY(h, hck(bamrex_helmholtz_set_scalars(h->H, 1.0, dt * dt, split ? -0.5 * h->eps * dt : 0.0)));
+    I_TRY(h, hck(bamrex_helmholtz_set_scalars(h->H, 1.0, adt * adt, split ? -0.5 * h->eps * adt : 0.0)));
     I_TRY(h, hck(bamrex_helmholtz_set_acoeffs(h->H, nullptr, h->eps / (h->adia - 1))));
     I_TRY(h, hck(bamrex_helmholtz_set_bcoeffs(h->H, h->bf[0], h->bf[1], D > 2 ? h->bf[2] : nullptr)));
     I_TRY(h, hck(bamrex_helmholtz_set_ccoeffs(h->H, split ? h->vel : nullptr)));
@@ -670,23 +800,108 @@ int step_impl(bamrex_imex* h, double dt, int* iters, double* rel_res)
         // the previous pressure
         I_TRY(h, hck(bamrex_helmholtz_solve(h->H, h->p, h->rhs, h->tol_rel, h->tol_abs, h->max_iter, 0, &it, &rr)));
     }
-    if (iters) *iters = it;
-    if (rel_res) *rel_res = rr;
+    *iters = it;
+    *rel_res = rr;
     if (!std::isfinite(rr)) return ifail(h, BAMREX_ERR_NAN, "the pressure solve produced a non-finite residual");
     // MLMG aborts when it cannot reach the tolerance; here the step stops
     // before the update (the state is unchanged, the pressure holds the
     // solver's last iterate)
     if (!(rr <= h->tol_rel) && it >= h->max_iter)
         return ifail(h, BAMREX_ERR_NOT_CONVERGED, "the pressure solve did not reach its tolerance");
-    // 4. fluxes and the conservative update
+    // 4. the stage fluxes
     to_grown_kernel<<<gV, kThreads, 0, s>>>(h->p, h->gV, h->pg, h->g1, 1);
     I_TRY(h, ilaunch(h, "IMEX pressure copy"));
     I_TRY(h, fill_ghosts(h, h->pg, h->g1, 1, 1, false));
     for (int d = 0; d < D; ++d) {
-        flux_kernel<D><<<grid_for(h->gF[d].size()), kThreads, 0, s>>>(h->af[d], h->gA[d], h->Uex, h->enth, h->pg,
-                                                                       h->g1, h->fl[d], h->gF[d], d, c);
+        flux_kernel<D><<<grid_for(h->gF[d].size()), kThreads, 0, s>>>(h->af[d], h->gA[d], h->Uex, h->enth, h->pg, h->g1,
+                                                                       out[d], h->gF[d], d, c);
         I_TRY(h, ilaunch(h, "IMEX fluxes"));
     }
+    return BAMREX_OK;
+}
+
+// advance_imex_rk (Source/IMEX/IMEX_RK.cpp:23-86): per stage the two stage
+// states from the earlier stage fluxes, the stage pressure (later stages),
+// the stage fluxes; then the b-weighted flux sum and the conservative update
+template <int D>
+int step_impl(bamrex_imex* h, double dt, int* iters, double* rel_res)
+{
+    cudaStream_t s = h->stream;
+    const int gV = grid_for(h->gV.size());
+    // the step input with its ghost cells (fill_consv_boundary); it stays
+    // unchanged until the final update and is both stage states of stage 0
+    I_TRY(h, fill_ghosts(h, h->U, h->gU, h->NC, h->G, true));
+    int it_total = 0;
+    double rr_max = 0.0;
+    const double* Ue_prev = nullptr;
+    for (int st = 0; st < h->S; ++st) {
+        const double* Ui = h->U;
+        const double* Ue = h->U;
+        if (st > 0) {
+            StageArgs a;
+            std::memset(&a, 0, sizeof(a));
+            a.nprev = st;
+            for (int q = 0; q < st; ++q)
+                for (int d = 0; d < D; ++d) {
+                    a.F[q][d] = h->sf[q][d];
+                    a.c1[q][d] = (h->Ai[st][q] * dt) * h->idx[d];
+                    a.c2[q][d] = (h->Ae[st][q] * dt) * h->idx[d];
+                }
+            for (int d = 0; d < D; ++d) a.gF[d] = h->gF[d];
+            double* Ue_new = h->Uexb[st % 2];
+            stage_state_kernel<D><<<gV, kThreads, 0, s>>>(h->U, h->gU, h->Uimp, Ue_new, h->gV, a);
+            I_TRY(h, ilaunch(h, "IMEX stage states"));
+            I_TRY(h, fill_ghosts(h, h->Uimp, h->gU, h->NC, h->G, true));
+            I_TRY(h, fill_ghosts(h, Ue_new, h->gU, h->NC, h->G, true));
+            Ui = h->Uimp;
+            Ue = Ue_new;
+        }
+        const double adt = h->Ai[st][st] * dt;
+        if (st > 0) {
+            // compute_pressure from this stage's and the previous stage's
+            // explicit states
+            const IK c = make_consts(h, adt);
+            if (h->ke_method == BAMREX_IMEX_KE_EX) {
+                if (h->method == BAMREX_IMEX_MUSCL_RUSANOV) {
+                    muscl_states_kernel<D><<<grid_for(h->g2.size()), kThreads, 0, s>>>(Ue_prev, h->gU, h->SL, h->SR,
+                                                                                       h->g2, c, 0);
+                    I_TRY(h, ilaunch(h, "IMEX MUSCL states"));
+                    for (int d = 0; d < D; ++d) {
+                        muscl_faces_kernel<D><<<grid_for(h->gA[d].size()), kThreads, 0, s>>>(h->SL, h->SR, h->g2, h->af[d],
+                                                                                              h->gA[d], d, h->eps);
+                        I_TRY(h, ilaunch(h, "IMEX MUSCL-Rusanov faces"));
+                    }
+                } else {
+                    for (int d = 0; d < D; ++d) {
+                        rusanov_faces_kernel<D><<<grid_for(h->gA[d].size()), kThreads, 0, s>>>(Ue_prev, h->gU, h->af[d],
+                                                                                                h->gA[d], d, h->eps);
+                        I_TRY(h, ilaunch(h, "IMEX Rusanov faces"));
+                    }
+                }
+            }
+            stage_pressure_kernel<D><<<gV, kThreads, 0, s>>>(Ue, Ue_prev, h->gU, h->af[0], h->af[1], h->af[2], h->gA[0],
+                                                             h->gA[1], h->gA[2], h->p, h->gV, h->ke_method, c);
+            I_TRY(h, ilaunch(h, "IMEX stage pressure"));
+        }
+        int it = 0;
+        double rr = 0.0;
+        I_TRY(h, stage_flux<D>(h, Ui, Ue, adt, h->tab == BAMREX_IMEX_SP111, h->sf[st], &it, &rr));
+        it_total += it;
+        rr_max = std::max(rr_max, rr);
+        Ue_prev = Ue;
+    }
+    if (iters) *iters = it_total;
+    if (rel_res) *rel_res = rr_max;
+    if (h->S > 1) {
+        for (int d = 0; d < D; ++d) {
+            const long long nf = (long long)h->NC * h->gF[d].size();
+            flux_sum_kernel<<<grid_for(nf), kThreads, 0, s>>>(h->fl[d], h->sf[0][d], h->sf[1][d], h->S > 2 ? h->sf[2][d] : nullptr,
+                                                              h->S > 3 ? h->sf[3][d] : nullptr, h->b[0], h->b[1], h->b[2],
+                                                              h->b[3], h->S, nf);
+            I_TRY(h, ilaunch(h, "IMEX flux sum"));
+        }
+    }
+    const IK c = make_consts(h, dt);
     update_kernel<D><<<gV, kThreads, 0, s>>>(h->U, h->gU, h->fl[0], h->fl[1], h->fl[2], h->gF[0], h->gF[1], h->gF[2],
                                              h->gV, c);
     I_TRY(h, ilaunch(h, "IMEX update"));
@@ -745,6 +960,67 @@ extern "C" int bamrex_imex_create(bamrex_imex** out, const bamrex_imex_desc* d, 
     h->method = d->advection_flux;
     h->enth_method = d->enthalpy_method;
     h->ke_method = d->ke_method;
+    // IMEXButcherTableau (Source/IMEX/ButcherTableau.cpp:5-98)
+    h->tab = d->tableau;
+    switch (h->tab) {
+    case BAMREX_IMEX_SP111:
+        h->S = 1;
+        h->Ai[0][0] = 1;
+        h->b[0] = 1;
+        break;
+    case BAMREX_IMEX_SSP222: {
+        h->S = 2;
+        const double al = 1 - 1 / std::sqrt(2.0);
+        h->Ai[0][0] = al;
+        h->Ai[1][0] = 1 - 2 * al;
+        h->Ai[1][1] = al;
+        h->Ae[1][0] = 1;
+        h->b[0] = h->b[1] = 0.5;
+        break;
+    }
+    case BAMREX_IMEX_SASSP322:
+        h->S = 3;
+        h->Ai[0][0] = 0.5;
+        h->Ai[1][0] = -0.5;
+        h->Ai[1][1] = 0.5;
+        h->Ai[2][1] = 0.5;
+        h->Ai[2][2] = 0.5;
+        h->Ae[2][1] = 1;
+        h->b[1] = h->b[2] = 0.5;
+        break;
+    case BAMREX_IMEX_SASSP332:
+        h->S = 3;
+        h->Ai[0][0] = 0.25;
+        h->Ai[1][1] = 0.25;
+        h->Ai[2][0] = h->Ai[2][1] = h->Ai[2][2] = (double)1 / 3;
+        h->Ae[1][0] = 0.5;
+        h->Ae[2][0] = h->Ae[2][1] = 0.5;
+        h->b[0] = h->b[1] = h->b[2] = (double)1 / 3;
+        break;
+    case BAMREX_IMEX_SSP433: {
+        h->S = 4;
+        const double al = 0.24169426078821, be = 0.06042356519705, et = 0.12915286960590;
+        h->Ai[0][0] = al;
+        h->Ai[1][0] = -al;
+        h->Ai[1][1] = al;
+        h->Ai[2][1] = 1 - al;
+        h->Ai[2][2] = al;
+        h->Ai[3][0] = be;
+        h->Ai[3][1] = et;
+        h->Ai[3][2] = 0.5 - be - et - al;
+        h->Ai[3][3] = al;
+        h->Ae[2][1] = 1;
+        h->Ae[3][1] = 0.25;
+        h->Ae[3][2] = 0.25;
+        h->b[1] = (double)1 / 6;
+        h->b[2] = (double)1 / 6;
+        h->b[3] = (double)2 / 3;
+        break;
+    }
+    default:
+        if (h->own_stream) cudaStreamDestroy(h->stream);
+        return fail(BAMREX_ERR_ARG, "unknown Butcher tableau");
+    }
     if (stream) {
         h->stream = (cudaStream_t)stream;
     } else {
@@ -777,6 +1053,14 @@ extern "C" int bamrex_imex_create(bamrex_imex** out, const bamrex_imex_desc* d, 
         oAf[q] = take(NC * h->gA[q].size());
         oFl[q] = take(NC * h->gF[q].size());
     }
+    size_t oImp = 0, oExb[2] = { 0, 0 }, oSf[4][3] = {};
+    if (h->S > 1) {
+        oImp = take(NC * h->gU.size());
+        oExb[0] = take(NC * h->gU.size());
+        oExb[1] = take(NC * h->gU.size());
+        for (int st = 0; st < h->S; ++st)
+            for (int q = 0; q < D; ++q) oSf[st][q] = take(NC * h->gF[q].size());
+    }
     size_t oSL = 0, oSR = 0;
     if (G == 3) {
         oSL = take((long long)D * NC * h->g2.size());
@@ -806,6 +1090,15 @@ extern "C" int bamrex_imex_create(bamrex_imex** out, const bamrex_imex_desc* d, 
     if (G == 3) {
         h->SL = (double*)(A + oSL);
         h->SR = (double*)(A + oSR);
+    }
+    if (h->S > 1) {
+        h->Uimp = (double*)(A + oImp);
+        h->Uexb[0] = (double*)(A + oExb[0]);
+        h->Uexb[1] = (double*)(A + oExb[1]);
+        for (int st = 0; st < h->S; ++st)
+            for (int q = 0; q < D; ++q) h->sf[st][q] = (double*)(A + oSf[st][q]);
+    } else {
+        for (int q = 0; q < D; ++q) h->sf[0][q] = h->fl[q];
     }
     h->stage = (double*)(A + oSt);
     h->speed = (unsigned long long*)(A + oSp);

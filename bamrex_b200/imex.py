@@ -21,7 +21,7 @@ from .level import Parm
 class Imex:
     def __init__(self, spacedim, n, prob_lo, prob_hi, parm: Parm, bc_lo=None, bc_hi=None,
                  advection_flux=IMEX_RUSANOV, enthalpy_method=ENTH_REUSE_PRESSURE, ke_method=KE_EX, cfl=0.5,
-                 tol_rel=0.0, tol_abs=0.0, max_iter=0, stream=None):
+                 tol_rel=0.0, tol_abs=0.0, max_iter=0, tableau=0, stream=None):
         self.D = spacedim
         self.NC = spacedim + 2
         self.n = tuple(n) + (1,) * (3 - len(n))
@@ -35,7 +35,7 @@ class Imex:
             d.bc_hi[q] = int(bc_hi[q]) if bc_hi is not None and q < len(bc_hi) else 0
         d.parm = parm.to_c()
         d.advection_flux, d.enthalpy_method, d.ke_method = advection_flux, enthalpy_method, ke_method
-        d.cfl, d.tol_rel, d.tol_abs, d.max_iter = cfl, tol_rel, tol_abs, max_iter
+        d.cfl, d.tol_rel, d.tol_abs, d.max_iter, d.tableau = cfl, tol_rel, tol_abs, max_iter, tableau
         self.dx = [(d.prob_hi[q] - d.prob_lo[q]) / self.n[q] for q in range(spacedim)]
         self._h = ctypes.c_void_p()
         st = ctypes.c_void_p(stream.cuda_stream) if stream is not None else None

@@ -585,9 +585,9 @@ BAMREX_API int bamrex_helmholtz_solve_learned(bamrex_helmholtz *h, bamrex_precne
                                               int *fell_back);
 
 /* ------------------------------------------------------------------ */
-/* The first-order IMEX step (advance_imex_rk with the SP111 tableau and   */
-/* the linearised pressure equation, Source/IMEX/IMEX_RK.cpp:23-86,        */
-/* Source/IMEX/IMEX_O1.cpp:19-176) on one box covering the domain          */
+/* The IMEX step (advance_imex_rk with the linearised pressure equation,   */
+/* Source/IMEX/IMEX_RK.cpp:23-86, Source/IMEX/IMEX_O1.cpp:19-176) on one    */
+/* box covering the domain                                                  */
 /* ------------------------------------------------------------------ */
 
 typedef struct bamrex_imex bamrex_imex;
@@ -600,6 +600,14 @@ enum {
     BAMREX_IMEX_ENTH_CONSERVATIVE_EX = 2
 };
 enum { BAMREX_IMEX_KE_CONSERVATIVE = 0, BAMREX_IMEX_KE_EX = 1, BAMREX_IMEX_KE_SPLIT = 2 };
+/* imex.butcher_tableau (IMEXButcherTableau::TableauType, ButcherTableau.cpp) */
+enum {
+    BAMREX_IMEX_SP111 = 0,
+    BAMREX_IMEX_SSP222 = 1,
+    BAMREX_IMEX_SASSP322 = 2,
+    BAMREX_IMEX_SASSP332 = 3,
+    BAMREX_IMEX_SSP433 = 4
+};
 
 typedef struct bamrex_imex_desc {
     int spacedim;            /* 2 or 3 */
@@ -615,6 +623,7 @@ typedef struct bamrex_imex_desc {
     double cfl;              /* adv.cfl (0 = 0.5) */
     double tol_rel, tol_abs; /* pressure solve; 0 = 1e-12 / 1e-15 as solve_pressure */
     int max_iter;            /* 0 = 1000 as solve_pressure */
+    int tableau;             /* BAMREX_IMEX_SP111 ... SSP433 */
 } bamrex_imex_desc;
 
 /* Allocates the state (with ghost cells), the intermediate fields and the
@@ -632,8 +641,9 @@ BAMREX_API int bamrex_imex_get_state(bamrex_imex *h, double *U, double *p);
  * after the acoustic start-up (Source/AmrLevelAdv.cpp:417-468,
  * Source/System/Euler/Euler.cpp:107-129). */
 BAMREX_API int bamrex_imex_est_time_step(bamrex_imex *h, double *dt);
-/* One step of size dt; *iters and *rel_res report the pressure solve.  A
- * solve that does not reach its tolerance returns BAMREX_ERR_NOT_CONVERGED
+/* One step of size dt (every stage of the tableau); *iters and *rel_res
+ * report the pressure solves (total iterations, largest relative residual).
+ * A solve that does not reach its tolerance returns BAMREX_ERR_NOT_CONVERGED
  * and leaves the state unchanged. */
 BAMREX_API int bamrex_imex_step(bamrex_imex *h, double dt, int *iters, double *rel_res);
 /* Solve the pressure equation with one FGMRES(30) cycle preconditioned by
@@ -644,7 +654,8 @@ BAMREX_API int bamrex_imex_set_precnet(bamrex_imex *h, bamrex_precnet *net, int 
 /* The pressure operator of the step (its coefficients are those of the last
  * step). */
 BAMREX_API bamrex_helmholtz *bamrex_imex_operator(bamrex_imex *h);
-/* Intermediate fields of the last step, for checking: *count receives the
+/* Intermediate fields of the last stage, for checking (FLUX_d is the
+ * tableau-weighted sum of the stage fluxes): *count receives the
  * number of doubles (out NULL: size query).  UEX and ENTHALPY cover the
  * valid box grown by one cell in every direction; KE, RHS and PRESSURE the
  * valid box; FLUX_d the faces of direction d of the valid box ((D+2)

@@ -1,8 +1,10 @@
-"""TEST INFRASTRUCTURE ONLY -- numpy restatement of the first-order IMEX step.
+"""TEST INFRASTRUCTURE ONLY -- numpy restatement of the IMEX step.
 
-One SP111 step of advance_imex_rk (Source/IMEX/IMEX_RK.cpp:23-86: one implicit
-stage, a_11 = b_1 = 1, so the stage input is the step input) with the
-linearised pressure equation:
+advance_imex_rk (Source/IMEX/IMEX_RK.cpp:23-86, 196-235) with the tableaux of
+Source/IMEX/ButcherTableau.cpp:5-98 (stage states by the two-output
+conservative_update, Source/Fluxes/Update.H:216-300; later stages start from
+compute_pressure, Source/IMEX/IMEX_O1.cpp:292-378) and, per stage, the
+linearised pressure equation of compute_flux_imex_o1:
   * explicit advection: advance_rusanov_adv and advance_MUSCL_rusanov_adv
     with its local half step (Source/IMEX/IMEX_Fluxes.cpp:11-323), adv_flux
     and kinetic_energy (Source/IMEX_K/euler_K.H), minmod (Limiters.H:76-81);
@@ -121,10 +123,11 @@ def minmod(a, b):
     return np.where((a > 0) & (b > 0), np.fmin(a, b), np.where((a < 0) & (b < 0), np.fmax(a, b), 0.0))
 
 
-def explicit_update(Upad, G, D, n, dx, dt, eps, method, local_time_step=True):
-    """State advanced by the advection fluxes on the valid box grown by one
-    (Uex, padded by 1) and the advection fluxes on the faces of that box
-    (list over d of arrays (NC, ...) with one more face along d)."""
+def explicit_update(Upad, G, D, n, dx, dt, eps, method, local_time_step=True, Upad_update=None):
+    """State advanced by the advection fluxes of Upad on the valid box grown
+    by one (Uex, padded by 1; the update applies to Upad_update, default
+    Upad) and the advection fluxes on the faces of that box (list over d of
+    arrays (NC, ...) with one more face along d)."""
     grid = Grid(D, n, G)
     lo1, hi1 = _rng(D, n, 1)
     NC = D + 2
@@ -170,7 +173,7 @@ def explicit_update(Upad, G, D, n, dx, dt, eps, method, local_time_step=True):
             umax = np.maximum(np.fabs(L_i[1 + d] / L_i[0]), np.fabs(R_im[1 + d] / R_im[0]))
             faces.append(0.5 * ((FL + FR) - umax * (L_i - R_im)))
     # update on the grown box
-    U1 = Upad[(slice(None),) + grid.sl(lo1, hi1)]
+    U1 = (Upad if Upad_update is None else Upad_update)[(slice(None),) + grid.sl(lo1, hi1)]
     acc = None
     for d in range(D):
         F = faces[d]
@@ -185,22 +188,27 @@ def explicit_update(Upad, G, D, n, dx, dt, eps, method, local_time_step=True):
     return Uex, faces
 
 
-def imex_step(U, p, D, dx, dt, parm_gamma, eps, bc_lo, bc_hi, method=RUSANOV, enthalpy_method=REUSE_PRESSURE,
-              ke_method=KE_EX, p_new=None, tol_rel=1e-14, max_iter=400):
-    """One first-order IMEX step.  U: valid state (NC, nz, ny, nx); p: valid
-    pressure (nz, ny, nx).  p_new: use this pressure instead of solving
-    (to compare the steps around the solve bit for bit).  Returns a dict of
-    the new state, the solved pressure, the fluxes on the valid faces and
-    the intermediate fields."""
+def stage_flux(Uimp, Uexp, p, D, dx, dt, parm_gamma, eps, bc_lo, bc_hi, method=RUSANOV,
+               enthalpy_method=REUSE_PRESSURE, ke_method=KE_EX, local_time_step=True, p_new=None, tol_rel=1e-14,
+               max_iter=400):
+    """compute_flux_imex_o1 (Source/IMEX/IMEX_O1.cpp:19-176): fluxes of one
+    implicit stage of size dt from the explicit-stage state Uexp (advection
+    fluxes, enthalpy, kinetic energy, velocity) applied to Uimp.  U*: valid
+    states (NC, nz, ny, nx); p: valid pressure (nz, ny, nx).  p_new: use
+    this pressure instead of solving (to compare the steps around the solve
+    bit for bit).  Returns a dict of the solved pressure, the fluxes on the
+    valid faces and the intermediate fields."""
     NC = D + 2
+    U = Uexp
     n = [U.shape[3], U.shape[2], U.shape[1]]
     G = 3 if method == MUSCL_RUSANOV else 2
     adia = parm_gamma
     Upad = fill(U, D, G, bc_lo, bc_hi)
+    Upad_imp = fill(Uimp, D, G, bc_lo, bc_hi)
     grid = Grid(D, n, G)
     lo0, hi0 = _rng(D, n, 0)
     lo1, hi1 = _rng(D, n, 1)
-    Uex, afaces = explicit_update(Upad, G, D, n, dx, dt, eps, method)   # Uex padded by 1
+    Uex, afaces = explicit_update(Upad, G, D, n, dx, dt, eps, method, local_time_step, Upad_imp)  # padded by 1
     g1 = Grid(D, n, 1)
     U_in1 = Upad[(slice(None),) + grid.sl(lo1, hi1)]
     ppad = fill(p, D, 1, bc_lo, bc_hi, vector=False)
@@ -274,18 +282,126 @@ def imex_step(U, p, D, dx, dt, parm_gamma, eps, bc_lo, bc_hi, method=RUSANOV, en
         F[1 + d] = F[1 + d] + heps * (pi + pm)
         F[1 + D] = F[1 + D] + (0.5 * (hi_ * mi + hm * mm) - hdtdxe[d] * ((hi_ + hm) * (pi - pm)))
         fluxes.append(F)
-    # conservative update
+    return {"p": p_new, "fluxes": fluxes, "Uex": Uex, "enth": enth, "ke": ke, "rhs": rhs, "op": op,
+            "bfaces": bfaces}
+
+
+def _fdiff(F, d):
+    nf = F.shape[_ax(d)]
+    s_hi = [slice(None)] * 4
+    s_lo = [slice(None)] * 4
+    s_hi[_ax(d)] = slice(1, nf)
+    s_lo[_ax(d)] = slice(0, nf - 1)
+    return F[tuple(s_hi)] - F[tuple(s_lo)]
+
+
+def conservative_update(U, fluxes, D, dx, dt):
+    """Update.H:99-130: out = in - dt idx_x dFx - dt idx_y dFy [- ...]."""
     out = U.copy()
     for d in range(D):
-        F = fluxes[d]
-        nf = F.shape[_ax(d)]
-        s_hi = [slice(None)] * 4
-        s_lo = [slice(None)] * 4
-        s_hi[_ax(d)] = slice(1, nf)
-        s_lo[_ax(d)] = slice(0, nf - 1)
-        out = out - (dt * (1.0 / dx[d])) * (F[tuple(s_hi)] - F[tuple(s_lo)])
-    return {"U": out, "p": p_new, "fluxes": fluxes, "Uex": Uex, "enth": enth, "ke": ke, "rhs": rhs, "op": op,
-            "bfaces": bfaces}
+        out = out - (dt * (1.0 / dx[d])) * _fdiff(fluxes[d], d)
+    return out
+
+
+def imex_step(U, p, D, dx, dt, parm_gamma, eps, bc_lo, bc_hi, method=RUSANOV, enthalpy_method=REUSE_PRESSURE,
+              ke_method=KE_EX, p_new=None, tol_rel=1e-14, max_iter=400):
+    """One SP111 step: stage_flux with Uimp = Uexp = U and dt, then the
+    conservative update.  Returns stage_flux's dict plus the new state "U"."""
+    r = stage_flux(U, U, p, D, dx, dt, parm_gamma, eps, bc_lo, bc_hi, method, enthalpy_method, ke_method, True,
+                   p_new, tol_rel, max_iter)
+    r["U"] = conservative_update(U, r["fluxes"], D, dx, dt)
+    return r
+
+
+# IMEXButcherTableau (Source/IMEX/ButcherTableau.cpp:5-98): A_imp, A_exp, b
+def tableau(name):
+    if name == "SP111":
+        return [[1.0]], [[0.0]], [1.0]
+    if name == "SSP222":
+        a = 1 - 1 / np.sqrt(2)
+        return [[a, 0.0], [1 - 2 * a, a]], [[0.0, 0.0], [1.0, 0.0]], [0.5, 0.5]
+    if name == "SASSP322":
+        return ([[0.5, 0, 0], [-0.5, 0.5, 0], [0, 0.5, 0.5]], [[0, 0, 0], [0, 0, 0], [0, 1, 0]], [0, 0.5, 0.5])
+    if name == "SASSP332":
+        return ([[0.25, 0, 0], [0, 0.25, 0], [1 / 3, 1 / 3, 1 / 3]], [[0, 0, 0], [0.5, 0, 0], [0.5, 0.5, 0]],
+                [1 / 3, 1 / 3, 1 / 3])
+    if name == "SSP433":
+        al, be, et = 0.24169426078821, 0.06042356519705, 0.12915286960590
+        return ([[al, 0, 0, 0], [-al, al, 0, 0], [0, 1 - al, al, 0], [be, et, 0.5 - be - et - al, al]],
+                [[0, 0, 0, 0], [0, 0, 0, 0], [0, 1, 0, 0], [0, 0.25, 0.25, 0]], [0, 1 / 6, 1 / 6, 2 / 3])
+    raise ValueError(name)
+
+
+def stage_states(U, F, dts_imp, dts_exp, D, dx):
+    """conservative_update with two outputs (Update.H:216-300): each
+    output = in - sum over the earlier stages of (dt_i idx_x dFx + dt_i
+    idx_y dFy [+ ...])."""
+    outs = []
+    for dts in (dts_imp, dts_exp):
+        out = U.copy()
+        for i, Fi in enumerate(F):
+            acc = None
+            for d in range(D):
+                t = (dts[i] * (1.0 / dx[d])) * _fdiff(Fi[d], d)
+                acc = t if acc is None else acc + t
+            out = out - acc
+        outs.append(out)
+    return outs
+
+
+def stage_pressure(Unew, Uold, D, dx, adt, adia, eps, bc_lo, bc_hi, method, ke_method):
+    """compute_pressure (IMEX_O1.cpp:292-378) for the linearised scheme on
+    the valid cells."""
+    if ke_method == KE_SPLIT:
+        dot = Uold[1] * Unew[1]
+        for d in range(1, D):
+            dot = dot + Uold[1 + d] * Unew[1 + d]
+        return (adia - 1) * (Unew[1 + D] - 0.5 * eps * dot / Uold[0])
+    if ke_method == KE_EX:
+        n = [Unew.shape[3], Unew.shape[2], Unew.shape[1]]
+        G = 3 if method == MUSCL_RUSANOV else 2
+        Op = fill(Uold, D, G, bc_lo, bc_hi)
+        ex, _ = explicit_update(Op, G, D, n, dx, adt, eps, method, local_time_step=False)
+        ex = ex[(slice(None),) + Grid(D, n, 1).sl(*_rng(D, n, 0))]
+        m2 = ex[1] * ex[1]
+        for d in range(1, D):
+            m2 = m2 + ex[1 + d] * ex[1 + d]
+        return (adia - 1) * (Unew[1 + D] - 0.5 * eps * m2 / Unew[0])
+    return pressure_of(Unew, D, adia, eps)
+
+
+def imex_rk_step(U, p, D, dx, dt, parm_gamma, eps, bc_lo, bc_hi, method=RUSANOV, enthalpy_method=REUSE_PRESSURE,
+                 ke_method=KE_EX, name="SP111", p_stages=None, tol_rel=1e-14, max_iter=400):
+    """advance_imex_rk (Source/IMEX/IMEX_RK.cpp:23-86) with the named
+    tableau: per stage the two stage states, the stage pressure (stages after
+    the first), the stage fluxes; then the b-weighted flux sum (sum_fluxes)
+    and the conservative update.  p_stages: the pressure of each stage's
+    solve to use instead of solving."""
+    Ai, Ae, b = tableau(name)
+    s = len(b)
+    F, stages = [], []
+    Uexp_prev = None
+    for st in range(s):
+        dti = [Ai[st][i] * dt for i in range(s)]
+        dte = [Ae[st][i] * dt for i in range(s)]
+        Uimp, Uexp = stage_states(U, F, dti, dte, D, dx)
+        adt = Ai[st][st] * dt
+        if st > 0:
+            p = stage_pressure(Uexp, Uexp_prev, D, dx, adt, parm_gamma, eps, bc_lo, bc_hi, method, ke_method)
+        r = stage_flux(Uimp, Uexp, p, D, dx, adt, parm_gamma, eps, bc_lo, bc_hi, method, enthalpy_method, ke_method,
+                       name == "SP111", None if p_stages is None else p_stages[st], tol_rel, max_iter)
+        r["Uimp"], r["Uexp"], r["p_in"] = Uimp, Uexp, p
+        stages.append(r)
+        p = r["p"]
+        F.append(r["fluxes"])
+        Uexp_prev = Uexp
+    fsum = []
+    for d in range(D):
+        acc = F[0][d] * b[0]
+        for i in range(1, s):
+            acc = acc + F[i][d] * b[i]
+        fsum.append(acc)
+    return {"U": conservative_update(U, fsum, D, dx, dt), "p": p, "fluxes": fsum, "stages": stages}
 
 
 def pressure_of(U, D, adia, eps):

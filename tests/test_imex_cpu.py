@@ -105,3 +105,53 @@ def test_uniform_state_is_steady():
     for bc in (0, 1, 2):
         r = IO.imex_step(U, p, D, [1.0 / n] * D, 0.01, ADIA, EPS, [bc] * 3, [bc] * 3)
         np.testing.assert_allclose(r["U"], U, rtol=1e-14, atol=1e-14)
+
+
+TABLEAUX = ["SP111", "SSP222", "SASSP322", "SASSP332", "SSP433"]
+
+
+def test_rk_driver_with_sp111_is_the_first_order_step():
+    U, p = _smooth_state(2, 16, 3)
+    a = IO.imex_step(U, p, 2, [1 / 16] * 2, 0.01, ADIA, EPS, [1] * 3, [1] * 3, IO.MUSCL_RUSANOV, IO.REUSE_PRESSURE,
+                     IO.KE_SPLIT)
+    b = IO.imex_rk_step(U, p, 2, [1 / 16] * 2, 0.01, ADIA, EPS, [1] * 3, [1] * 3, IO.MUSCL_RUSANOV,
+                        IO.REUSE_PRESSURE, IO.KE_SPLIT, "SP111", p_stages=[a["p"]])
+    np.testing.assert_array_equal(a["U"], b["U"])
+
+
+def test_tableaux_rows():
+    """The tableaux of ButcherTableau.cpp (checked as Tests/
+    IMEXButcherTableaux01.cpp does): square s x s matrices, explicit part
+    strictly lower triangular, b summing to one."""
+    for name in TABLEAUX:
+        Ai, Ae, b = IO.tableau(name)
+        s = len(b)
+        assert len(Ai) == len(Ae) == s and all(len(r) == s for r in Ai + Ae)
+        assert all(Ae[i][j] == 0 for i in range(s) for j in range(i, s))
+        assert abs(sum(b) - 1) < 1e-14
+
+
+@pytest.mark.parametrize("name", TABLEAUX)
+@pytest.mark.parametrize("ke", [IO.KE_EX, IO.KE_SPLIT, IO.KE_CONSERVATIVE])
+def test_rk_conservation_and_convergence(name, ke):
+    """Every tableau keeps the periodic totals to round-off, and halving dt
+    over a fixed time shrinks the difference to a fine-step solution by
+    about two (the linearised stages are first order in time here)."""
+    D, n = 2, 16
+    U0, p0 = _smooth_state(D, n, 3)
+    dx = [1.0 / n] * D
+
+    def run(steps, tab, T=0.02):
+        U, p = U0.copy(), p0.copy()
+        for _ in range(steps):
+            r = IO.imex_rk_step(U, p, D, dx, T / steps, ADIA, EPS, [1] * 3, [1] * 3, IO.RUSANOV, IO.REUSE_PRESSURE,
+                                ke, tab, tol_rel=1e-13)
+            U, p = r["U"], r["p"]
+        return U
+
+    U1 = run(2, name)
+    scale = np.abs(U0).sum(axis=(1, 2, 3))
+    assert np.all(np.abs(U1.sum(axis=(1, 2, 3)) - U0.sum(axis=(1, 2, 3))) <= 1e-13 * scale)
+    ref = run(32, name)
+    e4, e8 = np.abs(run(4, name) - ref).max(), np.abs(run(8, name) - ref).max()
+    assert e8 < 0.6 * e4

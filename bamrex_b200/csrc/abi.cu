@@ -903,18 +903,18 @@ extern "C" int bamrex_level_create(bamrex_level** out, const bamrex_level_desc* 
     const size_t o_pack = take(sizeof(PackBox) * nb);
     const size_t o_stage = take((size_t)L->ncells * L->NC * 8);
     const size_t o_scal = take(sizeof(StepScalars));
-    cudaError_t e = cudaMalloc((void**)&L->arena, off);
+    cudaError_t e = dev_alloc((void**)&L->arena, off, L->stream);
     if (e != cudaSuccess) {
         if (L->own_stream) cudaStreamDestroy(L->stream);
         delete L;
-        return fail(BAMREX_ERR_OOM, std::string("cudaMalloc of the level arena failed: ") + cudaGetErrorString(e));
+        return fail(BAMREX_ERR_OOM, std::string("allocation of the level arena failed: ") + cudaGetErrorString(e));
     }
-    e = cudaMallocHost((void**)&L->h_scal, sizeof(StepScalars));
+    e = pinned_small_alloc((void**)&L->h_scal, sizeof(StepScalars));
     if (e != cudaSuccess) {
-        cudaFree(L->arena);
+        dev_free(L->arena, L->stream);
         if (L->own_stream) cudaStreamDestroy(L->stream);
         delete L;
-        return fail(BAMREX_ERR_OOM, "cudaMallocHost failed");
+        return fail(BAMREX_ERR_OOM, "pinned host allocation failed");
     }
     L->state[0] = L->arena + o_state0;
     L->state[1] = L->arena + o_state1;
@@ -976,10 +976,9 @@ extern "C" int bamrex_level_destroy(bamrex_level* L)
         cudaEventDestroy(ev.first);
         cudaEventDestroy(ev.second);
     }
-    if (L->arena) cudaFree(L->arena);
-    for (int d = 0; d < 3; ++d)
-        if (L->halo_mem[d]) cudaFree(L->halo_mem[d]);
-    if (L->h_scal) cudaFreeHost(L->h_scal);
+    dev_free(L->arena, L->stream);
+    for (int d = 0; d < 3; ++d) dev_free(L->halo_mem[d], L->stream);
+    pinned_small_free(L->h_scal);
     if (L->own_stream && L->stream) cudaStreamDestroy(L->stream);
     delete L;
     return BAMREX_OK;

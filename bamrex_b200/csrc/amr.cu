@@ -7,11 +7,14 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <new>
 #include <string>
+#include <thread>
 #include <tuple>
 #include <vector>
 
@@ -191,15 +194,69 @@ void map_into_domain(const bamrex_level* L, int* c, int& negmask)
     }
 }
 
+// Host worker threads for a table build of `work` records: about 64k
+// records a thread, at most the machine's threads (and 32).
+int table_threads(long long work)
+{
+    const long long hw = std::max(1u, std::thread::hardware_concurrency());
+    return (int)std::max(1LL, std::min({ hw, 32LL, work / 65536 + 1 }));
+}
+
+// fn(item, scratch) over items [0, n) on `nthreads` threads taking chunks of
+// `chunk` items in turn; each thread owns one Scratch. The first failure in
+// item order wins: fn returns an empty string on success, else the message.
+template <class Scratch, class F>
+int parallel_items(int n, int nthreads, int chunk, F&& fn)
+{
+    std::atomic<int> next(0);
+    std::mutex mu;
+    int bad_item = n;
+    std::string bad_msg;
+    auto worker = [&] {
+        Scratch scratch;
+        for (;;) {
+            const int b = next.fetch_add(chunk);
+            if (b >= n) return;
+            for (int it = b; it < std::min(n, b + chunk); ++it) {
+                std::string msg = fn(it, scratch);
+                if (msg.empty()) continue;
+                std::lock_guard<std::mutex> g(mu);
+                if (it < bad_item) {
+                    bad_item = it;
+                    bad_msg = std::move(msg);
+                }
+                break;
+            }
+        }
+    };
+    nthreads = std::max(1, std::min(nthreads, (n + chunk - 1) / std::max(1, chunk)));
+    if (nthreads == 1) {
+        worker();
+    } else {
+        std::vector<std::thread> th;
+        for (int t = 0; t < nthreads; ++t) th.emplace_back(worker);
+        for (auto& x : th) x.join();
+    }
+    return bad_item < n ? fail(BAMREX_ERR_ARG, bad_msg) : BAMREX_OK;
+}
+
+struct OwnerScratch {
+    std::vector<int> own, hits;
+};
+
 // Coarse patches (coarsened region grown by one coarse cell) of a set of
-// fine regions.
+// fine regions. Patches inside the coarse domain take each cell's owner from
+// one sweep over the boxes they meet; cells outside it are mapped by the
+// boundary rules and looked up one by one. Regions run on host threads, each
+// writing its own slice of `cells`.
 int build_patches(const bamrex_coupling* C, std::vector<CfRegion>& regs, std::vector<CfPatchCell>& cells,
                   const BoxIndex& cidx)
 {
     const bamrex_level* Lc = C->crse;
     long long pacc = 0, cacc = 0;
-    std::vector<int> own, hits;
-    for (auto& R : regs) {
+    std::vector<bamrex_box> patch(regs.size());
+    for (size_t n = 0; n < regs.size(); ++n) {
+        CfRegion& R = regs[n];
         bamrex_box w;
         for (int d = 0; d < 3; ++d) {
             w.lo[d] = R.lo[d] + R.shift[d];
@@ -218,30 +275,33 @@ int build_patches(const bamrex_coupling* C, std::vector<CfRegion>& regs, std::ve
         R.cell_begin = cacc;
         pacc += box_volume(p);
         cacc += (long long)(R.hi[0] - R.lo[0] + 1) * (R.hi[1] - R.lo[1] + 1) * (R.hi[2] - R.lo[2] + 1);
-        cell_owners(cidx, Lc->boxes, p, own, hits);
+        patch[n] = p;
+    }
+    cells.resize((size_t)pacc);
+    auto region = [&](int n, OwnerScratch& S) -> std::string {
+        const bamrex_box& p = patch[n];
+        CfPatchCell* out = cells.data() + regs[n].patch_begin;
+        cell_owners(cidx, Lc->boxes, p, S.own, S.hits);
+        bool inside = true;
+        for (int d = 0; d < C->D; ++d) inside = inside && p.lo[d] >= Lc->domain.lo[d] && p.hi[d] <= Lc->domain.hi[d];
         size_t q = 0;
         for (int k = p.lo[2]; k <= p.hi[2]; ++k)
             for (int j = p.lo[1]; j <= p.hi[1]; ++j)
                 for (int i = p.lo[0]; i <= p.hi[0]; ++i, ++q) {
                     int c[3] = { i, j, k };
-                    int neg = 0;
-                    map_into_domain(Lc, c, neg);
-                    const bool moved = c[0] != i || c[1] != j || c[2] != k;
-                    const int b = moved ? find_containing(cidx, Lc->boxes, c, hits) : own[q];
+                    int neg = 0, b = S.own[q];
+                    if (!inside) {
+                        map_into_domain(Lc, c, neg);
+                        if (c[0] != i || c[1] != j || c[2] != k) b = find_containing(cidx, Lc->boxes, c, S.hits);
+                    }
                     if (b < 0)
-                        return fail(BAMREX_ERR_ARG,
-                                    "fine level not properly nested: coarse cell (" + std::to_string(c[0]) + "," +
-                                        std::to_string(c[1]) + "," + std::to_string(c[2]) + ") is not a valid coarse cell");
-                    CfPatchCell pc;
-                    pc.box = b;
-                    pc.i = c[0];
-                    pc.j = c[1];
-                    pc.k = c[2];
-                    pc.negmask = neg;
-                    cells.push_back(pc);
+                        return "fine level not properly nested: coarse cell (" + std::to_string(c[0]) + "," +
+                               std::to_string(c[1]) + "," + std::to_string(c[2]) + ") is not a valid coarse cell";
+                    out[q] = CfPatchCell{ b, c[0], c[1], c[2], neg };
                 }
-    }
-    return BAMREX_OK;
+        return std::string();
+    };
+    return parallel_items<OwnerScratch>((int)regs.size(), table_threads(pacc), 8, region);
 }
 
 CfRegion make_region(int dst, const bamrex_box& b, const int* shift)
@@ -304,7 +364,8 @@ void build_ghost_regions(const bamrex_level* Lf, const BoxIndex& fidx, std::vect
     }
 }
 
-// Flux-register slots of direction d.
+// Flux-register slots of direction d. The fine boxes run on host threads,
+// each filling its own record lists, which are then joined in box order.
 int build_register(const bamrex_coupling* C, int d, const BoxIndex& fidx, const BoxIndex& cidx,
                    std::vector<FaceRec>& cf, std::vector<FaceRec>& ff, std::vector<RefluxRec>& rr)
 {
@@ -312,8 +373,15 @@ int build_register(const bamrex_coupling* C, int d, const BoxIndex& fidx, const 
     const bamrex_level* Lc = C->crse;
     const int r = C->r, D = C->D;
     const int dlo = Lf->domain.lo[d], dhi = Lf->domain.hi[d], len = dhi - dlo + 1;
-    std::vector<int> own, hits;
-    for (int b = 0; b < (int)Lf->boxes.size(); ++b) {
+    const int nbf = (int)Lf->boxes.size();
+    std::vector<std::vector<FaceRec>> cfb(nbf), ffb(nbf);
+    std::vector<std::vector<RefluxRec>> rrb(nbf);
+    // the r^(D-1) fine faces under a coarse face, transverse index fastest
+    // in x, then y, then z
+    const int tz = (D > 2 && d != 2) ? r : 1;
+    const int ty = (D > 1 && d != 1) ? r : 1;
+    const int tx = (d != 0) ? r : 1;
+    auto box = [&](int b, OwnerScratch& S) -> std::string {
         const bamrex_box& B = Lf->boxes[b];
         for (int side = 0; side < 2; ++side) {
             bamrex_box layer = B;
@@ -331,58 +399,69 @@ int build_register(const bamrex_coupling* C, int d, const BoxIndex& fidx, const 
             const int fface = side == 0 ? B.lo[d] : B.hi[d] + 1;
             for (const auto& p : pieces) {
                 const bamrex_box cp = coarsen(p, r, D);
-                cell_owners(cidx, Lc->boxes, cp, own, hits);
+                cell_owners(cidx, Lc->boxes, cp, S.own, S.hits);
                 size_t oq = 0;
                 for (int k = cp.lo[2]; k <= cp.hi[2]; ++k)
                     for (int j = cp.lo[1]; j <= cp.hi[1]; ++j)
                         for (int i = cp.lo[0]; i <= cp.hi[0]; ++i, ++oq) {
-                            int c[3] = { i, j, k };
-                            const int cb = own[oq];
-                            if (cb < 0) return fail(BAMREX_ERR_ARG, "fine level not properly nested (flux register)");
-                            RefluxRec q;
-                            q.box = cb;
-                            q.i = i;
-                            q.j = j;
-                            q.k = k;
-                            q.sign = side == 0 ? -1 : 1;
-                            rr.push_back(q);
-                            FaceRec f;
-                            f.box = cb;
-                            f.i = i;
-                            f.j = j;
-                            f.k = k;
+                            const int c[3] = { i, j, k };
+                            const int cb = S.own[oq];
+                            if (cb < 0) return "fine level not properly nested (flux register)";
+                            rrb[b].push_back(RefluxRec{ cb, i, j, k, side == 0 ? -1 : 1 });
+                            FaceRec f{ cb, i, j, k };
                             const int cface = c[d] + (side == 0 ? 1 : 0);
                             if (d == 0) f.i = cface;
                             else if (d == 1) f.j = cface;
                             else f.k = cface;
-                            cf.push_back(f);
-                            // the r^(D-1) fine faces under this coarse face,
-                            // transverse index fastest in x, then y, then z
-                            const int tz = (D > 2 && d != 2) ? r : 1;
-                            const int ty = (D > 1 && d != 1) ? r : 1;
-                            const int tx = (d != 0) ? r : 1;
+                            cfb[b].push_back(f);
                             for (int a2 = 0; a2 < tz; ++a2)
                                 for (int a1 = 0; a1 < ty; ++a1)
-                                    for (int a0 = 0; a0 < tx; ++a0) {
-                                        FaceRec g;
-                                        g.box = b;
-                                        g.i = d == 0 ? fface : c[0] * r + a0;
-                                        g.j = d == 1 ? fface : (D > 1 ? c[1] * r + a1 : 0);
-                                        g.k = d == 2 ? fface : (D > 2 ? c[2] * r + a2 : 0);
-                                        ff.push_back(g);
-                                    }
+                                    for (int a0 = 0; a0 < tx; ++a0)
+                                        ffb[b].push_back(FaceRec{ b, d == 0 ? fface : c[0] * r + a0,
+                                                                  d == 1 ? fface : (D > 1 ? c[1] * r + a1 : 0),
+                                                                  d == 2 ? fface : (D > 2 ? c[2] * r + a2 : 0) });
                         }
             }
         }
+        return std::string();
+    };
+    long long work = 0;
+    for (const auto& B : Lf->boxes) work += box_volume(B) / std::max(1, B.hi[d] - B.lo[d] + 1);
+    BX_TRY(parallel_items<OwnerScratch>(nbf, table_threads(work), 4, box));
+    size_t n = 0;
+    for (int b = 0; b < nbf; ++b) n += rrb[b].size();
+    rr.reserve(n);
+    cf.reserve(n);
+    ff.reserve(n * tx * ty * tz);
+    for (int b = 0; b < nbf; ++b) {
+        rr.insert(rr.end(), rrb[b].begin(), rrb[b].end());
+        cf.insert(cf.end(), cfb[b].begin(), cfb[b].end());
+        ff.insert(ff.end(), ffb[b].begin(), ffb[b].end());
     }
-    // a coarse cell may border the fine region on one side only
-    std::vector<unsigned long long> keys(rr.size());
+    // a coarse cell may border the fine region on one side only: mark each
+    // slot's cell in a bit map of the coarse domain (sorted keys where the
+    // domain is too large for one)
     const int* cl = Lc->domain.lo;
-    for (size_t q = 0; q < rr.size(); ++q)
-        keys[q] = ((unsigned long long)(rr[q].k - cl[2]) << 42) | ((unsigned long long)(rr[q].j - cl[1]) << 21) |
-                  (unsigned long long)(rr[q].i - cl[0]);
-    std::sort(keys.begin(), keys.end());
-    if (std::adjacent_find(keys.begin(), keys.end()) != keys.end())
+    const unsigned long long nx = Lc->domain.hi[0] - cl[0] + 1, ny = Lc->domain.hi[1] - cl[1] + 1,
+                             nz = Lc->domain.hi[2] - cl[2] + 1;
+    bool dup = false;
+    if (nx * ny * nz <= (1ULL << 27)) {
+        std::vector<unsigned long long> seen((nx * ny * nz + 63) / 64, 0ULL);
+        for (size_t q = 0; q < rr.size() && !dup; ++q) {
+            const unsigned long long key = ((unsigned long long)(rr[q].k - cl[2]) * ny + (rr[q].j - cl[1])) * nx + (rr[q].i - cl[0]);
+            const unsigned long long bit = 1ULL << (key & 63);
+            dup = (seen[key >> 6] & bit) != 0;
+            seen[key >> 6] |= bit;
+        }
+    } else {
+        std::vector<unsigned long long> keys(rr.size());
+        for (size_t q = 0; q < rr.size(); ++q)
+            keys[q] = ((unsigned long long)(rr[q].k - cl[2]) << 42) | ((unsigned long long)(rr[q].j - cl[1]) << 21) |
+                      (unsigned long long)(rr[q].i - cl[0]);
+        std::sort(keys.begin(), keys.end());
+        dup = std::adjacent_find(keys.begin(), keys.end()) != keys.end();
+    }
+    if (dup)
         return fail(BAMREX_ERR_ARG,
                     "fine boxes closer than two coarse cells: a coarse cell borders the fine region on both sides");
     return BAMREX_OK;
@@ -525,8 +604,8 @@ extern "C" int bamrex_coupling_create(bamrex_coupling** out, bamrex_level* crse,
     const size_t o_covf0 = take(sizeof(FabDev) * cov.size());
     const size_t o_covf1 = take(sizeof(FabDev) * cov.size());
     const size_t o_covs = take(sizeof(double) * C->NC * std::max<size_t>(1, cov.size()));
-    cudaError_t e = cudaMalloc((void**)&C->arena, off);
-    if (e != cudaSuccess) return fail(BAMREX_ERR_OOM, std::string("cudaMalloc of the coupling failed: ") + cudaGetErrorString(e));
+    cudaError_t e = dev_alloc((void**)&C->arena, off, crse->stream);
+    if (e != cudaSuccess) return fail(BAMREX_ERR_OOM, std::string("allocation of the coupling failed: ") + cudaGetErrorString(e));
     char* A = C->arena;
     C->old_state = A + o_old;
     C->d_old_fab = (FabDev*)(A + o_oldfab);
@@ -575,7 +654,7 @@ extern "C" int bamrex_coupling_create(bamrex_coupling** out, bamrex_level* crse,
     if (e == cudaSuccess) e = up(C->d_cov_box, cov.data(), sizeof(PackBox) * cov.size());
     for (int p = 0; p < 2 && e == cudaSuccess; ++p) e = up(C->d_cov_fab[p], covfab[p].data(), sizeof(FabDev) * cov.size());
     if (e != cudaSuccess) {
-        cudaFree(C->arena);
+        dev_free(C->arena, crse->stream);
         return cuda_fail(e, "coupling table upload");
     }
     const int per_slot = D == 1 ? 1 : (D == 2 ? r : r * r);
@@ -607,7 +686,7 @@ extern "C" int bamrex_coupling_destroy(bamrex_coupling* C)
         drop_tasks(C->crse, C->d_reg[d]);
         drop_tasks(C->fine, C->d_reg[d]);
     }
-    if (C->arena) cudaFree(C->arena);
+    dev_free(C->arena, C->crse ? C->crse->stream : nullptr);
     delete C;
     return BAMREX_OK;
 }
@@ -1255,7 +1334,7 @@ int set_level(bamrex_amr* A, int lev, const std::vector<bamrex_box>& boxes)
             void* dmem = nullptr;
             const size_t tb = sizeof(FabDev) * tab.size(), ob = sizeof(GhostOp) * ops.size();
             const std::vector<int> ct = ghost_chunk_table(ops, nchunks);
-            cudaError_t e = cudaMalloc(&dmem, align_up(tb, 256) + ghost_table_bytes(ops.size(), nchunks));
+            cudaError_t e = dev_alloc(&dmem, align_up(tb, 256) + ghost_table_bytes(ops.size(), nchunks), A->stream);
             if (e == cudaSuccess) e = cudaMemcpy(dmem, tab.data(), tb, cudaMemcpyHostToDevice);
             GhostOp* dops = (GhostOp*)((char*)dmem + align_up(tb, 256));
             if (e == cudaSuccess) e = cudaMemcpy(dops, ops.data(), ob, cudaMemcpyHostToDevice);
@@ -1263,7 +1342,7 @@ int set_level(bamrex_amr* A, int lev, const std::vector<bamrex_box>& boxes)
             if (e == cudaSuccess)
                 e = launch_ghost_fill(L->NC, L->fp32, dops, (int)ops.size(), nchunks, (const FabDev*)dmem, nullptr, A->stream);
             if (e == cudaSuccess) e = cudaStreamSynchronize(A->stream);
-            if (dmem) cudaFree(dmem);
+            dev_free(dmem, A->stream);
             if (e != cudaSuccess) rc = cuda_fail(e, "regrid copy");
         }
     }

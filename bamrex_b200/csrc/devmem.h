@@ -1,0 +1,32 @@
+// Device and pinned memory for the tables and states that levels, halo
+// plans and AMR couplings own.
+//
+// A regrid frees one level and its coupling and makes the next one of about
+// the same size. Plain cudaMalloc/cudaFree there maps and unmaps pages in the
+// driver on every call (and cudaFree synchronises the device), which costs
+// from a millisecond to, on a loaded host, hundreds. These helpers take the
+// blocks from a stream-ordered pool per device that keeps freed blocks
+// (release threshold = unlimited), so the next level reuses the same pages.
+// The pool is trimmed back to nothing when the library holds no block on
+// that device any more.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+
+namespace bamrex {
+
+// A block of `bytes` on the current device, ordered after the work already
+// queued on `s` and usable from every stream when the call returns.
+cudaError_t dev_alloc(void** p, size_t bytes, cudaStream_t s);
+
+// Give a block back; the caller has finished all work on it (every stream).
+void dev_free(void* p, cudaStream_t s);
+
+// Small pinned host blocks (up to 4 KB) for the scalars a step reads back,
+// cut from pinned slabs that are kept for the life of the process.
+cudaError_t pinned_small_alloc(void** p, size_t bytes);
+void pinned_small_free(void* p);
+
+}  // namespace bamrex

@@ -51,7 +51,7 @@ extern "C" int bamrex_level_set_halo(bamrex_level* L, int dir, const bamrex_regi
     }
     if (L->halo_mem[dir]) {
         cudaStreamSynchronize(L->stream);
-        cudaFree(L->halo_mem[dir]);
+        dev_free(L->halo_mem[dir], L->stream);
         L->halo_mem[dir] = nullptr;
     }
     size_t off = 0;
@@ -64,8 +64,8 @@ extern "C" int bamrex_level_set_halo(bamrex_level* L, int dir, const bamrex_regi
             off = align_up(off + sizeof(FabDev) * std::max<size_t>(1, fb[s][par].size()), 256);
         }
     }
-    cudaError_t e = cudaMalloc((void**)&L->halo_mem[dir], off);
-    if (e != cudaSuccess) return L->set_err(fail(BAMREX_ERR_OOM, "cudaMalloc of the halo tables failed"));
+    cudaError_t e = dev_alloc((void**)&L->halo_mem[dir], off, L->stream);
+    if (e != cudaSuccess) return L->set_err(fail(BAMREX_ERR_OOM, "allocation of the halo tables failed"));
     char* m = L->halo_mem[dir];
     bamrex_level::Halo* H[2] = { &L->halo_send[dir], &L->halo_recv[dir] };
     for (int s = 0; s < 2; ++s) {

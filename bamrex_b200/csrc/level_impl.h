@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "bamrex_cuda.h"
+#include "devmem.h"
 #include "launch.h"
 
 namespace bamrex {

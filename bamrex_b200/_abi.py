@@ -27,6 +27,13 @@ BC_TRANSMISSIVE, BC_PERIODIC, BC_REFLECTIVE = range(3)
 BCS = {"transmissive": BC_TRANSMISSIVE, "periodic": BC_PERIODIC, "reflective": BC_REFLECTIVE}
 # level state precision
 FP64, FP32_STORAGE = 0, 1
+# rigid bodies: shapes (Source/Geometry), combinations, RigidBodyBCType
+# (Source/BoundaryConditions/BCTypes.H:50-57), GFMFlag bits (Source/GFM/GFMFlag.H)
+SDF_PLANE, SDF_SPHERE, SDF_CYLINDER = range(3)
+SDF_UNION, SDF_INTERSECTION = range(2)
+RB_REFLECTIVE, RB_NO_SLIP, RB_FOEXTRAP = range(3)
+RB_BCS = {"reflective": RB_REFLECTIVE, "no_slip": RB_NO_SLIP, "foextrap": RB_FOEXTRAP}
+GFM_GHOST, GFM_INTERFACE, GFM_FILL = 1, 2, 4
 
 
 class BamrexError(RuntimeError):
@@ -161,6 +168,27 @@ class ImexDesc(ctypes.Structure):
     ]
 
 
+class Sdf(ctypes.Structure):
+    _fields_ = [
+        ("kind", ctypes.c_int),
+        ("center", ctypes.c_double * 3),
+        ("axis", ctypes.c_double * 3),
+        ("radius", ctypes.c_double),
+        ("fluid_inside", ctypes.c_int),
+    ]
+
+
+class BodyDesc(ctypes.Structure):
+    _fields_ = [
+        ("nshapes", ctypes.c_int),
+        ("combine", ctypes.c_int),
+        ("shapes", Sdf * 2),
+        ("rb_bc", ctypes.c_int),
+        ("stencil", ctypes.c_int),
+        ("fill_diagonals", ctypes.c_int),
+    ]
+
+
 class AmrDesc(ctypes.Structure):
     _fields_ = [
         ("base", LevelDesc),
@@ -230,6 +258,10 @@ SIGNATURES = {
     "bamrex_level_fill_dir": (_i, [_vp, _i]),
     "bamrex_level_sweep_dir": (_i, [_vp, _i, _d, _i]),
     "bamrex_level_wave_speed": (_i, [_vp, _dp]),
+    "bamrex_level_set_body": (_i, [_vp, ctypes.POINTER(BodyDesc)]),
+    "bamrex_level_fill_body_ghosts": (_i, [_vp]),
+    "bamrex_level_body_field": (_i, [_vp, _i, _dp]),
+    "bamrex_level_body_counts": (_i, [_vp, ctypes.POINTER(_ll), ctypes.POINTER(_ll)]),
     "bamrex_level_tag": (_i, [_vp, _i, _i, _d, _i, _i, _i, _d, ctypes.c_char_p]),
     "bamrex_coupling_create": (_i, [ctypes.POINTER(_vp), _vp, _vp, _i]),
     "bamrex_coupling_destroy": (_i, [_vp]),

@@ -25,10 +25,11 @@ INCLUDE = os.path.join(ROOT, "include")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
          "--expt-relaxed-constexpr", "-I", INCLUDE, "-I", CSRC]
-# Per-file extra flags: the AMR coupling kernels, the Helmholtz operator and
-# the IMEX step round every product and sum separately so a CPU restatement
+# Per-file extra flags: the AMR coupling kernels, the Helmholtz operator, the
+# IMEX step and the ghost-fluid rigid bodies round every product and sum separately so a CPU restatement
 # reproduces them exactly.
-FILE_FLAGS = {"amr_kernels.cu": ["-fmad=false"], "helmholtz.cu": ["-fmad=false"], "imex.cu": ["-fmad=false"]}
+FILE_FLAGS = {"amr_kernels.cu": ["-fmad=false"], "helmholtz.cu": ["-fmad=false"], "imex.cu": ["-fmad=false"],
+              "gfm.cu": ["-fmad=false"]}
 
 
 def nvcc() -> str:

@@ -678,7 +678,10 @@ int level_sweep(bamrex_level* L, int d, int parity, double dt_host, const StepSc
 
 int level_step(bamrex_level* L, int parity, double dt_host, StepScalars* scal, bool allow_timing)
 {
-    BX_TRY(level_fill(L, 0, parity, scal));
+    // with a rigid body: FillPatch, fill_ghost_rb and fill_consv_boundary
+    // (AmrLevelAdv_advance.cpp:108-116) fill every ghost cell first
+    if (L->body) BX_TRY(body_fill(L, parity, scal));
+    else BX_TRY(level_fill(L, 0, parity, scal));
     int p = parity;
     for (int d = 0; d < L->D; ++d) {
         BX_TRY(level_sweep(L, d, p, dt_host, scal, d == L->D - 1, allow_timing));
@@ -970,6 +973,7 @@ extern "C" int bamrex_level_destroy(bamrex_level* L)
 {
     if (!L) return BAMREX_OK;
     if (L->stream) cudaStreamSynchronize(L->stream);
+    body_destroy(L);
     for (int p = 0; p < 2; ++p)
         if (L->graph[p]) cudaGraphExecDestroy(L->graph[p]);
     for (auto& ev : L->events) {

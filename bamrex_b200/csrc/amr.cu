@@ -494,6 +494,7 @@ extern "C" int bamrex_coupling_create(bamrex_coupling** out, bamrex_level* crse,
     if (fine->D != D || fine->fp32 != crse->fp32 || fine->method != crse->method)
         return fail(BAMREX_ERR_ARG, "coarse and fine levels differ in dimension, precision or method");
     if (fine->stream != crse->stream) return fail(BAMREX_ERR_ARG, "coarse and fine levels must share a stream");
+    if (crse->body || fine->body) return fail(BAMREX_ERR_UNSUPPORTED, "rigid bodies on coupled AMR levels are not provided");
     if (fine->ngrow < 2) return fail(BAMREX_ERR_ARG, "fine ngrow must be >= 2");
     for (int d = 0; d < D; ++d) {
         if (fine->domain.lo[d] != crse->domain.lo[d] * r || fine->domain.hi[d] != (crse->domain.hi[d] + 1) * r - 1)

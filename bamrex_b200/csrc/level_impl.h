@@ -50,6 +50,9 @@ struct RegisterTask {
     int mode = 0;           // 0: reg = -(F * scale) (CrseInit); 1: reg += F * scale per face (FineAdd)
 };
 
+// Rigid body of a level (gfm.cu).
+struct BodyState;
+
 }  // namespace bamrex
 
 struct bamrex_level {
@@ -115,6 +118,9 @@ struct bamrex_level {
     double dir_ms[3] = { 0, 0, 0 };
     long long dir_launches[3] = { 0, 0, 0 };
 
+    // static rigid body by the ghost-fluid method (bamrex_level_set_body)
+    bamrex::BodyState* body = nullptr;
+
     cudaGraphExec_t graph[2] = { nullptr, nullptr };
     bool run_pending = false;
     int run_start_parity = 0;
@@ -146,6 +152,10 @@ int level_sweep(bamrex_level* L, int d, int parity, double dt_host, const StepSc
 // One split step starting from buffer `parity`; the result lands in
 // parity ^ (D & 1).  dt from the host (scal == nullptr) or from the device.
 int level_step(bamrex_level* L, int parity, double dt_host, StepScalars* scal, bool allow_timing);
+// The rigid-body ghost fill of buffer `parity` (gfm.cu); gate: the step
+// scalars whose `done` flag skips the work in device-stepped runs.
+int body_fill(bamrex_level* L, int parity, const StepScalars* gate);
+void body_destroy(bamrex_level* L);
 
 // Face fluxes of direction `dir` recomputed from the sweep input `in` at the
 // faces of a register task (face_flux.cu).

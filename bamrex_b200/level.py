@@ -306,6 +306,63 @@ class Level:
                                         float(phierr), buf))
         return np.frombuffer(buf.raw, dtype=np.uint8).copy()
 
+    # rigid body by the ghost-fluid method
+    def set_body(self, shapes, combine=_abi.SDF_UNION, rb_bc=_abi.RB_REFLECTIVE, stencil=2, fill_diagonals=False):
+        """A static rigid body (bamrex_level_set_body).  shapes: one or two
+        dicts with kind (SDF_PLANE / SDF_SPHERE / SDF_CYLINDER), center, axis
+        (plane normal out of the body / cylinder axis), radius, fluid_inside;
+        None removes the body."""
+        if shapes is None:
+            self._ck(lib().bamrex_level_set_body(self._h, None))
+            return
+        if isinstance(shapes, dict):
+            shapes = [shapes]
+        d = _abi.BodyDesc()
+        d.nshapes = len(shapes)
+        d.combine = int(combine)
+        for n, sh in enumerate(shapes):
+            f = d.shapes[n]
+            f.kind = int(sh["kind"])
+            for q in range(3):
+                c = sh.get("center", (0.0, 0.0, 0.0))
+                a = sh.get("axis", (0.0, 0.0, 1.0))
+                f.center[q] = float(c[q]) if q < len(c) else 0.0
+                f.axis[q] = float(a[q]) if q < len(a) else 0.0
+            f.radius = float(sh.get("radius", 0.0))
+            f.fluid_inside = 1 if sh.get("fluid_inside", False) else 0
+        d.rb_bc = int(rb_bc)
+        d.stencil = int(stencil)
+        d.fill_diagonals = 1 if fill_diagonals else 0
+        self._ck(lib().bamrex_level_set_body(self._h, ctypes.byref(d)))
+
+    def fill_body_ghosts(self):
+        """The rigid-body ghost fill on the current state (FillRBGhostCells)."""
+        self._ck(lib().bamrex_level_fill_body_ghosts(self._h))
+
+    def body_field(self, which) -> np.ndarray:
+        """Level set (0), normal component d (1 + d) or GFM flags (-1) of the
+        valid cells as a global (nz, ny, nx) array."""
+        out = np.empty(int(self.ncells))
+        self._ck(lib().bamrex_level_body_field(self._h, int(which), out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+        his = np.max(np.array([hi for _, hi in self.boxes]), axis=0)
+        n = [his[d] - self.dom_lo[d] + 1 for d in range(3)]
+        glob = np.full((n[2], n[1], n[0]), np.nan)
+        o = 0
+        L = self.dom_lo
+        for lo, hi in self.boxes:
+            shp = (hi[2] - lo[2] + 1, hi[1] - lo[1] + 1, hi[0] - lo[0] + 1)
+            m = shp[0] * shp[1] * shp[2]
+            glob[lo[2] - L[2]:hi[2] - L[2] + 1, lo[1] - L[1]:hi[1] - L[1] + 1, lo[0] - L[0]:hi[0] - L[0] + 1] = \
+                out[o:o + m].reshape(shp)
+            o += m
+        return glob
+
+    def body_counts(self):
+        """(interface ghost cells, body cells swept by the extrapolation)."""
+        a, b = ctypes.c_longlong(), ctypes.c_longlong()
+        self._ck(lib().bamrex_level_body_counts(self._h, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
     def conserved_sums(self):
         """sum(U) * cell volume per component (FP64, fixed order)."""
         out = (ctypes.c_double * self.NC)()

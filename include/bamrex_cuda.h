@@ -23,7 +23,7 @@
 extern "C" {
 #endif
 
-#define BAMREX_ABI_VERSION 2
+#define BAMREX_ABI_VERSION 3
 /* MAX_NCOMP = PUInd::size (Source/System/Parm.H:9) */
 #define BAMREX_MAX_NCOMP 8
 
@@ -328,6 +328,68 @@ BAMREX_API int bamrex_level_sweep_dir(bamrex_level *level, int dir, double dt, i
 /* Max wave speed |u| + c over this rank's valid cells (from the last sweep
  * that reduced it, else computed); synchronises the stream. */
 BAMREX_API int bamrex_level_wave_speed(bamrex_level *level, double *ws);
+
+/* ------------------------------------------------------------------ */
+/* Rigid bodies by the ghost-fluid method                               */
+/* ------------------------------------------------------------------ */
+
+/* Signed-distance shapes (Source/Geometry/PlaneSDF.H, SphereSDF.H,
+ * CylinderSDF.H); the level set is > 0 in the body, < 0 in the fluid. */
+enum { BAMREX_SDF_PLANE = 0, BAMREX_SDF_SPHERE = 1, BAMREX_SDF_CYLINDER = 2 };
+/* Two shapes combined (UnionSDF.H, IntersectionSDF.H). */
+enum { BAMREX_SDF_UNION = 0, BAMREX_SDF_INTERSECTION = 1 };
+/* RigidBodyBCType (Source/BoundaryConditions/BCTypes.H:50-57). */
+enum { BAMREX_RB_REFLECTIVE = 0, BAMREX_RB_NO_SLIP = 1, BAMREX_RB_FOEXTRAP = 2 };
+/* GFMFlag bits (Source/GFM/GFMFlag.H:10-21). */
+enum { BAMREX_GFM_GHOST = 1, BAMREX_GFM_INTERFACE = 2, BAMREX_GFM_FILL = 4 };
+
+typedef struct bamrex_sdf {
+    int kind;          /* BAMREX_SDF_* */
+    double center[3];  /* plane: a point of the plane; sphere, cylinder: centre */
+    double axis[3];    /* plane: normal pointing out of the body; cylinder: axis (normalised here) */
+    double radius;     /* sphere, cylinder */
+    int fluid_inside;  /* sphere, cylinder: has_fluid_inside */
+} bamrex_sdf;
+
+typedef struct bamrex_body_desc {
+    int nshapes;        /* 1 or 2 */
+    int combine;        /* BAMREX_SDF_UNION / _INTERSECTION of shapes[0] and shapes[1] */
+    bamrex_sdf shapes[2];
+    int rb_bc;          /* BAMREX_RB_* (the reference default: reflective) */
+    int stencil;        /* GFMFillInfo::stencil, 1..ngrow (default 2) */
+    int fill_diagonals; /* GFMFillInfo::fill_diagonals */
+} bamrex_body_desc;
+
+/* Give the level a static rigid body (AmrLevelAdv::init_levelset + the
+ * build_gfm_flags calls of AmrLevelAdv::initData, Source/AmrLevelAdv_LSinit.cpp:37-64,
+ * Source/AmrLevelAdv.cpp:250-269): the level set on every cell of every fab
+ * (fill_from_IF, cell centres), its normals on the fabs shrunk by one
+ * (fill_ls_normals, Source/Geometry/Normals.cpp:12-54) and the GFM flags of the
+ * valid cells (Source/GFM/GFMFlag.cpp:60-83), all on the device.  From then
+ * on every bamrex_level_advance / _run starts with the rigid-body ghost fill
+ * below (AmrLevelAdv_advance.cpp:110-116).  desc == NULL removes the body.
+ * Single levels only: a level with a coarse/fine coupling is refused. */
+BAMREX_API int bamrex_level_set_body(bamrex_level *level, const bamrex_body_desc *desc);
+
+/* The rigid-body ghost fill on the current state (FluidSystem::FillRBGhostCells
+ * = fill_ghost_rb, Source/GFM/RigidBody.cpp:24-170, then fill_consv_boundary):
+ * all ghost cells filled; interface ghost cells set from the state
+ * interpolated at their reflection 1.5 dx into the fluid (reflective: exact
+ * Riemann problem of the reflected normal velocity; no_slip: velocity
+ * negated; foextrap: as interpolated); inter-box fill; spacedim + 1 rounds of
+ * fast-sweeping extrapolation into the other body cells
+ * (Source/GFM/Extrapolate.cc:9-37, Extrapolate.H, FastSweep.H), each followed
+ * by the inter-box fill; then the boundary fill again.  Interface cells read
+ * the state from before the fill (the reference writes them in place). */
+BAMREX_API int bamrex_level_fill_body_ghosts(bamrex_level *level);
+
+/* The level set (which = 0), normal component d (which = 1 + d) or the GFM
+ * flags (which = -1) of every valid cell, as doubles in the packed order of
+ * bamrex_level_copy_out.  Synchronises the stream. */
+BAMREX_API int bamrex_level_body_field(bamrex_level *level, int which, double *out);
+
+/* Interface ghost cells, and body cells swept by the extrapolation, of the level. */
+BAMREX_API int bamrex_level_body_counts(const bamrex_level *level, long long *interface_cells, long long *swept_cells);
 
 /* ------------------------------------------------------------------ */
 /* AMR: coarse/fine coupling of two levels                              */

@@ -1,0 +1,256 @@
+"""GPU parity of the ghost-fluid rigid body (bamrex_level_set_body /
+bamrex_level_fill_body_ghosts / advance with a body, through the C ABI)
+against the CPU restatement oracle/gfm_oracle.py.
+
+Bars: the level set, normals and flags are the same formulas in the same
+operation order (no FMA contraction on either side): equal to the last bit.
+The ghost fill and the step carry pow() of the exact Riemann solver and the
+reference's long-double quotient of the extrapolation (a unit in the last
+place each): 1e-12 relative L-infinity per component, the per-step bar of
+the explicit path."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+RTOL = 1e-12
+
+
+@pytest.fixture(scope="module")
+def torch_cuda():
+    import torch
+    assert torch.cuda.is_available(), "GPU tests need a CUDA device"
+    return torch
+
+
+def rel_linf(got, ref):
+    errs = []
+    for n in range(ref.shape[0]):
+        scale = np.max(np.abs(ref[n]))
+        errs.append(np.max(np.abs(got[n] - ref[n])) / (scale if scale > 0 else 1.0))
+    return max(errs)
+
+
+def _split(D, n, nb):
+    """nb boxes along x (then y for nb == 4)."""
+    if nb == 4 and D >= 2:
+        hx, hy = n[0] // 2, n[1] // 2
+        out = []
+        for j in range(2):
+            for i in range(2):
+                lo = [i * hx, j * hy] + [0] * (D - 2)
+                hi = [(i + 1) * hx - 1, (j + 1) * hy - 1] + [n[d] - 1 for d in range(2, D)]
+                out.append((tuple(lo), tuple(hi)))
+        return out
+    h = n[0] // nb
+    return [(tuple([i * h] + [0] * (D - 1)),
+             tuple([(i + 1) * h - 1 if i < nb - 1 else n[0] - 1] + [n[d] - 1 for d in range(1, D)])) for i in range(nb)]
+
+
+def _pad(t):
+    return tuple(t) + (0,) * (3 - len(t))
+
+
+def _make(oracle, D, n, nb, ngrow=3, bc=0, method=0, cfl=0.8):
+    import bamrex_b200 as bx
+    boxes = _split(D, n, nb)
+    dx = [1.0 / n[d] for d in range(D)]
+    lay = oracle.LevelLayout(D, (0, 0, 0), _pad([x - 1 for x in n]), [(_pad(lo), _pad(hi)) for lo, hi in boxes], ngrow,
+                             dx, bc_lo=(bc,) * 3, bc_hi=(bc,) * 3)
+    lev = bx.Level(D, (0,) * D, tuple(x - 1 for x in n), [0.0] * D, [1.0] * D, boxes, bx.Parm(D), method=method, cfl=cfl,
+                   ngrow=ngrow, bc_lo=[bc] * D, bc_hi=[bc] * D)
+    return lay, lev
+
+
+def _flow(D, n, seed, gamma=1.4):
+    """A free stream with smooth random perturbations (physical everywhere)."""
+    rng = np.random.default_rng(seed)
+    shape = (n[2] if D > 2 else 1, n[1] if D > 1 else 1, n[0])
+    rho = 1.0 + 0.1 * rng.random(shape)
+    vel = [0.3 + 0.05 * rng.standard_normal(shape)] + [0.05 * rng.standard_normal(shape) for _ in range(D - 1)]
+    p = 1.0 + 0.1 * rng.random(shape)
+    U = np.zeros((D + 2,) + shape)
+    U[0] = rho
+    ke = np.zeros(shape)
+    for d in range(D):
+        U[1 + d] = rho * vel[d]
+        ke += vel[d] ** 2
+    U[1 + D] = p / (gamma - 1) + 0.5 * rho * ke
+    return U
+
+
+def _shapes(case):
+    """(gpu shape dicts, oracle shapes, combine)."""
+    from oracle import gfm_oracle as G
+    import bamrex_b200 as bx
+    if case == "cylinder":
+        s = [dict(kind=bx.SDF_CYLINDER, center=(0.52, 0.47, 0.0), axis=(0, 0, 1), radius=0.21)]
+        comb = bx.SDF_UNION
+    elif case == "sphere":
+        s = [dict(kind=bx.SDF_SPHERE, center=(0.5, 0.45, 0.55), radius=0.27)]
+        comb = bx.SDF_UNION
+    elif case == "two_cylinders":
+        s = [dict(kind=bx.SDF_CYLINDER, center=(0.3, 0.5, 0.0), axis=(0, 0, 1), radius=0.15),
+             dict(kind=bx.SDF_CYLINDER, center=(0.62, 0.41, 0.0), axis=(0, 0, 1), radius=0.17)]
+        comb = bx.SDF_UNION
+    else:  # a half disc: the intersection of a cylinder and a plane
+        s = [dict(kind=bx.SDF_CYLINDER, center=(0.5, 0.5, 0.0), axis=(0, 0, 1), radius=0.25),
+             dict(kind=bx.SDF_PLANE, center=(0.45, 0.5, 0.0), axis=(-1.0, 0.3, 0.0))]
+        comb = bx.SDF_INTERSECTION
+    so = [G.make_shape(x["kind"], x.get("center", (0, 0, 0)), x.get("axis", (0, 0, 1)), x.get("radius", 0.0),
+                       x.get("fluid_inside", False)) for x in s]
+    return s, so, comb
+
+
+LS_CASES = [(2, (40, 36), 3, "cylinder", 2, False), (2, (32, 32), 4, "two_cylinders", 3, True),
+            (2, (36, 36), 2, "half_disc", 2, False), (3, (16, 14, 12), 2, "sphere", 2, False),
+            (3, (12, 12, 12), 1, "cylinder", 3, True)]
+
+
+@pytest.mark.parametrize("case", LS_CASES, ids=lambda c: "%dd-%s" % (c[0], c[3]))
+def test_levelset_normals_flags(torch_cuda, oracle, case):
+    """Level set, normals and GFM flags on every valid cell, bit for bit."""
+    from oracle import gfm_oracle as G
+    D, n, nb, shape, stencil, diag = case
+    lay, lev = _make(oracle, D, n, nb)
+    s, so, comb = _shapes(shape)
+    lev.set_body(s, combine=comb, stencil=stencil, fill_diagonals=diag)
+    body = G.Body(lay, so, comb, (0.0,) * D, stencil=stencil, fill_diagonals=diag)
+    for which in range(D + 1):
+        np.testing.assert_array_equal(lev.body_field(which), body.field(which))
+    np.testing.assert_array_equal(lev.body_field(-1), body.field(-1))
+    fl = body.field(-1).astype(int)
+    ni, ns = lev.body_counts()
+    assert ni == int(np.sum(((fl & G.GHOST) != 0) & ((fl & G.INTERFACE) != 0)))
+    assert ns == int(np.sum(((fl & G.GHOST) != 0) & ((fl & G.INTERFACE) == 0)))
+    assert ni > 0 and ns > 0
+    lev.close()
+
+
+FILL_CASES = [(2, (40, 36), 3, "cylinder", 0), (2, (40, 36), 3, "cylinder", 1), (2, (40, 36), 3, "cylinder", 2),
+              (2, (32, 32), 4, "two_cylinders", 0), (2, (36, 36), 2, "half_disc", 0), (3, (16, 14, 12), 2, "sphere", 0),
+              (3, (16, 14, 12), 2, "sphere", 2)]
+
+
+@pytest.mark.parametrize("case", FILL_CASES, ids=lambda c: "%dd-%s-rb%d" % (c[0], c[3], c[4]))
+def test_body_ghost_fill(torch_cuda, oracle, case):
+    """FillRBGhostCells (interface cells, inter-box fill, fast-sweeping
+    extrapolation, boundary fill) vs the oracle."""
+    from oracle import gfm_oracle as G
+    D, n, nb, shape, rb = case
+    lay, lev = _make(oracle, D, n, nb)
+    s, so, comb = _shapes(shape)
+    u0 = _flow(D, n, seed=7 + rb)
+    lev.set_body(s, combine=comb, rb_bc=rb)
+    lev.set_state(u0)
+    lev.fill_body_ghosts()
+    got = lev.get_state()
+    body = G.Body(lay, so, comb, (0.0,) * D)
+    buf = lay.alloc()
+    lay.scatter(buf, u0)
+    lay.fill_boundary(buf)
+    assert G.fill_rb(lay, buf, body, rb, 1.4, 1.0) == 0
+    ref = lay.gather(buf)
+    assert not np.allclose(ref, u0)
+    err = rel_linf(got, ref)
+    assert err <= RTOL, err
+    lev.close()
+
+
+@pytest.mark.parametrize("case", [(2, (40, 36), 3, "cylinder", 0, 0), (2, (32, 32), 4, "two_cylinders", 2, 0),
+                                  (2, (40, 36), 3, "cylinder", 1, 1), (3, (16, 14, 12), 2, "sphere", 0, 0)],
+                         ids=lambda c: "%dd-%s-rb%d-m%d" % (c[0], c[3], c[4], c[5]))
+def test_step_with_body(torch_cuda, oracle, case):
+    """AmrLevelAdv::advance with a rigid body: FillPatch, FillRBGhostCells,
+    fill_consv_boundary, then the split sweeps, vs the oracle."""
+    from oracle import gfm_oracle as G
+    D, n, nb, shape, rb, method = case
+    lay, lev = _make(oracle, D, n, nb, method=method)
+    s, so, comb = _shapes(shape)
+    u0 = _flow(D, n, seed=31 + rb)
+    lev.set_body(s, combine=comb, rb_bc=rb)
+    lev.set_state(u0)
+    S1, S2 = lay.alloc(), lay.alloc()
+    lay.scatter(S1, u0)
+    lay.fill_boundary(S1)
+    dt = lay.est_time_step(S1, 1.4, 1.0, 0.8)
+    body = G.Body(lay, so, comb, (0.0,) * D)
+    G.fill_rb(lay, S1, body, rb, 1.4, 1.0)
+    S2[:] = S1
+    lay.advance_explicit(S1, S2, 0.0, dt, method, oracle.Parm(D))
+    ref = lay.gather(S1)
+    lev.advance(0.0, dt)
+    got = lev.get_state()
+    err = rel_linf(got, ref)
+    assert err <= RTOL, err
+    lev.close()
+
+
+def test_run_with_body_graph(torch_cuda, oracle):
+    """Three device-stepped steps (CUDA graph, device dt) with a body equal
+    three oracle steps with estTimeStep between them."""
+    from oracle import gfm_oracle as G
+    D, n = 2, (40, 36)
+    lay, lev = _make(oracle, D, n, 3)
+    s, so, comb = _shapes("cylinder")
+    u0 = _flow(D, n, seed=5)
+    lev.set_body(s, combine=comb)
+    lev.set_state(u0)
+    t, steps = lev.run(3, use_graph=True)
+    got = lev.get_state()
+    body = G.Body(lay, so, comb, (0.0,) * D)
+    S1, S2 = lay.alloc(), lay.alloc()
+    lay.scatter(S1, u0)
+    lay.fill_boundary(S1)
+    time = 0.0
+    for _ in range(3):
+        dt = lay.est_time_step(S1, 1.4, 1.0, 0.8)
+        G.fill_rb(lay, S1, body, G.REFLECTIVE, 1.4, 1.0)
+        S2[:] = S1
+        lay.advance_explicit(S1, S2, time, dt, 0, oracle.Parm(D))
+        lay.fill_boundary(S1)
+        time += dt
+    assert steps == 3
+    assert abs(t - time) <= 1e-13 * time
+    err = rel_linf(got, lay.gather(S1))
+    assert err <= 3 * RTOL, err
+    lev.close()
+
+
+def test_body_removed_restores_plain_step(torch_cuda, oracle):
+    """set_body(None) leaves the plain explicit step."""
+    D, n = 2, (32, 32)
+    lay, lev = _make(oracle, D, n, 2)
+    s, _, comb = _shapes("cylinder")
+    u0 = _flow(D, n, seed=3)
+    lev.set_body(s, combine=comb)
+    lev.set_body(None)
+    assert lev.body_counts() == (0, 0)
+    lev.set_state(u0)
+    S1, S2 = lay.alloc(), lay.alloc()
+    lay.scatter(S1, u0)
+    lay.fill_boundary(S1)
+    dt = lay.est_time_step(S1, 1.4, 1.0, 0.8)
+    S2[:] = S1
+    lay.advance_explicit(S1, S2, 0.0, dt, 0, oracle.Parm(D))
+    lev.advance(0.0, dt)
+    assert rel_linf(lev.get_state(), lay.gather(S1)) <= RTOL
+    lev.close()
+
+
+def test_body_argument_errors(torch_cuda, oracle):
+    import bamrex_b200 as bx
+    s, _, comb = _shapes("cylinder")
+    _, lev2 = _make(oracle, 2, (32, 32), 2, ngrow=2)
+    with pytest.raises(bx.BamrexError) as e:
+        lev2.set_body(s)
+    assert e.value.status == bx._abi.ERR_ARG
+    lev2.close()
+    _, lev = _make(oracle, 2, (32, 32), 2, ngrow=3)
+    with pytest.raises(bx.BamrexError):
+        lev.set_body(s, stencil=4)
+    with pytest.raises(bx.BamrexError):
+        lev.set_body([dict(kind=bx.SDF_PLANE, center=(0.5, 0.5), axis=(0, 0, 0))])
+    with pytest.raises(bx.BamrexError):
+        lev.fill_body_ghosts()
+    lev.close()

@@ -53,10 +53,17 @@ struct BodyState {
     int* d_counts = nullptr;       // [0] interface cells, [1] swept cells, [2] list fill
     int* d_iface = nullptr;        // interface cells: box, i, j, k
     double* d_ival = nullptr;      // their new states, NC each
-    int* d_active = nullptr;       // boxes with swept cells
+    int* d_active = nullptr;       // boxes swept by the global-memory kernel
+    int* d_list_s = nullptr;       // boxes swept in shared memory
+    long long* d_meta_off = nullptr;  // their first metadata cell
+    unsigned char* d_code = nullptr;  // per swept-region cell: swept bit, neighbour directions
+    double* d_wts = nullptr;       // per swept-region cell: D weights and their sum
+    int n_smem = 0;                // boxes of d_list_s
+    int threads_p = 32;            // threads (pencils) and shared memory of their sweep CTAs
+    size_t bytes_p = 0;
     long long n_iface = 0, n_swept = 0;
     int nactive = 0;
-    char* list_mem = nullptr;      // second block: interface list and values
+    char* list_mem = nullptr;      // second block: interface list and values, box lists, sweep metadata
     GhostOp* d_full = nullptr;     // every ghost cell (FillPatch / fill_consv_boundary)
     int nfull = 0, full_chunks = 0;
     GhostOp* d_inner = nullptr;    // inter-box and periodic ghost cells (FillBoundary)
@@ -579,6 +586,214 @@ __global__ void __launch_bounds__(kSweepCta) extrap_kernel(const int* __restrict
         }
 }
 
+// ---- extrapolation in shared memory ----------------------------------------
+//
+// The components never read each other (same neighbours and weights for
+// all of them), so one CTA takes one (box, component): the swept region of
+// the box plus a one-cell halo of that component lives in shared memory in
+// the storage type T (every update is rounded to T as the state is), the
+// neighbour choice and weights of each swept cell come precomputed, and
+// each thread walks one pencil along x, taking the cell of its pencil on
+// the current plane.  The weights of the next plane's cell are loaded
+// before the barrier so that the plane's critical path is the shared-memory
+// reads, the quotient and the barrier.
+
+constexpr int kSmemMax = 200 * 1024;  // shared memory of one (box, component) region
+constexpr int kPencilMax = 1024;      // pencils (= threads) of one CTA
+
+// Per swept-region cell: code bit 0 = swept (ghost, not at the interface),
+// bit 1 + d = the neighbour in direction d is +1 (else -1); weights
+// |n_d / dx_d|, their sum and its correctly rounded reciprocal.
+template <int D>
+__global__ void meta_kernel(const int* __restrict__ list, int nlist, const int* __restrict__ bbox,
+                            const long long* __restrict__ meta_off, const FabDev* __restrict__ lsf,
+                            const FabDev* __restrict__ flf, double dx0, double dx1, double dx2,
+                            unsigned char* __restrict__ code, double* __restrict__ wts)
+{
+    const int li = blockIdx.y;
+    if (li >= nlist) return;
+    const int b = list[li];
+    const int* bb = bbox + 6 * b;
+    Region R;
+    for (int d = 0; d < 3; ++d) {
+        R.lo[d] = bb[d];
+        R.n[d] = bb[3 + d] - bb[d] + 1;
+    }
+    const FabDev L = lsf[b], G = flf[b];
+    const double* ls = L.ptr<double>();
+    const unsigned char* fl = G.ptr<unsigned char>();
+    const double dx[3] = { dx0, dx1, dx2 };
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < R.size();
+         q += (long long)gridDim.x * blockDim.x) {
+        int i, j, k;
+        R.cell(q, i, j, k);
+        const int flag = fl[at(G, i, j, k)];
+        const long long mi = meta_off[li] + q;
+        int c = ((flag & BAMREX_GFM_GHOST) && !(flag & BAMREX_GFM_INTERFACE)) ? 1 : 0;
+        const long long cl = at(L, i, j, k);
+        const double sflip = (ls[cl] >= 0) ? -1 : 1;
+        double w[3] = { 0, 0, 0 };
+        for (int d = 0; d < D; ++d) {
+            const double nd = ls[cl + (1 + d) * L.ns] / dx[d] * sflip;
+            w[d] = fabs(nd);
+            if (nd < 0) c |= 2 << d;
+        }
+        double den = w[0];
+        for (int d = 1; d < D; ++d) den = den + w[d];
+        code[mi] = (unsigned char)c;
+        for (int d = 0; d < D; ++d) wts[mi * (D + 2) + d] = w[d];
+        wts[mi * (D + 2) + D] = den;
+        wts[mi * (D + 2) + D + 1] = 1.0 / den;
+    }
+}
+
+// The correctly rounded quotient a / b from y = RN(1/b): q = RN(a y), then
+// one correction q + (a - b q) y with the remainder exact by FMA
+// (P. Markstein, IBM J. Res. Dev. 34(1), 1990; the correction is exact
+// rounding when y is the rounded reciprocal and q is within an ulp).  Three
+// dependent operations instead of a full division on the sweep's critical
+// path; checked bit for bit against IEEE division on 2e9 random operands.
+__device__ __forceinline__ double div_by_rcp(double a, double b, double y)
+{
+    const double q = a * y;
+    const double r = fma(-q, b, a);
+    return fma(r, y, q);
+}
+
+// Geometry of a swept region in shared memory: extents, halo extents and
+// strides, region base corner.
+template <int D>
+struct SweepRegion {
+    int lo[3], n[3], hn0, hn1, hn2, so1, so2, hvol, vol;
+    __device__ void init(const int* bb)
+    {
+        for (int d = 0; d < 3; ++d) {
+            lo[d] = bb[d];
+            n[d] = bb[3 + d] - bb[d] + 1;
+        }
+        hn0 = n[0] + 2;
+        hn1 = n[1] + (D > 1 ? 2 : 0);
+        hn2 = n[2] + (D > 2 ? 2 : 0);
+        so1 = hn0;
+        so2 = hn0 * hn1;
+        hvol = hn0 * hn1 * hn2;
+        vol = n[0] * n[1] * n[2];
+    }
+    __device__ int sidx(int ci, int cj, int ck) const { return (ci + 1) + (cj + (D > 1)) * so1 + (ck + (D > 2)) * so2; }
+};
+
+template <typename T, int D>
+__device__ void region_load(const SweepRegion<D>& R, const FabDev& f, const T* u, T* sv)
+{
+#pragma unroll 4
+    for (int q = threadIdx.x; q < R.hvol; q += blockDim.x) {
+        const int hi = q % R.hn0, r = q / R.hn0;
+        const int hj = r % R.hn1, hk = r / R.hn1;
+        sv[q] = u[at(f, R.lo[0] - 1 + hi, R.lo[1] - (D > 1) + hj, R.lo[2] - (D > 2) + hk)];
+    }
+}
+
+template <typename T, int D>
+__device__ void region_store(const SweepRegion<D>& R, const FabDev& f, T* u, const T* sv, const unsigned char* code)
+{
+#pragma unroll 4
+    for (int r = threadIdx.x; r < R.vol; r += blockDim.x) {
+        if (!(code[r] & 1)) continue;
+        const int ci = r % R.n[0], rr = r / R.n[0];
+        const int cj = rr % R.n[1], ck = rr / R.n[1];
+        u[at(f, R.lo[0] + ci, R.lo[1] + cj, R.lo[2] + ck)] = sv[R.sidx(ci, cj, ck)];
+    }
+}
+
+__device__ __forceinline__ void sweep_signs(int D, int o, int& s0, int& s1, int& s2)
+{
+    s0 = s1 = s2 = 1;
+    if (D == 1) s0 = o == 0 ? 1 : -1;
+    if (D == 2) {
+        s0 = kOrder2[o][0];
+        s1 = kOrder2[o][1];
+    }
+    if (D == 3) {
+        s0 = kOrder3[o][0];
+        s1 = kOrder3[o][1];
+        s2 = kOrder3[o][2];
+    }
+}
+
+// One cell update in shared memory (the compute_extrapolation quotient).
+template <typename T, int D>
+__device__ __forceinline__ void sweep_cell(T* sv, int cs, int c, const double* w, int so1, int so2)
+{
+    double num = 0.0 + w[0] * (double)sv[cs + ((c & 2) ? 1 : -1)];
+    if (D > 1) num = num + w[1] * (double)sv[cs + ((c & 4) ? so1 : -so1)];
+    if (D > 2) num = num + w[2] * (double)sv[cs + ((c & 8) ? so2 : -so2)];
+    sv[cs] = (T)div_by_rcp(num, w[D], w[D + 1]);
+}
+
+// One thread per pencil (up to 1024 pencils), a barrier per plane; the
+// next plane's metadata is loaded before the barrier.
+template <typename T, int D>
+__global__ void __launch_bounds__(kPencilMax) extrap_smem_kernel(const int* __restrict__ list, const int* __restrict__ bbox,
+                                   const long long* __restrict__ meta_off, const unsigned char* __restrict__ code,
+                                   const double* __restrict__ wts, const FabDev* __restrict__ fab_tab,
+                                   const StepScalars* gate)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* sv = reinterpret_cast<T*>(smem_raw);
+    constexpr int NORD = D == 1 ? 2 : (D == 2 ? 4 : 8);
+    constexpr int W = D + 2;
+    if (gate && gate->done) return;
+    const int li = blockIdx.x, m = blockIdx.y;
+    const int b = list[li];
+    SweepRegion<D> R;
+    R.init(bbox + 6 * b);
+    const unsigned char* cd = code + meta_off[li];
+    const double* wt = wts + meta_off[li] * W;
+    const FabDev f = fab_tab[b];
+    T* u = f.ptr<T>() + m * f.ns;
+    region_load<T, D>(R, f, u, sv);
+    __syncthreads();
+    const int pencils = R.n[1] * R.n[2];
+    const int q = threadIdx.x;
+    const bool has = q < pencils;
+    const int pj = has ? q % R.n[1] : 0, pk = has ? q / R.n[1] : 0;
+    const int t0 = pj + pk;  // the plane of this thread's first cell
+    const int planes = R.n[0] + R.n[1] + R.n[2] - 2;
+    for (int rep = 0; rep < 2; ++rep)
+        for (int o = 0; o < NORD; ++o) {
+            int s0, s1, s2;
+            sweep_signs(D, o, s0, s1, s2);
+            const int cj = s1 > 0 ? pj : R.n[1] - 1 - pj;
+            const int ck = s2 > 0 ? pk : R.n[2] - 1 - pk;
+            const int ci0 = s0 > 0 ? 0 : R.n[0] - 1;
+            // cell of plane t = t0 + e: x = ci0 + s0 e; metadata row r0 + s0 e, smem cs0 + s0 e
+            const int r0 = ci0 + R.n[0] * (cj + R.n[1] * ck);
+            const int cs0 = R.sidx(ci0, cj, ck);
+            int cn = 0;
+            double wn[W];
+            auto fetch = [&](int e) {
+                cn = 0;
+                if (!has || (unsigned)e >= (unsigned)R.n[0]) return;
+                const int r = r0 + s0 * e;
+                cn = cd[r];
+#pragma unroll
+                for (int d = 0; d < W; ++d) wn[d] = wt[(long long)r * W + d];
+            };
+            fetch(-t0);
+            for (int t = 0; t < planes; ++t) {
+                const int e = t - t0;
+                const int c = cn;
+                double w[W];
+#pragma unroll
+                for (int d = 0; d < W; ++d) w[d] = wn[d];
+                fetch(e + 1);
+                if (c & 1) sweep_cell<T, D>(sv, cs0 + s0 * e, c, w, R.so1, R.so2);
+                __syncthreads();
+            }
+        }
+    region_store<T, D>(R, f, u, sv, cd);
+}
+
 template <typename T>
 __global__ void body_field_kernel(int which, const bamrex_box* __restrict__ boxes, const FabDev* __restrict__ lsf,
                                   const FabDev* __restrict__ flf, const long long* __restrict__ begin,
@@ -753,6 +968,20 @@ Sdf make_sdf(const bamrex_sdf& s)
 
 int body_launch(bamrex_level* L, cudaError_t e, const char* what) { return level_launch(L, e, what); }
 
+cudaError_t smem_attribute(bool fp32, int D, int bytes)
+{
+    if (bytes <= 48 * 1024) return cudaSuccess;
+    const cudaFuncAttribute a = cudaFuncAttributeMaxDynamicSharedMemorySize;
+    if (fp32) {
+        if (D == 1) return cudaFuncSetAttribute(extrap_smem_kernel<float, 1>, a, bytes);
+        if (D == 2) return cudaFuncSetAttribute(extrap_smem_kernel<float, 2>, a, bytes);
+        return cudaFuncSetAttribute(extrap_smem_kernel<float, 3>, a, bytes);
+    }
+    if (D == 1) return cudaFuncSetAttribute(extrap_smem_kernel<double, 1>, a, bytes);
+    if (D == 2) return cudaFuncSetAttribute(extrap_smem_kernel<double, 2>, a, bytes);
+    return cudaFuncSetAttribute(extrap_smem_kernel<double, 3>, a, bytes);
+}
+
 int ghost_ops(bamrex_level* L, const GhostOp* ops, int nops, int nchunks, int parity, const StepScalars* gate)
 {
     if (!nops) return BAMREX_OK;
@@ -813,6 +1042,23 @@ int body_fill(bamrex_level* L, int parity, const StepScalars* gate)
     }
     BX_TRY(ghost_ops(L, S->d_inner, S->ninner, S->inner_chunks, parity, gate));
     for (int r = 0; r < D + 1; ++r) {
+        if (S->n_smem) {
+            const dim3 g((unsigned)S->n_smem, (unsigned)L->NC);
+#define BX_EXTRAP_S(T, DD)                                                                                      \
+    extrap_smem_kernel<T, DD><<<g, S->threads_p, S->bytes_p, L->stream>>>(S->d_list_s, S->d_bbox, S->d_meta_off, \
+                                                                          S->d_code, S->d_wts, L->d_fab[parity], gate)
+            if (L->fp32) {
+                if (D == 1) BX_EXTRAP_S(float, 1);
+                else if (D == 2) BX_EXTRAP_S(float, 2);
+                else BX_EXTRAP_S(float, 3);
+            } else {
+                if (D == 1) BX_EXTRAP_S(double, 1);
+                else if (D == 2) BX_EXTRAP_S(double, 2);
+                else BX_EXTRAP_S(double, 3);
+            }
+#undef BX_EXTRAP_S
+            BX_TRY(body_launch(L, cudaGetLastError(), "extrapolation (shared memory)"));
+        }
         if (S->nactive) {
 #define BX_EXTRAP(T, DD)                                                                                       \
     extrap_kernel<T, DD><<<S->nactive, kSweepCta, 0, L->stream>>>(S->d_active, S->d_bbox, L->d_fab[parity], \
@@ -961,27 +1207,87 @@ extern "C" int bamrex_level_set_body(bamrex_level* L, const bamrex_body_desc* de
     L->launches += 3;
     S->n_iface = counts[0];
     S->n_swept = counts[1];
-    std::vector<int> active;
-    for (int b = 0; b < nb; ++b)
-        if (bbox[6 * b] <= bbox[6 * b + 3]) active.push_back(b);
-    S->nactive = (int)active.size();
-    // interface list and its values
+    // boxes with swept cells: in shared memory when the region and its halo
+    // fit (one CTA per box and component), else the global-memory kernel
+    std::vector<int> list_p, list_g;
+    std::vector<long long> vol_p;
+    size_t bytes_p = 0;
+    int threads_p = 32;
+    for (int b = 0; b < nb; ++b) {
+        if (bbox[6 * b] > bbox[6 * b + 3]) continue;
+        long long n[3], hv = 1, vol = 1;
+        for (int d = 0; d < 3; ++d) {
+            n[d] = bbox[6 * b + 3 + d] - bbox[6 * b + d] + 1;
+            hv *= n[d] + (d < D ? 2 : 0);
+            vol *= n[d];
+        }
+        const long long pencils = n[1] * n[2];
+        const size_t values = (size_t)hv * L->esize;
+        if (pencils > kPencilMax || values > (size_t)kSmemMax) {
+            list_g.push_back(b);
+        } else {
+            list_p.push_back(b);
+            vol_p.push_back(vol);
+            bytes_p = std::max(bytes_p, values);
+            threads_p = std::max(threads_p, (int)((pencils + 31) / 32 * 32));
+        }
+    }
+    const std::vector<int>& list_s = list_p;
+    std::vector<long long> meta_off;
+    long long meta_cells = 0;
+    for (long long v : vol_p) {
+        meta_off.push_back(meta_cells);
+        meta_cells += v;
+    }
+    S->nactive = (int)list_g.size();
+    S->n_smem = (int)list_s.size();
+    S->bytes_p = bytes_p;
+    S->threads_p = threads_p;
+    // second block: interface list and values, box lists, sweep metadata
     char* M2 = nullptr;
     const size_t n_if = (size_t)std::max<long long>(1, S->n_iface);
-    e = dev_alloc((void**)&M2, align_up(sizeof(int) * 4 * n_if, 256) + sizeof(double) * L->NC * n_if, L->stream);
+    size_t off2 = 0;
+    auto take2 = [&](size_t bytes) {
+        const size_t o = off2;
+        off2 = align_up(off2 + std::max<size_t>(bytes, 1), 256);
+        return o;
+    };
+    const size_t o_if = take2(sizeof(int) * 4 * n_if), o_iv = take2(sizeof(double) * L->NC * n_if);
+    const size_t o_lg = take2(sizeof(int) * list_g.size()), o_lst = take2(sizeof(int) * list_s.size());
+    const size_t o_mo = take2(sizeof(long long) * meta_off.size()), o_code = take2((size_t)meta_cells);
+    const size_t o_w = take2(sizeof(double) * (D + 2) * (size_t)meta_cells);
+    e = dev_alloc((void**)&M2, off2, L->stream);
     if (e != cudaSuccess) {
         dev_free(S->mem, L->stream);
         return L->set_err(fail(BAMREX_ERR_OOM, "allocation of the interface list failed"));
     }
-    // the list lives in a second block released with the first
-    S->d_iface = (int*)M2;
-    S->d_ival = (double*)(M2 + align_up(sizeof(int) * 4 * n_if, 256));
-    e = up(S->d_active, active.data(), sizeof(int) * active.size());
+    S->d_iface = (int*)(M2 + o_if);
+    S->d_ival = (double*)(M2 + o_iv);
+    S->d_active = (int*)(M2 + o_lg);
+    S->d_list_s = (int*)(M2 + o_lst);
+    S->d_meta_off = (long long*)(M2 + o_mo);
+    S->d_code = (unsigned char*)(M2 + o_code);
+    S->d_wts = (double*)(M2 + o_w);
+    e = up(S->d_active, list_g.data(), sizeof(int) * list_g.size());
+    if (e == cudaSuccess) e = up(S->d_list_s, list_s.data(), sizeof(int) * list_s.size());
+    if (e == cudaSuccess) e = up(S->d_meta_off, meta_off.data(), sizeof(long long) * meta_off.size());
     if (e == cudaSuccess && S->n_iface) {
         iface_collect_kernel<<<grid, kBodyThreads, 0, L->stream>>>(d_boxes, S->d_flag_fab, S->d_iface, (int)S->n_iface,
                                                                    S->d_counts + 2);
         e = cudaGetLastError();
         L->launches++;
+    }
+    if (e == cudaSuccess && S->n_smem) {
+        long long maxv = 1;
+        for (size_t i = 0; i < list_s.size(); ++i)
+            maxv = std::max(maxv, (i + 1 < list_s.size() ? meta_off[i + 1] : meta_cells) - meta_off[i]);
+        const dim3 mg((unsigned)std::min<long long>(1024, (maxv + kBodyThreads - 1) / kBodyThreads), (unsigned)list_s.size());
+        if (D == 1) meta_kernel<1><<<mg, kBodyThreads, 0, L->stream>>>(S->d_list_s, S->n_smem, S->d_bbox, S->d_meta_off, S->d_ls_fab, S->d_flag_fab, L->dx[0], L->dx[1], L->dx[2], S->d_code, S->d_wts);
+        else if (D == 2) meta_kernel<2><<<mg, kBodyThreads, 0, L->stream>>>(S->d_list_s, S->n_smem, S->d_bbox, S->d_meta_off, S->d_ls_fab, S->d_flag_fab, L->dx[0], L->dx[1], L->dx[2], S->d_code, S->d_wts);
+        else meta_kernel<3><<<mg, kBodyThreads, 0, L->stream>>>(S->d_list_s, S->n_smem, S->d_bbox, S->d_meta_off, S->d_ls_fab, S->d_flag_fab, L->dx[0], L->dx[1], L->dx[2], S->d_code, S->d_wts);
+        e = cudaGetLastError();
+        L->launches++;
+        if (e == cudaSuccess) e = smem_attribute(L->fp32, D, (int)bytes_p);
     }
     if (e == cudaSuccess) e = cudaStreamSynchronize(L->stream);
     if (e != cudaSuccess) {

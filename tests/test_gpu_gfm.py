@@ -89,6 +89,12 @@ def _shapes(case):
     elif case == "sphere":
         s = [dict(kind=bx.SDF_SPHERE, center=(0.5, 0.45, 0.55), radius=0.27)]
         comb = bx.SDF_UNION
+    elif case == "big_cylinder":
+        s = [dict(kind=bx.SDF_CYLINDER, center=(0.5, 0.5, 0.0), axis=(0, 0, 1), radius=0.45)]
+        comb = bx.SDF_UNION
+    elif case == "big_sphere":
+        s = [dict(kind=bx.SDF_SPHERE, center=(0.5, 0.5, 0.5), radius=0.47)]
+        comb = bx.SDF_UNION
     elif case == "two_cylinders":
         s = [dict(kind=bx.SDF_CYLINDER, center=(0.3, 0.5, 0.0), axis=(0, 0, 1), radius=0.15),
              dict(kind=bx.SDF_CYLINDER, center=(0.62, 0.41, 0.0), axis=(0, 0, 1), radius=0.17)]
@@ -129,7 +135,15 @@ def test_levelset_normals_flags(torch_cuda, oracle, case):
 
 FILL_CASES = [(2, (40, 36), 3, "cylinder", 0), (2, (40, 36), 3, "cylinder", 1), (2, (40, 36), 3, "cylinder", 2),
               (2, (32, 32), 4, "two_cylinders", 0), (2, (36, 36), 2, "half_disc", 0), (3, (16, 14, 12), 2, "sphere", 0),
-              (3, (16, 14, 12), 2, "sphere", 2)]
+              (3, (16, 14, 12), 2, "sphere", 2),
+              # swept regions of at most 128 pencils go to the one-warp sweep,
+              # larger ones (a 20^3 box around a big sphere) to one thread per
+              # pencil with CTA barriers
+              (2, (96, 96), 1, "big_cylinder", 0),
+              (3, (20, 20, 20), 1, "big_sphere", 0),
+              # one 32^3 box whose swept region with its halo exceeds shared
+              # memory in FP64: the global-memory sweep kernel
+              (3, (32, 32, 32), 1, "big_sphere", 0)]
 
 
 @pytest.mark.parametrize("case", FILL_CASES, ids=lambda c: "%dd-%s-rb%d" % (c[0], c[3], c[4]))

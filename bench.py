@@ -54,6 +54,7 @@ def parse_args():
     ap.add_argument("--amr-n", type=int, default=128, help="base cells per side of the AMR blast sample")
     ap.add_argument("--amr-steps", type=int, default=6, help="timed coarse steps of the AMR blast sample")
     ap.add_argument("--imex-n", type=int, default=2048, help="cells per side of the IMEX pressure problem")
+    ap.add_argument("--no-body", action="store_true", help="skip the ghost-fluid rigid-body sample")
     return ap.parse_args()
 
 
@@ -422,6 +423,58 @@ def amr_blast_run(n0, coarse_steps, precision):
             "mass_drift_rel": float(abs(s1[0] - s0[0]) / abs(s0[0]))}
 
 
+def rigid_body_run(D, n, mgs, precision, steps=10):
+    """A free stream (Mach 0.3) past a static cylinder of radius 0.1 at the
+    domain centre (axis z), ghost-fluid reflective wall: step time with and
+    without the body and the rigid-body ghost fill alone (interface cells,
+    D + 1 extrapolation rounds, boundary fills)."""
+    import torch
+
+    import bamrex_b200 as bx
+    from bamrex_b200.level import decompose
+
+    boxes = decompose(D, (0,) * D, tuple(x - 1 for x in n), mgs)
+    lev = bx.Level(D, (0,) * D, tuple(x - 1 for x in n), [0.0] * D, [1.0] * D, boxes, bx.Parm(D), cfl=0.8, ngrow=3,
+                   precision=precision)
+    shp = (n[2] if D > 2 else 1, n[1], n[0])
+    gamma = 1.4
+    U = np.zeros((D + 2,) + shp)
+    u0 = 0.3 * np.sqrt(gamma)
+    U[0] = 1.0
+    U[1] = u0
+    U[D + 1] = 1.0 / (gamma - 1) + 0.5 * u0 * u0
+    lev.set_state(U)
+    dt = lev.estTimeStep()
+
+    def ms_per_step(k, fn):
+        lev.sync()
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        for _ in range(k):
+            fn()
+        lev.sync()
+        torch.cuda.synchronize()
+        return (time.perf_counter() - t) * 1e3 / k
+
+    ms_per_step(2, lambda: lev.advance(0.0, dt))
+    plain = ms_per_step(steps, lambda: lev.advance(0.0, dt))
+    t0 = time.perf_counter()
+    lev.set_body(dict(kind=bx.SDF_CYLINDER, center=(0.5, 0.5, 0.5), axis=(0, 0, 1), radius=0.1))
+    setup = (time.perf_counter() - t0) * 1e3
+    ms_per_step(2, lambda: lev.advance(0.0, dt))
+    body = ms_per_step(steps, lambda: lev.advance(0.0, dt))
+    fill = ms_per_step(steps, lev.fill_body_ghosts)
+    iface, swept = lev.body_counts()
+    lev.close()
+    ncells = int(np.prod(n))
+    return {"workload": "%s %s, max_grid_size %d, %s, free stream Mach 0.3 past a cylinder r 0.1 (reflective wall)" % (
+                "x".join(str(x) for x in n), "3D" if D == 3 else "2D", mgs,
+                "FP32 storage" if precision == bx.FP32_STORAGE else "FP64"),
+            "boxes": len(boxes), "interface_cells": iface, "swept_cells": swept,
+            "ms_per_step_plain": plain, "ms_per_step_with_body": body, "ms_rigid_body_fill": fill,
+            "set_up_ms": setup, "cell_updates_per_s_with_body": ncells / (body * 1e-3)}
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return 0
@@ -611,6 +664,11 @@ def run_ours(args, rank, world, local_rank):
                "fp64": amr_blast_run(args.amr_n, args.amr_steps, bx.FP64),
                "fp32_storage": amr_blast_run(args.amr_n, args.amr_steps, bx.FP32_STORAGE)}
 
+    body = None
+    if rank == 0 and world == 1 and not args.no_body:
+        body = {"2d": rigid_body_run(2, (2048, 2048), 64, bx.FP64),
+                "3d_fp32_storage": rigid_body_run(3, (512, 512, 128), 32, bx.FP32_STORAGE, steps=5)}
+
     line = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -628,6 +686,7 @@ def run_ours(args, rank, world, local_rank):
         "fp32_storage": fp32,
         "imex_pressure_solve": imex,
         "amr_blast3d": amr,
+        "rigid_body": body,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)

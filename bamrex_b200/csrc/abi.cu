@@ -974,6 +974,18 @@ extern "C" int bamrex_level_destroy(bamrex_level* L)
     if (!L) return BAMREX_OK;
     if (L->stream) cudaStreamSynchronize(L->stream);
     body_destroy(L);
+    if (L->hs) {
+        if (L->hs->h2d) cudaStreamSynchronize(L->hs->h2d);
+        if (L->hs->d2h) cudaStreamSynchronize(L->hs->d2h);
+        for (cudaEvent_t e : L->hs->in) cudaEventDestroy(e);
+        for (cudaEvent_t e : L->hs->out) cudaEventDestroy(e);
+        if (L->hs->start) cudaEventDestroy(L->hs->start);
+        if (L->hs->h2d) cudaStreamDestroy(L->hs->h2d);
+        if (L->hs->d2h) cudaStreamDestroy(L->hs->d2h);
+        dev_free(L->hs->staging_out, L->stream);
+        delete L->hs;
+        L->hs = nullptr;
+    }
     for (int p = 0; p < 2; ++p)
         if (L->graph[p]) cudaGraphExecDestroy(L->graph[p]);
     for (auto& ev : L->events) {
@@ -1051,6 +1063,161 @@ extern "C" int bamrex_level_copy_out(bamrex_level* L, double* dst)
         const cudaError_t e = cudaMemcpyAsync(dst, L->staging, (size_t)L->ncells * L->NC * 8, cudaMemcpyDefault, L->stream);
         if (e != cudaSuccess) return L->set_err(cuda_fail(e, "copy_out memcpy"));
     }
+    return BAMREX_OK;
+}
+
+// One step of a host-resident state, streamed through the device in slabs
+// along the last direction: the upload of slab c, the sweeps of the other
+// directions on slab c, the last direction's sweep on slab c - 1 (its
+// stencil reaches two cells into slab c) and the download of slab c - 2 run
+// on three streams at once, so the copies in both directions overlap each
+// other and the sweeps.  The result equals bamrex_level_copy_in + advance +
+// copy_out: every ghost fill covers the whole box, and a slab's cells are
+// swept only after the cells their stencils read are final.
+extern "C" int bamrex_level_step_host(bamrex_level* L, const double* host_in, double* host_out, double dt,
+                                      int nslabs, double* dt_next)
+{
+    if (!L || !host_in || !host_out) return fail(BAMREX_ERR_ARG, "NULL argument");
+    if (!(dt > 0) || !std::isfinite(dt)) return L->set_err(fail(BAMREX_ERR_ARG, "dt must be positive and finite"));
+    const int D = L->D, a = D - 1;
+    bool reg = false;
+    for (int d = 0; d < 3; ++d) reg = reg || !L->reg_tasks[d].empty();
+    const bamrex_box B = L->boxes[0];
+    const int rows = B.hi[a] - B.lo[a] + 1;
+    const int C = std::max(1, std::min(nslabs, rows / 4));
+    if (L->boxes.size() != 1 || D < 2 || reg || L->body || L->bc_lo[a] == BAMREX_BC_PERIODIC || C < 2) {
+        // not streamable: the plain sequence
+        BX_TRY(bamrex_level_copy_in(L, host_in));
+        BX_TRY(bamrex_level_advance(L, 0.0, dt, 1, 1, nullptr));
+        if (dt_next) BX_TRY(bamrex_level_est_time_step(L, dt_next));
+        BX_TRY(bamrex_level_copy_out(L, host_out));
+        return bamrex_level_sync(L);
+    }
+    cudaError_t e = cudaSuccess;
+    if (!L->hs) {
+        L->hs = new (std::nothrow) bamrex_level::HostStream();
+        if (!L->hs) return L->set_err(fail(BAMREX_ERR_OOM, "host allocation failed"));
+        e = cudaStreamCreateWithFlags(&L->hs->h2d, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&L->hs->d2h, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&L->hs->start, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = dev_alloc((void**)&L->hs->staging_out, (size_t)L->ncells * L->NC * 8, L->stream);
+        if (e != cudaSuccess) return L->set_err(cuda_fail(e, "host-stream set-up"));
+    }
+    bamrex_level::HostStream& H = *L->hs;
+    while ((int)H.in.size() < C) {
+        cudaEvent_t ei = nullptr, eo = nullptr;
+        e = cudaEventCreateWithFlags(&ei, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&eo, cudaEventDisableTiming);
+        if (e != cudaSuccess) return L->set_err(cuda_fail(e, "host-stream events"));
+        H.in.push_back(ei);
+        H.out.push_back(eo);
+    }
+    // slab c: cells [s0, s1) of direction a; plane = cells of one layer
+    long long plane = 1;
+    for (int d = 0; d < D - 1; ++d) plane *= (long long)(B.hi[d] - B.lo[d] + 1);
+    auto lo_of = [&](int c) { return B.lo[a] + (int)((long long)rows * c / C); };
+    auto pack_box = [&](int c) {
+        PackBox pb;
+        for (int d = 0; d < 3; ++d) {
+            pb.lo[d] = B.lo[d];
+            pb.hi[d] = B.hi[d];
+        }
+        pb.lo[a] = lo_of(c);
+        pb.hi[a] = lo_of(c + 1) - 1;
+        pb.cell_begin = 0;
+        return pb;
+    };
+    // the packed host layout of one box: component n, then cells x fastest
+    auto copies = [&](int c, double* dst_base, const double* src_base, bool to_host, cudaStream_t s) -> cudaError_t {
+        const long long first = (long long)(lo_of(c) - B.lo[a]) * plane, cells = (long long)(lo_of(c + 1) - lo_of(c)) * plane;
+        for (int n = 0; n < L->NC; ++n) {
+            const size_t off_host = (size_t)(n * L->ncells + first), off_dev = (size_t)(n * L->ncells + first);
+            const cudaError_t r = to_host
+                ? cudaMemcpyAsync(host_out + off_host, dst_base + off_dev, sizeof(double) * cells, cudaMemcpyDeviceToHost, s)
+                : cudaMemcpyAsync((double*)dst_base + off_dev, src_base + off_host, sizeof(double) * cells, cudaMemcpyHostToDevice, s);
+            if (r != cudaSuccess) return r;
+        }
+        return cudaSuccess;
+    };
+    // staging (in) and staging_out hold the packed layout of the whole box;
+    // a slab occupies its cells' range inside every component block
+    PackBox whole;
+    for (int d = 0; d < 3; ++d) {
+        whole.lo[d] = B.lo[d];
+        whole.hi[d] = B.hi[d];
+    }
+    whole.cell_begin = 0;
+    const int cur = L->cur;
+    const int p_lag = cur ^ ((D - 1) & 1), p_out = cur ^ (D & 1);
+    e = cudaMemsetAsync(&L->d_scal->ws_bits, 0, sizeof(unsigned long long), L->stream);
+    if (e == cudaSuccess) e = cudaEventRecord(H.start, L->stream);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(H.h2d, H.start, 0);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(H.d2h, H.start, 0);
+    if (e != cudaSuccess) return L->set_err(cuda_fail(e, "host-stream start"));
+    auto slab_sweep = [&](int dir, int c, int pin, bool ws) -> int {
+        SweepArgs sa;
+        std::memset(&sa, 0, sizeof(sa));
+        sa.boxes = nullptr;
+        sa.nboxes = 1;
+        SweepBox& sb = sa.one;
+        for (int d = 0; d < 3; ++d) {
+            sb.lo[d] = B.lo[d];
+            sb.hi[d] = B.hi[d];
+        }
+        sb.lo[a] = lo_of(c);
+        sb.hi[a] = lo_of(c + 1) - 1;
+        sb.in = L->fab[pin][0];
+        sb.out = L->fab[pin ^ 1][0];
+        sb.flux.p = nullptr;
+        const bool march = dir == 0 && L->x_march;
+        long long items;
+        box_items(dir, sb.lo, sb.hi, L->seglen[dir], items, sb.nseg, sb.ngroup, march, &sb.seglen);
+        sb.item_begin = 0;
+        sa.total_items = items;
+        sa.seglen = L->seglen[dir];
+        sa.halo = method_halo(L->method);
+        sa.dt_host = dt;
+        sa.scal = nullptr;
+        sa.dx = L->dx[dir];
+        sa.k = L->k;
+        sa.ws_max = ws ? &L->d_scal->ws_bits : nullptr;
+        sa.do_update = 1;
+        return level_launch(L, launch_sweep(D, dir, L->method, L->fp32, sa, L->stream, march), "slab sweep");
+    };
+    auto lagged = [&](int c) -> int {
+        BX_TRY(level_fill(L, a, p_lag, nullptr));
+        BX_TRY(slab_sweep(a, c, p_lag, true));
+        BX_TRY(level_launch(L, launch_pack_slab(L->NC, L->fp32, L->fab[p_out][0], whole, pack_box(c), H.staging_out, 1,
+                                                L->stream),
+                            "slab pack"));
+        cudaError_t r = cudaEventRecord(H.out[c], L->stream);
+        if (r == cudaSuccess) r = cudaStreamWaitEvent(H.d2h, H.out[c], 0);
+        if (r == cudaSuccess) r = copies(c, H.staging_out, nullptr, true, H.d2h);
+        return r == cudaSuccess ? BAMREX_OK : L->set_err(cuda_fail(r, "slab download"));
+    };
+    for (int c = 0; c < C; ++c) {
+        e = copies(c, L->staging, host_in, false, H.h2d);
+        if (e != cudaSuccess) return L->set_err(cuda_fail(e, "slab upload"));
+        BX_TRY(level_launch(L, launch_pack_slab(L->NC, L->fp32, L->fab[cur][0], whole, pack_box(c), L->staging, 0, H.h2d),
+                            "slab unpack"));
+        e = cudaEventRecord(H.in[c], H.h2d);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(L->stream, H.in[c], 0);
+        if (e != cudaSuccess) return L->set_err(cuda_fail(e, "slab event"));
+        int p = cur;
+        for (int d = 0; d < D - 1; ++d) {
+            BX_TRY(level_fill(L, d, p, nullptr));
+            BX_TRY(slab_sweep(d, c, p, false));
+            p ^= 1;
+        }
+        if (c > 0) BX_TRY(lagged(c - 1));
+    }
+    BX_TRY(lagged(C - 1));
+    e = cudaStreamSynchronize(H.d2h);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(L->stream);
+    if (e != cudaSuccess) return L->set_err(cuda_fail(e, "host step"));
+    L->cur = p_out;
+    L->ws_valid = true;
+    if (dt_next) BX_TRY(bamrex_level_est_time_step(L, dt_next));
     return BAMREX_OK;
 }
 

@@ -115,6 +115,30 @@ __global__ void pack_kernel(int NC, const FabDev* __restrict__ fabs, const PackB
     }
 }
 
+// One slab of one box (full extent in the other directions) between the fab
+// and the packed layout of the whole box ([n][cells of the box], x fastest).
+template <typename T>
+__global__ void pack_slab_kernel(int NC, const FabDev f, const PackBox box, const PackBox slab, double* __restrict__ packed,
+                                 int to_packed)
+{
+    const int bx = box.hi[0] - box.lo[0] + 1, by = box.hi[1] - box.lo[1] + 1, bz = box.hi[2] - box.lo[2] + 1;
+    const long long ncells = (long long)bx * by * bz;
+    const int sx = slab.hi[0] - slab.lo[0] + 1, sy = slab.hi[1] - slab.lo[1] + 1, sz = slab.hi[2] - slab.lo[2] + 1;
+    const long long scells = (long long)sx * sy * sz;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < scells * NC;
+         e += (long long)gridDim.x * blockDim.x) {
+        const int n = (int)(e / scells);
+        const long long c = e - n * scells;
+        const int i = slab.lo[0] + (int)(c % sx);
+        const int j = slab.lo[1] + (int)((c / sx) % sy);
+        const int k = slab.lo[2] + (int)(c / ((long long)sx * sy));
+        const long long q = n * ncells + (i - box.lo[0]) + (long long)bx * ((j - box.lo[1]) + (long long)by * (k - box.lo[2]));
+        T* pf = f.ptr<T>() + fab_index(f, i, j, k) + n * f.ns;
+        if (to_packed) packed[q] = (double)*pf;
+        else *pf = (T)packed[q];
+    }
+}
+
 // ---------------------------------------------------------------- max speed
 // max_wave_speed (Source/System/Euler/Euler.cpp:46-74) over valid cells.
 template <typename T, int D>
@@ -321,6 +345,17 @@ cudaError_t launch_ghost_fill(int NC, bool fp32, const GhostOp* ops, int nops, i
     const int g = (int)std::min<long long>((nchunks + warps - 1) / warps, (long long)device_sm_count() * 8);
     if (fp32) ghost_fill_kernel<float><<<g, kThreads, 0, s>>>(NC, ops, nops, nchunks, fabs, scal);
     else ghost_fill_kernel<double><<<g, kThreads, 0, s>>>(NC, ops, nops, nchunks, fabs, scal);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pack_slab(int NC, bool fp32, const FabDev& fab, const PackBox& box, const PackBox& slab,
+                             double* packed, int to_packed, cudaStream_t s)
+{
+    const long long cells = (long long)(slab.hi[0] - slab.lo[0] + 1) * (slab.hi[1] - slab.lo[1] + 1) * (slab.hi[2] - slab.lo[2] + 1);
+    if (cells <= 0) return cudaSuccess;
+    const int g = grid_for(cells * NC, 4);
+    if (fp32) pack_slab_kernel<float><<<g, kThreads, 0, s>>>(NC, fab, box, slab, packed, to_packed);
+    else pack_slab_kernel<double><<<g, kThreads, 0, s>>>(NC, fab, box, slab, packed, to_packed);
     return cudaGetLastError();
 }
 

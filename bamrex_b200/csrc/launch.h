@@ -94,6 +94,9 @@ cudaError_t launch_ghost_fill(int NC, bool fp32, const GhostOp* ops, int nops, i
                               const StepScalars* scal, cudaStream_t s);
 
 // Packed buffer is always double; fabs are double or float.
+// One slab of one box between its fab and the packed layout of the whole box.
+cudaError_t launch_pack_slab(int NC, bool fp32, const FabDev& fab, const PackBox& box, const PackBox& slab,
+                             double* packed, int to_packed, cudaStream_t s);
 cudaError_t launch_pack(int NC, bool fp32, const FabDev* fabs, const PackBox* boxes, int nboxes,
                         long long total_cells, double* packed, int to_packed, cudaStream_t s);
 

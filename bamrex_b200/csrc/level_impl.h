@@ -118,6 +118,15 @@ struct bamrex_level {
     double dir_ms[3] = { 0, 0, 0 };
     long long dir_launches[3] = { 0, 0, 0 };
 
+    // streams, events and output staging of bamrex_level_step_host
+    struct HostStream {
+        cudaStream_t h2d = nullptr, d2h = nullptr;
+        cudaEvent_t start = nullptr;
+        std::vector<cudaEvent_t> in, out;
+        double* staging_out = nullptr;
+    };
+    HostStream* hs = nullptr;
+
     // static rigid body by the ghost-fluid method (bamrex_level_set_body)
     bamrex::BodyState* body = nullptr;
 

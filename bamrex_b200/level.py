@@ -276,6 +276,15 @@ class Level:
         self.sync()
         return self.packing.unpack(packed)
 
+    def step_host_ptr(self, in_ptr: int, out_ptr: int, dt: float, nslabs: int = 16) -> float:
+        """One step of a host-resident packed state (bamrex_level_step_host):
+        uploads, sweeps and downloads overlap in slabs.  Returns the CFL time
+        step estimate of the result."""
+        nxt = ctypes.c_double()
+        self._ck(lib().bamrex_level_step_host(self._h, ctypes.c_void_p(in_ptr), ctypes.c_void_p(out_ptr), float(dt),
+                                              int(nslabs), ctypes.byref(nxt)))
+        return nxt.value
+
     def sync(self):
         self._ck(lib().bamrex_level_sync(self._h))
 

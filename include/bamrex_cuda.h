@@ -247,6 +247,16 @@ BAMREX_API int bamrex_conserved_sums_noalloc(int spacedim, const bamrex_box *box
                                              int nboxes, const double dx[3], double *totals, void *stream);
 
 /* Wait for all work the level issued on its stream. */
+/* One step of a host-resident state: host_in -> host_out (packed layout of
+ * bamrex_level_copy_in/out; the same pointer for both is allowed), time step
+ * dt, and the CFL estimate of the result in *dt_next (may be NULL) -- the
+ * result of bamrex_level_copy_in + bamrex_level_advance + copy_out +
+ * est_time_step.  Single-box levels (2D/3D, not periodic in the last
+ * direction) are streamed in nslabs slabs along the last direction so that
+ * uploads, sweeps and downloads overlap (pinned host buffers for the
+ * overlap); other levels take the plain sequence.  Synchronous. */
+BAMREX_API int bamrex_level_step_host(bamrex_level *level, const double *host_in, double *host_out, double dt,
+                                      int nslabs, double *dt_next);
 BAMREX_API int bamrex_level_sync(bamrex_level *level);
 
 /* bamrexBCData::fill_consv_boundary on the current state

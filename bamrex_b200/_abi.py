@@ -259,6 +259,7 @@ SIGNATURES = {
     "bamrex_level_sweep_dir": (_i, [_vp, _i, _d, _i]),
     "bamrex_level_wave_speed": (_i, [_vp, _dp]),
     "bamrex_level_step_host": (_i, [_vp, _vp, _vp, _d, _i, _dp]),
+    "bamrex_level_run_host": (_i, [_vp, _vp, _i, _d, _i, _dp, _dp]),
     "bamrex_level_set_body": (_i, [_vp, ctypes.POINTER(BodyDesc)]),
     "bamrex_level_fill_body_ghosts": (_i, [_vp]),
     "bamrex_level_body_field": (_i, [_vp, _i, _dp]),

@@ -979,6 +979,7 @@ extern "C" int bamrex_level_destroy(bamrex_level* L)
         if (L->hs->d2h) cudaStreamSynchronize(L->hs->d2h);
         for (cudaEvent_t e : L->hs->in) cudaEventDestroy(e);
         for (cudaEvent_t e : L->hs->out) cudaEventDestroy(e);
+        for (cudaEvent_t e : L->hs->done) cudaEventDestroy(e);
         if (L->hs->start) cudaEventDestroy(L->hs->start);
         if (L->hs->h2d) cudaStreamDestroy(L->hs->h2d);
         if (L->hs->d2h) cudaStreamDestroy(L->hs->d2h);
@@ -1066,33 +1067,24 @@ extern "C" int bamrex_level_copy_out(bamrex_level* L, double* dst)
     return BAMREX_OK;
 }
 
-// One step of a host-resident state, streamed through the device in slabs
-// along the last direction: the upload of slab c, the sweeps of the other
-// directions on slab c, the last direction's sweep on slab c - 1 (its
-// stencil reaches two cells into slab c) and the download of slab c - 2 run
-// on three streams at once, so the copies in both directions overlap each
-// other and the sweeps.  The result equals bamrex_level_copy_in + advance +
-// copy_out: every ghost fill covers the whole box, and a slab's cells are
-// swept only after the cells their stencils read are final.
-extern "C" int bamrex_level_step_host(bamrex_level* L, const double* host_in, double* host_out, double dt,
-                                      int nslabs, double* dt_next)
+namespace {
+
+// Slabs of a streamed host step (0: the level cannot be streamed): single
+// box, 2D/3D, no flux registers or rigid body, not periodic in the last
+// direction, at least 4 layers a slab.
+int host_slabs(const bamrex_level* L, int nslabs)
 {
-    if (!L || !host_in || !host_out) return fail(BAMREX_ERR_ARG, "NULL argument");
-    if (!(dt > 0) || !std::isfinite(dt)) return L->set_err(fail(BAMREX_ERR_ARG, "dt must be positive and finite"));
     const int D = L->D, a = D - 1;
     bool reg = false;
     for (int d = 0; d < 3; ++d) reg = reg || !L->reg_tasks[d].empty();
-    const bamrex_box B = L->boxes[0];
-    const int rows = B.hi[a] - B.lo[a] + 1;
+    if (L->boxes.size() != 1 || D < 2 || reg || L->body || L->bc_lo[a] == BAMREX_BC_PERIODIC) return 0;
+    const int rows = L->boxes[0].hi[a] - L->boxes[0].lo[a] + 1;
     const int C = std::max(1, std::min(nslabs, rows / 4));
-    if (L->boxes.size() != 1 || D < 2 || reg || L->body || L->bc_lo[a] == BAMREX_BC_PERIODIC || C < 2) {
-        // not streamable: the plain sequence
-        BX_TRY(bamrex_level_copy_in(L, host_in));
-        BX_TRY(bamrex_level_advance(L, 0.0, dt, 1, 1, nullptr));
-        if (dt_next) BX_TRY(bamrex_level_est_time_step(L, dt_next));
-        BX_TRY(bamrex_level_copy_out(L, host_out));
-        return bamrex_level_sync(L);
-    }
+    return C >= 2 ? C : 0;
+}
+
+int host_stream_setup(bamrex_level* L, int C)
+{
     cudaError_t e = cudaSuccess;
     if (!L->hs) {
         L->hs = new (std::nothrow) bamrex_level::HostStream();
@@ -1105,18 +1097,37 @@ extern "C" int bamrex_level_step_host(bamrex_level* L, const double* host_in, do
     }
     bamrex_level::HostStream& H = *L->hs;
     while ((int)H.in.size() < C) {
-        cudaEvent_t ei = nullptr, eo = nullptr;
-        e = cudaEventCreateWithFlags(&ei, cudaEventDisableTiming);
-        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&eo, cudaEventDisableTiming);
+        cudaEvent_t ev[3] = { nullptr, nullptr, nullptr };
+        for (int q = 0; q < 3 && e == cudaSuccess; ++q) e = cudaEventCreateWithFlags(&ev[q], cudaEventDisableTiming);
         if (e != cudaSuccess) return L->set_err(cuda_fail(e, "host-stream events"));
-        H.in.push_back(ei);
-        H.out.push_back(eo);
+        H.in.push_back(ev[0]);
+        H.out.push_back(ev[1]);
+        H.done.push_back(ev[2]);
     }
-    // slab c: cells [s0, s1) of direction a; plane = cells of one layer
-    long long plane = 1;
+    return BAMREX_OK;
+}
+
+// Enqueue one step of a host-resident state streamed in C slabs along the
+// last direction: the upload of slab c, the sweeps of the other directions
+// on slab c, the last direction's sweep on slab c - 1 (its stencil reaches
+// two cells into slab c) and the download of slab c - 1 run on three
+// streams at once.  Every ghost fill covers the whole box and a slab's
+// cells are swept only after the cells their stencils read are final, so
+// the result is the plain step's.  device_dt: dt from the step scalars and
+// the next dt computed at the end of the step (time, steps advanced);
+// chained: slab c's upload waits for the previous step's download of slab c
+// (the host buffer is read and written in place).
+int host_step_enqueue(bamrex_level* L, const double* host_in, double* host_out, int C, double dt_host, bool device_dt,
+                      bool chained)
+{
+    bamrex_level::HostStream& H = *L->hs;
+    const int D = L->D, a = D - 1;
+    const bamrex_box B = L->boxes[0];
+    const int rows = B.hi[a] - B.lo[a] + 1;
+    long long plane = 1;  // cells of one layer across the last direction
     for (int d = 0; d < D - 1; ++d) plane *= (long long)(B.hi[d] - B.lo[d] + 1);
     auto lo_of = [&](int c) { return B.lo[a] + (int)((long long)rows * c / C); };
-    auto pack_box = [&](int c) {
+    auto slab_box = [&](int c) {
         PackBox pb;
         for (int d = 0; d < 3; ++d) {
             pb.lo[d] = B.lo[d];
@@ -1127,20 +1138,19 @@ extern "C" int bamrex_level_step_host(bamrex_level* L, const double* host_in, do
         pb.cell_begin = 0;
         return pb;
     };
-    // the packed host layout of one box: component n, then cells x fastest
-    auto copies = [&](int c, double* dst_base, const double* src_base, bool to_host, cudaStream_t s) -> cudaError_t {
+    // staging (in) and staging_out hold the packed layout of the whole box
+    // ([n][cells], x fastest); a slab is one range inside every component
+    auto copies = [&](int c, bool to_host, cudaStream_t s) -> cudaError_t {
         const long long first = (long long)(lo_of(c) - B.lo[a]) * plane, cells = (long long)(lo_of(c + 1) - lo_of(c)) * plane;
         for (int n = 0; n < L->NC; ++n) {
-            const size_t off_host = (size_t)(n * L->ncells + first), off_dev = (size_t)(n * L->ncells + first);
+            const size_t off = (size_t)(n * L->ncells + first);
             const cudaError_t r = to_host
-                ? cudaMemcpyAsync(host_out + off_host, dst_base + off_dev, sizeof(double) * cells, cudaMemcpyDeviceToHost, s)
-                : cudaMemcpyAsync((double*)dst_base + off_dev, src_base + off_host, sizeof(double) * cells, cudaMemcpyHostToDevice, s);
+                ? cudaMemcpyAsync(host_out + off, H.staging_out + off, sizeof(double) * cells, cudaMemcpyDeviceToHost, s)
+                : cudaMemcpyAsync(L->staging + off, host_in + off, sizeof(double) * cells, cudaMemcpyHostToDevice, s);
             if (r != cudaSuccess) return r;
         }
         return cudaSuccess;
     };
-    // staging (in) and staging_out hold the packed layout of the whole box;
-    // a slab occupies its cells' range inside every component block
     PackBox whole;
     for (int d = 0; d < 3; ++d) {
         whole.lo[d] = B.lo[d];
@@ -1149,10 +1159,15 @@ extern "C" int bamrex_level_step_host(bamrex_level* L, const double* host_in, do
     whole.cell_begin = 0;
     const int cur = L->cur;
     const int p_lag = cur ^ ((D - 1) & 1), p_out = cur ^ (D & 1);
-    e = cudaMemsetAsync(&L->d_scal->ws_bits, 0, sizeof(unsigned long long), L->stream);
-    if (e == cudaSuccess) e = cudaEventRecord(H.start, L->stream);
-    if (e == cudaSuccess) e = cudaStreamWaitEvent(H.h2d, H.start, 0);
-    if (e == cudaSuccess) e = cudaStreamWaitEvent(H.d2h, H.start, 0);
+    cudaError_t e = cudaSuccess;
+    if (!device_dt) e = cudaMemsetAsync(&L->d_scal->ws_bits, 0, sizeof(unsigned long long), L->stream);
+    if (!chained) {
+        // the first step waits for everything queued on the level before it;
+        // a chained step's dependencies on its predecessor are per slab
+        if (e == cudaSuccess) e = cudaEventRecord(H.start, L->stream);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(H.h2d, H.start, 0);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(H.d2h, H.start, 0);
+    }
     if (e != cudaSuccess) return L->set_err(cuda_fail(e, "host-stream start"));
     auto slab_sweep = [&](int dir, int c, int pin, bool ws) -> int {
         SweepArgs sa;
@@ -1160,12 +1175,11 @@ extern "C" int bamrex_level_step_host(bamrex_level* L, const double* host_in, do
         sa.boxes = nullptr;
         sa.nboxes = 1;
         SweepBox& sb = sa.one;
+        const PackBox pb = slab_box(c);
         for (int d = 0; d < 3; ++d) {
-            sb.lo[d] = B.lo[d];
-            sb.hi[d] = B.hi[d];
+            sb.lo[d] = pb.lo[d];
+            sb.hi[d] = pb.hi[d];
         }
-        sb.lo[a] = lo_of(c);
-        sb.hi[a] = lo_of(c + 1) - 1;
         sb.in = L->fab[pin][0];
         sb.out = L->fab[pin ^ 1][0];
         sb.flux.p = nullptr;
@@ -1176,48 +1190,115 @@ extern "C" int bamrex_level_step_host(bamrex_level* L, const double* host_in, do
         sa.total_items = items;
         sa.seglen = L->seglen[dir];
         sa.halo = method_halo(L->method);
-        sa.dt_host = dt;
-        sa.scal = nullptr;
+        sa.dt_host = dt_host;
+        sa.scal = device_dt ? L->d_scal : nullptr;
         sa.dx = L->dx[dir];
         sa.k = L->k;
         sa.ws_max = ws ? &L->d_scal->ws_bits : nullptr;
         sa.do_update = 1;
         return level_launch(L, launch_sweep(D, dir, L->method, L->fp32, sa, L->stream, march), "slab sweep");
     };
+    const StepScalars* gate = device_dt ? L->d_scal : nullptr;
     auto lagged = [&](int c) -> int {
-        BX_TRY(level_fill(L, a, p_lag, nullptr));
+        BX_TRY(level_fill(L, a, p_lag, gate));
         BX_TRY(slab_sweep(a, c, p_lag, true));
-        BX_TRY(level_launch(L, launch_pack_slab(L->NC, L->fp32, L->fab[p_out][0], whole, pack_box(c), H.staging_out, 1,
+        BX_TRY(level_launch(L, launch_pack_slab(L->NC, L->fp32, L->fab[p_out][0], whole, slab_box(c), H.staging_out, 1,
                                                 L->stream),
                             "slab pack"));
         cudaError_t r = cudaEventRecord(H.out[c], L->stream);
         if (r == cudaSuccess) r = cudaStreamWaitEvent(H.d2h, H.out[c], 0);
-        if (r == cudaSuccess) r = copies(c, H.staging_out, nullptr, true, H.d2h);
+        if (r == cudaSuccess) r = copies(c, true, H.d2h);
+        if (r == cudaSuccess) r = cudaEventRecord(H.done[c], H.d2h);
         return r == cudaSuccess ? BAMREX_OK : L->set_err(cuda_fail(r, "slab download"));
     };
     for (int c = 0; c < C; ++c) {
-        e = copies(c, L->staging, host_in, false, H.h2d);
+        // the previous step has read this slab's device rows (packed) and
+        // written its host rows (downloaded) once its download is done
+        if (chained) e = cudaStreamWaitEvent(H.h2d, H.done[c], 0);
+        if (e == cudaSuccess) e = copies(c, false, H.h2d);
         if (e != cudaSuccess) return L->set_err(cuda_fail(e, "slab upload"));
-        BX_TRY(level_launch(L, launch_pack_slab(L->NC, L->fp32, L->fab[cur][0], whole, pack_box(c), L->staging, 0, H.h2d),
+        BX_TRY(level_launch(L, launch_pack_slab(L->NC, L->fp32, L->fab[cur][0], whole, slab_box(c), L->staging, 0, H.h2d),
                             "slab unpack"));
         e = cudaEventRecord(H.in[c], H.h2d);
         if (e == cudaSuccess) e = cudaStreamWaitEvent(L->stream, H.in[c], 0);
         if (e != cudaSuccess) return L->set_err(cuda_fail(e, "slab event"));
         int p = cur;
         for (int d = 0; d < D - 1; ++d) {
-            BX_TRY(level_fill(L, d, p, nullptr));
+            BX_TRY(level_fill(L, d, p, gate));
             BX_TRY(slab_sweep(d, c, p, false));
             p ^= 1;
         }
         if (c > 0) BX_TRY(lagged(c - 1));
     }
     BX_TRY(lagged(C - 1));
-    e = cudaStreamSynchronize(H.d2h);
+    if (device_dt)
+        BX_TRY(level_launch(L, launch_step_dt(L->d_scal, D, L->dx[0], L->dx[1], L->dx[2], L->cfl, 1, L->stream), "step dt"));
+    L->cur = p_out;
+    L->ws_valid = !device_dt;
+    return BAMREX_OK;
+}
+
+}  // namespace
+
+extern "C" int bamrex_level_step_host(bamrex_level* L, const double* host_in, double* host_out, double dt,
+                                      int nslabs, double* dt_next)
+{
+    if (!L || !host_in || !host_out) return fail(BAMREX_ERR_ARG, "NULL argument");
+    if (!(dt > 0) || !std::isfinite(dt)) return L->set_err(fail(BAMREX_ERR_ARG, "dt must be positive and finite"));
+    const int C = host_slabs(L, nslabs);
+    if (!C) {
+        // not streamable: the plain sequence
+        BX_TRY(bamrex_level_copy_in(L, host_in));
+        BX_TRY(bamrex_level_advance(L, 0.0, dt, 1, 1, nullptr));
+        if (dt_next) BX_TRY(bamrex_level_est_time_step(L, dt_next));
+        BX_TRY(bamrex_level_copy_out(L, host_out));
+        return bamrex_level_sync(L);
+    }
+    BX_TRY(host_stream_setup(L, C));
+    BX_TRY(host_step_enqueue(L, host_in, host_out, C, dt, false, false));
+    cudaError_t e = cudaStreamSynchronize(L->hs->d2h);
     if (e == cudaSuccess) e = cudaStreamSynchronize(L->stream);
     if (e != cudaSuccess) return L->set_err(cuda_fail(e, "host step"));
-    L->cur = p_out;
-    L->ws_valid = true;
     if (dt_next) BX_TRY(bamrex_level_est_time_step(L, dt_next));
+    return BAMREX_OK;
+}
+
+extern "C" int bamrex_level_run_host(bamrex_level* L, double* host, int nsteps, double dt0, int nslabs, double* time_io,
+                                     double* dt_next)
+{
+    if (!L || !host || !time_io) return fail(BAMREX_ERR_ARG, "NULL argument");
+    if (nsteps < 0) return L->set_err(fail(BAMREX_ERR_ARG, "nsteps must be >= 0"));
+    if (!(dt0 > 0) || !std::isfinite(dt0)) return L->set_err(fail(BAMREX_ERR_ARG, "dt0 must be positive and finite"));
+    const int C = host_slabs(L, nslabs);
+    if (!C) {
+        // not streamable: one plain host step after the other
+        double t = *time_io, dt = dt0;
+        for (int st = 0; st < nsteps; ++st) {
+            double nxt = 0.0;
+            BX_TRY(bamrex_level_step_host(L, host, host, dt, nslabs, &nxt));
+            t += dt;
+            dt = nxt;
+        }
+        *time_io = t;
+        if (dt_next) *dt_next = dt;
+        return BAMREX_OK;
+    }
+    BX_TRY(host_stream_setup(L, C));
+    StepScalars* h = L->h_scal;
+    std::memset(h, 0, sizeof(*h));
+    h->time = *time_io;
+    h->dt = dt0;
+    h->stop_time = -1.0;
+    cudaError_t e = cudaMemcpyAsync(L->d_scal, h, sizeof(StepScalars), cudaMemcpyHostToDevice, L->stream);
+    if (e != cudaSuccess) return L->set_err(cuda_fail(e, "scalars upload"));
+    for (int s = 0; s < nsteps; ++s) BX_TRY(host_step_enqueue(L, host, host, C, 0.0, true, s > 0));
+    e = cudaMemcpyAsync(h, L->d_scal, sizeof(StepScalars), cudaMemcpyDeviceToHost, L->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(L->hs->d2h);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(L->stream);
+    if (e != cudaSuccess) return L->set_err(cuda_fail(e, "host run"));
+    if (h->status != 0) return L->set_err(fail(h->status, "non-finite time step during the run"));
+    *time_io = h->time;
+    if (dt_next) *dt_next = h->dt;
     return BAMREX_OK;
 }
 

@@ -122,7 +122,7 @@ struct bamrex_level {
     struct HostStream {
         cudaStream_t h2d = nullptr, d2h = nullptr;
         cudaEvent_t start = nullptr;
-        std::vector<cudaEvent_t> in, out;
+        std::vector<cudaEvent_t> in, out, done;  // per slab: unpacked, packed, downloaded
         double* staging_out = nullptr;
     };
     HostStream* hs = nullptr;

@@ -285,6 +285,14 @@ class Level:
                                               int(nslabs), ctypes.byref(nxt)))
         return nxt.value
 
+    def run_host_ptr(self, ptr: int, nsteps: int, dt0: float, time: float = 0.0, nslabs: int = 16):
+        """nsteps host round-trip steps of the packed state at ptr, in place
+        (bamrex_level_run_host).  Returns (time, next dt)."""
+        t, nxt = ctypes.c_double(time), ctypes.c_double()
+        self._ck(lib().bamrex_level_run_host(self._h, ctypes.c_void_p(ptr), int(nsteps), float(dt0), int(nslabs),
+                                             ctypes.byref(t), ctypes.byref(nxt)))
+        return t.value, nxt.value
+
     def sync(self):
         self._ck(lib().bamrex_level_sync(self._h))
 

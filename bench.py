@@ -44,7 +44,7 @@ def parse_args():
     ap.add_argument("--max-grid-size", type=int, default=0, help="box size (0: one box per rank)")
     ap.add_argument("--graph", type=int, default=0, help="1: time the CUDA-graph replay instead")
     ap.add_argument("--e2e-steps", type=int, default=10)
-    ap.add_argument("--e2e-slabs", type=int, default=16, help="slabs of the streamed host step")
+    ap.add_argument("--e2e-slabs", type=int, default=24, help="slabs of the streamed host steps")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp32", action="store_true", help="skip the FP32-storage variant")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
@@ -562,18 +562,18 @@ def run_ours(args, rank, world, local_rank):
         ms = float(t.item())
     assert steps_done == args.steps, (steps_done, args.steps)
 
-    # e2e through the public API with host buffers: per step the state goes
-    # host -> device, one step + estTimeStep, device -> host, in one
-    # bamrex_level_step_host call (slabs streamed: the copies in both
-    # directions overlap each other and the sweeps).
+    # e2e through the public API with host buffers: every step the state goes
+    # host -> device, one step + its CFL estimate, device -> host
+    # (bamrex_level_run_host: slabs streamed, the copies in both directions
+    # overlap each other, the sweeps and the neighbouring steps' copies).
     pk = lev.packing
     host = torch.empty(pk.size, dtype=torch.float64, pin_memory=True)
     host.numpy()[:] = pk.pack(u0)
     hptr = host.data_ptr()
     dt = lev.estTimeStep()
-    # one untimed call: the host step's streams, events and output staging
+    # one untimed step: the host step's streams, events and output staging
     # are created on first use
-    lev.step_host_ptr(hptr, hptr, dt, args.e2e_slabs)
+    lev.run_host_ptr(hptr, 1, dt, 0.0, args.e2e_slabs)
     host.numpy()[:] = pk.pack(u0)
     if dist:
         dist.barrier()
@@ -583,10 +583,7 @@ def run_ours(args, rank, world, local_rank):
     with torch.cuda.stream(stream):
         e0.record(stream)
         tsim = 0.0
-        for _ in range(args.e2e_steps):
-            dt_next = lev.step_host_ptr(hptr, hptr, dt, args.e2e_slabs)
-            tsim += dt
-            dt = dt_next
+        tsim, dt = lev.run_host_ptr(hptr, args.e2e_steps, dt, 0.0, args.e2e_slabs)
         e1.record(stream)
     lev.sync()
     t_e1 = time.time()
@@ -684,8 +681,9 @@ def run_ours(args, rank, world, local_rank):
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": state_bytes,
                 "d2h_bytes_per_step": state_bytes + 8,
-                "path": "bamrex_level_step_host per step: pinned host state in and out, %d slabs streamed "
-                        "(upload, sweeps, download overlapped), CFL estimate of the result" % args.e2e_slabs,
+                "path": "bamrex_level_run_host: every step the whole state host -> device and device -> host "
+                        "(pinned), %d slabs streamed (uploads, sweeps, downloads overlapped within and across "
+                        "steps), dt from the CFL estimate on the device" % args.e2e_slabs,
                 "steps": args.e2e_steps},
         "gpu_launches": launches,
         "clocks": clocks.summary(t_wall0, t_wall1),

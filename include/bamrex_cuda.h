@@ -257,6 +257,16 @@ BAMREX_API int bamrex_conserved_sums_noalloc(int spacedim, const bamrex_box *box
  * overlap); other levels take the plain sequence.  Synchronous. */
 BAMREX_API int bamrex_level_step_host(bamrex_level *level, const double *host_in, double *host_out, double dt,
                                       int nslabs, double *dt_next);
+/* nsteps steps of a host-resident state in place (host: packed layout),
+ * each one a host round trip as bamrex_level_step_host, the first with time
+ * step dt0 and the next ones with the CFL estimate of their input computed
+ * on the device; step k + 1's upload of a slab starts as soon as step k has
+ * downloaded it, so the copies of consecutive steps overlap.  *time_io
+ * advances by the steps' dt; *dt_next (may be NULL) is the estimate for the
+ * step after the last.  Levels that cannot be streamed take one plain host
+ * step after the other.  Synchronous. */
+BAMREX_API int bamrex_level_run_host(bamrex_level *level, double *host, int nsteps, double dt0, int nslabs,
+                                     double *time_io, double *dt_next);
 BAMREX_API int bamrex_level_sync(bamrex_level *level);
 
 /* bamrexBCData::fill_consv_boundary on the current state

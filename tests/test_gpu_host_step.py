@@ -74,3 +74,30 @@ def test_step_host_equals_plain_step(torch_cuda, case):
     # the device state is the step's result
     np.testing.assert_array_equal(lev.get_state(), ref)
     lev.close()
+
+
+@pytest.mark.parametrize("case", [CASES[0], CASES[2], CASES[4], CASES[5], CASES[7]], ids=lambda c: str(c))
+def test_run_host_equals_device_run(torch_cuda, case):
+    """bamrex_level_run_host (host round trip every step, copies of
+    consecutive steps overlapped, dt on the device) equals the
+    device-stepped run of the same steps bit for bit, time included."""
+    torch = torch_cuda
+    D, n, mgs, bc, method, prec, xm, slabs = case
+    u0 = _state(D, n, seed=5)
+    ref_lev = _level(D, n, mgs, bc, method, prec, xm)
+    ref_lev.set_state(u0)
+    t_ref, steps = ref_lev.run(4, use_graph=False)
+    assert steps == 4
+    ref = ref_lev.get_state()
+    ref_next = ref_lev.estTimeStep()
+    ref_lev.close()
+
+    lev = _level(D, n, mgs, bc, method, prec, xm)
+    lev.set_state(u0)
+    dt0 = lev.estTimeStep()
+    h = torch.tensor(lev.packing.pack(u0)).pin_memory()
+    t, nxt = lev.run_host_ptr(h.data_ptr(), 4, dt0, 0.0, slabs)
+    np.testing.assert_array_equal(lev.packing.unpack(h.numpy()), ref)
+    assert t == t_ref
+    assert nxt == ref_next
+    lev.close()

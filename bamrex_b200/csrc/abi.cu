@@ -934,10 +934,11 @@ extern "C" int bamrex_level_create(bamrex_level** out, const bamrex_level_desc* 
     L->staging = (double*)(L->arena + o_stage);
     L->d_scal = (StepScalars*)(L->arena + o_scal);
 
-    // upload tables (synchronous: setup only)
+    // upload tables on the level's stream (ordered before its kernels),
+    // then wait for them: setup only
     auto up = [&](void* dst, const void* src, size_t bytes) -> cudaError_t {
         if (!bytes) return cudaSuccess;
-        return cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice);
+        return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, L->stream);
     };
     cudaError_t ue = cudaSuccess;
     for (int p = 0; p < 2 && ue == cudaSuccess; ++p) ue = up(L->d_fab[p], L->fab[p].data(), sizeof(FabDev) * nb);
@@ -958,8 +959,9 @@ extern "C" int bamrex_level_create(bamrex_level** out, const bamrex_level_desc* 
         }
     }
     if (ue == cudaSuccess) ue = up(L->d_pack, pack_host.data(), sizeof(PackBox) * nb);
-    if (ue == cudaSuccess) ue = cudaMemset(L->arena + o_state0, 0, (size_t)(o_state1 - o_state0) * 2);
-    if (ue == cudaSuccess) ue = cudaMemset(L->d_scal, 0, sizeof(StepScalars));
+    if (ue == cudaSuccess) ue = cudaMemsetAsync(L->arena + o_state0, 0, (size_t)(o_state1 - o_state0) * 2, L->stream);
+    if (ue == cudaSuccess) ue = cudaMemsetAsync(L->d_scal, 0, sizeof(StepScalars), L->stream);
+    if (ue == cudaSuccess) ue = cudaStreamSynchronize(L->stream);
     if (ue != cudaSuccess) {
         const int r = cuda_fail(ue, "level table upload");
         bamrex_level_destroy(L);

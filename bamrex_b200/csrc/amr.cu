@@ -638,7 +638,7 @@ extern "C" int bamrex_coupling_create(bamrex_coupling** out, bamrex_level* crse,
     for (int b = 0; b < nbc; ++b)
         oldfab[b].p = C->old_state + ((char*)crse->fab[0][b].p - crse->state[0]);
     auto up = [&](void* dst, const void* src, size_t bytes) -> cudaError_t {
-        return bytes ? cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice) : cudaSuccess;
+        return bytes ? cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, crse->stream) : cudaSuccess;
     };
     e = up(C->d_old_fab, oldfab.data(), sizeof(FabDev) * nbc);
     for (int s = 0; s < 2 && e == cudaSuccess; ++s) {
@@ -649,11 +649,12 @@ extern "C" int bamrex_coupling_create(bamrex_coupling** out, bamrex_level* crse,
         e = up(C->d_cfaces[d], cf[d].data(), sizeof(FaceRec) * cf[d].size());
         if (e == cudaSuccess) e = up(C->d_ffaces[d], ff[d].data(), sizeof(FaceRec) * ff[d].size());
         if (e == cudaSuccess) e = up(C->d_rr[d], rr[d].data(), sizeof(RefluxRec) * rr[d].size());
-        if (e == cudaSuccess) e = cudaMemset(C->d_reg[d], 0, sizeof(double) * C->NC * rr[d].size());
+        if (e == cudaSuccess) e = cudaMemsetAsync(C->d_reg[d], 0, sizeof(double) * C->NC * rr[d].size(), crse->stream);
     }
     if (e == cudaSuccess) e = up(C->d_avg, avg.data(), sizeof(AvgOp) * avg.size());
     if (e == cudaSuccess) e = up(C->d_cov_box, cov.data(), sizeof(PackBox) * cov.size());
     for (int p = 0; p < 2 && e == cudaSuccess; ++p) e = up(C->d_cov_fab[p], covfab[p].data(), sizeof(FabDev) * cov.size());
+    if (e == cudaSuccess) e = cudaStreamSynchronize(crse->stream);
     if (e != cudaSuccess) {
         dev_free(C->arena, crse->stream);
         return cuda_fail(e, "coupling table upload");
@@ -1336,10 +1337,11 @@ int set_level(bamrex_amr* A, int lev, const std::vector<bamrex_box>& boxes)
             const size_t tb = sizeof(FabDev) * tab.size(), ob = sizeof(GhostOp) * ops.size();
             const std::vector<int> ct = ghost_chunk_table(ops, nchunks);
             cudaError_t e = dev_alloc(&dmem, align_up(tb, 256) + ghost_table_bytes(ops.size(), nchunks), A->stream);
-            if (e == cudaSuccess) e = cudaMemcpy(dmem, tab.data(), tb, cudaMemcpyHostToDevice);
+            if (e == cudaSuccess) e = cudaMemcpyAsync(dmem, tab.data(), tb, cudaMemcpyHostToDevice, A->stream);
             GhostOp* dops = (GhostOp*)((char*)dmem + align_up(tb, 256));
-            if (e == cudaSuccess) e = cudaMemcpy(dops, ops.data(), ob, cudaMemcpyHostToDevice);
-            if (e == cudaSuccess) e = cudaMemcpy(dops + ops.size(), ct.data(), sizeof(int) * ct.size(), cudaMemcpyHostToDevice);
+            if (e == cudaSuccess) e = cudaMemcpyAsync(dops, ops.data(), ob, cudaMemcpyHostToDevice, A->stream);
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(dops + ops.size(), ct.data(), sizeof(int) * ct.size(), cudaMemcpyHostToDevice, A->stream);
             if (e == cudaSuccess)
                 e = launch_ghost_fill(L->NC, L->fp32, dops, (int)ops.size(), nchunks, (const FabDev*)dmem, nullptr, A->stream);
             if (e == cudaSuccess) e = cudaStreamSynchronize(A->stream);

@@ -100,6 +100,10 @@ void dev_free(void* p, cudaStream_t s)
         }
     }
     if (dev < 0) return;  // not a pooled block
+    // as cudaFree: every stream's work on the block (table uploads and
+    // memsets on the default stream, copies on helper streams) is finished
+    // before the block can be handed out again or its pages released
+    cudaDeviceSynchronize();
     cudaFreeAsync(p, s);
     std::lock_guard<std::mutex> g(P.mu);
     if (--P.live[dev] == 0 && P.pool[dev]) {

@@ -21,7 +21,7 @@ namespace bamrex {
 // queued on `s` and usable from every stream when the call returns.
 cudaError_t dev_alloc(void** p, size_t bytes, cudaStream_t s);
 
-// Give a block back; the caller has finished all work on it (every stream).
+// Give a block back (after a device-wide synchronisation, as cudaFree).
 void dev_free(void* p, cudaStream_t s);
 
 // Small pinned host blocks (up to 4 KB) for the scalars a step reads back,

@@ -72,11 +72,13 @@ extern "C" int bamrex_level_set_halo(bamrex_level* L, int dir, const bamrex_regi
         H[s]->boxes = (PackBox*)(m + o_pb[s]);
         H[s]->nops = (int)pb[s].size();
         H[s]->cells = cells[s];
-        if (!pb[s].empty()) e = cudaMemcpy(H[s]->boxes, pb[s].data(), sizeof(PackBox) * pb[s].size(), cudaMemcpyHostToDevice);
+        if (!pb[s].empty())
+            e = cudaMemcpyAsync(H[s]->boxes, pb[s].data(), sizeof(PackBox) * pb[s].size(), cudaMemcpyHostToDevice, L->stream);
         for (int par = 0; par < 2 && e == cudaSuccess; ++par) {
             H[s]->fabs[par] = (FabDev*)(m + o_fb[s][par]);
             if (!fb[s][par].empty())
-                e = cudaMemcpy(H[s]->fabs[par], fb[s][par].data(), sizeof(FabDev) * fb[s][par].size(), cudaMemcpyHostToDevice);
+                e = cudaMemcpyAsync(H[s]->fabs[par], fb[s][par].data(), sizeof(FabDev) * fb[s][par].size(),
+                                    cudaMemcpyHostToDevice, L->stream);
         }
         if (e != cudaSuccess) return L->set_err(cuda_fail(e, "halo table upload"));
     }

@@ -929,6 +929,10 @@ extern "C" int bamrex_helmholtz_create(bamrex_helmholtz** out, const bamrex_helm
             cudaMemcpy(L.b[q], fo.data(), sizeof(double) * nf, cudaMemcpyHostToDevice);
         }
     }
+    // the default-stream memsets and copies above are complete before any
+    // kernel on the operator's (non-blocking) stream reads them
+    e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) return cuda_fail(e, "set-up");
     *out = H.release();
     return BAMREX_OK;
 }

@@ -713,6 +713,8 @@ extern "C" int bamrex_precnet_create(bamrex_precnet** out, int nx, int ny, int b
     P_TRY(pck(N.get(), cudaMemcpy(N->d_w, w.data(), sizeof(float) * P, cudaMemcpyHostToDevice), "weights"));
     P_TRY(pck(N.get(), cudaMemset(N->d_m, 0, sizeof(float) * P * 2), "moments"));
     P_TRY(alloc_acts(N.get()));
+    // complete before the network's kernels run on another stream
+    P_TRY(pck(N.get(), cudaDeviceSynchronize(), "set-up"));
     *out = N.release();
     return BAMREX_OK;
 }

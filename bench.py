@@ -56,6 +56,7 @@ def parse_args():
     ap.add_argument("--amr-steps", type=int, default=6, help="timed coarse steps of the AMR blast sample")
     ap.add_argument("--imex-n", type=int, default=2048, help="cells per side of the IMEX pressure problem")
     ap.add_argument("--no-body", action="store_true", help="skip the ghost-fluid rigid-body sample")
+    ap.add_argument("--body-cases", default="2d,3d", help="rigid-body cases to run (2d, 3d)")
     return ap.parse_args()
 
 
@@ -668,8 +669,12 @@ def run_ours(args, rank, world, local_rank):
 
     body = None
     if rank == 0 and world == 1 and not args.no_body:
-        body = {"2d": rigid_body_run(2, (2048, 2048), 64, bx.FP64),
-                "3d_fp32_storage": rigid_body_run(3, (512, 512, 128), 32, bx.FP32_STORAGE, steps=5)}
+        cases = args.body_cases.split(",")
+        body = {}
+        if "2d" in cases:
+            body["2d"] = rigid_body_run(2, (2048, 2048), 64, bx.FP64)
+        if "3d" in cases:
+            body["3d_fp32_storage"] = rigid_body_run(3, (512, 512, 128), 32, bx.FP32_STORAGE, steps=5)
 
     line = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,

@@ -56,8 +56,8 @@ struct BodyState {
     int* d_active = nullptr;       // boxes swept by the global-memory kernel
     int* d_list_s = nullptr;       // boxes swept in shared memory
     long long* d_meta_off = nullptr;  // their first metadata cell
-    unsigned char* d_code = nullptr;  // per swept-region cell: swept bit, neighbour directions
-    double* d_wts = nullptr;       // per swept-region cell: D weights and their sum
+    double* d_wts = nullptr;       // per swept-region cell: its sweep record (rec_words)
+    int ring = 1;                  // records each sweep thread keeps in flight
     int n_smem = 0;                // boxes of d_list_s
     int threads_p = 32;            // threads (pencils) and shared memory of their sweep CTAs
     size_t bytes_p = 0;
@@ -598,18 +598,25 @@ __global__ void __launch_bounds__(kSweepCta) extrap_kernel(const int* __restrict
 // before the barrier so that the plane's critical path is the shared-memory
 // reads, the quotient and the barrier.
 
-constexpr int kSmemMax = 200 * 1024;  // shared memory of one (box, component) region
+constexpr int kSmemMax = 224 * 1024;  // shared memory of one (box, component) sweep CTA
 constexpr int kPencilMax = 1024;      // pencils (= threads) of one CTA
 
-// Per swept-region cell: code bit 0 = swept (ghost, not at the interface),
-// bit 1 + d = the neighbour in direction d is +1 (else -1); weights
-// |n_d / dx_d|, their sum and its correctly rounded reciprocal.
+// Sweep metadata of a swept-region cell, one 16-byte aligned record of
+// rec_words<D>() doubles: w_d = |n_d / dx_d| with the sign giving the
+// neighbour (+: the cell at +1, -: at -1, so a zero weight is -0.0 as the
+// reference's i - 1 choice), their sum (negative for a cell the sweeps skip:
+// not a ghost, or at the interface) and the sum's correctly rounded
+// reciprocal.
+template <int D>
+__host__ __device__ constexpr int rec_words() { return (D + 3) & ~1; }
+
 template <int D>
 __global__ void meta_kernel(const int* __restrict__ list, int nlist, const int* __restrict__ bbox,
                             const long long* __restrict__ meta_off, const FabDev* __restrict__ lsf,
                             const FabDev* __restrict__ flf, double dx0, double dx1, double dx2,
-                            unsigned char* __restrict__ code, double* __restrict__ wts)
+                            double* __restrict__ wts)
 {
+    constexpr int RW = rec_words<D>();
     const int li = blockIdx.y;
     if (li >= nlist) return;
     const int b = list[li];
@@ -628,22 +635,20 @@ __global__ void meta_kernel(const int* __restrict__ list, int nlist, const int* 
         int i, j, k;
         R.cell(q, i, j, k);
         const int flag = fl[at(G, i, j, k)];
-        const long long mi = meta_off[li] + q;
-        int c = ((flag & BAMREX_GFM_GHOST) && !(flag & BAMREX_GFM_INTERFACE)) ? 1 : 0;
+        double* rec = wts + (meta_off[li] + q) * RW;
+        const bool swept = (flag & BAMREX_GFM_GHOST) && !(flag & BAMREX_GFM_INTERFACE);
         const long long cl = at(L, i, j, k);
         const double sflip = (ls[cl] >= 0) ? -1 : 1;
-        double w[3] = { 0, 0, 0 };
+        double den = 0.0;
         for (int d = 0; d < D; ++d) {
             const double nd = ls[cl + (1 + d) * L.ns] / dx[d] * sflip;
-            w[d] = fabs(nd);
-            if (nd < 0) c |= 2 << d;
+            const double w = fabs(nd);
+            rec[d] = nd < 0 ? w : -w;
+            den = d == 0 ? w : den + w;
         }
-        double den = w[0];
-        for (int d = 1; d < D; ++d) den = den + w[d];
-        code[mi] = (unsigned char)c;
-        for (int d = 0; d < D; ++d) wts[mi * (D + 2) + d] = w[d];
-        wts[mi * (D + 2) + D] = den;
-        wts[mi * (D + 2) + D + 1] = 1.0 / den;
+        rec[D] = swept ? den : -1.0;
+        rec[D + 1] = 1.0 / den;
+        for (int d = D + 2; d < RW; ++d) rec[d] = 0.0;
     }
 }
 
@@ -693,18 +698,6 @@ __device__ void region_load(const SweepRegion<D>& R, const FabDev& f, const T* u
     }
 }
 
-template <typename T, int D>
-__device__ void region_store(const SweepRegion<D>& R, const FabDev& f, T* u, const T* sv, const unsigned char* code)
-{
-#pragma unroll 4
-    for (int r = threadIdx.x; r < R.vol; r += blockDim.x) {
-        if (!(code[r] & 1)) continue;
-        const int ci = r % R.n[0], rr = r / R.n[0];
-        const int cj = rr % R.n[1], ck = rr / R.n[1];
-        u[at(f, R.lo[0] + ci, R.lo[1] + cj, R.lo[2] + ck)] = sv[R.sidx(ci, cj, ck)];
-    }
-}
-
 __device__ __forceinline__ void sweep_signs(int D, int o, int& s0, int& s1, int& s2)
 {
     s0 = s1 = s2 = 1;
@@ -720,35 +713,44 @@ __device__ __forceinline__ void sweep_signs(int D, int o, int& s0, int& s1, int&
     }
 }
 
-// One cell update in shared memory (the compute_extrapolation quotient).
-template <typename T, int D>
-__device__ __forceinline__ void sweep_cell(T* sv, int cs, int c, const double* w, int so1, int so2)
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src)
 {
-    double num = 0.0 + w[0] * (double)sv[cs + ((c & 2) ? 1 : -1)];
-    if (D > 1) num = num + w[1] * (double)sv[cs + ((c & 4) ? so1 : -so1)];
-    if (D > 2) num = num + w[2] * (double)sv[cs + ((c & 8) ? so2 : -so2)];
-    sv[cs] = (T)div_by_rcp(num, w[D], w[D + 1]);
+    const unsigned dst = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_group() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+// Shared memory of a sweep CTA: the region's values with their halo, then
+// each thread's ring of K metadata records.
+__host__ __device__ inline size_t sweep_smem_bytes(long long hvol, size_t esize, int threads, int K, int rec_bytes)
+{
+    return (((size_t)hvol * esize + 15) / 16 * 16) + (size_t)threads * K * rec_bytes;
 }
 
-// One thread per pencil (up to 1024 pencils), a barrier per plane; the
-// next plane's metadata is loaded before the barrier.
-template <typename T, int D>
+// One thread per pencil (up to 1024 pencils), a barrier per plane.  Each
+// thread streams the metadata record of its cell K - 1 planes ahead into a
+// ring of its own in shared memory (cp.async), so the plane's critical path
+// is the shared-memory reads, the quotient and the barrier; K = 1 (no room
+// for a ring) loads the next plane's record into registers instead.
+template <typename T, int D, int K>
 __global__ void __launch_bounds__(kPencilMax) extrap_smem_kernel(const int* __restrict__ list, const int* __restrict__ bbox,
-                                   const long long* __restrict__ meta_off, const unsigned char* __restrict__ code,
-                                   const double* __restrict__ wts, const FabDev* __restrict__ fab_tab,
-                                   const StepScalars* gate)
+                                   const long long* __restrict__ meta_off, const double* __restrict__ wts,
+                                   const FabDev* __restrict__ fab_tab, const StepScalars* gate)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* sv = reinterpret_cast<T*>(smem_raw);
     constexpr int NORD = D == 1 ? 2 : (D == 2 ? 4 : 8);
-    constexpr int W = D + 2;
+    constexpr int RW = rec_words<D>();
     if (gate && gate->done) return;
     const int li = blockIdx.x, m = blockIdx.y;
     const int b = list[li];
     SweepRegion<D> R;
     R.init(bbox + 6 * b);
-    const unsigned char* cd = code + meta_off[li];
-    const double* wt = wts + meta_off[li] * W;
+    const double* wt = wts + meta_off[li] * RW;
+    double* ring = reinterpret_cast<double*>(smem_raw + ((size_t)R.hvol * sizeof(T) + 15) / 16 * 16) +
+                   (size_t)threadIdx.x * K * RW;
     const FabDev f = fab_tab[b];
     T* u = f.ptr<T>() + m * f.ns;
     region_load<T, D>(R, f, u, sv);
@@ -766,32 +768,68 @@ __global__ void __launch_bounds__(kPencilMax) extrap_smem_kernel(const int* __re
             const int cj = s1 > 0 ? pj : R.n[1] - 1 - pj;
             const int ck = s2 > 0 ? pk : R.n[2] - 1 - pk;
             const int ci0 = s0 > 0 ? 0 : R.n[0] - 1;
-            // cell of plane t = t0 + e: x = ci0 + s0 e; metadata row r0 + s0 e, smem cs0 + s0 e
+            // cell of plane t = t0 + e: x = ci0 + s0 e; record r0 + s0 e, smem cs0 + s0 e
             const int r0 = ci0 + R.n[0] * (cj + R.n[1] * ck);
             const int cs0 = R.sidx(ci0, cj, ck);
-            int cn = 0;
-            double wn[W];
-            auto fetch = [&](int e) {
-                cn = 0;
-                if (!has || (unsigned)e >= (unsigned)R.n[0]) return;
-                const int r = r0 + s0 * e;
-                cn = cd[r];
-#pragma unroll
-                for (int d = 0; d < W; ++d) wn[d] = wt[(long long)r * W + d];
+            auto on_pencil = [&](int t) { return has && (unsigned)(t - t0) < (unsigned)R.n[0]; };
+            auto update = [&](int t, const double* rec) {
+                const double den = rec[D];
+                if (!(den >= 0)) return;
+                const int cs = cs0 + s0 * (t - t0);
+                double num = 0.0 + fabs(rec[0]) * (double)sv[cs + (signbit(rec[0]) ? -1 : 1)];
+                if (D > 1) num = num + fabs(rec[1]) * (double)sv[cs + (signbit(rec[1]) ? -R.so1 : R.so1)];
+                if (D > 2) num = num + fabs(rec[2]) * (double)sv[cs + (signbit(rec[2]) ? -R.so2 : R.so2)];
+                sv[cs] = (T)div_by_rcp(num, den, rec[D + 1]);
             };
-            fetch(-t0);
-            for (int t = 0; t < planes; ++t) {
-                const int e = t - t0;
-                const int c = cn;
-                double w[W];
+            if constexpr (K == 1) {
+                // no room for a ring: the next plane's record in registers
+                double nxt[RW];
+                auto fetch = [&](int t) {
+                    if (!on_pencil(t)) return;
+                    const double* src = wt + (long long)(r0 + s0 * (t - t0)) * RW;
 #pragma unroll
-                for (int d = 0; d < W; ++d) w[d] = wn[d];
-                fetch(e + 1);
-                if (c & 1) sweep_cell<T, D>(sv, cs0 + s0 * e, c, w, R.so1, R.so2);
-                __syncthreads();
+                    for (int w = 0; w < RW; ++w) nxt[w] = src[w];
+                };
+                fetch(0);
+                for (int t = 0; t < planes; ++t) {
+                    double cur[RW];
+#pragma unroll
+                    for (int w = 0; w < RW; ++w) cur[w] = nxt[w];
+                    fetch(t + 1);
+                    if (on_pencil(t)) update(t, cur);
+                    __syncthreads();
+                }
+            } else {
+                // the record of plane t goes to ring slot t % K (an empty
+                // group off the pencil keeps one group per plane)
+                auto issue = [&](int t) {
+                    if (on_pencil(t)) {
+                        const double* src = wt + (long long)(r0 + s0 * (t - t0)) * RW;
+                        double* dst = ring + (t % K) * RW;
+#pragma unroll
+                        for (int w = 0; w < RW; w += 2) cp_async16(dst + w, src + w);
+                    }
+                    cp_async_group();
+                };
+#pragma unroll
+                for (int t = 0; t < K - 1; ++t) issue(t);
+                for (int t = 0; t < planes; ++t) {
+                    issue(t + K - 1);
+                    cp_async_wait<K - 1>();
+                    if (on_pencil(t)) update(t, ring + (t % K) * RW);
+                    __syncthreads();
+                }
+                cp_async_wait<0>();
             }
         }
-    region_store<T, D>(R, f, u, sv, cd);
+    // swept cells back to the state
+#pragma unroll 4
+    for (int r = threadIdx.x; r < R.vol; r += blockDim.x) {
+        if (!(wt[(long long)r * RW + D] >= 0)) continue;
+        const int ci = r % R.n[0], rr = r / R.n[0];
+        const int cj = rr % R.n[1], ck = rr / R.n[1];
+        u[at(f, R.lo[0] + ci, R.lo[1] + cj, R.lo[2] + ck)] = sv[R.sidx(ci, cj, ck)];
+    }
 }
 
 template <typename T>
@@ -968,18 +1006,19 @@ Sdf make_sdf(const bamrex_sdf& s)
 
 int body_launch(bamrex_level* L, cudaError_t e, const char* what) { return level_launch(L, e, what); }
 
+template <int K>
 cudaError_t smem_attribute(bool fp32, int D, int bytes)
 {
     if (bytes <= 48 * 1024) return cudaSuccess;
     const cudaFuncAttribute a = cudaFuncAttributeMaxDynamicSharedMemorySize;
     if (fp32) {
-        if (D == 1) return cudaFuncSetAttribute(extrap_smem_kernel<float, 1>, a, bytes);
-        if (D == 2) return cudaFuncSetAttribute(extrap_smem_kernel<float, 2>, a, bytes);
-        return cudaFuncSetAttribute(extrap_smem_kernel<float, 3>, a, bytes);
+        if (D == 1) return cudaFuncSetAttribute(extrap_smem_kernel<float, 1, K>, a, bytes);
+        if (D == 2) return cudaFuncSetAttribute(extrap_smem_kernel<float, 2, K>, a, bytes);
+        return cudaFuncSetAttribute(extrap_smem_kernel<float, 3, K>, a, bytes);
     }
-    if (D == 1) return cudaFuncSetAttribute(extrap_smem_kernel<double, 1>, a, bytes);
-    if (D == 2) return cudaFuncSetAttribute(extrap_smem_kernel<double, 2>, a, bytes);
-    return cudaFuncSetAttribute(extrap_smem_kernel<double, 3>, a, bytes);
+    if (D == 1) return cudaFuncSetAttribute(extrap_smem_kernel<double, 1, K>, a, bytes);
+    if (D == 2) return cudaFuncSetAttribute(extrap_smem_kernel<double, 2, K>, a, bytes);
+    return cudaFuncSetAttribute(extrap_smem_kernel<double, 3, K>, a, bytes);
 }
 
 int ghost_ops(bamrex_level* L, const GhostOp* ops, int nops, int nchunks, int parity, const StepScalars* gate)
@@ -1044,18 +1083,21 @@ int body_fill(bamrex_level* L, int parity, const StepScalars* gate)
     for (int r = 0; r < D + 1; ++r) {
         if (S->n_smem) {
             const dim3 g((unsigned)S->n_smem, (unsigned)L->NC);
-#define BX_EXTRAP_S(T, DD)                                                                                      \
-    extrap_smem_kernel<T, DD><<<g, S->threads_p, S->bytes_p, L->stream>>>(S->d_list_s, S->d_bbox, S->d_meta_off, \
-                                                                          S->d_code, S->d_wts, L->d_fab[parity], gate)
+#define BX_EXTRAP_S(T, DD, KK)                                                                               \
+    extrap_smem_kernel<T, DD, KK><<<g, S->threads_p, S->bytes_p, L->stream>>>(S->d_list_s, S->d_bbox, S->d_meta_off, \
+                                                                              S->d_wts, L->d_fab[parity], gate)
+#define BX_EXTRAP_SK(T, DD) \
+    if (S->ring == 4) BX_EXTRAP_S(T, DD, 4); else if (S->ring == 2) BX_EXTRAP_S(T, DD, 2); else BX_EXTRAP_S(T, DD, 1)
             if (L->fp32) {
-                if (D == 1) BX_EXTRAP_S(float, 1);
-                else if (D == 2) BX_EXTRAP_S(float, 2);
-                else BX_EXTRAP_S(float, 3);
+                if (D == 1) { BX_EXTRAP_SK(float, 1); }
+                else if (D == 2) { BX_EXTRAP_SK(float, 2); }
+                else { BX_EXTRAP_SK(float, 3); }
             } else {
-                if (D == 1) BX_EXTRAP_S(double, 1);
-                else if (D == 2) BX_EXTRAP_S(double, 2);
-                else BX_EXTRAP_S(double, 3);
+                if (D == 1) { BX_EXTRAP_SK(double, 1); }
+                else if (D == 2) { BX_EXTRAP_SK(double, 2); }
+                else { BX_EXTRAP_SK(double, 3); }
             }
+#undef BX_EXTRAP_SK
 #undef BX_EXTRAP_S
             BX_TRY(body_launch(L, cudaGetLastError(), "extrapolation (shared memory)"));
         }
@@ -1213,6 +1255,7 @@ extern "C" int bamrex_level_set_body(bamrex_level* L, const bamrex_body_desc* de
     std::vector<long long> vol_p;
     size_t bytes_p = 0;
     int threads_p = 32;
+    const int rec_bytes = 8 * (D == 1 ? rec_words<1>() : (D == 2 ? rec_words<2>() : rec_words<3>()));
     for (int b = 0; b < nb; ++b) {
         if (bbox[6 * b] > bbox[6 * b + 3]) continue;
         long long n[3], hv = 1, vol = 1;
@@ -1222,7 +1265,8 @@ extern "C" int bamrex_level_set_body(bamrex_level* L, const bamrex_body_desc* de
             vol *= n[d];
         }
         const long long pencils = n[1] * n[2];
-        const size_t values = (size_t)hv * L->esize;
+        // the region's values (a ring comes on top only where it fits)
+        const size_t values = sweep_smem_bytes(hv, L->esize, 0, 1, rec_bytes);
         if (pencils > kPencilMax || values > (size_t)kSmemMax) {
             list_g.push_back(b);
         } else {
@@ -1232,6 +1276,15 @@ extern "C" int bamrex_level_set_body(bamrex_level* L, const bamrex_body_desc* de
             threads_p = std::max(threads_p, (int)((pencils + 31) / 32 * 32));
         }
     }
+    // the deepest ring (records in flight per thread) that fits
+    int ring = 1;
+    for (int K : { 4, 2 })
+        if (bytes_p + (size_t)threads_p * K * rec_bytes <= (size_t)kSmemMax) {
+            ring = K;
+            break;
+        }
+    S->ring = ring;
+    bytes_p += ring > 1 ? (size_t)threads_p * ring * rec_bytes : 0;
     const std::vector<int>& list_s = list_p;
     std::vector<long long> meta_off;
     long long meta_cells = 0;
@@ -1254,8 +1307,8 @@ extern "C" int bamrex_level_set_body(bamrex_level* L, const bamrex_body_desc* de
     };
     const size_t o_if = take2(sizeof(int) * 4 * n_if), o_iv = take2(sizeof(double) * L->NC * n_if);
     const size_t o_lg = take2(sizeof(int) * list_g.size()), o_lst = take2(sizeof(int) * list_s.size());
-    const size_t o_mo = take2(sizeof(long long) * meta_off.size()), o_code = take2((size_t)meta_cells);
-    const size_t o_w = take2(sizeof(double) * (D + 2) * (size_t)meta_cells);
+    const size_t o_mo = take2(sizeof(long long) * meta_off.size());
+    const size_t o_w = take2((size_t)rec_bytes * (size_t)meta_cells);
     e = dev_alloc((void**)&M2, off2, L->stream);
     if (e != cudaSuccess) {
         dev_free(S->mem, L->stream);
@@ -1266,7 +1319,6 @@ extern "C" int bamrex_level_set_body(bamrex_level* L, const bamrex_body_desc* de
     S->d_active = (int*)(M2 + o_lg);
     S->d_list_s = (int*)(M2 + o_lst);
     S->d_meta_off = (long long*)(M2 + o_mo);
-    S->d_code = (unsigned char*)(M2 + o_code);
     S->d_wts = (double*)(M2 + o_w);
     e = up(S->d_active, list_g.data(), sizeof(int) * list_g.size());
     if (e == cudaSuccess) e = up(S->d_list_s, list_s.data(), sizeof(int) * list_s.size());
@@ -1282,12 +1334,14 @@ extern "C" int bamrex_level_set_body(bamrex_level* L, const bamrex_body_desc* de
         for (size_t i = 0; i < list_s.size(); ++i)
             maxv = std::max(maxv, (i + 1 < list_s.size() ? meta_off[i + 1] : meta_cells) - meta_off[i]);
         const dim3 mg((unsigned)std::min<long long>(1024, (maxv + kBodyThreads - 1) / kBodyThreads), (unsigned)list_s.size());
-        if (D == 1) meta_kernel<1><<<mg, kBodyThreads, 0, L->stream>>>(S->d_list_s, S->n_smem, S->d_bbox, S->d_meta_off, S->d_ls_fab, S->d_flag_fab, L->dx[0], L->dx[1], L->dx[2], S->d_code, S->d_wts);
-        else if (D == 2) meta_kernel<2><<<mg, kBodyThreads, 0, L->stream>>>(S->d_list_s, S->n_smem, S->d_bbox, S->d_meta_off, S->d_ls_fab, S->d_flag_fab, L->dx[0], L->dx[1], L->dx[2], S->d_code, S->d_wts);
-        else meta_kernel<3><<<mg, kBodyThreads, 0, L->stream>>>(S->d_list_s, S->n_smem, S->d_bbox, S->d_meta_off, S->d_ls_fab, S->d_flag_fab, L->dx[0], L->dx[1], L->dx[2], S->d_code, S->d_wts);
+        if (D == 1) meta_kernel<1><<<mg, kBodyThreads, 0, L->stream>>>(S->d_list_s, S->n_smem, S->d_bbox, S->d_meta_off, S->d_ls_fab, S->d_flag_fab, L->dx[0], L->dx[1], L->dx[2], S->d_wts);
+        else if (D == 2) meta_kernel<2><<<mg, kBodyThreads, 0, L->stream>>>(S->d_list_s, S->n_smem, S->d_bbox, S->d_meta_off, S->d_ls_fab, S->d_flag_fab, L->dx[0], L->dx[1], L->dx[2], S->d_wts);
+        else meta_kernel<3><<<mg, kBodyThreads, 0, L->stream>>>(S->d_list_s, S->n_smem, S->d_bbox, S->d_meta_off, S->d_ls_fab, S->d_flag_fab, L->dx[0], L->dx[1], L->dx[2], S->d_wts);
         e = cudaGetLastError();
         L->launches++;
-        if (e == cudaSuccess) e = smem_attribute(L->fp32, D, (int)bytes_p);
+        if (e == cudaSuccess)
+            e = ring == 4 ? smem_attribute<4>(L->fp32, D, (int)bytes_p)
+                          : (ring == 2 ? smem_attribute<2>(L->fp32, D, (int)bytes_p) : smem_attribute<1>(L->fp32, D, (int)bytes_p));
     }
     if (e == cudaSuccess) e = cudaStreamSynchronize(L->stream);
     if (e != cudaSuccess) {

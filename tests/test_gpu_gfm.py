@@ -141,6 +141,9 @@ FILL_CASES = [(2, (40, 36), 3, "cylinder", 0), (2, (40, 36), 3, "cylinder", 1), 
               # pencil with CTA barriers
               (2, (96, 96), 1, "big_cylinder", 0),
               (3, (20, 20, 20), 1, "big_sphere", 0),
+              # a 28^3 box: values fit, a ring of two records per thread
+              # does not (the next record in registers instead)
+              (3, (28, 28, 28), 1, "big_sphere", 0),
               # one 32^3 box whose swept region with its halo exceeds shared
               # memory in FP64: the global-memory sweep kernel
               (3, (32, 32, 32), 1, "big_sphere", 0)]

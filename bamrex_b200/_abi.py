@@ -217,6 +217,7 @@ _vp, _i, _d, _ll = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_long
 _dp = ctypes.POINTER(ctypes.c_double)
 SIGNATURES = {
     "bamrex_abi_version": (_i, []),
+    "bamrex_release_memory": (_i, []),
     "bamrex_last_error": (ctypes.c_char_p, []),
     "bamrex_status_string": (ctypes.c_char_p, [_i]),
     "bamrex_parm_set_defaults": (_i, [ctypes.POINTER(CParm), _i]),

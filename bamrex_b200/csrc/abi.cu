@@ -236,6 +236,12 @@ extern "C" int bamrex_abi_version(void) { return BAMREX_ABI_VERSION; }
 
 extern "C" const char* bamrex_last_error(void) { return g_last_error.c_str(); }
 
+extern "C" int bamrex_release_memory(void)
+{
+    const int e = release_pooled();
+    return e ? cuda_fail((cudaError_t)e, "release_memory") : BAMREX_OK;
+}
+
 extern "C" const char* bamrex_status_string(int status)
 {
     switch (status) {

@@ -106,11 +106,17 @@ void dev_free(void* p, cudaStream_t s)
     cudaDeviceSynchronize();
     cudaFreeAsync(p, s);
     std::lock_guard<std::mutex> g(P.mu);
-    if (--P.live[dev] == 0 && P.pool[dev]) {
-        // nothing of this library left on the device: hand the pages back
-        cudaStreamSynchronize(s);
-        cudaMemPoolTrimTo(P.pool[dev], 0);
-    }
+    --P.live[dev];
+}
+
+int release_pooled()
+{
+    Pools& P = pools();
+    std::lock_guard<std::mutex> g(P.mu);
+    cudaError_t e = cudaDeviceSynchronize();
+    for (int d = 0; d < kMaxDevices && e == cudaSuccess; ++d)
+        if (P.pool[d]) e = cudaMemPoolTrimTo(P.pool[d], 0);
+    return e == cudaSuccess ? 0 : (int)e;
 }
 
 cudaError_t pinned_small_alloc(void** p, size_t bytes)

@@ -6,9 +6,9 @@
 // driver on every call (and cudaFree synchronises the device), which costs
 // from a millisecond to, on a loaded host, hundreds. These helpers take the
 // blocks from a stream-ordered pool per device that keeps freed blocks
-// (release threshold = unlimited), so the next level reuses the same pages.
-// The pool is trimmed back to nothing when the library holds no block on
-// that device any more.
+// (release threshold = unlimited), so the next level reuses the same pages,
+// also across hierarchies created one after the other.  The pages go back
+// to the driver at process exit or when release_pooled() is called.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -23,6 +23,10 @@ cudaError_t dev_alloc(void** p, size_t bytes, cudaStream_t s);
 
 // Give a block back (after a device-wide synchronisation, as cudaFree).
 void dev_free(void* p, cudaStream_t s);
+
+// Hand every page the pools keep but no block uses back to the driver
+// (0 or a cudaError_t).
+int release_pooled();
 
 // Small pinned host blocks (up to 4 KB) for the scalars a step reads back,
 // cut from pinned slabs that are kept for the life of the process.

@@ -81,6 +81,35 @@ def blast_3d(n=256, adiabatic=1.4, radius=0.2, centre=(0.5, 0.5, 0.5)):
     return consv_from_primv(3, q, adiabatic)
 
 
+def isentropic_vortex(D, n, prob_lo, prob_hi, centre, strength=5.0, scale=1.0, rho_bg=1.0, vel_bg=(0.0, 0.0, 0.0),
+                      p_bg=1.0, adiabatic=1.4, epsilon=1.0):
+    """The isentropic vortex of Exec/IsentropicVortex/Prob.cpp:87-123 at
+    time 0 on the cell centres of an n-cell box over [prob_lo, prob_hi]
+    (2D or 3D, the vortex uniform along z): with r^2 = |x - centre|^2 /
+    scale^2, dT = -(gamma-1) lambda^2 / (8 gamma pi^2) exp(1 - r^2),
+    rho = rho_bg + (1 + dT)^(1/(gamma-1)) - 1, p = p_bg + (1 + dT)^(gamma/
+    (gamma-1)) - 1, (u, v) = vel_bg + lambda / (2 pi) exp((1 - r^2)/2) (-y,
+    x) / scale.  scale = 1 is the reference's unit-core vortex."""
+    nx, ny = n[0], n[1]
+    nz = n[2] if D > 2 else 1
+    dx = [(prob_hi[d] - prob_lo[d]) / n[d] for d in range(D)]
+    x = (prob_lo[0] + (np.arange(nx) + 0.5) * dx[0] - centre[0]) / scale
+    y = (prob_lo[1] + (np.arange(ny) + 0.5) * dx[1] - centre[1]) / scale
+    X, Y = np.meshgrid(x, y)
+    r_sq = X * X + Y * Y
+    lam = strength
+    dT = -(adiabatic - 1) * lam * lam / (8 * adiabatic * np.pi * np.pi) * np.exp(1 - r_sq)
+    vel_mult = lam / (2 * np.pi) * np.exp((1 - r_sq) * 0.5)
+    q = np.zeros((D + 2, nz, ny, nx))
+    q[0] = rho_bg + (1 + dT) ** (1 / (adiabatic - 1)) - 1
+    q[1] = vel_bg[0] - vel_mult * Y
+    q[2] = vel_bg[1] + vel_mult * X
+    if D > 2:
+        q[3] = vel_bg[2]
+    q[1 + D] = p_bg + (1 + dT) ** (adiabatic / (adiabatic - 1)) - 1
+    return consv_from_primv(D, q, adiabatic, epsilon)
+
+
 def random_states(D, shape, seed=DEFAULT_SEED, adiabatic=1.4):
     """Random cells as Profiling/explicit_scaling.cpp:220-260: rho, p in
     [1,2], velocities in [-1,1] (our own seeded stream)."""

@@ -288,6 +288,7 @@ SIGNATURES = {
     "bamrex_amr_avg_down_all": (_i, [_vp]),
     "bamrex_amr_coarse_step": (_i, [_vp, _d, _dp, _dp]),
     "bamrex_amr_set_regrid_int": (_i, [_vp, _i]),
+    "bamrex_amr_set_body": (_i, [_vp, ctypes.POINTER(BodyDesc)]),
     "bamrex_amr_dt_level": (_i, [_vp, _dp]),
     "bamrex_amr_conserved_sums": (_i, [_vp, _dp]),
     "bamrex_helmholtz_create": (_i, [ctypes.POINTER(_vp), ctypes.POINTER(HelmholtzDesc), _vp]),

@@ -265,6 +265,16 @@ class Amr:
     def set_regrid_int(self, n):
         self._ck(lib().bamrex_amr_set_regrid_int(self._h, n))
 
+    def set_body(self, shapes, combine=_abi.SDF_UNION, rb_bc=_abi.RB_REFLECTIVE, stencil=2, fill_diagonals=False):
+        """A static rigid body on every level, present and future
+        (bamrex_amr_set_body); None removes it."""
+        from .level import body_desc
+        if shapes is None:
+            self._ck(lib().bamrex_amr_set_body(self._h, None))
+            return
+        d = body_desc(shapes, combine, rb_bc, stencil, fill_diagonals)
+        self._ck(lib().bamrex_amr_set_body(self._h, ctypes.byref(d)))
+
     def dt_level(self):
         out = (ctypes.c_double * _abi.MAX_LEVELS)()
         self._ck(lib().bamrex_amr_dt_level(self._h, out))

@@ -1376,6 +1376,10 @@ extern "C" int bamrex_level_est_time_step(bamrex_level* L, double* dt_est)
     cudaError_t e = cudaMemcpyAsync(L->h_scal, L->d_scal, sizeof(StepScalars), cudaMemcpyDeviceToHost, L->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(L->stream);
     if (e != cudaSuccess) return L->set_err(cuda_fail(e, "est_time_step"));
+    if (L->h_scal->status == BAMREX_ERR_ARG)
+        return L->set_err(fail(BAMREX_ERR_ARG, "a rigid-body interpolation stencil left the fab: raise ngrow"));
+    if (L->h_scal->status == BAMREX_ERR_NOT_CONVERGED)
+        return L->set_err(fail(BAMREX_ERR_NOT_CONVERGED, "an exact Riemann solve at a rigid-body interface did not converge"));
     L->ws_valid = true;
     const double ms = [&] {
         double v;

@@ -494,7 +494,6 @@ extern "C" int bamrex_coupling_create(bamrex_coupling** out, bamrex_level* crse,
     if (fine->D != D || fine->fp32 != crse->fp32 || fine->method != crse->method)
         return fail(BAMREX_ERR_ARG, "coarse and fine levels differ in dimension, precision or method");
     if (fine->stream != crse->stream) return fail(BAMREX_ERR_ARG, "coarse and fine levels must share a stream");
-    if (crse->body || fine->body) return fail(BAMREX_ERR_UNSUPPORTED, "rigid bodies on coupled AMR levels are not provided");
     if (fine->ngrow < 2) return fail(BAMREX_ERR_ARG, "fine ngrow must be >= 2");
     for (int d = 0; d < D; ++d) {
         if (fine->domain.lo[d] != crse->domain.lo[d] * r || fine->domain.hi[d] != (crse->domain.hi[d] + 1) * r - 1)
@@ -1231,6 +1230,8 @@ struct bamrex_amr {
     std::vector<double> dt_level;
     int steps = 0;
     bool have_dt = false;
+    bool has_body = false;     // a rigid body on every level (bamrex_amr_set_body)
+    bamrex_body_desc body;
     std::string err;
     int set_err(int code)
     {
@@ -1260,7 +1261,16 @@ int make_level(bamrex_amr* A, int lev, const std::vector<bamrex_box>& boxes, bam
     }
     d.boxes = boxes.data();
     d.nboxes = (int)boxes.size();
-    return bamrex_level_create(out, &d, A->stream);
+    BX_TRY(bamrex_level_create(out, &d, A->stream));
+    if (A->has_body) {
+        const int rc = bamrex_level_set_body(*out, &A->body);
+        if (rc != BAMREX_OK) {
+            bamrex_level_destroy(*out);
+            *out = nullptr;
+            return rc;
+        }
+    }
+    return BAMREX_OK;
 }
 
 void drop_levels_above(bamrex_amr* A, int lev)
@@ -1575,6 +1585,15 @@ extern "C" int bamrex_amr_coarse_step(bamrex_amr* A, double stop_time, double* t
     A->steps++;
     *time_io = time + A->dt_level[0];
     if (dt_out) *dt_out = A->dt_level[0];
+    return BAMREX_OK;
+}
+
+extern "C" int bamrex_amr_set_body(bamrex_amr* A, const bamrex_body_desc* desc)
+{
+    if (!A) return fail(BAMREX_ERR_ARG, "NULL hierarchy");
+    for (bamrex_level* L : A->levels) AMR_TRY(A, bamrex_level_set_body(L, desc));
+    A->has_body = desc != nullptr;
+    if (desc) A->body = *desc;
     return BAMREX_OK;
 }
 

@@ -186,6 +186,30 @@ class Packing:
 
 
 # ----------------------------------------------------------- level
+def body_desc(shapes, combine=_abi.SDF_UNION, rb_bc=_abi.RB_REFLECTIVE, stencil=2, fill_diagonals=False):
+    """bamrex_body_desc of one or two shape dicts (kind, center, axis,
+    radius, fluid_inside)."""
+    if isinstance(shapes, dict):
+        shapes = [shapes]
+    d = _abi.BodyDesc()
+    d.nshapes = len(shapes)
+    d.combine = int(combine)
+    for n, sh in enumerate(shapes):
+        f = d.shapes[n]
+        f.kind = int(sh["kind"])
+        for q in range(3):
+            c = sh.get("center", (0.0, 0.0, 0.0))
+            a = sh.get("axis", (0.0, 0.0, 1.0))
+            f.center[q] = float(c[q]) if q < len(c) else 0.0
+            f.axis[q] = float(a[q]) if q < len(a) else 0.0
+        f.radius = float(sh.get("radius", 0.0))
+        f.fluid_inside = 1 if sh.get("fluid_inside", False) else 0
+    d.rb_bc = int(rb_bc)
+    d.stencil = int(stencil)
+    d.fill_diagonals = 1 if fill_diagonals else 0
+    return d
+
+
 class Level:
     """One AMR level on the device (all boxes in one box table)."""
 
@@ -332,24 +356,7 @@ class Level:
         if shapes is None:
             self._ck(lib().bamrex_level_set_body(self._h, None))
             return
-        if isinstance(shapes, dict):
-            shapes = [shapes]
-        d = _abi.BodyDesc()
-        d.nshapes = len(shapes)
-        d.combine = int(combine)
-        for n, sh in enumerate(shapes):
-            f = d.shapes[n]
-            f.kind = int(sh["kind"])
-            for q in range(3):
-                c = sh.get("center", (0.0, 0.0, 0.0))
-                a = sh.get("axis", (0.0, 0.0, 1.0))
-                f.center[q] = float(c[q]) if q < len(c) else 0.0
-                f.axis[q] = float(a[q]) if q < len(a) else 0.0
-            f.radius = float(sh.get("radius", 0.0))
-            f.fluid_inside = 1 if sh.get("fluid_inside", False) else 0
-        d.rb_bc = int(rb_bc)
-        d.stencil = int(stencil)
-        d.fill_diagonals = 1 if fill_diagonals else 0
+        d = body_desc(shapes, combine, rb_bc, stencil, fill_diagonals)
         self._ck(lib().bamrex_level_set_body(self._h, ctypes.byref(d)))
 
     def fill_body_ghosts(self):

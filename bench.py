@@ -441,7 +441,7 @@ def rigid_body_run(D, n, mgs, precision, steps=10, vortex=False):
     boxes = decompose(D, (0,) * D, tuple(x - 1 for x in n), mgs)
     # cubic cells: the domain is [0, 1] along x
     lev = bx.Level(D, (0,) * D, tuple(x - 1 for x in n), [0.0] * D, [n[d] / n[0] for d in range(D)], boxes, bx.Parm(D),
-                   cfl=0.8, ngrow=3, precision=precision)
+                   cfl=0.8, ngrow=4, precision=precision)
     shp = (n[2] if D > 2 else 1, n[1], n[0])
     gamma = 1.4
     hi_phys = [n[d] / n[0] for d in range(D)]

@@ -392,8 +392,9 @@ typedef struct bamrex_body_desc {
  * valid cells (Source/GFM/GFMFlag.cpp:60-83), all on the device.  From then
  * on every bamrex_level_advance / _run starts with the rigid-body ghost fill
  * below (AmrLevelAdv_advance.cpp:110-116).  desc == NULL removes the body.
- * Single levels only: a level with a coarse/fine coupling is refused. */
-BAMREX_API int bamrex_level_set_body(bamrex_level *level, const bamrex_body_desc *desc);
+ * On a coupled AMR level the fill leaves the coarse/fine ghost cells as the
+ * coupling's fill_patch set them. */
+BAMREX_API int bamrex_level_set_body(bamrex_level *level, const bamrex_body_desc *desc); /* ngrow >= 4 */
 
 /* The rigid-body ghost fill on the current state (FluidSystem::FillRBGhostCells
  * = fill_ghost_rb, Source/GFM/RigidBody.cpp:24-170, then fill_consv_boundary):
@@ -545,6 +546,12 @@ BAMREX_API int bamrex_amr_avg_down_all(bamrex_amr *amr);
 BAMREX_API int bamrex_amr_coarse_step(bamrex_amr *amr, double stop_time, double *time_io, double *dt_out);
 /* Change amr.regrid_int (0: no more regrids). */
 BAMREX_API int bamrex_amr_set_regrid_int(bamrex_amr *amr, int regrid_int);
+/* A static rigid body on every level of the hierarchy, present and future
+ * (bamrex_level_set_body on each; each level computes its level set at its
+ * own resolution, as every AmrLevelAdv level does in initData); NULL
+ * removes it.  The fill runs after each level's coarse/fine ghost fill
+ * (FillPatcherFill, then FillRBGhostCells). */
+BAMREX_API int bamrex_amr_set_body(bamrex_amr *amr, const bamrex_body_desc *desc);
 /* dt of every level after the last computeInitialDt / computeNewDt. */
 BAMREX_API int bamrex_amr_dt_level(const bamrex_amr *amr, double *dt_level);
 /* Composite conserved totals: every level's sums minus those of its cells

@@ -416,6 +416,17 @@ class OAmr:
         self.dt_level = [0.0] * len(self.levels)
         self.steps = 0
         self.time = 0.0
+        self.bodies = None
+
+    def set_bodies(self, shapes, combine, prob_lo, rb_bc, adiabatic, epsilon=1.0, stencil=2, fill_diagonals=False):
+        """A static rigid body on every level (its level set at the level's
+        resolution, as every AmrLevelAdv level builds in initData); each
+        level's advance then runs FillRBGhostCells after its coarse/fine
+        ghost fill (Source/AmrLevelAdv_advance.cpp:108-116)."""
+        from oracle import gfm_oracle as G
+        self.bodies = [G.Body(L.lay, shapes, combine, prob_lo, stencil=stencil, fill_diagonals=fill_diagonals)
+                       for L in self.levels]
+        self.body_args = (rb_bc, adiabatic, epsilon)
 
     def avg_down_all(self):
         for l in range(len(self.levels) - 1, 0, -1):
@@ -447,6 +458,9 @@ class OAmr:
         L.lay.fill_boundary(L.S)
         if l > 0:
             self.cpl[l].fill_patch(time, [L.S])
+        if self.bodies is not None:
+            from oracle import gfm_oracle as G
+            G.fill_rb(L.lay, L.S, self.bodies[l], *self.body_args)
         S2 = L.S.copy()
         fl = L.lay.advance_explicit_fluxes(L.S, S2, time, dt, self.method, self.parm)
         if l + 1 < len(self.levels):

@@ -394,7 +394,10 @@ def fill_rb(lay, buf, body, rb_bc, gamma, eps):
         bg = lay.begins[b]
 
         def src(i, j, k, n, f=f, bg=bg):
-            return float(f[n, k - bg[2], j - bg[1], i - bg[0]])
+            idx = (k - bg[2], j - bg[1], i - bg[0])
+            if any(q < 0 or q >= s for q, s in zip(idx, f.shape[1:])):
+                raise IndexError("interpolation stencil outside the fab: more ghost cells needed")
+            return float(f[n, idx[0], idx[1], idx[2]])
 
         for k in range(lo[2], hi[2] + 1):
             for j in range(lo[1], hi[1] + 1):

@@ -211,7 +211,7 @@ def test_sdf_shapes():
 
 # ---- the rigid-body fill on the CPU ------------------------------------------
 
-def _cylinder_level(n=24, nbox=2, ngrow=3):
+def _cylinder_level(n=24, nbox=2, ngrow=4):
     D = 2
     half = n // nbox
     boxes = [((i * half, 0), ((i + 1) * half - 1, n - 1)) for i in range(nbox)]

@@ -288,7 +288,11 @@ BAMREX_API int bamrex_level_advance(bamrex_level *level, double time, double dt,
                          double *dt_out);
 
 /* AmrLevelAdv::estTimeStep (Source/AmrLevelAdv.cpp:395-477) on the current
- * state: cfl * min_d dx_d / max(|u| + c).  Synchronises the stream. */
+ * state: cfl * min_d dx_d / max(|u| + c).  Synchronises the stream.  On a
+ * level with a rigid body it also reports what the fills since the last
+ * call recorded: BAMREX_ERR_ARG when an interface's interpolation stencil
+ * left the fab (ngrow too small), BAMREX_ERR_NOT_CONVERGED when an exact
+ * Riemann solve at the interface took its 200 Newton iterations. */
 BAMREX_API int bamrex_level_est_time_step(bamrex_level *level, double *dt_est);
 
 /* The coarse-step loop of a single-level run (Amr::coarseTimeStep with

@@ -274,3 +274,64 @@ def test_rb_fill_reflective_interface_states():
     assert big.sum() > 4
     assert np.all(np.sign(p[big] - 1.0) == -np.sign(un_in[big]))
     assert np.all(out[0, 0] > 0)
+
+
+# ---- conditioning of a hierarchy step with a body --------------------------
+
+def _blob_state(D, n, seed):
+    rng = np.random.default_rng(seed)
+    x = (np.arange(n) + 0.5) / n
+    g = np.meshgrid(*([x] * D), indexing="ij")
+    shp = (1,) * (3 - D) + (n,) * D
+    ph = rng.uniform(0, 2 * np.pi, 3)
+    q = np.zeros((D + 2,) + shp)
+    q[0] = np.transpose(1 + 0.2 * np.sin(2 * np.pi * g[0] + ph[0]) * np.cos(2 * np.pi * g[-1] + ph[1])).reshape(shp)
+    q[D + 1] = np.transpose(1 + 0.1 * np.cos(2 * np.pi * g[-1] + ph[2])).reshape(shp)
+    q[1] = 0.3
+    return np.array(G.consv_from_primv(list(q), D, 1.4, 1.0))
+
+
+def _hierarchy_step_with_sphere(limiter_indices, rel_noise):
+    from oracle import oracle as O
+    from oracle.amr_oracle import OAmr
+    D, n = 3, 16
+    levels = [O.decompose(D, (0, 0, 0), (n - 1,) * 3, n // 2),
+              O.decompose(D, (n // 2,) * 3, (n + n // 2 - 1,) * 3, n // 2)]
+    OA = OAmr(D, (0, 0, 0), (n - 1,) * 3, [0.0] * D, [1.0] * D, levels,
+              O.Parm(D, limiter=O.VAN_LEER, limiter_indices=limiter_indices), O.MUSCL_HANCOCK, 0.8, ngrow=4)
+    OA.set_bodies([G.make_shape(G.SPHERE, (0.5, 0.5, 0.5), radius=0.17)], 0, (0.0,) * D, G.REFLECTIVE, 1.4)
+    rng = np.random.default_rng(7)
+    for l in range(2):
+        u = _blob_state(D, n * 2 ** l, 11)
+        if l == 1:
+            u = u * (1 + rel_noise * rng.standard_normal(u.shape))
+        OA.levels[l].set_dense(u)
+    OA.avg_down_all()
+    OA.coarse_step()
+    return [OA.levels[l].dense() for l in range(2)]
+
+
+def _max_change(a, b):
+    return max(float(np.nanmax(np.abs(x - y))) for x, y in zip(a, b))
+
+
+def test_oracle_body_limiter_sensitivity():
+    """Why the 3D hierarchy-with-body parity case limits every component on
+    itself. The reference limits every component on the energy's ratio by
+    default, and its ratio has a 0/0 branch (both differences exactly zero:
+    phi(1), a full slope; both at the rounding level: an arbitrary ratio).
+    Next to the sphere the energy is flat to the last bit while density and
+    momentum are not, so a relative change of 1e-15 in the fine level's input
+    (the size of the coarse/fine interpolation's rounding differences between
+    two machines) moves the restatement's own result after one coarse step by
+    1e-8 or more; limited component by component the same change stays at
+    the rounding level."""
+    from oracle import oracle as O
+    default = [1 + 3] * O.MAX_NCOMP
+    own = list(range(5)) + [4] * (O.MAX_NCOMP - 5)
+    base = _hierarchy_step_with_sphere(default, 0.0)
+    moved = _hierarchy_step_with_sphere(default, 1e-15)
+    assert _max_change(base, moved) > 1e-9
+    base = _hierarchy_step_with_sphere(own, 0.0)
+    moved = _hierarchy_step_with_sphere(own, 1e-15)
+    assert _max_change(base, moved) < 1e-13

@@ -586,7 +586,113 @@ def quadrant_initial_data(pp: ParmParse, s: Settings):
     return fn
 
 
-INITIAL_DATA = {"quadrant": quadrant_initial_data}
+def _two_states(s, prim_a, prim_b):
+    import numpy as np
+    from .problems import consv_from_primv
+    D = s.spacedim
+    out = []
+    for prim in (prim_a, prim_b):
+        q = np.array(prim, dtype=np.float64).reshape(D + 2, 1)
+        out.append(consv_from_primv(D, q, s.parm.adiabatic, s.parm.epsilon)[:, 0])
+    return out
+
+
+def _fill(D, mask, inside, outside):
+    import numpy as np
+    out = np.empty((D + 2,) + mask.shape)
+    for n in range(D + 2):
+        out[n] = np.where(mask, inside[n], outside[n])
+    return out
+
+
+def _mesh(amr, lev):
+    import numpy as np
+    x, y, z = amr.cell_centres(lev)
+    shape = (len(z), len(y), len(x))
+    return (np.broadcast_to(x[None, None, :], shape), np.broadcast_to(y[None, :, None], shape),
+            np.broadcast_to(z[:, None, None], shape))
+
+
+def riemann_initial_data(pp: ParmParse, s: Settings):
+    """initdata_euler of the reference's Riemann problem
+    (Exec/RiemannProblem/Prob.cpp:33-118): init.{density,velocity,
+    pressure}_{L,R}; in 1D the left state where x < (prob_lo + prob_hi)/2
+    with the velocity along x, in 2D and 3D the left state where y < 0.5 (a
+    fixed 0.5, as there) with the velocity along y. The exact-solution file
+    the reference also writes is not written."""
+    D = s.spacedim
+    init = pp.sub("init")
+    vals = {k: init.get(k, float) for k in ("density_L", "velocity_L", "pressure_L", "density_R", "velocity_R",
+                                            "pressure_R")}
+    vel = lambda v: [v] + [0.0] * (D - 1) if D == 1 else [0.0, v] + [0.0] * (D - 2)
+    left, right = _two_states(s, [vals["density_L"]] + vel(vals["velocity_L"]) + [vals["pressure_L"]],
+                              [vals["density_R"]] + vel(vals["velocity_R"]) + [vals["pressure_R"]])
+
+    def fn(amr, lev):
+        X, Y, _ = _mesh(amr, lev)
+        mask = X < (s.prob_lo[0] + s.prob_hi[0]) * 0.5 if D == 1 else Y < 0.5
+        return _fill(D, mask, left, right)
+    return fn
+
+
+def explosion_initial_data(pp: ParmParse, s: Settings):
+    """initdata of the reference's cylindrical explosion
+    (Exec/CylindricalExplosion/Prob.cpp:20-92): init.{density,pressure}_in
+    at rest where r < init.radius, init.{density,pressure}_out elsewhere,
+    r the distance from (1, 1, 1) (1D: r = x; 2D with init.setup_as_rp: x
+    or y by sym.rot_axis; 3D with init.force_cylindrical: the distance from
+    the line x = y = 1). init.radius has no default there (an unset value
+    is read uninitialised); here it is required."""
+    import numpy as np
+    D = s.spacedim
+    init = pp.sub("init")
+    d_in, p_in = init.get("density_in", float), init.get("pressure_in", float)
+    d_out, p_out = init.get("density_out", float), init.get("pressure_out", float)
+    radius = init.get("radius", float)
+    as_rp = init.query("setup_as_rp", bool, False)
+    cylindrical = init.query("force_cylindrical", bool, False)
+    rot_axis = pp.sub("sym").get("rot_axis", int) if as_rp else 0
+    inside, outside = _two_states(s, [d_in] + [0.0] * D + [p_in], [d_out] + [0.0] * D + [p_out])
+
+    def fn(amr, lev):
+        X, Y, Z = _mesh(amr, lev)
+        if D == 1:
+            r = X
+        elif D == 2:
+            r = (X if rot_axis == 0 else Y) if as_rp else np.sqrt((X - 1) * (X - 1) + (Y - 1) * (Y - 1))
+        elif cylindrical:
+            r = np.sqrt((X - 1) * (X - 1) + (Y - 1) * (Y - 1))
+        else:
+            r = np.sqrt((X - 1) * (X - 1) + (Y - 1) * (Y - 1) + (Z - 1) * (Z - 1))
+        return _fill(D, r < radius, inside, outside)
+    return fn
+
+
+def vortex_initial_data(pp: ParmParse, s: Settings):
+    """initdata of the reference's isentropic vortex
+    (Exec/IsentropicVortex/Prob.cpp:25-123 at time 0): init.lambda,
+    init.{density,u,v,w,pressure}_bg, centre (init.x_c, init.y_c). The
+    exact-solution file the reference also writes is not written."""
+    from .problems import isentropic_vortex
+    D = s.spacedim
+    if D < 2:
+        raise InputsError("the isentropic vortex needs two or three dimensions")
+    init = pp.sub("init")
+    lam = init.get("lambda", float)
+    rho, p = init.get("density_bg", float), init.get("pressure_bg", float)
+    vel = (init.get("u_bg", float), init.get("v_bg", float), init.get("w_bg", float))
+    centre = (init.get("x_c", float), init.get("y_c", float))
+
+    def fn(amr, lev):
+        lo, hi = amr.domain(lev)
+        n = [hi[d] - lo[d] + 1 for d in range(3)]
+        return isentropic_vortex(D, n, list(s.prob_lo), list(s.prob_hi), centre, strength=lam, rho_bg=rho,
+                                 vel_bg=vel, p_bg=p, adiabatic=s.parm.adiabatic, epsilon=s.parm.epsilon)
+    return fn
+
+
+INITIAL_DATA = {"QuadrantProblem": quadrant_initial_data, "RiemannProblem": riemann_initial_data,
+                "CylindricalExplosion": explosion_initial_data, "IsentropicVortex": vortex_initial_data}
 
 
 def plotfile_name(prefix: str, step: int) -> str:
@@ -596,14 +702,14 @@ def plotfile_name(prefix: str, step: int) -> str:
 
 
 def main(argv=None):
-    """python -m bamrex_b200.inputs --problem quadrant --dim 2 INPUTS
+    """python -m bamrex_b200.inputs --problem QuadrantProblem --dim 2 INPUTS
     [name=value ...]: the reference's executable for that problem on the
     device, with its plotfiles."""
     import argparse
     from .plotfile import write_amr_plotfile
     ap = argparse.ArgumentParser(description=main.__doc__)
     ap.add_argument("--problem", required=True, choices=sorted(INITIAL_DATA))
-    ap.add_argument("--dim", type=int, required=True, choices=(2, 3))
+    ap.add_argument("--dim", type=int, required=True, choices=(1, 2, 3))
     ap.add_argument("--fp32-storage", action="store_true")
     ap.add_argument("inputs")
     ap.add_argument("overrides", nargs="*")

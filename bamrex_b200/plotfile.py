@@ -1,7 +1,9 @@
-"""AMReX plotfiles of a hierarchy, as the reference's writePlotFile leaves
-them (Source/AmrLevelAdv.cpp:117-135 fills the rigid-body ghosts with
-first-order extrapolation, then AMReX's AmrLevel::writePlotFile writes
-every state component).
+"""AMReX plotfiles of a hierarchy (the reference's writePlotFile,
+Source/AmrLevelAdv.cpp:117-135, hands its state to AMReX's
+AmrLevel::writePlotFile). With a rigid body the reference first refills
+the cells inside the body by first-order extrapolation for nicer pictures;
+write_amr_plotfile writes them as the last step's rigid-body fill left
+them. The fluid cells are the same either way.
 
 Layout (AMReX's native plotfile format, "HyperCLaw-V1.1", restated from
 its published description):

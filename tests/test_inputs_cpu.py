@@ -340,16 +340,89 @@ def test_quadrant_initial_data(D):
     from bamrex_b200.problems import consv_from_primv
     pp = _pp(QUADRANT_2D + QUADRANT_STATES)
     s = I.read_settings(pp, D)
-    u = I.INITIAL_DATA["quadrant"](pp, s)(_Centres(D, 8), 0)
+    u = I.INITIAL_DATA["QuadrantProblem"](pp, s)(_Centres(D, 8), 0)
     assert u.shape == (D + 2,) + ((8,) if D == 3 else (1,)) + (8, 8)
     for (j, i), prim in (((7, 7), (0.5313, 0, 0, 0.4)), ((7, 0), (1, 0.7276, 0, 1)), ((0, 0), (0.8, 0, 0, 1)),
                          ((0, 7), (1, 0, 0.7276, 1))):
         q = np.array(list(prim[:3]) + [0.0] * (D - 2) + [prim[3]]).reshape(D + 2, 1)
         np.testing.assert_array_equal(u[:, 0, j, i], consv_from_primv(D, q, 1.4, 0.5)[:, 0])
     with pytest.raises(I.InputsError, match="init.pressure_BR not found"):
-        I.INITIAL_DATA["quadrant"](_pp(QUADRANT_2D + QUADRANT_STATES.replace("init.pressure_BR", "#")), s)
+        I.INITIAL_DATA["QuadrantProblem"](_pp(QUADRANT_2D + QUADRANT_STATES.replace("init.pressure_BR", "#")), s)
 
 
 def test_plotfile_names():
     assert I.plotfile_name("out/plt", 10) == "out/plt00010"
     assert I.plotfile_name("chk", 123456) == "chk123456"
+
+
+class _Level:
+    """Cell centres and domain of one level over [lo, hi]^D with n cells."""
+
+    def __init__(self, D, n, lo=0.0, hi=1.0):
+        self.D, self.n, self.lo, self.hi = D, n, lo, hi
+
+    def cell_centres(self, lev):
+        x = self.lo + (np.arange(self.n) + 0.5) * (self.hi - self.lo) / self.n
+        return [x if d < self.D else np.zeros(1) for d in range(3)]
+
+    def domain(self, lev):
+        return (0, 0, 0), tuple(self.n - 1 if d < self.D else 0 for d in range(3))
+
+
+def _prim(D, rho, vel, p):
+    from bamrex_b200.problems import consv_from_primv
+    q = np.array([rho] + list(vel) + [p], dtype=np.float64).reshape(D + 2, 1)
+    return consv_from_primv(D, q, 1.4, 0.5)[:, 0]
+
+
+RIEMANN = ("init.density_L = 1\ninit.velocity_L = 0.75\ninit.pressure_L = 1\n"
+           "init.density_R = 0.125\ninit.velocity_R = 0\ninit.pressure_R = 0.1\n")
+
+
+@pytest.mark.parametrize("D", [1, 2, 3])
+def test_riemann_initial_data(D):
+    pp = _pp(QUADRANT_2D + RIEMANN)
+    s = I.read_settings(pp, D)
+    u = I.INITIAL_DATA["RiemannProblem"](pp, s)(_Level(D, 8), 0)
+    vel_l = [0.75] + [0.0] * (D - 1) if D == 1 else [0.0, 0.75] + [0.0] * (D - 2)
+    left, right = _prim(D, 1, vel_l, 1), _prim(D, 0.125, [0.0] * D, 0.1)
+    if D == 1:  # split at the middle of [0, 2] in x
+        np.testing.assert_array_equal(u[:, 0, 0, 7], left)
+    else:       # split at y = 0.5
+        np.testing.assert_array_equal(u[:, 0, 3, 7], left)
+        np.testing.assert_array_equal(u[:, 0, 4, 0], right)
+
+
+def test_explosion_initial_data():
+    text = QUADRANT_2D + ("init.density_in = 1\ninit.pressure_in = 10\ninit.density_out = 0.125\n"
+                          "init.pressure_out = 0.1\ninit.radius = 0.4\n")
+    pp = _pp(text)
+    s = I.read_settings(pp, 3)
+    u = I.INITIAL_DATA["CylindricalExplosion"](pp, s)(_Level(3, 10, 0.0, 2.0), 0)
+    inside, outside = _prim(3, 1, [0, 0, 0], 10), _prim(3, 0.125, [0, 0, 0], 0.1)
+    np.testing.assert_array_equal(u[:, 5, 5, 5], inside)   # centre (1.1, 1.1, 1.1): r = 0.17
+    np.testing.assert_array_equal(u[:, 0, 5, 5], outside)  # z far from 1
+    pp = _pp(text + "init.force_cylindrical = true\n")
+    u = I.INITIAL_DATA["CylindricalExplosion"](pp, s)(_Level(3, 10, 0.0, 2.0), 0)
+    np.testing.assert_array_equal(u[:, 0, 5, 5], inside)   # a cylinder along z
+    pp = _pp(text + "init.setup_as_rp = 1\n")
+    with pytest.raises(I.InputsError, match="sym.rot_axis not found"):
+        I.INITIAL_DATA["CylindricalExplosion"](pp, I.read_settings(pp, 2))
+    pp = _pp(text + "init.setup_as_rp = 1\nsym.rot_axis = 1\n")
+    u = I.INITIAL_DATA["CylindricalExplosion"](pp, I.read_settings(pp, 2))(_Level(2, 10), 0)
+    np.testing.assert_array_equal(u[:, 0, 1, 9], _prim(2, 1, [0, 0], 10))  # r = y = 0.15
+    np.testing.assert_array_equal(u[:, 0, 4, 0], _prim(2, 0.125, [0, 0], 0.1))  # r = y = 0.45
+    with pytest.raises(I.InputsError, match="init.radius not found"):
+        I.INITIAL_DATA["CylindricalExplosion"](_pp(text.replace("init.radius", "#")), s)
+
+
+def test_vortex_initial_data():
+    from bamrex_b200.problems import isentropic_vortex
+    text = QUADRANT_2D + ("init.lambda = 5\ninit.density_bg = 1\ninit.u_bg = 0.1\ninit.v_bg = 0.2\n"
+                          "init.w_bg = 0\ninit.pressure_bg = 1\ninit.x_c = 1\ninit.y_c = 0.5\n")
+    pp = _pp(text)
+    s = I.read_settings(pp, 2)
+    u = I.INITIAL_DATA["IsentropicVortex"](pp, s)(_Level(2, 16), 0)
+    ref = isentropic_vortex(2, [16, 16, 1], [0.0, 0.0], [2.0, 1.0], (1.0, 0.5), strength=5.0, vel_bg=(0.1, 0.2, 0.0),
+                            adiabatic=1.4, epsilon=0.5)
+    np.testing.assert_array_equal(u, ref)

@@ -19,7 +19,9 @@ interface tagging) raise NotImplementedError naming the setting.
 
 The file format is ParmParse's: `name = value value ...` up to the end of
 the line, `#` starts a comment, a double-quoted value is one token,
-`FILE = path` reads another inputs file in place, and when a name is
+`FILE = path` reads another inputs file in place (a relative path from
+the working directory, as AMReX opens it, else from the including file's
+directory), and when a name is
 defined more than once the last definition is the one read. Command-line
 `name=value` arguments after the file are read as later definitions.
 """
@@ -65,7 +67,9 @@ def parse_text(text: str, base_dir: str = ".", table=None, _depth=0):
         if name == "FILE":
             if len(values) != 1:
                 raise InputsError("line %d: FILE takes one path" % lineno)
-            path = values[0] if os.path.isabs(values[0]) else os.path.join(base_dir, values[0])
+            path = values[0]
+            if not os.path.isabs(path) and not os.path.exists(path):
+                path = os.path.join(base_dir, path)
             with open(path) as f:
                 parse_text(f.read(), os.path.dirname(path), table, _depth + 1)
             continue

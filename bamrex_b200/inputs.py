@@ -18,7 +18,9 @@ defaults and refusals; settings of parts this package does not build
 interface tagging) raise NotImplementedError naming the setting.
 
 The file format is ParmParse's: `name = value value ...` up to the end of
-the line, `#` starts a comment, a double-quoted value is one token,
+the line, `#` starts a comment, a double-quoted value is one token, a
+number may be an arithmetic expression over other entries (`t_0 = D*6/M`,
+`stop_time = t_0+0.0015`; + - * / ^, sqrt, exp, log, sin, cos, ..., pi),
 `FILE = path` reads another inputs file in place (a relative path from
 the working directory, as AMReX opens it, else from the including file's
 directory), and when a name is
@@ -27,7 +29,9 @@ defined more than once the last definition is the one read. Command-line
 """
 from __future__ import annotations
 
+import ast
 import math
+import operator
 import os
 import shlex
 from dataclasses import dataclass, field
@@ -49,7 +53,54 @@ def _tokens(line: str):
     lex.whitespace_split = True
     lex.commenters = "#"
     lex.quotes = '"'
-    return list(lex)
+    lex.escape = ""
+    try:
+        return list(lex)
+    except ValueError as e:
+        raise InputsError("cannot split %r: %s" % (line.strip(), e)) from None
+
+
+_BINOPS = {ast.Add: operator.add, ast.Sub: operator.sub, ast.Mult: operator.mul, ast.Div: operator.truediv,
+           ast.Pow: operator.pow, ast.Mod: operator.mod}
+_UNOPS = {ast.UAdd: operator.pos, ast.USub: operator.neg}
+_FUNCS = {"sqrt": math.sqrt, "exp": math.exp, "log": math.log, "log10": math.log10, "sin": math.sin,
+          "cos": math.cos, "tan": math.tan, "asin": math.asin, "acos": math.acos, "atan": math.atan,
+          "atan2": math.atan2, "sinh": math.sinh, "cosh": math.cosh, "tanh": math.tanh, "abs": abs,
+          "fabs": abs, "floor": math.floor, "ceil": math.ceil, "pow": math.pow, "min": min, "max": max}
+_CONSTS = {"pi": math.pi}
+
+
+def _eval_expr(text: str, symbol):
+    """Value of an arithmetic expression (+ - * / ^ **, parentheses, the
+    functions of _FUNCS, pi) whose names are looked up by symbol(name)."""
+    try:
+        tree = ast.parse(text.replace("^", "**"), mode="eval")
+    except SyntaxError:
+        raise ValueError(text) from None
+
+    def ev(node):
+        if isinstance(node, ast.Expression):
+            return ev(node.body)
+        if isinstance(node, ast.Constant) and isinstance(node.value, (int, float)):
+            return node.value
+        if isinstance(node, ast.BinOp) and type(node.op) in _BINOPS:
+            return _BINOPS[type(node.op)](ev(node.left), ev(node.right))
+        if isinstance(node, ast.UnaryOp) and type(node.op) in _UNOPS:
+            return _UNOPS[type(node.op)](ev(node.operand))
+        if isinstance(node, ast.Call) and isinstance(node.func, ast.Name) and node.func.id in _FUNCS \
+                and not node.keywords:
+            return _FUNCS[node.func.id](*[ev(a) for a in node.args])
+        if isinstance(node, ast.Name):
+            return _CONSTS[node.id] if node.id in _CONSTS else symbol(node.id)
+        if isinstance(node, ast.Attribute):
+            parts = []
+            while isinstance(node, ast.Attribute):
+                parts.append(node.attr)
+                node = node.value
+            if isinstance(node, ast.Name):
+                return symbol(".".join([node.id] + parts[::-1]))
+        raise ValueError(text)
+    return ev(tree)
 
 
 def parse_text(text: str, base_dir: str = ".", table=None, _depth=0):
@@ -70,6 +121,9 @@ def parse_text(text: str, base_dir: str = ".", table=None, _depth=0):
             path = values[0]
             if not os.path.isabs(path) and not os.path.exists(path):
                 path = os.path.join(base_dir, path)
+            if not os.path.exists(path):
+                raise InputsError("line %d: FILE = %s: no such file (from the working directory or %s)"
+                                  % (lineno, values[0], base_dir))
             with open(path) as f:
                 parse_text(f.read(), os.path.dirname(path), table, _depth + 1)
             continue
@@ -140,8 +194,20 @@ class ParmParse:
         p = self.prefix + "." if self.prefix else ""
         return sorted({n[len(p):] for n, _ in self._table if n.startswith(p)})
 
-    @staticmethod
-    def _convert(full, tok, typ):
+    def _symbol(self, name, seen):
+        """A number-valued entry named in an expression: under this prefix
+        first, then as written."""
+        for full in ((self._full(name), name) if self.prefix else (name,)):
+            if full in seen:
+                raise InputsError("%s refers to itself" % full)
+            for n, v in reversed(self._table):
+                if n == full:
+                    if len(v) != 1:
+                        raise InputsError("%s: an expression needs a single value" % full)
+                    return self._convert(full, v[0], float, seen | {full})
+        raise InputsError("unknown name %r in an expression" % name)
+
+    def _convert(self, full, tok, typ, seen=frozenset()):
         try:
             if typ is bool:
                 t = tok.lower()
@@ -150,12 +216,20 @@ class ParmParse:
                 if t in ("false", "f", "0"):
                     return False
                 raise ValueError(tok)
-            if typ is int:
-                return int(tok)
-            if typ is float:
-                return float(tok)
+            if typ in (int, float):
+                try:
+                    return typ(tok)
+                except ValueError:
+                    v = _eval_expr(tok, lambda name: self._symbol(name, seen | {full}))
+                    if typ is int:
+                        if float(v) != int(v):
+                            raise ValueError(tok)
+                        return int(v)
+                    return float(v)
             return str(tok)
-        except ValueError:
+        except InputsError:
+            raise
+        except (ValueError, ZeroDivisionError, OverflowError, TypeError):
             raise InputsError("%s: cannot read %r as %s" % (full, tok, typ.__name__)) from None
 
     def query(self, name, typ=str, default=None):

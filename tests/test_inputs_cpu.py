@@ -426,3 +426,34 @@ def test_vortex_initial_data():
     ref = isentropic_vortex(2, [16, 16, 1], [0.0, 0.0], [2.0, 1.0], (1.0, 0.5), strength=5.0, vel_bg=(0.1, 0.2, 0.0),
                             adiabatic=1.4, epsilon=0.5)
     np.testing.assert_array_equal(u, ref)
+
+
+# ---- arithmetic values (ParmParse evaluates them against other entries) ------
+
+def test_expressions():
+    pp = _pp("D = 0.01\nM = 2\nadia = 1.4\np_amb = 1\nrho_amb = 1\n"
+             "t_0 = (D*6/(M*sqrt(adia*p_amb/rho_amb)))\nstop_time = t_0+0.0015\n"
+             "amr.plot_at = t_0 t_0+0.0002\namr.n_cell = 2*4 2^3\nhalf = 3/2\n"
+             "init.r = 0.25\ninit.area = pi*r^2\nr = 7\nloop_a = loop_b\nloop_b = \"loop_a + 1\"\n")
+    t0 = 0.01 * 6 / (2 * (1.4 ** 0.5))
+    assert pp.get("t_0", float) == pytest.approx(t0, rel=1e-15)
+    assert pp.get("stop_time", float) == pytest.approx(t0 + 0.0015, rel=1e-15)
+    assert pp.sub("amr").getarr("plot_at", float) == pytest.approx([t0, t0 + 0.0002], rel=1e-15)
+    assert pp.sub("amr").getarr("n_cell", int) == [8, 8]
+    assert pp.sub("init").get("area", float) == pytest.approx(3.141592653589793 / 16)  # init.r before r
+    with pytest.raises(I.InputsError, match="cannot read"):
+        pp.get("half", int)
+    with pytest.raises(I.InputsError, match="refers to itself"):
+        pp.get("loop_a", float)
+    with pytest.raises(I.InputsError, match="single value"):  # unquoted spaces make three values
+        _pp("a = b\nb = 1 + 2\n").get("a", float)
+    with pytest.raises(I.InputsError, match="unknown name"):
+        _pp("x = y + 1\n").get("x", float)
+    with pytest.raises(I.InputsError, match="cannot read"):
+        _pp("x = __import__('os')\n").get("x", float)
+
+
+def test_missing_include_is_an_inputs_error(tmp_path):
+    (tmp_path / "inputs").write_text("FILE = not_there\n")
+    with pytest.raises(I.InputsError, match="FILE = not_there: no such file"):
+        I.ParmParse.from_file(str(tmp_path / "inputs"))

@@ -322,8 +322,8 @@ def test_oracle_body_limiter_sensitivity():
     phi(1), a full slope; both at the rounding level: an arbitrary ratio).
     Next to the sphere the energy is flat to the last bit while density and
     momentum are not, so a relative change of 1e-15 in the fine level's input
-    (the size of the coarse/fine interpolation's rounding differences between
-    two machines) moves the restatement's own result after one coarse step by
+    (the size of the rounding differences between the device's step and the
+    restatement's) moves the restatement's own result after one coarse step by
     1e-8 or more; limited component by component the same change stays at
     the rounding level."""
     from oracle import oracle as O

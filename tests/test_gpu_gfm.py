@@ -308,8 +308,8 @@ def test_hierarchy_with_body_matches_oracle(torch_cuda, oracle, D):
     (every component limited on the energy's ratio) the limiter's 0/0 branch
     (a limiting variable flat to the last bit selects phi(1), one flat to
     rounding an arbitrary ratio) makes the step discontinuous in the last bit
-    of the energy next to the body, and the device's sweeps and average-down
-    round differently from the restatement (test_gfm_cpu.py,
+    of the energy next to the body, and the device's fast sweeps round
+    differently from the restatement (test_gfm_cpu.py,
     test_oracle_body_limiter_sensitivity: a 1e-15 change of the restatement's
     own input moves its result by 1e-8)."""
     import bamrex_b200 as bx

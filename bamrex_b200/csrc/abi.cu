@@ -1018,9 +1018,14 @@ extern "C" void* bamrex_level_stream(const bamrex_level* L) { return L ? (void*)
 extern "C" int bamrex_level_fab(const bamrex_level* L, int box, bamrex_array4* out)
 {
     if (!L || !out || box < 0 || box >= (int)L->boxes.size()) return fail(BAMREX_ERR_ARG, "bad level/box");
+    // bamrex_array4 describes doubles only: a float fab handed out as one
+    // would let an Array4 consumer read twice as far as the buffer goes
+    if (L->fp32)
+        return fail(BAMREX_ERR_UNSUPPORTED,
+                    "bamrex_level_fab: an FP32-storage level holds floats, which bamrex_array4 cannot describe");
     const FabDev& f = L->fab[L->cur][box];
     const bamrex_box& B = L->boxes[box];
-    out->p = static_cast<double*>(f.p);  // float elements for an FP32-storage level
+    out->p = static_cast<double*>(f.p);
     out->jstride = f.js;
     out->kstride = f.ks;
     out->nstride = f.ns;

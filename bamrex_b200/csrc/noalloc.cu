@@ -101,7 +101,10 @@ __global__ void __launch_bounds__(kThreads) sums_noalloc_kernel(int NC, int nbox
 std::mutex g_mu;
 void* g_addr[64] = {};
 
-// The scratch address on the current device, looked up once per device.
+// The scratch address on the current device, looked up once per device and
+// kept for the life of the process.  A cudaDeviceReset unloads the module,
+// after which the array may sit elsewhere: the entry point's documentation
+// rules out calls after a reset of the device.
 int scratch_address(unsigned char** out)
 {
     int dev = 0;

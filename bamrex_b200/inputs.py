@@ -72,7 +72,8 @@ _CONSTS = {"pi": math.pi}
 
 def _eval_expr(text: str, symbol):
     """Value of an arithmetic expression (+ - * / ^ **, parentheses, the
-    functions of _FUNCS, pi) whose names are looked up by symbol(name)."""
+    functions of _FUNCS, pi) whose names are looked up by symbol(name),
+    evaluated in double precision."""
     try:
         tree = ast.parse(text.replace("^", "**"), mode="eval")
     except SyntaxError:
@@ -81,8 +82,11 @@ def _eval_expr(text: str, symbol):
     def ev(node):
         if isinstance(node, ast.Expression):
             return ev(node.body)
-        if isinstance(node, ast.Constant) and isinstance(node.value, (int, float)):
-            return node.value
+        if isinstance(node, ast.Constant) and isinstance(node.value, (int, float)) \
+                and not isinstance(node.value, bool):
+            # in double, as ParmParse evaluates: 9^9^9 overflows instead of
+            # building an unbounded integer
+            return float(node.value)
         if isinstance(node, ast.BinOp) and type(node.op) in _BINOPS:
             return _BINOPS[type(node.op)](ev(node.left), ev(node.right))
         if isinstance(node, ast.UnaryOp) and type(node.op) in _UNOPS:

@@ -173,6 +173,8 @@ def cpu_baseline_run(n_full, seconds, warm_steps=0, fixed_steps=None):
     from bamrex_b200 import problems
     from oracle import oracle as o
 
+    march = o.use_native_build()
+    cpu = o.host_cpu()
     threads = o.num_threads(fast=True)
 
     def setup(n):
@@ -226,10 +228,11 @@ def cpu_baseline_run(n_full, seconds, warm_steps=0, fixed_steps=None):
     el = time.perf_counter() - t0
     value = n * n * steps / el
     return {"value": value, "unit": METRIC, "cores": threads, "kind": "port", "elapsed_s": el, "steps": steps,
-            "n": n,
+            "n": n, "cpu_model": cpu["model"], "isa": cpu["isa"], "march": march,
             "sample": "%d step(s) of the same 2D quadrant problem at %dx%d (64x64 boxes, the reference's "
-                      "max_grid_size), CPU restatement of the reference path, -O3 -march=x86-64-v3, OpenMP over "
-                      "boxes, %d threads" % (steps, n, n, threads)}
+                      "max_grid_size), CPU restatement of the reference path, -O3 -funroll-loops -march=%s "
+                      "(host %s, %s), OpenMP over boxes, %d threads"
+                      % (steps, n, n, march, cpu["model"], cpu["isa"], threads)}
 
 
 # ------------------------------------------------------------------ arms
@@ -500,7 +503,7 @@ def run_reference(args, rank, world):
         "data": "synthetic (seeded four-quadrant initial state)",
         "config": workload_config(args.n, None, 64, {"sample_n": r["n"], "threads": r["cores"]}),
         "cpu_baseline": {"value": r["value"], "unit": METRIC, "cores": r["cores"], "kind": r["kind"],
-                         "sample": r["sample"]},
+                         "sample": r["sample"], "cpu_model": r["cpu_model"], "isa": r["isa"], "march": r["march"]},
         "e2e": {"value": r["value"], "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "note": "the reference needs the AMReX library (not available offline), so its CPU path runs as the "
                 "line-by-line restatement in oracle/",
@@ -666,7 +669,7 @@ def run_ours(args, rank, world, local_rank):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         r = cpu_baseline_run(n, args.cpu_seconds)
-        cpu = {k: r[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        cpu = {k: r[k] for k in ("value", "unit", "cores", "kind", "sample", "cpu_model", "isa", "march")}
 
     imex = None
     if rank == 0 and world == 1 and not args.no_imex:

@@ -219,7 +219,9 @@ BAMREX_API void *bamrex_level_stream(const bamrex_level *level);
 /* The x-sweep kernel the level runs: BAMREX_XSWEEP_ROWS or _MARCH. */
 BAMREX_API int bamrex_level_x_mode(const bamrex_level *level);
 
-/* Number of valid cells, and the Array4 of box b of the current state. */
+/* Number of valid cells, and the Array4 of box b of the current state.
+ * bamrex_level_fab returns BAMREX_ERR_UNSUPPORTED for an FP32-storage level:
+ * its fabs hold floats, and bamrex_array4 describes doubles only. */
 BAMREX_API long long bamrex_level_num_cells(const bamrex_level *level);
 BAMREX_API int bamrex_level_fab(const bamrex_level *level, int box, bamrex_array4 *out);
 
@@ -243,7 +245,9 @@ BAMREX_API int bamrex_level_conserved_sums(bamrex_level *level, double *totals);
  * All scratch lives in one fixed file-scope device array: at most 4096
  * boxes per call (larger counts are rejected with BAMREX_ERR_ARG).  The
  * first call on each device looks up that array's address
- * (cudaGetSymbolAddress) and must come before any stream capture.  Calls
+ * (cudaGetSymbolAddress) and must come before any stream capture; the
+ * address is kept for the life of the process, so the function must not be
+ * called after a cudaDeviceReset of that device.  Calls
  * that overlap in time share the array and race: serialise them.  Issues
  * its work on `stream` and synchronises it.  totals: NCOMP doubles, equal
  * bit for bit to bamrex_level_conserved_sums on a level's own fabs. */

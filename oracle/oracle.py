@@ -72,6 +72,43 @@ class _OLevel(ctypes.Structure):
 
 
 _LIBS: dict[bool, ctypes.CDLL] = {}
+# The timing build (fast=True): the committed x86-64-v3 library, or one
+# compiled for this host's CPU by use_native_build().
+_FAST = {"path": os.path.join(_HERE, "liboracle_fast.so"), "march": "x86-64-v3"}
+
+
+def use_native_build() -> str:
+    """Compile the timing build with -march=native (the reference's own flag,
+    CMakeLists.txt:8) for the CPU this process runs on, into a temporary
+    directory, and use it for every later fast=True call.  Returns the -march
+    value in use ("native", or "x86-64-v3" when the compile fails or the
+    timing library is already loaded)."""
+    import tempfile
+    if True in _LIBS:
+        return _FAST["march"]
+    d = tempfile.mkdtemp(prefix="bamrex_oracle_native_")
+    out = os.path.join(d, "liboracle_native.so")
+    r = subprocess.run(["gcc", "-O3", "-funroll-loops", "-march=native", "-fPIC", "-shared", "-fopenmp", "-o", out,
+                        os.path.join(_HERE, "bamrex_oracle.c")], capture_output=True)
+    if r.returncode == 0 and os.path.exists(out):
+        _FAST.update(path=out, march="native")
+    return _FAST["march"]
+
+
+def host_cpu() -> dict:
+    """Model name and the widest x86 vector extension of this host's CPU."""
+    model, flags = "unknown", set()
+    try:
+        with open("/proc/cpuinfo") as fh:
+            for line in fh:
+                if line.startswith("model name") and model == "unknown":
+                    model = line.split(":", 1)[1].strip()
+                elif line.startswith("flags") and not flags:
+                    flags = set(line.split(":", 1)[1].split())
+    except OSError:
+        pass
+    isa = "avx512" if "avx512f" in flags else ("avx2" if "avx2" in flags else "sse")
+    return {"model": model, "isa": isa}
 
 
 def build(force: bool = False) -> None:
@@ -86,7 +123,7 @@ def lib(fast: bool = False) -> ctypes.CDLL:
     if fast in _LIBS:
         return _LIBS[fast]
     build()
-    L = ctypes.CDLL(os.path.join(_HERE, "liboracle_fast.so" if fast else "liboracle.so"))
+    L = ctypes.CDLL(_FAST["path"] if fast else os.path.join(_HERE, "liboracle.so"))
     dp = ctypes.POINTER(ctypes.c_double)
     ip = ctypes.POINTER(ctypes.c_int)
     L.oracle_consv_from_primv.argtypes = [ctypes.c_int, dp, ctypes.c_double, ctypes.c_double, dp]

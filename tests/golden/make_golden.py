@@ -9,7 +9,8 @@ Sources parsed:
   Tests/Euler01.cpp     tolerances and expected max wave speed
   Tests/Limiters01.cpp  minmod known answers
 
-Usage: python tests/golden/make_golden.py [--ref /path/to/BAMReX]
+Usage: python tests/golden/make_golden.py --ref /path/to/BAMReX
+       (or BAMREX_REFERENCE=/path/to/BAMReX python tests/golden/make_golden.py)
 """
 from __future__ import annotations
 
@@ -112,9 +113,12 @@ def minmod_cases(ref: str):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("BAMREX_REFERENCE"),
+                    help="the BAMReX source tree (default: $BAMREX_REFERENCE)")
     ap.add_argument("--out", default=os.path.join(HERE, "reference_known_answers.json"))
     a = ap.parse_args()
+    if not a.ref:
+        ap.error("give the BAMReX source tree with --ref or $BAMREX_REFERENCE")
     data = {
         "source": "BAMReX Tests/{hllc_test.H,HLLC01.cpp,BoxTest.H,Euler01.cpp,Limiters01.cpp}",
         "toro_wave_speeds": toro_fixtures(a.ref),

@@ -91,3 +91,21 @@ def test_conserved_sums_fp64_and_fp32(torch_cuda, oracle):
         np.testing.assert_array_equal(s1, s1b)
         assert np.all(np.abs(s1 - s0) <= tol * scale), (prec, s1 - s0)
         lev.close()
+
+
+def test_fp32_level_fab_is_refused(torch_cuda, oracle):
+    """bamrex_array4 describes doubles only, so an FP32-storage level does not
+    hand out its float fabs as one (a consumer would read past the buffer)."""
+    import ctypes
+
+    import bamrex_b200 as bx
+    from bamrex_b200._abi import ERR_UNSUPPORTED, Array4, lib
+    lay, lev = _levels(oracle, 2, 64, 32, 0, 1, 0.8, bx.FP32_STORAGE)
+    a = Array4()
+    assert lib().bamrex_level_fab(lev._h, 0, ctypes.byref(a)) == ERR_UNSUPPORTED
+    assert b"FP32-storage" in lib().bamrex_last_error()
+    assert not a.p
+    lev.close()
+    lay, lev = _levels(oracle, 2, 64, 32, 0, 1, 0.8, bx.FP64)
+    assert lib().bamrex_level_fab(lev._h, 0, ctypes.byref(a)) == 0 and a.p
+    lev.close()

@@ -451,6 +451,13 @@ def test_expressions():
         _pp("x = y + 1\n").get("x", float)
     with pytest.raises(I.InputsError, match="cannot read"):
         _pp("x = __import__('os')\n").get("x", float)
+    # evaluated in double as ParmParse does: a tower of powers overflows at
+    # once instead of growing an unbounded integer
+    with pytest.raises(I.InputsError, match="cannot read"):
+        _pp("x = 9^9^9\n").get("x", float)
+    with pytest.raises(I.InputsError, match="cannot read"):
+        _pp("n = 10^400\n").get("n", int)
+    assert _pp("n = 2^10\n").get("n", int) == 1024
 
 
 def test_missing_include_is_an_inputs_error(tmp_path):

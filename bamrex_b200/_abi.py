@@ -111,11 +111,15 @@ class LevelDesc(ctypes.Structure):
         ("s_segment", ctypes.c_int),
         ("precision", ctypes.c_int),
         ("x_mode", ctypes.c_int),
+        ("staging", ctypes.c_int),
+        ("staging_dir", ctypes.c_int * 3),
     ]
 
 
 # x-sweep kernels (BAMREX_XSWEEP_*)
 XSWEEP_AUTO, XSWEEP_ROWS, XSWEEP_MARCH = 0, 1, 2
+# sweep input staging (BAMREX_STAGING_*)
+STAGING_AUTO, STAGING_REGISTERS, STAGING_TMA, STAGING_WAVE = 0, 1, 2, 3
 
 MAX_LEVELS = 8
 # linear-operator boundary types (amrex::LinOpBCType subset)
@@ -237,6 +241,7 @@ SIGNATURES = {
     "bamrex_level_num_cells": (_ll, [_vp]),
     "bamrex_level_stream": (_vp, [_vp]),
     "bamrex_level_x_mode": (_i, [_vp]),
+    "bamrex_level_staging": (_i, [_vp, _i]),
     "bamrex_level_fab": (_i, [_vp, _i, ctypes.POINTER(Array4)]),
     "bamrex_level_copy_in": (_i, [_vp, _vp]),
     "bamrex_level_copy_out": (_i, [_vp, _vp]),

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <functional>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -225,6 +226,147 @@ bool prefer_x_march(int D, const std::vector<bamrex_box>& boxes, int seg_rows, i
         }
     }
     return march < rows;
+}
+
+// ---- TMA-staged sweeps (sweep_tma.cuh, sweep_wave.cuh): lane groups and
+// segments.  An item takes NL lines (tma_item_lines): wa along the faster
+// transverse direction A times NL / wa along B.
+// The choice of wa among NL, NL/2, NL/4 with the fewest line slots on the
+// box (2D: always NL).
+int tma_wa(int D, int dir, const int* lo, const int* hi, int NL)
+{
+    if (D == 2) return NL;
+    const int A = dir == 0 ? 1 : 0, B = dir == 2 ? 1 : 2;
+    const long long nA = hi[A] - lo[A] + 1, nB = hi[B] - lo[B] + 1;
+    int best = NL;
+    long long bslots = -1;
+    for (int wa : { NL, NL / 2, NL / 4 }) {
+        const int wb = NL / wa;
+        const long long slots = (nA + wa - 1) / wa * wa * ((nB + wb - 1) / wb * wb);
+        if (bslots < 0 || slots < bslots) {
+            best = wa;
+            bslots = slots;
+        }
+    }
+    return best;
+}
+
+// Work items of one box for a TMA-staged sweep: line groups x segments of
+// equal length bl (at most seglen).
+void tma_box_items(int D, int dir, const int* lo, const int* hi, int seglen, int NL, long long& items, int& nseg,
+                   int& ngroup, int& wa, int& bl)
+{
+    wa = tma_wa(D, dir, lo, hi, NL);
+    const int wb = NL / wa;
+    const int A = dir == 0 ? 1 : 0, B = dir == 2 ? 1 : 2;
+    const int n[3] = { hi[0] - lo[0] + 1, hi[1] - lo[1] + 1, hi[2] - lo[2] + 1 };
+    nseg = (n[dir] + seglen - 1) / seglen;
+    bl = (n[dir] + nseg - 1) / nseg;
+    const long long ngA = (n[A] + wa - 1) / wa, ngB = D == 3 ? (n[B] + wb - 1) / wb : 1;
+    ngroup = (int)(ngA * ngB);
+    items = (long long)ngroup * nseg;
+}
+
+// Steps one unit (a warp of the march, a block of the wavefront) spends on
+// a segment of len cells: the march's len + about 8 (warm-up, drain, first
+// tile); the wavefront's passes of pw positions over len + 2, plus one for
+// the first tile.
+long long tma_item_cost(bool wave, int pw, int len)
+{
+    return wave ? ((long long)(len + 3 + pw - 1) / pw + 1) * pw : (long long)len + 8;
+}
+
+// Segment length of a TMA-staged sweep: the candidate with the shortest
+// makespan when the resident units take the items round robin.
+int choose_tma_seglen(int D, int dir, const std::vector<bamrex_box>& boxes, long long resident_units, bool wave)
+{
+    const int NL = tma_item_lines(wave, dir), pw = tma_pass_positions(wave, dir);
+    // the usual lengths, and the widest box's extent split into 1 .. 24
+    // equal segments
+    std::vector<int> cand = { 4096, 2048, 1024, 768, 512, 384, 256, 192, 128, 96, 64, 48, 32 };
+    int nmax = 1;
+    for (const auto& b : boxes) nmax = std::max(nmax, b.hi[dir] - b.lo[dir] + 1);
+    for (int m = 1; m <= 24; ++m)
+        if ((nmax + m - 1) / m >= 32) cand.push_back((nmax + m - 1) / m);
+    std::sort(cand.begin(), cand.end(), std::greater<int>());
+    cand.erase(std::unique(cand.begin(), cand.end()), cand.end());
+    const long long W = std::max(1LL, resident_units);
+    int best = cand[0];
+    long long best_span = -1;
+    std::vector<long long> load;
+    for (int c : cand) {
+        long long total = 0;
+        for (const auto& b : boxes) {
+            long long it;
+            int nseg, ng, wa, bl;
+            tma_box_items(D, dir, b.lo, b.hi, c, NL, it, nseg, ng, wa, bl);
+            total += it;
+        }
+        const long long nw = std::min(W, total);
+        load.assign((size_t)nw, 0);
+        long long idx = 0;
+        for (const auto& b : boxes) {
+            long long it;
+            int nseg, ng, wa, bl;
+            tma_box_items(D, dir, b.lo, b.hi, c, NL, it, nseg, ng, wa, bl);
+            const int n = b.hi[dir] - b.lo[dir] + 1;
+            for (int g = 0; g < ng; ++g)
+                for (int sg = 0; sg < nseg; ++sg, ++idx)
+                    load[(size_t)(idx % nw)] += tma_item_cost(wave, pw, std::min(bl, n - sg * bl));
+        }
+        const long long span = *std::max_element(load.begin(), load.end());
+        if (best_span < 0 || span < best_span) {
+            best = c;
+            best_span = span;
+        }
+    }
+    return best;
+}
+
+// Kernel of a sweep direction when the level leaves the choice to the
+// library: the kind with the least estimated time, from the slot-steps each
+// spends on the level's boxes (idle lanes, warm-up, pass rounding included,
+// at the segment lengths each would choose) times a measured time per
+// slot-step (B200, 4096^2 2D and 256^3 3D, per direction and storage type).
+// rows / march: the two L2-loading x kernels.
+int auto_sweep_kind(int D, int d, bool fp32, const std::vector<bamrex_box>& boxes, int seg_rows, int seg_march,
+                    int seg_tma, int seg_wave, bool allow_tma)
+{
+    // picoseconds per slot-step: [fp32][D - 2][d] x {rows, march, TMA, wave}
+    static const double ps[2][2][3][4] = {
+        { { { 28, 37, 53, 27 }, { 0, 30, 29, 29 }, { 0, 0, 0, 0 } },
+          { { 39, 47, 70, 27.5 }, { 0, 36, 32, 28 }, { 0, 40, 35, 31 } } },
+        { { { 12.6, 16, 18.5, 13.5 }, { 0, 15, 11, 15 }, { 0, 0, 0, 0 } },
+          { { 16, 20, 23, 17 }, { 0, 19, 14, 19 }, { 0, 21, 15, 20 } } },
+    };
+    const double* c = ps[fp32 ? 1 : 0][D - 2][d];
+    double rows = 0, march = 0, tma = 0, wave = 0;
+    const int pw = tma_pass_positions(true, d), nlw = tma_item_lines(true, d);
+    for (const auto& b : boxes) {
+        const int n[3] = { b.hi[0] - b.lo[0] + 1, b.hi[1] - b.lo[1] + 1, b.hi[2] - b.lo[2] + 1 };
+        const int A = d == 0 ? 1 : 0, B = d == 2 ? 1 : 2;
+        const long long lines = (long long)n[A] * n[B];
+        auto segs = [&](int seglen, auto&& per) {
+            const int nseg = (n[d] + seglen - 1) / seglen, bl = (n[d] + nseg - 1) / nseg;
+            for (int x = 0; x < n[d]; x += bl) per(std::min(bl, n[d] - x));
+        };
+        if (d == 0) segs(seg_rows, [&](int len) { rows += (double)lines * 32.0 * ((len + 64 + 31) / 32); });
+        segs(seg_march, [&](int len) { march += (double)((lines + 31) / 32 * 32) * (len + 4); });
+        long long it;
+        int nseg, ng, wa, bl;
+        tma_box_items(D, d, b.lo, b.hi, seg_tma, 32, it, nseg, ng, wa, bl);
+        segs(seg_tma, [&](int len) { tma += (double)ng * 32 * (len + 8); });
+        tma_box_items(D, d, b.lo, b.hi, seg_wave, nlw, it, nseg, ng, wa, bl);
+        segs(seg_wave, [&](int len) { wave += (double)ng * nlw * ((len + 3 + pw - 1) / pw + 1) * pw; });
+    }
+    double best = d == 0 ? std::min(rows * c[0], march * c[1]) : march * c[1];
+    int kind = BAMREX_STAGING_REGISTERS;
+    if (allow_tma && tma * c[2] < best) {
+        best = tma * c[2];
+        kind = BAMREX_STAGING_TMA;
+    }
+    if (allow_tma && wave * c[3] < best) kind = BAMREX_STAGING_WAVE;
+    return kind;
 }
 
 }  // namespace
@@ -671,8 +813,14 @@ int level_sweep(bamrex_level* L, int d, int parity, double dt_host, const StepSc
     a.do_update = 1;
     const bool t = allow_timing && L->timing && L->ev_used < L->events.size();
     if (t) cudaEventRecord(L->events[L->ev_used].first, L->stream);
-    const int rc = level_launch(L, launch_sweep(L->D, d, L->method, L->fp32, a, L->stream, d == 0 && L->x_march),
-                                "sweep");
+    int rc;
+    if (L->tma(d)) {
+        a.status = &L->d_scal->status;
+        rc = level_launch(L, launch_sweep_tma(L->D, d, L->fp32, fast_limiter(L->D, L->method, L->k), L->wave(d), a, L->stream),
+                          "TMA-staged sweep");
+    } else {
+        rc = level_launch(L, launch_sweep(L->D, d, L->method, L->fp32, a, L->stream, d == 0 && L->x_march), "sweep");
+    }
     if (rc != BAMREX_OK) return rc;
     if (t) {
         cudaEventRecord(L->events[L->ev_used].second, L->stream);
@@ -830,6 +978,33 @@ extern "C" int bamrex_level_create(bamrex_level** out, const bamrex_level_desc* 
         L->fab[1].push_back(f);
     }
 
+    // ---- staging of each direction's sweep
+    if (desc->staging < BAMREX_STAGING_AUTO || desc->staging > BAMREX_STAGING_WAVE) {
+        delete L;
+        return fail(BAMREX_ERR_ARG, "staging must be BAMREX_STAGING_AUTO, _REGISTERS, _TMA or _WAVE");
+    }
+    {
+        const bool ok = tma_supported(D, L->method, L->k);
+        if ((desc->staging == BAMREX_STAGING_TMA || desc->staging == BAMREX_STAGING_WAVE) && !ok) {
+            delete L;
+            return fail(BAMREX_ERR_UNSUPPORTED, "TMA staging needs the fast MUSCL-Hancock path (energy limiting, "
+                                                "gamma 1.4) in 2D or 3D");
+        }
+        for (int d = 0; d < D; ++d) {
+            const int want = desc->staging_dir[d] != BAMREX_STAGING_AUTO ? desc->staging_dir[d] : desc->staging;
+            if (want < BAMREX_STAGING_AUTO || want > BAMREX_STAGING_WAVE) {
+                delete L;
+                return fail(BAMREX_ERR_ARG, "staging_dir must hold BAMREX_STAGING_* values");
+            }
+            if ((want == BAMREX_STAGING_TMA || want == BAMREX_STAGING_WAVE) && !ok) {
+                delete L;
+                return fail(BAMREX_ERR_UNSUPPORTED, "TMA staging needs the fast MUSCL-Hancock path (energy limiting, "
+                                                    "gamma 1.4) in 2D or 3D");
+            }
+            L->sweep_kind[d] = want == BAMREX_STAGING_AUTO ? -1 : want;  // -1: decided below by the cost model
+        }
+    }
+
     // ---- items and segment lengths
     std::vector<SweepBox> sweep_host[3];
     // x-sweep kernel: one warp per row segment, or one thread per row
@@ -844,11 +1019,32 @@ extern "C" int bamrex_level_create(bamrex_level** out, const bamrex_level_desc* 
         L->x_march = prefer_x_march(D, L->boxes, sr, sm);
     }
     for (int d = 0; d < D; ++d) {
+        if (L->sweep_kind[d] >= 0) continue;
+        if (!tma_supported(D, L->method, L->k)) {
+            L->sweep_kind[d] = BAMREX_STAGING_REGISTERS;
+            continue;
+        }
+        const int lim = fast_limiter(D, L->method, L->k);
+        auto seg_for = [&](bool tma_kind, bool wave, bool march) {
+            const int user = d == 0 ? desc->x_segment : desc->s_segment;
+            if (user > 0) return user;
+            if (tma_kind) return choose_tma_seglen(D, d, L->boxes, sweep_tma_resident_units(D, d, L->fp32, lim, wave), wave);
+            return choose_seglen(d, L->boxes, sweep_resident_warps(D, d, L->method, L->fp32, L->k, march), march);
+        };
+        const int sr = d == 0 ? (int)align_up((size_t)seg_for(false, false, false), 32) : 0;
+        const int sm = seg_for(false, false, d == 0);
+        L->sweep_kind[d] = auto_sweep_kind(D, d, L->fp32, L->boxes, sr, sm, seg_for(true, false, false),
+                                           seg_for(true, true, false), true);
+    }
+    for (int d = 0; d < D; ++d) {
         const bool march = d == 0 && L->x_march;
+        const int lim = fast_limiter(D, L->method, L->k);
         L->seglen[d] = d == 0 ? desc->x_segment : desc->s_segment;
         if (L->seglen[d] <= 0)
-            L->seglen[d] = choose_seglen(d, L->boxes, sweep_resident_warps(D, d, L->method, L->fp32, L->k, march), march);
-        if (d == 0 && !march) L->seglen[d] = (int)align_up((size_t)L->seglen[d], 32);
+            L->seglen[d] = L->tma(d) ? choose_tma_seglen(D, d, L->boxes,
+                                                         sweep_tma_resident_units(D, d, L->fp32, lim, L->wave(d)), L->wave(d))
+                                     : choose_seglen(d, L->boxes, sweep_resident_warps(D, d, L->method, L->fp32, L->k, march), march);
+        if (d == 0 && !march && !L->tma(d)) L->seglen[d] = (int)align_up((size_t)L->seglen[d], 32);
         long long acc = 0;
         for (int b = 0; b < nb; ++b) {
             SweepBox sb;
@@ -858,7 +1054,13 @@ extern "C" int bamrex_level_create(bamrex_level** out, const bamrex_level_desc* 
                 sb.hi[q] = L->boxes[b].hi[q];
             }
             long long it;
-            box_items(d, sb.lo, sb.hi, L->seglen[d], it, sb.nseg, sb.ngroup, march, &sb.seglen);
+            if (L->tma(d)) {
+                tma_box_items(D, d, sb.lo, sb.hi, L->seglen[d], tma_item_lines(L->wave(d), d), it, sb.nseg, sb.ngroup, sb.wa,
+                              sb.seglen);
+                sb.xoff = front;
+            } else {
+                box_items(d, sb.lo, sb.hi, L->seglen[d], it, sb.nseg, sb.ngroup, march, &sb.seglen);
+            }
             sb.item_begin = acc;
             acc += it;
             sweep_host[d].push_back(sb);
@@ -909,6 +1111,13 @@ extern "C" int bamrex_level_create(bamrex_level** out, const bamrex_level_desc* 
         for (int p = 0; p < 2; ++p) o_sweep[d][p] = take(sizeof(SweepBox) * nb);
     size_t o_ghost[3] = {};
     for (int d = 0; d < D; ++d) o_ghost[d] = take(std::max<size_t>(1, ghost_table_bytes(ghost_host[d].size(), L->ghost_chunks[d])));
+    // tensor maps of the TMA-staged directions: per direction and parity,
+    // one 128-byte map per box (64-byte aligned, as the TMA unit requires)
+    constexpr size_t kMapBytes = 128;
+    size_t o_tmap[3][2] = {};
+    for (int d = 0; d < D; ++d)
+        if (L->tma(d))
+            for (int p = 0; p < 2; ++p) o_tmap[d][p] = take(kMapBytes * nb);
     const size_t o_pack = take(sizeof(PackBox) * nb);
     const size_t o_stage = take((size_t)L->ncells * L->NC * 8);
     const size_t o_scal = take(sizeof(StepScalars));
@@ -956,7 +1165,25 @@ extern "C" int bamrex_level_create(bamrex_level** out, const bamrex_level_desc* 
                 t[b].out = L->fab[p ^ 1][b];
                 t[b].flux.p = nullptr;
             }
-            ue = up(L->d_sweep[d][p], t.data(), sizeof(SweepBox) * nb);
+            if (L->tma(d)) {
+                struct alignas(64) Map {
+                    unsigned char b[kMapBytes];
+                };
+                std::vector<Map> maps((size_t)nb);
+                char* dmaps = L->arena + o_tmap[d][p];
+                for (int b = 0; b < nb && ue == cudaSuccess; ++b) {
+                    const FabDev& f = L->fab[p][b];
+                    const bamrex_box& Bb = L->boxes[b];
+                    const int nyg = D > 1 ? Bb.hi[1] - Bb.lo[1] + 1 + 2 * g : 1;
+                    const int nzg = D > 2 ? Bb.hi[2] - Bb.lo[2] + 1 + 2 * g : 1;
+                    const char* row0 = static_cast<const char*>(f.p) - (size_t)front * L->esize;
+                    ue = encode_sweep_tmap(maps[(size_t)b].b, L->fp32, D, L->NC, d, L->wave(d), t[b].wa, row0, f.js, f.ks,
+                                           f.ns, nyg, nzg);
+                    t[b].tmap = dmaps + (size_t)b * kMapBytes;
+                }
+                if (ue == cudaSuccess) ue = up(dmaps, maps.data(), kMapBytes * nb);
+            }
+            if (ue == cudaSuccess) ue = up(L->d_sweep[d][p], t.data(), sizeof(SweepBox) * nb);
         }
         if (ue == cudaSuccess) ue = up(L->d_ghost[d], ghost_host[d].data(), sizeof(GhostOp) * ghost_host[d].size());
         if (ue == cudaSuccess) {
@@ -1044,6 +1271,12 @@ extern "C" int bamrex_level_x_mode(const bamrex_level* L)
 {
     if (!L) return fail(BAMREX_ERR_ARG, "NULL level");
     return L->x_march ? BAMREX_XSWEEP_MARCH : BAMREX_XSWEEP_ROWS;
+}
+
+extern "C" int bamrex_level_staging(const bamrex_level* L, int dir)
+{
+    if (!L || dir < 0 || dir >= L->D) return -fail(BAMREX_ERR_ARG, "bad level/direction");
+    return L->sweep_kind[dir];
 }
 
 extern "C" int bamrex_level_copy_in(bamrex_level* L, const double* src)
@@ -1309,7 +1542,9 @@ extern "C" int bamrex_level_run_host(bamrex_level* L, double* host, int nsteps, 
     if (e == cudaSuccess) e = cudaStreamSynchronize(L->hs->d2h);
     if (e == cudaSuccess) e = cudaStreamSynchronize(L->stream);
     if (e != cudaSuccess) return L->set_err(cuda_fail(e, "host run"));
-    if (h->status != 0) return L->set_err(fail(h->status, "non-finite time step during the run"));
+    if (h->status != 0)
+        return L->set_err(fail(h->status, h->status == BAMREX_ERR_TIMEOUT ? "a sweep gave up waiting for its staged input"
+                                                                          : "non-finite time step during the run"));
     *time_io = h->time;
     if (dt_next) *dt_next = h->dt;
     return BAMREX_OK;
@@ -1385,6 +1620,8 @@ extern "C" int bamrex_level_est_time_step(bamrex_level* L, double* dt_est)
         return L->set_err(fail(BAMREX_ERR_ARG, "a rigid-body interpolation stencil left the fab: raise ngrow"));
     if (L->h_scal->status == BAMREX_ERR_NOT_CONVERGED)
         return L->set_err(fail(BAMREX_ERR_NOT_CONVERGED, "an exact Riemann solve at a rigid-body interface did not converge"));
+    if (L->h_scal->status == BAMREX_ERR_TIMEOUT)
+        return L->set_err(fail(BAMREX_ERR_TIMEOUT, "a sweep gave up waiting for its staged input"));
     L->ws_valid = true;
     const double ms = [&] {
         double v;
@@ -1463,7 +1700,9 @@ extern "C" int bamrex_level_run_wait(bamrex_level* L, double* time_out, int* ste
     L->ws_valid = false;
     if (time_out) *time_out = h->time;
     if (steps_done) *steps_done = h->steps;
-    if (h->status != 0) return L->set_err(fail(h->status, "non-finite time step during the run"));
+    if (h->status != 0)
+        return L->set_err(fail(h->status, h->status == BAMREX_ERR_TIMEOUT ? "a sweep gave up waiting for its staged input"
+                                                                          : "non-finite time step during the run"));
     return BAMREX_OK;
 }
 

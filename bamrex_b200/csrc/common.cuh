@@ -61,6 +61,13 @@ struct SweepBox {
     int nseg;                  // segments along the sweep direction
     int ngroup;                // lane groups of 32 columns (marching sweeps)
     int seglen;                // cells per segment (the last one may be shorter)
+    // TMA-staged sweeps (sweep_tma.cuh): the tensor map of `in` for this
+    // direction (device memory), lines of a lane group along the faster
+    // transverse direction, and the elements between the map's x origin
+    // (the 256-byte aligned start of the padded row) and in.b0
+    const void* tmap;
+    int wa;
+    int xoff;
 };
 
 // Device-resident step scalars (graph-friendly time stepping).

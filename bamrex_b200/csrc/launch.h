@@ -90,6 +90,23 @@ long long sweep_resident_warps(int D, int dir, int method, bool fp32, const Cons
 // limiting, gamma with 1/z = 7), or -1 for the general kernels.
 int fast_limiter(int D, int method, const Consts& k);
 
+// TMA-staged sweeps: the per-warp march (sweep_tma.cuh) and the block
+// wavefront (sweep_wave.cuh, wave = true), for the fast path in 2D and 3D.
+// An item takes tma_item_lines lines (lane groups of wa along the faster
+// transverse direction); the wavefront walks tma_pass_positions positions
+// per pass.  encode_sweep_tmap writes the 128-byte tensor map (host memory
+// at `out`) of one fab for the kernel of direction dir (row_start: the
+// 256-byte aligned start of the fab's first padded row); the launch runs
+// over a level's box table (boxes carry tmap, wa, xoff).  Resident units:
+// warps (march) or blocks (wavefront).
+bool tma_supported(int D, int method, const Consts& k);
+int tma_item_lines(bool wave, int dir);
+int tma_pass_positions(bool wave, int dir);
+cudaError_t encode_sweep_tmap(void* out, bool fp32, int D, int NC, int dir, bool wave, int wa, const void* row_start,
+                              long long js, long long ks, long long ns, int nyg, int nzg);
+cudaError_t launch_sweep_tma(int D, int dir, bool fp32, int lim, bool wave, const SweepArgs& a, cudaStream_t s);
+long long sweep_tma_resident_units(int D, int dir, bool fp32, int lim, bool wave);
+
 cudaError_t launch_ghost_fill(int NC, bool fp32, const GhostOp* ops, int nops, int nchunks, const FabDev* fabs,
                               const StepScalars* scal, cudaStream_t s);
 

@@ -81,6 +81,12 @@ struct bamrex_level {
     long long items[3] = { 0, 0, 0 };
     int seglen[3] = { 0, 0, 0 };
     bool x_march = false;  // x sweep by the marching (thread-per-row) kernel
+    // kernel of each direction's sweep: BAMREX_STAGING_REGISTERS (sweep.cuh),
+    // _TMA (per-warp march, sweep_tma.cuh) or _WAVE (block wavefront,
+    // sweep_wave.cuh)
+    int sweep_kind[3] = { BAMREX_STAGING_REGISTERS, BAMREX_STAGING_REGISTERS, BAMREX_STAGING_REGISTERS };
+    bool tma(int d) const { return sweep_kind[d] == BAMREX_STAGING_TMA || sweep_kind[d] == BAMREX_STAGING_WAVE; }
+    bool wave(int d) const { return sweep_kind[d] == BAMREX_STAGING_WAVE; }
     bamrex::GhostOp* d_ghost[3] = { nullptr, nullptr, nullptr };
     int nghost[3] = { 0, 0, 0 };
     int ghost_chunks[3] = { 0, 0, 0 };

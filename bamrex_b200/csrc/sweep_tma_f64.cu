@@ -1,0 +1,6 @@
+// FP64 (drop-in) instantiations of the TMA-staged sweeps.
+#include "sweep_tma_pick.cuh"
+
+namespace bamrex {
+template const void* pick_tma_kernel<double>(int, int, int, bool, bool);
+}  // namespace bamrex

@@ -215,7 +215,7 @@ class Level:
 
     def __init__(self, spacedim, dom_lo, dom_hi, prob_lo, prob_hi, boxes, parm: Parm, method=_abi.MUSCL_HANCOCK,
                  cfl=0.9, ngrow=2, bc_lo=None, bc_hi=None, stream=None, x_segment=0, s_segment=0,
-                 precision=_abi.FP64, x_mode=_abi.XSWEEP_AUTO):
+                 precision=_abi.FP64, x_mode=_abi.XSWEEP_AUTO, staging=_abi.STAGING_AUTO, staging_dir=(0, 0, 0)):
         self.D, self.NC = spacedim, spacedim + 2
         self.boxes = [(tuple(lo) + (0,) * (3 - len(lo)), tuple(hi) + (0,) * (3 - len(hi))) for lo, hi in boxes]
         self.dom_lo = tuple(dom_lo) + (0,) * (3 - len(dom_lo))
@@ -240,6 +240,9 @@ class Level:
         d.s_segment = s_segment
         d.precision = precision
         d.x_mode = x_mode
+        d.staging = staging
+        for i in range(3):
+            d.staging_dir[i] = int(staging_dir[i])
         self.precision = precision
         self._h = ctypes.c_void_p()
         check(lib().bamrex_level_create(ctypes.byref(self._h), ctypes.byref(d), _stream_ptr(stream)))
@@ -324,6 +327,11 @@ class Level:
     def x_mode(self) -> int:
         """The x-sweep kernel in use: XSWEEP_ROWS or XSWEEP_MARCH."""
         return lib().bamrex_level_x_mode(self._h)
+
+    def staging(self, d) -> int:
+        """The kernel of the sweep of direction d: STAGING_REGISTERS,
+        STAGING_TMA or STAGING_WAVE."""
+        return lib().bamrex_level_staging(self._h, int(d))
 
     def stream_handle(self) -> int:
         """The cudaStream_t the level works on (as an integer)."""

@@ -23,7 +23,7 @@
 extern "C" {
 #endif
 
-#define BAMREX_ABI_VERSION 3
+#define BAMREX_ABI_VERSION 4
 /* MAX_NCOMP = PUInd::size (Source/System/Parm.H:9) */
 #define BAMREX_MAX_NCOMP 8
 
@@ -188,7 +188,30 @@ typedef struct bamrex_level_desc {
     int s_segment;          /* cells per thread item in y/z; 0 = automatic */
     int precision;          /* BAMREX_FP64 (0) or BAMREX_FP32_STORAGE */
     int x_mode;             /* BAMREX_XSWEEP_*: kernel of the x sweep; 0 = automatic */
+    int staging;            /* BAMREX_STAGING_*: how sweeps stage their input; 0 = automatic */
+    int staging_dir[3];     /* per direction, overriding `staging` where not 0 */
 } bamrex_level_desc;
+
+/* How a level's sweeps bring their input on chip and share the stencil.
+ * REGISTERS: the marching and row kernels load through L2 and carry each
+ * line's stencil in registers (every configuration).  TMA: a warp marches
+ * 32 lines, its tiles (positions x 32 lines x components) arriving by tiled
+ * tensor loads into shared memory, several in flight.  WAVE: a block of 8
+ * warps walks 32 lines (8 rows in x) in passes, one position per thread,
+ * its tiles arriving by tensor loads; cell stages and face fluxes pass
+ * between threads through shared memory.  TMA and WAVE serve the fast
+ * MUSCL-Hancock path in 2D and 3D (energy limiting, gamma with 1/z = 7);
+ * other configurations refuse them with BAMREX_ERR_UNSUPPORTED.  AUTO: per
+ * direction the kind with the least estimated time on the level's boxes (a
+ * slot-step count, warm-up and idle lanes included, times a time per
+ * slot-step measured on the B200).  All evaluate the same scheme per cell
+ * (results agree to rounding). */
+enum {
+    BAMREX_STAGING_AUTO = 0,
+    BAMREX_STAGING_REGISTERS = 1,
+    BAMREX_STAGING_TMA = 2,
+    BAMREX_STAGING_WAVE = 3
+};
 
 /* Kernel of a level's x sweep.  ROWS: a warp marches along a row segment,
  * lanes on consecutive cells (best for wide boxes: it spends two extra
@@ -218,6 +241,9 @@ BAMREX_API void *bamrex_level_stream(const bamrex_level *level);
 
 /* The x-sweep kernel the level runs: BAMREX_XSWEEP_ROWS or _MARCH. */
 BAMREX_API int bamrex_level_x_mode(const bamrex_level *level);
+/* The kernel of the sweep of direction dir: BAMREX_STAGING_REGISTERS, _TMA
+ * or _WAVE (negative on a bad argument). */
+BAMREX_API int bamrex_level_staging(const bamrex_level *level, int dir);
 
 /* Number of valid cells, and the Array4 of box b of the current state.
  * bamrex_level_fab returns BAMREX_ERR_UNSUPPORTED for an FP32-storage level:

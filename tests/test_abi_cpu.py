@@ -36,7 +36,7 @@ def test_library_exports_every_declared_symbol():
 def test_abi_version_and_status_strings():
     import bamrex_b200
     L = bamrex_b200.lib()
-    assert L.bamrex_abi_version() == 3
+    assert L.bamrex_abi_version() == 4
     assert L.bamrex_status_string(0) == b"ok"
     assert b"argument" in L.bamrex_status_string(1)
 

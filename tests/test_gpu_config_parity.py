@@ -53,12 +53,12 @@ def _oracle_step(oracle, lay, u, dt=None):
     return dt, lay.gather(S1)
 
 
-def _level(mgs, x_mode=0, precision=0):
+def _level(mgs, x_mode=0, precision=0, staging=0):
     import bamrex_b200 as bx
     hi = (N - 1, N - 1, 0)
     return bx.Level(2, (0, 0, 0), hi, [0.0, 0.0], [1.0, 1.0], bx.decompose(2, (0, 0, 0), hi, mgs),
                     bx.Parm(2, limiter=bx.MINBEE), method=bx.MUSCL_HANCOCK, cfl=0.8, x_mode=x_mode,
-                    precision=precision)
+                    precision=precision, staging=staging)
 
 
 def _check(got, ref, what):
@@ -71,11 +71,16 @@ def _check(got, ref, what):
         assert abs(tg - tr) <= TOTALS * scale, (what, "total", c, tg, tr)
 
 
-@pytest.mark.parametrize("mgs,x_mode", [(N, 1), (N, 2), (64, 0)], ids=["one_box_xrows", "one_box_xmarch", "box64"])
-def test_c2_steps_match_oracle(torch_cuda, oracle, c2, mgs, x_mode):
+@pytest.mark.parametrize("mgs,x_mode,staging", [(N, 1, 1), (N, 2, 1), (N, 0, 2), (N, 0, 3), (64, 0, 1), (64, 0, 2),
+                                                 (64, 0, 3)],
+                         ids=["one_box_xrows", "one_box_xmarch", "one_box_tma", "one_box_wave", "box64", "box64_tma",
+                              "box64_wave"])
+def test_c2_steps_match_oracle(torch_cuda, oracle, c2, mgs, x_mode, staging):
     """Two steps at 4096^2: the first from the initial state, the second from
-    the device's own result (the oracle takes the same input)."""
-    lev = _level(mgs, x_mode)
+    the device's own result (the oracle takes the same input); the sweeps
+    load through L2 (either x kernel) or are staged by TMA."""
+    lev = _level(mgs, x_mode, staging=staging)
+    assert lev.staging(0) == staging and lev.staging(1) == staging
     lev.set_state(c2["u0"])
     dt = lev.estTimeStep()
     assert abs(dt - c2["dt"]) <= 1e-14 * c2["dt"], (dt, c2["dt"])

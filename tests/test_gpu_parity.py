@@ -193,13 +193,13 @@ def test_unsplit_conservative_update(torch_cuda, oracle, D):
 
 
 # ------------------------------------------------------------------ levels
-def _make_levels(oracle, D, n, mgs, bc, method, limiter, cfl, x_mode=0):
+def _make_levels(oracle, D, n, mgs, bc, method, limiter, cfl, x_mode=0, staging=0):
     import bamrex_b200 as bx
     hi = tuple(n - 1 if d < D else 0 for d in range(3))
     boxes = oracle.decompose(D, (0, 0, 0), hi, mgs)
     lay = oracle.LevelLayout(D, (0, 0, 0), hi, boxes, 2, [1.0 / n] * D, bc_lo=(bc,) * 3, bc_hi=(bc,) * 3)
     lev = bx.Level(D, (0, 0, 0), hi, [0.0] * D, [1.0] * D, boxes, bx.Parm(D, limiter=limiter), method=method,
-                   cfl=cfl, bc_lo=(bc,) * 3, bc_hi=(bc,) * 3, x_mode=x_mode)
+                   cfl=cfl, bc_lo=(bc,) * 3, bc_hi=(bc,) * 3, x_mode=x_mode, staging=staging)
     return lay, lev
 
 
@@ -231,15 +231,30 @@ def _initial(kind, D, n):
     return problems.random_states(D, tuple(n if d < D else 1 for d in (2, 1, 0)), seed=21)
 
 
-@pytest.mark.parametrize("x_mode", [1, 2], ids=["xrows", "xmarch"])
+def _fast_path(D, method):
+    # MUSCL-Hancock with the default energy limiting and gamma 1.4 in 2D/3D:
+    # the configurations the TMA-staged sweeps serve
+    return D >= 2 and method == 0
+
+
+@pytest.mark.parametrize("x_mode,staging", [(1, 1), (2, 1), (0, 2), (0, 3)], ids=["xrows", "xmarch", "tma", "wave"])
 @pytest.mark.parametrize("case", LEVEL_CASES, ids=[str(c) for c in LEVEL_CASES])
-def test_level_step_parity(torch_cuda, oracle, case, x_mode):
+def test_level_step_parity(torch_cuda, oracle, case, x_mode, staging):
     """AmrLevelAdv::advance (one split step) on a whole level: same dt from
     estTimeStep, then the state after the step, vs the oracle; with either
-    x-sweep kernel (warp per row segment, thread per row)."""
+    x-sweep kernel loading through L2 (warp per row segment, thread per row),
+    and with every sweep staged by TMA where that path exists."""
+    import bamrex_b200 as bx
     D, n, mgs, bc, method, lim, cfl, init = case
-    lay, lev = _make_levels(oracle, D, n, mgs, bc, method, lim, cfl, x_mode)
-    assert lev.x_mode == (x_mode if D > 1 else 1)
+    tma = staging in (bx.STAGING_TMA, bx.STAGING_WAVE)
+    if tma and not _fast_path(D, method):
+        pytest.skip("no TMA-staged sweep for this configuration")
+    lay, lev = _make_levels(oracle, D, n, mgs, bc, method, lim, cfl, x_mode, staging)
+    if tma:
+        assert all(lev.staging(d) == staging for d in range(D))
+    else:
+        assert lev.x_mode == (x_mode if D > 1 else 1)
+        assert all(lev.staging(d) == bx.STAGING_REGISTERS for d in range(D))
     u0 = _initial(init, D, n)
     # oracle
     S1, S2 = lay.alloc(), lay.alloc()

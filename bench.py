@@ -52,11 +52,16 @@ def parse_args():
     ap.add_argument("--no-autotune", action="store_true", help="keep the library's default sweep segments")
     ap.add_argument("--x-mode", type=int, default=0, help="x-sweep kernel: 0 automatic, 1 warp per row, 2 thread per row")
     ap.add_argument("--no-amr", action="store_true", help="skip the 3D AMR blast sample")
-    ap.add_argument("--amr-n", type=int, default=128, help="base cells per side of the AMR blast sample")
-    ap.add_argument("--amr-steps", type=int, default=6, help="timed coarse steps of the AMR blast sample")
+    ap.add_argument("--amr-n", type=int, default=256, help="base cells per side of the AMR blast sample")
+    ap.add_argument("--amr-steps", type=int, default=100, help="timed coarse steps of the AMR blast sample (fixed grids)")
+    ap.add_argument("--amr-regrid-steps", type=int, default=10,
+                    help="timed coarse steps of the AMR blast sample with a regrid every 2")
     ap.add_argument("--imex-n", type=int, default=2048, help="cells per side of the IMEX pressure problem")
     ap.add_argument("--no-body", action="store_true", help="skip the ghost-fluid rigid-body sample")
     ap.add_argument("--body-cases", default="2d,3d", help="rigid-body cases to run (2d, 3d)")
+    ap.add_argument("--no-parity", action="store_true", help="skip the parity checks against the oracle")
+    ap.add_argument("--fp32-oracle-steps", type=int, default=10,
+                    help="steps of the FP32-storage L1 comparison with the FP64 oracle (0: skip)")
     return ap.parse_args()
 
 
@@ -73,6 +78,84 @@ def workload_config(n, boxes, mgs, extra=None):
     if extra:
         cfg.update(extra)
     return cfg
+
+
+KIND_NAMES = {1: "registers", 2: "tma", 3: "wave"}
+
+
+def sweep_kernel_name(D, d, kind, x_rows):
+    if kind == 3:
+        return "sweep_wave_kernel<%d,%d>" % (D, d)
+    if kind == 2:
+        return "sweep_tma_kernel<%d,%d>" % (D, d)
+    return "sweep_x_kernel<%d>" % D if (d == 0 and x_rows) else "sweep_s_kernel<%d,%d>" % (D, d)
+
+
+def parity_check(lev, u_start, n, steps_from):
+    """One step of the bench's own level (its kernels and segments) against
+    the oracle from the same input: relative L-infinity per component and
+    relative conserved totals (the drop-in bar: 1e-12 and 1e-13)."""
+    import numpy as np
+
+    from oracle import oracle as o
+    hi = (n - 1, n - 1, 0)
+    lay = o.LevelLayout(2, (0, 0, 0), hi, o.decompose(2, (0, 0, 0), hi, 64), 2, [1.0 / n, 1.0 / n])
+    S1, S2 = lay.alloc(), lay.alloc()
+    lay.scatter(S1, u_start)
+    lay.fill_boundary(S1)
+    dt_ref = lay.est_time_step(S1, 1.4, 1.0, 0.8)
+    S2[:] = S1
+    lay.advance_explicit(S1, S2, 0.0, dt_ref, o.MUSCL_HANCOCK, o.Parm(2, limiter=o.MINBEE))
+    ref = lay.gather(S1)
+    lev.set_state(u_start)
+    dt = lev.estTimeStep()
+    lev.advance(0.0, dt_ref)
+    got = lev.get_state()
+    linf = [float(np.max(np.abs(got[c] - ref[c])) / np.max(np.abs(ref[c]))) for c in range(4)]
+    tot = [float(abs(got[c].sum() - ref[c].sum()) / np.abs(ref[c]).sum()) for c in range(4)]
+    return {"from": steps_from, "rel_linf": linf, "rel_totals": tot, "dt_rel": abs(dt - dt_ref) / dt_ref,
+            "pass": max(linf) <= 1e-12 and max(tot) <= 1e-13 and abs(dt - dt_ref) <= 1e-14 * dt_ref}
+
+
+def fp32_l1_vs_oracle(n, u0, steps, lev32):
+    """FP32-storage state after `steps` steps of the oracle's dt sequence
+    against the FP64 oracle: relative L1 of density and energy."""
+    import numpy as np
+
+    from oracle import oracle as o
+    hi = (n - 1, n - 1, 0)
+    lay = o.LevelLayout(2, (0, 0, 0), hi, o.decompose(2, (0, 0, 0), hi, 64), 2, [1.0 / n, 1.0 / n])
+    S1, S2 = lay.alloc(), lay.alloc()
+    lay.scatter(S1, u0)
+    P = o.Parm(2, limiter=o.MINBEE)
+    lev32.set_state(u0)
+    t = 0.0
+    for _ in range(steps):
+        lay.fill_boundary(S1, fast=True)
+        dt = lay.est_time_step(S1, 1.4, 1.0, 0.8, fast=True)
+        S2[:] = S1
+        lay.advance_explicit(S1, S2, t, dt, o.MUSCL_HANCOCK, P, fast=True)
+        lev32.advance(t, dt)
+        t += dt
+    ref, got = lay.gather(S1), lev32.get_state()
+    return {"steps": steps, "rel_l1_rho": float(np.abs(got[0] - ref[0]).sum() / np.abs(ref[0]).sum()),
+            "rel_l1_E": float(np.abs(got[3] - ref[3]).sum() / np.abs(ref[3]).sum()),
+            "reference": "FP64 oracle (optimised build), same dt sequence"}
+
+
+def parity_scalars(parity):
+    """The parity figures as flat config entries."""
+    if not parity:
+        return {}
+    out = {}
+    for k in ("fp64_step_from_initial", "fp64_step_from_timed_state"):
+        if k in parity:
+            out["parity_%s_rel_linf" % k[5:]] = max(parity[k]["rel_linf"])
+            out["parity_%s_rel_totals" % k[5:]] = max(parity[k]["rel_totals"])
+    if "fp32_storage" in parity:
+        out["parity_fp32_l1_rho"] = parity["fp32_storage"]["rel_l1_rho"]
+        out["parity_fp32_l1_E"] = parity["fp32_storage"]["rel_l1_E"]
+    return out
 
 
 # ------------------------------------------------------------------ clocks
@@ -368,7 +451,7 @@ def _chop_drawn(boxes, choices, rng, D=3):
     return out
 
 
-def amr_blast_run(n0, coarse_steps, precision):
+def amr_blast_run(n0, coarse_steps, precision, regrid_steps=None):
     """The 3D spherical blast on a 3-level hierarchy (ratio 2, blocking
     factor 8, max_grid_size drawn per box from {16,32,48,64}, grad_error on
     rho >= 0.1, regrid every 2 coarse steps, subcycling): cell-updates/s
@@ -414,9 +497,11 @@ def amr_blast_run(n0, coarse_steps, precision):
     dt_fixed = time.perf_counter() - t0
     torch.cuda.nvtx.range_pop()
     s1 = A.conserved_sums()
+    kinds = [[A.level(lev).staging(d) for d in range(3)] for lev in range(A.finest_level + 1)]
     A.set_regrid_int(2)
+    nr = coarse_steps if regrid_steps is None else regrid_steps
     t0 = time.perf_counter()
-    for _ in range(coarse_steps):
+    for _ in range(nr):
         A.coarse_step()
     torch.cuda.synchronize()
     dt_regrid = time.perf_counter() - t0
@@ -424,7 +509,9 @@ def amr_blast_run(n0, coarse_steps, precision):
     return {"cells_per_level": cells, "boxes_per_level": nboxes, "coarse_steps": coarse_steps,
             "ms_per_coarse_step": dt_fixed / coarse_steps * 1e3,
             "cell_updates_per_s": updates_per_step * coarse_steps / dt_fixed,
-            "ms_per_coarse_step_with_regrid_every_2": dt_regrid / coarse_steps * 1e3,
+            "sweep_kernels_per_level": [",".join(KIND_NAMES[k] for k in kk) for kk in kinds],
+            "coarse_steps_with_regrid": nr,
+            "ms_per_coarse_step_with_regrid_every_2": dt_regrid / nr * 1e3,
             "mass_drift_rel": float(abs(s1[0] - s0[0]) / abs(s0[0]))}
 
 
@@ -519,6 +606,12 @@ def run_ours(args, rank, world, local_rank):
     import bamrex_b200 as bx
     from bamrex_b200 import problems
 
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        # the timing build of the CPU baseline for this host's CPU, before
+        # anything loads the oracle's default timing build
+        from oracle import oracle as o
+        o.use_native_build()
+
     dist = None
     if world > 1:
         import torch.distributed as dist
@@ -532,14 +625,19 @@ def run_ours(args, rank, world, local_rank):
     u0 = problems.quadrant_2d(n)
     stream = torch.cuda.Stream()
     parm = bx.Parm(D, limiter=bx.MINBEE)
-    xseg, sseg, tuned = 0, 0, None
+    setup = {"staging_dir": (0, 0, 0), "x_mode": args.x_mode, "x_segment": 0, "s_segment": 0}
+    tuned = None
     if not args.no_autotune:
-        from bamrex_b200.autotune import segment_table_summary, tune_segments
-        xseg, sseg, table = tune_segments(D, (0, 0, 0), hi, [0.0, 0.0], [1.0, 1.0], boxes, parm, u0, steps=3)
-        tuned = {"x_segment": xseg or "library default", "s_segment": sseg or "library default",
-                 "candidates_ms_per_step": segment_table_summary(table)}
+        from bamrex_b200.autotune import segment_table_summary, tune_sweeps
+        r = tune_sweeps(D, (0, 0, 0), hi, [0.0, 0.0], [1.0, 1.0], boxes, parm, u0, steps=3)
+        setup = {k: r[k] for k in setup}
+        tuned = {"kernels": [KIND_NAMES[k] for k in r["staging_dir"][:D]], "x_segment": r["x_segment"] or "library",
+                 "s_segment": r["s_segment"] or "library",
+                 "library_choice": [KIND_NAMES[k] for k in r["auto_kinds"]],
+                 "candidates_ms_per_step": segment_table_summary(r["table"])}
     lev = bx.Level(D, (0, 0, 0), hi, [0.0, 0.0], [1.0, 1.0], boxes, parm, method=bx.MUSCL_HANCOCK, cfl=0.8,
-                   stream=stream, x_segment=xseg, s_segment=sseg, x_mode=args.x_mode)
+                   stream=stream, **setup)
+    kinds = [lev.staging(d) for d in range(D)]
     x_rows = lev.x_mode == bx.XSWEEP_ROWS
     lev.set_state(u0)
     use_graph = bool(args.graph)
@@ -571,7 +669,7 @@ def run_ours(args, rank, world, local_rank):
     ms = ev0.elapsed_time(ev1)
     launches, sweep_ms, sweep_launches = lev.counters()
     lev.set_timing(False)
-    u_fp64 = lev.get_state() if (rank == 0 and not args.no_fp32) else None
+    u_fp64 = lev.get_state() if (rank == 0 and (not args.no_fp32 or not args.no_parity)) else None
     if dist:
         t = torch.tensor([ms], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -609,16 +707,29 @@ def run_ours(args, rank, world, local_rank):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_ms = float(t.item())
     clocks.stop()
+    # parity of the timed level itself (its kernels and segments) against
+    # the oracle, one step from the initial state and one from the state the
+    # timed steps reached
+    parity = None
+    if rank == 0 and world == 1 and not args.no_parity:
+        parity = {"fp64_step_from_initial": parity_check(lev, u0, n, "initial state"),
+                  "fp64_step_from_timed_state": parity_check(lev, u_fp64, n, "after the %d timed steps" % args.steps),
+                  "bar": "rel L-inf <= 1e-12 per component, conserved totals <= 1e-13, dt <= 1e-14"}
     lev.close()
 
     # FP32-storage variant on the same workload: throughput, roofline, and
-    # density / energy L1 error against the FP64 path after the same number
-    # of steps (the FP64 path matches the FP64 oracle to 1e-12 per step).
+    # density / energy L1 error against the FP64 oracle (and the FP64 path)
     fp32 = None
-    if u_fp64 is not None:
+    if u_fp64 is not None and not args.no_fp32:
+        setup32 = {"x_mode": args.x_mode}
+        if not args.no_autotune:
+            from bamrex_b200.autotune import tune_sweeps
+            r32 = tune_sweeps(D, (0, 0, 0), hi, [0.0, 0.0], [1.0, 1.0], boxes, parm, u0, precision=bx.FP32_STORAGE,
+                              steps=3)
+            setup32 = {k: r32[k] for k in ("staging_dir", "x_mode", "x_segment", "s_segment")}
         lev32 = bx.Level(D, (0, 0, 0), hi, [0.0, 0.0], [1.0, 1.0], boxes, bx.Parm(D, limiter=bx.MINBEE),
-                         method=bx.MUSCL_HANCOCK, cfl=0.8, stream=stream, precision=bx.FP32_STORAGE,
-                         x_mode=args.x_mode)
+                         method=bx.MUSCL_HANCOCK, cfl=0.8, stream=stream, precision=bx.FP32_STORAGE, **setup32)
+        kinds32 = [lev32.staging(d) for d in range(D)]
         lev32.set_state(u0)
         lev32.run(args.warmup, use_graph=use_graph)
         lev32.set_state(u0)
@@ -635,15 +746,21 @@ def run_ours(args, rank, world, local_rank):
         ms32 = f0.elapsed_time(f1)
         _, sweep_ms32, sweep_n32 = lev32.counters()
         u32 = lev32.get_state()
+        lev32.set_timing(False)
+        l1o = fp32_l1_vs_oracle(n, u0, args.fp32_oracle_steps, lev32) if args.fp32_oracle_steps > 0 else None
         lev32.close()
+        if parity is not None and l1o is not None:
+            parity["fp32_storage"] = l1o
         l1 = lambda a, b: float(np.abs(a - b).sum() / np.abs(b).sum())  # noqa: E731
         peak, _ = measured_peaks()
         ach32 = (2 * NC2D * 4 * n * n) / ((sweep_ms32 / sweep_n32) / 1e3) / 1e9 if sweep_n32 else None
         fp32 = {"value": n * n * args.steps / (ms32 / 1e3), "unit": METRIC, "ms_per_step": ms32 / args.steps,
                 "roofline": {"bound": "hbm", "achieved": ach32, "peak": peak, "unit": "GB/s",
                              "frac": ach32 / peak if ach32 else None, "algorithmic_bytes_per_cell_sweep": 32},
-                "rel_l1_rho": l1(u32[0], u_fp64[0]), "rel_l1_E": l1(u32[3], u_fp64[3]),
-                "l1_reference": "FP64 path after the same %d steps" % args.steps}
+                "kernels": ",".join(KIND_NAMES[k] for k in kinds32),
+                "rel_l1_rho_vs_fp64_path": l1(u32[0], u_fp64[0]), "rel_l1_E_vs_fp64_path": l1(u32[3], u_fp64[3]),
+                "l1_fp64_path": "the FP64 path after the same %d steps" % args.steps,
+                "l1_vs_fp64_oracle": l1o}
 
     cells = n * n
     value = world * cells * args.steps / (ms / 1e3)
@@ -659,12 +776,16 @@ def run_ours(args, rank, world, local_rank):
         traffic = profiled_traffic("mhm2d")
         roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                     "traffic": (traffic * cells) if traffic else None,
-                    "kernel": ("sweep_x_kernel<2,MUSCL>" if x_rows else "sweep_s_kernel<2,0,MUSCL>")
-                    + " + sweep_s_kernel<2,1,MUSCL> (both sweeps, averaged)",
+                    "kernel": " + ".join(sweep_kernel_name(2, d, kinds[d], x_rows) for d in range(D))
+                    + " (both sweeps, averaged)",
                     "algorithmic_bytes_per_launch": alg_bytes, "avg_launch_ms": per_launch_s * 1e3,
                     "sweep_share_of_step": sweep_ms / ms if ms > 0 else None,
                     "peak_source": "%s (MEASURED_PEAKS.json hbm_gbs)" % peak_kind if peak_kind == "measured"
                     else "fallback 6650 GB/s"}
+        if fp32:
+            roofline["fp32_storage_frac"] = fp32["roofline"]["frac"]
+            roofline["fp32_storage_achieved"] = fp32["roofline"]["achieved"]
+            roofline["fp32_storage_value"] = fp32["value"]
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -679,8 +800,8 @@ def run_ours(args, rank, world, local_rank):
         amr = {"workload": "3D spherical blast (p 10 inside r < 0.2, 0.1 outside, rho 1), base %d^3, 3 levels, "
                            "ratio 2, blocking factor 8, max_grid_size drawn per box from {16,32,48,64}, grad_error "
                            "on rho >= 0.1, MUSCL-Hancock/minbee, CFL 0.8, subcycling" % args.amr_n,
-               "fp64": amr_blast_run(args.amr_n, args.amr_steps, bx.FP64),
-               "fp32_storage": amr_blast_run(args.amr_n, args.amr_steps, bx.FP32_STORAGE)}
+               "fp64": amr_blast_run(args.amr_n, args.amr_steps, bx.FP64, args.amr_regrid_steps),
+               "fp32_storage": amr_blast_run(args.amr_n, args.amr_steps, bx.FP32_STORAGE, args.amr_regrid_steps)}
 
     body = None
     if rank == 0 and world == 1 and not args.no_body:
@@ -696,7 +817,9 @@ def run_ours(args, rank, world, local_rank):
         "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic (seeded four-quadrant initial state, generated on the host)",
         "config": workload_config(n, len(boxes), mgs, {"graph_replay": use_graph, "parallelism": "single",
-                                                        "x_sweep": "warp per row segment" if x_rows else "thread per row", "autotune": tuned}),
+                                                        "kernels": ",".join(KIND_NAMES[k] for k in kinds),
+                                                        "autotune": tuned,
+                                                        **parity_scalars(parity)}),
         "roofline": roofline,
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": state_bytes,
@@ -711,6 +834,7 @@ def run_ours(args, rank, world, local_rank):
         "imex_pressure_solve": imex,
         "amr_blast3d": amr,
         "rigid_body": body,
+        "parity": parity,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)

@@ -445,3 +445,46 @@ class Level:
         n = (ctypes.c_longlong * 3)()
         self._ck(lib().bamrex_level_sweep_times(self._h, ms, n))
         return [(ms[d], n[d]) for d in range(self.D)]
+
+
+def main(argv=None):
+    """Step a synthetic level on cuda:0 (for timing and profiling runs):
+
+        python -m bamrex_b200.level [--dim 2] [--n 4096] [--max-grid-size 0]
+            [--staging 0] [--x-mode 0] [--steps 4] [--fp32]
+
+    2D: the four-quadrant Riemann problem (minbee); 3D: seeded random cells
+    (minbee); MUSCL-Hancock + HLLC, CFL 0.8, transmissive.  Prints the
+    kernel of each direction's sweep and the sweep times per direction."""
+    import argparse
+    import json
+
+    from . import problems
+    ap = argparse.ArgumentParser(prog="python -m bamrex_b200.level")
+    ap.add_argument("--dim", type=int, default=2, choices=(2, 3))
+    ap.add_argument("--n", type=int, default=4096)
+    ap.add_argument("--max-grid-size", type=int, default=0)
+    ap.add_argument("--staging", type=int, default=_abi.STAGING_AUTO)
+    ap.add_argument("--x-mode", type=int, default=_abi.XSWEEP_AUTO)
+    ap.add_argument("--steps", type=int, default=4)
+    ap.add_argument("--fp32", action="store_true")
+    a = ap.parse_args(argv)
+    D, n = a.dim, a.n
+    hi = tuple(n - 1 if d < D else 0 for d in range(3))
+    u0 = problems.quadrant_2d(n) if D == 2 else problems.random_states(3, (n, n, n), seed=5)
+    lev = Level(D, (0, 0, 0), hi, [0.0] * D, [1.0] * D, decompose(D, (0, 0, 0), hi, a.max_grid_size or n),
+                Parm(D, limiter=_abi.MINBEE), method=_abi.MUSCL_HANCOCK, cfl=0.8, staging=a.staging, x_mode=a.x_mode,
+                precision=_abi.FP32_STORAGE if a.fp32 else _abi.FP64)
+    try:
+        lev.set_state(u0)
+        lev.set_timing(True)
+        lev.run(a.steps, use_graph=False)
+        out = {"kernels": [lev.staging(d) for d in range(D)],
+               "ms_per_sweep": [ms / max(1, k) for ms, k in lev.sweep_times()]}
+    finally:
+        lev.close()
+    print(json.dumps(out))
+
+
+if __name__ == "__main__":
+    main()

@@ -284,3 +284,95 @@ class Amr:
         out = (ctypes.c_double * (self.D + 2))()
         self._ck(lib().bamrex_amr_conserved_sums(self._h, out))
         return np.array(list(out))
+
+
+def chop_drawn(boxes, choices, rng, D=3):
+    """Boxes cut so each piece's sides are at most a max_grid_size drawn per
+    box from `choices` (all multiples of the blocking factor)."""
+    out = []
+    for lo, hi in boxes:
+        m = int(rng.choice(choices))
+        pieces = [(list(lo), list(hi))]
+        for d in range(D):
+            nxt = []
+            for plo, phi in pieces:
+                a = plo[d]
+                while a <= phi[d]:
+                    b = min(phi[d], a + m - 1)
+                    qlo, qhi = list(plo), list(phi)
+                    qlo[d], qhi[d] = a, b
+                    nxt.append((qlo, qhi))
+                    a = b + 1
+            pieces = nxt
+        out += [(tuple(a), tuple(b)) for a, b in pieces]
+    return out
+
+
+BLAST_BOX_SIZES = (16, 32, 48, 64)
+
+
+def blast_hierarchy(n0, precision=_abi.FP64, seed=20261203, stream=None):
+    """The 3D spherical blast (p 10 inside r < 0.2, 0.1 outside, rho 1) on a
+    3-level hierarchy: base n0^3 on [0,1]^3, ratio 2, blocking factor 8,
+    grad_error on rho >= 0.1, MUSCL-Hancock/minbee, CFL 0.8, boxes cut to a
+    max_grid_size drawn per box from {16, 32, 48, 64}.  The levels form
+    during four coarse steps with a regrid every 2 (the density is uniform
+    at t = 0), then their boxes are redrawn; returns the hierarchy with
+    regridding switched off and the random generator."""
+    from . import problems
+    hi = (n0 - 1,) * 3
+    rng = np.random.default_rng(seed)
+    base = chop_drawn([((0, 0, 0), hi)], BLAST_BOX_SIZES, rng)
+    A = Amr(3, (0, 0, 0), hi, [0.0] * 3, [1.0] * 3, base, Parm(3, limiter=_abi.MINBEE), cfl=0.8, max_level=2,
+            ref_ratio=2, blocking_factor=8, max_grid_size=64, n_error_buf=2, grid_eff=0.7, regrid_int=2,
+            phigrad=[0.1, 0.1], phigrad_var=0, precision=precision, stream=stream)
+    A.set_state(0, problems.blast_3d(n0, radius=0.2))
+    for _ in range(4):
+        A.coarse_step()
+    old = [A.boxes(lev) for lev in range(A.finest_level + 1)]
+    for lev in range(1, len(old)):
+        A.set_level_boxes(lev, chop_drawn(old[lev], BLAST_BOX_SIZES, rng))
+    A.set_regrid_int(0)
+    return A, rng
+
+
+def main(argv=None):
+    """Coarse steps of the 3D blast hierarchy on cuda:0 (for timing and
+    profiling runs):
+
+        python -m bamrex_b200.amr [--n 256] [--steps 4] [--fp32]
+
+    Prints the levels' cells, boxes and sweep kernels and the time per
+    coarse step (host clock around synchronised steps)."""
+    import argparse
+    import json
+    import time
+
+    import torch
+    ap = argparse.ArgumentParser(prog="python -m bamrex_b200.amr")
+    ap.add_argument("--n", type=int, default=256)
+    ap.add_argument("--steps", type=int, default=4)
+    ap.add_argument("--fp32", action="store_true")
+    a = ap.parse_args(argv)
+    A, _ = blast_hierarchy(a.n, _abi.FP32_STORAGE if a.fp32 else _abi.FP64)
+    try:
+        torch.cuda.synchronize()
+        torch.cuda.nvtx.range_push("amr_coarse_steps")
+        t0 = time.perf_counter()
+        for _ in range(a.steps):
+            A.coarse_step()
+        torch.cuda.synchronize()
+        el = time.perf_counter() - t0
+        torch.cuda.nvtx.range_pop()
+        out = {"cells": [sum(int(np.prod([h[d] - l[d] + 1 for d in range(3)])) for l, h in A.boxes(lev))
+                         for lev in range(A.finest_level + 1)],
+               "boxes": [len(A.boxes(lev)) for lev in range(A.finest_level + 1)],
+               "kernels": [[A.level(lev).staging(d) for d in range(3)] for lev in range(A.finest_level + 1)],
+               "ms_per_coarse_step": el / max(1, a.steps) * 1e3}
+    finally:
+        A.close()
+    print(json.dumps(out))
+
+
+if __name__ == "__main__":
+    main()

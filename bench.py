@@ -429,28 +429,6 @@ def imex_step_run(n, net, mode, steps=5):
     return out
 
 
-def _chop_drawn(boxes, choices, rng, D=3):
-    """Boxes cut so each piece's sides are at most a max_grid_size drawn per
-    box from `choices` (all multiples of the blocking factor)."""
-    out = []
-    for lo, hi in boxes:
-        m = int(rng.choice(choices))
-        pieces = [(list(lo), list(hi))]
-        for d in range(D):
-            nxt = []
-            for plo, phi in pieces:
-                a = plo[d]
-                while a <= phi[d]:
-                    b = min(phi[d], a + m - 1)
-                    qlo, qhi = list(plo), list(phi)
-                    qlo[d], qhi[d] = a, b
-                    nxt.append((qlo, qhi))
-                    a = b + 1
-            pieces = nxt
-        out += [(tuple(a), tuple(b)) for a, b in pieces]
-    return out
-
-
 def amr_blast_run(n0, coarse_steps, precision, regrid_steps=None):
     """The 3D spherical blast on a 3-level hierarchy (ratio 2, blocking
     factor 8, max_grid_size drawn per box from {16,32,48,64}, grad_error on
@@ -459,26 +437,9 @@ def amr_blast_run(n0, coarse_steps, precision, regrid_steps=None):
     import torch
 
     import bamrex_b200 as bx
-    from bamrex_b200 import problems
-    from bamrex_b200.amr import Amr
+    from bamrex_b200.amr import blast_hierarchy
 
-    hi = (n0 - 1,) * 3
-    rng = np.random.default_rng(20261203)
-    base = _chop_drawn([((0, 0, 0), hi)], (16, 32, 48, 64), rng)
-    A = Amr(3, (0, 0, 0), hi, [0.0] * 3, [1.0] * 3, base, bx.Parm(3, limiter=bx.MINBEE), cfl=0.8, max_level=2,
-            ref_ratio=2, blocking_factor=8, max_grid_size=64, n_error_buf=2, grid_eff=0.7, regrid_int=2,
-            phigrad=[0.1, 0.1], phigrad_var=0, precision=precision)
-    A.set_state(0, problems.blast_3d(n0, radius=0.2))
-    # the density is uniform at t = 0: levels form from the first regrids
-    for _ in range(4):
-        A.coarse_step()
-
-    def redraw():
-        old = [A.boxes(lev) for lev in range(A.finest_level + 1)]
-        for lev in range(1, len(old)):
-            A.set_level_boxes(lev, _chop_drawn(old[lev], (16, 32, 48, 64), rng))
-
-    redraw()
+    A, _ = blast_hierarchy(n0, precision)
     cells = [sum(int(np.prod([h[d] - l[d] + 1 for d in range(3)])) for l, h in A.boxes(lev))
              for lev in range(A.finest_level + 1)]
     nboxes = [len(A.boxes(lev)) for lev in range(A.finest_level + 1)]

@@ -8,15 +8,10 @@ takes 2^l substeps) and the composite totals within 1e-12.
 The base is 128^3 (the restatement's fill-patch and register arithmetic run
 in numpy, about half a minute per coarse step at this size); the device code
 path is the one of the 256^3 configuration."""
-import os
-import sys
-
 import numpy as np
 import pytest
 
 pytestmark = pytest.mark.gpu
-
-ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
 def _rel_linf(a, b):
@@ -27,26 +22,11 @@ def _rel_linf(a, b):
 def test_blast_hierarchy_coarse_step_matches_oracle(oracle):
     import torch
     assert torch.cuda.is_available()
-    import bamrex_b200 as bx
-    from bamrex_b200 import problems
-    from bamrex_b200.amr import Amr
+    from bamrex_b200.amr import blast_hierarchy
     from oracle.amr_oracle import OAmr
-    sys.path.insert(0, ROOT)
-    from bench import _chop_drawn
     n0 = 128
     hi = (n0 - 1,) * 3
-    rng = np.random.default_rng(20261203)
-    base = _chop_drawn([((0, 0, 0), hi)], (16, 32, 48, 64), rng)
-    A = Amr(3, (0, 0, 0), hi, [0.0] * 3, [1.0] * 3, base, bx.Parm(3, limiter=bx.MINBEE), cfl=0.8, max_level=2,
-            ref_ratio=2, blocking_factor=8, max_grid_size=64, n_error_buf=2, grid_eff=0.7, regrid_int=2,
-            phigrad=[0.1, 0.1], phigrad_var=0)
-    A.set_state(0, problems.blast_3d(n0, radius=0.2))
-    for _ in range(4):
-        A.coarse_step()
-    old = [A.boxes(lev) for lev in range(A.finest_level + 1)]
-    for lev in range(1, len(old)):
-        A.set_level_boxes(lev, _chop_drawn(old[lev], (16, 32, 48, 64), rng))
-    A.set_regrid_int(0)
+    A, _ = blast_hierarchy(n0)
     levels = [A.boxes(lev) for lev in range(A.finest_level + 1)]
     assert len(levels) == 3 and all(len(b) > 0 for b in levels)
     kinds = [[A.level(lev).staging(d) for d in range(3)] for lev in range(3)]

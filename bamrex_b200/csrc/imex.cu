@@ -651,6 +651,12 @@ struct bamrex_imex {
     bamrex_helmholtz* H = nullptr;
     bamrex_precnet* net = nullptr;
     int net_mode = 0;
+    // learned-solve policy: iterations of the last plain solve (warm-started
+    // from the previous pressure it needs few), consecutive learned cycles
+    // that fell back, and pressure solves so far
+    int plain_last = 0;
+    int learned_misses = 0;
+    long long solves = 0;
     char* arena = nullptr;
     Grid3 gU, g1, g2, gV, gA[3], gF[3];
     double *U = nullptr, *Uex = nullptr, *enth = nullptr, *ke = nullptr, *vel = nullptr, *rhs = nullptr;
@@ -787,13 +793,29 @@ int stage_flux(bamrex_imex* h, const double* Ui, const double* Ue, double adt, b
     I_TRY(h, hck(bamrex_helmholtz_set_ccoeffs(h->H, split ? h->vel : nullptr)));
     int it = 0;
     double rr = 0.0;
-    if (h->net) {
+    // The learned cycle gets a budget of FGMRES iterations worth about the
+    // plain solve it replaces (one preconditioner application per FGMRES
+    // iteration, two per BiCGStab iteration): 2 x the last plain count, at
+    // least 2, at most 30; when it misses the plain solve continues from its
+    // iterate.  After two misses in a row the steps solve plainly, trying the
+    // learned cycle again on every 16th solve.
+    const bool learned = h->net && (h->learned_misses < 2 || h->solves % 16 == 0);
+    ++h->solves;
+    if (learned) {
         int plain = 0, fb = 0;
-        // one FGMRES(30) cycle with the network; the plain solve continues
-        // from its iterate if that does not reach the tolerance
+        const int budget = h->plain_last > 0 ? std::min(30, std::max(2, 2 * h->plain_last)) : 30;
         I_TRY(h, hck(bamrex_helmholtz_solve_learned(h->H, h->net, h->net_mode, h->p, h->rhs, h->tol_rel, h->tol_abs,
-                                                    30, 30, &it, &plain, &rr, &fb)));
+                                                    budget, budget, &it, &plain, &rr, &fb)));
+        if (fb) {
+            h->learned_misses++;
+            h->plain_last = plain;
+        } else {
+            h->learned_misses = 0;
+        }
         it += plain;
+    } else if (h->net) {
+        I_TRY(h, hck(bamrex_helmholtz_solve(h->H, h->p, h->rhs, h->tol_rel, h->tol_abs, h->max_iter, 0, &it, &rr)));
+        h->plain_last = it;
     } else {
         // no CUDA graph: the scalars change every step (dt), so each step
         // would capture a new one, and the solve needs few iterations from
@@ -1223,6 +1245,9 @@ extern "C" int bamrex_imex_set_precnet(bamrex_imex* h, bamrex_precnet* net, int 
         return ifail(h, BAMREX_ERR_ARG, "unknown preconditioner mode");
     h->net = net;
     h->net_mode = mode;
+    h->plain_last = 0;
+    h->learned_misses = 0;
+    h->solves = 0;
     return BAMREX_OK;
 }
 

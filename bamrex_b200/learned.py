@@ -87,11 +87,16 @@ def network_input(r, beta_cc):
 
 
 def make_training_pairs(count, n=256, seed=7, tol=1e-7, corr_cells=32, log_sigma=1.0, mach=0.01, dx=1.0 / 2048,
-                        log=None):
+                        log=None, after_vcycle=False):
     """(input, target) pairs from the plain solver on n^2 periodic patches
     with the pressure problem's scalars at cell size dx: a fresh lognormal
     beta and a random right-hand side per pair (white noise blended with a
-    smooth field); target = solution * B / (rms(r) dx^2)."""
+    smooth field); target = solution * B / (rms(r) dx^2).
+
+    after_vcycle: the pair is what one multigrid V-cycle leaves of that
+    right-hand side instead, r' = r - A V(r) and its error A^-1 r' (the
+    network of the PRECOND_VCYCLE_NETWORK mode corrects the V-cycle: it sees
+    the V-cycle's residual and should return the error the V-cycle left)."""
     rng = np.random.default_rng(seed)
     eps = mach * mach
     a = eps / 0.4
@@ -111,6 +116,8 @@ def make_training_pairs(count, n=256, seed=7, tol=1e-7, corr_cells=32, log_sigma
         w = rng.uniform(0.0, 1.0)
         r = w * rng.standard_normal((1, n, n)) + (1 - w) * problems.gaussian_random_field((n, n), rng.uniform(1, 16),
                                                                                           None, rng)[None]
+        if after_vcycle:
+            r = r - h.apply(h.vcycle(r))
         e, it, rr = h.solve(r, tol_rel=tol)
         inp, s = network_input(r[0], beta[0])
         X[k] = inp

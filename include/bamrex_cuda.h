@@ -773,10 +773,13 @@ BAMREX_API int bamrex_imex_est_time_step(bamrex_imex *h, double *dt);
  * A solve that does not reach its tolerance returns BAMREX_ERR_NOT_CONVERGED
  * and leaves the state unchanged. */
 BAMREX_API int bamrex_imex_step(bamrex_imex *h, double dt, int *iters, double *rel_res);
-/* Solve the pressure equation with one FGMRES(30) cycle preconditioned by
- * the network (bamrex_helmholtz_solve_learned; the plain solve continues
- * from its iterate when that cycle does not reach the tolerance) instead of
- * BiCGStab + multigrid; net NULL restores the plain solve. */
+/* Solve the pressure equation with one FGMRES cycle preconditioned by the
+ * network (bamrex_helmholtz_solve_learned; the plain solve continues from
+ * its iterate when that cycle does not reach the tolerance) instead of
+ * BiCGStab + multigrid; net NULL restores the plain solve.  The cycle's
+ * iterations are capped at twice the last plain solve's (at least 2, at most
+ * 30); after two cycles in a row fall back, steps solve plainly and try the
+ * network again on every 16th solve. */
 BAMREX_API int bamrex_imex_set_precnet(bamrex_imex *h, bamrex_precnet *net, int mode);
 /* The pressure operator of the step (its coefficients are those of the last
  * step). */

@@ -216,6 +216,15 @@ class AmrDesc(ctypes.Structure):
     ]
 
 
+class AmrStepping(ctypes.Structure):
+    _fields_ = [
+        ("coarse_steps", ctypes.c_int),
+        ("have_dt", ctypes.c_int),
+        ("nlevels", ctypes.c_int),
+        ("dt_level", ctypes.c_double * MAX_LEVELS),
+    ]
+
+
 # Every symbol include/bamrex_cuda.h declares, with (restype, argtypes).
 _vp, _i, _d, _ll = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_longlong
 _dp = ctypes.POINTER(ctypes.c_double)
@@ -294,6 +303,8 @@ SIGNATURES = {
     "bamrex_amr_coarse_step": (_i, [_vp, _d, _dp, _dp]),
     "bamrex_amr_set_regrid_int": (_i, [_vp, _i]),
     "bamrex_amr_set_body": (_i, [_vp, ctypes.POINTER(BodyDesc)]),
+    "bamrex_amr_get_stepping": (_i, [_vp, ctypes.POINTER(AmrStepping)]),
+    "bamrex_amr_set_stepping": (_i, [_vp, ctypes.POINTER(AmrStepping)]),
     "bamrex_amr_dt_level": (_i, [_vp, _dp]),
     "bamrex_amr_conserved_sums": (_i, [_vp, _dp]),
     "bamrex_helmholtz_create": (_i, [ctypes.POINTER(_vp), ctypes.POINTER(HelmholtzDesc), _vp]),

@@ -262,6 +262,13 @@ class Amr:
             dts.append(self.coarse_step(stop_time))
         return dts
 
+    @property
+    def coarse_steps(self) -> int:
+        """Coarse steps taken (Amr::levelSteps(0)); a restart keeps counting."""
+        st = _abi.AmrStepping()
+        self._ck(lib().bamrex_amr_get_stepping(self._h, ctypes.byref(st)))
+        return st.coarse_steps
+
     def set_regrid_int(self, n):
         self._ck(lib().bamrex_amr_set_regrid_int(self._h, n))
 

@@ -252,11 +252,12 @@ int tma_wa(int D, int dir, const int* lo, const int* hi, int NL)
 }
 
 // Work items of one box for a TMA-staged sweep: line groups x segments of
-// equal length bl (at most seglen).
+// equal length bl (at most seglen).  wa_in > 0 imposes the group shape (a
+// part of a box swept with the box's tensor maps takes the box's).
 void tma_box_items(int D, int dir, const int* lo, const int* hi, int seglen, int NL, long long& items, int& nseg,
-                   int& ngroup, int& wa, int& bl)
+                   int& ngroup, int& wa, int& bl, int wa_in = 0)
 {
-    wa = tma_wa(D, dir, lo, hi, NL);
+    wa = wa_in > 0 ? wa_in : tma_wa(D, dir, lo, hi, NL);
     const int wb = NL / wa;
     const int A = dir == 0 ? 1 : 0, B = dir == 2 ? 1 : 2;
     const int n[3] = { hi[0] - lo[0] + 1, hi[1] - lo[1] + 1, hi[2] - lo[2] + 1 };
@@ -957,6 +958,7 @@ extern "C" int bamrex_level_create(bamrex_level** out, const bamrex_level_desc* 
     const int g = L->ngrow;
     const int al = (int)(256 / L->esize);  // elements per 256 bytes
     const int front = (al - g % al) % al;
+    L->xoff = front;
     std::vector<long long> fab_off(nb);
     long long per_buf = 0;
     for (int b = 0; b < nb; ++b) {
@@ -1171,6 +1173,7 @@ extern "C" int bamrex_level_create(bamrex_level** out, const bamrex_level_desc* 
                 };
                 std::vector<Map> maps((size_t)nb);
                 char* dmaps = L->arena + o_tmap[d][p];
+                L->d_tmap[d][p] = dmaps;
                 for (int b = 0; b < nb && ue == cudaSuccess; ++b) {
                     const FabDev& f = L->fab[p][b];
                     const bamrex_box& Bb = L->boxes[b];
@@ -1219,6 +1222,7 @@ extern "C" int bamrex_level_destroy(bamrex_level* L)
         if (L->hs->h2d) cudaStreamDestroy(L->hs->h2d);
         if (L->hs->d2h) cudaStreamDestroy(L->hs->d2h);
         dev_free(L->hs->staging_out, L->stream);
+        dev_free(L->hs->slab_tab, L->stream);
         delete L->hs;
         L->hs = nullptr;
     }
@@ -1342,6 +1346,53 @@ int host_stream_setup(bamrex_level* L, int C)
         if (e != cudaSuccess) return L->set_err(cuda_fail(e, "host-stream set-up"));
     }
     bamrex_level::HostStream& H = *L->hs;
+    bool any_tma = false;
+    for (int d = 0; d < L->D; ++d) any_tma = any_tma || L->tma(d);
+    if (any_tma && H.slabs != C) {
+        // the slabs' box-table entries of the TMA-staged directions (the
+        // whole fab's tensor maps serve every slab)
+        const int D = L->D, a = D - 1;
+        const bamrex_box B = L->boxes[0];
+        const int rows = B.hi[a] - B.lo[a] + 1;
+        std::vector<SweepBox> tab((size_t)3 * 2 * C);
+        H.slab_items.assign((size_t)3 * 2 * C, 0);
+        for (int d = 0; d < D; ++d) {
+            if (!L->tma(d)) continue;
+            for (int p = 0; p < 2; ++p)
+                for (int c = 0; c < C; ++c) {
+                    SweepBox& sb = tab[((size_t)d * 2 + p) * C + c];
+                    std::memset(&sb, 0, sizeof(sb));
+                    for (int q = 0; q < 3; ++q) {
+                        sb.lo[q] = B.lo[q];
+                        sb.hi[q] = B.hi[q];
+                    }
+                    sb.lo[a] = B.lo[a] + (int)((long long)rows * c / C);
+                    sb.hi[a] = B.lo[a] + (int)((long long)rows * (c + 1) / C) - 1;
+                    sb.in = L->fab[p][0];
+                    sb.out = L->fab[p ^ 1][0];
+                    sb.flux.p = nullptr;
+                    // the group shape of the whole box, which its tensor
+                    // maps' boxes are cut to
+                    const int NL = tma_item_lines(L->wave(d), d);
+                    long long it = 0;
+                    tma_box_items(D, d, sb.lo, sb.hi, L->seglen[d], NL, it, sb.nseg, sb.ngroup, sb.wa, sb.seglen,
+                                  tma_wa(D, d, B.lo, B.hi, NL));
+                    sb.item_begin = 0;
+                    sb.tmap = L->d_tmap[d][p];
+                    sb.xoff = L->xoff;
+                    H.slab_items[((size_t)d * 2 + p) * C + c] = it;
+                }
+        }
+        dev_free(H.slab_tab, L->stream);
+        H.slab_tab = nullptr;
+        H.slabs = 0;
+        e = dev_alloc((void**)&H.slab_tab, sizeof(SweepBox) * tab.size(), L->stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(H.slab_tab, tab.data(), sizeof(SweepBox) * tab.size(), cudaMemcpyHostToDevice, L->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(L->stream);
+        if (e != cudaSuccess) return L->set_err(cuda_fail(e, "slab box tables"));
+        H.slabs = C;
+    }
     while ((int)H.in.size() < C) {
         cudaEvent_t ev[3] = { nullptr, nullptr, nullptr };
         for (int q = 0; q < 3 && e == cudaSuccess; ++q) e = cudaEventCreateWithFlags(&ev[q], cudaEventDisableTiming);
@@ -1418,6 +1469,26 @@ int host_step_enqueue(bamrex_level* L, const double* host_in, double* host_out, 
     auto slab_sweep = [&](int dir, int c, int pin, bool ws) -> int {
         SweepArgs sa;
         std::memset(&sa, 0, sizeof(sa));
+        if (L->tma(dir)) {
+            // the level's own kernel for this direction, on the slab's entry
+            // of the slab box table: the same arithmetic as the plain step
+            const size_t idx = ((size_t)dir * 2 + pin) * C + c;
+            sa.boxes = H.slab_tab + idx;
+            sa.nboxes = 1;
+            sa.total_items = H.slab_items[idx];
+            sa.seglen = L->seglen[dir];
+            sa.halo = method_halo(L->method);
+            sa.dt_host = dt_host;
+            sa.scal = device_dt ? L->d_scal : nullptr;
+            sa.dx = L->dx[dir];
+            sa.k = L->k;
+            sa.ws_max = ws ? &L->d_scal->ws_bits : nullptr;
+            sa.do_update = 1;
+            sa.status = &L->d_scal->status;
+            return level_launch(L, launch_sweep_tma(D, dir, L->fp32, fast_limiter(D, L->method, L->k), L->wave(dir), sa,
+                                                    L->stream),
+                                "slab sweep");
+        }
         sa.boxes = nullptr;
         sa.nboxes = 1;
         SweepBox& sb = sa.one;

@@ -1611,6 +1611,28 @@ extern "C" int bamrex_amr_dt_level(const bamrex_amr* A, double* dt_level)
     return BAMREX_OK;
 }
 
+extern "C" int bamrex_amr_get_stepping(const bamrex_amr* A, bamrex_amr_stepping* out)
+{
+    if (!A || !out) return fail(BAMREX_ERR_ARG, "NULL argument");
+    std::memset(out, 0, sizeof(*out));
+    out->coarse_steps = A->steps;
+    out->have_dt = A->have_dt ? 1 : 0;
+    out->nlevels = (int)std::min<size_t>(A->dt_level.size(), BAMREX_MAX_LEVELS);
+    for (int l = 0; l < out->nlevels; ++l) out->dt_level[l] = A->dt_level[(size_t)l];
+    return BAMREX_OK;
+}
+
+extern "C" int bamrex_amr_set_stepping(bamrex_amr* A, const bamrex_amr_stepping* in)
+{
+    if (!A || !in) return fail(BAMREX_ERR_ARG, "NULL argument");
+    if (in->coarse_steps < 0 || in->nlevels < 0 || in->nlevels > BAMREX_MAX_LEVELS)
+        return amr_fail(A, BAMREX_ERR_ARG, "stepping state out of range");
+    A->steps = in->coarse_steps;
+    A->have_dt = in->have_dt != 0;
+    A->dt_level.assign(in->dt_level, in->dt_level + in->nlevels);
+    return BAMREX_OK;
+}
+
 extern "C" int bamrex_amr_conserved_sums(bamrex_amr* A, double* totals)
 {
     if (!A || !totals) return fail(BAMREX_ERR_ARG, "NULL argument");

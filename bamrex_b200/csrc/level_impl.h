@@ -86,6 +86,8 @@ struct bamrex_level {
     // sweep_wave.cuh)
     int sweep_kind[3] = { BAMREX_STAGING_REGISTERS, BAMREX_STAGING_REGISTERS, BAMREX_STAGING_REGISTERS };
     bool tma(int d) const { return sweep_kind[d] == BAMREX_STAGING_TMA || sweep_kind[d] == BAMREX_STAGING_WAVE; }
+    char* d_tmap[3][2] = {};  // tensor maps of the TMA-staged directions (per parity, one per box)
+    int xoff = 0;             // elements between a fab's padded row start and its first element
     bool wave(int d) const { return sweep_kind[d] == BAMREX_STAGING_WAVE; }
     bamrex::GhostOp* d_ghost[3] = { nullptr, nullptr, nullptr };
     int nghost[3] = { 0, 0, 0 };
@@ -130,6 +132,11 @@ struct bamrex_level {
         cudaEvent_t start = nullptr;
         std::vector<cudaEvent_t> in, out, done;  // per slab: unpacked, packed, downloaded
         double* staging_out = nullptr;
+        // TMA-staged directions: one box-table entry per (direction, input
+        // parity, slab) and its work items, for `slabs` slabs
+        bamrex::SweepBox* slab_tab = nullptr;
+        std::vector<long long> slab_items;
+        int slabs = 0;
     };
     HostStream* hs = nullptr;
 

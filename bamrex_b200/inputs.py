@@ -337,6 +337,7 @@ class Settings:
     check_int: int = -1
     check_file: str = "chk"
     checkpoint_files_output: bool = True
+    restart: str = ""
     # tagging.* (get_tagging_params)
     phierr: list = field(default_factory=list)
     phierr_var: int = 0
@@ -516,8 +517,9 @@ def read_settings(pp: ParmParse, spacedim: int) -> Settings:
     s.check_int = amr.query("check_int", int, -1)
     s.check_file = amr.query("check_file", str, "chk")
     s.checkpoint_files_output = amr.query("checkpoint_files_output", bool, True)
-    if amr.contains("restart"):
-        raise NotImplementedError("amr.restart: restarting from an AMReX checkpoint is not built")
+    # amr.restart names a checkpoint of this library (bamrex_b200.checkpoint);
+    # AMReX's own checkpoint files are not read
+    s.restart = amr.query("restart", str, "")
 
     # tagging
     tg = pp.sub("tagging")
@@ -562,13 +564,17 @@ def amr_kwargs(s: Settings, ngrow: int | None = None, precision=_abi.FP64):
                 phierr_var_is_primv=s.phierr_var_is_primv)
 
 
-def make_amr(s: Settings, initial_data=None, ngrow: int | None = None, precision=_abi.FP64):
+def make_amr(s: Settings, initial_data=None, ngrow: int | None = None, precision=_abi.FP64, base_boxes=None):
     """The device hierarchy of these settings with its rigid body; with
     `initial_data(amr, lev) -> (NC, nz, ny, nx) array` the initial
     hierarchy is built as Amr::init does (level 0, then tag, new level,
-    initial data, up to amr.max_level)."""
+    initial data, up to amr.max_level).  base_boxes replaces the base
+    level's grids (a restart takes the checkpoint's)."""
     from .amr import Amr
-    a = Amr(**amr_kwargs(s, ngrow, precision))
+    kw = amr_kwargs(s, ngrow, precision)
+    if base_boxes is not None:
+        kw["boxes"] = base_boxes
+    a = Amr(**kw)
     if s.body is not None:
         b = s.body
         a.set_body(b["shapes"], combine=b["combine"], rb_bc=b["rb_bc"])
@@ -590,6 +596,14 @@ def plot_due(s: Settings, step: int, time: float, dt: float) -> bool:
     return False
 
 
+def restart_amr(s: Settings, ngrow: int | None = None, precision=_abi.FP64):
+    """The hierarchy of these settings continuing the checkpoint amr.restart
+    (AmrLevelAdv::restart, Source/AmrLevelAdv.cpp:95-104): the checkpoint's
+    grids, state, time and stepping, these settings otherwise."""
+    from .checkpoint import restart_amr as _restart
+    return _restart(s.restart, lambda boxes: make_amr(s, None, ngrow, precision, base_boxes=boxes))
+
+
 def run(amr, s: Settings, on_plot=None, on_check=None):
     """The reference's main loop (Source/main.cpp:68-107) on a hierarchy
     made by make_amr: coarse steps clamped to the next of amr.plot_at and
@@ -598,10 +612,13 @@ def run(amr, s: Settings, on_plot=None, on_check=None):
     amr.plot_int or amr.plot_per is set, after plot_int steps, on crossing
     a multiple of plot_per, at each plot_at time, and at the end) and
     `on_check(amr, step, time)` where it writes a checkpoint (after
-    check_int steps and at the end). Returns (time, coarse steps)."""
-    steps = 0
-    last_plot = last_check = -1
-    if on_plot is not None and s.plot_files_output and (s.plot_int > 0 or s.plot_per > 0):
+    check_int steps and at the end). A restarted hierarchy keeps counting
+    coarse steps from its checkpoint (max_step counts them all) and writes
+    no initial plotfile. Returns (time, coarse steps)."""
+    steps = amr.coarse_steps
+    restarted = steps > 0
+    last_plot = last_check = steps if restarted else -1
+    if on_plot is not None and s.plot_files_output and (s.plot_int > 0 or s.plot_per > 0) and not restarted:
         on_plot(amr, steps, amr.time)
         last_plot = steps
     i_plot = 0
@@ -799,9 +816,12 @@ def main(argv=None):
     pp = ParmParse.from_file(a.inputs, a.overrides)
     s = read_settings(pp, a.dim)
     fn = INITIAL_DATA[a.problem](pp, s)
-    if s.checkpoint_files_output and s.check_int > 0:
-        print("note: amr.check_int is set; AMReX checkpoints are not written")
-    amr = make_amr(s, fn, precision=_abi.FP32_STORAGE if a.fp32_storage else _abi.FP64)
+    prec = _abi.FP32_STORAGE if a.fp32_storage else _abi.FP64
+    if s.restart:
+        amr = restart_amr(s, precision=prec)
+        print("restarted from %s at t = %.10g, coarse step %d" % (s.restart, amr.time, amr.coarse_steps))
+    else:
+        amr = make_amr(s, fn, precision=prec)
 
     def plot(amr_, step, time):
         path = plotfile_name(s.plot_file, step)
@@ -809,7 +829,14 @@ def main(argv=None):
         write_amr_plotfile(path, amr_, step)
         print("wrote %s at t = %.6g" % (path, time))
 
-    t, n = run(amr, s, on_plot=plot)
+    def check(amr_, step, time):
+        from .checkpoint import write_checkpoint
+        path = plotfile_name(s.check_file, step)
+        os.makedirs(os.path.dirname(path) or ".", exist_ok=True)
+        write_checkpoint(path, amr_)
+        print("wrote %s at t = %.6g" % (path, time))
+
+    t, n = run(amr, s, on_plot=plot, on_check=check)
     print("%d coarse steps, t = %.10g" % (n, t))
     amr.close()
 

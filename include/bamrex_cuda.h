@@ -588,6 +588,22 @@ BAMREX_API int bamrex_amr_set_regrid_int(bamrex_amr *amr, int regrid_int);
 BAMREX_API int bamrex_amr_set_body(bamrex_amr *amr, const bamrex_body_desc *desc);
 /* dt of every level after the last computeInitialDt / computeNewDt. */
 BAMREX_API int bamrex_amr_dt_level(const bamrex_amr *amr, double *dt_level);
+
+/* The stepping state a checkpoint keeps besides the levels' boxes and
+ * states (Amr::checkPoint's level steps and dt_level behind
+ * amr.checkPoint(), Source/main.cpp:96-99, with AmrLevelAdv::checkPoint /
+ * restart, Source/AmrLevelAdv.cpp:95-113): the coarse steps taken (they
+ * time the regrids), whether a time step has been set, and the time step
+ * of every level.  A restart rebuilds the levels and their states, then
+ * sets this; the next coarse step then continues the run bit for bit. */
+typedef struct bamrex_amr_stepping {
+    int coarse_steps;
+    int have_dt;
+    int nlevels;                           /* entries of dt_level in use */
+    double dt_level[BAMREX_MAX_LEVELS];
+} bamrex_amr_stepping;
+BAMREX_API int bamrex_amr_get_stepping(const bamrex_amr *amr, bamrex_amr_stepping *out);
+BAMREX_API int bamrex_amr_set_stepping(bamrex_amr *amr, const bamrex_amr_stepping *in);
 /* Composite conserved totals: every level's sums minus those of its cells
  * covered by the next finer level (NCOMP doubles; synchronises). */
 BAMREX_API int bamrex_amr_conserved_sums(bamrex_amr *amr, double *totals);

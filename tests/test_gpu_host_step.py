@@ -15,13 +15,13 @@ def torch_cuda():
     return torch
 
 
-def _level(D, n, mgs, bc, method=0, precision=0, x_mode=0):
+def _level(D, n, mgs, bc, method=0, precision=0, x_mode=0, staging=0):
     import bamrex_b200 as bx
     from bamrex_b200.level import decompose
     hi = tuple(x - 1 for x in n)
     boxes = decompose(D, (0,) * D, hi, mgs)
     return bx.Level(D, (0,) * D, hi, [0.0] * D, [1.0] * D, boxes, bx.Parm(D), method=method, cfl=0.8,
-                    bc_lo=(bc,) * D, bc_hi=(bc,) * D, precision=precision, x_mode=x_mode)
+                    bc_lo=(bc,) * D, bc_hi=(bc,) * D, precision=precision, x_mode=x_mode, staging=staging)
 
 
 def _state(D, n, seed):
@@ -46,12 +46,19 @@ CASES = [
 ]
 
 
-@pytest.mark.parametrize("case", CASES, ids=[str(c) for c in CASES])
+# the slabs swept by every kernel kind (registers, TMA march, wavefront): a
+# slab takes the whole box's tensor maps and lane-group shape
+STAGED = [(2, (96, 96), 96, 0, 0, 0, 0, 4, k) for k in (1, 2, 3)] + \
+    [(3, (24, 20, 28), 28, 0, 0, 0, 0, 5, k) for k in (1, 2, 3)] + [(3, (24, 20, 28), 28, 2, 0, 1, 0, 4, 3)]
+
+
+@pytest.mark.parametrize("case", CASES + STAGED, ids=[str(c) for c in CASES + STAGED])
 def test_step_host_equals_plain_step(torch_cuda, case):
     torch = torch_cuda
-    D, n, mgs, bc, method, prec, xm, slabs = case
+    D, n, mgs, bc, method, prec, xm, slabs = case[:8]
+    st = case[8] if len(case) > 8 else 0
     u0 = _state(D, n, seed=3)
-    ref_lev = _level(D, n, mgs, bc, method, prec, xm)
+    ref_lev = _level(D, n, mgs, bc, method, prec, xm, st)
     ref_lev.set_state(u0)
     dt = ref_lev.estTimeStep()
     ref_lev.advance(0.0, dt)
@@ -59,7 +66,7 @@ def test_step_host_equals_plain_step(torch_cuda, case):
     ref_next = ref_lev.estTimeStep()
     ref_lev.close()
 
-    lev = _level(D, n, mgs, bc, method, prec, xm)
+    lev = _level(D, n, mgs, bc, method, prec, xm, st)
     packed = lev.packing.pack(u0)
     h = torch.tensor(packed).pin_memory()
     out = torch.empty_like(h).pin_memory()

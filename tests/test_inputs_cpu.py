@@ -157,7 +157,6 @@ def test_periodic_geometry_overrides_faces():
     ("amr.ref_ratio = 2 4\n", NotImplementedError, "one ratio"),
     ("ls.geom_type = box\n", NotImplementedError, "geom_type = box"),
     ("ls.geom_type = teapot\n", I.InputsError, "Invalid geometry"),
-    ("amr.restart = chk00010\n", NotImplementedError, "restart"),
 ])
 def test_refusals(text, exc, match):
     with pytest.raises(exc, match=match):
@@ -225,8 +224,9 @@ def test_amr_arguments():
 # ---- the main loop ---------------------------------------------------------
 
 class _StandInAmr:
-    def __init__(self, dt, time=0.0):
+    def __init__(self, dt, time=0.0, coarse_steps=0):
         self.dt, self.time, self.calls = dt, time, []
+        self.coarse_steps = coarse_steps
 
     def coarse_step(self, stop_time=-1.0):
         dt = self.dt
@@ -234,12 +234,13 @@ class _StandInAmr:
             dt = stop_time - self.time
         self.calls.append(stop_time)
         self.time += dt
+        self.coarse_steps += 1
         return dt
 
 
-def _loop(text, dt):
+def _loop(text, dt, start_step=0, start_time=None):
     s = I.read_settings(_pp(text), 2)
-    amr = _StandInAmr(dt, s.strt_time)
+    amr = _StandInAmr(dt, s.strt_time if start_time is None else start_time, start_step)
     plots, checks = [], []
     t, n = I.run(amr, s, on_plot=lambda a, k, tt: plots.append(k), on_check=lambda a, k, tt: checks.append(k))
     return s, amr, t, n, plots, checks
@@ -464,3 +465,16 @@ def test_missing_include_is_an_inputs_error(tmp_path):
     (tmp_path / "inputs").write_text("FILE = not_there\n")
     with pytest.raises(I.InputsError, match="FILE = not_there: no such file"):
         I.ParmParse.from_file(str(tmp_path / "inputs"))
+
+
+def test_main_loop_after_a_restart():
+    """A hierarchy restarted at coarse step 4 keeps counting: max_step counts
+    the steps before the restart, no initial plotfile, the next plot and
+    checkpoint on the original cadence."""
+    text = QUADRANT_2D.replace("amr.plot_int        = 10", "amr.plot_int = 4") + \
+        "max_step = 10\nstop_time = 100\namr.check_int = 3\n"
+    s, amr, t, n, plots, checks = _loop(text, 0.1, start_step=4, start_time=0.4)
+    assert n == 10 and len(amr.calls) == 6
+    assert plots == [8, 10] and checks == [6, 9, 10]
+    assert s.restart == ""
+    assert I.read_settings(_pp(QUADRANT_2D + "amr.restart = chk00010\n"), 2).restart == "chk00010"

@@ -233,6 +233,9 @@ SIGNATURES = {
     "bamrex_release_memory": (_i, []),
     "bamrex_last_error": (ctypes.c_char_p, []),
     "bamrex_status_string": (ctypes.c_char_p, [_i]),
+    "bamrex_profile_enable": (_i, [_i]),
+    "bamrex_profile_reset": (_i, []),
+    "bamrex_profile_report": (_i, [ctypes.c_char_p, _i, ctypes.POINTER(ctypes.c_int)]),
     "bamrex_parm_set_defaults": (_i, [ctypes.POINTER(CParm), _i]),
     "bamrex_parm_init": (_i, [ctypes.POINTER(CParm)]),
     "bamrex_compute_flux": (_i, [_i, _i, _i, _d, ctypes.POINTER(Box), Array4, Array4, _dp, _d,
@@ -364,6 +367,30 @@ def lib() -> ctypes.CDLL:
         fn.argtypes = args
     _LIB = L
     return L
+
+
+def profile_enable(on=True) -> bool:
+    """Turn the library's host-side region timers on or off; returns the
+    previous setting."""
+    return bool(lib().bamrex_profile_enable(1 if on else 0))
+
+
+def profile_reset() -> None:
+    lib().bamrex_profile_reset()
+
+
+def profile_report() -> list:
+    """The region timers as [(name, calls, total_s, avg_ms, max_ms)], largest
+    total first."""
+    need = ctypes.c_int(0)
+    lib().bamrex_profile_report(None, 0, ctypes.byref(need))
+    buf = ctypes.create_string_buffer(max(1, need.value))
+    lib().bamrex_profile_report(buf, len(buf), ctypes.byref(need))
+    rows = []
+    for line in buf.value.decode().splitlines()[1:]:
+        name, calls, total, avg, mx = line.rsplit(" ", 4)
+        rows.append((name, int(calls), float(total), float(avg), float(mx)))
+    return rows
 
 
 def check(rc: int, level_handle=None, amr_handle=None) -> None:

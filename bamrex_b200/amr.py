@@ -347,10 +347,12 @@ def main(argv=None):
     """Coarse steps of the 3D blast hierarchy on cuda:0 (for timing and
     profiling runs):
 
-        python -m bamrex_b200.amr [--n 256] [--steps 4] [--fp32]
+        python -m bamrex_b200.amr [--n 256] [--steps 4] [--fp32] [--regrid-int K] [--profile]
 
     Prints the levels' cells, boxes and sweep kernels and the time per
-    coarse step (host clock around synchronised steps)."""
+    coarse step (host clock around synchronised steps); --regrid-int K
+    regrids every K coarse steps during the timed steps, --profile adds the
+    library's region timers (bamrex_profile_report) over those steps."""
     import argparse
     import json
     import time
@@ -360,9 +362,15 @@ def main(argv=None):
     ap.add_argument("--n", type=int, default=256)
     ap.add_argument("--steps", type=int, default=4)
     ap.add_argument("--fp32", action="store_true")
+    ap.add_argument("--regrid-int", type=int, default=0)
+    ap.add_argument("--profile", action="store_true")
     a = ap.parse_args(argv)
     A, _ = blast_hierarchy(a.n, _abi.FP32_STORAGE if a.fp32 else _abi.FP64)
     try:
+        A.set_regrid_int(a.regrid_int)
+        if a.profile:
+            _abi.profile_enable(True)
+            _abi.profile_reset()
         torch.cuda.synchronize()
         torch.cuda.nvtx.range_push("amr_coarse_steps")
         t0 = time.perf_counter()
@@ -376,6 +384,9 @@ def main(argv=None):
                "boxes": [len(A.boxes(lev)) for lev in range(A.finest_level + 1)],
                "kernels": [[A.level(lev).staging(d) for d in range(3)] for lev in range(A.finest_level + 1)],
                "ms_per_coarse_step": el / max(1, a.steps) * 1e3}
+        if a.profile:
+            out["regions"] = [{"name": n, "calls": c, "total_s": round(t, 6), "max_ms": round(m, 3)}
+                              for n, c, t, _, m in _abi.profile_report()]
     finally:
         A.close()
     print(json.dumps(out))

@@ -291,6 +291,9 @@ int choose_tma_seglen(int D, int dir, const std::vector<bamrex_box>& boxes, long
         if ((nmax + m - 1) / m >= 32) cand.push_back((nmax + m - 1) / m);
     std::sort(cand.begin(), cand.end(), std::greater<int>());
     cand.erase(std::unique(cand.begin(), cand.end()), cand.end());
+    // every candidate >= the widest extent cuts each box into one segment:
+    // the largest of them stands for all (it would win their ties)
+    while (cand.size() > 1 && cand[1] >= nmax) cand.erase(cand.begin() + 1);
     const long long W = std::max(1LL, resident_units);
     int best = cand[0];
     long long best_span = -1;
@@ -884,6 +887,8 @@ extern "C" int bamrex_level_create(bamrex_level** out, const bamrex_level_desc* 
         if ((desc->bc_lo[d] == BAMREX_BC_PERIODIC) != (desc->bc_hi[d] == BAMREX_BC_PERIODIC))
             return fail(BAMREX_ERR_ARG, "periodic boundaries must be set on both sides");
     }
+    BX_PROFILE("bamrex_level_create");
+    ProfPhases phase("level_create:validate");
     long long covered = 0;
     for (int b = 0; b < desc->nboxes; ++b) {
         const bamrex_box& B = desc->boxes[b];
@@ -952,6 +957,7 @@ extern "C" int bamrex_level_create(bamrex_level** out, const bamrex_level_desc* 
         L->own_stream = true;
     }
 
+    phase.next("level_create:layout");
     // ---- layout of the state fabs: rows padded to 256 bytes, first valid
     // cell of each row 256-byte aligned.
     const int nb = desc->nboxes;
@@ -980,6 +986,7 @@ extern "C" int bamrex_level_create(bamrex_level** out, const bamrex_level_desc* 
         L->fab[1].push_back(f);
     }
 
+    phase.next("level_create:sweep_tables");
     // ---- staging of each direction's sweep
     if (desc->staging < BAMREX_STAGING_AUTO || desc->staging > BAMREX_STAGING_WAVE) {
         delete L;
@@ -1070,6 +1077,7 @@ extern "C" int bamrex_level_create(bamrex_level** out, const bamrex_level_desc* 
         L->items[d] = acc;
     }
 
+    phase.next("level_create:ghost_ops");
     // ---- ghost ops
     BoxIndex bidx;
     bidx.build(L->domain, L->boxes, D);
@@ -1095,6 +1103,7 @@ extern "C" int bamrex_level_create(bamrex_level** out, const bamrex_level_desc* 
         }
     }
 
+    phase.next("level_create:arena");
     // ---- one arena
     size_t off = 0;
     auto take = [&](size_t bytes) {
@@ -1121,7 +1130,6 @@ extern "C" int bamrex_level_create(bamrex_level** out, const bamrex_level_desc* 
         if (L->tma(d))
             for (int p = 0; p < 2; ++p) o_tmap[d][p] = take(kMapBytes * nb);
     const size_t o_pack = take(sizeof(PackBox) * nb);
-    const size_t o_stage = take((size_t)L->ncells * L->NC * 8);
     const size_t o_scal = take(sizeof(StepScalars));
     cudaError_t e = dev_alloc((void**)&L->arena, off, L->stream);
     if (e != cudaSuccess) {
@@ -1148,9 +1156,9 @@ extern "C" int bamrex_level_create(bamrex_level** out, const bamrex_level_desc* 
         L->d_ghost[d] = (GhostOp*)(L->arena + o_ghost[d]);
     }
     L->d_pack = (PackBox*)(L->arena + o_pack);
-    L->staging = (double*)(L->arena + o_stage);
     L->d_scal = (StepScalars*)(L->arena + o_scal);
 
+    phase.next("level_create:upload");
     // upload tables on the level's stream (ordered before its kernels),
     // then wait for them: setup only
     auto up = [&](void* dst, const void* src, size_t bytes) -> cudaError_t {
@@ -1233,6 +1241,8 @@ extern "C" int bamrex_level_destroy(bamrex_level* L)
         cudaEventDestroy(ev.second);
     }
     dev_free(L->arena, L->stream);
+    dev_free(L->staging, L->stream);
+    dev_free(L->tag_buf, L->stream);
     for (int d = 0; d < 3; ++d) dev_free(L->halo_mem[d], L->stream);
     pinned_small_free(L->h_scal);
     if (L->own_stream && L->stream) cudaStreamDestroy(L->stream);
@@ -1283,6 +1293,22 @@ extern "C" int bamrex_level_staging(const bamrex_level* L, int dir)
     return L->sweep_kind[dir];
 }
 
+namespace bamrex {
+
+int level_staging_ready(bamrex_level* L)
+{
+    if (L->staging) return BAMREX_OK;
+    void* p = nullptr;
+    const cudaError_t e = dev_alloc(&p, (size_t)L->ncells * L->NC * 8, L->stream);
+    if (e != cudaSuccess)
+        return L->set_err(fail(BAMREX_ERR_OOM, std::string("allocation of the level's host staging buffer failed: ") +
+                                                   cudaGetErrorString(e)));
+    L->staging = static_cast<double*>(p);
+    return BAMREX_OK;
+}
+
+}  // namespace bamrex
+
 extern "C" int bamrex_level_copy_in(bamrex_level* L, const double* src)
 {
     if (!L || !src) return fail(BAMREX_ERR_ARG, "NULL argument");
@@ -1290,6 +1316,7 @@ extern "C" int bamrex_level_copy_in(bamrex_level* L, const double* src)
     const double* from = src;
     if (cudaPointerGetAttributes(&at, src) != cudaSuccess || at.type != cudaMemoryTypeDevice) {
         cudaGetLastError();
+        BX_TRY(level_staging_ready(L));
         const cudaError_t e = cudaMemcpyAsync(L->staging, src, (size_t)L->ncells * L->NC * 8, cudaMemcpyDefault, L->stream);
         if (e != cudaSuccess) return L->set_err(cuda_fail(e, "copy_in memcpy"));
         from = L->staging;
@@ -1307,6 +1334,7 @@ extern "C" int bamrex_level_copy_out(bamrex_level* L, double* dst)
     cudaPointerAttributes at;
     const bool dev = cudaPointerGetAttributes(&at, dst) == cudaSuccess && at.type == cudaMemoryTypeDevice;
     cudaGetLastError();
+    if (!dev) BX_TRY(level_staging_ready(L));
     double* to = dev ? dst : L->staging;
     BX_TRY(level_launch(L, launch_pack(L->NC, L->fp32, L->d_fab[L->cur], L->d_pack, (int)L->boxes.size(), L->ncells, to, 1, L->stream),
                         "pack"));
@@ -1335,6 +1363,7 @@ int host_slabs(const bamrex_level* L, int nslabs)
 
 int host_stream_setup(bamrex_level* L, int C)
 {
+    BX_TRY(level_staging_ready(L));
     cudaError_t e = cudaSuccess;
     if (!L->hs) {
         L->hs = new (std::nothrow) bamrex_level::HostStream();

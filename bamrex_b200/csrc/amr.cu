@@ -13,6 +13,7 @@
 #include <memory>
 #include <mutex>
 #include <new>
+#include <numeric>
 #include <string>
 #include <thread>
 #include <tuple>
@@ -107,19 +108,6 @@ void subtract_boxes(const bamrex_box& region, const BoxIndex& idx, const std::ve
     out.insert(out.end(), cur.begin(), cur.end());
 }
 
-int find_containing(const BoxIndex& idx, const std::vector<bamrex_box>& boxes, const int* c, std::vector<int>& hits)
-{
-    idx.query(c, c, hits);
-    int best = -1;
-    for (int h : hits) {
-        const bamrex_box& b = boxes[h];
-        if (c[0] >= b.lo[0] && c[0] <= b.hi[0] && c[1] >= b.lo[1] && c[1] <= b.hi[1] && c[2] >= b.lo[2] &&
-            c[2] <= b.hi[2])
-            best = (best < 0) ? h : std::min(best, h);
-    }
-    return best;
-}
-
 // The box containing each cell of q (x fastest), -1 where none; a level's
 // boxes are disjoint, so the owner is unique.
 void cell_owners(const BoxIndex& idx, const std::vector<bamrex_box>& boxes, const bamrex_box& q, std::vector<int>& own,
@@ -152,12 +140,14 @@ struct bamrex_coupling {
     bool old_valid = false;
     double t_old = 0, t_new = 0;
     // interpolation: [0] coarse/fine ghosts, [1] whole fine boxes (FillCoarsePatch)
+    // (the patch values of set [1] live only while fill_coarse_patch runs)
     CfRegion* d_reg_set[2] = { nullptr, nullptr };
     int nreg_set[2] = { 0, 0 };
     long long ncell_set[2] = { 0, 0 };
-    CfPatchCell* d_pcell_set[2] = { nullptr, nullptr };
     long long npatch_set[2] = { 0, 0 };
     double* d_patch_set[2] = { nullptr, nullptr };
+    OwnerMap own;         // owners of the coarse level's cells
+    CoarseDomain cdom;
     // flux registers
     int nslots[3] = { 0, 0, 0 };
     FaceRec* d_cfaces[3] = { nullptr, nullptr, nullptr };
@@ -192,6 +182,41 @@ void map_into_domain(const bamrex_level* L, int* c, int& negmask)
             c[d] = c[d] < lo ? lo : hi;
         }
     }
+}
+
+// Gather arguments of patch set `set` (mode as CfGatherArgs) into `patch`.
+CfGatherArgs gather_args(const bamrex_coupling* C, int set, int mode, double a_old, double a_new, double* patch)
+{
+    CfGatherArgs a;
+    a.regions = C->d_reg_set[set];
+    a.nregions = C->nreg_set[set];
+    a.npatch = C->npatch_set[set];
+    a.own = C->own;
+    a.dom = C->cdom;
+    a.crse_old = C->d_old_fab;
+    a.crse_new = C->crse->d_fab[C->crse->cur];
+    a.NC = C->NC;
+    a.mode = mode;
+    a.a_old = a_old;
+    a.a_new = a_new;
+    a.patch = patch;
+    a.bad = nullptr;
+    return a;
+}
+
+// "coarse cell (i,j,k) is not a valid coarse cell" for patch cell idx of
+// a region set.
+std::string describe_patch_cell(const bamrex_coupling* C, const std::vector<CfRegion>& R, long long idx)
+{
+    size_t n = 0;
+    while (n + 1 < R.size() && R[n + 1].patch_begin <= idx) ++n;
+    const long long local = idx - R[n].patch_begin, row = local / R[n].pn[0];
+    int c[3] = { R[n].plo[0] + (int)(local - row * R[n].pn[0]), R[n].plo[1] + (int)(row % R[n].pn[1]),
+                 R[n].plo[2] + (int)(row / R[n].pn[1]) };
+    int neg = 0;
+    map_into_domain(C->crse, c, neg);
+    return "coarse cell (" + std::to_string(c[0]) + "," + std::to_string(c[1]) + "," + std::to_string(c[2]) +
+           ") is not a valid coarse cell";
 }
 
 // Host worker threads for a table build of `work` records: about 64k
@@ -245,16 +270,11 @@ struct OwnerScratch {
 };
 
 // Coarse patches (coarsened region grown by one coarse cell) of a set of
-// fine regions. Patches inside the coarse domain take each cell's owner from
-// one sweep over the boxes they meet; cells outside it are mapped by the
-// boundary rules and looked up one by one. Regions run on host threads, each
-// writing its own slice of `cells`.
-int build_patches(const bamrex_coupling* C, std::vector<CfRegion>& regs, std::vector<CfPatchCell>& cells,
-                  const BoxIndex& cidx)
+// fine regions: each region's patch box and its place in the patch and cell
+// numbering.  The owners of the patch cells are looked up on the device.
+long long build_patches(const bamrex_coupling* C, std::vector<CfRegion>& regs)
 {
-    const bamrex_level* Lc = C->crse;
     long long pacc = 0, cacc = 0;
-    std::vector<bamrex_box> patch(regs.size());
     for (size_t n = 0; n < regs.size(); ++n) {
         CfRegion& R = regs[n];
         bamrex_box w;
@@ -275,33 +295,41 @@ int build_patches(const bamrex_coupling* C, std::vector<CfRegion>& regs, std::ve
         R.cell_begin = cacc;
         pacc += box_volume(p);
         cacc += (long long)(R.hi[0] - R.lo[0] + 1) * (R.hi[1] - R.lo[1] + 1) * (R.hi[2] - R.lo[2] + 1);
-        patch[n] = p;
     }
-    cells.resize((size_t)pacc);
-    auto region = [&](int n, OwnerScratch& S) -> std::string {
-        const bamrex_box& p = patch[n];
-        CfPatchCell* out = cells.data() + regs[n].patch_begin;
-        cell_owners(cidx, Lc->boxes, p, S.own, S.hits);
-        bool inside = true;
-        for (int d = 0; d < C->D; ++d) inside = inside && p.lo[d] >= Lc->domain.lo[d] && p.hi[d] <= Lc->domain.hi[d];
-        size_t q = 0;
-        for (int k = p.lo[2]; k <= p.hi[2]; ++k)
-            for (int j = p.lo[1]; j <= p.hi[1]; ++j)
-                for (int i = p.lo[0]; i <= p.hi[0]; ++i, ++q) {
-                    int c[3] = { i, j, k };
-                    int neg = 0, b = S.own[q];
-                    if (!inside) {
-                        map_into_domain(Lc, c, neg);
-                        if (c[0] != i || c[1] != j || c[2] != k) b = find_containing(cidx, Lc->boxes, c, S.hits);
-                    }
-                    if (b < 0)
-                        return "fine level not properly nested: coarse cell (" + std::to_string(c[0]) + "," +
-                               std::to_string(c[1]) + "," + std::to_string(c[2]) + ") is not a valid coarse cell";
-                    out[q] = CfPatchCell{ b, c[0], c[1], c[2], neg };
-                }
-        return std::string();
-    };
-    return parallel_items<OwnerScratch>((int)regs.size(), table_threads(pacc), 8, region);
+    return pacc;
+}
+
+// Owner map of a level (OwnerMap): blocks as large as the greatest common
+// divisor of the box corners' offsets from the domain corner and of the
+// domain's extent, per direction.
+int build_owner_map(const bamrex_level* L, std::vector<int>& owner, int* g, int* nb)
+{
+    long long total = 1;
+    for (int d = 0; d < 3; ++d) {
+        const int n = L->domain.hi[d] - L->domain.lo[d] + 1;
+        int gg = n;
+        for (const auto& b : L->boxes) {
+            gg = std::gcd(gg, b.lo[d] - L->domain.lo[d]);
+            gg = std::gcd(gg, b.hi[d] + 1 - L->domain.lo[d]);
+        }
+        g[d] = std::max(1, gg);
+        nb[d] = n / g[d];
+        total *= nb[d];
+    }
+    if (total > (1LL << 28))
+        return fail(BAMREX_ERR_UNSUPPORTED, "coarse level boxes too finely aligned for its owner map (more than 2^28 blocks)");
+    owner.assign((size_t)total, -1);
+    for (int b = 0; b < (int)L->boxes.size(); ++b) {
+        int lo[3], hi[3];
+        for (int d = 0; d < 3; ++d) {
+            lo[d] = (L->boxes[b].lo[d] - L->domain.lo[d]) / g[d];
+            hi[d] = (L->boxes[b].hi[d] + 1 - L->domain.lo[d]) / g[d] - 1;
+        }
+        for (int K = lo[2]; K <= hi[2]; ++K)
+            for (int J = lo[1]; J <= hi[1]; ++J)
+                for (int I = lo[0]; I <= hi[0]; ++I) owner[((size_t)K * nb[1] + J) * nb[0] + I] = b;
+    }
+    return BAMREX_OK;
 }
 
 CfRegion make_region(int dst, const bamrex_box& b, const int* shift)
@@ -509,6 +537,8 @@ extern "C" int bamrex_coupling_create(bamrex_coupling** out, bamrex_level* crse,
         if (crse->domain.hi[d] - crse->domain.lo[d] >= (1 << 21))
             return fail(BAMREX_ERR_ARG, "coarse domain wider than 2^21 cells");
 
+    BX_PROFILE("bamrex_coupling_create");
+    ProfPhases phase("coupling_create:index");
     std::unique_ptr<bamrex_coupling> C(new (std::nothrow) bamrex_coupling());
     if (!C) return fail(BAMREX_ERR_OOM, "host allocation failed");
     C->crse = crse;
@@ -521,19 +551,25 @@ extern "C" int bamrex_coupling_create(bamrex_coupling** out, bamrex_level* crse,
     fidx.build(fine->domain, fine->boxes, D);
     cidx.build(crse->domain, crse->boxes, D);
 
+    phase.next("coupling_create:patches");
     // interpolation regions and their coarse patches
     std::vector<CfRegion> regs[2];
-    std::vector<CfPatchCell> pcells[2];
     build_ghost_regions(fine, fidx, regs[0]);
     const int zero[3] = { 0, 0, 0 };
     for (int b = 0; b < (int)fine->boxes.size(); ++b) regs[1].push_back(make_region(b, fine->boxes[b], zero));
-    for (int s = 0; s < 2; ++s) BX_TRY(build_patches(C.get(), regs[s], pcells[s], cidx));
+    long long npatch[2];
+    for (int s = 0; s < 2; ++s) npatch[s] = build_patches(C.get(), regs[s]);
+    std::vector<int> owner;
+    int og[3], onb[3];
+    BX_TRY(build_owner_map(crse, owner, og, onb));
 
+    phase.next("coupling_create:registers");
     // flux registers
     std::vector<FaceRec> cf[3], ff[3];
     std::vector<RefluxRec> rr[3];
     for (int d = 0; d < D; ++d) BX_TRY(build_register(C.get(), d, fidx, cidx, cf[d], ff[d], rr[d]));
 
+    phase.next("coupling_create:avg_down");
     // average_down
     std::vector<AvgOp> avg;
     {
@@ -576,6 +612,7 @@ extern "C" int bamrex_coupling_create(bamrex_coupling** out, bamrex_level* crse,
         for (int p = 0; p < 2; ++p) covfab[p].push_back(crse->fab[p][avg[i].crse]);
     }
 
+    phase.next("coupling_create:upload");
     // one arena
     size_t off = 0;
     auto take = [&](size_t bytes) {
@@ -586,12 +623,11 @@ extern "C" int bamrex_coupling_create(bamrex_coupling** out, bamrex_level* crse,
     const int nbc = (int)crse->boxes.size();
     const size_t o_old = take(crse->state_bytes);
     const size_t o_oldfab = take(sizeof(FabDev) * nbc);
-    size_t o_reg[2], o_pc[2], o_patch[2];
-    for (int s = 0; s < 2; ++s) {
-        o_reg[s] = take(sizeof(CfRegion) * regs[s].size());
-        o_pc[s] = take(sizeof(CfPatchCell) * pcells[s].size());
-        o_patch[s] = take(sizeof(double) * C->NC * pcells[s].size());
-    }
+    size_t o_reg[2];
+    for (int s = 0; s < 2; ++s) o_reg[s] = take(sizeof(CfRegion) * regs[s].size());
+    const size_t o_patch0 = take(sizeof(double) * C->NC * npatch[0]);
+    const size_t o_owner = take(sizeof(int) * owner.size());
+    const size_t o_bad = take(2 * sizeof(unsigned long long));
     size_t o_cf[3] = {}, o_ff[3] = {}, o_rr[3] = {}, o_rg[3] = {};
     for (int d = 0; d < D; ++d) {
         o_cf[d] = take(sizeof(FaceRec) * cf[d].size());
@@ -616,10 +652,21 @@ extern "C" int bamrex_coupling_create(bamrex_coupling** out, bamrex_level* crse,
                                           : regs[s].back().cell_begin + (long long)(regs[s].back().hi[0] - regs[s].back().lo[0] + 1) *
                                                                           (regs[s].back().hi[1] - regs[s].back().lo[1] + 1) *
                                                                           (regs[s].back().hi[2] - regs[s].back().lo[2] + 1);
-        C->d_pcell_set[s] = (CfPatchCell*)(A + o_pc[s]);
-        C->npatch_set[s] = (long long)pcells[s].size();
-        C->d_patch_set[s] = (double*)(A + o_patch[s]);
+        C->npatch_set[s] = npatch[s];
     }
+    C->d_patch_set[0] = (double*)(A + o_patch0);
+    C->own.owner = (const int*)(A + o_owner);
+    for (int d = 0; d < 3; ++d) {
+        C->own.lo[d] = crse->domain.lo[d];
+        C->own.g[d] = og[d];
+        C->own.nb[d] = onb[d];
+        C->cdom.lo[d] = crse->domain.lo[d];
+        C->cdom.hi[d] = crse->domain.hi[d];
+        C->cdom.bc_lo[d] = crse->bc_lo[d];
+        C->cdom.bc_hi[d] = crse->bc_hi[d];
+    }
+    C->cdom.D = D;
+    unsigned long long* d_bad = (unsigned long long*)(A + o_bad);
     for (int d = 0; d < D; ++d) {
         C->nslots[d] = (int)rr[d].size();
         C->d_cfaces[d] = (FaceRec*)(A + o_cf[d]);
@@ -642,8 +689,18 @@ extern "C" int bamrex_coupling_create(bamrex_coupling** out, bamrex_level* crse,
     e = up(C->d_old_fab, oldfab.data(), sizeof(FabDev) * nbc);
     for (int s = 0; s < 2 && e == cudaSuccess; ++s) {
         e = up(C->d_reg_set[s], regs[s].data(), sizeof(CfRegion) * regs[s].size());
-        if (e == cudaSuccess) e = up(C->d_pcell_set[s], pcells[s].data(), sizeof(CfPatchCell) * pcells[s].size());
     }
+    if (e == cudaSuccess) e = up((void*)C->own.owner, owner.data(), sizeof(int) * owner.size());
+    // every patch cell of both sets must be a valid coarse cell (proper
+    // nesting): checked once here on the device
+    if (e == cudaSuccess) e = cudaMemsetAsync(d_bad, 0xff, 2 * sizeof(unsigned long long), crse->stream);
+    for (int s = 0; s < 2 && e == cudaSuccess; ++s) {
+        CfGatherArgs ga = gather_args(C.get(), s, 3, 0.0, 1.0, nullptr);
+        ga.bad = d_bad + s;
+        e = launch_cf_gather(crse->fp32, ga, crse->stream);
+    }
+    unsigned long long bad[2] = { ~0ULL, ~0ULL };
+    if (e == cudaSuccess) e = cudaMemcpyAsync(bad, d_bad, sizeof(bad), cudaMemcpyDeviceToHost, crse->stream);
     for (int d = 0; d < D && e == cudaSuccess; ++d) {
         e = up(C->d_cfaces[d], cf[d].data(), sizeof(FaceRec) * cf[d].size());
         if (e == cudaSuccess) e = up(C->d_ffaces[d], ff[d].data(), sizeof(FaceRec) * ff[d].size());
@@ -658,6 +715,12 @@ extern "C" int bamrex_coupling_create(bamrex_coupling** out, bamrex_level* crse,
         dev_free(C->arena, crse->stream);
         return cuda_fail(e, "coupling table upload");
     }
+    for (int s = 0; s < 2; ++s)
+        if (bad[s] != ~0ULL) {
+            const std::string where = describe_patch_cell(C.get(), regs[s], (long long)bad[s]);
+            dev_free(C->arena, crse->stream);
+            return fail(BAMREX_ERR_ARG, "fine level not properly nested: " + where);
+        }
     const int per_slot = D == 1 ? 1 : (D == 2 ? r : r * r);
     for (int d = 0; d < D; ++d) {
         if (!C->nslots[d]) continue;
@@ -709,14 +772,26 @@ static int run_interp(bamrex_coupling* C, int set, int mode, double a_old, doubl
     bamrex_level* Lc = C->crse;
     bamrex_level* Lf = C->fine;
     if (!C->ncell_set[set]) return BAMREX_OK;
-    BX_TRY(cpl_launch(C, launch_cf_gather(C->NC, Lc->fp32, C->d_pcell_set[set], C->npatch_set[set], C->d_old_fab,
-                                          Lc->d_fab[Lc->cur], mode, a_old, a_new, C->d_patch_set[set], Lc->stream),
+    double* patch = C->d_patch_set[set];
+    if (set == 1) {
+        cudaError_t e = dev_alloc((void**)&patch, sizeof(double) * C->NC * C->npatch_set[1], Lc->stream);
+        if (e != cudaSuccess) return fail(BAMREX_ERR_OOM, std::string("coarse patch allocation failed: ") + cudaGetErrorString(e));
+    }
+    struct Release {
+        double* p;
+        cudaStream_t s;
+        ~Release()
+        {
+            if (p) dev_free(p, s);
+        }
+    } release{ set == 1 ? patch : nullptr, Lc->stream };
+    BX_TRY(cpl_launch(C, launch_cf_gather(Lc->fp32, gather_args(C, set, mode, a_old, a_new, patch), Lc->stream),
                       "coarse patch gather"));
     CfInterpArgs a;
     a.regions = C->d_reg_set[set];
     a.nregions = C->nreg_set[set];
     a.ncells = C->ncell_set[set];
-    a.patch = C->d_patch_set[set];
+    a.patch = patch;
     a.npatch = C->npatch_set[set];
     a.fine0 = Lf->d_fab[0];
     a.fine1 = Lf->d_fab[1];
@@ -833,7 +908,11 @@ extern "C" int bamrex_level_tag(bamrex_level* L, int grad_var, int grad_var_is_p
     spec.grad_var = grad_var;
     spec.grad_primv = grad_var_is_primv ? 1 : 0;
     spec.grad_thr = grad_threshold;
-    char* dtags = reinterpret_cast<char*>(L->staging);  // ncells bytes <= staging size
+    if (!L->tag_buf) {
+        const cudaError_t ea = dev_alloc((void**)&L->tag_buf, (size_t)std::max(1LL, L->ncells), L->stream);
+        if (ea != cudaSuccess) return L->set_err(cuda_fail(ea, "tag buffer allocation"));
+    }
+    char* dtags = L->tag_buf;
     BX_TRY(level_launch(L, launch_tag(L->D, L->fp32, L->d_fab[L->cur], L->d_pack, (int)L->boxes.size(), L->ncells, L->k,
                                       spec, dtags, L->stream),
                         "tagging"));
@@ -1121,6 +1200,7 @@ extern "C" int bamrex_cluster_tags(int D, const bamrex_box* domain, const int* p
                                    int max_grid_size, int n_error_buf, int n_proper, double grid_eff,
                                    bamrex_box* out, int max_out, int* nout)
 {
+    BX_PROFILE("bamrex_cluster_tags");
     if (!domain || !boxes || !tags || !nout || D < 1 || D > 3 || nboxes < 1) return fail(BAMREX_ERR_ARG, "bad argument");
     if (ref_ratio != 2 && ref_ratio != 4) return fail(BAMREX_ERR_ARG, "ref_ratio must be 2 or 4");
     if (blocking_factor < 2 * ref_ratio || blocking_factor % (2 * ref_ratio) != 0)
@@ -1142,6 +1222,7 @@ extern "C" int bamrex_cluster_tags(int D, const bamrex_box* domain, const int* p
         for (int d = 0; d < 3; ++d)
             if (B.lo[d] < dl[d] || B.hi[d] >= dl[d] + n[d] || B.hi[d] < B.lo[d])
                 return fail(BAMREX_ERR_ARG, "box outside the domain");
+    ProfPhases phase("cluster_tags:mark");
     BlockedSpace bs;
     bs.D = D;
     bs.c = c;
@@ -1183,6 +1264,7 @@ extern "C" int bamrex_cluster_tags(int D, const bamrex_box* domain, const int* p
         for (int J = 0; J < nt[1]; ++J)
             for (int I = 0; I < nt[0]; ++I)
                 if (bs.near_tag.at(I, J, K) && bs.is_allowed(I, J, K)) btag.at(I, J, K) = 1;
+    phase.next("cluster_tags:cluster");
     Cluster cl;
     cl.tags = &btag;
     cl.eff = grid_eff;
@@ -1193,6 +1275,7 @@ extern "C" int bamrex_cluster_tags(int D, const bamrex_box* domain, const int* p
         all.hi[d] = nt[d] - 1;
     }
     cl.run(all, 0);
+    phase.next("cluster_tags:clip_chop");
     std::vector<bamrex_box> clipped, chopped;
     for (const auto& b : cl.out) clip_to_allowed(bs, b, D, clipped);
     const int mgs_t = max_grid_size / blocking_factor;
@@ -1304,15 +1387,20 @@ int set_level(bamrex_amr* A, int lev, const std::vector<bamrex_box>& boxes)
             if (b.lo[d] % bf != 0 || (b.hi[d] + 1) % bf != 0)
                 return amr_fail(A, BAMREX_ERR_ARG, "fine boxes must be aligned to blocking_factor");
     if (lev <= finest && same_boxes(boxes, A->levels[lev]->boxes)) return BAMREX_OK;
+    BX_PROFILE("amr_set_level");
+    ProfPhases phase("amr_set_level:make_level");
     bamrex_level* L = nullptr;
     AMR_TRY(A, make_level(A, lev, boxes, &L));
+    phase.next("amr_set_level:coupling");
     bamrex_coupling* C = nullptr;
     int rc = bamrex_coupling_create(&C, A->levels[lev - 1], L, A->desc.ref_ratio);
     if (rc != BAMREX_OK) {
         bamrex_level_destroy(L);
         return A->set_err(rc);
     }
+    phase.next("amr_set_level:fill_coarse_patch");
     rc = bamrex_coupling_fill_coarse_patch(C);
+    phase.next("amr_set_level:copy_old");
     if (rc == BAMREX_OK && lev <= finest) {
         // old data of this level where the new boxes overlap it
         bamrex_level* O = A->levels[lev];
@@ -1365,6 +1453,7 @@ int set_level(bamrex_amr* A, int lev, const std::vector<bamrex_box>& boxes)
         bamrex_level_destroy(L);
         return A->set_err(rc);
     }
+    phase.next("amr_set_level:recouple_finer");
     // the next finer level stays if it is still properly nested in the new
     // boxes (coupled afresh), else it and everything above it go
     bamrex_coupling* C2 = nullptr;
@@ -1374,6 +1463,7 @@ int set_level(bamrex_amr* A, int lev, const std::vector<bamrex_box>& boxes)
         A->cpl[lev + 1] = nullptr;
         keep_finer = bamrex_coupling_create(&C2, L, A->levels[lev + 1], A->desc.ref_ratio) == BAMREX_OK;
     }
+    phase.next("amr_set_level:destroy_old");
     if (lev <= finest) {
         bamrex_coupling_destroy(A->cpl[lev]);
         bamrex_level_destroy(A->levels[lev]);
@@ -1393,6 +1483,7 @@ int set_level(bamrex_amr* A, int lev, const std::vector<bamrex_box>& boxes)
 
 int level_tags(bamrex_amr* A, int l, double time, std::vector<char>& tags)
 {
+    BX_PROFILE("amr_regrid:tags");
     bamrex_level* L = A->levels[l];
     if (l > 0) AMR_TRY(A, bamrex_coupling_fill_patch(A->cpl[l], time));
     const bamrex_amr_desc& d = A->desc;
@@ -1406,6 +1497,7 @@ int level_tags(bamrex_amr* A, int l, double time, std::vector<char>& tags)
 
 int regrid(bamrex_amr* A, int lbase, double time)
 {
+    BX_PROFILE("amr_regrid");
     const bamrex_amr_desc& d = A->desc;
     for (int l = lbase; l < d.max_level && l < (int)A->levels.size(); ++l) {
         std::vector<char> tags;
@@ -1577,10 +1669,14 @@ extern "C" int bamrex_amr_coarse_step(bamrex_amr* A, double stop_time, double* t
         BX_TRY(regrid(A, 0, time));
         regridded = true;
     }
+    BX_PROFILE("amr_coarse_step");
+    ProfPhases phase("amr_coarse_step:dt");
     BX_TRY(compute_dt(A, time, stop_time, A->steps == 0, regridded));
     if (!(A->dt_level[0] > 0) || !std::isfinite(A->dt_level[0]))
         return amr_fail(A, BAMREX_ERR_NAN, "non-positive or non-finite coarse time step");
+    phase.next("amr_coarse_step:enqueue");
     BX_TRY(time_step(A, 0, time));
+    phase.next("amr_coarse_step:sync");
     AMR_TRY(A, bamrex_level_sync(A->levels[0]));
     A->steps++;
     *time_io = time + A->dt_level[0];

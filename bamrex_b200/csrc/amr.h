@@ -24,15 +24,6 @@
 
 namespace bamrex {
 
-// One cell of a coarse patch: the coarse state at (i,j,k) of box `box`
-// (after periodic / reflective / extrapolating boundary mapping), with the
-// components in negmask (bit n) sign-flipped by a reflecting wall.
-struct CfPatchCell {
-    int box;
-    int i, j, k;
-    int negmask;
-};
-
 // A fine ghost region filled by interpolation: fine cells [lo, hi] of box
 // dst (unshifted index space), whose periodic image is cell + shift; the
 // coarse patch [plo, plo + pn) of the image starts at patch_begin.
@@ -72,9 +63,44 @@ struct CfInterpArgs {
     int D, NC, ratio;
 };
 
-cudaError_t launch_cf_gather(int NC, bool fp32, const CfPatchCell* cells, long long ncells, const FabDev* crse_old,
-                             const FabDev* crse_new, int mode, double a_old, double a_new, double* patch,
-                             cudaStream_t s);
+// Which box of a level holds each cell, at the granularity of the level's
+// box corners: blocks of g[0] x g[1] x g[2] cells from the domain's low
+// corner; owner[(K * nb[1] + J) * nb[0] + I] is the box covering block
+// (I, J, K), -1 where no box does.
+struct OwnerMap {
+    const int* owner;
+    int lo[3], g[3], nb[3];
+};
+
+// The coarse domain and its boundary kinds: a patch cell outside it is read
+// at its periodic image, its mirror image (with the normal momentum
+// negated) or the nearest domain cell, by the side's boundary kind.
+struct CoarseDomain {
+    int lo[3], hi[3];
+    int bc_lo[3], bc_hi[3];
+    int D;
+};
+
+// The coarse patches of a set of regions, gathered cell by cell: patch cell
+// e lies in the region whose [patch_begin, patch_begin + volume) holds e, at
+// plo + (x, y, z) with x fastest; its coarse cell is mapped into the domain
+// and looked up in the owner map.
+struct CfGatherArgs {
+    const CfRegion* regions;  // ascending patch_begin
+    int nregions;
+    long long npatch;
+    OwnerMap own;
+    CoarseDomain dom;
+    const FabDev* crse_old;
+    const FabDev* crse_new;
+    int NC;
+    int mode;  // 0 old, 1 new, 2 a_old * old + a_new * new, 3 check the owners only
+    double a_old, a_new;
+    double* patch;            // NC * npatch, component-major (not written in mode 3)
+    unsigned long long* bad;  // mode 3: lowered to the first patch cell with no owner
+};
+
+cudaError_t launch_cf_gather(bool fp32, const CfGatherArgs& a, cudaStream_t s);
 cudaError_t launch_cf_interp(bool fp32, const CfInterpArgs& a, cudaStream_t s);
 cudaError_t launch_avg_down(int D, int NC, int ratio, bool fp32, const AvgOp* ops, int nops, long long ncells,
                             const FabDev* crse, const FabDev* fine, cudaStream_t s);

@@ -8,6 +8,7 @@
 #include <algorithm>
 
 #include "amr.h"
+#include "bamrex_cuda.h"
 #include "common.cuh"
 #include "euler.cuh"
 
@@ -43,25 +44,82 @@ __device__ __forceinline__ int find_begin(const V* v, int n, long long idx)
 __device__ __forceinline__ int floor_div(int a, int b) { return a >= 0 ? a / b : -((-a + b - 1) / b); }
 
 // ------------------------------------------------------------ coarse patch
-// mode 0: old state, 1: new state, 2: a_old * old + a_new * new
-template <typename T>
-__global__ void cf_gather_kernel(int NC, const CfPatchCell* __restrict__ cells, long long n,
-                                 const FabDev* __restrict__ old_fabs, const FabDev* __restrict__ new_fabs, int mode,
-                                 double a_old, double a_new, double* __restrict__ patch)
+__device__ __forceinline__ int find_patch_begin(const CfRegion* v, int n, long long idx)
 {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (v[mid].patch_begin <= idx) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+// Coarse cell c mapped into the domain by the boundary kinds; a mirror
+// image flips the sign of the normal momentum (bit 1 + d of negmask).
+__device__ __forceinline__ void map_into_domain(const CoarseDomain& dm, int* c, int& negmask)
+{
+    for (int d = 0; d < dm.D; ++d) {
+        const int lo = dm.lo[d], hi = dm.hi[d], len = hi - lo + 1;
+        if (c[d] >= lo && c[d] <= hi) continue;
+        const int bc = c[d] < lo ? dm.bc_lo[d] : dm.bc_hi[d];
+        if (bc == BAMREX_BC_PERIODIC) {
+            c[d] = lo + (((c[d] - lo) % len) + len) % len;
+        } else if (bc == BAMREX_BC_REFLECTIVE) {
+            c[d] = c[d] < lo ? 2 * lo - 1 - c[d] : 2 * hi + 1 - c[d];
+            negmask ^= 1 << (1 + d);
+        } else {
+            c[d] = c[d] < lo ? lo : hi;
+        }
+    }
+}
+
+__device__ __forceinline__ int owner_of(const OwnerMap& m, const int* c)
+{
+    int blk[3];
+    for (int d = 0; d < 3; ++d) {
+        const int off = c[d] - m.lo[d];
+        if (off < 0) return -1;
+        blk[d] = off / m.g[d];
+        if (blk[d] >= m.nb[d]) return -1;
+    }
+    return m.owner[((long long)blk[2] * m.nb[1] + blk[1]) * m.nb[0] + blk[0]];
+}
+
+// mode 0: old state, 1: new state, 2: a_old * old + a_new * new, 3: only
+// check that every patch cell has an owner
+template <typename T>
+__global__ void cf_gather_kernel(const CfGatherArgs a)
+{
+    const long long n = a.npatch;
     for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n;
          e += (long long)gridDim.x * blockDim.x) {
-        const CfPatchCell c = cells[e];
-        const FabDev& fo = old_fabs[c.box];
-        const FabDev& fn = new_fabs[c.box];
-        const long long io = fidx(fo, c.i, c.j, c.k), in = fidx(fn, c.i, c.j, c.k);
-        for (int m = 0; m < NC; ++m) {
+        const CfRegion& R = a.regions[find_patch_begin(a.regions, a.nregions, e)];
+        const long long local = e - R.patch_begin;
+        const long long row = local / R.pn[0];
+        int c[3] = { R.plo[0] + (int)(local - row * R.pn[0]), R.plo[1] + (int)(row % R.pn[1]),
+                     R.plo[2] + (int)(row / R.pn[1]) };
+        int neg = 0;
+        map_into_domain(a.dom, c, neg);
+        const int b = owner_of(a.own, c);
+        if (a.mode == 3) {
+            if (b < 0) atomicMin(a.bad, (unsigned long long)e);
+            continue;
+        }
+        if (b < 0) {
+            // not reached: the coupling checks every patch cell when it is made
+            for (int m = 0; m < a.NC; ++m) a.patch[(long long)m * n + e] = 0.0;
+            continue;
+        }
+        const FabDev& fo = a.crse_old[b];
+        const FabDev& fn = a.crse_new[b];
+        const long long io = fidx(fo, c[0], c[1], c[2]), in = fidx(fn, c[0], c[1], c[2]);
+        for (int m = 0; m < a.NC; ++m) {
             double v;
-            if (mode == 0) v = (double)fo.ptr<T>()[io + m * fo.ns];
-            else if (mode == 1) v = (double)fn.ptr<T>()[in + m * fn.ns];
-            else v = a_old * (double)fo.ptr<T>()[io + m * fo.ns] + a_new * (double)fn.ptr<T>()[in + m * fn.ns];
-            if ((c.negmask >> m) & 1) v = -v;
-            patch[(long long)m * n + e] = v;
+            if (a.mode == 0) v = (double)fo.ptr<T>()[io + m * fo.ns];
+            else if (a.mode == 1) v = (double)fn.ptr<T>()[in + m * fn.ns];
+            else v = a.a_old * (double)fo.ptr<T>()[io + m * fo.ns] + a.a_new * (double)fn.ptr<T>()[in + m * fn.ns];
+            if ((neg >> m) & 1) v = -v;
+            a.patch[(long long)m * n + e] = v;
         }
     }
 }
@@ -227,14 +285,12 @@ __global__ void tag_kernel(const FabDev* __restrict__ fab_tab, const PackBox* __
 
 }  // namespace
 
-cudaError_t launch_cf_gather(int NC, bool fp32, const CfPatchCell* cells, long long ncells, const FabDev* crse_old,
-                             const FabDev* crse_new, int mode, double a_old, double a_new, double* patch,
-                             cudaStream_t s)
+cudaError_t launch_cf_gather(bool fp32, const CfGatherArgs& a, cudaStream_t s)
 {
-    if (ncells <= 0) return cudaSuccess;
-    const int g = grid_for(ncells);
-    if (fp32) cf_gather_kernel<float><<<g, kThreads, 0, s>>>(NC, cells, ncells, crse_old, crse_new, mode, a_old, a_new, patch);
-    else cf_gather_kernel<double><<<g, kThreads, 0, s>>>(NC, cells, ncells, crse_old, crse_new, mode, a_old, a_new, patch);
+    if (a.npatch <= 0) return cudaSuccess;
+    const int g = grid_for(a.npatch);
+    if (fp32) cf_gather_kernel<float><<<g, kThreads, 0, s>>>(a);
+    else cf_gather_kernel<double><<<g, kThreads, 0, s>>>(a);
     return cudaGetLastError();
 }
 

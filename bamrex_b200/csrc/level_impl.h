@@ -11,6 +11,7 @@
 #include "bamrex_cuda.h"
 #include "devmem.h"
 #include "launch.h"
+#include "profiler.h"
 
 namespace bamrex {
 
@@ -95,7 +96,8 @@ struct bamrex_level {
     bamrex::PackBox* d_pack = nullptr;
     long long ncells = 0;
     size_t state_bytes = 0;  // bytes of one state buffer
-    double* staging = nullptr;
+    double* staging = nullptr;  // host copies, allocated on first use
+    char* tag_buf = nullptr;    // errorEst tags, allocated on first use
     bamrex::StepScalars* d_scal = nullptr;
     bamrex::StepScalars* h_scal = nullptr;  // pinned
     int cur = 0;
@@ -166,6 +168,9 @@ struct BoxIndex {
 };
 
 int level_launch(bamrex_level* L, cudaError_t e, const char* what);
+// The level's buffer for host copies (packed layout, ncells x NC doubles),
+// allocated on first use.
+int level_staging_ready(bamrex_level* L);
 int level_fill(bamrex_level* L, int d, int parity, const StepScalars* scal);
 // One sweep of direction d from buffer `parity` into parity ^ 1; reduce_ws:
 // also reduce the max wave speed of the output into d_scal->ws_bits.

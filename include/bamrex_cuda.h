@@ -114,6 +114,18 @@ BAMREX_API int bamrex_release_memory(void);
 BAMREX_API const char *bamrex_last_error(void);
 BAMREX_API const char *bamrex_status_string(int status);
 
+/* Host-side region timers (the reference's BL_PROFILE scopes under AMReX's
+ * TinyProfiler, e.g. Source/AmrLevelAdv_advance.cpp:24, Source/main.cpp:21):
+ * wall time per named phase of level creation, regrid, coarse steps.  Off by
+ * default; on with bamrex_profile_enable(1) or the environment variable
+ * BAMREX_TINY_PROFILE=1.  enable returns the previous setting.  The report
+ * is text, one region per line after a header, "name calls total_s avg_ms
+ * max_ms", sorted by total time; *needed is its size with the terminating
+ * NUL, and at most cap - 1 characters are written. */
+BAMREX_API int bamrex_profile_enable(int on);
+BAMREX_API int bamrex_profile_reset(void);
+BAMREX_API int bamrex_profile_report(char *out, int cap, int *needed);
+
 /* FluidSystem::set_parm_defaults (Source/System/FluidSystem.cpp:52-71) for a
  * spacedim-dimensional fluid (limiting variable = energy, UInd::E = 1+D). */
 BAMREX_API int bamrex_parm_set_defaults(bamrex_parm *parm, int spacedim);

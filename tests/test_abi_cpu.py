@@ -41,6 +41,34 @@ def test_abi_version_and_status_strings():
     assert b"argument" in L.bamrex_status_string(1)
 
 
+def test_region_timers_record_host_phases():
+    """The region timers (the BL_PROFILE / TinyProfiler counterpart) time
+    host-side phases; grid generation is host code, so it runs here."""
+    import bamrex_b200 as bx
+    from bamrex_b200.amr import cluster_tags
+    prev = bx.profile_enable(True)
+    try:
+        bx.profile_reset()
+        assert bx.profile_report() == []
+        tags = np.zeros((32, 32), dtype=np.int8)
+        tags[10:14, 12:20] = 1
+        for _ in range(2):
+            cluster_tags(2, (0, 0, 0), (31, 31, 0), [((0, 0, 0), (31, 31, 0))], tags, ref_ratio=2,
+                         blocking_factor=8, max_grid_size=32)
+        rows = {r[0]: r for r in bx.profile_report()}
+        assert rows["bamrex_cluster_tags"][1] == 2
+        for phase in ("cluster_tags:mark", "cluster_tags:cluster", "cluster_tags:clip_chop"):
+            assert rows[phase][1] == 2 and rows[phase][2] >= 0
+        assert rows["bamrex_cluster_tags"][2] >= rows["cluster_tags:cluster"][2]
+        bx.profile_enable(False)
+        bx.profile_reset()
+        cluster_tags(2, (0, 0, 0), (31, 31, 0), [((0, 0, 0), (31, 31, 0))], tags)
+        assert bx.profile_report() == []
+    finally:
+        bx.profile_enable(prev)
+        bx.profile_reset()
+
+
 @pytest.mark.parametrize("D", [1, 2, 3])
 def test_parm_defaults_match_fluidsystem(D):
     """FluidSystem::set_parm_defaults + init_parm (FluidSystem.cpp:52-101)."""

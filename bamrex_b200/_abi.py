@@ -276,6 +276,12 @@ SIGNATURES = {
     "bamrex_level_fill_dir": (_i, [_vp, _i]),
     "bamrex_level_sweep_dir": (_i, [_vp, _i, _d, _i]),
     "bamrex_level_wave_speed": (_i, [_vp, _dp]),
+    "bamrex_level_dist_begin": (_i, [_vp, _d, _d]),
+    "bamrex_level_wave_speed_async": (_i, [_vp, _vp]),
+    "bamrex_level_dist_dt": (_i, [_vp, _vp, _i]),
+    "bamrex_level_fill_dir_device": (_i, [_vp, _i]),
+    "bamrex_level_sweep_dir_device": (_i, [_vp, _i, _i]),
+    "bamrex_level_dist_end": (_i, [_vp, _dp, _dp, ctypes.POINTER(ctypes.c_int)]),
     "bamrex_level_step_host": (_i, [_vp, _vp, _vp, _d, _i, _dp]),
     "bamrex_level_run_host": (_i, [_vp, _vp, _i, _d, _i, _dp, _dp]),
     "bamrex_level_set_body": (_i, [_vp, ctypes.POINTER(BodyDesc)]),

@@ -146,3 +146,89 @@ extern "C" int bamrex_level_wave_speed(bamrex_level* L, double* ws)
     std::memcpy(ws, &bits, sizeof(double));
     return BAMREX_OK;
 }
+
+// ---------------------------------------------------------------------------
+// The split step with its time step on the device.  Per step a host driver
+// enqueues, without waiting: the halo exchange and sweep of each direction
+// (dt read from the level's step scalars), a copy of this rank's max wave
+// speed into a device buffer, an all-reduce MAX of that buffer over the
+// ranks (NCCL on the level's stream), and bamrex_level_dist_dt, which
+// takes the global max and sets the next dt (estTimeStep and the stop-time
+// clamp of computeNewDt, Source/AmrLevelAdv.cpp:395-477, 600-611).
+
+extern "C" int bamrex_level_dist_begin(bamrex_level* L, double time, double stop_time)
+{
+    if (!L) return fail(BAMREX_ERR_ARG, "NULL level");
+    if (L->run_pending) return L->set_err(fail(BAMREX_ERR_ARG, "a run is pending: call bamrex_level_run_wait"));
+    StepScalars* h = L->h_scal;
+    std::memset(h, 0, sizeof(*h));
+    h->time = time;
+    h->stop_time = stop_time;
+    cudaError_t e = cudaMemcpyAsync(L->d_scal, h, sizeof(StepScalars), cudaMemcpyHostToDevice, L->stream);
+    if (e != cudaSuccess) return L->set_err(cuda_fail(e, "scalars upload"));
+    BX_TRY(level_launch(L, launch_max_wave_speed(L->D, L->fp32, L->d_fab[L->cur], L->d_pack, (int)L->boxes.size(),
+                                                 L->ncells, L->k, &L->d_scal->ws_bits, L->d_scal, L->stream),
+                        "max wave speed"));
+    L->run_pending = true;
+    L->run_start_parity = L->cur;
+    return BAMREX_OK;
+}
+
+extern "C" int bamrex_level_wave_speed_async(bamrex_level* L, double* dst_device)
+{
+    if (!L || !dst_device) return fail(BAMREX_ERR_ARG, "NULL argument");
+    if (!L->run_pending) return L->set_err(fail(BAMREX_ERR_ARG, "call bamrex_level_dist_begin first"));
+    // a max of non-negative doubles kept as their bit patterns: the bits are
+    // the double
+    const cudaError_t e = cudaMemcpyAsync(dst_device, &L->d_scal->ws_bits, sizeof(double), cudaMemcpyDeviceToDevice, L->stream);
+    return e == cudaSuccess ? BAMREX_OK : L->set_err(cuda_fail(e, "wave speed copy"));
+}
+
+extern "C" int bamrex_level_dist_dt(bamrex_level* L, const double* ws_device, int first)
+{
+    if (!L || !ws_device) return fail(BAMREX_ERR_ARG, "NULL argument");
+    if (!L->run_pending) return L->set_err(fail(BAMREX_ERR_ARG, "call bamrex_level_dist_begin first"));
+    const cudaError_t e = cudaMemcpyAsync(&L->d_scal->ws_bits, ws_device, sizeof(double), cudaMemcpyDeviceToDevice, L->stream);
+    if (e != cudaSuccess) return L->set_err(cuda_fail(e, "wave speed copy"));
+    return level_launch(L, launch_step_dt(L->d_scal, L->D, L->dx[0], L->dx[1], L->dx[2], L->cfl, first ? 0 : 1, L->stream),
+                        "step dt");
+}
+
+extern "C" int bamrex_level_fill_dir_device(bamrex_level* L, int dir)
+{
+    if (!L || dir < 0 || dir >= L->D) return fail(BAMREX_ERR_ARG, "bad argument");
+    if (!L->run_pending) return L->set_err(fail(BAMREX_ERR_ARG, "call bamrex_level_dist_begin first"));
+    return level_fill(L, dir, L->cur, L->d_scal);
+}
+
+extern "C" int bamrex_level_sweep_dir_device(bamrex_level* L, int dir, int reduce_ws)
+{
+    if (!L || dir < 0 || dir >= L->D) return fail(BAMREX_ERR_ARG, "bad argument");
+    if (!L->run_pending) return L->set_err(fail(BAMREX_ERR_ARG, "call bamrex_level_dist_begin first"));
+    if (!L->reg_tasks[dir].empty())
+        return L->set_err(fail(BAMREX_ERR_UNSUPPORTED, "flux registers are recorded by bamrex_level_advance only"));
+    // the step scalars' ws_bits is zero here: bamrex_level_dist_dt cleared it
+    BX_TRY(level_sweep(L, dir, L->cur, 0.0, L->d_scal, reduce_ws != 0, true));
+    L->cur ^= 1;
+    return BAMREX_OK;
+}
+
+extern "C" int bamrex_level_dist_end(bamrex_level* L, double* time, double* dt, int* steps)
+{
+    if (!L) return fail(BAMREX_ERR_ARG, "NULL level");
+    if (!L->run_pending) return L->set_err(fail(BAMREX_ERR_ARG, "no run pending"));
+    StepScalars* h = L->h_scal;
+    cudaError_t e = cudaMemcpyAsync(h, L->d_scal, sizeof(StepScalars), cudaMemcpyDeviceToHost, L->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(L->stream);
+    L->run_pending = false;
+    if (e != cudaSuccess) return L->set_err(cuda_fail(e, "split run"));
+    // sweeps skipped after the stop time flipped the host's parity too: the
+    // result is where the counted steps left it
+    if (h->done) L->cur = L->run_start_parity ^ ((h->steps * L->D) & 1);
+    L->ws_valid = false;
+    if (time) *time = h->time;
+    if (dt) *dt = h->dt;
+    if (steps) *steps = h->steps;
+    if (h->status) return L->set_err(fail(h->status, "non-finite or non-positive time step on the device"));
+    return BAMREX_OK;
+}

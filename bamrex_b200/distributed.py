@@ -202,6 +202,43 @@ class DeviceEngine:
         check(lib().bamrex_level_wave_speed(self.level._h, ctypes.byref(out)), self.level._h)
         return out.value
 
+    # the step with dt on the device (bamrex_level_dist_*): nothing here waits
+    def ws_buffer(self):
+        with self.stream_context():
+            return self.torch.zeros(1, dtype=self.torch.float64, device="cuda")
+
+    def begin(self, time, stop_time):
+        from ._abi import check, lib
+        check(lib().bamrex_level_dist_begin(self.level._h, float(time), float(stop_time)), self.level._h)
+
+    def wave_speed_into(self, ws):
+        import ctypes
+        from ._abi import check, lib
+        check(lib().bamrex_level_wave_speed_async(self.level._h, ctypes.c_void_p(ws.data_ptr())), self.level._h)
+
+    def device_dt(self, ws, first):
+        import ctypes
+        from ._abi import check, lib
+        check(lib().bamrex_level_dist_dt(self.level._h, ctypes.c_void_p(ws.data_ptr()), 1 if first else 0),
+              self.level._h)
+
+    def fill_dir_device(self, d):
+        from ._abi import check, lib
+        check(lib().bamrex_level_fill_dir_device(self.level._h, d), self.level._h)
+
+    def sweep_dir_device(self, d, reduce_ws):
+        from ._abi import check, lib
+        check(lib().bamrex_level_sweep_dir_device(self.level._h, d, 1 if reduce_ws else 0), self.level._h)
+
+    def end(self):
+        """(time, next dt, steps taken); waits for the level's stream."""
+        import ctypes
+        from ._abi import check, lib
+        t, dt, n = ctypes.c_double(), ctypes.c_double(), ctypes.c_int()
+        check(lib().bamrex_level_dist_end(self.level._h, ctypes.byref(t), ctypes.byref(dt), ctypes.byref(n)),
+              self.level._h)
+        return t.value, dt.value, n.value
+
 
 class DistLevel:
     """The split step of one level whose boxes are spread over the ranks of
@@ -258,9 +295,46 @@ class DistLevel:
             self.e.sweep_dir(d, dt, d == self.D - 1)
 
     def run(self, nsteps):
+        """nsteps steps with dt computed on the host each step (two waits a
+        step); returns the dts."""
         dts = []
         for _ in range(nsteps):
             dt = self.est_time_step()
             self.advance(dt)
             dts.append(dt)
         return dts
+
+    def _global_max_into(self, ws):
+        self.e.wave_speed_into(ws)
+        if self.dist is not None:
+            with self.e.stream_context():
+                self.dist.all_reduce(ws, op=self.dist.ReduceOp.MAX)
+
+    def run_device(self, nsteps, time=0.0, stop_time=-1.0):
+        """nsteps steps with dt kept on the device: this rank's max wave speed
+        is all-reduced in a device buffer and the next dt computed from it on
+        the level's stream, so the host enqueues the whole run without
+        waiting (computeNewDt across ranks, Source/AmrLevelAdv.cpp:487-619).
+        Returns (time, next dt, steps taken)."""
+        if not hasattr(self, "_ws"):
+            self._ws = self.e.ws_buffer()
+        ws = self._ws
+        self.e.begin(time, stop_time)
+        try:
+            self._global_max_into(ws)
+            self.e.device_dt(ws, True)
+            for _ in range(nsteps):
+                for d in range(self.D):
+                    if self.world > 1:
+                        self.exchange(d)
+                    self.e.fill_dir_device(d)
+                    self.e.sweep_dir_device(d, d == self.D - 1)
+                self._global_max_into(ws)
+                self.e.device_dt(ws, False)
+        except BaseException:
+            try:
+                self.e.end()
+            except Exception:
+                pass
+            raise
+        return self.e.end()

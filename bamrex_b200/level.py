@@ -455,9 +455,11 @@ def main(argv=None):
 
     2D: the four-quadrant Riemann problem (minbee); 3D: seeded random cells
     (minbee); MUSCL-Hancock + HLLC, CFL 0.8, transmissive.  Prints the
-    kernel of each direction's sweep and the sweep times per direction."""
+    kernel of each direction's sweep, the sweep times per direction and the
+    whole step (graph-replayed steps, host clock around synchronised runs)."""
     import argparse
     import json
+    import time
 
     from . import problems
     ap = argparse.ArgumentParser(prog="python -m bamrex_b200.level")
@@ -481,6 +483,16 @@ def main(argv=None):
         lev.run(a.steps, use_graph=False)
         out = {"kernels": [lev.staging(d) for d in range(D)],
                "ms_per_sweep": [ms / max(1, k) for ms, k in lev.sweep_times()]}
+        lev.set_timing(False)
+        lev.set_state(u0)
+        lev.run(2)
+        lev.sync()
+        t0 = time.perf_counter()
+        lev.run(a.steps)
+        lev.sync()
+        ms = (time.perf_counter() - t0) * 1e3 / max(1, a.steps)
+        out["ms_per_step"] = ms
+        out["cell_updates_per_s"] = float(n) ** D / (ms * 1e-3)
     finally:
         lev.close()
     print(json.dumps(out))

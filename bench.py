@@ -60,6 +60,8 @@ def parse_args():
     ap.add_argument("--no-body", action="store_true", help="skip the ghost-fluid rigid-body sample")
     ap.add_argument("--body-cases", default="2d,3d", help="rigid-body cases to run (2d, 3d)")
     ap.add_argument("--no-parity", action="store_true", help="skip the parity checks against the oracle")
+    ap.add_argument("--split", action="store_true",
+                    help="run the multi-rank (split-level, NCCL) path also on one rank")
     ap.add_argument("--fp32-oracle-steps", type=int, default=10,
                     help="steps of the FP32-storage L1 comparison with the FP64 oracle (0: skip)")
     return ap.parse_args()
@@ -810,7 +812,9 @@ def run_ours(args, rank, world, local_rank):
 def run_ours_dist(args, rank, world, local_rank):
     """N ranks, one GPU each: the domain is N blocks of n x n stacked in y
     (weak scaling), one block per rank; halos cross ranks over NCCL between
-    sweeps and the time step is max-reduced over the ranks every step."""
+    sweeps and the max wave speed is all-reduced over the ranks in a device
+    buffer every step, the next dt computed from it on the device, so the
+    host enqueues the timed steps without waiting."""
     import torch
     import torch.distributed as dist
 
@@ -838,7 +842,7 @@ def run_ours_dist(args, rank, world, local_rank):
     del glob
     dl = DistLevel(DeviceEngine(lev), D, (0, 0, 0), hi, boxes, owners, 2, (0, 0, 0), (0, 0, 0), lev.dx, 0.8, rank,
                    world, dist)
-    dl.run(args.warmup)
+    dl.run_device(args.warmup)
     lev.set_timing(True)
     lev.reset_counters()
     clocks = ClockSampler(dev_index)
@@ -849,7 +853,7 @@ def run_ours_dist(args, rank, world, local_rank):
     t_wall0 = time.time()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
-    dl.run(args.steps)
+    dl.run_device(args.steps)
     ev1.record(stream)
     torch.cuda.synchronize()
     dist.barrier()
@@ -872,7 +876,7 @@ def run_ours_dist(args, rank, world, local_rank):
     t0 = time.perf_counter()
     for _ in range(args.e2e_steps):
         lev.copy_in_ptr(h_in.data_ptr())
-        dl.advance(dl.est_time_step())
+        dl.run_device(1)
         lev.copy_out_ptr(h_out.data_ptr())
         lev.sync()
     e2e_s = time.perf_counter() - t0
@@ -898,11 +902,12 @@ def run_ours_dist(args, rank, world, local_rank):
         "config": {"workload": "2D four-quadrant Riemann problem, %d blocks of %dx%d stacked in y (one per GPU), "
                                "MUSCL-Hancock/minbee + HLLC, CFL 0.8, transmissive" % (world, n, n),
                    "cells": cells, "boxes": len(boxes), "l2": "inputs larger than L2", "seed": 20261203,
-                   "parallelism": "domain decomposition: halo exchange over NCCL between sweeps, dt max-reduced"},
+                   "parallelism": "domain decomposition: halo exchange over NCCL between sweeps, max wave speed "
+                                  "all-reduced on the device, dt computed on the device"},
         "roofline": roofline,
         "cpu_baseline": None,
         "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": nloc * 8 * world,
-                "d2h_bytes_per_step": nloc * 8 * world + 8,
+                "d2h_bytes_per_step": nloc * 8 * world + 48,
                 "path": "per rank: bamrex_level_copy_in (pinned host) + split step with NCCL halos + "
                         "bamrex_level_copy_out", "steps": args.e2e_steps},
         "gpu_launches": launches,
@@ -920,10 +925,15 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return run_reference(args, rank, world)
-    if world > 1:
+    if world > 1 or args.split:
         import torch
         import torch.distributed as dist
         torch.cuda.set_device(local_rank)
+        if world == 1:
+            os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+            os.environ.setdefault("MASTER_PORT", "29531")
+            os.environ.setdefault("RANK", "0")
+            os.environ.setdefault("WORLD_SIZE", "1")
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
         try:
             return run_ours_dist(args, rank, world, local_rank)

@@ -399,6 +399,27 @@ BAMREX_API int bamrex_level_sweep_dir(bamrex_level *level, int dir, double dt, i
  * that reduced it, else computed); synchronises the stream. */
 BAMREX_API int bamrex_level_wave_speed(bamrex_level *level, double *ws);
 
+/* The split step with the time step kept on the device, so a host driver
+ * never waits inside a run.  dist_begin uploads the start time and the stop
+ * time (< 0: none) and reduces this rank's max wave speed; per step the
+ * driver enqueues, in order: wave_speed_async (this rank's max wave speed,
+ * a double, copied to dst_device on the level's stream), an all-reduce MAX
+ * of that buffer over the ranks (e.g. NCCL on the level's stream), dist_dt
+ * (dt from the global max: estTimeStep with the stop-time clamp of
+ * computeInitialDt / computeNewDt, Source/AmrLevelAdv.cpp:395-477,
+ * 513-523, 600-611; first != 0 before the first step, 0 after each step,
+ * which also advances the time and step count), then for every direction
+ * the halo exchange, fill_dir_device and sweep_dir_device (the last with
+ * reduce_ws != 0).  dist_end waits and returns the time, the next dt and
+ * the steps taken; it reports a non-finite or non-positive dt the device
+ * met.  Steps enqueued past the stop time do nothing. */
+BAMREX_API int bamrex_level_dist_begin(bamrex_level *level, double time, double stop_time);
+BAMREX_API int bamrex_level_wave_speed_async(bamrex_level *level, double *dst_device);
+BAMREX_API int bamrex_level_dist_dt(bamrex_level *level, const double *ws_device, int first);
+BAMREX_API int bamrex_level_fill_dir_device(bamrex_level *level, int dir);
+BAMREX_API int bamrex_level_sweep_dir_device(bamrex_level *level, int dir, int reduce_ws);
+BAMREX_API int bamrex_level_dist_end(bamrex_level *level, double *time, double *dt, int *steps);
+
 /* ------------------------------------------------------------------ */
 /* Rigid bodies by the ghost-fluid method                               */
 /* ------------------------------------------------------------------ */

@@ -13,7 +13,7 @@ import pytest
 class OracleEngine:
     """CPU engine for DistLevel over the oracle's per-box layout."""
 
-    def __init__(self, lay, parm, method):
+    def __init__(self, lay, parm, method, dx=None, cfl=0.8):
         import torch
         self.torch, self.device = torch, "cpu"
         self.lay, self.parm, self.method = lay, parm, method
@@ -21,6 +21,7 @@ class OracleEngine:
         self.S = [lay.alloc(), lay.alloc()]
         self.cur = 0
         self.halo = {}
+        self.dx, self.cfl = dx, cfl
 
     def set_halo(self, d, send, recv):
         self.halo[d] = (send, recv)
@@ -62,6 +63,53 @@ class OracleEngine:
     def wave_speed(self):
         return self.lay.max_wave_speed(self.S[self.cur], self.parm.adiabatic, self.parm.epsilon)
 
+    # the device-dt protocol (bamrex_level_dist_*), mirrored on the host:
+    # step scalars, the dt kernel's arithmetic, sweeps skipped once done
+    def ws_buffer(self):
+        return self.torch.zeros(1, dtype=self.torch.float64)
+
+    def begin(self, time, stop_time):
+        self.time, self.stop, self.dt, self.steps, self.done = time, stop_time, 0.0, 0, False
+        self.start = self.cur
+
+    def wave_speed_into(self, ws):
+        ws[0] = self.wave_speed()
+
+    def device_dt(self, ws, first):
+        if self.done:
+            return
+        if not first:
+            self.time = self.time + self.dt
+            self.steps += 1
+        ms = float(ws[0])
+        dt_est = 1.0e20
+        for d in range(len(self.dx)):
+            dt_est = min(dt_est, self.dx[d] / ms)
+        dt_est *= self.cfl
+        dt0 = dt_est
+        if self.stop >= 0.0:
+            eps = 0.001 * dt0
+            if self.time + dt0 > self.stop - eps:
+                dt0 = self.stop - self.time
+            if not self.time < self.stop:
+                self.done = True
+        self.dt = dt0
+
+    def fill_dir_device(self, d):
+        if not self.done:
+            self.fill_dir(d)
+
+    def sweep_dir_device(self, d, reduce_ws):
+        if self.done:
+            self.cur ^= 1
+            return
+        self.sweep_dir(d, self.dt, reduce_ws)
+
+    def end(self):
+        if self.done:
+            self.cur = self.start ^ ((self.steps * len(self.dx)) & 1)
+        return self.time, self.dt, self.steps
+
 
 def _case(name):
     from bamrex_b200 import problems
@@ -75,7 +123,7 @@ def _case(name):
     return 3, n, 8, problems.blast_3d(n, radius=0.3), (2, 2, 2), 1
 
 
-def _worker(rank, world, port, name, nsteps, out):
+def _worker(rank, world, port, name, nsteps, out, device_dt=False, stop_time=-1.0):
     import torch.distributed as dist
     from bamrex_b200.distributed import DistLevel, partition
     from oracle import oracle as O
@@ -88,10 +136,14 @@ def _worker(rank, world, port, name, nsteps, out):
         local = [b for b in range(len(boxes)) if owners[b] == rank]
         dx = [1.0 / n] * D
         lay = O.LevelLayout(D, (0, 0, 0), hi, [boxes[b] for b in local], 2, dx, bc_lo=bc, bc_hi=bc)
-        eng = OracleEngine(lay, O.Parm(D, limiter=lim), O.MUSCL_HANCOCK)
+        eng = OracleEngine(lay, O.Parm(D, limiter=lim), O.MUSCL_HANCOCK, dx, 0.8)
         lay.scatter(eng.S[0], u0)
         dl = DistLevel(eng, D, (0, 0, 0), hi, boxes, owners, 2, bc, bc, dx, 0.8, rank, world, dist)
-        dts = dl.run(nsteps)
+        if device_dt:
+            t_end, _, taken = dl.run_device(nsteps, 0.0, stop_time)
+            dts = (t_end, taken)
+        else:
+            dts = dl.run(nsteps)
         glob = lay.gather(eng.S[eng.cur])
         # rank 0 collects every rank's boxes and compares with one process
         parts = [None] * world
@@ -102,8 +154,14 @@ def _worker(rank, world, port, name, nsteps, out):
                 m = ~np.isnan(g)
                 full[m] = g[m]
             ref_lay = O.LevelLayout(D, (0, 0, 0), hi, boxes, 2, dx, bc_lo=bc, bc_hi=bc)
-            ref, t, rdts = O.run_level(ref_lay, u0, O.Parm(D, limiter=lim), O.MUSCL_HANCOCK, 0.8, nsteps=nsteps)
-            np.save(out, np.array([float(np.array_equal(full, ref)), float(rdts == dts), float(np.sum(owners)),
+            if device_dt:
+                ref, t, rdts = O.run_level(ref_lay, u0, O.Parm(D, limiter=lim), O.MUSCL_HANCOCK, 0.8, nsteps=nsteps,
+                                           stop_time=stop_time if stop_time >= 0 else None)
+                same_dt = float(dts == (t, len(rdts)))
+            else:
+                ref, t, rdts = O.run_level(ref_lay, u0, O.Parm(D, limiter=lim), O.MUSCL_HANCOCK, 0.8, nsteps=nsteps)
+                same_dt = float(rdts == dts)
+            np.save(out, np.array([float(np.array_equal(full, ref)), same_dt, float(np.sum(owners)),
                                    float(np.abs(full - ref).max())]))
     finally:
         dist.destroy_process_group()
@@ -122,6 +180,22 @@ def test_two_ranks_equal_one(tmp_path, name):
     import torch.multiprocessing as mp
     out = str(tmp_path / "r.npy")
     mp.spawn(_worker, args=(2, _free_port(), name, 4, out), nprocs=2, join=True)
+    same, same_dt, owned, diff = np.load(out)
+    assert owned > 0, "both ranks own boxes"
+    assert same_dt == 1.0
+    assert same == 1.0, diff
+
+
+@pytest.mark.parametrize("name,stop_time", [("quadrant2d", -1.0), ("periodic2d", -1.0), ("blast3d", -1.0),
+                                            ("quadrant2d", 0.015)])
+def test_two_ranks_device_dt_equal_one(tmp_path, name, stop_time):
+    """The run with dt kept on the device (the wave speed all-reduced in a
+    buffer, dt computed from it where the sweeps read it; no host wait
+    inside the run): same state, time and step count as one process, also
+    when the stop time ends the run early."""
+    import torch.multiprocessing as mp
+    out = str(tmp_path / "r.npy")
+    mp.spawn(_worker, args=(2, _free_port(), name, 6, out, True, stop_time), nprocs=2, join=True)
     same, same_dt, owned, diff = np.load(out)
     assert owned > 0, "both ranks own boxes"
     assert same_dt == 1.0

@@ -81,3 +81,36 @@ def test_two_levels_with_device_halos_equal_one(oracle, D, n, mgs, bc):
     for lev, *_ in ranks:
         lev.close()
     ref.close()
+
+
+@pytest.mark.parametrize("D,n,mgs,stop", [(2, 128, 32, -1.0), (3, 32, 16, -1.0), (2, 128, 64, 0.01)])
+def test_device_dt_split_run_equals_level_run(oracle, D, n, mgs, stop):
+    """The split step with dt on the device (bamrex_level_dist_*: the wave
+    speed copied to a buffer, dt computed from it on the level's stream, the
+    sweeps reading it) equals the level's own device-stepped run bit for
+    bit, time and step count included, also when the stop time ends it."""
+    import torch
+    assert torch.cuda.is_available()
+    import bamrex_b200 as bx
+    from bamrex_b200 import problems
+    from bamrex_b200.distributed import DeviceEngine, DistLevel
+    hi = tuple(n - 1 if d < D else 0 for d in range(3))
+    boxes = oracle.decompose(D, (0, 0, 0), hi, mgs)
+    u0 = problems.quadrant_2d(n) if D == 2 else problems.blast_3d(n, radius=0.3)
+    parm = bx.Parm(D, limiter=bx.MINBEE)
+    a = bx.Level(D, (0, 0, 0), hi, [0.0] * D, [1.0] * D, boxes, parm, cfl=0.8)
+    b = bx.Level(D, (0, 0, 0), hi, [0.0] * D, [1.0] * D, boxes, parm, cfl=0.8)
+    try:
+        a.set_state(u0)
+        b.set_state(u0)
+        dl = DistLevel(DeviceEngine(a), D, (0, 0, 0), hi, boxes, [0] * len(boxes), 2, (0, 0, 0), (0, 0, 0),
+                       [1.0 / n] * D, 0.8, 0, 1, None)
+        t_a, _, steps_a = dl.run_device(7, 0.0, stop)
+        t_b, steps_b = b.run(7, stop_time=stop, use_graph=False)
+        assert steps_a == steps_b and t_a == t_b
+        if stop > 0:
+            assert steps_a < 7 and t_a == stop
+        np.testing.assert_array_equal(a.get_state(), b.get_state())
+    finally:
+        a.close()
+        b.close()

@@ -284,6 +284,7 @@ SIGNATURES = {
     "bamrex_level_dist_end": (_i, [_vp, _dp, _dp, ctypes.POINTER(ctypes.c_int)]),
     "bamrex_level_step_host": (_i, [_vp, _vp, _vp, _d, _i, _dp]),
     "bamrex_level_run_host": (_i, [_vp, _vp, _i, _d, _i, _dp, _dp]),
+    "bamrex_level_host_slabs": (_i, [_vp, _i, ctypes.POINTER(ctypes.c_int)]),
     "bamrex_level_set_body": (_i, [_vp, ctypes.POINTER(BodyDesc)]),
     "bamrex_level_fill_body_ghosts": (_i, [_vp]),
     "bamrex_level_body_field": (_i, [_vp, _i, _dp]),
@@ -311,6 +312,9 @@ SIGNATURES = {
     "bamrex_amr_avg_down_all": (_i, [_vp]),
     "bamrex_amr_coarse_step": (_i, [_vp, _d, _dp, _dp]),
     "bamrex_amr_set_regrid_int": (_i, [_vp, _i]),
+    "bamrex_amr_set_graph": (_i, [_vp, _i]),
+    "bamrex_amr_graph_stats": (_i, [_vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_longlong),
+                                    ctypes.POINTER(ctypes.c_longlong)]),
     "bamrex_amr_set_body": (_i, [_vp, ctypes.POINTER(BodyDesc)]),
     "bamrex_amr_get_stepping": (_i, [_vp, ctypes.POINTER(AmrStepping)]),
     "bamrex_amr_set_stepping": (_i, [_vp, ctypes.POINTER(AmrStepping)]),

@@ -272,6 +272,18 @@ class Amr:
     def set_regrid_int(self, n):
         self._ck(lib().bamrex_amr_set_regrid_int(self._h, n))
 
+    def set_graph(self, on: bool):
+        """Coarse steps replayed as CUDA graphs with the time steps on the
+        device (bamrex_amr_set_graph; on by default)."""
+        self._ck(lib().bamrex_amr_set_graph(self._h, 1 if on else 0))
+
+    def graph_stats(self):
+        """(graphs captured, coarse steps replayed, kernel nodes of the
+        current levels' graph) (bamrex_amr_graph_stats)."""
+        c, r, k = ctypes.c_int(), ctypes.c_longlong(), ctypes.c_longlong()
+        self._ck(lib().bamrex_amr_graph_stats(self._h, ctypes.byref(c), ctypes.byref(r), ctypes.byref(k)))
+        return c.value, r.value, k.value
+
     def set_body(self, shapes, combine=_abi.SDF_UNION, rb_bc=_abi.RB_REFLECTIVE, stencil=2, fill_diagonals=False):
         """A static rigid body on every level, present and future
         (bamrex_amr_set_body); None removes it."""

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 #include <functional>
 #include <cmath>
 #include <cstdint>
@@ -834,7 +835,7 @@ int level_sweep(bamrex_level* L, int d, int parity, double dt_host, const StepSc
     return BAMREX_OK;
 }
 
-int level_step(bamrex_level* L, int parity, double dt_host, StepScalars* scal, bool allow_timing)
+int level_step(bamrex_level* L, int parity, double dt_host, StepScalars* scal, bool allow_timing, bool next_dt)
 {
     // with a rigid body: FillPatch, fill_ghost_rb and fill_consv_boundary
     // (AmrLevelAdv_advance.cpp:108-116) fill every ghost cell first
@@ -848,19 +849,24 @@ int level_step(bamrex_level* L, int parity, double dt_host, StepScalars* scal, b
             // which the next sweep overwrites).  The flux is scaled by dt and
             // the face area as AmrLevelAdv::advance does before
             // FineAdd/CrseInit (Source/AmrLevelAdv_advance.cpp:192-210).
-            if (scal) return L->set_err(fail(BAMREX_ERR_UNSUPPORTED, "flux registers need a host time step"));
-            double scale = dt_host;
+            // With dt on the device the kernel forms the same product there.
+            double scale = dt_host, area[2] = { 1.0, 1.0 };
+            int na = 0;
             for (int e = 0; e < L->D; ++e)
-                if (e != d) scale *= L->dx[e];
+                if (e != d) {
+                    scale *= L->dx[e];
+                    area[na++] = L->dx[e];
+                }
             for (const RegisterTask& t : L->reg_tasks[d])
                 BX_TRY(level_launch(L, launch_register_faces(L->D, d, L->method, L->fp32, L->k, L->d_fab[p], t, L->NC,
-                                                             dt_host, L->dx[d], scale, L->stream),
+                                                             dt_host, L->dx[d], scale, scal, area[0], area[1],
+                                                             L->stream),
                                     "flux register faces"));
         }
         p ^= 1;
         if (d + 1 < L->D) BX_TRY(level_fill(L, d + 1, p, scal));
     }
-    if (scal)
+    if (scal && next_dt)
         BX_TRY(level_launch(L, launch_step_dt(scal, L->D, L->dx[0], L->dx[1], L->dx[2], L->cfl, 1, L->stream), "step dt"));
     return BAMREX_OK;
 }
@@ -1357,6 +1363,12 @@ int host_slabs(const bamrex_level* L, int nslabs)
     for (int d = 0; d < 3; ++d) reg = reg || !L->reg_tasks[d].empty();
     if (L->boxes.size() != 1 || D < 2 || reg || L->body || L->bc_lo[a] == BAMREX_BC_PERIODIC) return 0;
     const int rows = L->boxes[0].hi[a] - L->boxes[0].lo[a] + 1;
+    if (nslabs <= 0) {
+        // automatic: slabs of at least 16 MiB per component (smaller copies
+        // lose PCIe bandwidth when both directions run), 2 to 64 of them
+        const long long comp_bytes = (long long)sizeof(double) * L->ncells;
+        nslabs = (int)std::max(2LL, std::min(64LL, comp_bytes / (16LL << 20)));
+    }
     const int C = std::max(1, std::min(nslabs, rows / 4));
     return C >= 2 ? C : 0;
 }
@@ -1465,9 +1477,20 @@ int host_step_enqueue(bamrex_level* L, const double* host_in, double* host_out, 
         return pb;
     };
     // staging (in) and staging_out hold the packed layout of the whole box
-    // ([n][cells], x fastest); a slab is one range inside every component
+    // ([n][cells], x fastest); a slab is one range inside every component,
+    // moved by one strided copy (NC rows, a component apart) where the pitch
+    // allows: PCIe keeps both directions at full rate with few large copies,
+    // not with one small copy per component
     auto copies = [&](int c, bool to_host, cudaStream_t s) -> cudaError_t {
         const long long first = (long long)(lo_of(c) - B.lo[a]) * plane, cells = (long long)(lo_of(c + 1) - lo_of(c)) * plane;
+        const size_t pitch = sizeof(double) * (size_t)L->ncells;
+        if (pitch <= (size_t)INT_MAX) {
+            const size_t off = (size_t)first;
+            return to_host ? cudaMemcpy2DAsync(host_out + off, pitch, H.staging_out + off, pitch, sizeof(double) * cells,
+                                               L->NC, cudaMemcpyDeviceToHost, s)
+                           : cudaMemcpy2DAsync(L->staging + off, pitch, host_in + off, pitch, sizeof(double) * cells, L->NC,
+                                               cudaMemcpyHostToDevice, s);
+        }
         for (int n = 0; n < L->NC; ++n) {
             const size_t off = (size_t)(n * L->ncells + first);
             const cudaError_t r = to_host
@@ -1647,6 +1670,13 @@ extern "C" int bamrex_level_run_host(bamrex_level* L, double* host, int nsteps, 
                                                                           : "non-finite time step during the run"));
     *time_io = h->time;
     if (dt_next) *dt_next = h->dt;
+    return BAMREX_OK;
+}
+
+extern "C" int bamrex_level_host_slabs(const bamrex_level* L, int nslabs, int* slabs)
+{
+    if (!L || !slabs) return fail(BAMREX_ERR_ARG, "NULL argument");
+    *slabs = host_slabs(L, nslabs);
     return BAMREX_OK;
 }
 

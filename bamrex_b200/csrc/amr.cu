@@ -134,9 +134,9 @@ struct bamrex_coupling {
     bamrex_level* fine = nullptr;
     int r = 2, D = 0, NC = 0;
     char* arena = nullptr;
-    // coarse old time level
-    char* old_state = nullptr;
-    FabDev* d_old_fab = nullptr;
+    // coarse old time level: the coarse values of the ghost patch cells
+    // (set 0) at t_old, the only old data a fill reads
+    double* d_patch_old = nullptr;
     bool old_valid = false;
     double t_old = 0, t_new = 0;
     // interpolation: [0] coarse/fine ghosts, [1] whole fine boxes (FillCoarsePatch)
@@ -193,7 +193,7 @@ CfGatherArgs gather_args(const bamrex_coupling* C, int set, int mode, double a_o
     a.npatch = C->npatch_set[set];
     a.own = C->own;
     a.dom = C->cdom;
-    a.crse_old = C->d_old_fab;
+    a.patch_old = C->d_patch_old;
     a.crse_new = C->crse->d_fab[C->crse->cur];
     a.NC = C->NC;
     a.mode = mode;
@@ -201,6 +201,8 @@ CfGatherArgs gather_args(const bamrex_coupling* C, int set, int mode, double a_o
     a.a_new = a_new;
     a.patch = patch;
     a.bad = nullptr;
+    a.amr = nullptr;
+    a.lc = 0;
     return a;
 }
 
@@ -620,9 +622,7 @@ extern "C" int bamrex_coupling_create(bamrex_coupling** out, bamrex_level* crse,
         off = align_up(off + std::max<size_t>(bytes, 1), 256);
         return o;
     };
-    const int nbc = (int)crse->boxes.size();
-    const size_t o_old = take(crse->state_bytes);
-    const size_t o_oldfab = take(sizeof(FabDev) * nbc);
+    const size_t o_old = take(sizeof(double) * C->NC * npatch[0]);
     size_t o_reg[2];
     for (int s = 0; s < 2; ++s) o_reg[s] = take(sizeof(CfRegion) * regs[s].size());
     const size_t o_patch0 = take(sizeof(double) * C->NC * npatch[0]);
@@ -643,8 +643,7 @@ extern "C" int bamrex_coupling_create(bamrex_coupling** out, bamrex_level* crse,
     cudaError_t e = dev_alloc((void**)&C->arena, off, crse->stream);
     if (e != cudaSuccess) return fail(BAMREX_ERR_OOM, std::string("allocation of the coupling failed: ") + cudaGetErrorString(e));
     char* A = C->arena;
-    C->old_state = A + o_old;
-    C->d_old_fab = (FabDev*)(A + o_oldfab);
+    C->d_patch_old = (double*)(A + o_old);
     for (int s = 0; s < 2; ++s) {
         C->d_reg_set[s] = (CfRegion*)(A + o_reg[s]);
         C->nreg_set[s] = (int)regs[s].size();
@@ -680,13 +679,9 @@ extern "C" int bamrex_coupling_create(bamrex_coupling** out, bamrex_level* crse,
     C->d_cov_fab[1] = (FabDev*)(A + o_covf1);
     C->d_cov_sums = (double*)(A + o_covs);
 
-    std::vector<FabDev> oldfab = crse->fab[0];
-    for (int b = 0; b < nbc; ++b)
-        oldfab[b].p = C->old_state + ((char*)crse->fab[0][b].p - crse->state[0]);
     auto up = [&](void* dst, const void* src, size_t bytes) -> cudaError_t {
         return bytes ? cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, crse->stream) : cudaSuccess;
     };
-    e = up(C->d_old_fab, oldfab.data(), sizeof(FabDev) * nbc);
     for (int s = 0; s < 2 && e == cudaSuccess; ++s) {
         e = up(C->d_reg_set[s], regs[s].data(), sizeof(CfRegion) * regs[s].size());
     }
@@ -755,19 +750,28 @@ extern "C" int bamrex_coupling_destroy(bamrex_coupling* C)
     return BAMREX_OK;
 }
 
+// The coarse values the fine level's ghost patches read, kept for t_old
+// (AMReX keeps the whole old MultiFab; only these cells are ever read).
+static int save_patch_old(bamrex_coupling* C)
+{
+    bamrex_level* Lc = C->crse;
+    return cpl_launch(C, launch_cf_gather(Lc->fp32, gather_args(C, 0, 4, 0.0, 1.0, C->d_patch_old), Lc->stream),
+                      "coarse old patch");
+}
+
 extern "C" int bamrex_coupling_save_coarse_old(bamrex_coupling* C, double t_old, double t_new)
 {
     if (!C) return fail(BAMREX_ERR_ARG, "NULL coupling");
     if (!(t_new > t_old)) return fail(BAMREX_ERR_ARG, "t_new must exceed t_old");
-    bamrex_level* Lc = C->crse;
-    BX_CK(cudaMemcpyAsync(C->old_state, Lc->state[Lc->cur], Lc->state_bytes, cudaMemcpyDeviceToDevice, Lc->stream));
+    BX_TRY(save_patch_old(C));
     C->old_valid = true;
     C->t_old = t_old;
     C->t_new = t_new;
     return BAMREX_OK;
 }
 
-static int run_interp(bamrex_coupling* C, int set, int mode, double a_old, double a_new)
+static int run_interp(bamrex_coupling* C, int set, int mode, double a_old, double a_new, const AmrDev* amr = nullptr,
+                      int lc = 0)
 {
     bamrex_level* Lc = C->crse;
     bamrex_level* Lf = C->fine;
@@ -785,8 +789,10 @@ static int run_interp(bamrex_coupling* C, int set, int mode, double a_old, doubl
             if (p) dev_free(p, s);
         }
     } release{ set == 1 ? patch : nullptr, Lc->stream };
-    BX_TRY(cpl_launch(C, launch_cf_gather(Lc->fp32, gather_args(C, set, mode, a_old, a_new, patch), Lc->stream),
-                      "coarse patch gather"));
+    CfGatherArgs ga = gather_args(C, set, mode, a_old, a_new, patch);
+    ga.amr = amr;
+    ga.lc = lc;
+    BX_TRY(cpl_launch(C, launch_cf_gather(Lc->fp32, ga, Lc->stream), "coarse patch gather"));
     CfInterpArgs a;
     a.regions = C->d_reg_set[set];
     a.nregions = C->nreg_set[set];
@@ -1315,6 +1321,24 @@ struct bamrex_amr {
     bool have_dt = false;
     bool has_body = false;     // a rigid body on every level (bamrex_amr_set_body)
     bamrex_body_desc body;
+    // coarse steps as CUDA graphs (time steps computed on the device): one
+    // graph per level-state key, all dropped when the levels change
+    bool use_graph = true;
+    unsigned generation = 0;
+    AmrDev* d_amr = nullptr;
+    AmrDev* h_amr = nullptr;   // pinned: the step's dt and status, read back
+    double* h_up = nullptr;    // pinned: {time, stop_time} uploaded per step
+    struct StepGraph {
+        unsigned gen = 0;
+        std::vector<int> key;   // per level: current buffer, CFL estimate valid
+        cudaGraphExec_t exec = nullptr;
+        std::vector<int> post;  // the key after the step
+        long long kernels = 0;  // kernel launches inside the graph
+    };
+    std::vector<StepGraph> graphs;
+    int graph_captures = 0;
+    long long graph_replays = 0;
+    int gen_steps = 0;  // coarse steps since the levels last changed
     std::string err;
     int set_err(int code)
     {
@@ -1356,8 +1380,18 @@ int make_level(bamrex_amr* A, int lev, const std::vector<bamrex_box>& boxes, bam
     return BAMREX_OK;
 }
 
+void drop_step_graphs(bamrex_amr* A)
+{
+    for (auto& g : A->graphs)
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+    A->graphs.clear();
+    A->generation++;
+    A->gen_steps = 0;
+}
+
 void drop_levels_above(bamrex_amr* A, int lev)
 {
+    if ((int)A->levels.size() > lev + 1) drop_step_graphs(A);
     while ((int)A->levels.size() > lev + 1) {
         const int l = (int)A->levels.size() - 1;
         bamrex_coupling_destroy(A->cpl[l]);
@@ -1388,6 +1422,7 @@ int set_level(bamrex_amr* A, int lev, const std::vector<bamrex_box>& boxes)
                 return amr_fail(A, BAMREX_ERR_ARG, "fine boxes must be aligned to blocking_factor");
     if (lev <= finest && same_boxes(boxes, A->levels[lev]->boxes)) return BAMREX_OK;
     BX_PROFILE("amr_set_level");
+    drop_step_graphs(A);
     ProfPhases phase("amr_set_level:make_level");
     bamrex_level* L = nullptr;
     AMR_TRY(A, make_level(A, lev, boxes, &L));
@@ -1571,6 +1606,199 @@ int time_step(bamrex_amr* A, int l, double time)
     return BAMREX_OK;
 }
 
+// ---------------------------------------------------------------------
+// A coarse step with the time steps on the device, replayed as one graph.
+//
+// The host path above reads every level's CFL estimate back, forms the
+// coarse dt and enqueues the subcycled recursion with host values.  Here
+// the estimates, the coarse dt (amr_dt_kernel: the same operations) and
+// the substeps' start times (amr_substep_kernel: parent start + i * dt)
+// stay on the device; the levels' sweeps and flux registers read their dt
+// from their step scalars and the coarse/fine fills pick their time weights
+// from the device times.  The recursion does not depend on the values, so
+// it is captured once per level-state key and replayed every coarse step.
+// ---------------------------------------------------------------------
+
+// bamrex_level_advance with the level's device dt (set by amr_dt_kernel).
+int level_advance_dev(bamrex_level* L)
+{
+    const cudaError_t e = cudaMemsetAsync(&L->d_scal->ws_bits, 0, sizeof(unsigned long long), L->stream);
+    if (e != cudaSuccess) return L->set_err(cuda_fail(e, "memset"));
+    BX_TRY(level_step(L, L->cur, 0.0, L->d_scal, false, false));
+    L->cur ^= (L->D & 1);
+    L->ws_valid = true;
+    return BAMREX_OK;
+}
+
+// time_step on device times: substep i of level l within its parent's step.
+int time_step_dev(bamrex_amr* A, int l, int i)
+{
+    const int finest = (int)A->levels.size() - 1;
+    bamrex_level* L = A->levels[l];
+    if (l > 0) BX_CK(launch_amr_substep(A->d_amr, l, i, A->stream));
+    if (l < finest) {
+        // bamrex_coupling_save_coarse_old; its times are set on the host
+        // after the step (host_step_times)
+        bamrex_coupling* C = A->cpl[l + 1];
+        AMR_TRY(A, save_patch_old(C));
+        C->old_valid = true;
+    }
+    if (l > 0) AMR_TRY(A, run_interp(A->cpl[l], 0, 2, 0.0, 1.0, A->d_amr, l - 1));
+    AMR_TRY(A, level_advance_dev(L));
+    if (l < finest) {
+        for (int j = 0; j < A->desc.ref_ratio; ++j) BX_TRY(time_step_dev(A, l + 1, j));
+        if (A->desc.do_reflux) AMR_TRY(A, bamrex_coupling_reflux(A->cpl[l + 1]));
+        AMR_TRY(A, bamrex_coupling_avg_down(A->cpl[l + 1]));
+    }
+    return BAMREX_OK;
+}
+
+// The couplings' coarse old/new times the host recursion leaves (time_step).
+void host_step_times(bamrex_amr* A, int l, double time)
+{
+    if (l + 1 >= (int)A->levels.size()) return;
+    bamrex_coupling* C = A->cpl[l + 1];
+    C->old_valid = true;
+    C->t_old = time;
+    C->t_new = time + A->dt_level[l];
+    const double dtf = A->dt_level[l + 1];
+    for (int i = 0; i < A->desc.ref_ratio; ++i) host_step_times(A, l + 1, time + i * dtf);
+}
+
+std::vector<int> step_key(const bamrex_amr* A)
+{
+    std::vector<int> k;
+    for (const bamrex_level* L : A->levels) {
+        k.push_back(L->cur);
+        k.push_back(L->ws_valid ? 1 : 0);
+    }
+    return k;
+}
+
+void set_step_key(bamrex_amr* A, const std::vector<int>& k)
+{
+    for (size_t l = 0; l < A->levels.size(); ++l) {
+        A->levels[l]->cur = k[2 * l];
+        A->levels[l]->ws_valid = k[2 * l + 1] != 0;
+    }
+}
+
+AmrLevelsArg levels_arg(const bamrex_amr* A)
+{
+    AmrLevelsArg a;
+    std::memset(&a, 0, sizeof(a));
+    a.nl = (int)A->levels.size();
+    a.D = A->D;
+    a.ratio = A->desc.ref_ratio;
+    for (int l = 0; l < a.nl; ++l) {
+        const bamrex_level* L = A->levels[l];
+        a.scal[l] = L->d_scal;
+        a.cfl[l] = L->cfl;
+        for (int d = 0; d < 3; ++d) a.dx[l][d] = L->dx[d];
+    }
+    return a;
+}
+
+int coarse_step_graph(bamrex_amr* A, double stop_time, double time)
+{
+    cudaError_t e = cudaSuccess;
+    if (!A->d_amr) {
+        e = dev_alloc((void**)&A->d_amr, sizeof(AmrDev), A->stream);
+        if (e == cudaSuccess) e = cudaMemsetAsync(A->d_amr, 0, sizeof(AmrDev), A->stream);
+        if (e == cudaSuccess) e = pinned_small_alloc((void**)&A->h_amr, sizeof(AmrDev));
+        if (e == cudaSuccess) e = pinned_small_alloc((void**)&A->h_up, 4 * sizeof(double));
+        if (e != cudaSuccess) return amr_fail(A, BAMREX_ERR_CUDA, std::string("step block: ") + cudaGetErrorString(e));
+    }
+    // the estimates the host path reads (bamrex_level_est_time_step): the
+    // max wave speed of every level whose fused value is stale
+    {
+        BX_PROFILE("amr_coarse_step:dt");
+        for (bamrex_level* L : A->levels) {
+            if (L->ws_valid) continue;
+            e = cudaMemsetAsync(&L->d_scal->ws_bits, 0, sizeof(unsigned long long), L->stream);
+            if (e == cudaSuccess)
+                e = launch_max_wave_speed(L->D, L->fp32, L->d_fab[L->cur], L->d_pack, (int)L->boxes.size(), L->ncells,
+                                          L->k, &L->d_scal->ws_bits, nullptr, L->stream);
+            if (e != cudaSuccess) return amr_fail(A, BAMREX_ERR_CUDA, std::string("max wave speed: ") + cudaGetErrorString(e));
+            L->launches++;
+            L->ws_valid = true;
+        }
+        // {time, stop_time, dt0, status} of the step
+        A->h_up[0] = time;
+        A->h_up[1] = stop_time;
+        A->h_up[2] = 0.0;
+        A->h_up[3] = 0.0;
+        e = cudaMemcpyAsync(A->d_amr, A->h_up, 4 * sizeof(double), cudaMemcpyHostToDevice, A->stream);
+        if (e == cudaSuccess) e = launch_amr_dt(A->d_amr, levels_arg(A), A->stream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(A->h_amr, A->d_amr, sizeof(AmrDev), cudaMemcpyDeviceToHost, A->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(A->stream);
+        if (e != cudaSuccess) return amr_fail(A, BAMREX_ERR_CUDA, std::string("coarse time step: ") + cudaGetErrorString(e));
+    }
+    const AmrDev& h = *A->h_amr;
+    if (h.status == BAMREX_ERR_ARG)
+        return amr_fail(A, BAMREX_ERR_ARG, "a rigid-body interpolation stencil left the fab: raise ngrow");
+    if (h.status == BAMREX_ERR_NOT_CONVERGED)
+        return amr_fail(A, BAMREX_ERR_NOT_CONVERGED, "an exact Riemann solve at a rigid-body interface did not converge");
+    if (h.status == BAMREX_ERR_TIMEOUT)
+        return amr_fail(A, BAMREX_ERR_TIMEOUT, "a sweep gave up waiting for its staged input");
+    if (h.status != 0 || !(h.dt0 > 0) || !std::isfinite(h.dt0))
+        return amr_fail(A, BAMREX_ERR_NAN, "non-positive or non-finite coarse time step");
+    A->dt_level.assign(A->levels.size(), 0.0);
+    for (size_t l = 0; l < A->levels.size(); ++l) A->dt_level[l] = h.dt[l];
+    A->have_dt = true;
+
+    const std::vector<int> key = step_key(A);
+    bamrex_amr::StepGraph* G = nullptr;
+    for (auto& g : A->graphs)
+        if (g.gen == A->generation && g.key == key) G = &g;
+    if (!G) {
+        BX_PROFILE("amr_coarse_step:capture");
+        bamrex_amr::StepGraph g;
+        g.gen = A->generation;
+        g.key = key;
+        cudaGraph_t gr = nullptr;
+        e = cudaStreamBeginCapture(A->stream, cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) return amr_fail(A, BAMREX_ERR_CUDA, std::string("begin capture: ") + cudaGetErrorString(e));
+        const int rc = time_step_dev(A, 0, 0);
+        e = cudaStreamEndCapture(A->stream, &gr);
+        if (rc != BAMREX_OK || e != cudaSuccess) {
+            if (gr) cudaGraphDestroy(gr);
+            set_step_key(A, key);
+            if (rc != BAMREX_OK) return A->set_err(rc);
+            return amr_fail(A, BAMREX_ERR_CUDA, std::string("end capture: ") + cudaGetErrorString(e));
+        }
+        g.post = step_key(A);
+        size_t nn = 0;
+        if (cudaGraphGetNodes(gr, nullptr, &nn) == cudaSuccess && nn) {
+            std::vector<cudaGraphNode_t> nodes(nn);
+            if (cudaGraphGetNodes(gr, nodes.data(), &nn) == cudaSuccess)
+                for (size_t q = 0; q < nn; ++q) {
+                    cudaGraphNodeType t;
+                    if (cudaGraphNodeGetType(nodes[q], &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) g.kernels++;
+                }
+        }
+        e = cudaGraphInstantiate(&g.exec, gr, 0);
+        cudaGraphDestroy(gr);
+        if (e != cudaSuccess) {
+            set_step_key(A, key);
+            return amr_fail(A, BAMREX_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+        }
+        A->graphs.push_back(std::move(g));
+        G = &A->graphs.back();
+        A->graph_captures++;
+    }
+    {
+        BX_PROFILE("amr_coarse_step:replay");
+        e = cudaGraphLaunch(G->exec, A->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(A->stream);
+        if (e != cudaSuccess) return amr_fail(A, BAMREX_ERR_CUDA, std::string("coarse step graph: ") + cudaGetErrorString(e));
+    }
+    A->graph_replays++;
+    set_step_key(A, G->post);
+    host_step_times(A, 0, time);
+    return BAMREX_OK;
+}
+
 }  // namespace
 
 extern "C" int bamrex_amr_create(bamrex_amr** out, const bamrex_amr_desc* desc, void* stream)
@@ -1612,6 +1840,10 @@ extern "C" int bamrex_amr_create(bamrex_amr** out, const bamrex_amr_desc* desc, 
 extern "C" int bamrex_amr_destroy(bamrex_amr* A)
 {
     if (!A) return BAMREX_OK;
+    drop_step_graphs(A);
+    if (A->d_amr) dev_free(A->d_amr, A->stream);
+    pinned_small_free(A->h_amr);
+    pinned_small_free(A->h_up);
     drop_levels_above(A, 0);
     if (!A->levels.empty()) bamrex_level_destroy(A->levels[0]);
     if (A->own_stream) cudaStreamDestroy(A->stream);
@@ -1670,6 +1902,21 @@ extern "C" int bamrex_amr_coarse_step(bamrex_amr* A, double stop_time, double* t
         regridded = true;
     }
     BX_PROFILE("amr_coarse_step");
+    // Graphs once the levels have taken a step as they are and will keep
+    // them for a few steps (a graph captured for one replay costs more than
+    // it saves); the first step after a regrid takes the host path, whose
+    // dt rule also differs there.
+    const bool graph = A->use_graph && !regridded && A->steps > 0 && A->have_dt && A->gen_steps > 0 &&
+                       (A->desc.regrid_int <= 0 || A->desc.regrid_int >= 4 || A->desc.max_level == 0) &&
+                       (int)A->levels.size() <= kAmrMaxLevels;
+    if (graph) {
+        BX_TRY(coarse_step_graph(A, stop_time, time));
+        A->steps++;
+        A->gen_steps++;
+        *time_io = time + A->dt_level[0];
+        if (dt_out) *dt_out = A->dt_level[0];
+        return BAMREX_OK;
+    }
     ProfPhases phase("amr_coarse_step:dt");
     BX_TRY(compute_dt(A, time, stop_time, A->steps == 0, regridded));
     if (!(A->dt_level[0] > 0) || !std::isfinite(A->dt_level[0]))
@@ -1679,14 +1926,37 @@ extern "C" int bamrex_amr_coarse_step(bamrex_amr* A, double stop_time, double* t
     phase.next("amr_coarse_step:sync");
     AMR_TRY(A, bamrex_level_sync(A->levels[0]));
     A->steps++;
+    A->gen_steps++;
     *time_io = time + A->dt_level[0];
     if (dt_out) *dt_out = A->dt_level[0];
+    return BAMREX_OK;
+}
+
+extern "C" int bamrex_amr_set_graph(bamrex_amr* A, int use_graph)
+{
+    if (!A) return fail(BAMREX_ERR_ARG, "NULL hierarchy");
+    A->use_graph = use_graph != 0;
+    if (!A->use_graph) drop_step_graphs(A);
+    return BAMREX_OK;
+}
+
+extern "C" int bamrex_amr_graph_stats(const bamrex_amr* A, int* captures, long long* replays, long long* kernels)
+{
+    if (!A) return fail(BAMREX_ERR_ARG, "NULL hierarchy");
+    if (captures) *captures = A->graph_captures;
+    if (replays) *replays = A->graph_replays;
+    if (kernels) {
+        *kernels = 0;
+        for (const auto& g : A->graphs)
+            if (g.gen == A->generation) *kernels = std::max(*kernels, g.kernels);
+    }
     return BAMREX_OK;
 }
 
 extern "C" int bamrex_amr_set_body(bamrex_amr* A, const bamrex_body_desc* desc)
 {
     if (!A) return fail(BAMREX_ERR_ARG, "NULL hierarchy");
+    drop_step_graphs(A);
     for (bamrex_level* L : A->levels) AMR_TRY(A, bamrex_level_set_body(L, desc));
     A->has_body = desc != nullptr;
     if (desc) A->body = *desc;

@@ -85,22 +85,61 @@ struct CoarseDomain {
 // e lies in the region whose [patch_begin, patch_begin + volume) holds e, at
 // plo + (x, y, z) with x fastest; its coarse cell is mapped into the domain
 // and looked up in the owner map.
+// Time stepping of a hierarchy on the device (a coarse step replayed as one
+// CUDA graph): the coarse time, the stop time, every level's time step and
+// the start time of every level's current substep, computed there with the
+// host recursion's own arithmetic (Source/AmrLevelAdv.cpp:487-619).
+constexpr int kAmrMaxLevels = 8;
+struct AmrDev {
+    double time;       // coarse time at the start of the step (host-written)
+    double stop_time;  // < 0: none (host-written)
+    double dt0;        // the coarse step's dt
+    int status;        // BAMREX_* raised during the step
+    int pad;
+    double dt[kAmrMaxLevels];     // dt of each level
+    double t_sub[kAmrMaxLevels];  // start time of each level's current substep
+};
+
+// Per-level arguments of the device time step (by value).
+struct AmrLevelsArg {
+    StepScalars* scal[kAmrMaxLevels];
+    double dx[kAmrMaxLevels][3];
+    double cfl[kAmrMaxLevels];
+    int nl, D, ratio;
+};
+
 struct CfGatherArgs {
     const CfRegion* regions;  // ascending patch_begin
     int nregions;
     long long npatch;
     OwnerMap own;
     CoarseDomain dom;
-    const FabDev* crse_old;
+    const double* patch_old;  // the coarse old values of the patch cells (saved by mode 4)
     const FabDev* crse_new;
     int NC;
-    int mode;  // 0 old, 1 new, 2 a_old * old + a_new * new, 3 check the owners only
+    // 0 old, 1 new, 2 a_old * old + a_new * new, 3 check the owners only,
+    // 4 save: the current coarse values of the patch cells as they are (no
+    // boundary sign) into `patch`, which then serves as patch_old
+    int mode;
     double a_old, a_new;
     double* patch;            // NC * npatch, component-major (not written in mode 3)
     unsigned long long* bad;  // mode 3: lowered to the first patch cell with no owner
+    // non-null: mode and weights from the device times of the coarse level
+    // lc (its substep start and dt) and the fine level lc + 1, decided as
+    // bamrex_coupling_fill_patch decides them on the host
+    const AmrDev* amr;
+    int lc;
 };
 
 cudaError_t launch_cf_gather(bool fp32, const CfGatherArgs& a, cudaStream_t s);
+// The coarse step's dt from every level's max wave speed (est_time_step +
+// computeNewDt without a regrid) into a->dt and each level's scalars; the
+// first level status (a rigid-body or staging failure of an earlier step)
+// or a non-finite estimate into a->status.
+cudaError_t launch_amr_dt(AmrDev* a, const AmrLevelsArg& lv, cudaStream_t s);
+// t_sub[l] = t_sub[l - 1] + i * dt[l]: the start of substep i of level l.
+cudaError_t launch_amr_substep(AmrDev* a, int l, int i, cudaStream_t s);
+
 cudaError_t launch_cf_interp(bool fp32, const CfInterpArgs& a, cudaStream_t s);
 cudaError_t launch_avg_down(int D, int NC, int ratio, bool fp32, const AvgOp* ops, int nops, long long ncells,
                             const FabDev* crse, const FabDev* fine, cudaStream_t s);

@@ -91,6 +91,25 @@ template <typename T>
 __global__ void cf_gather_kernel(const CfGatherArgs a)
 {
     const long long n = a.npatch;
+    int mode = a.mode;
+    double a_old = a.a_old, a_new = a.a_new;
+    if (a.amr) {
+        // bamrex_coupling_fill_patch's choice, from the device times
+        const double t_old = a.amr->t_sub[a.lc];
+        const double t_new = t_old + a.amr->dt[a.lc];
+        const double time = a.amr->t_sub[a.lc + 1];
+        const double span = t_new - t_old;
+        const double teps = 1e-3 * span;
+        mode = 2;
+        if (fabs(time - t_old) < teps) {
+            mode = 0;
+        } else if (fabs(time - t_new) < teps) {
+            mode = 1;
+        } else {
+            a_old = (t_new - time) / span;
+            a_new = (time - t_old) / span;
+        }
+    }
     for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n;
          e += (long long)gridDim.x * blockDim.x) {
         const CfRegion& R = a.regions[find_patch_begin(a.regions, a.nregions, e)];
@@ -101,7 +120,7 @@ __global__ void cf_gather_kernel(const CfGatherArgs a)
         int neg = 0;
         map_into_domain(a.dom, c, neg);
         const int b = owner_of(a.own, c);
-        if (a.mode == 3) {
+        if (mode == 3) {
             if (b < 0) atomicMin(a.bad, (unsigned long long)e);
             continue;
         }
@@ -110,14 +129,17 @@ __global__ void cf_gather_kernel(const CfGatherArgs a)
             for (int m = 0; m < a.NC; ++m) a.patch[(long long)m * n + e] = 0.0;
             continue;
         }
-        const FabDev& fo = a.crse_old[b];
         const FabDev& fn = a.crse_new[b];
-        const long long io = fidx(fo, c[0], c[1], c[2]), in = fidx(fn, c[0], c[1], c[2]);
+        const long long in = fidx(fn, c[0], c[1], c[2]);
+        if (mode == 4) {
+            for (int m = 0; m < a.NC; ++m) a.patch[(long long)m * n + e] = (double)fn.ptr<T>()[in + m * fn.ns];
+            continue;
+        }
         for (int m = 0; m < a.NC; ++m) {
             double v;
-            if (a.mode == 0) v = (double)fo.ptr<T>()[io + m * fo.ns];
-            else if (a.mode == 1) v = (double)fn.ptr<T>()[in + m * fn.ns];
-            else v = a.a_old * (double)fo.ptr<T>()[io + m * fo.ns] + a.a_new * (double)fn.ptr<T>()[in + m * fn.ns];
+            if (mode == 0) v = a.patch_old[(long long)m * n + e];
+            else if (mode == 1) v = (double)fn.ptr<T>()[in + m * fn.ns];
+            else v = a_old * a.patch_old[(long long)m * n + e] + a_new * (double)fn.ptr<T>()[in + m * fn.ns];
             if ((neg >> m) & 1) v = -v;
             a.patch[(long long)m * n + e] = v;
         }
@@ -283,7 +305,66 @@ __global__ void tag_kernel(const FabDev* __restrict__ fab_tab, const PackBox* __
     }
 }
 
+// computeNewDt of a hierarchy without a regrid (Source/AmrLevelAdv.cpp:
+// 487-619 with AMReX's Amr::computeNewDt): each level's estTimeStep from its
+// max wave speed, the coarse dt the smallest of n_l * dt_l, clamped to the
+// stop time, and dt / n_l on level l; the same operations in the same order
+// as the host path (bamrex_level_est_time_step, compute_dt), so the values
+// are equal bit for bit.  A non-finite or non-positive estimate, or a level
+// status, goes to a->status; the host reads it before it steps.
+__global__ void amr_dt_kernel(AmrDev* a, const AmrLevelsArg lv)
+{
+    int status = 0;
+    for (int l = 0; l < lv.nl; ++l)
+        if (!status && lv.scal[l]->status) status = lv.scal[l]->status;
+    double dt0 = 1.0e100;
+    long long nf = 1;
+    for (int l = 0; l < lv.nl; ++l) {
+        const double ms = __longlong_as_double((long long)lv.scal[l]->ws_bits);
+        double e = 1.0e20;
+        for (int d = 0; d < lv.D; ++d) {
+            const double x = lv.dx[l][d] / ms;
+            e = (x < e) ? x : e;
+        }
+        e = e * lv.cfl[l];
+        if (!isfinite(e) || !(e > 0.0)) status = status ? status : 3; /* BAMREX_ERR_NAN */
+        if (l > 0) nf *= lv.ratio;
+        const double c = (double)nf * e;
+        dt0 = (c < dt0) ? c : dt0;
+    }
+    const double eps = 0.001 * dt0;
+    if (a->stop_time >= 0.0 && (a->time + dt0) > (a->stop_time - eps)) dt0 = a->stop_time - a->time;
+    if (!(dt0 > 0.0) || !isfinite(dt0)) status = status ? status : 3;
+    nf = 1;
+    for (int l = 0; l < lv.nl; ++l) {
+        if (l > 0) nf *= lv.ratio;
+        a->dt[l] = dt0 / (double)nf;
+        lv.scal[l]->dt = a->dt[l];
+        lv.scal[l]->done = 0;
+    }
+    a->t_sub[0] = a->time;
+    a->dt0 = dt0;
+    a->status = status;
+}
+
+__global__ void amr_substep_kernel(AmrDev* a, int l, int i)
+{
+    a->t_sub[l] = a->t_sub[l - 1] + (double)i * a->dt[l];
+}
+
 }  // namespace
+
+cudaError_t launch_amr_dt(AmrDev* a, const AmrLevelsArg& lv, cudaStream_t s)
+{
+    amr_dt_kernel<<<1, 1, 0, s>>>(a, lv);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_amr_substep(AmrDev* a, int l, int i, cudaStream_t s)
+{
+    amr_substep_kernel<<<1, 1, 0, s>>>(a, l, i);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_cf_gather(bool fp32, const CfGatherArgs& a, cudaStream_t s)
 {

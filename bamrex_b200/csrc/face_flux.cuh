@@ -18,13 +18,22 @@ constexpr int kRegThreads = 128;
 template <typename T, int D, int DIR, int METHOD, int LIM>
 __global__ void __launch_bounds__(kRegThreads) register_faces_kernel(const FabDev* __restrict__ fabs, const RegisterTask t,
                                                                      const Consts kc, double dt, double dx,
-                                                                     double scale)
+                                                                     double scale, const StepScalars* scal,
+                                                                     double area1, double area2)
 {
     using S = Scheme<T, D, DIR, METHOD, LIM>;
     constexpr int NC = D + 2;
     const int slot = blockIdx.x * blockDim.x + threadIdx.x;
     if (slot >= t.nslots) return;
     const K<T> k(kc);
+    if (scal) {
+        // dt on the device: the sweep's own, and the face scale as the host
+        // forms it (dt times the other directions' spacings, in order)
+        if (scal->done) return;
+        dt = scal->dt;
+        scale = dt * area1;
+        scale = scale * area2;
+    }
     // the sweep kernels' step factors (sweep.cuh, step_factors)
     const T hdtdx = (T)(0.5 * dt / dx);
     const T half_dx_dt = (T)(0.5 * dx / dt);

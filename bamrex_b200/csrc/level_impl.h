@@ -177,8 +177,11 @@ int level_fill(bamrex_level* L, int d, int parity, const StepScalars* scal);
 int level_sweep(bamrex_level* L, int d, int parity, double dt_host, const StepScalars* scal, bool reduce_ws,
                 bool allow_timing);
 // One split step starting from buffer `parity`; the result lands in
-// parity ^ (D & 1).  dt from the host (scal == nullptr) or from the device.
-int level_step(bamrex_level* L, int parity, double dt_host, StepScalars* scal, bool allow_timing);
+// parity ^ (D & 1).  dt from the host (scal == nullptr) or from the device;
+// next_dt (device dt only): end the step with the level's own next dt
+// (time, step count, CFL estimate); off inside a hierarchy's coarse step,
+// whose levels keep the dt the hierarchy gave them.
+int level_step(bamrex_level* L, int parity, double dt_host, StepScalars* scal, bool allow_timing, bool next_dt = true);
 // The rigid-body ghost fill of buffer `parity` (gfm.cu); gate: the step
 // scalars whose `done` flag skips the work in device-stepped runs.
 int body_fill(bamrex_level* L, int parity, const StepScalars* gate);
@@ -188,7 +191,7 @@ void body_destroy(bamrex_level* L);
 // faces of a register task (face_flux.cu).
 cudaError_t launch_register_faces(int D, int dir, int method, bool fp32, const Consts& k, const FabDev* in,
                                   const RegisterTask& t, int NC, double dt, double dx_dir, double scale,
-                                  cudaStream_t s);
+                                  const StepScalars* scal, double area1, double area2, cudaStream_t s);
 
 // The preconditioner network (precnet.cu) on device buffers: its input
 // buffer (batch x 2 x ny x nx floats), output buffer (batch x ny x nx),

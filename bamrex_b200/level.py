@@ -303,7 +303,7 @@ class Level:
         self.sync()
         return self.packing.unpack(packed)
 
-    def step_host_ptr(self, in_ptr: int, out_ptr: int, dt: float, nslabs: int = 16) -> float:
+    def step_host_ptr(self, in_ptr: int, out_ptr: int, dt: float, nslabs: int = 0) -> float:
         """One step of a host-resident packed state (bamrex_level_step_host):
         uploads, sweeps and downloads overlap in slabs.  Returns the CFL time
         step estimate of the result."""
@@ -312,13 +312,20 @@ class Level:
                                               int(nslabs), ctypes.byref(nxt)))
         return nxt.value
 
-    def run_host_ptr(self, ptr: int, nsteps: int, dt0: float, time: float = 0.0, nslabs: int = 16):
+    def run_host_ptr(self, ptr: int, nsteps: int, dt0: float, time: float = 0.0, nslabs: int = 0):
         """nsteps host round-trip steps of the packed state at ptr, in place
         (bamrex_level_run_host).  Returns (time, next dt)."""
         t, nxt = ctypes.c_double(time), ctypes.c_double()
         self._ck(lib().bamrex_level_run_host(self._h, ctypes.c_void_p(ptr), int(nsteps), float(dt0), int(nslabs),
                                              ctypes.byref(t), ctypes.byref(nxt)))
         return t.value, nxt.value
+
+    def host_slabs(self, nslabs: int = 0) -> int:
+        """Slabs the host steps stream this level in for nslabs (0: not
+        streamed; bamrex_level_host_slabs)."""
+        n = ctypes.c_int()
+        self._ck(lib().bamrex_level_host_slabs(self._h, int(nslabs), ctypes.byref(n)))
+        return n.value
 
     def sync(self):
         self._ck(lib().bamrex_level_sync(self._h))

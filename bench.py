@@ -44,7 +44,7 @@ def parse_args():
     ap.add_argument("--max-grid-size", type=int, default=0, help="box size (0: one box per rank)")
     ap.add_argument("--graph", type=int, default=0, help="1: time the CUDA-graph replay instead")
     ap.add_argument("--e2e-steps", type=int, default=10)
-    ap.add_argument("--e2e-slabs", type=int, default=24, help="slabs of the streamed host steps")
+    ap.add_argument("--e2e-slabs", type=int, default=0, help="slabs of the streamed host steps (0: the library picks)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp32", action="store_true", help="skip the FP32-storage variant")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
@@ -454,6 +454,23 @@ def amr_blast_run(n0, coarse_steps, precision, regrid_steps=None):
     s0 = A.conserved_sums()
     # stepping alone (fixed grids), then with a regrid every 2 coarse steps
     A.set_regrid_int(0)
+    # the host-driven coarse step (every launch from the host, dt read back
+    # per level) for comparison, then the graph-replayed one (warmed up: the
+    # first step after a change of the levels is host-driven, the next two
+    # capture the graphs of the two buffer states of the 3D base level)
+    n_host = min(20, coarse_steps)
+    A.set_graph(False)
+    A.coarse_step()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(n_host):
+        A.coarse_step()
+    torch.cuda.synchronize()
+    dt_host = time.perf_counter() - t0
+    A.set_graph(True)
+    for _ in range(3):
+        A.coarse_step()
+    caps0, reps0, _ = A.graph_stats()
     torch.cuda.synchronize()
     # an NVTX range lets a profiler capture exactly these steps
     # (ncu --nvtx --nvtx-include "amr_fixed_steps_fp64/")
@@ -464,6 +481,7 @@ def amr_blast_run(n0, coarse_steps, precision, regrid_steps=None):
     torch.cuda.synchronize()
     dt_fixed = time.perf_counter() - t0
     torch.cuda.nvtx.range_pop()
+    caps1, reps1, kernels = A.graph_stats()
     s1 = A.conserved_sums()
     kinds = [[A.level(lev).staging(d) for d in range(3)] for lev in range(A.finest_level + 1)]
     A.set_regrid_int(2)
@@ -477,6 +495,14 @@ def amr_blast_run(n0, coarse_steps, precision, regrid_steps=None):
     return {"cells_per_level": cells, "boxes_per_level": nboxes, "coarse_steps": coarse_steps,
             "ms_per_coarse_step": dt_fixed / coarse_steps * 1e3,
             "cell_updates_per_s": updates_per_step * coarse_steps / dt_fixed,
+            "coarse_step_graph": {
+                "replayed_steps": reps1 - reps0, "captures_in_timed_steps": caps1 - caps0,
+                "kernel_nodes_per_graph": kernels,
+                "launches_per_coarse_step": (len(cells) - 1) + 2,
+                "launches_note": "per coarse step: the max wave speed of each level but the finest (its own comes "
+                                 "fused with its last sweep), the device dt kernel, one graph launch",
+                "host_driven_ms_per_coarse_step": dt_host / n_host * 1e3,
+                "host_driven_kernel_launches_per_coarse_step": kernels + (len(cells) - 1)},
             "sweep_kernels_per_level": [",".join(KIND_NAMES[k] for k in kk) for kk in kinds],
             "coarse_steps_with_regrid": nr,
             "ms_per_coarse_step_with_regrid_every_2": dt_regrid / nr * 1e3,
@@ -656,6 +682,7 @@ def run_ours(args, rank, world, local_rank):
     # one untimed step: the host step's streams, events and output staging
     # are created on first use
     lev.run_host_ptr(hptr, 1, dt, 0.0, args.e2e_slabs)
+    e2e_slabs = lev.host_slabs(args.e2e_slabs)
     host.numpy()[:] = pk.pack(u0)
     if dist:
         dist.barrier()
@@ -675,6 +702,37 @@ def run_ours(args, rank, world, local_rank):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_ms = float(t.item())
     clocks.stop()
+    # the copy roof of that path on this host: one state-sized pinned upload
+    # and download at once (two streams), best of 3
+    pcie = None
+    if rank == 0:
+        e2e_bytes = 8 * pk.size
+        dev_buf = torch.empty(pk.size, dtype=torch.float64, device="cuda")
+        host_dn = torch.empty(pk.size, dtype=torch.float64, pin_memory=True)
+        s_up, s_dn = torch.cuda.Stream(), torch.cuda.Stream()
+        dev_src = torch.zeros(pk.size, dtype=torch.float64, device="cuda")
+        best = 1e30
+        for _ in range(3):
+            torch.cuda.synchronize()
+            c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            c0.record()
+            s_up.wait_stream(torch.cuda.current_stream())
+            s_dn.wait_stream(torch.cuda.current_stream())
+            with torch.cuda.stream(s_up):
+                dev_buf.copy_(host, non_blocking=True)
+            with torch.cuda.stream(s_dn):
+                host_dn.copy_(dev_src, non_blocking=True)
+            torch.cuda.current_stream().wait_stream(s_up)
+            torch.cuda.current_stream().wait_stream(s_dn)
+            c1.record()
+            torch.cuda.synchronize()
+            best = min(best, c0.elapsed_time(c1))
+        roof_gbs = 2 * e2e_bytes / (best * 1e-3) / 1e9
+        got_gbs = 2 * e2e_bytes * args.e2e_steps / (e2e_ms * 1e-3) / 1e9
+        pcie = {"bidirectional_copy_GBps": roof_gbs, "achieved_GBps": got_gbs, "frac": got_gbs / roof_gbs,
+                "how": "one %d-byte pinned host->device and device->host copy at once on two streams, best of 3; "
+                       "achieved = (h2d + d2h bytes) x steps / e2e time" % e2e_bytes}
+        del dev_buf, host_dn, dev_src
     # parity of the timed level itself (its kernels and segments) against
     # the oracle, one step from the initial state and one from the state the
     # timed steps reached
@@ -794,8 +852,9 @@ def run_ours(args, rank, world, local_rank):
                 "d2h_bytes_per_step": state_bytes + 8,
                 "path": "bamrex_level_run_host: every step the whole state host -> device and device -> host "
                         "(pinned), %d slabs streamed (uploads, sweeps, downloads overlapped within and across "
-                        "steps), dt from the CFL estimate on the device" % args.e2e_slabs,
-                "steps": args.e2e_steps},
+                        "steps; one strided copy per slab and direction), dt from the CFL estimate on the device"
+                        % e2e_slabs,
+                "steps": args.e2e_steps, "pcie_roof": pcie},
         "gpu_launches": launches,
         "clocks": clocks.summary(t_wall0, t_wall1),
         "fp32_storage": fp32,

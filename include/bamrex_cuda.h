@@ -300,7 +300,10 @@ BAMREX_API int bamrex_conserved_sums_noalloc(int spacedim, const bamrex_box *box
  * est_time_step.  Single-box levels (2D/3D, not periodic in the last
  * direction) are streamed in nslabs slabs along the last direction so that
  * uploads, sweeps and downloads overlap (pinned host buffers for the
- * overlap); other levels take the plain sequence.  Synchronous. */
+ * overlap; one strided copy per slab and direction); nslabs <= 0 picks slabs
+ * of at least 16 MiB per component (2 to 64 of them), since smaller copies
+ * lose PCIe bandwidth when both directions run at once.  Other levels take
+ * the plain sequence.  Synchronous. */
 BAMREX_API int bamrex_level_step_host(bamrex_level *level, const double *host_in, double *host_out, double dt,
                                       int nslabs, double *dt_next);
 /* nsteps steps of a host-resident state in place (host: packed layout),
@@ -313,6 +316,11 @@ BAMREX_API int bamrex_level_step_host(bamrex_level *level, const double *host_in
  * step after the other.  Synchronous. */
 BAMREX_API int bamrex_level_run_host(bamrex_level *level, double *host, int nsteps, double dt0, int nslabs,
                                      double *time_io, double *dt_next);
+/* The number of slabs bamrex_level_step_host / bamrex_level_run_host stream
+ * the level in for this nslabs (0: the level is not streamed and takes the
+ * plain sequence).  No reference counterpart: the reference keeps its state
+ * on the host and has no host round trip to schedule. */
+BAMREX_API int bamrex_level_host_slabs(const bamrex_level *level, int nslabs, int *slabs);
 BAMREX_API int bamrex_level_sync(bamrex_level *level);
 
 /* bamrexBCData::fill_consv_boundary on the current state
@@ -611,6 +619,21 @@ BAMREX_API int bamrex_amr_avg_down_all(bamrex_amr *amr);
  * first when regrid_int divides the coarse steps taken.  *time_io is the time
  * on entry and the new time on return; *dt_out the coarse dt taken. */
 BAMREX_API int bamrex_amr_coarse_step(bamrex_amr *amr, double stop_time, double *time_io, double *dt_out);
+/* Coarse steps as CUDA graphs (default on).  Once the levels have taken a
+ * coarse step as they are, and when regrids are at least 4 coarse steps
+ * apart (or never come), a coarse step without a regrid runs as: the stale
+ * levels' max wave speeds, the coarse dt computed on the device (the same
+ * operations as the host path, so the same dt bit for bit) and read back,
+ * then the whole subcycled recursion (coarse/fine fills with their time
+ * weights taken from device times, every level's sweeps and flux
+ * registers with their dt read on the device, reflux, average_down) as one
+ * graph replay, captured once per state of the levels' buffers.  The
+ * result equals the host-driven step bit for bit.  No reference
+ * counterpart: the reference steps its levels from the host. */
+BAMREX_API int bamrex_amr_set_graph(bamrex_amr *amr, int use_graph);
+/* Graphs captured, coarse steps replayed, and kernel nodes in the current
+ * levels' graph (any pointer may be NULL). */
+BAMREX_API int bamrex_amr_graph_stats(const bamrex_amr *amr, int *captures, long long *replays, long long *kernels);
 /* Change amr.regrid_int (0: no more regrids). */
 BAMREX_API int bamrex_amr_set_regrid_int(bamrex_amr *amr, int regrid_int);
 /* A static rigid body on every level of the hierarchy, present and future

@@ -213,6 +213,22 @@ class AmrDesc(ctypes.Structure):
         ("phierr_var_is_primv", ctypes.c_int),
         ("phierr", ctypes.c_double * MAX_LEVELS),
         ("max_phierr_lev", ctypes.c_int),
+        ("max_int_lev", ctypes.c_int),
+        ("lstol", ctypes.c_double * MAX_LEVELS),
+        ("max_box_lev", ctypes.c_int),
+        ("box_lo", ctypes.c_double * 3),
+        ("box_hi", ctypes.c_double * 3),
+    ]
+
+
+class TagDesc(ctypes.Structure):
+    _fields_ = [
+        ("do_err", ctypes.c_int), ("err_var", ctypes.c_int), ("err_var_is_primv", ctypes.c_int),
+        ("phierr", ctypes.c_double),
+        ("do_grad", ctypes.c_int), ("grad_var", ctypes.c_int), ("grad_var_is_primv", ctypes.c_int),
+        ("phigrad", ctypes.c_double),
+        ("do_box", ctypes.c_int), ("box_lo", ctypes.c_double * 3), ("box_hi", ctypes.c_double * 3),
+        ("do_interface", ctypes.c_int), ("lstol", ctypes.c_double),
     ]
 
 
@@ -290,6 +306,7 @@ SIGNATURES = {
     "bamrex_level_body_field": (_i, [_vp, _i, _dp]),
     "bamrex_level_body_counts": (_i, [_vp, ctypes.POINTER(_ll), ctypes.POINTER(_ll)]),
     "bamrex_level_tag": (_i, [_vp, _i, _i, _d, _i, _i, _i, _d, ctypes.c_char_p]),
+    "bamrex_level_tag_ex": (_i, [_vp, _vp, ctypes.c_char_p]),
     "bamrex_coupling_create": (_i, [ctypes.POINTER(_vp), _vp, _vp, _i]),
     "bamrex_coupling_destroy": (_i, [_vp]),
     "bamrex_coupling_save_coarse_old": (_i, [_vp, _d, _d]),

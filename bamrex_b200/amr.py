@@ -97,7 +97,8 @@ class Amr:
                  cfl=0.9, ngrow=2, bc_lo=None, bc_hi=None, precision=_abi.FP64, max_level=1, ref_ratio=2,
                  blocking_factor=8, max_grid_size=32, n_error_buf=2, n_proper=1, grid_eff=0.7, regrid_int=0,
                  do_reflux=True, phigrad=None, phigrad_var=0, phigrad_var_is_primv=False, phierr=None, phierr_var=0,
-                 phierr_var_is_primv=False, stream=None):
+                 phierr_var_is_primv=False, max_int_lev=-1, lstol=None, max_box_lev=-1, refine_box=None,
+                 stream=None):
         self.D = spacedim
         self.parm, self.method, self.cfl, self.precision = parm, method, cfl, precision
         self.ratio = ref_ratio
@@ -146,6 +147,16 @@ class Amr:
         for i, v in enumerate(phierr[:_abi.MAX_LEVELS]):
             d.phierr[i] = v
         d.max_phierr_lev = len(phierr)
+        # interface tagging (tagging.max_int_lev / lstol) and box tagging
+        # (tagging.max_box_lev / box_x, box_y, box_z as refine_box = (lo, hi))
+        d.max_int_lev = int(max_int_lev)
+        for i, v in enumerate(list(lstol or [])[:_abi.MAX_LEVELS]):
+            d.lstol[i] = v
+        d.max_box_lev = int(max_box_lev)
+        if refine_box is not None:
+            for q in range(3):
+                d.box_lo[q] = float(refine_box[0][q]) if q < len(refine_box[0]) else 0.0
+                d.box_hi[q] = float(refine_box[1][q]) if q < len(refine_box[1]) else 0.0
         self._desc = d
         self._h = ctypes.c_void_p()
         st = ctypes.c_void_p(stream.cuda_stream) if stream is not None else None

@@ -897,23 +897,34 @@ extern "C" int bamrex_coupling_register(bamrex_coupling* C, int dir, double* reg
     return BAMREX_OK;
 }
 
-extern "C" int bamrex_level_tag(bamrex_level* L, int grad_var, int grad_var_is_primv, double grad_threshold,
-                                int do_err, int err_var, int err_var_is_primv, double phierr, char* tags)
+static int level_tag_spec(bamrex_level* L, const bamrex_tag_desc& t, char* tags)
 {
     if (!L || !tags) return fail(BAMREX_ERR_ARG, "NULL argument");
-    const bool do_grad = grad_threshold > 0;
-    if ((do_grad && (grad_var < 0 || grad_var >= L->NC)) || (do_err && (err_var < 0 || err_var >= L->NC)))
+    const bool do_grad = t.do_grad && t.phigrad > 0;
+    if ((do_grad && (t.grad_var < 0 || t.grad_var >= L->NC)) || (t.do_err && (t.err_var < 0 || t.err_var >= L->NC)))
         return L->set_err(fail(BAMREX_ERR_ARG, "tagging variable index outside the state vector"));
     for (int d = 0; d < L->D; ++d) BX_TRY(level_fill(L, d, L->cur, nullptr));
     TagSpec spec;
-    spec.do_err = do_err ? 1 : 0;
-    spec.err_var = err_var;
-    spec.err_primv = err_var_is_primv ? 1 : 0;
-    spec.err_thr = phierr;
+    std::memset(&spec, 0, sizeof(spec));
+    spec.do_err = t.do_err ? 1 : 0;
+    spec.err_var = t.err_var;
+    spec.err_primv = t.err_var_is_primv ? 1 : 0;
+    spec.err_thr = t.phierr;
     spec.do_grad = do_grad ? 1 : 0;
-    spec.grad_var = grad_var;
-    spec.grad_primv = grad_var_is_primv ? 1 : 0;
-    spec.grad_thr = grad_threshold;
+    spec.grad_var = t.grad_var;
+    spec.grad_primv = t.grad_var_is_primv ? 1 : 0;
+    spec.grad_thr = t.phigrad;
+    spec.do_box = t.do_box ? 1 : 0;
+    for (int d = 0; d < 3; ++d) {
+        spec.box_lo[d] = t.box_lo[d];
+        spec.box_hi[d] = t.box_hi[d];
+        spec.dx[d] = L->dx[d];
+        spec.prob_lo[d] = L->prob_lo[d];
+    }
+    if (body_tag_tables(L, &spec.ls_tab, &spec.flag_tab)) {
+        spec.do_iface = t.do_interface ? 1 : 0;
+        spec.lstol = t.lstol;
+    }
     if (!L->tag_buf) {
         const cudaError_t ea = dev_alloc((void**)&L->tag_buf, (size_t)std::max(1LL, L->ncells), L->stream);
         if (ea != cudaSuccess) return L->set_err(cuda_fail(ea, "tag buffer allocation"));
@@ -926,6 +937,28 @@ extern "C" int bamrex_level_tag(bamrex_level* L, int grad_var, int grad_var_is_p
     if (e == cudaSuccess) e = cudaStreamSynchronize(L->stream);
     if (e != cudaSuccess) return L->set_err(cuda_fail(e, "tag readback"));
     return BAMREX_OK;
+}
+
+extern "C" int bamrex_level_tag(bamrex_level* L, int grad_var, int grad_var_is_primv, double grad_threshold,
+                                int do_err, int err_var, int err_var_is_primv, double phierr, char* tags)
+{
+    bamrex_tag_desc t;
+    std::memset(&t, 0, sizeof(t));
+    t.do_grad = grad_threshold > 0;
+    t.grad_var = grad_var;
+    t.grad_var_is_primv = grad_var_is_primv;
+    t.phigrad = grad_threshold;
+    t.do_err = do_err;
+    t.err_var = err_var;
+    t.err_var_is_primv = err_var_is_primv;
+    t.phierr = phierr;
+    return level_tag_spec(L, t, tags);
+}
+
+extern "C" int bamrex_level_tag_ex(bamrex_level* L, const bamrex_tag_desc* desc, char* tags)
+{
+    if (!desc) return fail(BAMREX_ERR_ARG, "NULL argument");
+    return level_tag_spec(L, *desc, tags);
 }
 
 // ======================================================================
@@ -1522,11 +1555,25 @@ int level_tags(bamrex_amr* A, int l, double time, std::vector<char>& tags)
     bamrex_level* L = A->levels[l];
     if (l > 0) AMR_TRY(A, bamrex_coupling_fill_patch(A->cpl[l], time));
     const bamrex_amr_desc& d = A->desc;
-    const double gthr = l < d.max_phigrad_lev ? d.phigrad[l] : 0.0;
-    const int do_err = l < d.max_phierr_lev ? 1 : 0;
+    bamrex_tag_desc t;
+    std::memset(&t, 0, sizeof(t));
+    t.do_grad = l < d.max_phigrad_lev;
+    t.phigrad = t.do_grad ? d.phigrad[l] : 0.0;
+    t.grad_var = d.phigrad_var;
+    t.grad_var_is_primv = d.phigrad_var_is_primv;
+    t.do_err = l < d.max_phierr_lev;
+    t.phierr = t.do_err ? d.phierr[l] : 0.0;
+    t.err_var = d.phierr_var;
+    t.err_var_is_primv = d.phierr_var_is_primv;
+    t.do_box = l < d.max_box_lev;
+    for (int q = 0; q < 3; ++q) {
+        t.box_lo[q] = d.box_lo[q];
+        t.box_hi[q] = d.box_hi[q];
+    }
+    t.do_interface = A->has_body && l < d.max_int_lev;
+    t.lstol = (t.do_interface && l < BAMREX_MAX_LEVELS) ? d.lstol[l] : 0.0;
     tags.assign((size_t)L->ncells, 0);
-    AMR_TRY(A, bamrex_level_tag(L, d.phigrad_var, d.phigrad_var_is_primv, gthr, do_err, d.phierr_var, d.phierr_var_is_primv,
-                                do_err ? d.phierr[l] : 0.0, tags.data()));
+    AMR_TRY(A, bamrex_level_tag_ex(L, &t, tags.data()));
     return BAMREX_OK;
 }
 

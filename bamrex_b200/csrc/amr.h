@@ -152,10 +152,21 @@ struct TagSpec {
     int do_err, err_var, err_primv;
     int do_grad, grad_var, grad_primv;
     double err_thr, grad_thr;
+    // box_error: cell centres (i + 1/2) dx + prob_lo inside [box_lo, box_hi]
+    int do_box;
+    double box_lo[3], box_hi[3], dx[3], prob_lo[3];
+    // a rigid body's level set (component 0 of its fabs) and GFM flags (one
+    // byte per cell), per box; flag_tab non-null: ghost_error clears solid
+    // cells not at the interface; do_iface: interface_error with lstol
+    const FabDev* ls_tab;
+    const FabDev* flag_tab;
+    int do_iface;
+    double lstol;
 };
 
-// grad_error / state_error tagging (Source/Src_K/tagging_K.H:9-60) over the
-// valid cells of a level, tags (0/1) in the packed cell order.
+// errorEst tagging (Source/Src_K/tagging_K.H:9-105: state_error,
+// grad_error, box_error, interface_error, then ghost_error) over the valid
+// cells of a level, tags (0/1) in the packed cell order.
 cudaError_t launch_tag(int D, bool fp32, const FabDev* fabs, const PackBox* boxes, int nboxes, long long ncells,
                        const Consts& k, const TagSpec& spec, char* tags, cudaStream_t s);
 

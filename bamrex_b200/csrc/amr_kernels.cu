@@ -301,6 +301,27 @@ __global__ void tag_kernel(const FabDev* __restrict__ fab_tab, const PackBox* __
             }
             if (fmax(ax, fmax(ay, az)) >= spec.grad_thr * fmax(fabs(v), 1e-14)) t = 1;
         }
+        // box_error (tagging_K.H:87-103)
+        if (spec.do_box) {
+            const int ijk[3] = { i, j, k };
+            bool in = true;
+            for (int d = 0; d < D; ++d) {
+                const double p = (ijk[d] + 0.5) * spec.dx[d] + spec.prob_lo[d];
+                in = in && spec.box_lo[d] <= p && p <= spec.box_hi[d];
+            }
+            if (in) t = 1;
+        }
+        if (spec.flag_tab) {
+            const FabDev& ff = spec.flag_tab[b];
+            const int fl = ((const unsigned char*)ff.p)[fidx(ff, i, j, k)];
+            // interface_error (tagging_K.H:62-72)
+            if (spec.do_iface) {
+                const FabDev& lf = spec.ls_tab[b];
+                if ((fl & BAMREX_GFM_INTERFACE) || fabs(lf.ptr<double>()[fidx(lf, i, j, k)]) <= spec.lstol) t = 1;
+            }
+            // ghost_error (tagging_K.H:74-84)
+            if ((fl & BAMREX_GFM_GHOST) && !(fl & BAMREX_GFM_INTERFACE)) t = 0;
+        }
         tags[c] = t;
     }
 }

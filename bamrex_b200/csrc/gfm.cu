@@ -1006,10 +1006,15 @@ Sdf make_sdf(const bamrex_sdf& s)
 
 int body_launch(bamrex_level* L, cudaError_t e, const char* what) { return level_launch(L, e, what); }
 
+// The dynamic shared-memory limit of the sweep kernel: a property of the
+// kernel, shared by every level that uses it, so it is raised to the most
+// any level may ask (kSmemMax) rather than to this level's need (a level
+// set up later with a smaller region must not lower it under another's).
 template <int K>
 cudaError_t smem_attribute(bool fp32, int D, int bytes)
 {
     if (bytes <= 48 * 1024) return cudaSuccess;
+    bytes = kSmemMax;
     const cudaFuncAttribute a = cudaFuncAttributeMaxDynamicSharedMemorySize;
     if (fp32) {
         if (D == 1) return cudaFuncSetAttribute(extrap_smem_kernel<float, 1, K>, a, bytes);
@@ -1035,6 +1040,14 @@ dim3 box_grid(const bamrex_level* L, long long max_cells)
 }
 
 }  // namespace
+
+bool body_tag_tables(const bamrex_level* L, const FabDev** ls_tab, const FabDev** flag_tab)
+{
+    if (!L->body) return false;
+    *ls_tab = L->body->d_ls_fab;
+    *flag_tab = L->body->d_flag_fab;
+    return true;
+}
 
 void body_destroy(bamrex_level* L)
 {

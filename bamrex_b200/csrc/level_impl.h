@@ -186,6 +186,9 @@ int level_step(bamrex_level* L, int parity, double dt_host, StepScalars* scal, b
 // scalars whose `done` flag skips the work in device-stepped runs.
 int body_fill(bamrex_level* L, int parity, const StepScalars* gate);
 void body_destroy(bamrex_level* L);
+// The rigid body's level-set and GFM-flag fab tables (device), or false
+// when the level has no body.
+bool body_tag_tables(const bamrex_level* L, const FabDev** ls_tab, const FabDev** flag_tab);
 
 // Face fluxes of direction `dir` recomputed from the sweep input `in` at the
 // faces of a register task (face_flux.cu).

@@ -345,6 +345,10 @@ class Settings:
     phigrad: list = field(default_factory=list)
     phigrad_var: int = 0
     phigrad_var_is_primv: bool = False
+    max_int_lev: int = -1
+    lstol: list = field(default_factory=list)
+    max_box_lev: int = -1
+    refine_box: tuple | None = None
     # ls.* (SDF::make_sdf): shapes for bamrex_b200.level.body_desc, or None
     body: dict | None = None
 
@@ -523,9 +527,22 @@ def read_settings(pp: ParmParse, spacedim: int) -> Settings:
 
     # tagging
     tg = pp.sub("tagging")
-    for name in ("max_int_lev", "max_box_lev"):
-        if tg.query(name, int, -1) != -1:
-            raise NotImplementedError("tagging.%s: interface and box tagging are not built" % name)
+    # interface tagging: |level set| <= lstol[lev] or an interface cell
+    # (Tagging_params.cpp:66-71; lstol sized max_int_lev, zeros where the
+    # inputs give fewer values)
+    s.max_int_lev = tg.query("max_int_lev", int, -1)
+    if s.max_int_lev > 0:
+        vals = tg.queryarr("lstol", float, []) or []
+        s.lstol = (list(vals) + [0.0] * s.max_int_lev)[:s.max_int_lev]
+    # box tagging: the box_x / box_y / box_z intervals (Tagging_params.cpp:72-84)
+    s.max_box_lev = tg.query("max_box_lev", int, -1)
+    if s.max_box_lev != -1:
+        lo, hi = [], []
+        for nm in ("box_x", "box_y", "box_z")[:D]:
+            v = tg.getarr(nm, float, n=2)
+            lo.append(v[0])
+            hi.append(v[1])
+        s.refine_box = (lo, hi)
     for kind in ("phierr", "phigrad"):
         max_lev = tg.query("max_%s_lev" % kind, int, -1)
         if max_lev == -1:
@@ -561,7 +578,8 @@ def amr_kwargs(s: Settings, ngrow: int | None = None, precision=_abi.FP64):
                 n_proper=s.n_proper, grid_eff=s.grid_eff, regrid_int=s.regrid_int if s.max_level > 0 else 0,
                 do_reflux=s.do_reflux, phigrad=s.phigrad, phigrad_var=s.phigrad_var,
                 phigrad_var_is_primv=s.phigrad_var_is_primv, phierr=s.phierr, phierr_var=s.phierr_var,
-                phierr_var_is_primv=s.phierr_var_is_primv)
+                phierr_var_is_primv=s.phierr_var_is_primv, max_int_lev=s.max_int_lev, lstol=s.lstol,
+                max_box_lev=s.max_box_lev, refine_box=s.refine_box)
 
 
 def make_amr(s: Settings, initial_data=None, ngrow: int | None = None, precision=_abi.FP64, base_boxes=None):

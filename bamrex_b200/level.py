@@ -362,6 +362,28 @@ class Level:
                                         float(phierr), buf))
         return np.frombuffer(buf.raw, dtype=np.uint8).copy()
 
+    def tag_ex(self, grad_var=0, grad_threshold=0.0, grad_var_is_primv=False, err_var=None, phierr=0.0,
+               err_var_is_primv=False, box=None, lstol=None) -> np.ndarray:
+        """Every errorEst criterion (bamrex_level_tag_ex): as tag, plus
+        box=(lo, hi) in physical coordinates (box_error) and, on a level with
+        a rigid body, lstol (interface_error; None: off); ghost_error clears
+        solid cells away from the interface whenever the level has a body."""
+        t = _abi.TagDesc()
+        t.do_err, t.err_var = (0, 0) if err_var is None else (1, int(err_var))
+        t.err_var_is_primv, t.phierr = 1 if err_var_is_primv else 0, float(phierr)
+        t.do_grad, t.grad_var = (1 if grad_threshold > 0 else 0), int(grad_var)
+        t.grad_var_is_primv, t.phigrad = 1 if grad_var_is_primv else 0, float(grad_threshold)
+        if box is not None:
+            t.do_box = 1
+            for q in range(3):
+                t.box_lo[q] = float(box[0][q]) if q < len(box[0]) else 0.0
+                t.box_hi[q] = float(box[1][q]) if q < len(box[1]) else 0.0
+        if lstol is not None:
+            t.do_interface, t.lstol = 1, float(lstol)
+        buf = ctypes.create_string_buffer(int(self.ncells))
+        self._ck(lib().bamrex_level_tag_ex(self._h, ctypes.byref(t), buf))
+        return np.frombuffer(buf.raw, dtype=np.uint8).copy()
+
     # rigid body by the ghost-fluid method
     def set_body(self, shapes, combine=_abi.SDF_UNION, rb_bc=_abi.RB_REFLECTIVE, stencil=2, fill_diagonals=False):
         """A static rigid body (bamrex_level_set_body).  shapes: one or two

@@ -507,6 +507,26 @@ BAMREX_API int bamrex_level_body_counts(const bamrex_level *level, long long *in
 BAMREX_API int bamrex_level_tag(bamrex_level *level, int grad_var, int grad_var_is_primv, double grad_threshold,
                                 int do_err, int err_var, int err_var_is_primv, double phierr, char *tags);
 
+/* Every criterion of AmrLevelAdv::errorEst (Source/AmrLevelAdv.cpp:711-832):
+ * state_error and grad_error as bamrex_level_tag; box_error
+ * (tagging_K.H:87-103): cells whose centre lies in [box_lo, box_hi] in every
+ * direction; interface_error (tagging_K.H:62-72), on a level with a rigid
+ * body: cells at the interface or with |level set| <= lstol.  On a level
+ * with a rigid body, ghost_error (tagging_K.H:74-84) then clears the tags of
+ * ghost (solid) cells not at the interface, as the reference does whenever
+ * rigid bodies are enabled (bamrex_level_tag does the same). */
+typedef struct bamrex_tag_desc {
+    int do_err, err_var, err_var_is_primv;
+    double phierr;
+    int do_grad, grad_var, grad_var_is_primv;
+    double phigrad;                  /* relative threshold */
+    int do_box;
+    double box_lo[3], box_hi[3];     /* physical coordinates (tagging.box_x/y/z) */
+    int do_interface;
+    double lstol;
+} bamrex_tag_desc;
+BAMREX_API int bamrex_level_tag_ex(bamrex_level *level, const bamrex_tag_desc *desc, char *tags);
+
 /* The coupling of a coarse level and the next finer level (refinement ratio
  * 2 or 4).  It stands for the AMReX pieces the reference calls between two
  * AmrLevelAdv levels: the FluxRegister (FineAdd / CrseInit in
@@ -594,6 +614,10 @@ typedef struct bamrex_amr_desc {
     int phierr_var, phierr_var_is_primv;
     double phierr[BAMREX_MAX_LEVELS];    /* tagging.phierr per level */
     int max_phierr_lev;                  /* tagging.max_phierr_lev */
+    int max_int_lev;                     /* tagging.max_int_lev: interface tagging on levels below it */
+    double lstol[BAMREX_MAX_LEVELS];     /* tagging.lstol per level */
+    int max_box_lev;                     /* tagging.max_box_lev: box tagging on levels below it */
+    double box_lo[3], box_hi[3];         /* tagging.box_x / box_y / box_z */
 } bamrex_amr_desc;
 
 BAMREX_API int bamrex_amr_create(bamrex_amr **out, const bamrex_amr_desc *desc, void *stream);

@@ -397,6 +397,39 @@ def tag_level(lev: OLevel, grad_var=0, grad_threshold=0.0, err_var=None, phierr=
     return np.concatenate(out)
 
 
+def tag_level_extra(tags, boxes, dom_lo, D, dx, prob_lo, box=None, ls=None, flags=None, lstol=None):
+    """The criteria errorEst applies after grad_error / state_error
+    (Source/AmrLevelAdv.cpp:780-830), on packed tags: box_error
+    (Source/Src_K/tagging_K.H:87-103: the cell centre (i + 1/2) dx + prob_lo
+    inside box = (lo, hi) in every direction), interface_error
+    (tagging_K.H:62-72, with lstol: at the interface or |level set| <=
+    lstol) and ghost_error (tagging_K.H:74-84: a ghost cell not at the
+    interface is cleared; whenever there is a body, flags given).  ls and
+    flags are global (nz, ny, nx) arrays of the valid cells (level set,
+    GFM flags: 1 ghost, 2 interface)."""
+    out = np.array(tags, dtype=np.uint8).copy()
+    o = 0
+    for lo, hi in boxes:
+        shp = (hi[2] - lo[2] + 1, hi[1] - lo[1] + 1, hi[0] - lo[0] + 1)
+        m = shp[0] * shp[1] * shp[2]
+        t = out[o:o + m].reshape(shp)
+        if box is not None:
+            inside = np.ones(shp, dtype=bool)
+            for d in range(D):
+                p = (np.arange(lo[d], hi[d] + 1) + 0.5) * dx[d] + prob_lo[d]
+                ok = (box[0][d] <= p) & (p <= box[1][d])
+                inside &= ok.reshape([-1 if q == 2 - d else 1 for q in range(3)])
+            t[inside] = 1
+        if flags is not None:
+            sl = tuple(slice(lo[q] - dom_lo[q], hi[q] - dom_lo[q] + 1) for q in (2, 1, 0))
+            F = flags[sl].astype(np.int64)
+            if lstol is not None:
+                t[((F & 2) != 0) | (np.abs(ls[sl]) <= lstol)] = 1
+            t[((F & 1) != 0) & ((F & 2) == 0)] = 0
+        o += m
+    return out
+
+
 class OAmr:
     """The subcycled hierarchy on oracle levels with fixed grids."""
 

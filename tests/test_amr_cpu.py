@@ -203,3 +203,42 @@ def test_cluster_tags_matches_dense_restatement(seed):
         got = cluster_tags(D, (0, 0, 0), hi, boxes, tags, **kw)
         want = AO.cluster_tags_dense(D, (0, 0, 0), hi, boxes, tags, **kw)
         assert got == want, (D, n, kw)
+
+
+def test_tag_extra_restatement_small_cases():
+    """box_error, interface_error and ghost_error of the restatement on
+    hand-checked cells: the box tags the cells whose centres it contains,
+    |level set| <= lstol and interface flags tag, solid cells away from the
+    interface are cleared even where another criterion tagged them."""
+    import numpy as np
+    from oracle.amr_oracle import tag_level_extra
+    D = 2
+    boxes = [((0, 0, 0), (3, 1, 0)), ((0, 2, 0), (3, 3, 0))]
+    dx = [0.25, 0.25, 1.0]
+    tags = np.zeros(16, dtype=np.uint8)
+    tags[0] = 1  # (0, 0) from another criterion
+    out = tag_level_extra(tags, boxes, (0, 0, 0), D, dx, (0.0, 0.0, 0.0), box=((0.3, 0.3), (0.6, 0.9)))
+    # centres 0.375, 0.625 in x (0.625 > 0.6: out), 0.375 ... 0.875 in y
+    want = np.zeros((4, 4), dtype=np.uint8)
+    want[1:4, 1] = 1
+    got = np.zeros((4, 4), dtype=np.uint8)
+    got[0:2] = out[:8].reshape(2, 4)
+    got[2:4] = out[8:].reshape(2, 4)
+    want[0, 0] = 1
+    np.testing.assert_array_equal(got, want)
+    ls = np.full((1, 4, 4), 1.0)
+    ls[0, 3, 3] = 0.01
+    flags = np.zeros((1, 4, 4), dtype=np.int64)
+    flags[0, 0, 0] = 1          # solid, not at the interface: cleared
+    flags[0, 0, 1] = 1 | 2      # solid at the interface: tagged
+    flags[0, 2, 0] = 2          # fluid at the interface: tagged
+    out = tag_level_extra(tags, boxes, (0, 0, 0), D, dx, (0.0, 0.0, 0.0), ls=ls, flags=flags, lstol=0.05)
+    got = np.zeros((4, 4), dtype=np.uint8)
+    got[0:2] = out[:8].reshape(2, 4)
+    got[2:4] = out[8:].reshape(2, 4)
+    want = np.zeros((4, 4), dtype=np.uint8)
+    want[0, 1] = want[2, 0] = want[3, 3] = 1
+    np.testing.assert_array_equal(got, want)
+    # without lstol only ghost_error applies
+    out = tag_level_extra(np.ones(16, dtype=np.uint8), boxes, (0, 0, 0), D, dx, (0.0, 0.0, 0.0), ls=ls, flags=flags)
+    assert out[0] == 0 and out[1] == 1 and out.sum() == 15

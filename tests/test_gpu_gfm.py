@@ -359,3 +359,98 @@ def test_hierarchy_with_body_matches_oracle(torch_cuda, oracle, D):
             e = float(np.max(np.abs(got[m] - ref[m])) / np.max(np.abs(ref[m])))
             assert e <= 1e-12 * 2 ** l, (s, l, e)
     A.close()
+
+
+@pytest.mark.parametrize("D", [2, 3])
+def test_tagging_with_body_matches_oracle(torch_cuda, oracle, D):
+    """errorEst on a level with a rigid body (bamrex_level_tag_ex): grad_error,
+    box_error and interface_error, then ghost_error clearing the solid cells
+    away from the interface, identical to the restatement
+    (oracle.amr_oracle.tag_level + tag_level_extra on the restated level set
+    and flags); bamrex_level_tag on the same level applies ghost_error."""
+    from oracle import gfm_oracle as G
+    from oracle.amr_oracle import OLevel, tag_level, tag_level_extra
+    n = (48, 48) if D == 2 else (24, 24, 24)
+    nb = 3 if D == 2 else 8
+    lay, lev = _make(oracle, D, n, nb)
+    s, so, comb = _shapes("cylinder" if D == 2 else "sphere")
+    u0 = _flow(D, n, seed=9)
+    lev.set_body(s, combine=comb)
+    lev.set_state(u0)
+    box = ((0.1, 0.6, 0.2), (0.35, 0.9, 0.7))
+    t = lev.tag_ex(grad_var=0, grad_threshold=0.08, box=box, lstol=0.05)
+    t_plain = lev.tag(grad_var=0, grad_threshold=0.08)
+    t_box = lev.tag_ex(box=box)
+    lev.close()
+    boxes = [(_pad(lo), _pad(hi)) for lo, hi in _split(D, n, nb)]
+    dx = [1.0 / n[d] for d in range(D)] + [1.0] * (3 - D)
+    o = OLevel(D, (0, 0, 0), _pad([x - 1 for x in n]), boxes, 2, dx, (0, 0, 0), (0, 0, 0))
+    o.set_dense(u0)
+    o.lay.fill_boundary(o.S)
+    body = G.Body(lay, so, comb, (0.0,) * D)
+    ls, fl = body.field(0), body.field(-1).astype(np.int64)
+    base = tag_level(o, grad_var=0, grad_threshold=0.08)
+    want = tag_level_extra(base, boxes, (0, 0, 0), D, dx, (0.0, 0.0, 0.0), box=box, ls=ls, flags=fl, lstol=0.05)
+    np.testing.assert_array_equal(t, want)
+    np.testing.assert_array_equal(t_plain, tag_level_extra(base, boxes, (0, 0, 0), D, dx, (0.0, 0.0, 0.0), ls=ls,
+                                                           flags=fl))
+    np.testing.assert_array_equal(t_box, tag_level_extra(np.zeros_like(base), boxes, (0, 0, 0), D, dx,
+                                                         (0.0, 0.0, 0.0), box=box, ls=ls, flags=fl))
+    # every criterion decides some cells
+    solid = ((fl & 1) != 0) & ((fl & 2) == 0)
+    assert solid.sum() > 0 and 0 < t.sum() < t.size and t_box.sum() > 0
+    assert t.sum() != t_plain.sum()
+
+
+def test_hierarchy_regrid_around_body(torch_cuda):
+    """Interface tagging drives the regrid of a hierarchy with a rigid body
+    (tagging.max_int_lev / lstol): level 1 covers every level-0 cell at the
+    interface or within lstol of it, and no coarse cell deep in the solid
+    is tagged (ghost_error) - the fine boxes stay near the interface."""
+    import bamrex_b200 as bx
+    from bamrex_b200.amr import Amr
+    D, n = 2, 64
+    hi = (n - 1, n - 1, 0)
+    A = Amr(D, (0, 0, 0), hi, [0.0] * D, [1.0] * D, [((0, 0, 0), hi)], bx.Parm(D), cfl=0.8, ngrow=4, max_level=1,
+            blocking_factor=8, max_grid_size=32, n_error_buf=1, max_int_lev=1, lstol=[0.03])
+    A.set_body(dict(kind=bx.SDF_CYLINDER, center=(0.5, 0.5, 0.0), axis=(0, 0, 1), radius=0.25))
+    A.set_state(0, _flow(D, (n, n), seed=4))
+    A.regrid(0, 0.0)
+    assert A.finest_level == 1
+    ls = A.level(0).body_field(0)[0]
+    fl = A.level(0).body_field(-1)[0].astype(np.int64)
+    covered = np.zeros((n, n), dtype=bool)
+    for lo, hi1 in A.boxes(1):
+        covered[lo[1] // 2:hi1[1] // 2 + 1, lo[0] // 2:hi1[0] // 2 + 1] = True
+    want = ((fl & 2) != 0) | (np.abs(ls) <= 0.03)
+    assert want.sum() > 0 and covered[want].all()
+    # deep in the solid (a disc of radius 0.1 about the centre) nothing is refined
+    x = (np.arange(n) + 0.5) / n
+    X, Y = np.meshgrid(x, x)
+    deep = (X - 0.5) ** 2 + (Y - 0.5) ** 2 < 0.1 ** 2
+    assert not covered[deep].any()
+    A.close()
+
+
+def test_extrapolation_limit_shared_by_levels(torch_cuda, oracle):
+    """Two levels whose rigid-body sweeps need different amounts of shared
+    memory (both above the default 48 KB): setting up the smaller one after
+    the larger must not break the larger one's fill (the limit belongs to
+    the kernel, not to a level); its step equals the step of the same level
+    made alone."""
+    def run(extra):
+        _, a = _make(oracle, 3, (24, 24, 24), 1)
+        s, _, comb = _shapes("big_sphere")
+        a.set_body(s, combine=comb)
+        b = None
+        if extra:
+            _, b = _make(oracle, 3, (20, 20, 20), 1)
+            b.set_body(s, combine=comb)
+        a.set_state(_flow(3, (24, 24, 24), seed=2))
+        a.advance(0.0, 1e-3)
+        got = a.get_state()
+        a.close()
+        if b is not None:
+            b.close()
+        return got
+    np.testing.assert_array_equal(run(True), run(False))

@@ -152,7 +152,7 @@ def test_periodic_geometry_overrides_faces():
     ("limiting.energy = pressure\n", I.InputsError, "Invalid variable name"),
     ("geometry.coord_sys = 1\n", I.InputsError, "coord_sys = 0"),
     ("strt_time = -1\n", I.InputsError, "non-negative strt_time"),
-    ("tagging.max_int_lev = 2\n", NotImplementedError, "max_int_lev"),
+    ("tagging.max_box_lev = 1\ntagging.box_x = 0.1 0.2\n", I.InputsError, "box_y"),
     ("amr.ref_ratio = 4 4\n", NotImplementedError, "ratio 2"),
     ("amr.ref_ratio = 2 4\n", NotImplementedError, "one ratio"),
     ("ls.geom_type = box\n", NotImplementedError, "geom_type = box"),
@@ -219,6 +219,15 @@ def test_amr_arguments():
     body = I.read_settings(_pp(QUADRANT_2D + "ls.geom_type = sphere\nls.sphere_center = 1 0.5 0\n"
                                "ls.sphere_radius = 0.1\nls.sphere_has_fluid_inside = 0\n"), 2)
     assert I.amr_kwargs(body)["ngrow"] == 4
+    # interface and box tagging (Tagging_params.cpp:66-84): lstol padded with
+    # zeros to max_int_lev, the refine box from box_x / box_y
+    tagged = I.read_settings(_pp(QUADRANT_2D + "tagging.max_int_lev = 3\ntagging.lstol = 0.1 0.05\n"
+                                 "tagging.max_box_lev = 1\ntagging.box_x = 0.1 0.4\ntagging.box_y = 0.2 0.3\n"), 2)
+    kw = I.amr_kwargs(tagged)
+    assert kw["max_int_lev"] == 3 and kw["lstol"] == [0.1, 0.05, 0.0]
+    assert kw["max_box_lev"] == 1 and kw["refine_box"] == ([0.1, 0.2], [0.4, 0.3])
+    plain = I.amr_kwargs(s)
+    assert plain["max_int_lev"] == -1 and plain["max_box_lev"] == -1 and plain["refine_box"] is None
 
 
 # ---- the main loop ---------------------------------------------------------

@@ -196,6 +196,15 @@ cudaError_t launch_register_faces(int D, int dir, int method, bool fp32, const C
                                   const RegisterTask& t, int NC, double dt, double dx_dir, double scale,
                                   const StepScalars* scal, double area1, double area2, cudaStream_t s);
 
+// The network's 3x3 convolutions (16 -> 16, 2 -> 16, 16 -> 1) on the
+// tcgen05 tensor cores (conv_tc.cu): NCHW FP32 activations, BF16-rounded
+// weights [co][ci][9] and biases; widths that are multiples of 128.
+// *status is set to BAMREX_ERR_TIMEOUT by a block that gave up waiting
+// for its MMAs.
+bool conv_tc_supported(int cin, int cout, int H, int W);
+cudaError_t launch_conv_tc(int cin, int cout, const float* x, float* y, const float* w, const float* bias, int H, int W,
+                           int batch, int relu, int* status, cudaStream_t s);
+
 // The preconditioner network (precnet.cu) on device buffers: its input
 // buffer (batch x 2 x ny x nx floats), output buffer (batch x ny x nx),
 // size, and a forward pass on stream s.

@@ -331,16 +331,20 @@ __global__ void sum_parts_kernel(const float* __restrict__ part, int nblocks, in
     }
 }
 
+// Forward pool and upsample-add walk rows over blocks and the pixels of a
+// row over threads (one division per row).
 __global__ void pool_fwd_kernel(const float* __restrict__ x, float* __restrict__ y, int c, int H, int W, int batch)
 {
     const int h = H / 2, w = W / 2;
-    const long long total = (long long)batch * c * h * w;
-    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
-        const int i = (int)(t % w), j = (int)((t / w) % h);
-        const long long plane = t / ((long long)h * w);
-        const float* xp = x + plane * H * W;
-        y[t] = 0.25f * (xp[(2 * j) * W + 2 * i] + xp[(2 * j) * W + 2 * i + 1] + xp[(2 * j + 1) * W + 2 * i] +
-                        xp[(2 * j + 1) * W + 2 * i + 1]);
+    const long long rows = (long long)batch * c * h;
+    for (long long row = blockIdx.x; row < rows; row += gridDim.x) {
+        const long long plane = row / h;
+        const int j = (int)(row - plane * h);
+        const float* x0 = x + (plane * H + 2 * j) * (long long)W;
+        const float* x1 = x0 + W;
+        float* yr = y + row * w;
+        for (int i = threadIdx.x; i < w; i += blockDim.x)
+            yr[i] = 0.25f * (x0[2 * i] + x0[2 * i + 1] + x1[2 * i] + x1[2 * i + 1]);
     }
 }
 
@@ -359,12 +363,15 @@ __global__ void pool_bwd_kernel(const float* __restrict__ dy, float* __restrict_
 __global__ void upadd_fwd_kernel(const float* __restrict__ a, const float* __restrict__ s, float* __restrict__ y, int c,
                                  int H, int W, int batch)
 {
-    const long long total = (long long)batch * c * H * W;
     const int h = H / 2, w = W / 2;
-    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
-        const int i = (int)(t % W), j = (int)((t / W) % H);
-        const long long plane = t / ((long long)H * W);
-        y[t] = a[plane * h * w + (j / 2) * w + i / 2] + s[t];
+    const long long rows = (long long)batch * c * H;
+    for (long long row = blockIdx.x; row < rows; row += gridDim.x) {
+        const long long plane = row / H;
+        const int j = (int)(row - plane * H);
+        const float* ar = a + (plane * h + j / 2) * (long long)w;
+        const float* sr = s + row * W;
+        float* yr = y + row * W;
+        for (int i = threadIdx.x; i < W; i += blockDim.x) yr[i] = ar[i / 2] + sr[i];
     }
 }
 
@@ -479,7 +486,11 @@ struct bamrex_precnet {
     size_t act_floats = 0;
     int adam_t = 0;
     bool wb_dirty = true;
-    bool tensor_cores = true;  // inference forward of 16 -> 16 convolutions on the tensor cores
+    // the 16 -> 16 convolutions of inference: 0 FP32 CUDA cores, 1 tensor
+    // cores (tcgen05 where the width is a multiple of 128, mma.sync
+    // elsewhere), 2 mma.sync only
+    int tc_mode = 1;
+    int* d_status = nullptr;   // set by a tcgen05 convolution that gave up waiting
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     std::string err;
@@ -509,6 +520,18 @@ int pck(bamrex_precnet* N, cudaError_t e, const char* what)
         int rc_ = (call);                 \
         if (rc_ != BAMREX_OK) return rc_; \
     } while (0)
+
+// A tcgen05 convolution that gave up waiting for its MMAs leaves a
+// status: reported (and cleared) by the calls that wait for the stream.
+int check_status(bamrex_precnet* N)
+{
+    int st = 0;
+    P_TRY(pck(N, cudaMemcpy(&st, N->d_status, sizeof(int), cudaMemcpyDeviceToHost), "status"));
+    if (!st) return BAMREX_OK;
+    cudaMemset(N->d_status, 0, sizeof(int));
+    return pfail(N, BAMREX_ERR_TIMEOUT, "a tensor-core convolution gave up waiting for its MMAs");
+}
+
 
 void build_graph(bamrex_precnet* N)
 {
@@ -585,9 +608,13 @@ int launch_conv_fwd(bamrex_precnet* N, const Layer& L)
     const long long n = (long long)H * W * N->batch;
     const float* w = N->d_wb + L.w_off;
     const float* b = N->d_wb + L.b_off;
+    if (N->tc_mode == 1 && conv_tc_supported(L.cin, L.cout, H, W))
+        return pck(N, launch_conv_tc(L.cin, L.cout, A(N, L.in), A(N, L.out), w, b, H, W, N->batch, L.relu, N->d_status,
+                                     N->stream),
+                   "conv forward (tcgen05)");
     if (L.cin == 2 && L.cout == C)
         conv_fwd_kernel<2, C><<<gridn(n), kT, 0, N->stream>>>(A(N, L.in), A(N, L.out), w, b, H, W, N->batch, L.relu);
-    else if (L.cin == C && L.cout == C && N->tensor_cores && W % kMmaTW == 0 && H % kMmaTH == 0) {
+    else if (L.cin == C && L.cout == C && N->tc_mode != 0 && W % kMmaTW == 0 && H % kMmaTH == 0) {
         const long long tiles = (long long)N->batch * (W / kMmaTW) * (H / kMmaTH);
         const int grid = (int)std::max(1LL, std::min(tiles, (long long)device_sm_count() * 8));
         conv16_mma_kernel<<<grid, 128, 0, N->stream>>>(A(N, L.in), A(N, L.out), w, b, H, W, N->batch, L.relu);
@@ -697,7 +724,9 @@ extern "C" int bamrex_precnet_create(bamrex_precnet** out, int nx, int ny, int b
         N->own_stream = true;
     }
     const size_t P = (size_t)N->nparams;
-    P_TRY(pck(N.get(), cudaMalloc((void**)&N->d_w, sizeof(float) * P * 5), "parameters"));
+    P_TRY(pck(N.get(), cudaMalloc((void**)&N->d_w, sizeof(float) * (P * 5 + 4)), "parameters"));
+    N->d_status = reinterpret_cast<int*>(N->d_w + 5 * P);
+    P_TRY(pck(N.get(), cudaMemsetAsync(N->d_status, 0, sizeof(int), N->stream), "status"));
     N->d_wb = N->d_w + P;
     N->d_g = N->d_w + 2 * P;
     N->d_m = N->d_w + 3 * P;
@@ -776,7 +805,8 @@ extern "C" int bamrex_precnet_forward(bamrex_precnet* N, const float* in, float*
     P_TRY(forward(N));
     P_TRY(pck(N, cudaMemcpyAsync(out, A(N, (int)N->acts.size() - 1), sizeof(float) * nout, cudaMemcpyDefault, N->stream),
               "output"));
-    return pck(N, cudaStreamSynchronize(N->stream), "sync");
+    P_TRY(pck(N, cudaStreamSynchronize(N->stream), "sync"));
+    return check_status(N);
 }
 
 // Gradient of sum(out * dout) w.r.t. the parameters (after a forward on
@@ -802,10 +832,10 @@ extern "C" int bamrex_precnet_train_step(bamrex_precnet* N, const float* in, con
     const size_t nin = (size_t)N->batch * 2 * HW, nout = (size_t)N->batch * HW;
     P_TRY(pck(N, cudaMemcpyAsync(A(N, 0), in, sizeof(float) * nin, cudaMemcpyDefault, N->stream), "input"));
     P_TRY(pck(N, cudaMemcpyAsync(N->d_tgt, target, sizeof(float) * nout, cudaMemcpyDefault, N->stream), "target"));
-    const bool tc = N->tensor_cores;
-    N->tensor_cores = false;  // the backward differentiates the FP32 forward
+    const int tc = N->tc_mode;
+    N->tc_mode = 0;  // the backward differentiates the FP32 forward
     const int frc = forward(N);
-    N->tensor_cores = tc;
+    N->tc_mode = tc;
     P_TRY(frc);
     const int last = (int)N->acts.size() - 1;
     const int nb = 512;
@@ -857,6 +887,7 @@ int precnet_run(bamrex_precnet* N, cudaStream_t s)
 extern "C" int bamrex_precnet_set_tensor_cores(bamrex_precnet* N, int on)
 {
     if (!N) return fail(BAMREX_ERR_ARG, "NULL network");
-    N->tensor_cores = on != 0;
+    if (on < 0 || on > 2) return pfail(N, BAMREX_ERR_ARG, "tensor-core mode must be 0, 1 or 2");
+    N->tc_mode = on;
     return BAMREX_OK;
 }

@@ -47,7 +47,12 @@ class PrecNet:
         self.nx, self.ny, self.batch = nx, ny, batch
 
     def set_tensor_cores(self, on=True):
-        self._ck(lib().bamrex_precnet_set_tensor_cores(self._h, 1 if on else 0))
+        """Where the 16 -> 16 convolutions of inference run: True / 1 the
+        tensor cores (tcgen05 on levels whose width is a multiple of 128,
+        mma.sync elsewhere), 2 mma.sync only, False / 0 the FP32 CUDA cores
+        (bamrex_precnet_set_tensor_cores)."""
+        mode = int(on) if not isinstance(on, bool) else (1 if on else 0)
+        self._ck(lib().bamrex_precnet_set_tensor_cores(self._h, mode))
 
     def get_weights(self):
         w = np.empty(self.num_params, dtype=np.float32)
@@ -175,16 +180,20 @@ def solve_learned_device(h: Helmholtz, net, x, rhs, tol_rel=1e-8, tol_abs=0.0, m
 
 
 def _main(argv=None):
-    """python -m bamrex_b200.learned [--n N] [--forwards K]: forward passes
-    of the preconditioner network (untrained weights) on an N x N grid."""
+    """python -m bamrex_b200.learned [--n N] [--forwards K] [--mode M]:
+    forward passes of the preconditioner network (untrained weights) on an
+    N x N grid."""
     import argparse
 
     import torch
     ap = argparse.ArgumentParser()
     ap.add_argument("--n", type=int, default=1024)
     ap.add_argument("--forwards", type=int, default=3)
+    ap.add_argument("--mode", type=int, default=1,
+                    help="16 -> 16 convolutions: 1 tensor cores (tcgen05 / mma.sync), 2 mma.sync, 0 FP32 CUDA cores")
     a = ap.parse_args(argv)
     net = PrecNet(a.n, a.n, batch=1, seed=1)
+    net.set_tensor_cores(a.mode)
     inp = np.random.default_rng(0).standard_normal((1, 2, a.n, a.n)).astype(np.float32)
     for k in range(a.forwards):
         t0 = time.perf_counter()

@@ -774,10 +774,13 @@ BAMREX_API int bamrex_precnet_set_weights(bamrex_precnet *net, const float *w);
 BAMREX_API int bamrex_precnet_forward(bamrex_precnet *net, const float *in, float *out);
 /* Parameter gradient of sum(out * dout) after a forward on the same input. */
 BAMREX_API int bamrex_precnet_backward(bamrex_precnet *net, const float *dout, float *grad);
-/* Inference forwards (bamrex_precnet_forward and the learned solve) run the
- * 16-channel convolutions on the tensor cores (BF16 operands, FP32
- * accumulators) when on != 0 (the default) and the level's width is a
- * multiple of 32 and its height of 4; training always uses the FP32 path. */
+/* Where inference forwards (bamrex_precnet_forward and the learned solve)
+ * run the 16 -> 16 channel convolutions: on = 1 (the default) the tensor
+ * cores with BF16 operands and FP32 accumulators -- tcgen05.mma with the
+ * accumulators in tensor memory on levels whose width is a multiple of 128,
+ * mma.sync on the others whose width is a multiple of 32 and height of 4,
+ * the FP32 CUDA cores elsewhere; on = 2 mma.sync only (where it applies);
+ * on = 0 the FP32 CUDA cores.  Training always uses the FP32 path. */
 BAMREX_API int bamrex_precnet_set_tensor_cores(bamrex_precnet *net, int on);
 /* One Adam step on the relative squared error ||out - target||^2 / ||target||^2
  * averaged over the batch; *loss is the value before the step. */

@@ -60,6 +60,33 @@ def test_tensor_core_forward_matches_fp32(torch_cuda):
     net.close()
 
 
+def test_tcgen05_forward_matches_mma_and_fp32(torch_cuda):
+    """The 16 -> 16 convolutions on tcgen05 agree with the FP32 CUDA cores to
+    BF16 rounding.  The network is 1024 wide (every level a multiple of 128,
+    so tcgen05 runs everywhere) and 48 high, so its coarsest level (6 rows)
+    is one mma.sync cannot take: there mma.sync-only mode falls back to the
+    FP32 kernel while tcgen05 runs, and the two modes differ."""
+    from bamrex_b200.learned import PrecNet
+    rng = np.random.default_rng(8)
+    net = PrecNet(1024, 48, batch=2, seed=5)
+    x = rng.standard_normal((2, 2, 48, 1024)).astype(np.float32)
+    outs = {}
+    for mode in (0, 1, 2):
+        net.set_tensor_cores(mode)
+        outs[mode] = net.forward(x)
+        assert np.all(np.isfinite(outs[mode]))
+    ref = np.linalg.norm(outs[0])
+    assert np.linalg.norm(outs[1] - outs[0]) <= 2e-2 * ref
+    assert np.linalg.norm(outs[2] - outs[0]) <= 2e-2 * ref
+    assert not np.array_equal(outs[1], outs[2]) and not np.array_equal(outs[1], outs[0])
+    # repeated forwards give the same result (no state left between calls)
+    net.set_tensor_cores(1)
+    np.testing.assert_array_equal(net.forward(x), outs[1])
+    with pytest.raises(Exception):
+        net.set_tensor_cores(3)
+    net.close()
+
+
 @pytest.fixture(scope="module")
 def trained(torch_cuda):
     """A network trained on 160 pairs from the plain solver at 64^2."""

@@ -22,6 +22,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdint>
 #include <cstring>
 #include <memory>
 #include <new>
@@ -90,17 +91,29 @@ __device__ __forceinline__ double nbr(const double* __restrict__ x, const HLev& 
 
 // y = A x (mode 0) or y = rhs - A x (mode 1), the operator of
 // mlalapgrad_adotx with dhx = B dxinv^2, chdx = C c 0.5 dxinv.
-template <int D>
-__global__ void apply_kernel(const HLev L, const HOp op, const double* __restrict__ x, double* __restrict__ y,
-                             const double* __restrict__ rhs, int mode)
-{
+struct ApplyCoef {
     double dxinv[3], dh[3];
+};
+
+__device__ __forceinline__ ApplyCoef apply_coef(const HLev& L, const HOp& op)
+{
+    ApplyCoef a;
     for (int d = 0; d < 3; ++d) {
-        dxinv[d] = 1.0 / L.dx[d];
-        dh[d] = op.bscal * dxinv[d] * dxinv[d];
+        a.dxinv[d] = 1.0 / L.dx[d];
+        a.dh[d] = op.bscal * a.dxinv[d] * a.dxinv[d];
     }
-    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < L.ncell;
-         c += (long long)gridDim.x * blockDim.x) {
+    return a;
+}
+
+// (A x)_c, or rhs_c - (A x)_c with mode 1.
+template <int D>
+__device__ __forceinline__ double apply_value(const HLev& L, const HOp& op, const ApplyCoef& ac,
+                                              const double* __restrict__ x, const double* __restrict__ rhs, int mode,
+                                              long long c)
+{
+    const double* dxinv = ac.dxinv;
+    const double* dh = ac.dh;
+    {
         const int i = (int)(c % L.n[0]);
         const int j = (int)((c / L.n[0]) % L.n[1]);
         const int k = (int)(c / ((long long)L.n[0] * L.n[1]));
@@ -122,8 +135,18 @@ __global__ void apply_kernel(const HLev L, const HOp op, const double* __restric
                 v = v + chd * (xp[d] - xm[d]);
             }
         }
-        y[c] = mode ? rhs[c] - v : v;
+        return mode ? rhs[c] - v : v;
     }
+}
+
+template <int D>
+__global__ void apply_kernel(const HLev L, const HOp op, const double* __restrict__ x, double* __restrict__ y,
+                             const double* __restrict__ rhs, int mode)
+{
+    const ApplyCoef ac = apply_coef(L, op);
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < L.ncell;
+         c += (long long)gridDim.x * blockDim.x)
+        y[c] = apply_value<D>(L, op, ac, x, rhs, mode, c);
 }
 
 // The Gauss-Seidel update of one cell from its neighbours pm/pp (boundary
@@ -142,21 +165,17 @@ __device__ __forceinline__ GsCoef gs_coef(const HLev& L, const HOp& op)
     return g;
 }
 
+// The update itself from the cell's coefficients (a, the low / high face
+// coefficients bl / bh, the gradient coefficients cc) and neighbours.
 template <int D>
-__device__ __forceinline__ double gsrb_value(const HLev& L, const HOp& op, const GsCoef& gc, long long c, int i, int j,
-                                             int k, double pc, const double (&pm)[3], const double (&pp)[3],
-                                             const double (&cfm)[3], const double (&cfp)[3], double rhs)
+__device__ __forceinline__ double gsrb_core(const HOp& op, const GsCoef& gc, double a, const double (&bl)[3],
+                                            const double (&bh)[3], const double (&cc)[3], double pc,
+                                            const double (&pm)[3], const double (&pp)[3], const double (&cfm)[3],
+                                            const double (&cfp)[3], double rhs)
 {
     const double* dh = gc.dh;
     const double* cdh = gc.cdh;
-    double bl[3], bh[3], cc[3];
-    for (int d = 0; d < D; ++d) {
-        const int ih = i + (d == 0), jh = j + (d == 1), kh = k + (d == 2);
-        bl[d] = L.b[d][fidx(L, d, i, j, k)];
-        bh[d] = L.b[d][fidx(L, d, ih, jh, kh)];
-        cc[d] = L.c ? L.c[(long long)d * L.ncell + c] : 0.0;
-    }
-    double gamma = op.ascal * L.a[c];
+    double gamma = op.ascal * a;
     for (int d = 0; d < D; ++d) gamma = gamma + dh[d] * (bl[d] + bh[d]);
     double delta = dh[0] * (bl[0] * cfm[0] + bh[0] * cfp[0]);
     for (int d = 1; d < D; ++d) delta = delta + dh[d] * (bl[d] * cfm[d] + bh[d] * cfp[d]);
@@ -173,6 +192,21 @@ __device__ __forceinline__ double gsrb_value(const HLev& L, const HOp& op, const
     }
     // MLALapGrad_2D_K.H:205-228
     return (rhs + rho - pc * delta) / (gamma - delta);
+}
+
+template <int D>
+__device__ __forceinline__ double gsrb_value(const HLev& L, const HOp& op, const GsCoef& gc, long long c, int i, int j,
+                                             int k, double pc, const double (&pm)[3], const double (&pp)[3],
+                                             const double (&cfm)[3], const double (&cfp)[3], double rhs)
+{
+    double bl[3], bh[3], cc[3];
+    for (int d = 0; d < D; ++d) {
+        const int ih = i + (d == 0), jh = j + (d == 1), kh = k + (d == 2);
+        bl[d] = L.b[d][fidx(L, d, i, j, k)];
+        bh[d] = L.b[d][fidx(L, d, ih, jh, kh)];
+        cc[d] = L.c ? L.c[(long long)d * L.ncell + c] : 0.0;
+    }
+    return gsrb_core<D>(op, gc, L.a[c], bl, bh, cc, pc, pm, pp, cfm, cfp, rhs);
 }
 
 // One colour of the red-black smoother: cells with (i+j+k+color) even.
@@ -210,86 +244,220 @@ __global__ void gsrb_kernel(const HLev L, const HOp op, double* __restrict__ phi
 // One read and one write of phi per sweep instead of two each.  Requires
 // n0 % 32 == 0 and n1 % 16 == 0.
 constexpr int kGsTX = 32, kGsTY = 16;
+constexpr int kGsSX = kGsTX + 4, kGsSY = kGsTY + 4;   // the tile with a 2-cell halo
 
+// One tile of the fused sweep: sp holds the tile's phi window (2-cell halo)
+// on entry; the coefficients of the red pass (tile + 1-cell ring) and the
+// black pass (tile) come from global memory, or, when sa is non-null, from
+// the staged windows sa / sr / sbx / sby of a, rhs and the x / y face
+// coefficients (same window origin; only for tiles away from the domain
+// boundary, where no boundary condition applies and every neighbour is
+// inside the window).
+__device__ __forceinline__ void gsrb2_tile(const HLev& L, const HOp& op, const GsCoef& gc, double (*sp)[kGsSX],
+                                           const double* __restrict__ rhs, int i0, int j0, const double* sa,
+                                           const double* sr, const double* sbx, const double* sby)
+{
+    for (int pass = 0; pass < 2; ++pass) {
+        // pass 0: red on [-1, TX] x [-1, TY]; pass 1: black on the tile.
+        // Threads take the cells of the pass's colour only: row lj holds
+        // w / 2 of them, at columns of parity (lj + pass + i0 + j0) & 1.
+        const int lo = pass == 0 ? -1 : 0;
+        const int w = kGsTX + (pass == 0 ? 2 : 0), h = kGsTY + (pass == 0 ? 2 : 0);
+        const int wh = w / 2;
+        for (int q = threadIdx.x; q < wh * h; q += blockDim.x) {
+            const int lj = lo + q / wh;
+            const int par = ((i0 + j0 + lj + lo + pass) & 1);  // first column of the colour in this row
+            const int li = lo + 2 * (q % wh) + par;
+            const double pc = sp[lj + 2][li + 2];
+            double pm[3], pp[3], cfm[3] = { 0, 0, 0 }, cfp[3] = { 0, 0, 0 };
+            if (sa) {
+                const int o = (lj + 2) * kGsSX + li + 2;
+                pm[0] = sp[lj + 2][li + 1];
+                pp[0] = sp[lj + 2][li + 3];
+                pm[1] = sp[lj + 1][li + 2];
+                pp[1] = sp[lj + 3][li + 2];
+                const double bl[3] = { sbx[o], sby[o], 0.0 }, bh[3] = { sbx[o + 1], sby[o + kGsSX], 0.0 };
+                const double cc[3] = { 0.0, 0.0, 0.0 };
+                sp[lj + 2][li + 2] = gsrb_core<2>(op, gc, sa[o], bl, bh, cc, pc, pm, pp, cfm, cfp, sr[o]);
+                continue;
+            }
+            const int gi0 = i0 + li, gj0 = j0 + lj;
+            // the cell itself in global indices (a periodic image for halo cells)
+            int gi = gi0, gj = gj0;
+            if (gi < 0 || gi >= L.n[0]) {
+                if (op.bc_lo[0] != BAMREX_LINOP_PERIODIC) continue;
+                gi = gi < 0 ? gi + L.n[0] : gi - L.n[0];
+            }
+            if (gj < 0 || gj >= L.n[1]) {
+                if (op.bc_lo[1] != BAMREX_LINOP_PERIODIC) continue;
+                gj = gj < 0 ? gj + L.n[1] : gj - L.n[1];
+            }
+            const int nn[2] = { L.n[0], L.n[1] };
+            const int g[2] = { gi, gj };
+            for (int d = 0; d < 2; ++d) {
+                const int si = d == 0 ? 1 : 0, sj = d == 1 ? 1 : 0;
+                pm[d] = sp[lj + 2 - sj][li + 2 - si];
+                pp[d] = sp[lj + 2 + sj][li + 2 + si];
+                if (g[d] == 0 && op.bc_lo[d] != BAMREX_LINOP_PERIODIC) {
+                    cfm[d] = op.bc_lo[d] == BAMREX_LINOP_NEUMANN ? 1.0 : -1.0;
+                    pm[d] = cfm[d] * pc;
+                }
+                if (g[d] == nn[d] - 1 && op.bc_hi[d] != BAMREX_LINOP_PERIODIC) {
+                    cfp[d] = op.bc_hi[d] == BAMREX_LINOP_NEUMANN ? 1.0 : -1.0;
+                    pp[d] = cfp[d] * pc;
+                }
+            }
+            const long long c = (long long)gj * L.n[0] + gi;
+            sp[lj + 2][li + 2] = gsrb_value<2>(L, op, gc, c, gi, gj, 0, pc, pm, pp, cfm, cfp, rhs[c]);
+        }
+        __syncthreads();
+    }
+}
+
+// phi of a tile's window (periodic images; outside a non-periodic face the
+// value is never read) by plain loads.
+__device__ __forceinline__ void gsrb2_load_phi(const HLev& L, const HOp& op, const double* __restrict__ phi,
+                                               double (*sp)[kGsSX], int i0, int j0)
+{
+    for (int q = threadIdx.x; q < kGsSX * kGsSY; q += blockDim.x) {
+        const int li = q % kGsSX - 2, lj = q / kGsSX - 2;
+        int gi = i0 + li, gj = j0 + lj;
+        if (gi < 0) gi = op.bc_lo[0] == BAMREX_LINOP_PERIODIC ? gi + L.n[0] : 0;
+        if (gi >= L.n[0]) gi = op.bc_hi[0] == BAMREX_LINOP_PERIODIC ? gi - L.n[0] : L.n[0] - 1;
+        if (gj < 0) gj = op.bc_lo[1] == BAMREX_LINOP_PERIODIC ? gj + L.n[1] : 0;
+        if (gj >= L.n[1]) gj = op.bc_hi[1] == BAMREX_LINOP_PERIODIC ? gj - L.n[1] : L.n[1] - 1;
+        sp[lj + 2][li + 2] = phi[(long long)gj * L.n[0] + gi];
+    }
+}
+
+__device__ __forceinline__ void gsrb2_store(const HLev& L, double* __restrict__ phi_out, double (*sp)[kGsSX], int i0,
+                                            int j0)
+{
+    for (int q = threadIdx.x; q < kGsTX * kGsTY; q += blockDim.x) {
+        const int li = q % kGsTX, lj = q / kGsTX;
+        phi_out[(long long)(j0 + lj) * L.n[0] + i0 + li] = sp[lj + 2][li + 2];
+    }
+}
+
+// A full 2D sweep (red, then black) in one launch over tiles of 32 x 16
+// cells: the tile and a 2-cell halo of phi are staged in shared memory,
+// red is updated on the tile grown by one cell (the halo's red cells are
+// recomputed from the same inputs their own tile uses, so every value is
+// the one the two half-sweeps give), then black on the tile, which is
+// written to the other buffer (tiles read their halos from the old one).
+// One read and one write of phi per sweep instead of two each.  Requires
+// n0 % 32 == 0 and n1 % 16 == 0.
 __global__ void __launch_bounds__(256) gsrb2_fused_kernel(const HLev L, const HOp op, const double* __restrict__ phi,
                                                           double* __restrict__ phi_out, const double* __restrict__ rhs)
 {
-    constexpr int SX = kGsTX + 4, SY = kGsTY + 4;
-    __shared__ double sp[SY][SX];
+    __shared__ double sp[kGsSY][kGsSX];
     const GsCoef gc = gs_coef(L, op);
     const int tx = L.n[0] / kGsTX, ty = L.n[1] / kGsTY;
     for (int tile = blockIdx.x; tile < tx * ty; tile += gridDim.x) {
         const int i0 = (tile % tx) * kGsTX, j0 = (tile / tx) * kGsTY;
         __syncthreads();
-        for (int q = threadIdx.x; q < SX * SY; q += blockDim.x) {
-            const int li = q % SX - 2, lj = q / SX - 2;
-            int gi = i0 + li, gj = j0 + lj;
-            // periodic images; outside a non-periodic face the value is never read
-            if (gi < 0) gi = op.bc_lo[0] == BAMREX_LINOP_PERIODIC ? gi + L.n[0] : 0;
-            if (gi >= L.n[0]) gi = op.bc_hi[0] == BAMREX_LINOP_PERIODIC ? gi - L.n[0] : L.n[0] - 1;
-            if (gj < 0) gj = op.bc_lo[1] == BAMREX_LINOP_PERIODIC ? gj + L.n[1] : 0;
-            if (gj >= L.n[1]) gj = op.bc_hi[1] == BAMREX_LINOP_PERIODIC ? gj - L.n[1] : L.n[1] - 1;
-            sp[lj + 2][li + 2] = phi[(long long)gj * L.n[0] + gi];
-        }
+        gsrb2_load_phi(L, op, phi, sp, i0, j0);
         __syncthreads();
-        for (int pass = 0; pass < 2; ++pass) {
-            // pass 0: red on [-1, TX] x [-1, TY]; pass 1: black on the tile.
-            // Threads take the cells of the pass's colour only: row lj holds
-            // w / 2 of them, at columns of parity (lj + pass + i0 + j0) & 1.
-            const int lo = pass == 0 ? -1 : 0;
-            const int w = kGsTX + (pass == 0 ? 2 : 0), h = kGsTY + (pass == 0 ? 2 : 0);
-            const int wh = w / 2;
-            for (int q = threadIdx.x; q < wh * h; q += blockDim.x) {
-                const int lj = lo + q / wh;
-                const int par = ((i0 + j0 + lj + lo + pass) & 1);  // first column of the colour in this row
-                const int li = lo + 2 * (q % wh) + par;
-                const int gi0 = i0 + li, gj0 = j0 + lj;
-                // the cell itself in global indices (a periodic image for halo cells)
-                int gi = gi0, gj = gj0;
-                if (gi < 0 || gi >= L.n[0]) {
-                    if (op.bc_lo[0] != BAMREX_LINOP_PERIODIC) continue;
-                    gi = gi < 0 ? gi + L.n[0] : gi - L.n[0];
-                }
-                if (gj < 0 || gj >= L.n[1]) {
-                    if (op.bc_lo[1] != BAMREX_LINOP_PERIODIC) continue;
-                    gj = gj < 0 ? gj + L.n[1] : gj - L.n[1];
-                }
-                const double pc = sp[lj + 2][li + 2];
-                double pm[3], pp[3], cfm[3] = { 0, 0, 0 }, cfp[3] = { 0, 0, 0 };
-                const int nn[2] = { L.n[0], L.n[1] };
-                const int g[2] = { gi, gj };
-                for (int d = 0; d < 2; ++d) {
-                    const int si = d == 0 ? 1 : 0, sj = d == 1 ? 1 : 0;
-                    pm[d] = sp[lj + 2 - sj][li + 2 - si];
-                    pp[d] = sp[lj + 2 + sj][li + 2 + si];
-                    if (g[d] == 0 && op.bc_lo[d] != BAMREX_LINOP_PERIODIC) {
-                        cfm[d] = op.bc_lo[d] == BAMREX_LINOP_NEUMANN ? 1.0 : -1.0;
-                        pm[d] = cfm[d] * pc;
-                    }
-                    if (g[d] == nn[d] - 1 && op.bc_hi[d] != BAMREX_LINOP_PERIODIC) {
-                        cfp[d] = op.bc_hi[d] == BAMREX_LINOP_NEUMANN ? 1.0 : -1.0;
-                        pp[d] = cfp[d] * pc;
-                    }
-                }
-                const long long c = (long long)gj * L.n[0] + gi;
-                sp[lj + 2][li + 2] = gsrb_value<2>(L, op, gc, c, gi, gj, 0, pc, pm, pp, cfm, cfp, rhs[c]);
-            }
-            __syncthreads();
-        }
-        for (int q = threadIdx.x; q < kGsTX * kGsTY; q += blockDim.x) {
-            const int li = q % kGsTX, lj = q / kGsTX;
-            phi_out[(long long)(j0 + lj) * L.n[0] + i0 + li] = sp[lj + 2][li + 2];
+        gsrb2_tile(L, op, gc, sp, rhs, i0, j0, nullptr, nullptr, nullptr, nullptr);
+        gsrb2_store(L, phi_out, sp, i0, j0);
+    }
+}
+
+// The same sweep with every input of a tile staged: tiles away from the
+// domain boundary copy the windows of phi, a, rhs and both face
+// coefficients (20 x 36 values each, coalesced rows) into shared memory
+// with cp.async, the next tile's while the current one is swept, so the
+// sweep reads no global memory and waits on no load; boundary tiles take
+// the plain path of gsrb2_fused_kernel.  Operators without a gradient term
+// (c == nullptr).  The arithmetic is gsrb_core's, so the result is the
+// plain sweep's bit for bit.
+constexpr int kGsWin = kGsSX * kGsSY;                       // values of one window
+constexpr int kGsStageBytes = 5 * kGsWin * (int)sizeof(double);
+constexpr int kGsStagedSmem = 2 * kGsStageBytes;
+
+__device__ __forceinline__ bool gsrb2_interior(const HLev& L, int i0, int j0)
+{
+    return i0 >= kGsTX && i0 + kGsTX + 2 < L.n[0] && j0 >= kGsTY && j0 + kGsTY + 2 < L.n[1];
+}
+
+__device__ __forceinline__ void cp_async8(double* dst, const double* src)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)), "l"(src)
+                 : "memory");
+}
+
+// The five windows of an interior tile into stage st: phi, a, rhs (cells),
+// x faces (row stride n0 + 1), y faces (row stride n0); origin (i0-2, j0-2).
+__device__ __forceinline__ void gsrb2_prefetch(const HLev& L, const double* __restrict__ phi,
+                                               const double* __restrict__ rhs, double* st, int i0, int j0)
+{
+    const int nx = L.n[0];
+    for (int q = threadIdx.x; q < kGsWin; q += blockDim.x) {
+        const int li = q % kGsSX, lj = q / kGsSX;
+        const long long gc = (long long)(j0 - 2 + lj) * nx + (i0 - 2 + li);
+        cp_async8(st + q, phi + gc);
+        cp_async8(st + kGsWin + q, L.a + gc);
+        cp_async8(st + 2 * kGsWin + q, rhs + gc);
+        cp_async8(st + 3 * kGsWin + q, L.b[0] + (long long)(j0 - 2 + lj) * (nx + 1) + (i0 - 2 + li));
+        cp_async8(st + 4 * kGsWin + q, L.b[1] + gc);
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+}
+
+__global__ void __launch_bounds__(256) gsrb2_staged_kernel(const HLev L, const HOp op, const double* __restrict__ phi,
+                                                           double* __restrict__ phi_out, const double* __restrict__ rhs)
+{
+    extern __shared__ __align__(16) double gs_stage[];
+    __shared__ double sp_plain[kGsSY][kGsSX];
+    const GsCoef gc = gs_coef(L, op);
+    const int tx = L.n[0] / kGsTX, ty = L.n[1] / kGsTY;
+    const int ntiles = tx * ty;
+    auto origin = [&](int tile, int& i0, int& j0) {
+        i0 = (tile % tx) * kGsTX;
+        j0 = (tile / tx) * kGsTY;
+    };
+    int buf = 0;
+    {
+        int i0, j0;
+        if (blockIdx.x < ntiles) {
+            origin(blockIdx.x, i0, j0);
+            if (gsrb2_interior(L, i0, j0)) gsrb2_prefetch(L, phi, rhs, gs_stage, i0, j0);
         }
     }
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        int i0, j0;
+        origin(tile, i0, j0);
+        const bool staged = gsrb2_interior(L, i0, j0);
+        double* st = gs_stage + buf * (5 * kGsWin);
+        if (staged) asm volatile("cp.async.wait_all;" ::: "memory");
+        __syncthreads();  // this tile's window is in; the other stage is free
+        const int next = tile + gridDim.x;
+        if (next < ntiles) {
+            int ni, nj;
+            origin(next, ni, nj);
+            if (gsrb2_interior(L, ni, nj)) gsrb2_prefetch(L, phi, rhs, gs_stage + (buf ^ 1) * (5 * kGsWin), ni, nj);
+        }
+        if (staged) {
+            double (*sp)[kGsSX] = reinterpret_cast<double (*)[kGsSX]>(st);
+            gsrb2_tile(L, op, gc, sp, rhs, i0, j0, st + kGsWin, st + 2 * kGsWin, st + 3 * kGsWin, st + 4 * kGsWin);
+            gsrb2_store(L, phi_out, sp, i0, j0);
+        } else {
+            gsrb2_load_phi(L, op, phi, sp_plain, i0, j0);
+            __syncthreads();
+            gsrb2_tile(L, op, gc, sp_plain, rhs, i0, j0, nullptr, nullptr, nullptr, nullptr);
+            gsrb2_store(L, phi_out, sp_plain, i0, j0);
+        }
+        buf ^= 1;
+    }
+    asm volatile("cp.async.wait_all;" ::: "memory");
 }
 
 // rhs_c = mean of the 2^D children of the fine residual
 template <int D>
-__global__ void restrict_kernel(const HLev F, const HLev C)
+__device__ __forceinline__ void restrict_cell(const HLev& F, const HLev& C, long long c)
 {
     const double w = D == 3 ? 0.125 : (D == 2 ? 0.25 : 0.5);
-    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < C.ncell;
-         c += (long long)gridDim.x * blockDim.x) {
+    {
         const int i = (int)(c % C.n[0]);
         const int j = (int)((c / C.n[0]) % C.n[1]);
         const int k = (int)(c / ((long long)C.n[0] * C.n[1]));
@@ -303,17 +471,157 @@ __global__ void restrict_kernel(const HLev F, const HLev C)
     }
 }
 
+template <int D>
+__global__ void restrict_kernel(const HLev F, const HLev C)
+{
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < C.ncell;
+         c += (long long)gridDim.x * blockDim.x)
+        restrict_cell<D>(F, C, c);
+}
+
 // phi_f += phi_c(parent)
+template <int D>
+__device__ __forceinline__ void prolong_cell(const HLev& F, const HLev& C, long long c)
+{
+    const int i = (int)(c % F.n[0]);
+    const int j = (int)((c / F.n[0]) % F.n[1]);
+    const int k = (int)(c / ((long long)F.n[0] * F.n[1]));
+    F.phi[c] = F.phi[c] + C.phi[cidx(C, i / 2, D > 1 ? j / 2 : j, D > 2 ? k / 2 : k)];
+}
+
 template <int D>
 __global__ void prolong_kernel(const HLev F, const HLev C)
 {
     for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < F.ncell;
-         c += (long long)gridDim.x * blockDim.x) {
-        const int i = (int)(c % F.n[0]);
-        const int j = (int)((c / F.n[0]) % F.n[1]);
-        const int k = (int)(c / ((long long)F.n[0] * F.n[1]));
-        F.phi[c] = F.phi[c] + C.phi[cidx(C, i / 2, D > 1 ? j / 2 : j, D > 2 ? k / 2 : k)];
+         c += (long long)gridDim.x * blockDim.x)
+        prolong_cell<D>(F, C, c);
+}
+
+// The coarse end of a V-cycle in one block: from level 0 of `lv` (the
+// first level of at most kSmallCells cells) down to the bottom and back,
+// every phase a block-strided loop over the level's cells followed by a
+// block barrier (the launches of the multi-block cycle, each a grid-wide
+// step, become barriers): nu1 red-black sweeps, the residual, restriction,
+// the bottom's sweeps, prolongation, nu2 sweeps.  The levels' coefficients
+// and work arrays live in shared memory for the whole cycle (copied in at
+// the start; the first level's phi copied back at the end).  Each cell's
+// arithmetic is the multi-block kernels' (gsrb_value, apply_value,
+// restrict_cell, prolong_cell), and a colour's cells never read each
+// other, so the result is the same bit for bit; the launches and their
+// global-memory round trips are gone.
+constexpr int kSmallLevels = 12;
+constexpr int kSmallThreads = 512;
+constexpr long long kSmallCells = 1024;
+constexpr int kSmallSmemMax = 200 * 1024;
+struct HLevs {
+    HLev lev[kSmallLevels];
+    int n;
+};
+
+// doubles of one level in the shared layout: phi, rhs, res, a, the face
+// coefficients of each direction, the gradient coefficients if present
+__host__ __device__ __forceinline__ long long face_count(const HLev& L, int d)
+{
+    return (long long)(L.n[0] + (d == 0)) * (L.n[1] + (d == 1)) * (L.n[2] + (d == 2));
+}
+__host__ __device__ __forceinline__ long long small_level_doubles(const HLev& L, int D)
+{
+    long long t = 4 * L.ncell;
+    for (int d = 0; d < D; ++d) t += face_count(L, d);
+    if (L.c) t += (long long)D * L.ncell;
+    return t;
+}
+
+template <int D>
+__device__ void small_sweeps(const HLev L, const HOp& op, int sweeps)
+{
+    const GsCoef gc = gs_coef(L, op);
+    for (int s = 0; s < sweeps; ++s)
+        for (int color = 0; color < 2; ++color) {
+            for (int c = threadIdx.x; c < (int)L.ncell; c += blockDim.x) {
+                const int i = c % L.n[0];
+                const int j = (c / L.n[0]) % L.n[1];
+                const int k = c / (L.n[0] * L.n[1]);
+                if ((i + j + k + color) & 1) continue;
+                const double pc = L.phi[c];
+                double pm[3], pp[3], cfm[3], cfp[3];
+                for (int d = 0; d < D; ++d) {
+                    pm[d] = nbr(L.phi, L, op, i, j, k, d, -1, pc, cfm[d]);
+                    pp[d] = nbr(L.phi, L, op, i, j, k, d, +1, pc, cfp[d]);
+                }
+                L.phi[c] = gsrb_value<D>(L, op, gc, c, i, j, k, pc, pm, pp, cfm, cfp, L.rhs[c]);
+            }
+            __syncthreads();
+        }
+}
+
+__device__ __forceinline__ void small_copy(double* dst, const double* src, long long n)
+{
+    for (long long q = threadIdx.x; q < n; q += blockDim.x) dst[q] = src[q];
+}
+
+template <int D>
+__global__ void __launch_bounds__(kSmallThreads) vcycle_small_kernel(const HLevs lv, const HOp op, int nu1, int nu2,
+                                                                     int bottom)
+{
+    extern __shared__ double small_sm[];
+    __shared__ HLev S[kSmallLevels];
+    const int nl = lv.n;
+    if (threadIdx.x == 0) {
+        long long off = 0;
+        for (int l = 0; l < nl; ++l) {
+            const HLev& G = lv.lev[l];
+            HLev& L = S[l];
+            L = G;
+            L.phi = small_sm + off;
+            off += G.ncell;
+            L.rhs = small_sm + off;
+            off += G.ncell;
+            L.res = small_sm + off;
+            off += G.ncell;
+            L.a = small_sm + off;
+            off += G.ncell;
+            for (int d = 0; d < D; ++d) {
+                L.b[d] = small_sm + off;
+                off += face_count(G, d);
+            }
+            if (G.c) {
+                L.c = small_sm + off;
+                off += (long long)D * G.ncell;
+            }
+        }
     }
+    __syncthreads();
+    for (int l = 0; l < nl; ++l) {
+        const HLev& G = lv.lev[l];
+        small_copy(S[l].a, G.a, G.ncell);
+        for (int d = 0; d < D; ++d) small_copy(S[l].b[d], G.b[d], face_count(G, d));
+        if (G.c) small_copy(S[l].c, G.c, (long long)D * G.ncell);
+    }
+    small_copy(S[0].phi, lv.lev[0].phi, lv.lev[0].ncell);
+    small_copy(S[0].rhs, lv.lev[0].rhs, lv.lev[0].ncell);
+    __syncthreads();
+    // the level descriptions in registers (the shared copies would be
+    // re-read after every barrier)
+    for (int l = 0; l + 1 < nl; ++l) {
+        const HLev F = S[l];
+        const HLev C = S[l + 1];
+        small_sweeps<D>(F, op, nu1);
+        const ApplyCoef ac = apply_coef(F, op);
+        for (int c = threadIdx.x; c < (int)F.ncell; c += blockDim.x) F.res[c] = apply_value<D>(F, op, ac, F.phi, F.rhs, 1, c);
+        __syncthreads();
+        for (int c = threadIdx.x; c < (int)C.ncell; c += blockDim.x) restrict_cell<D>(F, C, c);
+        __syncthreads();
+    }
+    small_sweeps<D>(S[nl - 1], op, bottom);
+    for (int l = nl - 2; l >= 0; --l) {
+        const HLev F = S[l];
+        const HLev C = S[l + 1];
+        for (int c = threadIdx.x; c < (int)F.ncell; c += blockDim.x) prolong_cell<D>(F, C, c);
+        __syncthreads();
+        small_sweeps<D>(F, op, nu2);
+    }
+    small_copy(lv.lev[0].phi, S[0].phi, lv.lev[0].ncell);
 }
 
 // averageDownCoeffs: cell coefficients by the mean of the children, face
@@ -589,6 +897,8 @@ int grid_for(long long n)
 struct bamrex_helmholtz {
     int D = 2;
     HOp op;
+    bool staged_smoother = true;  // 2D fused sweeps with cp.async-staged tiles
+    bool small_cycle = true;      // levels of <= 1024 cells cycled by one block in shared memory
     int nu1 = 2, nu2 = 2, bottom = 16;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
@@ -666,10 +976,27 @@ int smooth(bamrex_helmholtz* H, int l, int sweeps)
         // ping-pong between phi and tmp; an odd count ends with a copy back
         const int tiles = (L.n[0] / kGsTX) * (L.n[1] / kGsTY);
         const int g = std::max(1, std::min(tiles, device_sm_count() * 8));
+        // tiles staged by cp.async where the operator has no gradient term
+        const bool staged = L.c == nullptr && H->staged_smoother;
+        if (staged) {
+            static bool attr_set[64] = { false };
+            int dev = 0;
+            cudaGetDevice(&dev);
+            if (!attr_set[dev & 63]) {
+                H_TRY(hck(H, cudaFuncSetAttribute(gsrb2_staged_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                  kGsStagedSmem),
+                          "smoother shared memory"));
+                attr_set[dev & 63] = true;
+            }
+        }
+        const int gs = std::max(1, std::min(tiles, device_sm_count() * 3));
         for (int s = 0; s < sweeps; ++s) {
             const double* in = (s & 1) ? L.tmp : L.phi;
             double* out = (s & 1) ? L.phi : L.tmp;
-            gsrb2_fused_kernel<<<g, 256, 0, H->stream>>>(L, H->op, in, out, L.rhs);
+            if (staged)
+                gsrb2_staged_kernel<<<gs, 256, kGsStagedSmem, H->stream>>>(L, H->op, in, out, L.rhs);
+            else
+                gsrb2_fused_kernel<<<g, 256, 0, H->stream>>>(L, H->op, in, out, L.rhs);
             H_TRY(hck(H, cudaGetLastError(), "helmholtz gsrb (fused)"));
         }
         if (sweeps & 1)
@@ -687,6 +1014,33 @@ int smooth(bamrex_helmholtz* H, int l, int sweeps)
 int vcycle(bamrex_helmholtz* H, int l)
 {
     const int nl = (int)H->lev.size();
+    if (H->small_cycle && H->lev[l].ncell <= kSmallCells && nl - l <= kSmallLevels) {
+        // the rest of the cycle in one block, its levels in shared memory
+        HLevs lv;
+        lv.n = nl - l;
+        long long doubles = 0;
+        for (int q = l; q < nl; ++q) {
+            lv.lev[q - l] = H->lev[q];
+            doubles += small_level_doubles(H->lev[q], H->D);
+        }
+        const long long bytes = doubles * (long long)sizeof(double);
+        if (bytes <= kSmallSmemMax) {
+            static bool attr_set[2][64] = { { false } };
+            int dev = 0;
+            cudaGetDevice(&dev);
+            const void* fn = H->D == 3 ? (const void*)vcycle_small_kernel<3> : (const void*)vcycle_small_kernel<2>;
+            if (!attr_set[H->D == 3][dev & 63]) {
+                H_TRY(hck(H, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmallSmemMax),
+                          "coarse V-cycle shared memory"));
+                attr_set[H->D == 3][dev & 63] = true;
+            }
+            if (H->D == 3)
+                vcycle_small_kernel<3><<<1, kSmallThreads, (size_t)bytes, H->stream>>>(lv, H->op, H->nu1, H->nu2, H->bottom);
+            else
+                vcycle_small_kernel<2><<<1, kSmallThreads, (size_t)bytes, H->stream>>>(lv, H->op, H->nu1, H->nu2, H->bottom);
+            return hck(H, cudaGetLastError(), "coarse V-cycle");
+        }
+    }
     if (l == nl - 1) return smooth(H, l, H->bottom);
     H_TRY(smooth(H, l, H->nu1));
     const HLev& F = H->lev[l];

@@ -420,9 +420,10 @@ __device__ __forceinline__ float log2_abs(double x)
 }
 
 // x^(-z) with 1/z ~ 7 for x >= 1e-14 (HLLC.H:272), and 1/x as a by-product.
-// FP64: seed y0 = 2^(-log2(x)/7) in single precision, then one step of the
-// series of (1 - e)^(-1/7), e = 1 - x y0^7 (third-order convergence: |e| ~
-// 1e-7 leaves ~1e-22), then the factor x^(1/7 - z) ~ 1 + (1/7 - z) ln x;
+// FP64: seed y0 = 2^(-log2(x)/7) in single precision (the hardware
+// approximations of log2 and exp2, a few ulp), then one step of the series
+// of (1 - e)^(-1/7), e = 1 - x y0^7 (third-order convergence: |e| ~ 2e-6
+// leaves ~5e-19), then the factor x^(1/7 - z) ~ 1 + (1/7 - z) ln x;
 // 1/x = y0^7 / (1 - e) ~ y0^7 (1 + e + e^2).  FP32: exp2(-z log2 x) on the
 // special-function unit.
 __device__ __forceinline__ void root7_neg_z(double x, const K<double>& c, double& y, double& inv_x)
@@ -431,7 +432,7 @@ __device__ __forceinline__ void root7_neg_z(double x, const K<double>& c, double
     const float q = -lf * (1.0f / 7.0f);
     const float qi = floorf(q);
     const double p2 = __longlong_as_double((long long)((int)qi + 1023) << 52);
-    const double y0 = p2 * (double)exp2f(q - qi);
+    const double y0 = p2 * (double)ex2_fast(q - qi);
     const double y2 = y0 * y0, y3 = y2 * y0, y6 = y3 * y3, y7 = y6 * y0;
     const double e = fma(-x, y7, 1.0);
     const double t = e * fma(e, 8.0 / 98.0, 1.0 / 7.0);

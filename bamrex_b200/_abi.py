@@ -297,6 +297,8 @@ SIGNATURES = {
     "bamrex_level_dist_dt": (_i, [_vp, _vp, _i]),
     "bamrex_level_fill_dir_device": (_i, [_vp, _i]),
     "bamrex_level_sweep_dir_device": (_i, [_vp, _i, _i]),
+    "bamrex_level_set_sweep_split": (_i, [_vp, _i, ctypes.POINTER(ctypes.c_int), _i]),
+    "bamrex_level_sweep_dir_device_part": (_i, [_vp, _i, _i, _i]),
     "bamrex_level_dist_end": (_i, [_vp, _dp, _dp, ctypes.POINTER(ctypes.c_int)]),
     "bamrex_level_step_host": (_i, [_vp, _vp, _vp, _d, _i, _dp]),
     "bamrex_level_run_host": (_i, [_vp, _vp, _i, _d, _i, _dp, _dp]),

@@ -801,13 +801,20 @@ int level_fill(bamrex_level* L, int d, int parity, const StepScalars* scal)
 }
 
 int level_sweep(bamrex_level* L, int d, int parity, double dt_host, const StepScalars* scal, bool reduce_ws,
-                bool allow_timing)
+                bool allow_timing, int part)
 {
     SweepArgs a;
     std::memset(&a, 0, sizeof(a));
     a.boxes = L->d_sweep[d][parity];
     a.nboxes = (int)L->boxes.size();
     a.total_items = L->items[d];
+    if (part >= 0) {
+        // one part of a split sweep (its own box table)
+        a.boxes = L->d_split[d][parity][part];
+        a.nboxes = L->split_nboxes[d][part];
+        a.total_items = L->split_items[d][part];
+        if (a.total_items == 0) return BAMREX_OK;
+    }
     a.seglen = L->seglen[d];
     a.halo = method_halo(L->method);
     a.dt_host = dt_host;
@@ -1250,6 +1257,7 @@ extern "C" int bamrex_level_destroy(bamrex_level* L)
     dev_free(L->staging, L->stream);
     dev_free(L->tag_buf, L->stream);
     for (int d = 0; d < 3; ++d) dev_free(L->halo_mem[d], L->stream);
+    for (int d = 0; d < 3; ++d) dev_free(L->split_mem[d], L->stream);
     pinned_small_free(L->h_scal);
     if (L->own_stream && L->stream) cudaStreamDestroy(L->stream);
     delete L;

@@ -213,6 +213,73 @@ extern "C" int bamrex_level_sweep_dir_device(bamrex_level* L, int dir, int reduc
     return BAMREX_OK;
 }
 
+extern "C" int bamrex_level_set_sweep_split(bamrex_level* L, int dir, const int* boxes, int nboxes)
+{
+    if (!L || dir < 0 || dir >= L->D || nboxes < 0 || (nboxes > 0 && !boxes)) return fail(BAMREX_ERR_ARG, "bad argument");
+    const int nb = (int)L->boxes.size();
+    std::vector<char> in_part1((size_t)nb, 0);
+    for (int i = 0; i < nboxes; ++i) {
+        if (boxes[i] < 0 || boxes[i] >= nb) return L->set_err(fail(BAMREX_ERR_ARG, "split box index out of range"));
+        in_part1[(size_t)boxes[i]] = 1;
+    }
+    // the level's own tables, each box entry kept as it is (kernel shape,
+    // tensor map, segments) and renumbered within its part
+    std::vector<SweepBox> full[2];
+    cudaError_t e = cudaSuccess;
+    for (int p = 0; p < 2 && e == cudaSuccess; ++p) {
+        full[p].resize((size_t)nb);
+        e = cudaMemcpyAsync(full[p].data(), L->d_sweep[dir][p], sizeof(SweepBox) * nb, cudaMemcpyDeviceToHost, L->stream);
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(L->stream);
+    if (e != cudaSuccess) return L->set_err(cuda_fail(e, "sweep split tables"));
+    std::vector<SweepBox> part[2][2];  // [parity][part]
+    long long items[2] = { 0, 0 };
+    for (int b = 0; b < nb; ++b) {
+        const int q = in_part1[(size_t)b];
+        const long long n = (b + 1 < nb ? full[0][(size_t)b + 1].item_begin : L->items[dir]) - full[0][(size_t)b].item_begin;
+        for (int p = 0; p < 2; ++p) {
+            SweepBox sb = full[p][(size_t)b];
+            sb.item_begin = items[q];
+            part[p][q].push_back(sb);
+        }
+        items[q] += n;
+    }
+    dev_free(L->split_mem[dir], L->stream);
+    L->split_mem[dir] = nullptr;
+    char* mem = nullptr;
+    e = dev_alloc((void**)&mem, sizeof(SweepBox) * (size_t)std::max(1, 2 * nb), L->stream);
+    if (e != cudaSuccess) return L->set_err(fail(BAMREX_ERR_OOM, "sweep split tables"));
+    L->split_mem[dir] = mem;
+    size_t off = 0;
+    for (int p = 0; p < 2 && e == cudaSuccess; ++p)
+        for (int q = 0; q < 2 && e == cudaSuccess; ++q) {
+            L->d_split[dir][p][q] = reinterpret_cast<SweepBox*>(mem) + off;
+            if (!part[p][q].empty())
+                e = cudaMemcpyAsync(L->d_split[dir][p][q], part[p][q].data(), sizeof(SweepBox) * part[p][q].size(),
+                                    cudaMemcpyHostToDevice, L->stream);
+            off += part[p][q].size();
+        }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(L->stream);
+    if (e != cudaSuccess) return L->set_err(cuda_fail(e, "sweep split tables"));
+    for (int q = 0; q < 2; ++q) {
+        L->split_items[dir][q] = items[q];
+        L->split_nboxes[dir][q] = (int)part[0][q].size();
+    }
+    return BAMREX_OK;
+}
+
+extern "C" int bamrex_level_sweep_dir_device_part(bamrex_level* L, int dir, int reduce_ws, int part)
+{
+    if (!L || dir < 0 || dir >= L->D || part < 0 || part > 1) return fail(BAMREX_ERR_ARG, "bad argument");
+    if (!L->run_pending) return L->set_err(fail(BAMREX_ERR_ARG, "call bamrex_level_dist_begin first"));
+    if (!L->split_mem[dir]) return L->set_err(fail(BAMREX_ERR_ARG, "call bamrex_level_set_sweep_split first"));
+    if (!L->reg_tasks[dir].empty())
+        return L->set_err(fail(BAMREX_ERR_UNSUPPORTED, "flux registers are recorded by bamrex_level_advance only"));
+    BX_TRY(level_sweep(L, dir, L->cur, 0.0, L->d_scal, reduce_ws != 0, true, part));
+    if (part == 1) L->cur ^= 1;  // the direction is complete
+    return BAMREX_OK;
+}
+
 extern "C" int bamrex_level_dist_end(bamrex_level* L, double* time, double* dt, int* steps)
 {
     if (!L) return fail(BAMREX_ERR_ARG, "NULL level");

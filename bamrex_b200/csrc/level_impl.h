@@ -116,6 +116,14 @@ struct bamrex_level {
     };
     Halo halo_send[3], halo_recv[3];
     char* halo_mem[3] = { nullptr, nullptr, nullptr };
+    // the sweep of a direction split in two launches over complementary box
+    // sets (bamrex_level_set_sweep_split): part 0 the boxes whose ghost cells
+    // in that direction are all local, part 1 the others; per direction,
+    // parity and part a box table (item_begin from 0) and its work items
+    bamrex::SweepBox* d_split[3][2][2] = {};
+    long long split_items[3][2] = {};
+    int split_nboxes[3][2] = {};
+    char* split_mem[3] = { nullptr, nullptr, nullptr };
 
     // accounting
     long long launches = 0;
@@ -175,7 +183,7 @@ int level_fill(bamrex_level* L, int d, int parity, const StepScalars* scal);
 // One sweep of direction d from buffer `parity` into parity ^ 1; reduce_ws:
 // also reduce the max wave speed of the output into d_scal->ws_bits.
 int level_sweep(bamrex_level* L, int d, int parity, double dt_host, const StepScalars* scal, bool reduce_ws,
-                bool allow_timing);
+                bool allow_timing, int part = -1);
 // One split step starting from buffer `parity`; the result lands in
 // parity ^ (D & 1).  dt from the host (scal == nullptr) or from the device;
 // next_dt (device dt only): end the step with the level's own next dt

@@ -230,6 +230,18 @@ class DeviceEngine:
         from ._abi import check, lib
         check(lib().bamrex_level_sweep_dir_device(self.level._h, d, 1 if reduce_ws else 0), self.level._h)
 
+    def set_split(self, d, edge_boxes):
+        """Direction d's sweep in two parts: part 1 the local boxes listed
+        (their ghost cells come from other ranks), part 0 the others."""
+        import ctypes
+        from ._abi import check, lib
+        arr = (ctypes.c_int * max(1, len(edge_boxes)))(*edge_boxes)
+        check(lib().bamrex_level_set_sweep_split(self.level._h, d, arr, len(edge_boxes)), self.level._h)
+
+    def sweep_dir_device_part(self, d, reduce_ws, part):
+        from ._abi import check, lib
+        check(lib().bamrex_level_sweep_dir_device_part(self.level._h, d, 1 if reduce_ws else 0, part), self.level._h)
+
     def end(self):
         """(time, next dt, steps taken); waits for the level's stream."""
         import ctypes
@@ -244,7 +256,8 @@ class DistLevel:
     """The split step of one level whose boxes are spread over the ranks of
     a torch.distributed process group."""
 
-    def __init__(self, engine, D, dom_lo, dom_hi, boxes, owners, ngrow, bc_lo, bc_hi, dx, cfl, rank, world, dist):
+    def __init__(self, engine, D, dom_lo, dom_hi, boxes, owners, ngrow, bc_lo, bc_hi, dx, cfl, rank, world, dist,
+                 overlap=True):
         self.e, self.D, self.dx, self.cfl = engine, D, list(dx), cfl
         self.rank, self.world, self.dist = rank, world, dist
         self.plan = HaloPlan(D, dom_lo, dom_hi, boxes, owners, ngrow, bc_lo, bc_hi, rank)
@@ -253,21 +266,44 @@ class DistLevel:
             send, recv = self.plan.dirs[d]
             engine.set_halo(d, send, recv)
             self.bufs.append((engine.buffer(send["cells"]), engine.buffer(recv["cells"])))
+        # interior sweeps while halos travel: per direction the local boxes
+        # that receive ghost cells from other ranks are swept after the
+        # exchange, every other box while it is in flight
+        self.overlap = bool(overlap) and world > 1 and hasattr(engine, "set_split")
+        if self.overlap:
+            for d in range(D):
+                edge = sorted({lb for (lb, _lo, _hi, _off) in self.plan.dirs[d][1]["regions"]})
+                engine.set_split(d, edge)
 
-    def exchange(self, d):
+    def exchange_start(self, d):
+        """Pack direction d's halo and post its sends and receives (every
+        rank posts the same pairs in the same order); returns the requests."""
         send, recv = self.plan.dirs[d]
         sbuf, rbuf = self.bufs[d]
         self.e.pack(d, sbuf)
         NC = self.e.NC
+        # one batch (an NCCL group): separate sends and receives of a pair of
+        # ranks, each posting its receive first, could wait on each other in
+        # the pair's stream
+        ops = [self.dist.P2POp(self.dist.irecv, rbuf[start * NC:(start + n) * NC], peer)
+               for peer, start, n in recv["peers"]]
+        ops += [self.dist.P2POp(self.dist.isend, sbuf[start * NC:(start + n) * NC], peer)
+                for peer, start, n in send["peers"]]
+        if not ops:
+            return []
         with self.e.stream_context():
-            reqs = []
-            for peer, start, n in recv["peers"]:
-                reqs.append(self.dist.irecv(rbuf[start * NC:(start + n) * NC], src=peer))
-            for peer, start, n in send["peers"]:
-                reqs.append(self.dist.isend(sbuf[start * NC:(start + n) * NC], dst=peer))
+            return self.dist.batch_isend_irecv(ops)
+
+    def exchange_finish(self, d, reqs):
+        """Wait for direction d's requests (with NCCL: the level's stream
+        waits, the host does not) and unpack the received ghost cells."""
+        with self.e.stream_context():
             for r in reqs:
                 r.wait()
-        self.e.unpack(d, rbuf)
+        self.e.unpack(d, self.bufs[d][1])
+
+    def exchange(self, d):
+        self.exchange_finish(d, self.exchange_start(d))
 
     def global_wave_speed(self):
         ws = self.e.wave_speed()
@@ -325,10 +361,19 @@ class DistLevel:
             self.e.device_dt(ws, True)
             for _ in range(nsteps):
                 for d in range(self.D):
+                    last = d == self.D - 1
+                    if self.overlap:
+                        # the interior boxes sweep while the halo is in flight
+                        reqs = self.exchange_start(d)
+                        self.e.fill_dir_device(d)
+                        self.e.sweep_dir_device_part(d, last, 0)
+                        self.exchange_finish(d, reqs)
+                        self.e.sweep_dir_device_part(d, last, 1)
+                        continue
                     if self.world > 1:
                         self.exchange(d)
                     self.e.fill_dir_device(d)
-                    self.e.sweep_dir_device(d, d == self.D - 1)
+                    self.e.sweep_dir_device(d, last)
                 self._global_max_into(ws)
                 self.e.device_dt(ws, False)
         except BaseException:

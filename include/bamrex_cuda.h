@@ -426,6 +426,16 @@ BAMREX_API int bamrex_level_wave_speed_async(bamrex_level *level, double *dst_de
 BAMREX_API int bamrex_level_dist_dt(bamrex_level *level, const double *ws_device, int first);
 BAMREX_API int bamrex_level_fill_dir_device(bamrex_level *level, int dir);
 BAMREX_API int bamrex_level_sweep_dir_device(bamrex_level *level, int dir, int reduce_ws);
+/* Interior sweeps while halos travel (the MPI overlap of FillBoundary with
+ * the MFIter loop of advance_explicit, Source/AmrLevelAdv_advance.cpp:356).
+ * set_sweep_split lists the boxes (local indices) whose ghost cells in
+ * direction dir come from other ranks; sweep_dir_device_part then sweeps
+ * part 0 (every other box: no remote ghost cells, so it can run while the
+ * exchange is in flight) or part 1 (the listed boxes, after the unpack),
+ * with the arithmetic and kernels of bamrex_level_sweep_dir_device; part 1
+ * completes the direction.  The split is set up once (synchronous). */
+BAMREX_API int bamrex_level_set_sweep_split(bamrex_level *level, int dir, const int *boxes, int nboxes);
+BAMREX_API int bamrex_level_sweep_dir_device_part(bamrex_level *level, int dir, int reduce_ws, int part);
 BAMREX_API int bamrex_level_dist_end(bamrex_level *level, double *time, double *dt, int *steps);
 
 /* ------------------------------------------------------------------ */

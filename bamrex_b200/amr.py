@@ -98,7 +98,7 @@ class Amr:
                  blocking_factor=8, max_grid_size=32, n_error_buf=2, n_proper=1, grid_eff=0.7, regrid_int=0,
                  do_reflux=True, phigrad=None, phigrad_var=0, phigrad_var_is_primv=False, phierr=None, phierr_var=0,
                  phierr_var_is_primv=False, max_int_lev=-1, lstol=None, max_box_lev=-1, refine_box=None,
-                 stream=None):
+                 staging=_abi.STAGING_AUTO, stream=None):
         self.D = spacedim
         self.parm, self.method, self.cfl, self.precision = parm, method, cfl, precision
         self.ratio = ref_ratio
@@ -126,6 +126,7 @@ class Amr:
         b.cfl = cfl
         b.parm = parm.to_c()
         b.precision = precision
+        b.staging = staging  # sweep kernels of every level (bamrex_level_desc.staging)
         d.max_level = max_level
         d.ref_ratio = ref_ratio
         d.blocking_factor = blocking_factor
@@ -341,7 +342,7 @@ def chop_drawn(boxes, choices, rng, D=3):
 BLAST_BOX_SIZES = (16, 32, 48, 64)
 
 
-def blast_hierarchy(n0, precision=_abi.FP64, seed=20261203, stream=None):
+def blast_hierarchy(n0, precision=_abi.FP64, seed=20261203, stream=None, staging=_abi.STAGING_AUTO):
     """The 3D spherical blast (p 10 inside r < 0.2, 0.1 outside, rho 1) on a
     3-level hierarchy: base n0^3 on [0,1]^3, ratio 2, blocking factor 8,
     grad_error on rho >= 0.1, MUSCL-Hancock/minbee, CFL 0.8, boxes cut to a
@@ -355,7 +356,7 @@ def blast_hierarchy(n0, precision=_abi.FP64, seed=20261203, stream=None):
     base = chop_drawn([((0, 0, 0), hi)], BLAST_BOX_SIZES, rng)
     A = Amr(3, (0, 0, 0), hi, [0.0] * 3, [1.0] * 3, base, Parm(3, limiter=_abi.MINBEE), cfl=0.8, max_level=2,
             ref_ratio=2, blocking_factor=8, max_grid_size=64, n_error_buf=2, grid_eff=0.7, regrid_int=2,
-            phigrad=[0.1, 0.1], phigrad_var=0, precision=precision, stream=stream)
+            phigrad=[0.1, 0.1], phigrad_var=0, precision=precision, staging=staging, stream=stream)
     A.set_state(0, problems.blast_3d(n0, radius=0.2))
     for _ in range(4):
         A.coarse_step()
@@ -387,9 +388,13 @@ def main(argv=None):
     ap.add_argument("--fp32", action="store_true")
     ap.add_argument("--regrid-int", type=int, default=0)
     ap.add_argument("--profile", action="store_true")
+    ap.add_argument("--staging", type=int, default=_abi.STAGING_AUTO, help="sweep kernels of every level")
+    ap.add_argument("--warm-steps", type=int, default=0, help="untimed coarse steps on fixed grids first")
     a = ap.parse_args(argv)
-    A, _ = blast_hierarchy(a.n, _abi.FP32_STORAGE if a.fp32 else _abi.FP64)
+    A, _ = blast_hierarchy(a.n, _abi.FP32_STORAGE if a.fp32 else _abi.FP64, staging=a.staging)
     try:
+        for _ in range(a.warm_steps):
+            A.coarse_step()
         A.set_regrid_int(a.regrid_int)
         if a.profile:
             _abi.profile_enable(True)

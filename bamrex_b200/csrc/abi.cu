@@ -12,6 +12,7 @@
 #include <cstring>
 #include <new>
 #include <string>
+#include <thread>
 #include <utility>
 #include <vector>
 
@@ -296,10 +297,11 @@ int choose_tma_seglen(int D, int dir, const std::vector<bamrex_box>& boxes, long
     // the largest of them stands for all (it would win their ties)
     while (cand.size() > 1 && cand[1] >= nmax) cand.erase(cand.begin() + 1);
     const long long W = std::max(1LL, resident_units);
-    int best = cand[0];
-    long long best_span = -1;
-    std::vector<long long> load;
-    for (int c : cand) {
+    // the span of each candidate, candidates on host threads when the level
+    // has many boxes; the first of the smallest spans wins, as in order
+    std::vector<long long> spans(cand.size(), 0);
+    auto span_of = [&](int c) {
+        std::vector<long long> load;
         long long total = 0;
         for (const auto& b : boxes) {
             long long it;
@@ -319,12 +321,27 @@ int choose_tma_seglen(int D, int dir, const std::vector<bamrex_box>& boxes, long
                 for (int sg = 0; sg < nseg; ++sg, ++idx)
                     load[(size_t)(idx % nw)] += tma_item_cost(wave, pw, std::min(bl, n - sg * bl));
         }
-        const long long span = *std::max_element(load.begin(), load.end());
-        if (best_span < 0 || span < best_span) {
-            best = c;
-            best_span = span;
-        }
+        return *std::max_element(load.begin(), load.end());
+    };
+    const int nth = boxes.size() >= 256 ? (int)std::min<size_t>(cand.size(), std::max(1u, std::thread::hardware_concurrency()))
+                                        : 1;
+    if (nth > 1) {
+        std::vector<std::thread> th;
+        for (int t = 0; t < nth; ++t)
+            th.emplace_back([&, t] {
+                for (size_t i = (size_t)t; i < cand.size(); i += (size_t)nth) spans[i] = span_of(cand[i]);
+            });
+        for (auto& x : th) x.join();
+    } else {
+        for (size_t i = 0; i < cand.size(); ++i) spans[i] = span_of(cand[i]);
     }
+    int best = cand[0];
+    long long best_span = -1;
+    for (size_t i = 0; i < cand.size(); ++i)
+        if (best_span < 0 || spans[i] < best_span) {
+            best = cand[i];
+            best_span = spans[i];
+        }
     return best;
 }
 
@@ -1095,10 +1112,21 @@ extern "C" int bamrex_level_create(bamrex_level** out, const bamrex_level_desc* 
     BoxIndex bidx;
     bidx.build(L->domain, L->boxes, D);
     std::vector<GhostOp> ghost_host[3];
-    for (int d = 0; d < D; ++d) {
-        build_ghost_ops(L, d, bidx, ghost_host[d]);
-        L->nghost[d] = (int)ghost_host[d].size();
-        L->ghost_chunks[d] = number_ghost_ops(ghost_host[d]);
+    {
+        // the directions on host threads for levels of many boxes
+        auto one_dir = [&](int d) {
+            build_ghost_ops(L, d, bidx, ghost_host[d]);
+            L->nghost[d] = (int)ghost_host[d].size();
+            L->ghost_chunks[d] = number_ghost_ops(ghost_host[d]);
+        };
+        if (nb >= 256 && D > 1) {
+            std::vector<std::thread> th;
+            for (int d = 1; d < D; ++d) th.emplace_back(one_dir, d);
+            one_dir(0);
+            for (auto& x : th) x.join();
+        } else {
+            for (int d = 0; d < D; ++d) one_dir(d);
+        }
     }
 
     // ---- pack boxes

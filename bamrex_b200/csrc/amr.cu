@@ -349,11 +349,14 @@ CfRegion make_region(int dst, const bamrex_box& b, const int* shift)
 
 // The fine ghost regions to interpolate: face slabs of depth ngrow of every
 // fine box, inside the domain (or the periodic image outside it), minus the
-// fine boxes.
+// fine boxes.  Boxes on host threads, their regions joined in box order.
 void build_ghost_regions(const bamrex_level* Lf, const BoxIndex& fidx, std::vector<CfRegion>& regs)
 {
     const int g = Lf->ngrow;
-    for (int b = 0; b < (int)Lf->boxes.size(); ++b) {
+    const int nbf = (int)Lf->boxes.size();
+    std::vector<std::vector<CfRegion>> per(nbf);
+    auto one_box = [&](int b, int&) -> std::string {
+        std::vector<CfRegion>& regs = per[(size_t)b];
         const bamrex_box& B = Lf->boxes[b];
         for (int d = 0; d < Lf->D; ++d) {
             const int dlo = Lf->domain.lo[d], dhi = Lf->domain.hi[d], len = dhi - dlo + 1;
@@ -391,7 +394,13 @@ void build_ghost_regions(const bamrex_level* Lf, const BoxIndex& fidx, std::vect
                 for (const auto& p : pieces) regs.push_back(make_region(b, p, shift));
             }
         }
-    }
+        return std::string();
+    };
+    parallel_items<int>(nbf, table_threads((long long)nbf * 4096), 16, one_box);
+    size_t n = 0;
+    for (const auto& v : per) n += v.size();
+    regs.reserve(regs.size() + n);
+    for (const auto& v : per) regs.insert(regs.end(), v.begin(), v.end());
 }
 
 // Flux-register slots of direction d. The fine boxes run on host threads,
@@ -457,32 +466,49 @@ int build_register(const bamrex_coupling* C, int d, const BoxIndex& fidx, const 
     };
     long long work = 0;
     for (const auto& B : Lf->boxes) work += box_volume(B) / std::max(1, B.hi[d] - B.lo[d] + 1);
+    ProfPhases phase("registers:boxes");
     BX_TRY(parallel_items<OwnerScratch>(nbf, table_threads(work), 4, box));
-    size_t n = 0;
-    for (int b = 0; b < nbf; ++b) n += rrb[b].size();
-    rr.reserve(n);
-    cf.reserve(n);
-    ff.reserve(n * tx * ty * tz);
-    for (int b = 0; b < nbf; ++b) {
-        rr.insert(rr.end(), rrb[b].begin(), rrb[b].end());
-        cf.insert(cf.end(), cfb[b].begin(), cfb[b].end());
-        ff.insert(ff.end(), ffb[b].begin(), ffb[b].end());
-    }
+    phase.next("registers:join");
+    // join in box order, the boxes' lists copied on host threads
+    std::vector<size_t> at(nbf + 1, 0);
+    for (int b = 0; b < nbf; ++b) at[b + 1] = at[b] + rrb[b].size();
+    const size_t n = at[nbf], per_rec = (size_t)tx * ty * tz;
+    rr.resize(n);
+    cf.resize(n);
+    ff.resize(n * per_rec);
+    const int jt = table_threads((long long)n);
+    parallel_items<int>(nbf, jt, 16, [&](int b, int&) -> std::string {
+        std::copy(rrb[b].begin(), rrb[b].end(), rr.begin() + at[b]);
+        std::copy(cfb[b].begin(), cfb[b].end(), cf.begin() + at[b]);
+        std::copy(ffb[b].begin(), ffb[b].end(), ff.begin() + at[b] * per_rec);
+        return std::string();
+    });
+    phase.next("registers:dup");
     // a coarse cell may border the fine region on one side only: mark each
     // slot's cell in a bit map of the coarse domain (sorted keys where the
-    // domain is too large for one)
+    // domain is too large for one); marks by atomic OR on host threads
     const int* cl = Lc->domain.lo;
     const unsigned long long nx = Lc->domain.hi[0] - cl[0] + 1, ny = Lc->domain.hi[1] - cl[1] + 1,
                              nz = Lc->domain.hi[2] - cl[2] + 1;
     bool dup = false;
     if (nx * ny * nz <= (1ULL << 27)) {
         std::vector<unsigned long long> seen((nx * ny * nz + 63) / 64, 0ULL);
-        for (size_t q = 0; q < rr.size() && !dup; ++q) {
-            const unsigned long long key = ((unsigned long long)(rr[q].k - cl[2]) * ny + (rr[q].j - cl[1])) * nx + (rr[q].i - cl[0]);
-            const unsigned long long bit = 1ULL << (key & 63);
-            dup = (seen[key >> 6] & bit) != 0;
-            seen[key >> 6] |= bit;
-        }
+        std::atomic<bool> any(false);
+        constexpr size_t kChunk = 65536;
+        parallel_items<int>((int)((n + kChunk - 1) / kChunk), jt, 1, [&](int c, int&) -> std::string {
+            const size_t q1 = std::min(n, (size_t)(c + 1) * kChunk);
+            for (size_t q = (size_t)c * kChunk; q < q1; ++q) {
+                const unsigned long long key =
+                    ((unsigned long long)(rr[q].k - cl[2]) * ny + (rr[q].j - cl[1])) * nx + (rr[q].i - cl[0]);
+                const unsigned long long bit = 1ULL << (key & 63);
+                if (__atomic_fetch_or(&seen[key >> 6], bit, __ATOMIC_RELAXED) & bit) {
+                    any.store(true, std::memory_order_relaxed);
+                    break;
+                }
+            }
+            return std::string();
+        });
+        dup = any.load();
     } else {
         std::vector<unsigned long long> keys(rr.size());
         for (size_t q = 0; q < rr.size(); ++q)
@@ -995,7 +1021,6 @@ struct BlockedSpace {
     BoxIndex idx;
     Mask3 near_tag;   // a tag within n_error_buf of the footprint
     Mask3 allowed;    // 0 / 1, 2 = not evaluated yet
-    std::vector<int> hits;
 
     int cell(int d) const { return d < D ? c : 1; }
 
@@ -1039,10 +1064,13 @@ struct BlockedSpace {
                 for (int py = 0; py < np[1]; ++py)
                     for (int J = lo[1][py]; J <= hi[1][py]; ++J)
                         for (int px = 0; px < np[0]; ++px)
-                            for (int I = lo[0][px]; I <= hi[0][px]; ++I) near_tag.at(I, J, K) = 1;
+                            for (int I = lo[0][px]; I <= hi[0][px]; ++I)
+                                __atomic_store_n(&near_tag.at(I, J, K), (unsigned char)1, __ATOMIC_RELAXED);
     }
 
-    bool is_allowed(int I, int J, int K)
+    // the cache entry of (I, J, K) is written by its caller only; hits:
+    // the caller's scratch
+    bool is_allowed(int I, int J, int K, std::vector<int>& hits)
     {
         unsigned char& v = allowed.at(I, J, K);
         if (v != 2) return v != 0;
@@ -1079,58 +1107,40 @@ struct Cluster {
     int D;
     std::vector<bamrex_box> out;
 
-    long long count(const bamrex_box& b) const
-    {
-        long long c = 0;
-        for (int k = b.lo[2]; k <= b.hi[2]; ++k)
-            for (int j = b.lo[1]; j <= b.hi[1]; ++j)
-                for (int i = b.lo[0]; i <= b.hi[0]; ++i) c += tags->at(i, j, k) ? 1 : 0;
-        return c;
-    }
-
-    bool shrink(bamrex_box& b) const
-    {
-        int lo[3] = { b.hi[0] + 1, b.hi[1] + 1, b.hi[2] + 1 }, hi[3] = { b.lo[0] - 1, b.lo[1] - 1, b.lo[2] - 1 };
-        bool any = false;
-        for (int k = b.lo[2]; k <= b.hi[2]; ++k)
-            for (int j = b.lo[1]; j <= b.hi[1]; ++j)
-                for (int i = b.lo[0]; i <= b.hi[0]; ++i)
-                    if (tags->at(i, j, k)) {
-                        any = true;
-                        const int c[3] = { i, j, k };
-                        for (int d = 0; d < 3; ++d) {
-                            lo[d] = std::min(lo[d], c[d]);
-                            hi[d] = std::max(hi[d], c[d]);
-                        }
-                    }
-        if (!any) return false;
-        for (int d = 0; d < 3; ++d) {
-            b.lo[d] = lo[d];
-            b.hi[d] = hi[d];
-        }
-        return true;
-    }
-
+    // One pass over b: the tag signatures along each direction, from which
+    // the tight bounding box (the first and last non-zero entries) and the
+    // tag count follow; the signatures of the tight box are the non-zero
+    // range of these, as no tag lies outside it.
     void run(bamrex_box b, int depth)
     {
-        if (!shrink(b)) return;
-        const long long vol = box_volume(b), nt = count(b);
-        bool all_unit = true;
-        for (int d = 0; d < D; ++d) all_unit = all_unit && b.hi[d] == b.lo[d];
-        if ((double)nt >= eff * (double)vol || all_unit || depth > 64) {
-            out.push_back(b);
-            return;
-        }
-        // signatures along each direction
         std::vector<long long> sig[3];
         for (int d = 0; d < D; ++d) sig[d].assign(b.hi[d] - b.lo[d] + 1, 0);
+        long long nt = 0;
         for (int k = b.lo[2]; k <= b.hi[2]; ++k)
             for (int j = b.lo[1]; j <= b.hi[1]; ++j)
                 for (int i = b.lo[0]; i <= b.hi[0]; ++i)
                     if (tags->at(i, j, k)) {
                         const int c[3] = { i, j, k };
                         for (int d = 0; d < D; ++d) sig[d][c[d] - b.lo[d]]++;
+                        ++nt;
                     }
+        if (nt == 0) return;
+        for (int d = 0; d < D; ++d) {
+            int f = 0, l = (int)sig[d].size() - 1;
+            while (sig[d][f] == 0) ++f;
+            while (sig[d][l] == 0) --l;
+            sig[d].erase(sig[d].begin() + l + 1, sig[d].end());
+            sig[d].erase(sig[d].begin(), sig[d].begin() + f);
+            b.hi[d] = b.lo[d] + l;
+            b.lo[d] += f;
+        }
+        const long long vol = box_volume(b);
+        bool all_unit = true;
+        for (int d = 0; d < D; ++d) all_unit = all_unit && b.hi[d] == b.lo[d];
+        if ((double)nt >= eff * (double)vol || all_unit || depth > 64) {
+            out.push_back(b);
+            return;
+        }
         int best_d = -1, best_cut = 0;
         // 1) a hole (zero signature) closest to the middle
         long long best_score = -1;
@@ -1187,12 +1197,13 @@ struct Cluster {
 
 // Split b until every piece lies inside the allowed blocked cells (pieces
 // with no allowed cell are dropped).
-void clip_to_allowed(BlockedSpace& bs, const bamrex_box& b, int D, std::vector<bamrex_box>& out)
+void clip_to_allowed(BlockedSpace& bs, const bamrex_box& b, int D, std::vector<bamrex_box>& out,
+                     std::vector<int>& hits)
 {
     long long nin = 0;
     for (int k = b.lo[2]; k <= b.hi[2]; ++k)
         for (int j = b.lo[1]; j <= b.hi[1]; ++j)
-            for (int i = b.lo[0]; i <= b.hi[0]; ++i) nin += bs.is_allowed(i, j, k) ? 1 : 0;
+            for (int i = b.lo[0]; i <= b.hi[0]; ++i) nin += bs.is_allowed(i, j, k, hits) ? 1 : 0;
     if (nin == 0) return;
     if (nin == box_volume(b)) {
         out.push_back(b);
@@ -1207,8 +1218,8 @@ void clip_to_allowed(BlockedSpace& bs, const bamrex_box& b, int D, std::vector<b
     bamrex_box a = b, c = b;
     a.hi[best_d] = b.lo[best_d] + len / 2 - 1;
     c.lo[best_d] = b.lo[best_d] + len / 2;
-    clip_to_allowed(bs, a, D, out);
-    clip_to_allowed(bs, c, D, out);
+    clip_to_allowed(bs, a, D, out, hits);
+    clip_to_allowed(bs, c, D, out, hits);
 }
 
 void chop(const bamrex_box& b, int D, int mgs, std::vector<bamrex_box>& out)
@@ -1277,15 +1288,28 @@ extern "C" int bamrex_cluster_tags(int D, const bamrex_box* domain, const int* p
     bs.idx.build(*domain, bxs, D);
     bs.near_tag.init(nt, 0);
     bs.allowed.init(nt, 2);
-    // runs of tagged cells along x, box by box in packed order
-    long long off = 0;
-    for (const auto& B : bxs) {
+    // runs of tagged cells along x, box by box in packed order, boxes on
+    // host threads (marks are idempotent stores of 1); zero words of eight
+    // tags are skipped whole
+    std::vector<long long> boff(bxs.size() + 1, 0);
+    for (size_t b = 0; b < bxs.size(); ++b) boff[b + 1] = boff[b] + box_volume(bxs[b]);
+    auto scan_box = [&](int b, int&) -> std::string {
+        const bamrex_box& B = bxs[(size_t)b];
         const int len = B.hi[0] - B.lo[0] + 1;
+        long long off = boff[(size_t)b];
         for (int k = B.lo[2]; k <= B.hi[2]; ++k)
             for (int j = B.lo[1]; j <= B.hi[1]; ++j) {
                 const char* row = tags + off;
                 off += len;
                 for (int i = 0; i < len;) {
+                    if (i + 8 <= len) {
+                        unsigned long long w;
+                        std::memcpy(&w, row + i, 8);
+                        if (!w) {
+                            i += 8;
+                            continue;
+                        }
+                    }
                     if (!row[i]) {
                         ++i;
                         continue;
@@ -1296,13 +1320,20 @@ extern "C" int bamrex_cluster_tags(int D, const bamrex_box* domain, const int* p
                     i = e + 1;
                 }
             }
-    }
+        return std::string();
+    };
+    BX_TRY(parallel_items<int>((int)bxs.size(), table_threads(boff.back() / 8), 8, scan_box));
+    phase.next("cluster_tags:allowed");
+    // blocked cells near a tag and allowed, planes of K on host threads
     Mask3 btag;
     btag.init(nt, 0);
-    for (int K = 0; K < nt[2]; ++K)
+    auto plane = [&](int K, std::vector<int>& hits) -> std::string {
         for (int J = 0; J < nt[1]; ++J)
             for (int I = 0; I < nt[0]; ++I)
-                if (bs.near_tag.at(I, J, K) && bs.is_allowed(I, J, K)) btag.at(I, J, K) = 1;
+                if (bs.near_tag.at(I, J, K) && bs.is_allowed(I, J, K, hits)) btag.at(I, J, K) = 1;
+        return std::string();
+    };
+    BX_TRY(parallel_items<std::vector<int>>(nt[2], table_threads((long long)nt[0] * nt[1] * nt[2] / 4), 1, plane));
     phase.next("cluster_tags:cluster");
     Cluster cl;
     cl.tags = &btag;
@@ -1315,8 +1346,18 @@ extern "C" int bamrex_cluster_tags(int D, const bamrex_box* domain, const int* p
     }
     cl.run(all, 0);
     phase.next("cluster_tags:clip_chop");
+    // the clusters are disjoint, so each blocked cell's cache entry is
+    // evaluated by one thread; pieces joined in cluster order
+    std::vector<std::vector<bamrex_box>> pieces(cl.out.size());
+    long long cvol = 0;
+    for (const auto& b : cl.out) cvol += box_volume(b);
+    BX_TRY(parallel_items<std::vector<int>>((int)cl.out.size(), table_threads(cvol / 4), 4,
+                                            [&](int q, std::vector<int>& hits) -> std::string {
+                                                clip_to_allowed(bs, cl.out[(size_t)q], D, pieces[(size_t)q], hits);
+                                                return std::string();
+                                            }));
     std::vector<bamrex_box> clipped, chopped;
-    for (const auto& b : cl.out) clip_to_allowed(bs, b, D, clipped);
+    for (const auto& p : pieces) clipped.insert(clipped.end(), p.begin(), p.end());
     const int mgs_t = max_grid_size / blocking_factor;
     for (const auto& b : clipped) chop(b, D, mgs_t, chopped);
     std::sort(chopped.begin(), chopped.end(), [](const bamrex_box& a, const bamrex_box& b) {
@@ -1444,7 +1485,10 @@ bool same_boxes(const std::vector<bamrex_box>& a, const std::vector<bamrex_box>&
     return true;
 }
 
-int set_level(bamrex_amr* A, int lev, const std::vector<bamrex_box>& boxes)
+// defer_finer: leave the next finer level uncoupled (cpl[lev + 1] null) for
+// couple_missing, as a regrid about to replace that level would throw the
+// coupling away
+int set_level(bamrex_amr* A, int lev, const std::vector<bamrex_box>& boxes, bool defer_finer = false)
 {
     const int finest = (int)A->levels.size() - 1;
     if (lev < 1 || lev > finest + 1 || lev > A->desc.max_level) return amr_fail(A, BAMREX_ERR_ARG, "level out of range");
@@ -1529,7 +1573,7 @@ int set_level(bamrex_amr* A, int lev, const std::vector<bamrex_box>& boxes)
     if (lev + 1 <= finest) {
         bamrex_coupling_destroy(A->cpl[lev + 1]);
         A->cpl[lev + 1] = nullptr;
-        keep_finer = bamrex_coupling_create(&C2, L, A->levels[lev + 1], A->desc.ref_ratio) == BAMREX_OK;
+        keep_finer = defer_finer || bamrex_coupling_create(&C2, L, A->levels[lev + 1], A->desc.ref_ratio) == BAMREX_OK;
     }
     phase.next("amr_set_level:destroy_old");
     if (lev <= finest) {
@@ -1545,6 +1589,24 @@ int set_level(bamrex_amr* A, int lev, const std::vector<bamrex_box>& boxes)
     if (lev + 1 <= finest) {
         if (keep_finer) A->cpl[lev + 1] = C2;
         else drop_levels_above(A, lev);
+    }
+    return BAMREX_OK;
+}
+
+// Couple every level from 1 to upto (at most the finest) that a deferred
+// set_level left uncoupled; a level that is not properly nested in the one
+// below goes, with everything above it.
+int couple_missing(bamrex_amr* A, int upto)
+{
+    for (int l = 1; l <= upto && l < (int)A->levels.size(); ++l) {
+        if (A->cpl[l]) continue;
+        bamrex_coupling* C = nullptr;
+        if (bamrex_coupling_create(&C, A->levels[l - 1], A->levels[l], A->desc.ref_ratio) == BAMREX_OK) {
+            A->cpl[l] = C;
+        } else {
+            drop_levels_above(A, l - 1);
+            break;
+        }
     }
     return BAMREX_OK;
 }
@@ -1577,11 +1639,12 @@ int level_tags(bamrex_amr* A, int l, double time, std::vector<char>& tags)
     return BAMREX_OK;
 }
 
-int regrid(bamrex_amr* A, int lbase, double time)
+int regrid_levels(bamrex_amr* A, int lbase, double time)
 {
-    BX_PROFILE("amr_regrid");
     const bamrex_amr_desc& d = A->desc;
     for (int l = lbase; l < d.max_level && l < (int)A->levels.size(); ++l) {
+        BX_TRY(couple_missing(A, l));  // level l's ghost fill needs its coupling
+        if (l >= (int)A->levels.size()) break;
         std::vector<char> tags;
         BX_TRY(level_tags(A, l, time, tags));
         bamrex_level* L = A->levels[l];
@@ -1601,9 +1664,20 @@ int regrid(bamrex_amr* A, int lbase, double time)
             drop_levels_above(A, l);
             break;
         }
-        BX_TRY(set_level(A, l + 1, nb));
+        BX_TRY(set_level(A, l + 1, nb, true));
     }
     return BAMREX_OK;
+}
+
+// Regrid levels lbase+1 and up: every level replaced defers the coupling of
+// the one above it, which the next round of the loop usually replaces too;
+// what is left uncoupled is coupled at the end, on every path.
+int regrid(bamrex_amr* A, int lbase, double time)
+{
+    BX_PROFILE("amr_regrid");
+    const int rc = regrid_levels(A, lbase, time);
+    const int rc2 = couple_missing(A, (int)A->levels.size() - 1);
+    return rc != BAMREX_OK ? rc : rc2;
 }
 
 int compute_dt(bamrex_amr* A, double time, double stop_time, bool initial, bool post_regrid)

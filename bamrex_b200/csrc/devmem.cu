@@ -2,10 +2,13 @@
 // in devmem.h).
 #include "devmem.h"
 
+#include <chrono>
 #include <cstdint>
 #include <mutex>
 #include <unordered_map>
 #include <vector>
+
+#include "profiler.h"
 
 namespace bamrex {
 namespace {
@@ -14,11 +17,34 @@ constexpr int kMaxDevices = 64;
 constexpr size_t kPinnedBlock = 4096;
 constexpr size_t kPinnedSlab = 64 * kPinnedBlock;
 
+// Blocks of kCacheMin bytes and more keep their pages and addresses after
+// dev_free: up to kCacheBlocks per device wait here, whole, for a request
+// of their size class or a little below (kCacheSlack).  Handing a large
+// range back to the pool and taking it out again costs the pool about as
+// much as mapping it afresh (a third of a second for a 10 GB level arena,
+// measured), where reusing a kept block costs nothing.
+constexpr size_t kCacheMin = size_t(64) << 20;
+constexpr int kCacheBlocks = 8;
+constexpr size_t kCacheSlack = 4;  // a kept block serves requests down to 3/4 of its size
+
+struct Block {
+    int dev = -1;
+    size_t bytes = 0;
+};
+
+struct Kept {
+    void* p;
+    size_t bytes;
+    unsigned long long stamp;  // order of keeping: the oldest goes first
+};
+
 struct Pools {
     std::mutex mu;
     cudaMemPool_t pool[kMaxDevices] = {};
     long long live[kMaxDevices] = {};
-    std::unordered_map<void*, int> owner;  // block -> device
+    std::unordered_map<void*, Block> owner;  // block -> device and size
+    std::vector<Kept> kept[kMaxDevices];
+    unsigned long long stamp = 0;
     std::vector<void*> pinned_free;
 };
 
@@ -66,6 +92,20 @@ size_t size_class(size_t bytes)
     return (bytes + step - 1) / step * step;
 }
 
+// Kept blocks of device `dev` back to its pool (they are idle: dev_free
+// synchronised the device before keeping them); called with P.mu held.
+void release_kept(Pools& P, int dev)
+{
+    if (P.kept[dev].empty()) return;
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (cur != dev) cudaSetDevice(dev);
+    for (const Kept& k : P.kept[dev]) cudaFreeAsync(k.p, 0);
+    P.kept[dev].clear();
+    cudaStreamSynchronize(0);
+    if (cur != dev && cur >= 0) cudaSetDevice(cur);
+}
+
 }  // namespace
 
 cudaError_t dev_alloc(void** p, size_t bytes, cudaStream_t s)
@@ -80,12 +120,56 @@ cudaError_t dev_alloc(void** p, size_t bytes, cudaStream_t s)
     {
         std::lock_guard<std::mutex> g(P.mu);
         e = device_pool(P, dev, &pool);
+        if (e != cudaSuccess) return e;
+        if (bytes >= kCacheMin) {
+            // the smallest kept block that fits and is not much larger
+            std::vector<Kept>& K = P.kept[dev];
+            int best = -1;
+            for (int i = 0; i < (int)K.size(); ++i)
+                if (K[i].bytes >= bytes && K[i].bytes - K[i].bytes / kCacheSlack <= bytes &&
+                    (best < 0 || K[i].bytes < K[best].bytes))
+                    best = i;
+            if (best >= 0) {
+                BX_PROFILE("dev_alloc:kept");
+                *p = K[best].p;
+                P.owner[*p] = Block{ dev, K[best].bytes };
+                K.erase(K.begin() + best);
+                ++P.live[dev];
+                return cudaSuccess;
+            }
+        }
     }
-    if (e != cudaSuccess) return e;
+    // profiled: whether the pool had to map pages for the block (grow) or
+    // handed out pages it kept (reuse), and the wait for the stream
+    const bool prof = g_profile_on.load(std::memory_order_relaxed) != 0;
+    uint64_t res0 = 0, res1 = 0;
+    std::chrono::steady_clock::time_point t0;
+    if (prof) {
+        cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &res0);
+        t0 = std::chrono::steady_clock::now();
+    }
     e = cudaMallocFromPoolAsync(p, bytes ? bytes : 1, pool, s);
+    if (e == cudaErrorMemoryAllocation) {
+        // the kept blocks' pages may be what is missing: give them to the
+        // pool and try once more
+        cudaGetLastError();
+        bool had = false;
+        {
+            std::lock_guard<std::mutex> g(P.mu);
+            had = !P.kept[dev].empty();
+            release_kept(P, dev);
+        }
+        if (had) e = cudaMallocFromPoolAsync(p, bytes ? bytes : 1, pool, s);
+    }
     if (e != cudaSuccess) {
         *p = nullptr;
         return e;
+    }
+    if (prof) {
+        const auto t1 = std::chrono::steady_clock::now();
+        cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &res1);
+        profile_record(res1 > res0 ? "dev_alloc:pool_grow" : "dev_alloc:pool_reuse",
+                       std::chrono::duration<double>(t1 - t0).count());
     }
     // the tables are uploaded with copies outside `s`: the block must be
     // ready for every stream when this returns
@@ -96,7 +180,7 @@ cudaError_t dev_alloc(void** p, size_t bytes, cudaStream_t s)
         return e;
     }
     std::lock_guard<std::mutex> g(P.mu);
-    P.owner[*p] = dev;
+    P.owner[*p] = Block{ dev, bytes ? bytes : 1 };
     ++P.live[dev];
     return cudaSuccess;
 }
@@ -105,23 +189,36 @@ void dev_free(void* p, cudaStream_t s)
 {
     if (!p) return;
     Pools& P = pools();
-    int dev = -1;
+    Block b;
     {
         std::lock_guard<std::mutex> g(P.mu);
         auto it = P.owner.find(p);
         if (it != P.owner.end()) {
-            dev = it->second;
+            b = it->second;
             P.owner.erase(it);
         }
     }
-    if (dev < 0) return;  // not a pooled block
+    if (b.dev < 0) return;  // not a pooled block
     // as cudaFree: every stream's work on the block (table uploads and
     // memsets on the default stream, copies on helper streams) is finished
     // before the block can be handed out again or its pages released
     cudaDeviceSynchronize();
-    cudaFreeAsync(p, s);
     std::lock_guard<std::mutex> g(P.mu);
-    --P.live[dev];
+    --P.live[b.dev];
+    if (b.bytes >= kCacheMin) {
+        std::vector<Kept>& K = P.kept[b.dev];
+        K.push_back(Kept{ p, b.bytes, ++P.stamp });
+        if ((int)K.size() > kCacheBlocks) {
+            // the block kept longest goes back to the pool
+            int old = 0;
+            for (int i = 1; i < (int)K.size(); ++i)
+                if (K[i].stamp < K[old].stamp) old = i;
+            cudaFreeAsync(K[old].p, s);
+            K.erase(K.begin() + old);
+        }
+        return;
+    }
+    cudaFreeAsync(p, s);
 }
 
 int release_pooled()
@@ -129,8 +226,11 @@ int release_pooled()
     Pools& P = pools();
     std::lock_guard<std::mutex> g(P.mu);
     cudaError_t e = cudaDeviceSynchronize();
-    for (int d = 0; d < kMaxDevices && e == cudaSuccess; ++d)
-        if (P.pool[d]) e = cudaMemPoolTrimTo(P.pool[d], 0);
+    for (int d = 0; d < kMaxDevices && e == cudaSuccess; ++d) {
+        if (!P.pool[d]) continue;
+        release_kept(P, d);
+        e = cudaMemPoolTrimTo(P.pool[d], 0);
+    }
     return e == cudaSuccess ? 0 : (int)e;
 }
 

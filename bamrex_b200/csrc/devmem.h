@@ -7,8 +7,10 @@
 // from a millisecond to, on a loaded host, hundreds. These helpers take the
 // blocks from a stream-ordered pool per device that keeps freed blocks
 // (release threshold = unlimited), so the next level reuses the same pages,
-// also across hierarchies created one after the other.  The pages go back
-// to the driver at process exit or when release_pooled() is called.
+// also across hierarchies created one after the other.  Freed blocks of
+// 64 MiB and more are kept whole (a few per device) and handed out again
+// as they are, which spares the pool re-dealing a large range.  The pages
+// go back to the driver at process exit or when release_pooled() is called.
 #pragma once
 
 #include <cuda_runtime.h>

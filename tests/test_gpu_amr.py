@@ -216,6 +216,54 @@ def test_tagging_matches_oracle(torch_cuda, oracle):
         assert 0 < x.sum() < x.size
 
 
+def test_regrid_keeps_fine_data_where_the_coarse_level_moved(torch_cuda, oracle):
+    """A regrid that moves level 1 away from part of level 2: the new level
+    2 takes the old level-2 values wherever its cells were level-2 cells
+    before (AMReX's regrid fills a remade level from its old data first,
+    Amr::regrid -> AmrLevel::init(old)), even though the old level 2 is not
+    properly nested in the new level 1, and the hierarchy steps on."""
+    import bamrex_b200 as bx
+    from bamrex_b200.amr import Amr
+    D, n = 2, 64
+    hi0 = (n - 1, n - 1, 0)
+    A = Amr(D, (0, 0, 0), hi0, [0.0] * 3, [1.0] * 3, oracle.decompose(D, (0, 0, 0), hi0, 32), bx.Parm(D),
+            max_level=2, blocking_factor=8, max_grid_size=32, n_error_buf=2, phierr=[1.5, 1.5], phierr_var=0)
+
+    def state(lev, c0):
+        # a dense square over coarse cells [c0, c0 + 16)^2 at rest, p = 1
+        m, s = n * 2 ** lev, 2 ** lev
+        u = np.zeros((4, 1, m, m))
+        u[0] = 1.0
+        u[3] = 2.5
+        u[0, 0, c0 * s:(c0 + 16) * s, c0 * s:(c0 + 16) * s] = 2.0
+        return u
+
+    try:
+        A.init(lambda amr, lev: state(lev, 16))
+        assert A.finest_level == 2
+        # a fine-scale energy pattern on level 2 that no interpolation from
+        # level 1 reproduces
+        pat = A.get_state(2)
+        j, i = np.indices(pat.shape[2:])
+        pat[3, 0] += 0.01 * ((i + 2 * j) % 3)
+        A.set_state(2, pat)
+        A.set_state(0, state(0, 24))
+        A.set_state(1, state(1, 24))
+        old1 = A.boxes(1)
+        A.regrid(0)
+        assert A.finest_level == 2 and A.boxes(1) != old1
+        new2 = A.get_state(2)
+        kept = ~np.isnan(new2[0]) & ~np.isnan(pat[0])
+        assert kept.any() and (~np.isnan(new2[0]) & np.isnan(pat[0])).any()
+        np.testing.assert_array_equal(new2[:, kept], pat[:, kept])
+        A.coarse_step()
+        for lev in range(3):
+            s = A.get_state(lev)
+            assert np.isfinite(s[:, ~np.isnan(s[0])]).all()
+    finally:
+        A.close()
+
+
 def test_blast_regrid_and_step(torch_cuda, oracle):
     """The spherical-blast hierarchy: tag (grad_error >= 0.1 on the
     pressure; the initial density is uniform), build levels 1 and 2 from the

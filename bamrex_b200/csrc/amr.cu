@@ -17,6 +17,7 @@
 #include <string>
 #include <thread>
 #include <tuple>
+#include <utility>
 #include <vector>
 
 #include "amr.h"
@@ -403,10 +404,43 @@ void build_ghost_regions(const bamrex_level* Lf, const BoxIndex& fidx, std::vect
     for (const auto& v : per) regs.insert(regs.end(), v.begin(), v.end());
 }
 
+// An allocator whose resize() leaves new elements uninitialised, so that a
+// joined table of records is written (and its pages first touched) once,
+// by the threads that copy into it.
+template <class T>
+struct NoInit : std::allocator<T> {
+    template <class U>
+    struct rebind {
+        using other = NoInit<U>;
+    };
+    NoInit() = default;
+    template <class U>
+    NoInit(const NoInit<U>&) noexcept
+    {
+    }
+    template <class U, class... Args>
+    void construct(U* p, Args&&... args)
+    {
+        if constexpr (sizeof...(Args) == 0) ::new ((void*)p) U;
+        else ::new ((void*)p) U(std::forward<Args>(args)...);
+    }
+};
+using FaceRecs = std::vector<FaceRec, NoInit<FaceRec>>;
+using RefluxRecs = std::vector<RefluxRec, NoInit<RefluxRec>>;
+
+// The bit map of a coarse domain for the duplicate-slot check, one per host
+// thread that builds couplings, kept between calls and left all zero.
+std::vector<unsigned long long>& slot_bitmap(size_t words)
+{
+    thread_local std::vector<unsigned long long> bits;
+    if (bits.size() < words) bits.assign(words, 0ULL);
+    return bits;
+}
+
 // Flux-register slots of direction d. The fine boxes run on host threads,
 // each filling its own record lists, which are then joined in box order.
-int build_register(const bamrex_coupling* C, int d, const BoxIndex& fidx, const BoxIndex& cidx,
-                   std::vector<FaceRec>& cf, std::vector<FaceRec>& ff, std::vector<RefluxRec>& rr)
+int build_register(const bamrex_coupling* C, int d, const BoxIndex& fidx, const BoxIndex& cidx, FaceRecs& cf,
+                   FaceRecs& ff, RefluxRecs& rr)
 {
     const bamrex_level* Lf = C->fine;
     const bamrex_level* Lc = C->crse;
@@ -492,20 +526,25 @@ int build_register(const bamrex_coupling* C, int d, const BoxIndex& fidx, const 
                              nz = Lc->domain.hi[2] - cl[2] + 1;
     bool dup = false;
     if (nx * ny * nz <= (1ULL << 27)) {
-        std::vector<unsigned long long> seen((nx * ny * nz + 63) / 64, 0ULL);
+        std::vector<unsigned long long>& seen = slot_bitmap((nx * ny * nz + 63) / 64);
         std::atomic<bool> any(false);
         constexpr size_t kChunk = 65536;
-        parallel_items<int>((int)((n + kChunk - 1) / kChunk), jt, 1, [&](int c, int&) -> std::string {
+        const int nchunk = (int)((n + kChunk - 1) / kChunk);
+        auto key_of = [&](size_t q) {
+            return ((unsigned long long)(rr[q].k - cl[2]) * ny + (rr[q].j - cl[1])) * nx + (rr[q].i - cl[0]);
+        };
+        parallel_items<int>(nchunk, jt, 1, [&](int c, int&) -> std::string {
             const size_t q1 = std::min(n, (size_t)(c + 1) * kChunk);
             for (size_t q = (size_t)c * kChunk; q < q1; ++q) {
-                const unsigned long long key =
-                    ((unsigned long long)(rr[q].k - cl[2]) * ny + (rr[q].j - cl[1])) * nx + (rr[q].i - cl[0]);
-                const unsigned long long bit = 1ULL << (key & 63);
-                if (__atomic_fetch_or(&seen[key >> 6], bit, __ATOMIC_RELAXED) & bit) {
-                    any.store(true, std::memory_order_relaxed);
-                    break;
-                }
+                const unsigned long long key = key_of(q), bit = 1ULL << (key & 63);
+                if (__atomic_fetch_or(&seen[key >> 6], bit, __ATOMIC_RELAXED) & bit) any.store(true, std::memory_order_relaxed);
             }
+            return std::string();
+        });
+        // back to all zero: only the words the slots touched
+        parallel_items<int>(nchunk, jt, 1, [&](int c, int&) -> std::string {
+            const size_t q1 = std::min(n, (size_t)(c + 1) * kChunk);
+            for (size_t q = (size_t)c * kChunk; q < q1; ++q) __atomic_store_n(&seen[key_of(q) >> 6], 0ULL, __ATOMIC_RELAXED);
             return std::string();
         });
         dup = any.load();
@@ -593,8 +632,8 @@ extern "C" int bamrex_coupling_create(bamrex_coupling** out, bamrex_level* crse,
 
     phase.next("coupling_create:registers");
     // flux registers
-    std::vector<FaceRec> cf[3], ff[3];
-    std::vector<RefluxRec> rr[3];
+    FaceRecs cf[3], ff[3];
+    RefluxRecs rr[3];
     for (int d = 0; d < D; ++d) BX_TRY(build_register(C.get(), d, fidx, cidx, cf[d], ff[d], rr[d]));
 
     phase.next("coupling_create:avg_down");

@@ -1044,17 +1044,31 @@ extern "C" int bamrex_level_create(bamrex_level** out, const bamrex_level_desc* 
         }
     }
 
-    // ---- items and segment lengths
+    // ---- items and segment lengths (each choice computed once)
+    int memo_reg[3][2], memo_tma[3][2];
+    for (int d = 0; d < 3; ++d)
+        for (int w = 0; w < 2; ++w) memo_reg[d][w] = memo_tma[d][w] = -1;
+    auto reg_seg = [&](int d, bool march) {
+        int& m = memo_reg[d][march ? 1 : 0];
+        if (m < 0) m = choose_seglen(d, L->boxes, sweep_resident_warps(D, d, L->method, L->fp32, L->k, march), march);
+        return m;
+    };
+    auto tma_seg = [&](int d, bool wave) {
+        int& m = memo_tma[d][wave ? 1 : 0];
+        if (m < 0) {
+            const int lim = fast_limiter(D, L->method, L->k);
+            m = choose_tma_seglen(D, d, L->boxes, sweep_tma_resident_units(D, d, L->fp32, lim, wave), wave);
+        }
+        return m;
+    };
     std::vector<SweepBox> sweep_host[3];
     // x-sweep kernel: one warp per row segment, or one thread per row
     // (levels of narrow boxes); automatic by the lane-slot estimate
     if (desc->x_mode == BAMREX_XSWEEP_MARCH) L->x_march = D >= 2;
     else if (desc->x_mode == BAMREX_XSWEEP_ROWS) L->x_march = false;
     else {
-        const int sr = desc->x_segment > 0 ? (int)align_up((size_t)desc->x_segment, 32)
-                                           : choose_seglen(0, L->boxes, sweep_resident_warps(D, 0, L->method, L->fp32, L->k));
-        const int sm = desc->x_segment > 0 ? desc->x_segment
-                                           : choose_seglen(0, L->boxes, sweep_resident_warps(D, 0, L->method, L->fp32, L->k, true), true);
+        const int sr = desc->x_segment > 0 ? (int)align_up((size_t)desc->x_segment, 32) : reg_seg(0, false);
+        const int sm = desc->x_segment > 0 ? desc->x_segment : reg_seg(0, true);
         L->x_march = prefer_x_march(D, L->boxes, sr, sm);
     }
     for (int d = 0; d < D; ++d) {
@@ -1063,12 +1077,10 @@ extern "C" int bamrex_level_create(bamrex_level** out, const bamrex_level_desc* 
             L->sweep_kind[d] = BAMREX_STAGING_REGISTERS;
             continue;
         }
-        const int lim = fast_limiter(D, L->method, L->k);
         auto seg_for = [&](bool tma_kind, bool wave, bool march) {
             const int user = d == 0 ? desc->x_segment : desc->s_segment;
             if (user > 0) return user;
-            if (tma_kind) return choose_tma_seglen(D, d, L->boxes, sweep_tma_resident_units(D, d, L->fp32, lim, wave), wave);
-            return choose_seglen(d, L->boxes, sweep_resident_warps(D, d, L->method, L->fp32, L->k, march), march);
+            return tma_kind ? tma_seg(d, wave) : reg_seg(d, march);
         };
         const int sr = d == 0 ? (int)align_up((size_t)seg_for(false, false, false), 32) : 0;
         const int sm = seg_for(false, false, d == 0);
@@ -1077,12 +1089,8 @@ extern "C" int bamrex_level_create(bamrex_level** out, const bamrex_level_desc* 
     }
     for (int d = 0; d < D; ++d) {
         const bool march = d == 0 && L->x_march;
-        const int lim = fast_limiter(D, L->method, L->k);
         L->seglen[d] = d == 0 ? desc->x_segment : desc->s_segment;
-        if (L->seglen[d] <= 0)
-            L->seglen[d] = L->tma(d) ? choose_tma_seglen(D, d, L->boxes,
-                                                         sweep_tma_resident_units(D, d, L->fp32, lim, L->wave(d)), L->wave(d))
-                                     : choose_seglen(d, L->boxes, sweep_resident_warps(D, d, L->method, L->fp32, L->k, march), march);
+        if (L->seglen[d] <= 0) L->seglen[d] = L->tma(d) ? tma_seg(d, L->wave(d)) : reg_seg(d, march);
         if (d == 0 && !march && !L->tma(d)) L->seglen[d] = (int)align_up((size_t)L->seglen[d], 32);
         long long acc = 0;
         for (int b = 0; b < nb; ++b) {

@@ -24,7 +24,7 @@ constexpr size_t kPinnedSlab = 64 * kPinnedBlock;
 // much as mapping it afresh (a third of a second for a 10 GB level arena,
 // measured), where reusing a kept block costs nothing.
 constexpr size_t kCacheMin = size_t(64) << 20;
-constexpr int kCacheBlocks = 8;
+constexpr int kCacheBlocks = 16;
 constexpr size_t kCacheSlack = 4;  // a kept block serves requests down to 3/4 of its size
 
 struct Block {
@@ -110,7 +110,12 @@ void release_kept(Pools& P, int dev)
 
 cudaError_t dev_alloc(void** p, size_t bytes, cudaStream_t s)
 {
+    // a kept block is looked for at the request's size class; a large block
+    // taken from the pool is made one eighth larger, so that the kept block
+    // of a level that grows a little at every regrid still fits the level
+    // two regrids on
     bytes = size_class(bytes);
+    const size_t alloc = bytes >= kCacheMin ? size_class(bytes + bytes / 8) : bytes;
     *p = nullptr;
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
@@ -148,10 +153,11 @@ cudaError_t dev_alloc(void** p, size_t bytes, cudaStream_t s)
         cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &res0);
         t0 = std::chrono::steady_clock::now();
     }
-    e = cudaMallocFromPoolAsync(p, bytes ? bytes : 1, pool, s);
+    size_t got = alloc ? alloc : 1;
+    e = cudaMallocFromPoolAsync(p, got, pool, s);
     if (e == cudaErrorMemoryAllocation) {
         // the kept blocks' pages may be what is missing: give them to the
-        // pool and try once more
+        // pool and try once more, then without the extra eighth
         cudaGetLastError();
         bool had = false;
         {
@@ -159,7 +165,12 @@ cudaError_t dev_alloc(void** p, size_t bytes, cudaStream_t s)
             had = !P.kept[dev].empty();
             release_kept(P, dev);
         }
-        if (had) e = cudaMallocFromPoolAsync(p, bytes ? bytes : 1, pool, s);
+        if (had) e = cudaMallocFromPoolAsync(p, got, pool, s);
+        if (e == cudaErrorMemoryAllocation && alloc > bytes) {
+            cudaGetLastError();
+            got = bytes ? bytes : 1;
+            e = cudaMallocFromPoolAsync(p, got, pool, s);
+        }
     }
     if (e != cudaSuccess) {
         *p = nullptr;
@@ -180,7 +191,7 @@ cudaError_t dev_alloc(void** p, size_t bytes, cudaStream_t s)
         return e;
     }
     std::lock_guard<std::mutex> g(P.mu);
-    P.owner[*p] = Block{ dev, bytes ? bytes : 1 };
+    P.owner[*p] = Block{ dev, got };
     ++P.live[dev];
     return cudaSuccess;
 }

@@ -817,6 +817,17 @@ int level_fill(bamrex_level* L, int d, int parity, const StepScalars* scal)
                         "ghost fill");
 }
 
+// The x ghost fill of a step: without the slabs the x sweep (and the x
+// flux-register faces) read from the neighbouring boxes.
+int level_fill_step_x(bamrex_level* L, int parity, const StepScalars* scal)
+{
+    if (!x_halos_fused(L)) return level_fill(L, 0, parity, scal);
+    if (L->nghost_x == 0) return BAMREX_OK;
+    return level_launch(L, launch_ghost_fill(L->NC, L->fp32, L->d_ghost_x, L->nghost_x, L->ghost_chunks_x, L->d_fab[parity],
+                                             scal, L->stream),
+                        "ghost fill");
+}
+
 int level_sweep(bamrex_level* L, int d, int parity, double dt_host, const StepScalars* scal, bool reduce_ws,
                 bool allow_timing, int part)
 {
@@ -840,6 +851,7 @@ int level_sweep(bamrex_level* L, int d, int parity, double dt_host, const StepSc
     a.k = L->k;
     a.ws_max = reduce_ws ? &L->d_scal->ws_bits : nullptr;
     a.do_update = 1;
+    a.xnb_on = d == 0 && x_halos_fused(L) ? 1 : 0;
     const bool t = allow_timing && L->timing && L->ev_used < L->events.size();
     if (t) cudaEventRecord(L->events[L->ev_used].first, L->stream);
     int rc;
@@ -864,7 +876,7 @@ int level_step(bamrex_level* L, int parity, double dt_host, StepScalars* scal, b
     // with a rigid body: FillPatch, fill_ghost_rb and fill_consv_boundary
     // (AmrLevelAdv_advance.cpp:108-116) fill every ghost cell first
     if (L->body) BX_TRY(body_fill(L, parity, scal));
-    else BX_TRY(level_fill(L, 0, parity, scal));
+    else BX_TRY(level_fill_step_x(L, parity, scal));
     int p = parity;
     for (int d = 0; d < L->D; ++d) {
         BX_TRY(level_sweep(L, d, p, dt_host, scal, d == L->D - 1, allow_timing));
@@ -884,7 +896,8 @@ int level_step(bamrex_level* L, int parity, double dt_host, StepScalars* scal, b
             for (const RegisterTask& t : L->reg_tasks[d])
                 BX_TRY(level_launch(L, launch_register_faces(L->D, d, L->method, L->fp32, L->k, L->d_fab[p], t, L->NC,
                                                              dt_host, L->dx[d], scale, scal, area[0], area[1],
-                                                             L->stream),
+                                                             L->stream,
+                                                             d == 0 && x_halos_fused(L) ? L->d_sweep[0][p] : nullptr),
                                     "flux register faces"));
         }
         p ^= 1;
@@ -1137,6 +1150,53 @@ extern "C" int bamrex_level_create(bamrex_level** out, const bamrex_level_desc* 
         }
     }
 
+    // ---- x halos read in place by the marching x sweep: per box and side,
+    // the same-level box that holds the box's whole x ghost slab (inside the
+    // domain); the step's x fill then leaves those slabs out
+    std::vector<int> xnb[2];
+    std::vector<GhostOp> ghost_x;
+    if (D >= 2 && L->x_march && !L->tma(0)) {
+        for (int side = 0; side < 2; ++side) xnb[side].assign((size_t)nb, -1);
+        std::vector<int> hits;
+        int nfused = 0;
+        for (int b = 0; b < nb; ++b)
+            for (int side = 0; side < 2; ++side) {
+                bamrex_box slab = L->boxes[b];
+                if (side == 0) {
+                    slab.hi[0] = slab.lo[0] - 1;
+                    slab.lo[0] -= g;
+                } else {
+                    slab.lo[0] = slab.hi[0] + 1;
+                    slab.hi[0] += g;
+                }
+                if (slab.lo[0] < L->domain.lo[0] || slab.hi[0] > L->domain.hi[0]) continue;
+                bidx.query(slab.lo, slab.hi, hits);
+                for (int q : hits) {
+                    const bamrex_box& Q = L->boxes[q];
+                    bool in = q != b;
+                    for (int e = 0; e < 3 && in; ++e) in = Q.lo[e] <= slab.lo[e] && slab.hi[e] <= Q.hi[e];
+                    if (in) {
+                        xnb[side][(size_t)b] = q;
+                        ++nfused;
+                        break;
+                    }
+                }
+            }
+        if (nfused) {
+            L->x_fused = true;
+            for (const GhostOp& op : ghost_host[0]) {
+                bool plain = op.src != op.dst && op.negmask == 0;
+                for (int e = 0; e < 3; ++e) plain = plain && op.mul[e] == 1 && op.off[e] == 0;
+                const bamrex_box& Bd = L->boxes[op.dst];
+                const bool below = plain && op.src == xnb[0][(size_t)op.dst] && op.hi[0] < Bd.lo[0];
+                const bool above = plain && op.src == xnb[1][(size_t)op.dst] && op.lo[0] > Bd.hi[0];
+                if (!below && !above) ghost_x.push_back(op);
+            }
+            L->nghost_x = (int)ghost_x.size();
+            L->ghost_chunks_x = number_ghost_ops(ghost_x);
+        }
+    }
+
     // ---- pack boxes
     std::vector<PackBox> pack_host(nb);
     {
@@ -1171,6 +1231,7 @@ extern "C" int bamrex_level_create(bamrex_level** out, const bamrex_level_desc* 
         for (int p = 0; p < 2; ++p) o_sweep[d][p] = take(sizeof(SweepBox) * nb);
     size_t o_ghost[3] = {};
     for (int d = 0; d < D; ++d) o_ghost[d] = take(std::max<size_t>(1, ghost_table_bytes(ghost_host[d].size(), L->ghost_chunks[d])));
+    const size_t o_ghost_x = take(std::max<size_t>(1, ghost_table_bytes(ghost_x.size(), L->ghost_chunks_x)));
     // tensor maps of the TMA-staged directions: per direction and parity,
     // one 128-byte map per box (64-byte aligned, as the TMA unit requires)
     constexpr size_t kMapBytes = 128;
@@ -1204,6 +1265,7 @@ extern "C" int bamrex_level_create(bamrex_level** out, const bamrex_level_desc* 
         for (int p = 0; p < 2; ++p) L->d_sweep[d][p] = (SweepBox*)(L->arena + o_sweep[d][p]);
         L->d_ghost[d] = (GhostOp*)(L->arena + o_ghost[d]);
     }
+    L->d_ghost_x = (GhostOp*)(L->arena + o_ghost_x);
     L->d_pack = (PackBox*)(L->arena + o_pack);
     L->d_scal = (StepScalars*)(L->arena + o_scal);
 
@@ -1223,6 +1285,9 @@ extern "C" int bamrex_level_create(bamrex_level** out, const bamrex_level_desc* 
                 t[b].in = L->fab[p][b];
                 t[b].out = L->fab[p ^ 1][b];
                 t[b].flux.p = nullptr;
+                if (d == 0 && L->x_fused)
+                    for (int side = 0; side < 2; ++side)
+                        if (xnb[side][(size_t)b] >= 0) t[b].xnb[side] = L->fab[p][(size_t)xnb[side][(size_t)b]];
             }
             if (L->tma(d)) {
                 struct alignas(64) Map {
@@ -1249,6 +1314,13 @@ extern "C" int bamrex_level_create(bamrex_level** out, const bamrex_level_desc* 
         if (ue == cudaSuccess) {
             const std::vector<int> ct = ghost_chunk_table(ghost_host[d], L->ghost_chunks[d]);
             ue = up(L->d_ghost[d] + ghost_host[d].size(), ct.data(), sizeof(int) * ct.size());
+        }
+    }
+    if (ue == cudaSuccess && L->x_fused) {
+        ue = up(L->d_ghost_x, ghost_x.data(), sizeof(GhostOp) * ghost_x.size());
+        if (ue == cudaSuccess) {
+            const std::vector<int> ct = ghost_chunk_table(ghost_x, L->ghost_chunks_x);
+            ue = up(L->d_ghost_x + ghost_x.size(), ct.data(), sizeof(int) * ct.size());
         }
     }
     if (ue == cudaSuccess) ue = up(L->d_pack, pack_host.data(), sizeof(PackBox) * nb);

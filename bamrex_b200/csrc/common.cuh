@@ -68,6 +68,10 @@ struct SweepBox {
     const void* tmap;
     int wa;
     int xoff;
+    // marching x sweep: the same-level fab holding all of this box's ghost
+    // cells below lo (xnb[0]) / above hi (xnb[1]) in x, read in place of
+    // the ghost cells when SweepArgs::xnb_on (p == nullptr: none)
+    FabDev xnb[2];
 };
 
 // Device-resident step scalars (graph-friendly time stepping).
@@ -96,6 +100,7 @@ struct SweepArgs {
     unsigned long long* ws_max;  // non-null: reduce max wave speed of Uout
     int do_update;             // 0: flux-only mode
     int* status;
+    int xnb_on;                // marching x sweep: read x halos from SweepBox::xnb
 };
 
 }  // namespace bamrex

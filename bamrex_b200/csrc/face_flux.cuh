@@ -19,7 +19,8 @@ template <typename T, int D, int DIR, int METHOD, int LIM>
 __global__ void __launch_bounds__(kRegThreads) register_faces_kernel(const FabDev* __restrict__ fabs, const RegisterTask t,
                                                                      const Consts kc, double dt, double dx,
                                                                      double scale, const StepScalars* scal,
-                                                                     double area1, double area2)
+                                                                     double area1, double area2,
+                                                                     const SweepBox* __restrict__ xsw)
 {
     using S = Scheme<T, D, DIR, METHOD, LIM>;
     constexpr int NC = D + 2;
@@ -50,12 +51,32 @@ __global__ void __launch_bounds__(kRegThreads) register_faces_kernel(const FabDe
         const T* p = fb.ptr<T>() + (long long)(r.i - fb.b0) + (long long)(r.j - fb.b1) * fb.js +
                      (long long)(r.k - fb.b2) * fb.ks;
         T Um2[NC], Um1[NC], U0[NC], Up1[NC];
+        if (DIR == 0 && xsw) {
+            // x halos read where the marching x sweep reads them: from the
+            // neighbouring box that holds them (the step's x ghost fill
+            // skips those ghost cells)
+            const SweepBox& B = xsw[r.box];
+            auto ld = [&](int x, T (&u)[NC]) {
+                const FabDev* g = &fb;
+                if (x < B.lo[0] && B.xnb[0].p) g = &B.xnb[0];
+                else if (x > B.hi[0] && B.xnb[1].p) g = &B.xnb[1];
+                const T* q = g->ptr<T>() + (long long)(x - g->b0) + (long long)(r.j - g->b1) * g->js +
+                             (long long)(r.k - g->b2) * g->ks;
 #pragma unroll
-        for (int n = 0; n < NC; ++n) {
-            Um2[n] = p[n * fb.ns - 2 * s];
-            Um1[n] = p[n * fb.ns - s];
-            U0[n] = p[n * fb.ns];
-            Up1[n] = p[n * fb.ns + s];
+                for (int n = 0; n < NC; ++n) u[n] = q[n * g->ns];
+            };
+            ld(r.i - 2, Um2);
+            ld(r.i - 1, Um1);
+            ld(r.i, U0);
+            ld(r.i + 1, Up1);
+        } else {
+#pragma unroll
+            for (int n = 0; n < NC; ++n) {
+                Um2[n] = p[n * fb.ns - 2 * s];
+                Um1[n] = p[n * fb.ns - s];
+                U0[n] = p[n * fb.ns];
+                Up1[n] = p[n * fb.ns + s];
+            }
         }
         T ULa[NC], URa[NC], ULb[NC], URb[NC], F[NC];
         S::cell(Um2, Um1, U0, k, hdtdx, ULa, URa);  // cell left of the face

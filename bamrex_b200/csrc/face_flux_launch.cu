@@ -12,7 +12,8 @@ extern template const void* pick_register_kernel<float>(int, int, int, int);
 
 cudaError_t launch_register_faces(int D, int dir, int method, bool fp32, const Consts& k, const FabDev* in,
                                   const RegisterTask& t, int NC, double dt, double dx_dir, double scale,
-                                  const StepScalars* scal, double area1, double area2, cudaStream_t s)
+                                  const StepScalars* scal, double area1, double area2, cudaStream_t s,
+                                  const SweepBox* xsw)
 {
     (void)NC;
     const int lim = fast_limiter(D, method, k);
@@ -25,7 +26,7 @@ cudaError_t launch_register_faces(int D, int dir, int method, bool fp32, const C
     RegisterTask tt = t;
     Consts kc = k;
     void* args[] = { (void*)&in, (void*)&tt, (void*)&kc, (void*)&dt, (void*)&dx_dir, (void*)&scale,
-                     (void*)&scal, (void*)&area1, (void*)&area2 };
+                     (void*)&scal, (void*)&area1, (void*)&area2, (void*)&xsw };
     return cudaLaunchKernel(fn, dim3(grid), dim3(threads), args, 0, s);
 }
 

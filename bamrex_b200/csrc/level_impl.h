@@ -82,6 +82,11 @@ struct bamrex_level {
     long long items[3] = { 0, 0, 0 };
     int seglen[3] = { 0, 0, 0 };
     bool x_march = false;  // x sweep by the marching (thread-per-row) kernel
+    // x halos read from the neighbouring boxes by the marching x sweep: the
+    // step's x ghost fill then runs the ops left (d_ghost_x), not d_ghost[0]
+    bool x_fused = false;
+    bamrex::GhostOp* d_ghost_x = nullptr;
+    int nghost_x = 0, ghost_chunks_x = 0;
     // kernel of each direction's sweep: BAMREX_STAGING_REGISTERS (sweep.cuh),
     // _TMA (per-warp march, sweep_tma.cuh) or _WAVE (block wavefront,
     // sweep_wave.cuh)
@@ -199,10 +204,16 @@ void body_destroy(bamrex_level* L);
 bool body_tag_tables(const bamrex_level* L, const FabDev** ls_tab, const FabDev** flag_tab);
 
 // Face fluxes of direction `dir` recomputed from the sweep input `in` at the
-// faces of a register task (face_flux.cu).
+// faces of a register task (face_flux.cu); xsw (direction 0 only, or null):
+// the x sweep's box table, whose neighbour fabs stand in for x ghost cells
+// the step's x fill skipped.
 cudaError_t launch_register_faces(int D, int dir, int method, bool fp32, const Consts& k, const FabDev* in,
                                   const RegisterTask& t, int NC, double dt, double dx_dir, double scale,
-                                  const StepScalars* scal, double area1, double area2, cudaStream_t s);
+                                  const StepScalars* scal, double area1, double area2, cudaStream_t s,
+                                  const SweepBox* xsw = nullptr);
+// Whether the x sweep of a step reads its x halos from the neighbouring
+// boxes (and the step's x ghost fill skips them).
+inline bool x_halos_fused(const bamrex_level* L) { return L->x_fused && !L->body; }
 
 // The network's 3x3 convolutions (16 -> 16, 2 -> 16, 16 -> 1) on the
 // tcgen05 tensor cores (conv_tc.cu): NCHW FP32 activations, BF16-rounded

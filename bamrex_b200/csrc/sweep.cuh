@@ -338,6 +338,12 @@ __global__ void __launch_bounds__(kSweepThreads, min_blocks<T>()) sweep_s_kernel
         const T* gin = nullptr;   // row 0 of the input / output fab, cell (lane % 4) of a chunk
         T* gout = nullptr;
         long long* srow = nullptr;  // per warp: the 32 rows' offsets in the input and output fabs
+                                    // and in the x neighbours' fabs (below, above)
+        // x halos read from the neighbouring boxes' fabs (null: from this
+        // box's ghost cells)
+        const T* xlo = nullptr;
+        const T* xhi = nullptr;
+        long long xlo_ns = 0, xhi_ns = 0;
         // start the asynchronous copy of the chunk at p0 into input buffer b
         // (positions outside the loadable range, or rows outside the box, get
         // the benign state); completes at the next wait_stage
@@ -345,13 +351,27 @@ __global__ void __launch_bounds__(kSweepThreads, min_blocks<T>()) sweep_s_kernel
             T* buf = sin + b * (NC * 32 * kStageW);
             const int c = lane & 3;
             const bool pin = p0 + c >= plo && p0 + c <= phi;
+            // the fab this lane's position lies in: a halo position of a
+            // box with a neighbour there reads the neighbour's own cell
+            const T* base = gin + p0;
+            long long ns = inns;
+            int so = 0;
+            if (xlo && p0 + c < B.lo[0]) {
+                base = xlo + (p0 + c);
+                ns = xlo_ns;
+                so = 64;
+            } else if (xhi && p0 + c > B.hi[0]) {
+                base = xhi + (p0 + c);
+                ns = xhi_ns;
+                so = 96;
+            }
 #pragma unroll
             for (int i = 0; i < 4; ++i) {
                 const int r = (lane >> 2) + 8 * i;
                 if (pin && r < rows_left) {
-                    const T* src = gin + srow[r] + p0;
+                    const T* src = base + srow[so + r];
 #pragma unroll
-                    for (int n = 0; n < NC; ++n) cp_async_elem(&buf[stage_slot(n * 32 + r, c)], src + n * inns);
+                    for (int n = 0; n < NC; ++n) cp_async_elem(&buf[stage_slot(n * 32 + r, c)], src + n * ns);
                 } else {
                     T u[NC];
                     benign(u);
@@ -386,7 +406,7 @@ __global__ void __launch_bounds__(kSweepThreads, min_blocks<T>()) sweep_s_kernel
             sout = sin + 2 * NC * 32 * kStageW;
             srow = reinterpret_cast<long long*>(bamrex_stage_smem + (size_t)(kSweepThreads / 32) *
                                                                           stage_elems_per_warp<T, NC>() * sizeof(T)) +
-                   wib * 64;
+                   wib * 128;
             // lane (r0 = lane / 4, c = lane % 4) moves rows r0 + 8 i, cell c
             gin = B.in.ptr<T>() + (lane & 3);
             gout = B.out.ptr<T>() + (lane & 3);
@@ -395,6 +415,24 @@ __global__ void __launch_bounds__(kSweepThreads, min_blocks<T>()) sweep_s_kernel
             wait_stage();  // the previous item's copies have landed and its reads are done
             srow[lane] = inoff;        // this lane's row: cell (i, lp, tr) at inoff + i
             srow[32 + lane] = outoff;
+            if (a.xnb_on) {
+                // a neighbour's fab covers the box's whole halo on that side
+                // (lanes past the box's rows keep in-range offsets of row 0)
+                if (B.xnb[0].p && s0 - H < B.lo[0]) {
+                    long long o, st;
+                    column(B.xnb[0], o, st);
+                    srow[64 + lane] = o;
+                    xlo = B.xnb[0].ptr<T>();
+                    xlo_ns = B.xnb[0].ns;
+                }
+                if (B.xnb[1].p && s1 - 1 + H > B.hi[0]) {
+                    long long o, st;
+                    column(B.xnb[1], o, st);
+                    srow[96 + lane] = o;
+                    xhi = B.xnb[1].ptr<T>();
+                    xhi_ns = B.xnb[1].ns;
+                }
+            }
             __syncwarp();
             issue(pbase, 0);
             wait_stage();

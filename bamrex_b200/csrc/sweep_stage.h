@@ -21,10 +21,11 @@ constexpr int stage_elems_per_warp() { return 3 * NC * 32 * kStageW; }
 __host__ __device__ constexpr int stage_slot(int row, int c) { return row * kStageW + ((c + (row >> 2)) & (kStageW - 1)); }
 
 // Dynamic shared memory of one block of the marching x sweep: the buffers,
-// then per warp the offsets of its 32 rows in the input and output fabs.
+// then per warp the offsets of its 32 rows in the input and output fabs and
+// in the fabs of the x neighbours below and above.
 inline int march_x_smem_bytes(int D, bool fp32)
 {
-    return (kStageBlockThreads / 32) * (3 * (D + 2) * 32 * kStageW * (fp32 ? 4 : 8) + 64 * 8);
+    return (kStageBlockThreads / 32) * (3 * (D + 2) * 32 * kStageW * (fp32 ? 4 : 8) + 128 * 8);
 }
 
 #ifdef __CUDACC__

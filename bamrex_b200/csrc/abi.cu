@@ -349,7 +349,9 @@ int choose_tma_seglen(int D, int dir, const std::vector<bamrex_box>& boxes, long
 // library: the kind with the least estimated time, from the slot-steps each
 // spends on the level's boxes (idle lanes, warm-up, pass rounding included,
 // at the segment lengths each would choose) times a measured time per
-// slot-step (B200, 4096^2 2D and 256^3 3D, per direction and storage type).
+// slot-step (B200, 4096^2 2D and 256^3 3D, per direction and storage type;
+// the FP64 3D y / z march and TMA figures refitted on 256^3 levels in 16^3,
+// 32^3 and 64^3 boxes, where the TMA march was the fastest y / z kernel).
 // rows / march: the two L2-loading x kernels.
 int auto_sweep_kind(int D, int d, bool fp32, const std::vector<bamrex_box>& boxes, int seg_rows, int seg_march,
                     int seg_tma, int seg_wave, bool allow_tma)
@@ -357,7 +359,7 @@ int auto_sweep_kind(int D, int d, bool fp32, const std::vector<bamrex_box>& boxe
     // picoseconds per slot-step: [fp32][D - 2][d] x {rows, march, TMA, wave}
     static const double ps[2][2][3][4] = {
         { { { 28, 37, 53, 27 }, { 0, 30, 29, 29 }, { 0, 0, 0, 0 } },
-          { { 39, 47, 70, 27.5 }, { 0, 36, 32, 28 }, { 0, 40, 35, 31 } } },
+          { { 39, 47, 70, 27.5 }, { 0, 31.5, 25, 28 }, { 0, 35, 27.5, 31 } } },
         { { { 12.6, 16, 18.5, 13.5 }, { 0, 15, 11, 15 }, { 0, 0, 0, 0 } },
           { { 16, 20, 23, 17 }, { 0, 19, 14, 19 }, { 0, 21, 15, 20 } } },
     };

@@ -205,6 +205,29 @@ def test_cluster_tags_matches_dense_restatement(seed):
         assert got == want, (D, n, kw)
 
 
+def test_cluster_tags_threaded_matches_dense_restatement():
+    """A level large enough (256^3 cells, 64^3 blocked cells) that the tag
+    scan, the allowed-cell test and the clipping run on several host threads
+    still gives exactly the restatement's boxes: sparse random tags and a
+    tagged spherical shell, periodic and non-periodic sides."""
+    from bamrex_b200.amr import cluster_tags
+    from oracle import amr_oracle as AO
+    rng = np.random.default_rng(4242)
+    n = 256
+    hi = (n - 1,) * 3
+    z, y, x = np.meshgrid(*([np.arange(n) + 0.5] * 3), indexing="ij")
+    shell = np.abs(np.sqrt((x - 128) ** 2 + (y - 120) ** 2 + (z - 136) ** 2) - 70) < 2
+    for per in ((0, 0, 0), (1, 0, 1)):
+        boxes = _random_level_boxes(rng, 3, n, 4)
+        t = shell | (rng.random([n] * 3) < 0.0005)
+        kw = dict(ref_ratio=2, blocking_factor=8, max_grid_size=32, n_error_buf=2, n_proper=1, grid_eff=0.7,
+                  periodic=per)
+        tags = _packed(3, t, boxes)
+        got = cluster_tags(3, (0, 0, 0), hi, boxes, tags, **kw)
+        want = AO.cluster_tags_dense(3, (0, 0, 0), hi, boxes, tags, **kw)
+        assert len(got) > 100 and got == want
+
+
 def test_tag_extra_restatement_small_cases():
     """box_error, interface_error and ghost_error of the restatement on
     hand-checked cells: the box tags the cells whose centres it contains,

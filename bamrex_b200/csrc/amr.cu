@@ -404,29 +404,27 @@ void build_ghost_regions(const bamrex_level* Lf, const BoxIndex& fidx, std::vect
     for (const auto& v : per) regs.insert(regs.end(), v.begin(), v.end());
 }
 
-// An allocator whose resize() leaves new elements uninitialised, so that a
-// joined table of records is written (and its pages first touched) once,
-// by the threads that copy into it.
+// A table of records in a buffer the caller owns (the coupling's pinned
+// staging buffer, or host memory where that cannot be had).
 template <class T>
-struct NoInit : std::allocator<T> {
-    template <class U>
-    struct rebind {
-        using other = NoInit<U>;
-    };
-    NoInit() = default;
-    template <class U>
-    NoInit(const NoInit<U>&) noexcept
-    {
-    }
-    template <class U, class... Args>
-    void construct(U* p, Args&&... args)
-    {
-        if constexpr (sizeof...(Args) == 0) ::new ((void*)p) U;
-        else ::new ((void*)p) U(std::forward<Args>(args)...);
-    }
+struct RecSpan {
+    T* p = nullptr;
+    size_t n = 0;
+    size_t size() const { return n; }
+    T* data() const { return p; }
+    T& operator[](size_t i) const { return p[i]; }
 };
-using FaceRecs = std::vector<FaceRec, NoInit<FaceRec>>;
-using RefluxRecs = std::vector<RefluxRec, NoInit<RefluxRec>>;
+using FaceRecs = RecSpan<FaceRec>;
+using RefluxRecs = RecSpan<RefluxRec>;
+
+// One direction's flux-register records per fine box, before the join.
+struct RegParts {
+    std::vector<std::vector<FaceRec>> cfb, ffb;
+    std::vector<std::vector<RefluxRec>> rrb;
+    std::vector<size_t> at;  // first slot of each box
+    size_t n = 0;            // slots
+    size_t per_rec = 1;      // fine faces per slot
+};
 
 // The bit map of a coarse domain for the duplicate-slot check, one per host
 // thread that builds couplings, kept between calls and left all zero.
@@ -437,18 +435,22 @@ std::vector<unsigned long long>& slot_bitmap(size_t words)
     return bits;
 }
 
-// Flux-register slots of direction d. The fine boxes run on host threads,
-// each filling its own record lists, which are then joined in box order.
-int build_register(const bamrex_coupling* C, int d, const BoxIndex& fidx, const BoxIndex& cidx, FaceRecs& cf,
-                   FaceRecs& ff, RefluxRecs& rr)
+// Flux-register slots of direction d, per fine box: the fine boxes run on
+// host threads, each filling its own record lists (register_join then
+// joins them in box order).
+int register_parts(const bamrex_coupling* C, int d, const BoxIndex& fidx, const BoxIndex& cidx, RegParts& P)
 {
     const bamrex_level* Lf = C->fine;
     const bamrex_level* Lc = C->crse;
     const int r = C->r, D = C->D;
     const int dlo = Lf->domain.lo[d], dhi = Lf->domain.hi[d], len = dhi - dlo + 1;
     const int nbf = (int)Lf->boxes.size();
-    std::vector<std::vector<FaceRec>> cfb(nbf), ffb(nbf);
-    std::vector<std::vector<RefluxRec>> rrb(nbf);
+    P.cfb.assign((size_t)nbf, {});
+    P.ffb.assign((size_t)nbf, {});
+    P.rrb.assign((size_t)nbf, {});
+    auto& cfb = P.cfb;
+    auto& ffb = P.ffb;
+    auto& rrb = P.rrb;
     // the r^(D-1) fine faces under a coarse face, transverse index fastest
     // in x, then y, then z
     const int tz = (D > 2 && d != 2) ? r : 1;
@@ -502,19 +504,28 @@ int build_register(const bamrex_coupling* C, int d, const BoxIndex& fidx, const 
     for (const auto& B : Lf->boxes) work += box_volume(B) / std::max(1, B.hi[d] - B.lo[d] + 1);
     ProfPhases phase("registers:boxes");
     BX_TRY(parallel_items<OwnerScratch>(nbf, table_threads(work), 4, box));
-    phase.next("registers:join");
-    // join in box order, the boxes' lists copied on host threads
-    std::vector<size_t> at(nbf + 1, 0);
-    for (int b = 0; b < nbf; ++b) at[b + 1] = at[b] + rrb[b].size();
-    const size_t n = at[nbf], per_rec = (size_t)tx * ty * tz;
-    rr.resize(n);
-    cf.resize(n);
-    ff.resize(n * per_rec);
+    P.at.assign((size_t)nbf + 1, 0);
+    for (int b = 0; b < nbf; ++b) P.at[(size_t)b + 1] = P.at[(size_t)b] + rrb[(size_t)b].size();
+    P.n = P.at[(size_t)nbf];
+    P.per_rec = (size_t)tx * ty * tz;
+    return BAMREX_OK;
+}
+
+// The records of register_parts joined in box order into the tables cf, ff
+// and rr (their buffers sized by the caller: P.n, P.n * P.per_rec, P.n),
+// the boxes' lists copied on host threads; then the check that no coarse
+// cell borders the fine region on both sides.
+int register_join(const bamrex_coupling* C, const RegParts& P, FaceRecs& cf, FaceRecs& ff, RefluxRecs& rr)
+{
+    const bamrex_level* Lc = C->crse;
+    const int nbf = (int)P.rrb.size();
+    const size_t n = P.n, per_rec = P.per_rec;
+    ProfPhases phase("registers:join");
     const int jt = table_threads((long long)n);
     parallel_items<int>(nbf, jt, 16, [&](int b, int&) -> std::string {
-        std::copy(rrb[b].begin(), rrb[b].end(), rr.begin() + at[b]);
-        std::copy(cfb[b].begin(), cfb[b].end(), cf.begin() + at[b]);
-        std::copy(ffb[b].begin(), ffb[b].end(), ff.begin() + at[b] * per_rec);
+        std::copy(P.rrb[(size_t)b].begin(), P.rrb[(size_t)b].end(), rr.data() + P.at[(size_t)b]);
+        std::copy(P.cfb[(size_t)b].begin(), P.cfb[(size_t)b].end(), cf.data() + P.at[(size_t)b]);
+        std::copy(P.ffb[(size_t)b].begin(), P.ffb[(size_t)b].end(), ff.data() + P.at[(size_t)b] * per_rec);
         return std::string();
     });
     phase.next("registers:dup");
@@ -632,9 +643,36 @@ extern "C" int bamrex_coupling_create(bamrex_coupling** out, bamrex_level* crse,
 
     phase.next("coupling_create:registers");
     // flux registers
+    RegParts parts[3];
+    for (int d = 0; d < D; ++d) BX_TRY(register_parts(C.get(), d, fidx, cidx, parts[d]));
+    // every direction's records in one pinned staging buffer, written once
+    // by the joining threads and uploaded from there (held to the end of
+    // this function, after the upload has completed)
+    size_t so[3][3] = {}, stage_bytes = 0;
+    for (int d = 0; d < D; ++d) {
+        const size_t sz[3] = { sizeof(RefluxRec) * parts[d].n, sizeof(FaceRec) * parts[d].n,
+                               sizeof(FaceRec) * parts[d].n * parts[d].per_rec };
+        for (int t = 0; t < 3; ++t) {
+            so[d][t] = stage_bytes;
+            stage_bytes = align_up(stage_bytes + sz[t], 64);
+        }
+    }
+    PinnedStage stage(stage_bytes);
+    std::vector<char> heap_stage;
+    char* sb = stage.data();
+    if (!sb && stage_bytes) {
+        heap_stage.resize(stage_bytes);
+        sb = heap_stage.data();
+    }
     FaceRecs cf[3], ff[3];
     RefluxRecs rr[3];
-    for (int d = 0; d < D; ++d) BX_TRY(build_register(C.get(), d, fidx, cidx, cf[d], ff[d], rr[d]));
+    for (int d = 0; d < D; ++d) {
+        rr[d] = RefluxRecs{ reinterpret_cast<RefluxRec*>(sb + so[d][0]), parts[d].n };
+        cf[d] = FaceRecs{ reinterpret_cast<FaceRec*>(sb + so[d][1]), parts[d].n };
+        ff[d] = FaceRecs{ reinterpret_cast<FaceRec*>(sb + so[d][2]), parts[d].n * parts[d].per_rec };
+        BX_TRY(register_join(C.get(), parts[d], cf[d], ff[d], rr[d]));
+        parts[d] = RegParts();
+    }
 
     phase.next("coupling_create:avg_down");
     // average_down

@@ -232,8 +232,52 @@ void dev_free(void* p, cudaStream_t s)
     cudaFreeAsync(p, s);
 }
 
+namespace {
+
+struct Stage {
+    std::mutex mu;
+    char* p = nullptr;
+    size_t cap = 0;
+};
+
+Stage& stage()
+{
+    static Stage* S = new Stage();  // never destroyed, as the pools
+    return *S;
+}
+
+}  // namespace
+
+PinnedStage::PinnedStage(size_t bytes) : lock_(stage().mu)
+{
+    Stage& S = stage();
+    if (bytes == 0) return;
+    if (S.cap < bytes) {
+        if (S.p) cudaFreeHost(S.p);
+        S.p = nullptr;
+        S.cap = 0;
+        const size_t want = bytes + bytes / 4;  // room for a level that grows
+        if (cudaMallocHost((void**)&S.p, want) == cudaSuccess) {
+            S.cap = want;
+        } else {
+            cudaGetLastError();
+            S.p = nullptr;
+        }
+    }
+    p_ = S.p;
+}
+
 int release_pooled()
 {
+    {
+        // the staging buffer first, under its own lock only (a holder of
+        // the stage may take the pools' lock, never the other way round)
+        Stage& S = stage();
+        std::lock_guard<std::mutex> sg(S.mu);
+        if (S.p) cudaFreeHost(S.p);
+        S.p = nullptr;
+        S.cap = 0;
+    }
     Pools& P = pools();
     std::lock_guard<std::mutex> g(P.mu);
     cudaError_t e = cudaDeviceSynchronize();

@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 
 #include <cstddef>
+#include <mutex>
 
 namespace bamrex {
 
@@ -29,6 +30,24 @@ void dev_free(void* p, cudaStream_t s);
 // Hand every page the pools keep but no block uses back to the driver
 // (0 or a cudaError_t).
 int release_pooled();
+
+// The process's pinned host staging buffer, at least `bytes` long, held with
+// its lock while the object lives: large table uploads are written there by
+// host threads and copied to the device in one DMA each, instead of going
+// through the driver's pageable path.  Grows (never shrinks) on demand;
+// data() is null if pinned memory could not be had.  The holder must let
+// its copies out of the buffer finish before the object goes.
+class PinnedStage {
+public:
+    explicit PinnedStage(size_t bytes);
+    char* data() const { return p_; }
+    PinnedStage(const PinnedStage&) = delete;
+    PinnedStage& operator=(const PinnedStage&) = delete;
+
+private:
+    std::unique_lock<std::mutex> lock_;
+    char* p_ = nullptr;
+};
 
 // Small pinned host blocks (up to 4 KB) for the scalars a step reads back,
 // cut from pinned slabs that are kept for the life of the process.

@@ -108,8 +108,10 @@ typedef struct bamrex_parm {
 /* Library identity and errors. */
 BAMREX_API int bamrex_abi_version(void);
 /* Device memory of destroyed levels, couplings and bodies stays in the
- * library's pool for the next ones; this hands the unused part back to the
- * driver (e.g. before a memory-hungry phase of the caller). */
+ * library's pool for the next ones (blocks of 64 MiB and more kept whole, to
+ * be handed out again as they are), and the pinned host buffer that stages
+ * table uploads is kept too; this hands all of it that no live object uses
+ * back to the driver (e.g. before a memory-hungry phase of the caller). */
 BAMREX_API int bamrex_release_memory(void);
 BAMREX_API const char *bamrex_last_error(void);
 BAMREX_API const char *bamrex_status_string(int status);

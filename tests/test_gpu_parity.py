@@ -1,6 +1,6 @@
 """GPU parity of the CUDA path (through the C ABI) against the CPU oracle.
 
-Bar (north star): FP64 results within 1e-12 relative L-infinity per
+Bar: FP64 results within 1e-12 relative L-infinity per
 component per step, from identical inputs; conserved totals within 1e-13.
 Relative L-infinity = max|gpu - ref| / max|ref| for each component.
 """
